@@ -1,0 +1,121 @@
+/*
+ * Test infrastructure (oracle): a plain-C, single-threaded restatement of the LPM-CPP
+ * implicit quasi-static step.  It is the checker for the device path: only tests, the smoke
+ * check and the CPU-baseline leg of the benchmark load it.  Each function names the
+ * reference file:line it follows.  Built by oracle/Makefile into oracle/liblpm_oracle.so.
+ */
+#ifndef LPM_ORACLE_H
+#define LPM_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* LatticeType order of include/lpm.h:97-106 */
+enum { LPMO_SQUARE2D = 0, LPMO_HEXAGON2D = 1, LPMO_SC3D = 2, LPMO_FCC3D = 3, LPMO_BCC3D = 4 };
+/* ParticleType order of include/lpm.h:89-95 (ElasticDamage / FatigueHCF are not on the path) */
+enum { LPMO_ELASTIC = 0, LPMO_J2 = 2 };
+
+typedef struct
+{
+    int lattice;
+    int ptype;
+    int n;                 /* particles */
+    const double *xyz;     /* n*3, generation order == particle id */
+    const int *type;       /* n, or NULL (all 0) */
+    double radius;
+    int plane_stress;
+    double E, mu, critical_bstrain;
+    double sigmay, xi, H, A; /* J2 only */
+    double nonlocal_L;
+    double nonlocal_cutoff_ratio; /* > 0: run the nonlocal neighbour search (assembly.h:118-130) */
+    int undamaged_type;
+    int max_iter;
+    double tol_iter;
+    double cg_rtol, cg_atol;   /* squared-norm tolerances of the RCI CG (solver.h:312-313) */
+    long long cg_maxit;        /* 0 -> problem size (solver.h:308) */
+} lpmo_desc;
+
+typedef struct
+{
+    const int *ids;
+    int count;
+    int flag;   /* 0 'x', 1 'y', 2 'z' */
+    double step;
+} lpmo_dispbc;
+
+typedef struct
+{
+    const int *ids;
+    int count;
+    double fx, fy, fz;
+} lpmo_forcebc;
+
+typedef struct
+{
+    const lpmo_dispbc *disp;
+    int ndisp;
+    const lpmo_forcebc *force;
+    int nforce;
+} lpmo_loadstep;
+
+typedef struct
+{
+    int newton_solves;     /* linear solves (Newton iterations that ran CG) */
+    long long cg_iters;
+    int cuts;              /* load-step halvings */
+    int converged;
+    double reaction_norm;  /* ||all reaction history|| */
+} lpmo_stats;
+
+typedef struct lpmo_problem lpmo_problem;
+
+/* utilities.h:15-91 */
+void lpmo_rmatrix(int eulerflag, const double angles[3], double R[9]);
+/* utilities.h:93-310 (+ a BCC generator, which the reference lacks); returns the count,
+ * writes at most cap points (n*3 doubles) when out != NULL */
+long lpmo_generate(int lattice, double radius, const double box[6], const double R[9], double *out, long cap);
+
+lpmo_problem *lpmo_create(const lpmo_desc *d);
+void lpmo_destroy(lpmo_problem *p);
+
+int lpmo_dim(const lpmo_problem *p);
+long lpmo_nbonds(const lpmo_problem *p);
+long lpmo_nconn_total(const lpmo_problem *p);
+long long lpmo_nnz_upper(const lpmo_problem *p);
+/* nb0/nb1: n each; p2: nbonds (per particle: layer-0 list then layer-1 list) */
+void lpmo_get_bonds(const lpmo_problem *p, int *nb0, int *nb1, int *p2);
+/* nconn/nlq: n each; conns: nconn_total */
+void lpmo_get_conns(const lpmo_problem *p, int *nconn, int *nlq, int *conns);
+
+/* assembly.h:133-138 then assembly.h:179-191 */
+void lpmo_update_geometry(lpmo_problem *p);
+void lpmo_update_force_state(lpmo_problem *p);
+void lpmo_update_state_var(lpmo_problem *p);
+/* solver.h:112-126; returns ||residual||, appends the reaction history */
+double lpmo_update_rr(lpmo_problem *p);
+
+/* stiffness.h:74-89 + 198-361 + 364-438: reference layout, 1-based upper CSR */
+void lpmo_assemble(lpmo_problem *p, int apply_bc);
+void lpmo_export_csr(const lpmo_problem *p, long long *K_pointer, long long *IK, long long *JK, double *K);
+/* solver.h:277-354 on the current K and residual; returns CG iterations, disp (n*dim) out */
+long long lpmo_cg(lpmo_problem *p, double *disp);
+
+/* solver.h:167-188 / 129-164 */
+void lpmo_apply_bc(lpmo_problem *p, const lpmo_loadstep *s);
+/* solver_static.h:99-152; returns 1 when converged */
+int lpmo_solve_problem_step(lpmo_problem *p, const lpmo_loadstep *s, lpmo_stats *st);
+/* one entry of solver_static.h:72-93: solve, and on failure reset, halve, retry */
+int lpmo_solve_load_step(lpmo_problem *p, const lpmo_loadstep *s, lpmo_stats *st);
+
+/* state read-back (n*3 / n*6 / n / n*nsv / nbonds) */
+void lpmo_read_state(const lpmo_problem *p, double *xyz, double *pin, double *stress, double *damage,
+                     double *damage_visual, double *state_var, double *bdamage);
+int lpmo_nstate_var(const lpmo_problem *p);
+void lpmo_read_residual(const lpmo_problem *p, double *res);
+void lpmo_set_xyz(lpmo_problem *p, const double *xyz);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

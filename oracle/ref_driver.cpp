@@ -1,0 +1,468 @@
+/*
+ * Test infrastructure (oracle): a driver that runs the LPM-CPP reference's own hot path
+ * (headers under <reference>/include, compiled unmodified) on a problem described by a
+ * small text spec, and writes its results as raw little-endian binaries.  It is built by
+ * oracle/Makefile into oracle/_ref/ and is only ever used as a checker or as the timed
+ * CPU baseline, never as part of the product.
+ *
+ * What it calls, in the order of an example's run() (examples/ex1_isoelasticity_2d_hex.cpp:31-120):
+ *   UnitCell, createRMatrix, createPlateHEX2D / createPlateSQ2D / createCuboidSC3D /
+ *   createCuboidFCC3D (include/utilities.h), Assembly(xyz, box, cell, ptype)
+ *   (include/assembly.h:98-106), setParticleProperty (include/particle_elastic.h:70-108,
+ *   include/particle_j2plasticity.h:154-198), LoadStep/DispBC/ForceBC, updateGeometry +
+ *   updateForceState, SolverStatic (include/solver_static.h:23-24) and either
+ *   SolverStatic::solveProblem (include/solver_static.h:65-96; "loop ref") or the same
+ *   step loop around SolverStatic::solveProblemStep without the per-step text dump
+ *   ("loop step", include/solver_static.h:72-93 minus line 89).
+ *
+ * Spec format: one directive per line, '#' starts a comment.
+ *   lattice hex2d|sq2d|sc3d|fcc3d      radius R       box x0 x1 y0 y1 z0 z1
+ *   euler FLAG A1 A2 A3 (radians)      ptype elastic|j2
+ *   plane_stress 0|1  E v  mu v  critical_bstrain v  j2 sigmay xi H A
+ *   nonlocal_L v  nonlocal_cutoff_ratio v  undamaged_type t  init_state_var 0|1
+ *   max_iter n  tol_iter v  cg_maxit_cap n
+ *   group NAME AXIS OP VALUE [AXIS OP VALUE]     (AXIS 0..2, OP '<' or '>'; conjunction)
+ *   settype NAME TYPE                            (assigned in spec order)
+ *   steps N
+ *   dispbc NAME FLAG STEP [FROM TO]              (FLAG x|y|z, steps FROM..TO-1)
+ *   forcebc NAME FX FY FZ [FROM TO]
+ *   dumpK STEP   (write the reference CSR after that load step; may repeat)
+ *   loop ref|step   out DIR   xyz_file PATH (optional: particle coordinates instead of a generator)
+ */
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+#include <map>
+#include <chrono>
+
+#include "lpm.h"
+#include "particle.h"
+#include "assembly.h"
+#include "utilities.h"
+#include "stiffness.h"
+#include "load_step.h"
+#include "solver_static.h"
+
+static const int NL = 2;
+
+struct Cond
+{
+    int axis;
+    char op;
+    double value;
+};
+
+struct GroupSpec
+{
+    std::string name;
+    std::vector<Cond> conds;
+};
+
+struct DispSpec
+{
+    std::string group;
+    char flag;
+    double step;
+    int from, to;
+};
+
+struct ForceSpec
+{
+    std::string group;
+    double fx, fy, fz;
+    int from, to;
+};
+
+struct Spec
+{
+    std::string lattice = "hex2d";
+    double radius = 0.1;
+    std::array<double, 6> box{0, 1, 0, 1, 0, 1};
+    int euler_flag = 0;
+    double angles[3] = {0, 0, 0};
+    std::string ptype = "elastic";
+    int plane_stress = 0;
+    double E = 69e3, mu = 0.3, critical_bstrain = 1.0;
+    double sigmay = 200, xi = 0, H = 0, A = 0;
+    double nonlocal_L = 0, nonlocal_cutoff_ratio = 0;
+    int undamaged_type = -1;
+    int init_state_var = 0;
+    int max_iter = 30;
+    double tol_iter = 1e-5;
+    long long cg_maxit_cap = 0;
+    std::vector<GroupSpec> groups;
+    std::vector<std::pair<std::string, int>> settypes;
+    int steps = 1;
+    std::vector<DispSpec> disp;
+    std::vector<ForceSpec> force;
+    std::vector<int> dumpK;
+    std::string loop = "step";
+    std::string out = ".";
+    std::string xyz_file;
+};
+
+static Spec parse(const char *path)
+{
+    Spec s;
+    std::ifstream f(path);
+    if (!f)
+    {
+        std::fprintf(stderr, "cannot open spec %s\n", path);
+        std::exit(2);
+    }
+    std::string line;
+    while (std::getline(f, line))
+    {
+        auto h = line.find('#');
+        if (h != std::string::npos)
+            line = line.substr(0, h);
+        std::istringstream is(line);
+        std::string k;
+        if (!(is >> k))
+            continue;
+        if (k == "lattice") is >> s.lattice;
+        else if (k == "radius") is >> s.radius;
+        else if (k == "box") for (int i = 0; i < 6; ++i) is >> s.box[i];
+        else if (k == "euler") is >> s.euler_flag >> s.angles[0] >> s.angles[1] >> s.angles[2];
+        else if (k == "ptype") is >> s.ptype;
+        else if (k == "plane_stress") is >> s.plane_stress;
+        else if (k == "E") is >> s.E;
+        else if (k == "mu") is >> s.mu;
+        else if (k == "critical_bstrain") is >> s.critical_bstrain;
+        else if (k == "j2") is >> s.sigmay >> s.xi >> s.H >> s.A;
+        else if (k == "nonlocal_L") is >> s.nonlocal_L;
+        else if (k == "nonlocal_cutoff_ratio") is >> s.nonlocal_cutoff_ratio;
+        else if (k == "undamaged_type") is >> s.undamaged_type;
+        else if (k == "init_state_var") is >> s.init_state_var;
+        else if (k == "max_iter") is >> s.max_iter;
+        else if (k == "tol_iter") is >> s.tol_iter;
+        else if (k == "cg_maxit_cap") is >> s.cg_maxit_cap;
+        else if (k == "group")
+        {
+            GroupSpec g;
+            is >> g.name;
+            Cond c;
+            std::string op;
+            while (is >> c.axis >> op >> c.value)
+            {
+                c.op = op[0];
+                g.conds.push_back(c);
+            }
+            s.groups.push_back(g);
+        }
+        else if (k == "settype")
+        {
+            std::string n;
+            int t;
+            is >> n >> t;
+            s.settypes.push_back({n, t});
+        }
+        else if (k == "steps") is >> s.steps;
+        else if (k == "dispbc")
+        {
+            DispSpec d;
+            std::string fl;
+            is >> d.group >> fl >> d.step;
+            d.flag = fl[0];
+            d.from = 0;
+            d.to = 1 << 30;
+            is >> d.from >> d.to;
+            s.disp.push_back(d);
+        }
+        else if (k == "forcebc")
+        {
+            ForceSpec d;
+            is >> d.group >> d.fx >> d.fy >> d.fz;
+            d.from = 0;
+            d.to = 1 << 30;
+            is >> d.from >> d.to;
+            s.force.push_back(d);
+        }
+        else if (k == "dumpK")
+        {
+            int st;
+            is >> st;
+            s.dumpK.push_back(st);
+        }
+        else if (k == "loop") is >> s.loop;
+        else if (k == "out") is >> s.out;
+        else if (k == "xyz_file") is >> s.xyz_file;
+        else
+        {
+            std::fprintf(stderr, "unknown spec directive '%s'\n", k.c_str());
+            std::exit(2);
+        }
+    }
+    return s;
+}
+
+template <typename T>
+static void write_bin(const std::string &path, const T *data, size_t count)
+{
+    FILE *f = std::fopen(path.c_str(), "wb");
+    if (!f)
+    {
+        std::fprintf(stderr, "cannot write %s\n", path.c_str());
+        std::exit(3);
+    }
+    if (count)
+        std::fwrite(data, sizeof(T), count, f);
+    std::fclose(f);
+}
+
+static double wall()
+{
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+static LatticeType lattice_of(const std::string &s)
+{
+    if (s == "hex2d") return LatticeType::Hexagon2D;
+    if (s == "sq2d") return LatticeType::Square2D;
+    if (s == "sc3d") return LatticeType::SimpleCubic3D;
+    if (s == "fcc3d") return LatticeType::FCC3D;
+    if (s == "bcc3d") return LatticeType::BCC3D_1Slip;
+    std::fprintf(stderr, "unknown lattice %s\n", s.c_str());
+    std::exit(2);
+}
+
+int main(int argc, char **argv)
+{
+    if (argc < 2)
+    {
+        std::fprintf(stderr, "usage: lpm_ref SPEC\n");
+        return 2;
+    }
+    Spec sp = parse(argv[1]);
+    lpm_shim_stats_g.cg_maxit_override = sp.cg_maxit_cap;
+    const double t_setup0 = wall();
+
+    UnitCell cell(lattice_of(sp.lattice), sp.radius);
+    double *R = createRMatrix(sp.euler_flag, sp.angles);
+    std::array<double, 2 * NDIM> box = sp.box;
+    std::vector<std::array<double, NDIM>> xyz;
+    if (!sp.xyz_file.empty())
+    {
+        FILE *f = std::fopen(sp.xyz_file.c_str(), "rb");
+        if (!f)
+        {
+            std::fprintf(stderr, "cannot open %s\n", sp.xyz_file.c_str());
+            return 2;
+        }
+        std::array<double, NDIM> p;
+        while (std::fread(p.data(), sizeof(double), 3, f) == 3)
+            xyz.push_back(p);
+        std::fclose(f);
+    }
+    else if (sp.lattice == "hex2d") xyz = createPlateHEX2D(box, cell, R);
+    else if (sp.lattice == "sq2d") xyz = createPlateSQ2D(box, cell, R);
+    else if (sp.lattice == "sc3d") xyz = createCuboidSC3D(box, cell, R);
+    else if (sp.lattice == "fcc3d") xyz = createCuboidFCC3D(box, cell, R);
+    else
+    {
+        std::fprintf(stderr, "lattice %s needs xyz_file\n", sp.lattice.c_str());
+        return 2;
+    }
+
+    ParticleType pt = (sp.ptype == "j2") ? ParticleType::J2Plasticity : ParticleType::Elastic;
+    Assembly<NL> ass{xyz, box, cell, pt};
+    const int N = ass.nparticle;
+    const int dim = cell.dim;
+
+    std::map<std::string, std::vector<Particle<NL> *>> groups;
+    for (auto &g : sp.groups)
+    {
+        std::vector<Particle<NL> *> mem;
+        for (Particle<NL> *p : ass.pt_sys)
+        {
+            bool ok = true;
+            for (auto &c : g.conds)
+                ok = ok && ((c.op == '<') ? (p->xyz[c.axis] < c.value) : (p->xyz[c.axis] > c.value));
+            if (ok)
+                mem.push_back(p);
+        }
+        groups[g.name] = mem;
+    }
+    for (auto &st : sp.settypes)
+        for (Particle<NL> *p : groups[st.first])
+            p->type = st.second;
+
+    for (Particle<NL> *p : ass.pt_sys)
+    {
+        if (pt == ParticleType::J2Plasticity)
+            dynamic_cast<ParticleJ2Plasticity<NL> *>(p)->setParticleProperty(
+                sp.nonlocal_L, sp.plane_stress != 0, sp.E, sp.mu, sp.sigmay, sp.xi, sp.H, sp.A, sp.critical_bstrain);
+        else
+            dynamic_cast<ParticleElastic<NL> *>(p)->setParticleProperty(sp.nonlocal_L, sp.plane_stress != 0, sp.E,
+                                                                        sp.mu, sp.critical_bstrain);
+    }
+
+    std::vector<LoadStep<NL>> load;
+    for (int s = 0; s < sp.steps; ++s)
+    {
+        LoadStep<NL> step;
+        for (auto &d : sp.disp)
+            if (s >= d.from && s < d.to)
+                step.dispBCs.push_back(DispBC<NL>(groups[d.group], LoadMode::Relative, d.flag, d.step));
+        for (auto &f : sp.force)
+            if (s >= f.from && s < f.to)
+                step.forceBCs.push_back(ForceBC<NL>(groups[f.group], LoadMode::Relative, f.fx, f.fy, f.fz));
+        load.push_back(step);
+    }
+
+    if (sp.nonlocal_cutoff_ratio > 0)
+        ass.searchNonlocalNeighbors(sp.nonlocal_cutoff_ratio);
+    ass.updateGeometry();
+    ass.updateForceState();
+    if (sp.init_state_var)
+        ass.updateStateVar();
+
+    SolverStatic<NL> solv{sp.undamaged_type, ass, StiffnessMode::Analytical, SolverMode::CG, "/dev/null",
+                          sp.max_iter, sp.tol_iter};
+    const double t_setup1 = wall();
+
+    /* setup outputs: coordinates, bonds (per particle: layer-0 list then layer-1 list), conns */
+    {
+        std::vector<double> x0(3 * (size_t)N);
+        std::vector<int> nb0(N), nb1(N), bp2, nconn(N), nlq(N), conns;
+        for (Particle<NL> *p : ass.pt_sys)
+        {
+            for (int k = 0; k < 3; ++k)
+                x0[3 * p->id + k] = p->xyz_initial[k];
+            nb0[p->id] = (int)p->bond_layers[0].size();
+            nb1[p->id] = (int)p->bond_layers[1].size();
+            nconn[p->id] = p->nconn;
+            nlq[p->id] = p->nconn_largeq;
+        }
+        for (Particle<NL> *p : ass.pt_sys)
+        {
+            for (int l = 0; l < NL; ++l)
+                for (Bond<NL> *b : p->bond_layers[l])
+                    bp2.push_back(b->p2->id);
+            for (Particle<NL> *c : p->conns)
+                conns.push_back(c->id);
+        }
+        std::vector<int> types(N);
+        for (Particle<NL> *p : ass.pt_sys)
+            types[p->id] = p->type;
+        write_bin(sp.out + "/xyz0.f64", x0.data(), x0.size());
+        write_bin(sp.out + "/nb0.i32", nb0.data(), nb0.size());
+        write_bin(sp.out + "/nb1.i32", nb1.data(), nb1.size());
+        write_bin(sp.out + "/bond_p2.i32", bp2.data(), bp2.size());
+        write_bin(sp.out + "/nconn.i32", nconn.data(), nconn.size());
+        write_bin(sp.out + "/nlq.i32", nlq.data(), nlq.size());
+        write_bin(sp.out + "/conns.i32", conns.data(), conns.size());
+        write_bin(sp.out + "/type.i32", types.data(), types.size());
+        std::vector<double> pin0(3 * (size_t)N);
+        for (Particle<NL> *p : ass.pt_sys)
+            for (int k = 0; k < 3; ++k)
+                pin0[3 * p->id + k] = p->Pin[k];
+        write_bin(sp.out + "/pin_init.f64", pin0.data(), pin0.size());
+    }
+
+    FILE *log = std::fopen((sp.out + "/steps.txt").c_str(), "w");
+    std::fprintf(log, "# N %d dim %d setup_s %.6f threads %d\n", N, dim, t_setup1 - t_setup0, omp_get_max_threads());
+    std::fprintf(log, "# step newton_solves cg_iters wall_s spmv_s cg_s create_s cuts reaction_norm cg_fail\n");
+
+    int start_index = 0;
+    for (int s = 0; s < sp.steps; ++s)
+    {
+        lpm_shim_stats st0 = lpm_shim_stats_g;
+        double t0 = wall();
+        int cuts = 0;
+        if (sp.loop == "ref")
+        {
+            std::vector<LoadStep<NL>> one{load[s]};
+            solv.solveProblem(one, start_index);
+            cuts = (int)one.size() - 1;
+        }
+        else
+        {
+            /* the loop of SolverStatic::solveProblem (include/solver_static.h:72-93) without the dump */
+            std::vector<LoadStep<NL>> one{load[s]};
+            int n_step = (int)one.size();
+            double dt = 1;
+            for (int i = 0; i < n_step; i++)
+            {
+                bool ok = solv.solveProblemStep(one[i], dt);
+                if (!ok)
+                {
+                    solv.ass.resetStateVar(true);
+                    one[i].loadCutHalf();
+                    one.insert(one.begin() + i, one[i]);
+                    ++n_step;
+                    ++cuts;
+                    --i;
+                    if (cuts > 40)
+                    {
+                        std::fprintf(stderr, "too many load cuts at step %d\n", s);
+                        return 4;
+                    }
+                }
+            }
+            start_index += n_step;
+        }
+        double t1 = wall();
+        lpm_shim_stats st1 = lpm_shim_stats_g;
+        double rn = cblas_dnrm2((MKL_INT)solv.reaction_force.size(), solv.reaction_force.data(), 1);
+        std::fprintf(log, "%d %lld %lld %.6f %.6f %.6f %.6f %d %.17g %lld\n", s, st1.cg_solves - st0.cg_solves,
+                     st1.cg_iterations - st0.cg_iterations, t1 - t0, st1.spmv_seconds - st0.spmv_seconds,
+                     st1.cg_seconds - st0.cg_seconds, st1.create_seconds - st0.create_seconds, cuts, rn,
+                     st1.cg_failures - st0.cg_failures);
+        std::fflush(log);
+
+        char tag[32];
+        std::snprintf(tag, sizeof tag, "%03d", s);
+        std::vector<double> x(3 * (size_t)N), pin(3 * (size_t)N), stress(6 * (size_t)N), dmg(N), dmgv(N), sv,
+            bdmg, dlp;
+        int nsv = (int)ass.pt_sys[0]->state_var.size();
+        sv.resize((size_t)nsv * N);
+        for (Particle<NL> *p : ass.pt_sys)
+        {
+            for (int k = 0; k < 3; ++k)
+            {
+                x[3 * p->id + k] = p->xyz[k];
+                pin[3 * p->id + k] = p->Pin[k];
+            }
+            for (int k = 0; k < 6; ++k)
+                stress[6 * p->id + k] = p->stress[k];
+            dmg[p->id] = p->damage;
+            dmgv[p->id] = p->damage_visual;
+            for (int k = 0; k < nsv; ++k)
+                sv[(size_t)nsv * p->id + k] = p->state_var[k];
+        }
+        for (Particle<NL> *p : ass.pt_sys)
+            for (int l = 0; l < NL; ++l)
+                for (Bond<NL> *b : p->bond_layers[l])
+                {
+                    bdmg.push_back(b->bdamage);
+                    dlp.push_back(b->dLp);
+                }
+        write_bin(sp.out + "/xyz_" + tag + ".f64", x.data(), x.size());
+        write_bin(sp.out + "/pin_" + tag + ".f64", pin.data(), pin.size());
+        write_bin(sp.out + "/stress_" + tag + ".f64", stress.data(), stress.size());
+        write_bin(sp.out + "/damage_" + tag + ".f64", dmg.data(), dmg.size());
+        write_bin(sp.out + "/damage_visual_" + tag + ".f64", dmgv.data(), dmgv.size());
+        write_bin(sp.out + "/state_var_" + tag + ".f64", sv.data(), sv.size());
+        write_bin(sp.out + "/bdamage_" + tag + ".f64", bdmg.data(), bdmg.size());
+        write_bin(sp.out + "/dlp_" + tag + ".f64", dlp.data(), dlp.size());
+
+        bool dump = false;
+        for (int d : sp.dumpK)
+            dump = dump || (d == s);
+        if (dump)
+        {
+            const long long nnz = solv.stiffness.K_pointer[N];
+            write_bin(sp.out + "/K_pointer_" + tag + ".i64", solv.stiffness.K_pointer, (size_t)N + 1);
+            write_bin(sp.out + "/IK_" + tag + ".i64", solv.stiffness.IK, (size_t)dim * N + 1);
+            write_bin(sp.out + "/JK_" + tag + ".i64", solv.stiffness.JK, (size_t)nnz);
+            write_bin(sp.out + "/K_" + tag + ".f64", solv.stiffness.K_global, (size_t)nnz);
+        }
+    }
+    std::fclose(log);
+    return 0;
+}
