@@ -1,0 +1,182 @@
+/*
+ * lpmgpu: B200-native implicit quasi-static step of the nonlocal lattice particle method.
+ *
+ * This is the C ABI of liblpmgpu.so: plain pointers, sizes and status codes, no CUDA or
+ * torch types.  It replaces, for one load step of LPM-CPP, the code path
+ *   SolverStatic<nlayer>::solveProblem / solveProblemStep   (include/solver_static.h:65-152)
+ *   Solver<nlayer>::NewtonIteration / updateRR / BCs / LPM_CG (include/solver.h:55-188, 277-354)
+ *   Stiffness<nlayer>::calcStiffness2D/3D / updateStiffnessDispBC (include/stiffness.h:198-438)
+ *   Assembly<nlayer>::createBonds / updateConnections / updateGeometry / updateForceState
+ *                                                            (include/assembly.h:133-266)
+ * (paths inside the LPM-CPP tree).  Every entry point returns an lpmgpu_status; none exits
+ * the process.  One handle belongs to one host thread at a time; the server API is the
+ * thread-safe entry for concurrent submitters.
+ */
+#ifndef LPMGPU_H
+#define LPMGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------------------- status */
+typedef enum
+{
+    LPMGPU_OK = 0,
+    LPMGPU_ERR_INVALID_ARG = 1,   /* bad pointer, size or enum value */
+    LPMGPU_ERR_CUDA = 2,          /* a CUDA runtime call failed (message via lpmgpu_last_error) */
+    LPMGPU_ERR_OUT_OF_MEMORY = 3, /* device allocation failed */
+    LPMGPU_ERR_NEWTON = 4,        /* Newton hit max_iter (solver_static.h:122, the load-cut trigger) */
+    LPMGPU_ERR_CG_MAXIT = 5,      /* a CG solve reached its cap; printed and ignored by the reference
+                                     (solver.h:338-349); reported through stats, never returned */
+    LPMGPU_ERR_TIMEOUT = 6,       /* a bounded device-side wait gave up; the context stays usable */
+    LPMGPU_ERR_TOPOLOGY = 7,      /* a particle without bonds, or more bonds/connections than supported */
+    LPMGPU_ERR_BUDGET = 8,        /* request larger than the server's HBM budget */
+    LPMGPU_ERR_CUTS = 9,          /* a load step was halved more than 30 times */
+    LPMGPU_ERR_NOT_READY = 10,    /* server: result not available yet */
+    LPMGPU_ERR_NO_DEVICE = 11     /* no CUDA device; the library has no CPU fallback */
+} lpmgpu_status;
+
+/* LatticeType (include/lpm.h:97-106); BCC3D covers the three BCC enum values */
+enum { LPMGPU_SQUARE2D = 0, LPMGPU_HEXAGON2D = 1, LPMGPU_SC3D = 2, LPMGPU_FCC3D = 3, LPMGPU_BCC3D = 4 };
+/* ParticleType (include/lpm.h:89-95) values on this path */
+enum { LPMGPU_ELASTIC = 0, LPMGPU_J2 = 2 };
+/* linear-solve precision */
+enum { LPMGPU_FP64 = 0, LPMGPU_MIXED = 1 };
+
+typedef struct lpmgpu_solver lpmgpu_solver;
+
+/* One problem (an Assembly plus its solver settings). */
+typedef struct
+{
+    int32_t lattice;         /* LPMGPU_SQUARE2D .. LPMGPU_BCC3D */
+    int32_t ptype;           /* LPMGPU_ELASTIC or LPMGPU_J2 */
+    int32_t n;               /* particles */
+    const double *xyz;       /* host, n*3; row q is particle id q (generation order) */
+    const int32_t *type;     /* host, n particle types, or NULL for all 0 */
+    double radius;           /* UnitCell radius */
+    int32_t plane_stress;    /* setParticleProperty is_plane_stress */
+    double E, mu;            /* Young's modulus, Poisson's ratio */
+    double critical_bstrain; /* elastic bond breaking strain (particle_elastic.h:60) */
+    double sigmay, xi, H, A; /* J2 parameters (particle_j2plasticity.h:155-163) */
+    double nonlocal_L;       /* nonlocal length (no nonlocal search is run: solver_static.h:37-52) */
+    int32_t undamaged_type;  /* SolverStatic undamaged_pt_type */
+    int32_t max_iter;        /* Newton iteration cap (max_NR_iter) */
+    double tol_iter;         /* Newton tolerance (tol_NR_iter) */
+    double cg_rtol, cg_atol; /* squared-norm CG test ||r||^2 <= rtol*||r0||^2 + atol (solver.h:312-313) */
+    int64_t cg_maxit;        /* CG cap, 0 = problem size (solver.h:308) */
+    int32_t precision;       /* LPMGPU_FP64 or LPMGPU_MIXED */
+    int32_t device;          /* CUDA device ordinal */
+} lpmgpu_desc;
+
+/* Displacement / force boundary condition of one load step (boundary.h:10-44, Relative mode). */
+typedef struct
+{
+    const int32_t *ids; /* host particle ids of the group */
+    int32_t count;
+    int32_t flag;       /* 0 'x', 1 'y', 2 'z' */
+    double step;
+} lpmgpu_dispbc;
+
+typedef struct
+{
+    const int32_t *ids;
+    int32_t count;
+    double fx, fy, fz;
+} lpmgpu_forcebc;
+
+typedef struct
+{
+    const lpmgpu_dispbc *disp;
+    int32_t ndisp;
+    const lpmgpu_forcebc *force;
+    int32_t nforce;
+} lpmgpu_load_step;
+
+typedef struct
+{
+    int32_t converged;       /* 1 when the load step (with any halvings) converged */
+    int32_t newton_solves;   /* linear solves (Newton iterations that ran CG) */
+    int32_t cuts;            /* load-step halvings (solver_static.h:78-87) */
+    int32_t damage_iters;    /* passes of the damage loop (solver_static.h:107-139) */
+    int64_t cg_iters;        /* CG iterations (FP32 inner + FP64 in mixed mode) */
+    int64_t cg_maxit_hits;   /* CG solves that stopped at their cap */
+    int32_t refinements;     /* mixed mode: outer refinement steps */
+    double reaction_norm;    /* ||reaction history|| (solver.h:64) */
+    double residual_norm;    /* final Newton residual norm */
+    double seconds;          /* device time of the call */
+} lpmgpu_stats;
+
+typedef struct
+{
+    int32_t n, dim;
+    int64_t nbonds;       /* directed bonds */
+    int64_t nnzb;         /* full symmetric block count (sum of nconn) */
+    int64_t nnz_upper;    /* reference K_pointer[n] */
+    int32_t max_bonds;    /* largest bond list */
+    int32_t max_conns;    /* largest connection list */
+    int64_t device_bytes; /* device memory held by the handle */
+} lpmgpu_sizes;
+
+const char *lpmgpu_version(void);
+const char *lpmgpu_status_string(int32_t status);
+/* message of the last CUDA error seen by this thread (empty when none) */
+const char *lpmgpu_last_error(void);
+
+/* Host-side lattice generators, the reference's createPlateSQ2D / createPlateHEX2D /
+ * createCuboidSC3D / createCuboidFCC3D (include/utilities.h:93-310) and a BCC generator the
+ * reference lacks.  Writes min(count, cap) points to out (3 doubles each); *count gets the total. */
+int32_t lpmgpu_generate_lattice(int32_t lattice, double radius, const double box[6], int32_t euler_flag,
+                                const double angles[3], double *out, int64_t cap, int64_t *count);
+
+/* Builds the device state: bonds and connections (Assembly ctor, assembly.h:98-106, 213-266),
+ * the block pattern, material constants (setParticleProperty), then updateGeometry +
+ * updateForceState as the examples do before constructing the solver. */
+int32_t lpmgpu_create(const lpmgpu_desc *desc, lpmgpu_solver **out);
+int32_t lpmgpu_destroy(lpmgpu_solver *h);
+int32_t lpmgpu_get_sizes(const lpmgpu_solver *h, lpmgpu_sizes *out);
+/* nb0/nb1/nconn/nlq: n each; bond_p2: nbonds (per particle, layer-0 list then layer-1 list,
+ * ascending partner id); conns: nnzb (per particle, ascending id).  Any pointer may be NULL. */
+int32_t lpmgpu_get_topology(const lpmgpu_solver *h, int32_t *nb0, int32_t *nb1, int32_t *bond_p2,
+                            int32_t *nconn, int32_t *nlq, int32_t *conns);
+
+/* Assembly::updateGeometry + updateForceState (assembly.h:133-138, 179-191) */
+int32_t lpmgpu_update_force_state(lpmgpu_solver *h);
+/* Assembly::updateStateVar (assembly.h:162-166): the J2 return map */
+int32_t lpmgpu_update_state_var(lpmgpu_solver *h);
+/* Solver::updateRR (solver.h:112-126); *norm gets ||residual|| */
+int32_t lpmgpu_update_rr(lpmgpu_solver *h, double *norm);
+/* Stiffness::reset + calcStiffness2D/3D (+ updateStiffnessDispBC when apply_bc) */
+int32_t lpmgpu_assemble(lpmgpu_solver *h, int32_t apply_bc);
+/* The assembled matrix in the reference's layout: 1-based upper CSR K_pointer[n+1],
+ * IK[dim*n+1], JK[nnz_upper], K[nnz_upper] (stiffness.h:24-26, 198-361).  Any may be NULL. */
+int32_t lpmgpu_export_ref_csr(const lpmgpu_solver *h, int64_t *K_pointer, int64_t *IK, int64_t *JK, double *K);
+/* Solver::LPM_CG (solver.h:277-354) on the current K and residual; disp (host, dim*n) may be NULL */
+int32_t lpmgpu_solve_linear(lpmgpu_solver *h, double *disp, lpmgpu_stats *stats);
+/* updateForceBC + updateDisplacementBC (solver.h:129-188) */
+int32_t lpmgpu_apply_load_step(lpmgpu_solver *h, const lpmgpu_load_step *step);
+/* SolverStatic::solveProblemStep (solver_static.h:99-152): returns LPMGPU_ERR_NEWTON on failure */
+int32_t lpmgpu_solve_problem_step(lpmgpu_solver *h, const lpmgpu_load_step *step, lpmgpu_stats *stats);
+/* One load step of SolverStatic::solveProblem (solver_static.h:72-93) with halve-and-retry */
+int32_t lpmgpu_solve_load_step(lpmgpu_solver *h, const lpmgpu_load_step *step, lpmgpu_stats *stats);
+/* Assembly::storeStateVar / resetStateVar(true) (assembly.h:141-159) */
+int32_t lpmgpu_store_state(lpmgpu_solver *h);
+int32_t lpmgpu_reset_state(lpmgpu_solver *h);
+
+/* Device state back to host (any pointer may be NULL): xyz n*3, Pin n*3, stress n*6 (s11 s22
+ * s33 s23 s13 s12), damage n, damage_visual n, state_var n*nsv (nsv = 7 for J2, else 1),
+ * bdamage nbonds, residual dim*n. */
+int32_t lpmgpu_read_state(const lpmgpu_solver *h, double *xyz, double *pin, double *stress, double *damage,
+                          double *damage_visual, double *state_var, double *bdamage);
+int32_t lpmgpu_read_residual(const lpmgpu_solver *h, double *residual);
+int32_t lpmgpu_set_xyz(lpmgpu_solver *h, const double *xyz);
+/* Device time of the last call's phases, seconds: [0] force/geometry, [1] assembly,
+ * [2] linear solves, [3] other */
+int32_t lpmgpu_get_phase_times(const lpmgpu_solver *h, double *t4);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,498 @@
+// Linear solve of the Newton step: the replacement for Solver::LPM_CG (include/solver.h:277-354),
+// i.e. MKL's RCI dcg with mkl_sparse_d_mv on the symmetric upper CSR.
+//
+// One persistent cooperative launch runs the whole unpreconditioned CG (x0 = 0, stop when
+// ||r||^2 <= rtol*||r0||^2 + atol, cap = problem size, the squared-norm test of MKL's dcg with
+// dpar[0] = dpar[1] = 1e-12 set at solver.h:312-313).  Per iteration:
+//   phase A  q = K p_new, with p_new = r + beta*p_old formed on the fly from the gathered
+//            r and p_old (so the direction update needs no pass of its own); partial p.q
+//   barrier
+//   phase B  x += alpha p_new, r -= alpha q; partial r.r
+//   barrier
+// Every reduction is a fixed tree, and every block reduces the per-block partials in the same
+// order, so all blocks take identical decisions and a run is bit-reproducible.  The grid
+// barrier is a sense-counting barrier with a time limit: a wait that exceeds it records
+// LPMGPU_ERR_TIMEOUT and the kernel returns.
+//
+// The block-CSR SpMV assigns one warp per particle row: the row's d*d*nconn values are
+// contiguous, so lanes stream them coalesced (cache-streaming loads, the matrix is read once
+// per iteration) while x gathers hit L2, where the vectors stay resident.
+//
+// Mixed precision (LPMGPU_MIXED): the same kernel on an FP32 copy of K with FP32 Krylov
+// vectors (dot products in FP64), inside an FP64 iterative refinement that recomputes the
+// true residual b - K x with the FP64 matrix and stops on the same squared-norm rule.
+#include <cooperative_groups.h>
+
+#include <cmath>
+
+#include "lpm_internal.cuh"
+
+namespace lpm
+{
+
+constexpr int kCGThreads = 512;
+constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull; // 4 s
+
+struct CGState
+{
+    int n;              // particle rows
+    int64_t ndof;
+    const int *__restrict__ rowptr;
+    const int *__restrict__ cols;
+    double rtol, atol, abs_stop; // abs_stop >= 0 overrides rtol/atol
+    int64_t maxit;
+    unsigned *bar;      // [0] arrivals, [1] generation
+    double *part;       // [grid][2]
+    int64_t *info;      // [0] iterations, [1] status bits (1 maxit, 2 timeout, 4 breakdown), [2..3] rr0/rr bits
+};
+
+__device__ __forceinline__ unsigned long long gtimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// returns false when the wait timed out (the flag is then also set in info[1])
+__device__ bool grid_barrier(unsigned *bar, int64_t *info, volatile int *s_fail)
+{
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        const unsigned gen = ld_acquire(bar + 1);
+        __threadfence();
+        const unsigned arrived = atomicAdd(bar, 1u);
+        if (arrived == gridDim.x - 1)
+        {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        }
+        else
+        {
+            const unsigned long long t0 = gtimer();
+            unsigned ns = 32;
+            while (ld_acquire(bar + 1) == gen)
+            {
+                if (gtimer() - t0 > kBarrierTimeoutNs)
+                {
+                    atomicOr(reinterpret_cast<unsigned long long *>(info + 1), 2ull);
+                    *s_fail = 1;
+                    break;
+                }
+                __nanosleep(ns);
+                if (ns < 256)
+                    ns <<= 1;
+            }
+        }
+        __threadfence();
+        // a block that sees another block's timeout stops too
+        if (*reinterpret_cast<volatile long long *>(info + 1) & 2)
+            *s_fail = 1;
+    }
+    __syncthreads();
+    return *s_fail == 0;
+}
+
+__device__ __forceinline__ double wsum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float wsumf(float v)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// block partial of v into part[blockIdx*2 + slot] (fixed tree)
+__device__ __forceinline__ void block_partial(double v, double *part, int slot, double *sh)
+{
+    v = wsum(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0)
+        sh[w] = v;
+    __syncthreads();
+    if (w == 0)
+    {
+        double r = (l < (int)(blockDim.x >> 5)) ? sh[l] : 0.0;
+        r = wsum(r);
+        if (l == 0)
+            part[2 * blockIdx.x + slot] = r;
+    }
+    __syncthreads();
+}
+
+// the same fixed-order sum of all blocks' partials, computed by every block
+__device__ __forceinline__ double grid_total(const double *part, int slot, double *sh)
+{
+    if (threadIdx.x < 32)
+    {
+        double v = 0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += 32)
+            v += __ldcg(part + 2 * b + slot);
+        v = wsum(v);
+        if (threadIdx.x == 0)
+            sh[0] = v;
+    }
+    __syncthreads();
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ T ldstream(const T *p)
+{
+    return __ldcs(p);
+}
+
+// q_i = sum_j K_ij (r_j + beta p_old_j) for particle row i, warp-cooperative; lane 0 returns
+template <typename TK, typename TV, int D>
+__device__ __forceinline__ void spmv_row(int row, const int *__restrict__ rowptr, const int *__restrict__ cols,
+                                         const TK *__restrict__ K, const TV *__restrict__ r,
+                                         const TV *__restrict__ pold, TV beta, TV acc[D])
+{
+    constexpr int E = D * D;
+    const int lane = threadIdx.x & 31;
+    const int start = rowptr[row], nblk = rowptr[row + 1] - start;
+    const int nval = nblk * E;
+    const TK *Kr = K + (int64_t)start * E;
+    const int *cr = cols + start;
+    TV a[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+        a[k] = TV(0);
+#pragma unroll 4
+    for (int v = lane; v < nval; v += 32)
+    {
+        const int blk = v / E, e = v - blk * E, rr = e / D, cc = e - rr * D;
+        const int j = ldstream(cr + blk);
+        const int64_t xi = (int64_t)j * D + cc;
+        const TV xv = r[xi] + beta * pold[xi];
+        const TV prod = (TV)ldstream(Kr + v) * xv;
+#pragma unroll
+        for (int k = 0; k < D; ++k)
+            if (rr == k)
+                a[k] += prod;
+    }
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+    {
+        TV v = a[k];
+        for (int o = 16; o > 0; o >>= 1)
+            v += __shfl_xor_sync(0xffffffffu, v, o);
+        acc[k] = v;
+    }
+}
+
+template <typename TK, typename TV, int D>
+__global__ void __launch_bounds__(kCGThreads) k_cg(CGState s, const TK *__restrict__ K, const TV *__restrict__ b,
+                                                   TV *__restrict__ x, TV *__restrict__ r, TV *__restrict__ pa,
+                                                   TV *__restrict__ pb, TV *__restrict__ q)
+{
+    __shared__ double sh[32];
+    __shared__ int s_fail;
+    if (threadIdx.x == 0)
+        s_fail = 0;
+    __syncthreads();
+    const int64_t T = (int64_t)gridDim.x * blockDim.x;
+    const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int W = (int)(T >> 5);
+    const int gw = (int)(gt >> 5);
+    const int lane = threadIdx.x & 31;
+
+    double loc = 0;
+    for (int64_t k = gt; k < s.ndof; k += T)
+    {
+        const TV v = b[k];
+        r[k] = v;
+        x[k] = TV(0);
+        pa[k] = TV(0);
+        loc += (double)v * (double)v;
+    }
+    block_partial(loc, s.part, 0, sh);
+    if (!grid_barrier(s.bar, s.info, &s_fail))
+        return;
+    double rr = grid_total(s.part, 0, sh);
+    const double stop = (s.abs_stop >= 0) ? s.abs_stop : s.rtol * rr + s.atol;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        s.info[0] = 0;
+        reinterpret_cast<double *>(s.info)[2] = rr;
+        reinterpret_cast<double *>(s.info)[3] = rr;
+    }
+    if (rr <= stop)
+        return;
+    TV beta = TV(0);
+    TV *pold = pa, *pnew = pb;
+    for (int64_t it = 1;; ++it)
+    {
+        double lpq = 0;
+        for (int row = gw; row < s.n; row += W)
+        {
+            TV acc[D];
+            spmv_row<TK, TV, D>(row, s.rowptr, s.cols, K, r, pold, beta, acc);
+            if (lane < D)
+            {
+                const int64_t k = (int64_t)row * D + lane;
+                const TV pn = r[k] + beta * pold[k];
+                pnew[k] = pn;
+                TV qv = acc[0];
+#pragma unroll
+                for (int c = 1; c < D; ++c)
+                    if (lane == c)
+                        qv = acc[c];
+                q[k] = qv;
+                lpq += (double)pn * (double)qv;
+            }
+        }
+        block_partial(lpq, s.part, 1, sh);
+        if (!grid_barrier(s.bar, s.info, &s_fail))
+            return;
+        const double pq = grid_total(s.part, 1, sh);
+        if (pq == 0.0)
+        {
+            if (blockIdx.x == 0 && threadIdx.x == 0)
+            {
+                s.info[0] = it - 1;
+                atomicOr(reinterpret_cast<unsigned long long *>(s.info + 1), 4ull);
+            }
+            return;
+        }
+        const double alpha = rr / pq;
+        const TV al = (TV)alpha;
+        double lrr = 0;
+        for (int64_t k = gt; k < s.ndof; k += T)
+        {
+            const TV pn = pnew[k];
+            x[k] = x[k] + al * pn;
+            const TV rv = r[k] - al * q[k];
+            r[k] = rv;
+            lrr += (double)rv * (double)rv;
+        }
+        block_partial(lrr, s.part, 0, sh);
+        if (!grid_barrier(s.bar, s.info, &s_fail))
+            return;
+        const double rn = grid_total(s.part, 0, sh);
+        const bool done = rn <= stop;
+        const bool capped = it >= s.maxit;
+        if (done || capped)
+        {
+            if (blockIdx.x == 0 && threadIdx.x == 0)
+            {
+                s.info[0] = it;
+                reinterpret_cast<double *>(s.info)[3] = rn;
+                if (!done)
+                    atomicOr(reinterpret_cast<unsigned long long *>(s.info + 1), 1ull);
+            }
+            return;
+        }
+        beta = (TV)(rn / rr);
+        rr = rn;
+        TV *t = pold;
+        pold = pnew;
+        pnew = t;
+    }
+}
+
+// ---- helpers for the mixed-precision refinement
+template <typename TA, typename TB>
+__global__ void k_convert(int64_t m, const TA *__restrict__ a, TB *__restrict__ b)
+{
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x)
+        b[k] = (TB)a[k];
+}
+
+__global__ void k_add_f32(int64_t m, const float *__restrict__ d, double *__restrict__ x)
+{
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x)
+        x[k] += (double)d[k];
+}
+
+// r = b - K x (FP64), partial ||r||^2 per block
+template <int D>
+__global__ void __launch_bounds__(256) k_residual64(int n, const int *__restrict__ rowptr, const int *__restrict__ cols,
+                                                    const double *__restrict__ K, const double *__restrict__ b,
+                                                    const double *__restrict__ x, double *__restrict__ r,
+                                                    double *__restrict__ part)
+{
+    __shared__ double sh[32];
+    const int W = (gridDim.x * blockDim.x) >> 5;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    double loc = 0;
+    for (int row = gw; row < n; row += W)
+    {
+        double acc[D];
+        spmv_row<double, double, D>(row, rowptr, cols, K, x, x, 0.0, acc);
+        if (lane < D)
+        {
+            double qv = acc[0];
+            for (int c = 1; c < D; ++c)
+                if (lane == c)
+                    qv = acc[c];
+            const int64_t k = (int64_t)row * D + lane;
+            const double v = b[k] - qv;
+            r[k] = v;
+            loc += v * v;
+        }
+    }
+    block_partial(loc, part, 0, sh);
+}
+
+__global__ void k_sum_partials(int nblk, const double *__restrict__ part, double *__restrict__ out)
+{
+    __shared__ double sh[32];
+    double v = 0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+        v += part[2 * b];
+    v = wsum(v);
+    if ((threadIdx.x & 31) == 0)
+        sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32)
+    {
+        double t = (threadIdx.x < blockDim.x / 32) ? sh[threadIdx.x] : 0.0;
+        t = wsum(t);
+        if (threadIdx.x == 0)
+            *out = t;
+    }
+}
+
+template <typename TK, typename TV, int D>
+static cudaError_t run_cg(Problem &p, const TK *K, const TV *b, TV *x, TV *r, TV *pa, TV *pb, TV *q, double rtol,
+                          double atol, double abs_stop, int64_t maxit, CGResult &out, double *rr_final)
+{
+    static int occ_cache[2][2][4] = {};
+    int &occ = occ_cache[sizeof(TK) == 8][sizeof(TV) == 8][D];
+    cudaError_t e;
+    if (occ == 0)
+    {
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg<TK, TV, D>, kCGThreads, 0);
+        if (e != cudaSuccess)
+            return e;
+        if (occ < 1)
+            occ = 1;
+    }
+    int grid = p.num_sms * std::min(occ, 2);
+    const int64_t rows_warps = ((int64_t)p.n + 0) / ((kCGThreads / 32)) + 1;
+    if (grid > rows_warps)
+        grid = (int)std::max<int64_t>(1, rows_warps);
+    if (grid > kMaxGridBlocks)
+        grid = kMaxGridBlocks;
+    CGState s;
+    s.n = p.n;
+    s.ndof = (int64_t)p.n * D;
+    s.rowptr = p.cstart;
+    s.cols = p.conns;
+    s.rtol = rtol;
+    s.atol = atol;
+    s.abs_stop = abs_stop;
+    s.maxit = maxit;
+    s.bar = p.barrier;
+    s.part = p.partials;
+    s.info = p.cg_info;
+    if ((e = cudaMemsetAsync(p.barrier, 0, 2 * sizeof(unsigned), p.stream)) != cudaSuccess)
+        return e;
+    if ((e = cudaMemsetAsync(p.cg_info, 0, 4 * sizeof(int64_t), p.stream)) != cudaSuccess)
+        return e;
+    void *args[] = {&s, &K, &b, &x, &r, &pa, &pb, &q};
+    e = cudaLaunchCooperativeKernel((const void *)k_cg<TK, TV, D>, dim3(grid), dim3(kCGThreads), args, 0, p.stream);
+    if (e != cudaSuccess)
+        return e;
+    if ((e = cudaMemcpyAsync(p.cg_info_host, p.cg_info, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, p.stream)) !=
+        cudaSuccess)
+        return e;
+    if ((e = cudaStreamSynchronize(p.stream)) != cudaSuccess)
+        return e;
+    out.iters += p.cg_info_host[0];
+    if (p.cg_info_host[1] & 1)
+        out.maxit_hits++;
+    if (p.cg_info_host[1] & 2)
+        out.timeout = true;
+    if (rr_final)
+        *rr_final = reinterpret_cast<double *>(p.cg_info_host)[3];
+    return cudaSuccess;
+}
+
+template <int D>
+static cudaError_t solve_dim(Problem &p, CGResult &out)
+{
+    const int64_t ndof = (int64_t)p.n * D;
+    const int64_t maxit = p.desc.cg_maxit > 0 ? p.desc.cg_maxit : ndof;
+    if (p.desc.precision != LPMGPU_MIXED)
+        return run_cg<double, double, D>(p, p.K, p.res, p.x, p.r, p.p0, p.p1, p.q, p.desc.cg_rtol, p.desc.cg_atol,
+                                         -1.0, maxit, out, nullptr);
+    // FP32 Krylov solve inside FP64 iterative refinement on the same stopping rule
+    cudaError_t e;
+    const int nb_res = std::min(div_up(ndof, 256), 4 * p.num_sms);
+    // rr0 = ||b||^2 via r = b - K*0
+    if ((e = cudaMemsetAsync(p.x, 0, sizeof(double) * ndof, p.stream)) != cudaSuccess)
+        return e;
+    double rr0 = 0, rr = 0;
+    auto true_residual = [&](double &val) -> cudaError_t {
+        k_residual64<D><<<nb_res, 256, 0, p.stream>>>(p.n, p.cstart, p.conns, p.K, p.res, p.x, p.r, p.partials);
+        k_sum_partials<<<1, 256, 0, p.stream>>>(nb_res, p.partials, reinterpret_cast<double *>(p.cg_info) + 3);
+        cudaError_t e2 = cudaMemcpyAsync(&val, reinterpret_cast<double *>(p.cg_info) + 3, sizeof(double),
+                                         cudaMemcpyDeviceToHost, p.stream);
+        if (e2 != cudaSuccess)
+            return e2;
+        return cudaStreamSynchronize(p.stream);
+    };
+    if ((e = true_residual(rr0)) != cudaSuccess)
+        return e;
+    const double stop = p.desc.cg_rtol * rr0 + p.desc.cg_atol;
+    rr = rr0;
+    const int gconv = std::min(div_up(ndof, 256), 8 * p.num_sms);
+    for (int ref = 0; ref < 30 && !(rr <= stop); ++ref)
+    {
+        k_convert<double, float><<<gconv, 256, 0, p.stream>>>(ndof, p.r, p.b32);
+        // the inner solve aims a little below the outer target, measured on its own residual
+        CGResult inner;
+        double rr_in = 0;
+        if ((e = run_cg<float, float, D>(p, p.K32, p.b32, p.x32, p.r32, p.pa32, p.pb32, p.q32, 0.0, 0.0, 0.25 * stop,
+                                         maxit, inner, &rr_in)) != cudaSuccess)
+            return e;
+        out.iters += inner.iters;
+        out.maxit_hits += inner.maxit_hits;
+        out.timeout = out.timeout || inner.timeout;
+        out.refinements++;
+        if (inner.timeout)
+            break;
+        k_add_f32<<<gconv, 256, 0, p.stream>>>(ndof, p.x32, p.x);
+        if ((e = true_residual(rr)) != cudaSuccess)
+            return e;
+        if (inner.iters == 0)
+            break;
+    }
+    return cudaSuccess;
+}
+
+__global__ void k_to_f32(int64_t m, const double *__restrict__ a, float *__restrict__ b)
+{
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x)
+        b[k] = (float)a[k];
+}
+
+cudaError_t launch_k_to_f32(Problem &p)
+{
+    const int64_t m = p.nnzb * p.dim * p.dim;
+    k_to_f32<<<std::min(div_up(m, 256), 16 * p.num_sms), 256, 0, p.stream>>>(m, p.K, p.K32);
+    return cudaGetLastError();
+}
+
+cudaError_t solve_linear(Problem &p, CGResult &out)
+{
+    return p.dim == 2 ? solve_dim<2>(p, out) : solve_dim<3>(p, out);
+}
+
+} // namespace lpm

@@ -1,0 +1,142 @@
+// Internal declarations of liblpmgpu: device state of one problem, launch helpers and the
+// kernels' entry points.  Everything here is compiled with -fmad=false so that each C
+// operator rounds once, as in the reference's own build (-ffp-contract=off): the bond,
+// force and stiffness kernels then reproduce the reference's arithmetic bit for bit.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/lpmgpu.h"
+
+namespace lpm
+{
+
+constexpr int kMaxBonds = 32;    // bonds per particle supported by the fixed-size staging
+constexpr int kMaxConns = 128;   // connections per particle (SC 61, FCC/BCC below 100)
+constexpr int kMaxCand = 512;    // connection candidates per particle before sort-unique
+constexpr double kEps = 1e-6;    // include/lpm.h:41
+
+// std::max semantics ((a < b) ? b : a), which keeps the first argument when b is NaN
+__host__ __device__ inline double std_max(double a, double b) { return (a < b) ? b : a; }
+
+struct Cell
+{
+    int lattice = 0, dim = 2, nneighbors = 0;
+    double radius = 0, cutoff[2] = {0, 0}, pvol = 0;
+    double el[9] = {0};
+};
+
+// Unit cell constants of include/unit_cell.h:27-122
+Cell make_cell(int lattice, double radius);
+// setParticleProperty (particle_elastic.h:70-108): Kn/Tv coefficients
+void kntv(const Cell &c, int plane_stress, double E, double mu, double out[3]);
+
+// Reduction scratch: per-block partial sums and the scalars they reduce to.
+struct Scalars
+{
+    double res_sq;        // ||residual||^2 of the last updateRR
+    double reaction_sq;   // running in-order-free sum of squares of the reaction history
+    double norm_diag;     // ||diag(K)|| before the BC elimination
+    double pad;
+    int any_flag;         // damage update: some bond broke / damage changed
+    int err;              // topology overflow or a timed-out wait
+    int pad2[2];
+};
+
+// Device state of one problem.  Particles are indexed by id; bonds are owner-major CSR
+// (bstart), each particle's layer-0 list first then its layer-1 list, both ascending in the
+// partner id (assembly.h:218-229).  The stiffness is a full symmetric block-CSR (row i holds
+// the blocks of conns(i), ascending), d x d row-major doubles per block.
+struct Problem
+{
+    lpmgpu_desc desc{};
+    Cell cell;
+    int n = 0, dim = 2, nsv = 1;
+    int64_t nbonds = 0, nnzb = 0, nnz_upper = 0;
+    int max_bonds = 0, max_conns = 0;
+    double kntv[3] = {0, 0, 0};
+    cudaStream_t stream = nullptr;
+    int device = 0, num_sms = 0;
+
+    // particles
+    double *xyz = nullptr, *xyz_last = nullptr, *pin = nullptr, *pex = nullptr, *stress = nullptr;
+    double *damage = nullptr, *damage_last = nullptr, *damage_visual = nullptr;
+    double *ddot_local = nullptr, *sv = nullptr, *sv_last = nullptr;
+    int *cons = nullptr, *type = nullptr, *nb = nullptr, *nb0 = nullptr, *bstart = nullptr;
+    double *dLe_total = nullptr, *TdLe_total = nullptr, *cs_sum = nullptr;
+    // bonds
+    int *bp2 = nullptr, *brev = nullptr;
+    double *dis0 = nullptr, *dis = nullptr, *dis_last = nullptr, *dLe = nullptr, *dLp = nullptr,
+           *dLp_last = nullptr, *bstrain = nullptr, *Kn = nullptr, *Tv = nullptr, *cs = nullptr,
+           *bforce = nullptr, *bforce_last = nullptr, *bdamage = nullptr, *bdamage_last = nullptr;
+    // connections and matrices
+    int *cstart = nullptr, *conns = nullptr, *nlq = nullptr;
+    int64_t *kp_ref = nullptr;        // reference K_pointer (n+1)
+    double *K = nullptr;              // nnzb * d*d
+    float *K32 = nullptr;             // mixed precision copy
+    double *diag_raw = nullptr;       // n*d unmodified diagonal (for norm_diag)
+    // vectors (n*d)
+    double *res = nullptr, *x = nullptr, *r = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr;
+    float *x32 = nullptr, *r32 = nullptr, *pa32 = nullptr, *pb32 = nullptr, *q32 = nullptr, *b32 = nullptr;
+    // reductions
+    double *partials = nullptr;       // kMaxGridBlocks * 4
+    Scalars *scal = nullptr;
+    Scalars *scal_host = nullptr;     // pinned mirror
+    unsigned *barrier = nullptr;      // [0] count, [1] generation
+    int64_t *cg_info = nullptr;       // device CG status words
+    int64_t *cg_info_host = nullptr;  // pinned mirror
+    // timing
+    cudaEvent_t ev[8];
+    double phase_s[4] = {0, 0, 0, 0};
+    int64_t device_bytes = 0;
+    std::vector<void *> allocs;
+};
+
+constexpr int kMaxGridBlocks = 4096;
+
+// ---- kernels' host entry points (each enqueues on p.stream and returns a CUDA status)
+cudaError_t build_topology(Problem &p, const double *xyz_host, int *err_code);
+cudaError_t launch_geometry_force(Problem &p);
+cudaError_t launch_update_rr(Problem &p);       // residual + norms into p.scal
+cudaError_t launch_update_rr_impl(Problem &p, bool accumulate_reaction);
+cudaError_t launch_k_to_f32(Problem &p);        // FP32 copy of K for the mixed-precision solve
+cudaError_t launch_assemble(Problem &p, bool apply_bc);
+cudaError_t launch_update_state_var(Problem &p);
+cudaError_t launch_static_damage(Problem &p);   // sets p.scal->any_flag
+cudaError_t launch_add_disp(Problem &p);        // xyz += x (solveLinearSystem position update)
+cudaError_t launch_export_ref(const Problem &p, int64_t *IK, int64_t *JK, double *K); // device outputs
+cudaError_t launch_apply_bc(Problem &p, const lpmgpu_load_step &s);
+
+struct CGResult
+{
+    int64_t iters = 0;
+    int64_t maxit_hits = 0;
+    int refinements = 0;
+    bool timeout = false;
+};
+// Solves K x = res (current residual) into p.x with the reference's stopping rule.
+cudaError_t solve_linear(Problem &p, CGResult &out);
+
+// error text for lpmgpu_last_error
+void set_last_error(const std::string &s);
+
+template <typename T>
+cudaError_t dalloc(Problem &p, T **ptr, size_t count)
+{
+    void *v = nullptr;
+    size_t bytes = sizeof(T) * (count ? count : 1);
+    cudaError_t e = cudaMalloc(&v, bytes);
+    if (e != cudaSuccess)
+        return e;
+    p.allocs.push_back(v);
+    p.device_bytes += (int64_t)bytes;
+    *ptr = static_cast<T *>(v);
+    return cudaMemsetAsync(v, 0, bytes, p.stream);
+}
+
+inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+} // namespace lpm

@@ -1,0 +1,463 @@
+// Per-Newton-iteration particle physics on the device, one thread per particle, each bond
+// loop in the reference's list order so the sums round exactly as the reference does:
+//   Particle::updateBondsGeometry / Bond::updatebGeometry  include/particle.h:164-181, bond.h:30-39
+//   ParticleElastic::updateBondsForce                      include/particle_elastic.h:38-50
+//   ParticleJ2Plasticity::updateBondsForce                 include/particle_j2plasticity.h:63-76
+//   Particle::updateParticleForce / Stress / DamageVisual  include/particle.h:151-240
+//   Solver::updateRR                                       include/solver.h:112-126
+//   ParticleJ2Plasticity::updateParticleStateVariables     include/particle_j2plasticity.h:78-140
+//   SolverStatic::updateStaticDamage                       include/solver_static.h:32-62
+//   Solver::updateForceBC / updateDisplacementBC           include/solver.h:129-188
+// The reference finds the opposite bond with a linear find_if per bond (particle.h:207);
+// here it is the precomputed brev index.
+#include "lpm_internal.cuh"
+
+namespace lpm
+{
+
+struct PhysArgs
+{
+    int n, dim, ptype;
+    const int *__restrict__ bstart, *__restrict__ nb0, *__restrict__ bp2, *__restrict__ brev;
+    double *__restrict__ xyz;
+    const double *__restrict__ dis0, *__restrict__ Kn, *__restrict__ Tv;
+    double *__restrict__ dis, *__restrict__ dLe, *__restrict__ dLp, *__restrict__ bstrain, *__restrict__ cs;
+    double *__restrict__ bforce, *__restrict__ bdamage;
+    double *__restrict__ dLe_total, *__restrict__ TdLe_total, *__restrict__ cs_sum;
+    const double *__restrict__ damage;
+};
+
+// updateBondsGeometry + updateBondsForce of particle i
+__global__ void k_geometry_force(PhysArgs a)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n)
+        return;
+    const int b0 = a.bstart[i], b1 = b0 + a.nb0[i], be = a.bstart[i + 1];
+    const double xi0 = a.xyz[3 * i], xi1 = a.xyz[3 * i + 1], xi2 = a.xyz[3 * i + 2];
+    double dlt[2];
+    for (int L = 0; L < 2; ++L)
+    {
+        const int lo = L == 0 ? b0 : b1, hi = L == 0 ? b1 : be;
+        double s = 0, ts = 0, cx = 0, cy = 0, cz = 0;
+        for (int b = lo; b < hi; ++b)
+        {
+            const int j = a.bp2[b];
+            const double dx = xi0 - a.xyz[3 * j], dy = xi1 - a.xyz[3 * j + 1], dz = xi2 - a.xyz[3 * j + 2];
+            const bool broken = fabs(a.bdamage[b] - 1.0) < kEps;
+            const double dis = sqrt(dx * dx + dy * dy + dz * dz);
+            const double d0 = a.dis0[b];
+            const double dL = broken ? 0.0 : (dis - d0);
+            const double bst = broken ? 0.0 : (dL / dis);
+            const double dle = broken ? 0.0 : (dis - d0 - a.dLp[b]);
+            const double c0 = broken ? 0.0 : (dx / dis);
+            const double c1 = broken ? 0.0 : (dy / dis);
+            const double c2 = broken ? 0.0 : (dz / dis);
+            a.dis[b] = dis;
+            a.bstrain[b] = bst;
+            a.dLe[b] = dle;
+            a.cs[3 * (int64_t)b] = c0;
+            a.cs[3 * (int64_t)b + 1] = c1;
+            a.cs[3 * (int64_t)b + 2] = c2;
+            s += dle;
+            ts += a.Tv[b] * dle;
+            cx += c0;
+            cy += c1;
+            cz += c2;
+        }
+        dlt[L] = s;
+        a.dLe_total[2 * i + L] = s;
+        a.TdLe_total[2 * i + L] = ts;
+        a.cs_sum[6 * i + 3 * L] = cx;
+        a.cs_sum[6 * i + 3 * L + 1] = cy;
+        a.cs_sum[6 * i + 3 * L + 2] = cz;
+    }
+    const double di = a.damage[i];
+    for (int b = b0; b < be; ++b)
+    {
+        const int L = b < b1 ? 0 : 1;
+        double f = 2. * a.Kn[b] * a.dLe[b] + 2. * a.Tv[b] * dlt[L];
+        double D = a.bdamage[b];
+        if (a.ptype == LPMGPU_J2)
+        {
+            D = std_max(D, std_max(di, a.damage[a.bp2[b]]));
+            a.bdamage[b] = D;
+        }
+        f *= (1.0 - D);
+        a.bforce[b] = f;
+    }
+}
+
+struct ForceArgs
+{
+    int n, dim, nneighbors;
+    double pvol;
+    const int *__restrict__ bstart, *__restrict__ brev, *__restrict__ nb, *__restrict__ cons;
+    const double *__restrict__ cs, *__restrict__ dis, *__restrict__ bforce, *__restrict__ bdamage,
+        *__restrict__ pex;
+    double *__restrict__ pin, *__restrict__ stress, *__restrict__ damage_visual, *__restrict__ res;
+    double *__restrict__ partials; // [grid][2]: residual^2, reaction^2
+};
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// deterministic block sum (fixed tree), result valid in thread 0
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double *sh)
+{
+    v = warp_sum(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0)
+        sh[w] = v;
+    __syncthreads();
+    double r = 0;
+    if (w == 0)
+    {
+        r = (l < NT / 32) ? sh[l] : 0.0;
+        r = warp_sum(r);
+    }
+    __syncthreads();
+    return r;
+}
+
+// updateParticleForce + updateParticleStress + updateParticleDamageVisual, then updateRR
+constexpr int kForceThreads = 256;
+__global__ void __launch_bounds__(kForceThreads) k_internal_force(ForceArgs a)
+{
+    __shared__ double sh[32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double rsq = 0.0, rea = 0.0;
+    if (i < a.n)
+    {
+        const int b0 = a.bstart[i], be = a.bstart[i + 1];
+        double P0 = 0., P1 = 0., P2 = 0.;
+        for (int b = b0; b < be; ++b)
+        {
+            const double fs = a.bforce[b] + a.bforce[a.brev[b]];
+            P0 += a.cs[3 * (int64_t)b] * 0.5 * fs;
+            P1 += a.cs[3 * (int64_t)b + 1] * 0.5 * fs;
+            P2 += a.cs[3 * (int64_t)b + 2] * 0.5 * fs;
+        }
+        a.pin[3 * i] = P0;
+        a.pin[3 * i + 1] = P1;
+        a.pin[3 * i + 2] = P2;
+        const int nbi = a.nb[i];
+        const double V_m = a.pvol * nbi / a.nneighbors;
+        double S0 = 0, S1 = 0, S2 = 0, S3 = 0, S4 = 0, S5 = 0, dv = 0;
+        for (int b = b0; b < be; ++b)
+        {
+            const double fs = a.bforce[b] + a.bforce[a.brev[b]];
+            const double cx = a.cs[3 * (int64_t)b], cy = a.cs[3 * (int64_t)b + 1], cz = a.cs[3 * (int64_t)b + 2];
+            const double w = 0.5 / V_m * (a.dis[b]) * 0.5 * fs;
+            S0 += w * (cx) * (cx);
+            S1 += w * (cy) * (cy);
+            S2 += w * (cz) * (cz);
+            S3 += w * (cy) * (cz);
+            S4 += w * (cx) * (cz);
+            S5 += w * (cx) * (cy);
+            dv += a.bdamage[b];
+        }
+        double *st = a.stress + 6 * (int64_t)i;
+        st[0] = S0;
+        st[1] = S1;
+        st[2] = S2;
+        st[3] = S3;
+        st[4] = S4;
+        st[5] = S5;
+        a.damage_visual[i] = dv / (double)nbi;
+        const double P[3] = {P0, P1, P2};
+        for (int k = 0; k < a.dim; ++k)
+        {
+            const int c = a.cons[3 * i + k];
+            const double v = (1 - c) * (a.pex[3 * i + k] - P[k]);
+            a.res[(int64_t)a.dim * i + k] = v;
+            rsq += v * v;
+            if (c == 1)
+                rea += P[k] * P[k];
+        }
+    }
+    const double s0 = block_sum<kForceThreads>(rsq, sh);
+    const double s1 = block_sum<kForceThreads>(rea, sh);
+    if (threadIdx.x == 0)
+    {
+        a.partials[2 * blockIdx.x] = s0;
+        a.partials[2 * blockIdx.x + 1] = s1;
+    }
+}
+
+// fixed-order sum of the per-block partials; accumulates the reaction history
+__global__ void k_finalize_rr(int nblk, const double *__restrict__ partials, Scalars *scal, int accumulate)
+{
+    __shared__ double sh[32];
+    double r = 0, q = 0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+    {
+        r += partials[2 * b];
+        q += partials[2 * b + 1];
+    }
+    const double R = block_sum<256>(r, sh);
+    const double Q = block_sum<256>(q, sh);
+    if (threadIdx.x == 0)
+    {
+        scal->res_sq = R;
+        if (accumulate)
+            scal->reaction_sq += Q;
+    }
+}
+
+cudaError_t launch_geometry_force(Problem &p)
+{
+    PhysArgs a;
+    a.n = p.n;
+    a.dim = p.dim;
+    a.ptype = p.desc.ptype;
+    a.bstart = p.bstart;
+    a.nb0 = p.nb0;
+    a.bp2 = p.bp2;
+    a.brev = p.brev;
+    a.xyz = p.xyz;
+    a.dis0 = p.dis0;
+    a.Kn = p.Kn;
+    a.Tv = p.Tv;
+    a.dis = p.dis;
+    a.dLe = p.dLe;
+    a.dLp = p.dLp;
+    a.bstrain = p.bstrain;
+    a.cs = p.cs;
+    a.bforce = p.bforce;
+    a.bdamage = p.bdamage;
+    a.dLe_total = p.dLe_total;
+    a.TdLe_total = p.TdLe_total;
+    a.cs_sum = p.cs_sum;
+    a.damage = p.damage;
+    k_geometry_force<<<div_up(p.n, 128), 128, 0, p.stream>>>(a);
+    return cudaGetLastError();
+}
+
+// accumulate_reaction: Solver::updateRR appends the reaction forces to the history
+// (solver.h:122-123); Assembly::updateForceState alone (solver_static.h:132-133) does not
+cudaError_t launch_update_rr_impl(Problem &p, bool accumulate_reaction)
+{
+    ForceArgs a;
+    a.n = p.n;
+    a.dim = p.dim;
+    a.nneighbors = p.cell.nneighbors;
+    a.pvol = p.cell.pvol;
+    a.bstart = p.bstart;
+    a.brev = p.brev;
+    a.nb = p.nb;
+    a.cons = p.cons;
+    a.cs = p.cs;
+    a.dis = p.dis;
+    a.bforce = p.bforce;
+    a.bdamage = p.bdamage;
+    a.pex = p.pex;
+    a.pin = p.pin;
+    a.stress = p.stress;
+    a.damage_visual = p.damage_visual;
+    a.res = p.res;
+    a.partials = p.partials;
+    const int nblk = div_up(p.n, kForceThreads);
+    k_internal_force<<<nblk, kForceThreads, 0, p.stream>>>(a);
+    k_finalize_rr<<<1, 256, 0, p.stream>>>(nblk, p.partials, p.scal, accumulate_reaction ? 1 : 0);
+    return cudaGetLastError();
+}
+
+// ParticleJ2Plasticity::updateParticleStateVariables (particle_j2plasticity.h:78-140)
+__global__ void k_j2_update(int n, double E, double mu, double sigmay, double xi, double H, double A,
+                            const int *__restrict__ bstart, const double *__restrict__ stress,
+                            const double *__restrict__ dis, const double *__restrict__ cs, double *__restrict__ sv,
+                            double *__restrict__ dLp, double *__restrict__ ddot_local)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    double *s = sv + 7 * (int64_t)i;
+    double st[6], dpl[6] = {0, 0, 0, 0, 0, 0};
+    double sigma_eq = 0.0, triax = 0.0, dlambda = 0.0;
+    for (int j = 0; j < 6; ++j)
+        st[j] = stress[6 * (int64_t)i + j];
+    const double sigma_m = 1.0 / 3.0 * (st[0] + st[1] + st[2]);
+    for (int j = 0; j < 3; j++)
+        st[j] -= sigma_m;
+    for (int j = 0; j < 6; j++)
+        st[j] -= s[j + 1];
+    for (int j = 0; j < 6; j++)
+    {
+        if (j < 3)
+            sigma_eq += st[j] * st[j];
+        else
+            sigma_eq += 2.0 * st[j] * st[j];
+    }
+    sigma_eq = sqrt(3.0 / 2.0 * sigma_eq);
+    const double yield = sigma_eq - (sigmay + (1.0 - xi) * H * s[0]);
+    const double G = E / 2 / (1 + mu);
+    if (yield > 0.0)
+        dlambda = yield / (3 * G + H);
+    s[0] += dlambda;
+    for (int j = 0; j < 6; j++)
+        if (fabs(sigma_eq) > kEps)
+        {
+            dpl[j] = dlambda * 1.5 * st[j] / sigma_eq;
+            s[j + 1] += 2. / 3. * xi * H * dpl[j];
+        }
+    for (int b = bstart[i]; b < bstart[i + 1]; ++b)
+    {
+        const double cx = cs[3 * (int64_t)b], cy = cs[3 * (int64_t)b + 1], cz = cs[3 * (int64_t)b + 2];
+        const double ddLp = dis[b] * (dpl[0] * cx * cx + dpl[1] * cy * cy + dpl[2] * cz * cz + 2 * dpl[3] * cy * cz +
+                                      2 * dpl[4] * cx * cz + 2 * dpl[5] * cx * cy);
+        dLp[b] += ddLp;
+    }
+    if (sigma_eq > kEps)
+        triax = sigma_m / sigma_eq;
+    ddot_local[i] = dlambda * (1.0 + A * triax);
+}
+
+cudaError_t launch_update_state_var(Problem &p)
+{
+    if (p.desc.ptype != LPMGPU_J2)
+        return cudaSuccess;
+    k_j2_update<<<div_up(p.n, 128), 128, 0, p.stream>>>(p.n, p.desc.E, p.desc.mu, p.desc.sigmay, p.desc.xi, p.desc.H,
+                                                        p.desc.A, p.bstart, p.stress, p.dis, p.cs, p.sv, p.dLp,
+                                                        p.ddot_local);
+    return cudaGetLastError();
+}
+
+// SolverStatic::updateStaticDamage.  No nonlocal neighbour search is run on this path, so the
+// nonlocal rate is 0/0 (solver_static.h:39-51) exactly as in the reference when
+// searchNonlocalNeighbors was not called; elastic particles ignore it, J2 particles add it.
+__global__ void k_static_damage(int n, int ptype, int undamaged, double critical, const int *__restrict__ type,
+                                const int *__restrict__ bstart, const double *__restrict__ bstrain,
+                                double *__restrict__ bdamage, double *__restrict__ damage,
+                                const double *__restrict__ damage_last, Scalars *scal)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || type[i] == undamaged)
+        return;
+    bool changed = false;
+    if (ptype == LPMGPU_J2)
+    {
+        volatile double zero = 0.0;
+        const double ddot_nonlocal = zero / zero;
+        double d = damage[i] + ddot_nonlocal;
+        if (d >= 0.0) // damage_threshold is never assigned (particle_j2plasticity.h:22,148)
+            d = 1;
+        damage[i] = d;
+        changed = fabs(d - damage_last[i]) > 1e-3;
+    }
+    else
+    {
+        for (int b = bstart[i]; b < bstart[i + 1]; ++b)
+            if (bstrain[b] >= critical && fabs(bdamage[b] - 1.0) > kEps)
+            {
+                changed = true;
+                bdamage[b] = 1;
+            }
+    }
+    if (changed)
+        atomicExch(&scal->any_flag, 1);
+}
+
+cudaError_t launch_static_damage(Problem &p)
+{
+    cudaError_t e = cudaMemsetAsync(&p.scal->any_flag, 0, sizeof(int), p.stream);
+    if (e != cudaSuccess)
+        return e;
+    k_static_damage<<<div_up(p.n, 128), 128, 0, p.stream>>>(p.n, p.desc.ptype, p.desc.undamaged_type,
+                                                            p.desc.critical_bstrain, p.type, p.bstart, p.bstrain,
+                                                            p.bdamage, p.damage, p.damage_last, p.scal);
+    return cudaGetLastError();
+}
+
+// Solver::solveLinearSystem position update (solver.h:101-108)
+__global__ void k_add_disp(int n, int dim, const double *__restrict__ x, double *__restrict__ xyz)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    for (int k = 0; k < dim; ++k)
+        xyz[3 * i + k] = xyz[3 * i + k] + (0.0 + x[(int64_t)dim * i + k]);
+}
+
+cudaError_t launch_add_disp(Problem &p)
+{
+    k_add_disp<<<div_up(p.n, 256), 256, 0, p.stream>>>(p.n, p.dim, p.x, p.xyz);
+    return cudaGetLastError();
+}
+
+__global__ void k_force_bc(int count, const int *__restrict__ ids, double fx, double fy, double fz,
+                           double *__restrict__ pex)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= count)
+        return;
+    const int i = ids[q];
+    pex[3 * i] += fx / count;
+    pex[3 * i + 1] += fy / count;
+    pex[3 * i + 2] += fz / count;
+}
+
+__global__ void k_disp_bc(int count, const int *__restrict__ ids, int flag, double step, double *__restrict__ xyz,
+                          int *__restrict__ cons)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= count)
+        return;
+    const int i = ids[q];
+    xyz[3 * i + flag] = xyz[3 * i + flag] + step;
+    cons[3 * i + flag] = 1;
+}
+
+// updateForceBC then updateDisplacementBC, each BC in order.  A particle that appears twice in
+// one group would be updated by two threads; the reference's groups hold distinct particles.
+cudaError_t launch_apply_bc(Problem &p, const lpmgpu_load_step &s)
+{
+    size_t total = 0;
+    for (int f = 0; f < s.nforce; ++f)
+        total += (size_t)s.force[f].count;
+    for (int d = 0; d < s.ndisp; ++d)
+        total += (size_t)s.disp[d].count;
+    if (total == 0)
+        return cudaSuccess;
+    int *dids = nullptr;
+    cudaError_t e = cudaMallocAsync(&dids, sizeof(int) * total, p.stream);
+    if (e != cudaSuccess)
+        return e;
+    std::vector<int> h(total);
+    size_t o = 0;
+    for (int f = 0; f < s.nforce; ++f)
+        for (int q = 0; q < s.force[f].count; ++q)
+            h[o++] = s.force[f].ids[q];
+    for (int d = 0; d < s.ndisp; ++d)
+        for (int q = 0; q < s.disp[d].count; ++q)
+            h[o++] = s.disp[d].ids[q];
+    e = cudaMemcpyAsync(dids, h.data(), sizeof(int) * total, cudaMemcpyHostToDevice, p.stream);
+    o = 0;
+    for (int f = 0; f < s.nforce && e == cudaSuccess; ++f)
+    {
+        const auto &b = s.force[f];
+        if (b.count > 0)
+            k_force_bc<<<div_up(b.count, 256), 256, 0, p.stream>>>(b.count, dids + o, b.fx, b.fy, b.fz, p.pex);
+        o += b.count;
+    }
+    for (int d = 0; d < s.ndisp && e == cudaSuccess; ++d)
+    {
+        const auto &b = s.disp[d];
+        if (b.count > 0)
+            k_disp_bc<<<div_up(b.count, 256), 256, 0, p.stream>>>(b.count, dids + o, b.flag, b.step, p.xyz, p.cons);
+        o += b.count;
+    }
+    if (e == cudaSuccess)
+        e = cudaGetLastError();
+    // the host vector must outlive the async copy
+    cudaError_t s2 = cudaStreamSynchronize(p.stream);
+    cudaFreeAsync(dids, p.stream);
+    return e != cudaSuccess ? e : s2;
+}
+
+} // namespace lpm

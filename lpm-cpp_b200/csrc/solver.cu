@@ -1,0 +1,831 @@
+// Host runtime of liblpmgpu: problem construction, the Newton loop, the damage loop and the
+// load-step halving, and the C ABI of include/lpmgpu.h.  All heavy work is device kernels on
+// the handle's stream; the host only reads back the few scalars each decision needs.
+//   Solver::NewtonIteration           include/solver.h:55-90
+//   SolverStatic::solveProblemStep    include/solver_static.h:99-152
+//   SolverStatic::solveProblem        include/solver_static.h:65-96 (one load step per call)
+//   Assembly::storeStateVar / resetStateVar  include/assembly.h:141-159
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "lpm_internal.cuh"
+
+struct lpmgpu_solver
+{
+    lpm::Problem p;
+};
+
+namespace lpm
+{
+
+static thread_local std::string g_last_error;
+
+void set_last_error(const std::string &s) { g_last_error = s; }
+
+static int32_t cuda_fail(cudaError_t e, const char *what)
+{
+    set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+    if (e == cudaErrorMemoryAllocation)
+        return LPMGPU_ERR_OUT_OF_MEMORY;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+        return LPMGPU_ERR_NO_DEVICE;
+    return LPMGPU_ERR_CUDA;
+}
+
+#define CK(x)                                                                                                          \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        cudaError_t e_ = (x);                                                                                          \
+        if (e_ != cudaSuccess)                                                                                         \
+            return cuda_fail(e_, #x);                                                                                  \
+    } while (0)
+
+#define ST(x)                                                                                                          \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        int32_t s_ = (x);                                                                                              \
+        if (s_ != LPMGPU_OK)                                                                                           \
+            return s_;                                                                                                 \
+    } while (0)
+
+static int32_t sync_scalars(Problem &p)
+{
+    CK(cudaMemcpyAsync(p.scal_host, p.scal, sizeof(Scalars), cudaMemcpyDeviceToHost, p.stream));
+    CK(cudaStreamSynchronize(p.stream));
+    return LPMGPU_OK;
+}
+
+// Assembly::updateGeometry + updateForceState (and updateRR when with_rr)
+static int32_t force_state(Problem &p, bool with_rr)
+{
+    CK(cudaEventRecord(p.ev[0], p.stream));
+    CK(launch_geometry_force(p));
+    CK(launch_update_rr_impl(p, with_rr));
+    CK(cudaEventRecord(p.ev[1], p.stream));
+    ST(sync_scalars(p));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, p.ev[0], p.ev[1]);
+    p.phase_s[0] += ms * 1e-3;
+    return LPMGPU_OK;
+}
+
+static int32_t assemble(Problem &p, bool apply_bc)
+{
+    CK(cudaEventRecord(p.ev[2], p.stream));
+    CK(launch_assemble(p, apply_bc));
+    if (p.desc.precision == LPMGPU_MIXED)
+        CK(launch_k_to_f32(p));
+    CK(cudaEventRecord(p.ev[3], p.stream));
+    CK(cudaEventSynchronize(p.ev[3]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, p.ev[2], p.ev[3]);
+    p.phase_s[1] += ms * 1e-3;
+    return LPMGPU_OK;
+}
+
+static int32_t linear_solve(Problem &p, lpmgpu_stats *st)
+{
+    CGResult r;
+    CK(cudaEventRecord(p.ev[4], p.stream));
+    CK(solve_linear(p, r));
+    CK(cudaEventRecord(p.ev[5], p.stream));
+    CK(cudaEventSynchronize(p.ev[5]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, p.ev[4], p.ev[5]);
+    p.phase_s[2] += ms * 1e-3;
+    if (st)
+    {
+        st->newton_solves++;
+        st->cg_iters += r.iters;
+        st->cg_maxit_hits += r.maxit_hits;
+        st->refinements += r.refinements;
+    }
+    if (r.timeout)
+    {
+        set_last_error("a device-side barrier wait timed out in the CG kernel");
+        return LPMGPU_ERR_TIMEOUT;
+    }
+    return LPMGPU_OK;
+}
+
+// Solver::NewtonIteration (solver.h:55-90): K fixed, positions += disp per iteration.
+// *ni gets the iteration count, or max_iter on failure.
+static int32_t newton(Problem &p, lpmgpu_stats *st, int *ni)
+{
+    ST(force_state(p, true));
+    double nres = std::sqrt(p.scal_host->res_sq);
+    const double nreac = std::sqrt(p.scal_host->reaction_sq);
+    const double tol_mult = std_max(nres, nreac);
+    int k = 0;
+    while (nres > p.desc.tol_iter * tol_mult)
+    {
+        if (++k > p.desc.max_iter)
+        {
+            *ni = p.desc.max_iter;
+            if (st)
+                st->residual_norm = nres;
+            return LPMGPU_OK;
+        }
+        ST(linear_solve(p, st));
+        CK(launch_add_disp(p));
+        ST(force_state(p, true));
+        nres = std::sqrt(p.scal_host->res_sq);
+    }
+    if (st)
+        st->residual_norm = nres;
+    *ni = k;
+    return LPMGPU_OK;
+}
+
+static int32_t store_state(Problem &p)
+{
+    const size_t n = p.n, nb = (size_t)p.nbonds;
+    CK(cudaMemcpyAsync(p.xyz_last, p.xyz, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, p.stream));
+    CK(cudaMemcpyAsync(p.damage_last, p.damage, sizeof(double) * n, cudaMemcpyDeviceToDevice, p.stream));
+    CK(cudaMemcpyAsync(p.sv_last, p.sv, sizeof(double) * p.nsv * n, cudaMemcpyDeviceToDevice, p.stream));
+    CK(cudaMemcpyAsync(p.dis_last, p.dis, sizeof(double) * nb, cudaMemcpyDeviceToDevice, p.stream));
+    CK(cudaMemcpyAsync(p.bdamage_last, p.bdamage, sizeof(double) * nb, cudaMemcpyDeviceToDevice, p.stream));
+    CK(cudaMemcpyAsync(p.bforce_last, p.bforce, sizeof(double) * nb, cudaMemcpyDeviceToDevice, p.stream));
+    CK(cudaMemcpyAsync(p.dLp_last, p.dLp, sizeof(double) * nb, cudaMemcpyDeviceToDevice, p.stream));
+    return LPMGPU_OK;
+}
+
+static int32_t reset_state(Problem &p)
+{
+    const size_t n = p.n, nb = (size_t)p.nbonds;
+    CK(cudaMemcpyAsync(p.xyz, p.xyz_last, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, p.stream));
+    CK(cudaMemcpyAsync(p.damage, p.damage_last, sizeof(double) * n, cudaMemcpyDeviceToDevice, p.stream));
+    CK(cudaMemcpyAsync(p.sv, p.sv_last, sizeof(double) * p.nsv * n, cudaMemcpyDeviceToDevice, p.stream));
+    CK(cudaMemcpyAsync(p.dis, p.dis_last, sizeof(double) * nb, cudaMemcpyDeviceToDevice, p.stream));
+    CK(cudaMemcpyAsync(p.bdamage, p.bdamage_last, sizeof(double) * nb, cudaMemcpyDeviceToDevice, p.stream));
+    CK(cudaMemcpyAsync(p.bforce, p.bforce_last, sizeof(double) * nb, cudaMemcpyDeviceToDevice, p.stream));
+    CK(cudaMemcpyAsync(p.dLp, p.dLp_last, sizeof(double) * nb, cudaMemcpyDeviceToDevice, p.stream));
+    return LPMGPU_OK;
+}
+
+// SolverStatic::solveProblemStep: returns LPMGPU_OK or LPMGPU_ERR_NEWTON
+static int32_t problem_step(Problem &p, const lpmgpu_load_step &s, lpmgpu_stats *st)
+{
+    CK(launch_apply_bc(p, s));
+    int n_newton = 0;
+    bool new_damaged = false;
+    do
+    {
+        if (st)
+            st->damage_iters++;
+        ST(assemble(p, true));
+        ST(newton(p, st, &n_newton));
+        if (n_newton >= p.desc.max_iter)
+            break;
+        CK(launch_update_state_var(p));
+        CK(launch_static_damage(p));
+        ST(sync_scalars(p));
+        new_damaged = p.scal_host->any_flag != 0;
+        ST(store_state(p));
+        if (new_damaged)
+            ST(force_state(p, false));
+    } while (new_damaged);
+    if (st)
+        st->reaction_norm = std::sqrt(p.scal_host->reaction_sq);
+    return n_newton < p.desc.max_iter ? LPMGPU_OK : LPMGPU_ERR_NEWTON;
+}
+
+static int32_t scaled_step(Problem &p, const lpmgpu_load_step &s, double scale, lpmgpu_stats *st, int depth)
+{
+    std::vector<lpmgpu_dispbc> db(s.disp, s.disp + s.ndisp);
+    std::vector<lpmgpu_forcebc> fb(s.force, s.force + s.nforce);
+    for (auto &d : db)
+        d.step *= scale;
+    for (auto &f : fb)
+    {
+        f.fx *= scale;
+        f.fy *= scale;
+        f.fz *= scale;
+    }
+    lpmgpu_load_step sc{db.data(), s.ndisp, fb.data(), s.nforce};
+    int32_t r = problem_step(p, sc, st);
+    if (r != LPMGPU_ERR_NEWTON)
+        return r;
+    if (depth >= 30)
+        return LPMGPU_ERR_CUTS;
+    // solver_static.h:78-87: reset to the last converged state, halve, run both halves
+    ST(reset_state(p));
+    if (st)
+        st->cuts++;
+    ST(scaled_step(p, s, scale / 2.0, st, depth + 1));
+    return scaled_step(p, s, scale / 2.0, st, depth + 1);
+}
+
+// ---- lattice generators (include/utilities.h:93-310), host side
+static void rmatrix(int f, const double a[3], double R[9])
+{
+    const double a1 = a[0], a2 = a[1], a3 = a[2];
+    if (f == 0)
+    {
+        R[0] = cos(a2) * cos(a3);
+        R[1] = -cos(a2) * sin(a3);
+        R[2] = sin(a2);
+        R[3] = cos(a1) * sin(a3) + sin(a1) * sin(a2) * cos(a3);
+        R[4] = cos(a1) * cos(a3) - sin(a1) * sin(a2) * sin(a3);
+        R[5] = -sin(a1) * cos(a2);
+        R[6] = sin(a1) * sin(a3) - cos(a1) * sin(a2) * cos(a3);
+        R[7] = sin(a1) * cos(a3) + cos(a1) * sin(a2) * sin(a3);
+        R[8] = cos(a1) * cos(a2);
+    }
+    else if (f == 1)
+    {
+        R[0] = -cos(a1) * cos(a2) * cos(a3) - sin(a1) * sin(a3);
+        R[1] = cos(a3) * sin(a1) - sin(a3) * cos(a2) * cos(a1);
+        R[2] = sin(a2) * cos(a1);
+        R[3] = sin(a3) * cos(a1) - cos(a3) * cos(a2) * sin(a1);
+        R[4] = -cos(a1) * cos(a3) - sin(a1) * cos(a2) * sin(a3);
+        R[5] = sin(a2) * sin(a1);
+        R[6] = cos(a3) * sin(a2);
+        R[7] = sin(a3) * sin(a2);
+        R[8] = cos(a2);
+    }
+    else
+    {
+        R[0] = -sin(a1) * cos(a2) * sin(a3) + cos(a1) * cos(a3);
+        R[1] = -sin(a3) * cos(a1) - cos(a3) * cos(a2) * sin(a1);
+        R[2] = sin(a1) * sin(a2);
+        R[3] = cos(a3) * sin(a1) + sin(a3) * cos(a2) * cos(a1);
+        R[4] = -sin(a1) * sin(a3) + cos(a1) * cos(a2) * cos(a3);
+        R[5] = -cos(a1) * sin(a2);
+        R[6] = sin(a2) * sin(a3);
+        R[7] = sin(a2) * cos(a3);
+        R[8] = cos(a2);
+    }
+}
+
+struct Gen
+{
+    double *out;
+    int64_t cap, n = 0;
+    const double *box;
+    const double *R;
+    bool check_z;
+    void add(double x, double y, double z, bool z_from_rot = true)
+    {
+        const double p[3] = {x, y, z};
+        double q[3];
+        for (int i = 0; i < 3; ++i)
+        {
+            double s = 0.0;
+            for (int j = 0; j < 3; ++j)
+                s += R[3 * i + j] * p[j];
+            q[i] = 1.0 * s;
+        }
+        if (!(q[0] >= box[0] && q[0] <= box[1] && q[1] >= box[2] && q[1] <= box[3]))
+            return;
+        if (check_z && !(q[2] >= box[4] && q[2] <= box[5]))
+            return;
+        if (out && n < cap)
+        {
+            out[3 * n] = q[0];
+            out[3 * n + 1] = q[1];
+            out[3 * n + 2] = z_from_rot ? q[2] : 0.0;
+        }
+        n++;
+    }
+};
+
+static int64_t generate(int lattice, double r, const double *box, const double *R, double *out, int64_t cap)
+{
+    Gen g{out, cap, 0, box, R, lattice >= LPMGPU_SC3D};
+    if (lattice == LPMGPU_SQUARE2D)
+    {
+        const double a = sqrt((box[1] - box[0]) * (box[1] - box[0]) + (box[3] - box[2]) * (box[3] - box[2]));
+        const double hx = 2 * r, hy = hx;
+        const int first = (int)floor((a - -a) / hx), rows = (int)floor((a - -a) / hy);
+        for (int j = 1; j <= rows; j++)
+            for (int i = 1; i <= first; i++)
+                g.add(-a + hx * (i - 1) + r, -a + hy * (j - 1) + r, 0, false);
+    }
+    else if (lattice == LPMGPU_HEXAGON2D)
+    {
+        const double a = sqrt((box[1] - box[0]) * (box[1] - box[0]) + (box[3] - box[2]) * (box[3] - box[2]));
+        const double hx = 2 * r, hy = hx * sqrt(3.0) / 2.0;
+        const int first = 1 + (int)floor((a - -a) / hx), rows = 1 + (int)floor((a - -a) / hy);
+        for (int j = 1; j <= rows; j++)
+        {
+            const double y = -a + hy * (j - 1);
+            if (j % 2 == 1)
+                for (int i = 1; i <= first; i++)
+                    g.add(-a + hx * (i - 1), y, 0);
+            else
+                for (int i = 1; i <= first - 1; i++)
+                    g.add(-a + hx * (2 * i - 1) / 2.0, y, 0);
+        }
+    }
+    else if (lattice == LPMGPU_SC3D)
+    {
+        const double a = sqrt((box[1] - box[0]) * (box[1] - box[0]) + (box[3] - box[2]) * (box[3] - box[2]) +
+                              (box[5] - box[4]) * (box[5] - box[4]));
+        const double h = 2 * r;
+        const int first = 1 + (int)floor((a - -a) / h), rows = first, layers = first;
+        for (int k = 1; k <= layers; k++)
+            for (int j = 1; j <= rows; j++)
+                for (int i = 1; i <= first; i++)
+                    g.add(box[0] + h * (i - 1), -a + h * (j - 1), -a + h * (k - 1));
+    }
+    else if (lattice == LPMGPU_FCC3D)
+    {
+        const double a = sqrt((box[1] - box[0]) * (box[1] - box[0]) + (box[3] - box[2]) * (box[3] - box[2]) +
+                              (box[5] - box[4]) * (box[5] - box[4]));
+        const double h = 4 * r / sqrt(2.0);
+        const int first = 1 + (int)floor((a - -a) / h);
+        const int rows = 1 + (int)floor((a - -a) / (h / 2.0)), layers = rows;
+        for (int k = 1; k <= layers; k++)
+        {
+            const double z = -a + h / 2.0 * (k - 1);
+            for (int j = 1; j <= rows; j++)
+            {
+                const double y = -a + h / 2.0 * (j - 1);
+                const bool full = ((k % 2 == 1) == (j % 2 == 1));
+                const int cnt = full ? first : first - 1;
+                for (int i = 1; i <= cnt; i++)
+                    g.add(full ? -a + h * (i - 1) : -a + h * (i - 1) + h / 2.0, y, z);
+            }
+        }
+    }
+    else
+    {
+        // BCC (no reference generator): cubic cell 4r/sqrt(3), corner and body-centre sites
+        const double a = sqrt((box[1] - box[0]) * (box[1] - box[0]) + (box[3] - box[2]) * (box[3] - box[2]) +
+                              (box[5] - box[4]) * (box[5] - box[4]));
+        const double h = 4 * r / sqrt(3.0);
+        const int first = 1 + (int)floor((a - -a) / h), layers = 1 + (int)floor((a - -a) / (h / 2.0));
+        for (int k = 1; k <= layers; k++)
+        {
+            const double z = -a + h / 2.0 * (k - 1);
+            const bool corner = (k % 2 == 1);
+            const int cnt = corner ? first : first - 1;
+            for (int j = 1; j <= cnt; j++)
+                for (int i = 1; i <= cnt; i++)
+                    g.add(corner ? -a + h * (i - 1) : -a + h * (i - 1) + h / 2.0,
+                          corner ? -a + h * (j - 1) : -a + h * (j - 1) + h / 2.0, z);
+        }
+    }
+    return g.n;
+}
+
+} // namespace lpm
+
+using namespace lpm;
+
+cudaError_t lpm::launch_update_rr(Problem &p) { return launch_update_rr_impl(p, true); }
+
+extern "C" {
+
+const char *lpmgpu_version(void) { return "lpmgpu 0.1 (sm_100a)"; }
+
+const char *lpmgpu_status_string(int32_t s)
+{
+    switch (s)
+    {
+    case LPMGPU_OK: return "ok";
+    case LPMGPU_ERR_INVALID_ARG: return "invalid argument";
+    case LPMGPU_ERR_CUDA: return "CUDA error";
+    case LPMGPU_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case LPMGPU_ERR_NEWTON: return "Newton iteration did not converge";
+    case LPMGPU_ERR_CG_MAXIT: return "CG reached its iteration cap";
+    case LPMGPU_ERR_TIMEOUT: return "device wait timed out";
+    case LPMGPU_ERR_TOPOLOGY: return "unsupported particle topology";
+    case LPMGPU_ERR_BUDGET: return "HBM budget exceeded";
+    case LPMGPU_ERR_CUTS: return "load step halved too many times";
+    case LPMGPU_ERR_NOT_READY: return "result not ready";
+    case LPMGPU_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+    }
+}
+
+const char *lpmgpu_last_error(void) { return g_last_error.c_str(); }
+
+int32_t lpmgpu_generate_lattice(int32_t lattice, double radius, const double box[6], int32_t euler_flag,
+                                const double angles[3], double *out, int64_t cap, int64_t *count)
+{
+    if (!box || !angles || !count || lattice < 0 || lattice > LPMGPU_BCC3D || !(radius > 0))
+        return LPMGPU_ERR_INVALID_ARG;
+    double R[9];
+    rmatrix(euler_flag, angles, R);
+    *count = generate(lattice, radius, box, R, out, out ? cap : 0);
+    return LPMGPU_OK;
+}
+
+static void free_problem(Problem &p)
+{
+    for (void *v : p.allocs)
+        cudaFree(v);
+    p.allocs.clear();
+    if (p.scal_host)
+        cudaFreeHost(p.scal_host);
+    if (p.cg_info_host)
+        cudaFreeHost(p.cg_info_host);
+    for (auto &e : p.ev)
+        if (e)
+            cudaEventDestroy(e);
+    if (p.stream)
+        cudaStreamDestroy(p.stream);
+}
+
+int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
+{
+    if (!d || !out || !d->xyz || d->n <= 0 || d->lattice < 0 || d->lattice > LPMGPU_BCC3D ||
+        (d->ptype != LPMGPU_ELASTIC && d->ptype != LPMGPU_J2) || !(d->radius > 0) || d->max_iter < 0)
+        return LPMGPU_ERR_INVALID_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    {
+        set_last_error("no CUDA device visible; liblpmgpu has no CPU path");
+        return LPMGPU_ERR_NO_DEVICE;
+    }
+    auto *h = new lpmgpu_solver();
+    Problem &p = h->p;
+    p.desc = *d;
+    p.desc.xyz = nullptr;
+    p.desc.type = nullptr;
+    p.device = d->device;
+    for (auto &e : p.ev)
+        e = nullptr;
+    auto fail = [&](int32_t code) {
+        free_problem(p);
+        delete h;
+        return code;
+    };
+#define CKF(x)                                                                                                         \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        cudaError_t e_ = (x);                                                                                          \
+        if (e_ != cudaSuccess)                                                                                         \
+            return fail(cuda_fail(e_, #x));                                                                            \
+    } while (0)
+    CKF(cudaSetDevice(p.device));
+    CKF(cudaStreamCreateWithFlags(&p.stream, cudaStreamNonBlocking));
+    CKF(cudaDeviceGetAttribute(&p.num_sms, cudaDevAttrMultiProcessorCount, p.device));
+    for (auto &e : p.ev)
+        CKF(cudaEventCreate(&e));
+    p.cell = make_cell(d->lattice, d->radius);
+    p.n = d->n;
+    p.dim = p.cell.dim;
+    p.nsv = (d->ptype == LPMGPU_J2) ? 7 : 1;
+    kntv(p.cell, d->plane_stress, d->E, d->mu, p.kntv);
+    const size_t n = p.n;
+    CKF(cudaMallocHost(&p.scal_host, sizeof(Scalars)));
+    CKF(cudaMallocHost(&p.cg_info_host, 4 * sizeof(int64_t)));
+    CKF(dalloc(p, &p.scal, 1));
+    CKF(dalloc(p, &p.partials, 2 * std::max<size_t>((size_t)kMaxGridBlocks, n / 64 + 1) + 16));
+    CKF(dalloc(p, &p.barrier, 4));
+    CKF(dalloc(p, &p.cg_info, 4));
+    CKF(dalloc(p, &p.xyz, 3 * n));
+    CKF(dalloc(p, &p.xyz_last, 3 * n));
+    CKF(dalloc(p, &p.pin, 3 * n));
+    CKF(dalloc(p, &p.pex, 3 * n));
+    CKF(dalloc(p, &p.stress, 6 * n));
+    CKF(dalloc(p, &p.damage, n));
+    CKF(dalloc(p, &p.damage_last, n));
+    CKF(dalloc(p, &p.damage_visual, n));
+    CKF(dalloc(p, &p.ddot_local, n));
+    CKF(dalloc(p, &p.sv, p.nsv * n));
+    CKF(dalloc(p, &p.sv_last, p.nsv * n));
+    CKF(dalloc(p, &p.cons, 3 * n));
+    CKF(dalloc(p, &p.type, n));
+    CKF(dalloc(p, &p.dLe_total, 2 * n));
+    CKF(dalloc(p, &p.TdLe_total, 2 * n));
+    CKF(dalloc(p, &p.cs_sum, 6 * n));
+    CKF(cudaMemcpyAsync(p.xyz, d->xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, p.stream));
+    CKF(cudaMemcpyAsync(p.xyz_last, d->xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, p.stream));
+    if (d->type)
+        CKF(cudaMemcpyAsync(p.type, d->type, sizeof(int) * n, cudaMemcpyHostToDevice, p.stream));
+    int topo_err = 0;
+    CKF(build_topology(p, d->xyz, &topo_err));
+    if (topo_err)
+    {
+        set_last_error("a particle has no bonds, or more bonds / connections than supported");
+        return fail(topo_err);
+    }
+    const size_t ndof = n * p.dim;
+    CKF(dalloc(p, &p.K, (size_t)p.nnzb * p.dim * p.dim));
+    CKF(dalloc(p, &p.diag_raw, ndof));
+    CKF(dalloc(p, &p.res, ndof));
+    CKF(dalloc(p, &p.x, ndof));
+    CKF(dalloc(p, &p.r, ndof));
+    CKF(dalloc(p, &p.p0, ndof));
+    CKF(dalloc(p, &p.p1, ndof));
+    CKF(dalloc(p, &p.q, ndof));
+    if (d->precision == LPMGPU_MIXED)
+    {
+        CKF(dalloc(p, &p.K32, (size_t)p.nnzb * p.dim * p.dim));
+        CKF(dalloc(p, &p.x32, ndof));
+        CKF(dalloc(p, &p.r32, ndof));
+        CKF(dalloc(p, &p.pa32, ndof));
+        CKF(dalloc(p, &p.pb32, ndof));
+        CKF(dalloc(p, &p.q32, ndof));
+        CKF(dalloc(p, &p.b32, ndof));
+    }
+    // the examples run updateGeometry + updateForceState before constructing the solver
+    CKF(launch_geometry_force(p));
+    CKF(launch_update_rr_impl(p, false));
+    CKF(cudaStreamSynchronize(p.stream));
+#undef CKF
+    *out = h;
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_destroy(lpmgpu_solver *h)
+{
+    if (!h)
+        return LPMGPU_ERR_INVALID_ARG;
+    cudaSetDevice(h->p.device);
+    cudaStreamSynchronize(h->p.stream);
+    free_problem(h->p);
+    delete h;
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_get_sizes(const lpmgpu_solver *h, lpmgpu_sizes *o)
+{
+    if (!h || !o)
+        return LPMGPU_ERR_INVALID_ARG;
+    const Problem &p = h->p;
+    o->n = p.n;
+    o->dim = p.dim;
+    o->nbonds = p.nbonds;
+    o->nnzb = p.nnzb;
+    o->nnz_upper = p.nnz_upper;
+    o->max_bonds = p.max_bonds;
+    o->max_conns = p.max_conns;
+    o->device_bytes = p.device_bytes;
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_get_topology(const lpmgpu_solver *h, int32_t *nb0, int32_t *nb1, int32_t *bond_p2, int32_t *nconn,
+                            int32_t *nlq, int32_t *conns)
+{
+    if (!h)
+        return LPMGPU_ERR_INVALID_ARG;
+    const Problem &p = h->p;
+    const size_t n = p.n;
+    std::vector<int> nb(n), n0(n), cst(n + 1);
+    CK(cudaSetDevice(p.device));
+    CK(cudaMemcpy(nb.data(), p.nb, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(n0.data(), p.nb0, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(cst.data(), p.cstart, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; ++i)
+    {
+        if (nb0)
+            nb0[i] = n0[i];
+        if (nb1)
+            nb1[i] = nb[i] - n0[i];
+        if (nconn)
+            nconn[i] = cst[i + 1] - cst[i];
+    }
+    if (bond_p2)
+        CK(cudaMemcpy(bond_p2, p.bp2, sizeof(int) * p.nbonds, cudaMemcpyDeviceToHost));
+    if (nlq)
+        CK(cudaMemcpy(nlq, p.nlq, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    if (conns)
+        CK(cudaMemcpy(conns, p.conns, sizeof(int) * p.nnzb, cudaMemcpyDeviceToHost));
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_update_force_state(lpmgpu_solver *h)
+{
+    if (!h)
+        return LPMGPU_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->p.device));
+    return force_state(h->p, false);
+}
+
+int32_t lpmgpu_update_state_var(lpmgpu_solver *h)
+{
+    if (!h)
+        return LPMGPU_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->p.device));
+    CK(launch_update_state_var(h->p));
+    CK(cudaStreamSynchronize(h->p.stream));
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_update_rr(lpmgpu_solver *h, double *norm)
+{
+    if (!h)
+        return LPMGPU_ERR_INVALID_ARG;
+    Problem &p = h->p;
+    CK(cudaSetDevice(p.device));
+    CK(launch_update_rr_impl(p, true));
+    ST(sync_scalars(p));
+    if (norm)
+        *norm = std::sqrt(p.scal_host->res_sq);
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_assemble(lpmgpu_solver *h, int32_t apply_bc)
+{
+    if (!h)
+        return LPMGPU_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->p.device));
+    return assemble(h->p, apply_bc != 0);
+}
+
+int32_t lpmgpu_export_ref_csr(const lpmgpu_solver *h, int64_t *K_pointer, int64_t *IK, int64_t *JK, double *K)
+{
+    if (!h)
+        return LPMGPU_ERR_INVALID_ARG;
+    const Problem &p = h->p;
+    CK(cudaSetDevice(p.device));
+    const size_t n = p.n, nnz = (size_t)p.nnz_upper;
+    if (K_pointer)
+        CK(cudaMemcpy(K_pointer, p.kp_ref, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost));
+    if (!IK && !JK && !K)
+        return LPMGPU_OK;
+    int64_t *dIK = nullptr, *dJK = nullptr;
+    double *dK = nullptr;
+    CK(cudaMalloc(&dIK, sizeof(int64_t) * (p.dim * n + 1)));
+    CK(cudaMalloc(&dJK, sizeof(int64_t) * (nnz + 1)));
+    CK(cudaMalloc(&dK, sizeof(double) * (nnz + 1)));
+    cudaError_t e = launch_export_ref(p, dIK, dJK, dK);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(p.stream);
+    if (e == cudaSuccess && IK)
+        e = cudaMemcpy(IK, dIK, sizeof(int64_t) * (p.dim * n + 1), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && JK)
+        e = cudaMemcpy(JK, dJK, sizeof(int64_t) * nnz, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && K)
+        e = cudaMemcpy(K, dK, sizeof(double) * nnz, cudaMemcpyDeviceToHost);
+    cudaFree(dIK);
+    cudaFree(dJK);
+    cudaFree(dK);
+    CK(e);
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_solve_linear(lpmgpu_solver *h, double *disp, lpmgpu_stats *st)
+{
+    if (!h)
+        return LPMGPU_ERR_INVALID_ARG;
+    Problem &p = h->p;
+    CK(cudaSetDevice(p.device));
+    if (st)
+        std::memset(st, 0, sizeof *st);
+    ST(linear_solve(p, st));
+    if (disp)
+        CK(cudaMemcpy(disp, p.x, sizeof(double) * p.n * p.dim, cudaMemcpyDeviceToHost));
+    return LPMGPU_OK;
+}
+
+static int32_t check_step(const Problem &p, const lpmgpu_load_step *s)
+{
+    if (!s || (s->ndisp > 0 && !s->disp) || (s->nforce > 0 && !s->force))
+        return LPMGPU_ERR_INVALID_ARG;
+    for (int q = 0; q < s->ndisp; ++q)
+    {
+        const auto &b = s->disp[q];
+        if (b.count < 0 || (b.count > 0 && !b.ids) || b.flag < 0 || b.flag > 2)
+            return LPMGPU_ERR_INVALID_ARG;
+        for (int k = 0; k < b.count; ++k)
+            if (b.ids[k] < 0 || b.ids[k] >= p.n)
+                return LPMGPU_ERR_INVALID_ARG;
+    }
+    for (int q = 0; q < s->nforce; ++q)
+    {
+        const auto &b = s->force[q];
+        if (b.count < 0 || (b.count > 0 && !b.ids))
+            return LPMGPU_ERR_INVALID_ARG;
+        for (int k = 0; k < b.count; ++k)
+            if (b.ids[k] < 0 || b.ids[k] >= p.n)
+                return LPMGPU_ERR_INVALID_ARG;
+    }
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_apply_load_step(lpmgpu_solver *h, const lpmgpu_load_step *s)
+{
+    if (!h)
+        return LPMGPU_ERR_INVALID_ARG;
+    ST(check_step(h->p, s));
+    CK(cudaSetDevice(h->p.device));
+    CK(launch_apply_bc(h->p, *s));
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_solve_problem_step(lpmgpu_solver *h, const lpmgpu_load_step *s, lpmgpu_stats *st)
+{
+    if (!h)
+        return LPMGPU_ERR_INVALID_ARG;
+    ST(check_step(h->p, s));
+    CK(cudaSetDevice(h->p.device));
+    if (st)
+        std::memset(st, 0, sizeof *st);
+    int32_t r = problem_step(h->p, *s, st);
+    if (st)
+        st->converged = (r == LPMGPU_OK);
+    return r;
+}
+
+int32_t lpmgpu_solve_load_step(lpmgpu_solver *h, const lpmgpu_load_step *s, lpmgpu_stats *st)
+{
+    if (!h)
+        return LPMGPU_ERR_INVALID_ARG;
+    ST(check_step(h->p, s));
+    Problem &p = h->p;
+    CK(cudaSetDevice(p.device));
+    lpmgpu_stats local;
+    lpmgpu_stats *S = st ? st : &local;
+    std::memset(S, 0, sizeof *S);
+    for (double &t : p.phase_s)
+        t = 0;
+    CK(cudaEventRecord(p.ev[6], p.stream));
+    int32_t r = scaled_step(p, *s, 1.0, S, 0);
+    CK(cudaEventRecord(p.ev[7], p.stream));
+    CK(cudaEventSynchronize(p.ev[7]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, p.ev[6], p.ev[7]);
+    S->seconds = ms * 1e-3;
+    S->converged = (r == LPMGPU_OK);
+    S->reaction_norm = std::sqrt(p.scal_host->reaction_sq);
+    return r;
+}
+
+int32_t lpmgpu_store_state(lpmgpu_solver *h)
+{
+    if (!h)
+        return LPMGPU_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->p.device));
+    ST(store_state(h->p));
+    CK(cudaStreamSynchronize(h->p.stream));
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_reset_state(lpmgpu_solver *h)
+{
+    if (!h)
+        return LPMGPU_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->p.device));
+    ST(reset_state(h->p));
+    CK(cudaStreamSynchronize(h->p.stream));
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_read_state(const lpmgpu_solver *h, double *xyz, double *pin, double *stress, double *damage,
+                          double *damage_visual, double *state_var, double *bdamage)
+{
+    if (!h)
+        return LPMGPU_ERR_INVALID_ARG;
+    const Problem &p = h->p;
+    const size_t n = p.n;
+    CK(cudaSetDevice(p.device));
+    CK(cudaStreamSynchronize(p.stream));
+    if (xyz)
+        CK(cudaMemcpy(xyz, p.xyz, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+    if (pin)
+        CK(cudaMemcpy(pin, p.pin, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost));
+    if (stress)
+        CK(cudaMemcpy(stress, p.stress, sizeof(double) * 6 * n, cudaMemcpyDeviceToHost));
+    if (damage)
+        CK(cudaMemcpy(damage, p.damage, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    if (damage_visual)
+        CK(cudaMemcpy(damage_visual, p.damage_visual, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    if (state_var)
+        CK(cudaMemcpy(state_var, p.sv, sizeof(double) * p.nsv * n, cudaMemcpyDeviceToHost));
+    if (bdamage)
+        CK(cudaMemcpy(bdamage, p.bdamage, sizeof(double) * p.nbonds, cudaMemcpyDeviceToHost));
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_read_residual(const lpmgpu_solver *h, double *res)
+{
+    if (!h || !res)
+        return LPMGPU_ERR_INVALID_ARG;
+    const Problem &p = h->p;
+    CK(cudaSetDevice(p.device));
+    CK(cudaStreamSynchronize(p.stream));
+    CK(cudaMemcpy(res, p.res, sizeof(double) * p.n * p.dim, cudaMemcpyDeviceToHost));
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_set_xyz(lpmgpu_solver *h, const double *xyz)
+{
+    if (!h || !xyz)
+        return LPMGPU_ERR_INVALID_ARG;
+    Problem &p = h->p;
+    CK(cudaSetDevice(p.device));
+    CK(cudaMemcpyAsync(p.xyz, xyz, sizeof(double) * 3 * p.n, cudaMemcpyHostToDevice, p.stream));
+    CK(cudaStreamSynchronize(p.stream));
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_get_phase_times(const lpmgpu_solver *h, double *t4)
+{
+    if (!h || !t4)
+        return LPMGPU_ERR_INVALID_ARG;
+    for (int k = 0; k < 4; ++k)
+        t4[k] = h->p.phase_s[k];
+    return LPMGPU_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,552 @@
+"""Host-side mirror of the LPM-CPP interface for the implicit quasi-static step, over the C ABI
+of liblpmgpu.so (include/lpmgpu.h).
+
+The names follow the reference so an example's ``run()`` reads the same:
+``UnitCell``, ``createRMatrix``, ``createPlateHEX2D`` / ``createPlateSQ2D`` /
+``createCuboidSC3D`` / ``createCuboidFCC3D`` (include/utilities.h), ``Assembly``
+(include/assembly.h), ``LoadStep`` / ``DispBC`` / ``ForceBC`` (include/load_step.h,
+include/boundary.h) and ``SolverStatic`` with ``solveProblem(load, start_index)``
+(include/solver_static.h).  The solver runs on the GPU only: without liblpmgpu.so or a CUDA
+device the constructors raise; nothing falls back to the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblpmgpu.so")
+
+
+class LatticeType(enum.IntEnum):
+    Square2D = 0
+    Hexagon2D = 1
+    SimpleCubic3D = 2
+    FCC3D = 3
+    BCC3D = 4
+
+
+class ParticleType(enum.IntEnum):
+    Elastic = 0
+    J2Plasticity = 2
+
+
+class LoadMode(enum.IntEnum):
+    Relative = 0
+    Absolute = 1
+
+
+class SolverMode(enum.IntEnum):
+    CG = 0
+    PARDISO = 1
+
+
+class StiffnessMode(enum.IntEnum):
+    Analytical = 0
+    FiniteDifference = 1
+
+
+class Precision(enum.IntEnum):
+    FP64 = 0
+    MIXED = 1
+
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory",
+          4: "Newton iteration did not converge", 5: "CG reached its iteration cap",
+          6: "device wait timed out", 7: "unsupported particle topology", 8: "HBM budget exceeded",
+          9: "load step halved too many times", 10: "result not ready", 11: "no CUDA device"}
+OK, ERR_NEWTON, ERR_CUTS, ERR_NOT_READY = 0, 4, 9, 10
+
+
+class LpmGpuError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = STATUS.get(status, "unknown")
+        detail = ""
+        if _lib is not None:
+            detail = _lib.lpmgpu_last_error().decode(errors="replace")
+        super().__init__(f"{where}: {msg} ({status}){': ' + detail if detail else ''}")
+        self.status = status
+
+
+# ---------------------------------------------------------------------------- C ABI structs
+class Desc(C.Structure):
+    _fields_ = [
+        ("lattice", C.c_int32), ("ptype", C.c_int32), ("n", C.c_int32),
+        ("xyz", C.POINTER(C.c_double)), ("type", C.POINTER(C.c_int32)),
+        ("radius", C.c_double), ("plane_stress", C.c_int32),
+        ("E", C.c_double), ("mu", C.c_double), ("critical_bstrain", C.c_double),
+        ("sigmay", C.c_double), ("xi", C.c_double), ("H", C.c_double), ("A", C.c_double),
+        ("nonlocal_L", C.c_double), ("undamaged_type", C.c_int32), ("max_iter", C.c_int32),
+        ("tol_iter", C.c_double), ("cg_rtol", C.c_double), ("cg_atol", C.c_double),
+        ("cg_maxit", C.c_int64), ("precision", C.c_int32), ("device", C.c_int32),
+    ]
+
+
+class CDispBC(C.Structure):
+    _fields_ = [("ids", C.POINTER(C.c_int32)), ("count", C.c_int32), ("flag", C.c_int32), ("step", C.c_double)]
+
+
+class CForceBC(C.Structure):
+    _fields_ = [("ids", C.POINTER(C.c_int32)), ("count", C.c_int32),
+                ("fx", C.c_double), ("fy", C.c_double), ("fz", C.c_double)]
+
+
+class CLoadStep(C.Structure):
+    _fields_ = [("disp", C.POINTER(CDispBC)), ("ndisp", C.c_int32),
+                ("force", C.POINTER(CForceBC)), ("nforce", C.c_int32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("converged", C.c_int32), ("newton_solves", C.c_int32), ("cuts", C.c_int32),
+                ("damage_iters", C.c_int32), ("cg_iters", C.c_int64), ("cg_maxit_hits", C.c_int64),
+                ("refinements", C.c_int32), ("reaction_norm", C.c_double), ("residual_norm", C.c_double),
+                ("seconds", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Sizes(C.Structure):
+    _fields_ = [("n", C.c_int32), ("dim", C.c_int32), ("nbonds", C.c_int64), ("nnzb", C.c_int64),
+                ("nnz_upper", C.c_int64), ("max_bonds", C.c_int32), ("max_conns", C.c_int32),
+                ("device_bytes", C.c_int64)]
+
+
+_lib = None
+
+# every symbol declared in include/lpmgpu.h
+EXPORTS = [
+    "lpmgpu_version", "lpmgpu_status_string", "lpmgpu_last_error", "lpmgpu_generate_lattice",
+    "lpmgpu_create", "lpmgpu_destroy", "lpmgpu_get_sizes", "lpmgpu_get_topology",
+    "lpmgpu_update_force_state", "lpmgpu_update_state_var", "lpmgpu_update_rr", "lpmgpu_assemble",
+    "lpmgpu_export_ref_csr", "lpmgpu_solve_linear", "lpmgpu_apply_load_step",
+    "lpmgpu_solve_problem_step", "lpmgpu_solve_load_step", "lpmgpu_store_state", "lpmgpu_reset_state",
+    "lpmgpu_read_state", "lpmgpu_read_residual", "lpmgpu_set_xyz", "lpmgpu_get_phase_times",
+]
+
+
+def lib():
+    """Loads liblpmgpu.so (built by lpm-cpp_b200/build.py); raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'`")
+    L = C.CDLL(LIB_PATH)
+    vp, dp, ip, lp = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_int64)
+    sig = {
+        "lpmgpu_version": (C.c_char_p, []),
+        "lpmgpu_status_string": (C.c_char_p, [C.c_int32]),
+        "lpmgpu_last_error": (C.c_char_p, []),
+        "lpmgpu_generate_lattice": (C.c_int32, [C.c_int32, C.c_double, dp, C.c_int32, dp, dp, C.c_int64, lp]),
+        "lpmgpu_create": (C.c_int32, [C.POINTER(Desc), C.POINTER(vp)]),
+        "lpmgpu_destroy": (C.c_int32, [vp]),
+        "lpmgpu_get_sizes": (C.c_int32, [vp, C.POINTER(Sizes)]),
+        "lpmgpu_get_topology": (C.c_int32, [vp, ip, ip, ip, ip, ip, ip]),
+        "lpmgpu_update_force_state": (C.c_int32, [vp]),
+        "lpmgpu_update_state_var": (C.c_int32, [vp]),
+        "lpmgpu_update_rr": (C.c_int32, [vp, dp]),
+        "lpmgpu_assemble": (C.c_int32, [vp, C.c_int32]),
+        "lpmgpu_export_ref_csr": (C.c_int32, [vp, lp, lp, lp, dp]),
+        "lpmgpu_solve_linear": (C.c_int32, [vp, dp, C.POINTER(Stats)]),
+        "lpmgpu_apply_load_step": (C.c_int32, [vp, C.POINTER(CLoadStep)]),
+        "lpmgpu_solve_problem_step": (C.c_int32, [vp, C.POINTER(CLoadStep), C.POINTER(Stats)]),
+        "lpmgpu_solve_load_step": (C.c_int32, [vp, C.POINTER(CLoadStep), C.POINTER(Stats)]),
+        "lpmgpu_store_state": (C.c_int32, [vp]),
+        "lpmgpu_reset_state": (C.c_int32, [vp]),
+        "lpmgpu_read_state": (C.c_int32, [vp, dp, dp, dp, dp, dp, dp, dp]),
+        "lpmgpu_read_residual": (C.c_int32, [vp, dp]),
+        "lpmgpu_set_xyz": (C.c_int32, [vp, dp]),
+        "lpmgpu_get_phase_times": (C.c_int32, [vp, dp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def _lp(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_int64))
+
+
+def _check(status, where):
+    if status != OK:
+        raise LpmGpuError(status, where)
+
+
+# ---------------------------------------------------------------------------- unit cell / generators
+class UnitCell:
+    """include/unit_cell.h:27-122 (constants only; the device computes the same ones)."""
+
+    def __init__(self, lattice: LatticeType, radius: float):
+        self.lattice = LatticeType(lattice)
+        self.radius = float(radius)
+        r, s2, s3 = self.radius, np.sqrt(2.0), np.sqrt(3.0)
+        if self.lattice == LatticeType.Square2D:
+            self.dim, self.nneighbors, self.neighbor_cutoff = 2, 8, [2.0 * r, 2.0 * s2 * r]
+        elif self.lattice == LatticeType.Hexagon2D:
+            self.dim, self.nneighbors, self.neighbor_cutoff = 2, 12, [2.0 * r, 2.0 * s3 * r]
+        elif self.lattice in (LatticeType.SimpleCubic3D, LatticeType.FCC3D):
+            self.dim, self.nneighbors, self.neighbor_cutoff = 3, 18, [2.0 * r, 2.0 * s2 * r]
+        else:
+            self.dim, self.nneighbors, self.neighbor_cutoff = 3, 14, [2.0 * r, 4.0 / s3 * r]
+
+
+def createRMatrix(eulerflag: int, angles: Sequence[float]):
+    """include/utilities.h:15-91; returned as (flag, angles) for the generators."""
+    return (int(eulerflag), np.ascontiguousarray(angles, dtype=np.float64))
+
+
+def _generate(lattice: LatticeType, box, cell: UnitCell, R) -> np.ndarray:
+    L = lib()
+    b = np.ascontiguousarray(box, dtype=np.float64)
+    flag, ang = R if R is not None else (0, np.zeros(3))
+    cnt = C.c_int64(0)
+    _check(L.lpmgpu_generate_lattice(int(lattice), cell.radius, _dp(b), flag, _dp(ang), None, 0, C.byref(cnt)),
+           "lpmgpu_generate_lattice")
+    out = np.zeros((cnt.value, 3))
+    _check(L.lpmgpu_generate_lattice(int(lattice), cell.radius, _dp(b), flag, _dp(ang), _dp(out), cnt.value,
+                                     C.byref(cnt)), "lpmgpu_generate_lattice")
+    return out
+
+
+def createPlateSQ2D(box, cell, R=None):
+    return _generate(LatticeType.Square2D, box, cell, R)
+
+
+def createPlateHEX2D(box, cell, R=None):
+    return _generate(LatticeType.Hexagon2D, box, cell, R)
+
+
+def createCuboidSC3D(box, cell, R=None):
+    return _generate(LatticeType.SimpleCubic3D, box, cell, R)
+
+
+def createCuboidFCC3D(box, cell, R=None):
+    return _generate(LatticeType.FCC3D, box, cell, R)
+
+
+def createCuboidBCC3D(box, cell, R=None):
+    """No counterpart in the reference: corner + body-centre sites, nearest distance 2r."""
+    return _generate(LatticeType.BCC3D, box, cell, R)
+
+
+# ---------------------------------------------------------------------------- assembly and loads
+@dataclass
+class Material:
+    """Arguments of setParticleProperty (particle_elastic.h:70, particle_j2plasticity.h:155)."""
+    plane_stress: bool = False
+    E: float = 69e3
+    mu: float = 0.3
+    critical_bstrain: float = 1.0
+    sigmay: float = 0.0
+    xi: float = 0.0
+    H: float = 0.0
+    A: float = 0.0
+    nonlocal_L: float = 0.0
+
+
+class Assembly:
+    """Particle system built from coordinates (include/assembly.h:98-106).  The bonds and
+    connections are built on the device when the solver is constructed."""
+
+    def __init__(self, xyz, box, cell: UnitCell, ptype: ParticleType = ParticleType.Elastic):
+        self.xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        self.box = list(box)
+        self.cell = cell
+        self.ptype = ParticleType(ptype)
+        self.nparticle = len(self.xyz)
+        self.type = np.zeros(self.nparticle, dtype=np.int32)
+        self.material = Material()
+
+    def setParticleProperty(self, nonlocal_L, is_plane_stress, E, mu, *rest):
+        """Elastic: (nonlocal_L, is_plane_stress, E, mu, critical_bstrain);
+        J2: (nonlocal_L, is_plane_stress, E, mu, sigmay, xi, H, A, critical_bstrain)."""
+        m = Material(plane_stress=bool(is_plane_stress), E=float(E), mu=float(mu), nonlocal_L=float(nonlocal_L))
+        if self.ptype == ParticleType.J2Plasticity:
+            m.sigmay, m.xi, m.H, m.A, m.critical_bstrain = map(float, rest)
+        else:
+            (m.critical_bstrain,) = map(float, rest)
+        self.material = m
+
+    def group(self, mask) -> np.ndarray:
+        return np.nonzero(np.asarray(mask))[0].astype(np.int32)
+
+
+_FLAG = {"x": 0, "y": 1, "z": 2}
+
+
+@dataclass
+class DispBC:
+    group: np.ndarray
+    load_mode: LoadMode
+    flag: str
+    step: float
+
+    def cutHalf(self):
+        self.step /= 2.0
+
+
+@dataclass
+class ForceBC:
+    group: np.ndarray
+    load_mode: LoadMode
+    fx: float
+    fy: float
+    fz: float
+
+    def cutHalf(self):
+        self.fx /= 2.0
+        self.fy /= 2.0
+        self.fz /= 2.0
+
+
+@dataclass
+class LoadStep:
+    dispBCs: List[DispBC] = field(default_factory=list)
+    forceBCs: List[ForceBC] = field(default_factory=list)
+
+    def loadCutHalf(self):
+        for d in self.dispBCs:
+            d.cutHalf()
+        for f in self.forceBCs:
+            f.cutHalf()
+
+
+class _CStep:
+    """Keeps the ctypes arrays of one load step alive for a call."""
+
+    def __init__(self, step: LoadStep):
+        for bc in list(step.dispBCs) + list(step.forceBCs):
+            if bc.load_mode != LoadMode.Relative:
+                raise ValueError("only LoadMode.Relative is supported (Absolute teleports particles in the "
+                                 "reference, solver.h:140-141)")
+        self.keep = []
+        nd, nf = len(step.dispBCs), len(step.forceBCs)
+        self.d = (CDispBC * max(nd, 1))()
+        self.f = (CForceBC * max(nf, 1))()
+        for q, bc in enumerate(step.dispBCs):
+            ids = np.ascontiguousarray(bc.group, dtype=np.int32)
+            self.keep.append(ids)
+            self.d[q] = CDispBC(_ip(ids), len(ids), _FLAG[bc.flag] if isinstance(bc.flag, str) else int(bc.flag),
+                                float(bc.step))
+        for q, bc in enumerate(step.forceBCs):
+            ids = np.ascontiguousarray(bc.group, dtype=np.int32)
+            self.keep.append(ids)
+            self.f[q] = CForceBC(_ip(ids), len(ids), float(bc.fx), float(bc.fy), float(bc.fz))
+        self.s = CLoadStep(self.d, nd, self.f, nf)
+
+
+# ---------------------------------------------------------------------------- solver
+class GpuProblem:
+    """One device-resident problem: the handle of include/lpmgpu.h."""
+
+    def __init__(self, ass: Assembly, undamaged_pt_type=-1, max_iter=30, tol_iter=1e-5,
+                 precision: Precision = Precision.FP64, cg_rtol=1e-12, cg_atol=1e-12, cg_maxit=0, device=0):
+        L = lib()
+        self.ass = ass
+        m = ass.material
+        d = Desc()
+        d.lattice, d.ptype, d.n = int(ass.cell.lattice), int(ass.ptype), ass.nparticle
+        self._xyz = np.ascontiguousarray(ass.xyz, dtype=np.float64)
+        self._type = np.ascontiguousarray(ass.type, dtype=np.int32)
+        d.xyz, d.type = _dp(self._xyz), _ip(self._type)
+        d.radius, d.plane_stress = ass.cell.radius, int(m.plane_stress)
+        d.E, d.mu, d.critical_bstrain = m.E, m.mu, m.critical_bstrain
+        d.sigmay, d.xi, d.H, d.A, d.nonlocal_L = m.sigmay, m.xi, m.H, m.A, m.nonlocal_L
+        d.undamaged_type, d.max_iter, d.tol_iter = int(undamaged_pt_type), int(max_iter), float(tol_iter)
+        d.cg_rtol, d.cg_atol, d.cg_maxit = float(cg_rtol), float(cg_atol), int(cg_maxit)
+        d.precision, d.device = int(precision), int(device)
+        h = C.c_void_p()
+        _check(L.lpmgpu_create(C.byref(d), C.byref(h)), "lpmgpu_create")
+        self._h = h
+        s = Sizes()
+        _check(L.lpmgpu_get_sizes(h, C.byref(s)), "lpmgpu_get_sizes")
+        self.sizes = {k: getattr(s, k) for k, _ in s._fields_}
+        self.n, self.dim = s.n, s.dim
+        self.nsv = 7 if ass.ptype == ParticleType.J2Plasticity else 1
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lpmgpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- topology and matrices
+    def topology(self):
+        n, nb, nnzb = self.n, self.sizes["nbonds"], self.sizes["nnzb"]
+        nb0, nb1, p2 = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(nb, np.int32)
+        nconn, nlq, conns = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(nnzb, np.int32)
+        _check(lib().lpmgpu_get_topology(self._h, _ip(nb0), _ip(nb1), _ip(p2), _ip(nconn), _ip(nlq), _ip(conns)),
+               "lpmgpu_get_topology")
+        return {"nb0": nb0, "nb1": nb1, "bond_p2": p2, "nconn": nconn, "nlq": nlq, "conns": conns}
+
+    def export_csr(self):
+        nnz = self.sizes["nnz_upper"]
+        Kp = np.zeros(self.n + 1, np.int64)
+        IK = np.zeros(self.dim * self.n + 1, np.int64)
+        JK = np.zeros(nnz, np.int64)
+        K = np.zeros(nnz)
+        _check(lib().lpmgpu_export_ref_csr(self._h, _lp(Kp), _lp(IK), _lp(JK), _dp(K)), "lpmgpu_export_ref_csr")
+        return Kp, IK, JK, K
+
+    # ---- physics steps
+    def update_force_state(self):
+        _check(lib().lpmgpu_update_force_state(self._h), "lpmgpu_update_force_state")
+
+    def update_state_var(self):
+        _check(lib().lpmgpu_update_state_var(self._h), "lpmgpu_update_state_var")
+
+    def update_rr(self) -> float:
+        v = C.c_double(0)
+        _check(lib().lpmgpu_update_rr(self._h, C.byref(v)), "lpmgpu_update_rr")
+        return v.value
+
+    def assemble(self, apply_bc=True):
+        _check(lib().lpmgpu_assemble(self._h, int(apply_bc)), "lpmgpu_assemble")
+
+    def solve_linear(self):
+        disp = np.zeros(self.dim * self.n)
+        st = Stats()
+        _check(lib().lpmgpu_solve_linear(self._h, _dp(disp), C.byref(st)), "lpmgpu_solve_linear")
+        return disp, st.as_dict()
+
+    def apply_load_step(self, step: LoadStep):
+        cs = _CStep(step)
+        _check(lib().lpmgpu_apply_load_step(self._h, C.byref(cs.s)), "lpmgpu_apply_load_step")
+
+    def solve_problem_step(self, step: LoadStep):
+        cs = _CStep(step)
+        st = Stats()
+        r = lib().lpmgpu_solve_problem_step(self._h, C.byref(cs.s), C.byref(st))
+        if r not in (OK, ERR_NEWTON):
+            _check(r, "lpmgpu_solve_problem_step")
+        return r == OK, st.as_dict()
+
+    def solve_load_step(self, step: LoadStep):
+        cs = _CStep(step)
+        st = Stats()
+        r = lib().lpmgpu_solve_load_step(self._h, C.byref(cs.s), C.byref(st))
+        if r not in (OK, ERR_CUTS):
+            _check(r, "lpmgpu_solve_load_step")
+        return r == OK, st.as_dict()
+
+    def store_state(self):
+        _check(lib().lpmgpu_store_state(self._h), "lpmgpu_store_state")
+
+    def reset_state(self):
+        _check(lib().lpmgpu_reset_state(self._h), "lpmgpu_reset_state")
+
+    def set_xyz(self, xyz):
+        a = np.ascontiguousarray(xyz, dtype=np.float64)
+        _check(lib().lpmgpu_set_xyz(self._h, _dp(a)), "lpmgpu_set_xyz")
+
+    def state(self, fields=("xyz", "pin", "stress", "damage", "damage_visual", "state_var", "bdamage")):
+        n = self.n
+        shapes = {"xyz": (n, 3), "pin": (n, 3), "stress": (n, 6), "damage": (n,), "damage_visual": (n,),
+                  "state_var": (n, self.nsv), "bdamage": (self.sizes["nbonds"],)}
+        out = {k: np.zeros(shapes[k]) for k in fields}
+        args = [_dp(out.get(k)) for k in ("xyz", "pin", "stress", "damage", "damage_visual", "state_var",
+                                          "bdamage")]
+        _check(lib().lpmgpu_read_state(self._h, *args), "lpmgpu_read_state")
+        return out
+
+    def residual(self):
+        r = np.zeros(self.dim * self.n)
+        _check(lib().lpmgpu_read_residual(self._h, _dp(r)), "lpmgpu_read_residual")
+        return r
+
+    def phase_times(self):
+        t = np.zeros(4)
+        _check(lib().lpmgpu_get_phase_times(self._h, _dp(t)), "lpmgpu_get_phase_times")
+        return {"force_s": t[0], "assembly_s": t[1], "linear_s": t[2], "other_s": t[3]}
+
+
+class _StiffnessView:
+    """``solv.stiffness.K_global / K_pointer / IK / JK`` (stiffness.h:24-26), read on demand."""
+
+    def __init__(self, prob: GpuProblem):
+        self._p = prob
+
+    def _load(self):
+        self.K_pointer, self.IK, self.JK, self.K_global = self._p.export_csr()
+
+    def __getattr__(self, name):
+        if name in ("K_pointer", "IK", "JK", "K_global"):
+            self._load()
+            return self.__dict__[name]
+        raise AttributeError(name)
+
+
+class SolverStatic:
+    """SolverStatic<nlayer> (include/solver_static.h:17-29) on the GPU: same constructor
+    arguments, same solveProblem(load, start_index) contract; extra keyword arguments choose
+    the precision and CG tolerances."""
+
+    def __init__(self, undamaged_pt_type: int, ass: Assembly, stiff_mode=StiffnessMode.Analytical,
+                 sol_mode=SolverMode.CG, dumpFile: str = "", max_iter: int = 30, tol: float = 1e-5, *,
+                 precision: Precision = Precision.FP64, cg_rtol=1e-12, cg_atol=1e-12, cg_maxit=0, device=0):
+        if StiffnessMode(stiff_mode) != StiffnessMode.Analytical:
+            raise ValueError("only StiffnessMode.Analytical is on the device path")
+        self.ass = ass
+        self.dumpFile = dumpFile
+        self.max_NR_iter, self.tol_NR_iter = max_iter, tol
+        self.problem = GpuProblem(ass, undamaged_pt_type, max_iter, tol, precision, cg_rtol, cg_atol, cg_maxit,
+                                  device)
+        self.stiffness = _StiffnessView(self.problem)
+        self.history: List[dict] = []
+
+    def solveProblemStep(self, load_step: LoadStep, dt: float = 1.0) -> bool:
+        ok, st = self.problem.solve_problem_step(load_step)
+        self.history.append(st)
+        return ok
+
+    def solveProblem(self, load: List[LoadStep], start_index: int = 0) -> int:
+        """Runs every load step with the reference's halve-and-retry (solver_static.h:65-96).
+        Returns the new start_index (the reference updates its int& argument)."""
+        for i, step in enumerate(load):
+            ok, st = self.problem.solve_load_step(step)
+            st["step"] = i + start_index
+            self.history.append(st)
+            if not ok:
+                raise LpmGpuError(ERR_CUTS, f"load step {i + start_index}")
+            if self.dumpFile:
+                self.writeDump(self.dumpFile, i + start_index)
+        return start_index + len(load)
+
+    def writeDump(self, path: str, step: int):
+        """Assembly::writeDump (include/assembly.h:310-335) text format."""
+        s = self.problem.state()
+        a = self.ass
+        with open(path, "a+") as f:
+            f.write("ITEM: TIMESTEP\n%d\nITEM: NUMBER OF ATOMS\n%d\nITEM: BOX BOUNDS pp pp pp\n" % (step, a.nparticle))
+            for k in range(3):
+                f.write("%8.8f %8.8f\n" % (a.box[2 * k], a.box[2 * k + 1]))
+            f.write("ITEM: ATOMS id type x y z dx dy dz s11 s22 s33 s23 s13 s12 damage damage_visual "
+                    "state_var[0] \n")
+            x, st, dmg, dv, sv = s["xyz"], s["stress"], s["damage"], s["damage_visual"], s["state_var"]
+            for i in range(a.nparticle):
+                u = x[i] - a.xyz[i]
+                f.write("%d %d %.4e %.4e %.4e %.4e %.4e %.4e %.4e %.4e %.4e %.4e %.4e %.4e %.4e %.4e %.4e\n" % (
+                    i, a.type[i], x[i, 0], x[i, 1], x[i, 2], u[0], u[1], u[2], st[i, 0], st[i, 1], st[i, 2],
+                    st[i, 3], st[i, 4], st[i, 5], dmg[i], dv[i], sv[i, 0]))

@@ -28,6 +28,9 @@
  *   forcebc NAME FX FY FZ [FROM TO]
  *   dumpK STEP   (write the reference CSR after that load step; may repeat)
  *   loop ref|step   out DIR   xyz_file PATH (optional: particle coordinates instead of a generator)
+ *   groupfile NAME PATH   (group from raw int32 particle ids)   typefile PATH (raw int32 types)
+ *   cg_tol RTOL ATOL      (overrides the squared-norm tolerances the reference sets at
+ *                          solver.h:312-313; applied inside the MKL stand-in, test use only)
  */
 #include <cstdio>
 #include <cstdlib>
@@ -103,7 +106,26 @@ struct Spec
     std::string loop = "step";
     std::string out = ".";
     std::string xyz_file;
+    std::vector<std::pair<std::string, std::string>> groupfiles;
+    std::string typefile;
+    double cg_rtol = -1, cg_atol = -1;
 };
+
+static std::vector<int> read_i32(const std::string &path)
+{
+    std::vector<int> v;
+    FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f)
+    {
+        std::fprintf(stderr, "cannot open %s\n", path.c_str());
+        std::exit(2);
+    }
+    int x;
+    while (std::fread(&x, sizeof(int), 1, f) == 1)
+        v.push_back(x);
+    std::fclose(f);
+    return v;
+}
 
 static Spec parse(const char *path)
 {
@@ -191,6 +213,14 @@ static Spec parse(const char *path)
         else if (k == "loop") is >> s.loop;
         else if (k == "out") is >> s.out;
         else if (k == "xyz_file") is >> s.xyz_file;
+        else if (k == "groupfile")
+        {
+            std::string n, pth;
+            is >> n >> pth;
+            s.groupfiles.push_back({n, pth});
+        }
+        else if (k == "typefile") is >> s.typefile;
+        else if (k == "cg_tol") is >> s.cg_rtol >> s.cg_atol;
         else
         {
             std::fprintf(stderr, "unknown spec directive '%s'\n", k.c_str());
@@ -239,6 +269,8 @@ int main(int argc, char **argv)
     }
     Spec sp = parse(argv[1]);
     lpm_shim_stats_g.cg_maxit_override = sp.cg_maxit_cap;
+    lpm_shim_stats_g.cg_rtol_override = sp.cg_rtol;
+    lpm_shim_stats_g.cg_atol_override = sp.cg_atol;
     const double t_setup0 = wall();
 
     UnitCell cell(lattice_of(sp.lattice), sp.radius);
@@ -286,6 +318,19 @@ int main(int argc, char **argv)
                 mem.push_back(p);
         }
         groups[g.name] = mem;
+    }
+    for (auto &gf : sp.groupfiles)
+    {
+        std::vector<Particle<NL> *> mem;
+        for (int id : read_i32(gf.second))
+            mem.push_back(ass.pt_sys[id]);
+        groups[gf.first] = mem;
+    }
+    if (!sp.typefile.empty())
+    {
+        std::vector<int> t = read_i32(sp.typefile);
+        for (Particle<NL> *p : ass.pt_sys)
+            p->type = t[p->id];
     }
     for (auto &st : sp.settypes)
         for (Particle<NL> *p : groups[st.first])

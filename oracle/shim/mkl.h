@@ -94,6 +94,8 @@ struct lpm_shim_stats
     double create_seconds;    /* wall time inside mkl_sparse_d_create_csr */
     long long cg_failures;    /* dcg returned a negative request */
     long long cg_maxit_override; /* if > 0, caps ipar[4] at this value (bounded CPU samples) */
+    double cg_rtol_override;     /* if >= 0, replaces dpar[0] at dcg_check (tightened parity runs) */
+    double cg_atol_override;     /* if >= 0, replaces dpar[1] at dcg_check */
 };
 extern struct lpm_shim_stats lpm_shim_stats_g;
 }

@@ -28,7 +28,7 @@
 #endif
 
 extern "C" {
-struct lpm_shim_stats lpm_shim_stats_g = {0, 0, 0, 0.0, 0.0, 0.0, 0, 0};
+struct lpm_shim_stats lpm_shim_stats_g = {0, 0, 0, 0.0, 0.0, 0.0, 0, 0, -1.0, -1.0};
 }
 
 static double now_s()
@@ -236,6 +236,10 @@ void dcg_check(const MKL_INT *n, const double *x, const double *b, MKL_INT *rci_
     }
     if (lpm_shim_stats_g.cg_maxit_override > 0 && ipar[4] > lpm_shim_stats_g.cg_maxit_override)
         ipar[4] = (MKL_INT)lpm_shim_stats_g.cg_maxit_override;
+    if (lpm_shim_stats_g.cg_rtol_override >= 0)
+        dpar[0] = lpm_shim_stats_g.cg_rtol_override;
+    if (lpm_shim_stats_g.cg_atol_override >= 0)
+        dpar[1] = lpm_shim_stats_g.cg_atol_override;
     *rci_request = 0;
 }
 

@@ -1,0 +1,47 @@
+"""Shared helpers: build the same problem in the CPU oracle and on the device."""
+import importlib
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from oracle import oracle as O  # noqa: E402
+
+LPM = importlib.import_module("lpm-cpp_b200.lpm")
+CFG = importlib.import_module("lpm-cpp_b200.configs")
+
+LAT_NAME = {0: "sq2d", 1: "hex2d", 2: "sc3d", 3: "fcc3d", 4: "bcc3d"}
+
+
+def oracle_problem(case, cg_rtol=1e-12, cg_atol=1e-12, tol_iter=None, max_iter=None):
+    m = case.material
+    mat = O.Material(ptype="j2" if int(case.ptype) == 2 else "elastic", plane_stress=m.plane_stress, E=m.E, mu=m.mu,
+                     critical_bstrain=m.critical_bstrain, sigmay=m.sigmay, xi=m.xi, H=m.H, A=m.A,
+                     nonlocal_L=m.nonlocal_L)
+    return O.OracleProblem(LAT_NAME[int(case.lattice)], case.radius, case.xyz, mat, types=case.types,
+                           undamaged_type=case.undamaged_type,
+                           max_iter=case.max_iter if max_iter is None else max_iter,
+                           tol_iter=case.tol_iter if tol_iter is None else tol_iter, cg_rtol=cg_rtol, cg_atol=cg_atol)
+
+
+def gpu_problem(case, precision=0, cg_rtol=1e-12, cg_atol=1e-12, tol_iter=None, max_iter=None):
+    return LPM.GpuProblem(case.assembly(), undamaged_pt_type=case.undamaged_type,
+                          max_iter=case.max_iter if max_iter is None else max_iter,
+                          tol_iter=case.tol_iter if tol_iter is None else tol_iter,
+                          precision=LPM.Precision(precision), cg_rtol=cg_rtol, cg_atol=cg_atol)
+
+
+def oracle_step_args(case, s):
+    disp, force = case.steps[s]
+    flag = {"x": 0, "y": 1, "z": 2}
+    return ([(case.groups[g], flag[f], v) for g, f, v in disp],
+            [(case.groups[g], fx, fy, fz) for g, fx, fy, fz in force])
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)

@@ -1,0 +1,194 @@
+"""Parity of the device path (through the C ABI) with the CPU oracle on the same inputs.
+
+Bars: bond lists, connection lists and the reference CSR pattern bit-exact; internal forces
+bit-exact; stiffness entries within 1e-12 of max|K| (bit-exact except the BC diagonal, whose
+norm is a tree sum on the device); displacements within 1e-8 relative (FP64 path, both sides
+solving tightly) and 1e-6 relative (mixed path).
+"""
+import numpy as np
+import pytest
+
+from _util import CFG, LPM, O, gpu_problem, oracle_problem, oracle_step_args, rel
+
+pytestmark = pytest.mark.gpu
+
+K_TOL = 1e-12
+FP64_DISP_TOL = 1e-8
+MIXED_DISP_TOL = 1e-6
+
+
+def small_cases():
+    return {
+        "hex": CFG.hex_plate(size=3.0, radius=0.1, steps=3, total_disp=0.003),
+        "sc": CFG.sc_cube(size=2.4, radius=0.2, steps=3, total_disp=0.003),
+        "sq": _square(),
+        "fcc_j2": CFG.fcc_bar(size=(1.6, 1.6, 2.4), radius=0.2, steps=3, strain=0.02),
+        "sc_j2": CFG.sc_cube(size=2.0, radius=0.25, steps=3, total_disp=0.06, ptype=LPM.ParticleType.J2Plasticity,
+                             j2=(200.0, 0.0, 38714.0, 10.0)),
+    }
+
+
+def _square():
+    c = CFG.hex_plate(size=2.0, radius=0.1, steps=2, total_disp=0.002)
+    xyz = LPM.createPlateSQ2D(c.box, LPM.UnitCell(LPM.LatticeType.Square2D, 0.1))
+    top = np.nonzero(xyz[:, 1] > c.box[3] - 0.2)[0].astype(np.int32)
+    bot = np.nonzero(xyz[:, 1] < c.box[2] + 0.2)[0].astype(np.int32)
+    c.lattice, c.xyz, c.types = LPM.LatticeType.Square2D, xyz, np.zeros(len(xyz), np.int32)
+    c.groups = {"top": top, "bottom": bot}
+    c.name = "sq2d"
+    return c
+
+
+CASES = small_cases()
+
+
+@pytest.fixture(scope="module", params=sorted(CASES))
+def case(request):
+    return CASES[request.param]
+
+
+def test_topology_bit_exact(case):
+    g = gpu_problem(case)
+    o = oracle_problem(case)
+    t = g.topology()
+    nb0, nb1, p2 = o.bonds()
+    nconn, nlq, conns = o.conns()
+    assert np.array_equal(t["nb0"], nb0)
+    assert np.array_equal(t["nb1"], nb1)
+    assert np.array_equal(t["bond_p2"], p2)
+    assert np.array_equal(t["nconn"], nconn)
+    assert np.array_equal(t["nlq"], nlq)
+    assert np.array_equal(t["conns"], conns)
+    Kp, IK, JK, K = g.export_csr()
+    assert g.sizes["nnz_upper"] == o.export_csr()[0][-1]
+    assert np.array_equal(Kp, o.export_csr()[0])
+
+
+def test_initial_force_bit_exact(case):
+    g = gpu_problem(case)
+    o = oracle_problem(case)
+    o.update_geometry()
+    o.update_force_state()
+    sg, so = g.state(), o.state()
+    assert np.array_equal(sg["pin"], so["pin"])
+    assert np.array_equal(sg["stress"], so["stress"])
+    assert np.array_equal(sg["damage_visual"], so["damage_visual"])
+
+
+def test_stiffness_matches(case):
+    g = gpu_problem(case)
+    o = oracle_problem(case)
+    o.update_geometry()
+    o.update_force_state()
+    disp, force = oracle_step_args(case, 0)
+    o.apply_bc(disp, force)
+    g.apply_load_step(case.load_step(0))
+    for apply_bc in (False, True):
+        o.assemble(apply_bc)
+        g.assemble(apply_bc)
+        Kp, IK, JK, K = g.export_csr()
+        oKp, oIK, oJK, oK = o.export_csr()
+        assert np.array_equal(IK, oIK)
+        assert np.array_equal(JK, oJK)
+        err = np.abs(K - oK).max() / np.abs(oK).max()
+        assert err <= K_TOL, f"apply_bc={apply_bc}: max rel {err}"
+        if not apply_bc:
+            assert np.array_equal(K, oK), "stiffness before the BC elimination should be bit-exact"
+
+
+def test_linear_solve(case):
+    g = gpu_problem(case, cg_rtol=1e-24, cg_atol=0.0)
+    o = oracle_problem(case, cg_rtol=1e-24, cg_atol=0.0)
+    o.update_geometry()
+    o.update_force_state()
+    disp, force = oracle_step_args(case, 0)
+    o.apply_bc(disp, force)
+    g.apply_load_step(case.load_step(0))
+    o.assemble(True)
+    g.assemble(True)
+    o.update_geometry()
+    o.update_force_state()
+    ro = o.update_rr()
+    g.update_force_state()
+    rg = g.update_rr()
+    assert np.array_equal(g.residual(), o.residual())
+    assert abs(rg - ro) <= 1e-14 * max(ro, 1e-300)
+    xo, _ = o.cg()
+    xg, st = g.solve_linear()
+    assert rel(xg, xo) <= 1e-9, rel(xg, xo)
+    assert st["cg_iters"] > 0
+
+
+@pytest.mark.parametrize("precision,tol", [(0, FP64_DISP_TOL), (1, MIXED_DISP_TOL)])
+def test_load_steps(case, precision, tol):
+    kw = dict(cg_rtol=1e-24, cg_atol=0.0, tol_iter=1e-9)
+    g = gpu_problem(case, precision=precision, **kw)
+    o = oracle_problem(case, **kw)
+    o.update_geometry()
+    o.update_force_state()
+    x0 = case.xyz
+    for s in range(len(case.steps)):
+        okg, stg = g.solve_load_step(case.load_step(s))
+        oko, sto = o.solve_load_step(*oracle_step_args(case, s))
+        assert okg and oko
+        sg, so = g.state(), o.state()
+        e = rel(sg["xyz"] - x0, so["xyz"] - x0)
+        assert e <= tol, f"step {s}: rel disp err {e}"
+        assert abs(stg["reaction_norm"] - sto["reaction_norm"]) <= tol * sto["reaction_norm"] * 10
+        if int(case.ptype) == 2:
+            e_sv = rel(sg["state_var"], so["state_var"])
+            assert e_sv <= 100 * tol, f"step {s}: state_var rel err {e_sv}"
+
+
+def test_reference_tolerances_fp64():
+    """The reference's own settings (CG 1e-12 on squared norms, Newton 1e-5): same Newton and
+    close CG iteration counts, displacements close."""
+    case = CFG.hex_plate(size=3.0, radius=0.1, steps=2, total_disp=0.002)
+    g = gpu_problem(case)
+    o = oracle_problem(case)
+    o.update_geometry()
+    o.update_force_state()
+    for s in range(2):
+        okg, stg = g.solve_load_step(case.load_step(s))
+        oko, sto = o.solve_load_step(*oracle_step_args(case, s))
+        assert okg and oko
+        assert stg["newton_solves"] == sto["newton_solves"]
+        assert abs(stg["cg_iters"] - sto["cg_iters"]) <= 0.05 * sto["cg_iters"] + 3
+        assert rel(g.state()["xyz"] - case.xyz, o.state()["xyz"] - case.xyz) <= 1e-5
+
+
+def test_damage_bonds_break():
+    """Brittle bonds (particle_elastic.h:52-68): the same bonds break in the same load steps."""
+    case = CFG.hex_plate(size=2.0, radius=0.1, steps=3, total_disp=0.024, critical_bstrain=3e-3)
+    kw = dict(cg_rtol=1e-24, cg_atol=0.0, tol_iter=1e-9)
+    g = gpu_problem(case, **kw)
+    o = oracle_problem(case, **kw)
+    o.update_geometry()
+    o.update_force_state()
+    broke = 0
+    for s in range(3):
+        okg, stg = g.solve_load_step(case.load_step(s))
+        oko, sto = o.solve_load_step(*oracle_step_args(case, s))
+        assert okg == oko
+        bg, bo = g.state()["bdamage"], o.state()["bdamage"]
+        assert np.array_equal(bg, bo), f"step {s}: broken bond sets differ"
+        broke = int((bo == 1).sum())
+        assert rel(g.state()["xyz"] - case.xyz, o.state()["xyz"] - case.xyz) <= FP64_DISP_TOL
+    assert broke > 0, "the case should break some bonds"
+
+
+def test_cut_back_matches():
+    """A small Newton cap makes the full step fail; it is halved and retried
+    (solver_static.h:78-87), with the same number of cuts as the oracle."""
+    case = CFG.hex_plate(size=2.0, radius=0.1, steps=1, total_disp=0.01)
+    kw = dict(cg_rtol=1e-24, cg_atol=0.0, tol_iter=1e-9, max_iter=5)
+    g = gpu_problem(case, **kw)
+    o = oracle_problem(case, **kw)
+    o.update_geometry()
+    o.update_force_state()
+    okg, stg = g.solve_load_step(case.load_step(0))
+    oko, sto = o.solve_load_step(*oracle_step_args(case, 0))
+    assert okg == oko
+    assert stg["cuts"] == sto["cuts"]
+    if okg:
+        assert rel(g.state()["xyz"] - case.xyz, o.state()["xyz"] - case.xyz) <= FP64_DISP_TOL
