@@ -1,0 +1,429 @@
+#!/usr/bin/env python
+"""Benchmark of the implicit quasi-static LPM load step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config sc3d|hex2d]
+
+A step is one quasi-static load step (stiffness assembly, Newton iterations with CG solves,
+damage/state update) of the workload.  Default workload: the 3D simple-cubic cube of
+20 x 20 x 20 mm at particle radius 0.2 mm (127,500 particles, 382,500 DOF), elastic
+E = 200 GPa, nu = 0.25, pulled 0.001 mm per step (20-step path; further steps repeat the
+increment).  Inputs are synthetic (the reference's lattice generator).  The stiffness matrix
+(~0.56 GB in FP64) exceeds the 126 MB L2, so no flush is needed between steps.
+
+Headline `value`: DOF-iterations per second of the FP64 path (sum over CG iterations of the DOF
+count, divided by device time), the reference's own precision.  Beside it: load-step solves/s,
+p50/p99 load-step latency, the mixed FP32-Krylov/FP64-refinement path with its displacement
+error against the FP64 path, the end-to-end rate through the C ABI with host buffers, the HBM
+roofline of the CG kernel and the reference's CPU path timed on this host.
+
+With N > 1 (torchrun) every rank solves its own replica (the path does not shard inside one
+solve): value is the sum over ranks, time is the max over ranks, scaling "weak".
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "LPM solves/sec & DOF-iter/s at ≤1e-6 rel err vs FP64; p50/p99 solve latency"
+UNIT = "DOF-iter/s"
+NEWTON_TOL = 1e-8  # tight enough that FP64 and mixed agree to 1e-6 in displacement
+
+
+def args_():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="sc3d", choices=["sc3d", "hex2d"])
+    ap.add_argument("--size", type=float, default=20.0, help="specimen edge in mm (20 = the headline workload)")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-cg-cap", type=int, default=400, help="CG iterations per solve in the CPU sample")
+    return ap.parse_args()
+
+
+def workload(name, size=20.0):
+    cfg = importlib.import_module("lpm-cpp_b200.configs")
+    if name == "hex2d":
+        c = cfg.hex_plate(size=size, radius=0.1, steps=10, total_disp=0.01, tol_iter=NEWTON_TOL)
+        desc = f"hex2d {size:g}x{size:g} mm r=0.1 plane stress, E=69 GPa, 10 x 0.001 mm top-edge tension"
+    else:
+        c = cfg.sc_cube(size=size, radius=0.2, steps=20, total_disp=0.001 * 20 * size / 20.0, tol_iter=NEWTON_TOL)
+        desc = (f"sc3d {size:g}x{size:g}x{size:g} mm r=0.2 elastic, E=200 GPa nu=0.25, "
+                f"20 x {0.001 * size / 20.0:g} mm top-face tension")
+    return c, desc
+
+
+def step_of(case, s):
+    return case.load_step(s % len(case.steps))
+
+
+def algorithmic_bytes_per_iter(nnzb, n, dim, s_k, s_v):
+    """Bytes one CG iteration must move: the block matrix (values + int32 block column), the
+    row pointers and 9 vector passes (read p, write Ap, read Ap, r/w x, r/w r, r/w p)."""
+    return nnzb * (dim * dim * s_k + 4) + (n + 1) * 4 + 9 * dim * n * s_v
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel_tag):
+    """DRAM bytes per CG iteration from the committed ncu summary, if there is one."""
+    path = os.path.join(ROOT, "profiles", f"{kernel_tag}.md")
+    try:
+        with open(path) as f:
+            m = re.search(r"traffic_bytes_per_iter:\s*([0-9.eE+]+)", f.read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(prefix="clk_", suffix=".csv")
+        os.close(fd)
+        self.fh = open(self.path, "w")
+        self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                      "-lms", "200", "-i", str(self.device)], stdout=self.fh,
+                                     stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                t = [x.strip() for x in line.split(",")]
+                if len(t) < 9:
+                    continue
+                try:
+                    sm.append(float(t[1]))
+                    mx.append(float(t[2]))
+                except ValueError:
+                    continue
+                for k, nm in enumerate(names):
+                    if t[5 + k].lower() == "active":
+                        reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def reduce_ranks(pairs, dist, device):
+    """[(value, "max"|"sum"), ...] reduced over the ranks of the process group (identity with
+    no group).  Timing is the max over ranks, work is the sum."""
+    if dist is None:
+        return [float(v) for v, _ in pairs]
+    import torch
+    out = []
+    for v, op in pairs:
+        t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+        out.append(float(t.item()))
+    return out
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ------------------------------------------------------------------------------------ our arm
+def run_ours(a):
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    lpm = importlib.import_module("lpm-cpp_b200.lpm")
+    case, desc = workload(a.config, a.size)
+    W, K = a.warmup, a.steps
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def allreduce(v, op):
+        return reduce_ranks([(v, op)], dist, "cuda")[0]
+
+    prob = lpm.GpuProblem(case.assembly(), undamaged_pt_type=case.undamaged_type, max_iter=case.max_iter,
+                          tol_iter=case.tol_iter, precision=lpm.Precision.FP64, device=local)
+    sizes = prob.sizes
+    n, dim, nnzb = sizes["n"], sizes["dim"], sizes["nnzb"]
+    ndof = n * dim
+    stream = torch.cuda.ExternalStream(prob.stream_ptr())
+    for s in range(W):
+        ok, _ = prob.solve_load_step(step_of(case, s))
+        assert ok, f"warm-up step {s} did not converge"
+    barrier()
+    torch.cuda.synchronize()
+    c0 = prob.counters()
+    clk = ClockSampler(local)
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    stats = []
+    for s in range(W, W + K):
+        ok, st = prob.solve_load_step(step_of(case, s))
+        assert ok, f"step {s} did not converge"
+        stats.append(st)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1)
+    c1 = prob.counters()
+    barrier()
+    xyz_fp64 = prob.state(("xyz",))["xyz"]
+
+    iters = sum(st["cg_iters"] for st in stats)
+    ms_max = allreduce(ms, "max")
+    dof_iters_total = allreduce(float(ndof * iters), "sum")
+    value = dof_iters_total / (ms_max * 1e-3)
+    lat = sorted(st["seconds"] * 1e3 for st in stats)
+    cg_s = c1["cg_kernel_seconds"] - c0["cg_kernel_seconds"]
+    cg_it = c1["cg_iters"] - c0["cg_iters"]
+    cg_launch = c1["cg_launches"] - c0["cg_launches"]
+    b_iter = algorithmic_bytes_per_iter(nnzb, n, dim, 8, 8)
+    peak, peak_kind = measured_peak()
+    achieved = b_iter * cg_it / cg_s / 1e9 if cg_s > 0 else 0.0
+    tr = profiled_traffic("cg_fp64_sc3d") if a.config == "sc3d" and a.size == 20.0 else None
+    roof = {"bound": "hbm", "kernel": "k_cg<double,double,3> (persistent CG)", "achieved": round(achieved, 1),
+            "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+            "traffic": (tr * cg_it / max(cg_launch, 1)) if tr else None,
+            "algorithmic_bytes_per_iter": b_iter, "iters_per_launch": cg_it / max(cg_launch, 1),
+            "avg_launch_ms": cg_s / max(cg_launch, 1) * 1e3}
+
+    # end to end through the C ABI with host buffers: pinned group ids in, positions out
+    pin_groups = {}
+    for g, ids in case.groups.items():
+        t = torch.empty(len(ids), dtype=torch.int32, pin_memory=True)
+        t.numpy()[:] = ids
+        pin_groups[g] = t
+    out = torch.empty((n, 3), dtype=torch.float64, pin_memory=True)
+    h2d = 0
+    steps_e2e = []
+    for s in range(W + K, W + 2 * K):
+        disp, force = case.steps[s % len(case.steps)]
+        st = lpm.LoadStep()
+        for g, fl, v in disp:
+            st.dispBCs.append(lpm.DispBC(pin_groups[g].numpy(), lpm.LoadMode.Relative, fl, v))
+        for g, fx, fy, fz in force:
+            st.forceBCs.append(lpm.ForceBC(pin_groups[g].numpy(), lpm.LoadMode.Relative, fx, fy, fz))
+        steps_e2e.append(st)
+        h2d = sum(len(b.group) * 4 for b in st.dispBCs + st.forceBCs)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_iters = 0
+    for st in steps_e2e:
+        ok, s2 = prob.solve_load_step(st)
+        assert ok
+        e2e_iters += s2["cg_iters"]
+        prob.read_xyz_into(out.numpy())
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    wall_max = allreduce(wall, "max")
+    e2e_total = allreduce(float(ndof * e2e_iters), "sum")
+    e2e = {"value": e2e_total / wall_max, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": n * 3 * 8,
+           "solves_per_s": world * K / wall_max}
+    counters_total = c1["kernel_launches"] - c0["kernel_launches"]
+    prob.close()
+
+    # mixed precision on the same path, compared with the FP64 positions after the same steps
+    mixed = None
+    if not a.no_mixed:
+        pm = lpm.GpuProblem(case.assembly(), undamaged_pt_type=case.undamaged_type, max_iter=case.max_iter,
+                            tol_iter=case.tol_iter, precision=lpm.Precision.MIXED, device=local)
+        sm = torch.cuda.ExternalStream(pm.stream_ptr())
+        for s in range(W):
+            ok, _ = pm.solve_load_step(step_of(case, s))
+            assert ok
+        barrier()
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(sm)
+        mst = []
+        for s in range(W, W + K):
+            ok, st = pm.solve_load_step(step_of(case, s))
+            assert ok
+            mst.append(st)
+        f1.record(sm)
+        torch.cuda.synchronize()
+        mms = allreduce(f0.elapsed_time(f1), "max")
+        xm = pm.state(("xyz",))["xyz"]
+        u64, um = xyz_fp64 - case.xyz, xm - case.xyz
+        err = float(np.linalg.norm(um - u64) / np.linalg.norm(u64))
+        miters = sum(st["cg_iters"] for st in mst)
+        mixed = {"solves_per_s": world * K / (mms * 1e-3), "ms_per_step": mms / K,
+                 "dof_iter_per_s": allreduce(float(ndof * miters), "sum") / (mms * 1e-3),
+                 "rel_disp_err_vs_fp64": err, "cg_iters_per_step": miters / K,
+                 "speedup_vs_fp64": (ms_max / K) / (mms / K)}
+        pm.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(case, a.cpu_cg_cap)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (reference lattice generator)",
+            "config": {"workload": desc, "particles": n, "dof": ndof, "block_nnz": nnzb,
+                       "nnz_upper_ref_csr": sizes["nnz_upper"], "newton_tol": NEWTON_TOL,
+                       "cg_test": "||r||^2 <= 1e-12 ||r0||^2 + 1e-12 (reference)",
+                       "l2": "stiffness larger than L2 (126 MB); no flush", "parallelism": f"replicas x{world}"},
+            "solves_per_s": world * K / (ms_max * 1e-3),
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "newton_per_step": sum(st["newton_solves"] for st in stats) / K,
+            "cg_iters_per_step": iters / K,
+            "roofline": roof, "e2e": e2e, "gpu_launches": counters_total, "clocks": clocks,
+            "mixed": mixed, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------------------------ CPU legs
+def _ref_sample(case, steps, cg_cap, threads, timeout=1800):
+    from oracle import oracle as O
+    d = tempfile.mkdtemp(prefix="lpmref_")
+    try:
+        spec = O.write_ref_spec(case, d, steps=steps, max_iter=1, cg_maxit_cap=cg_cap, loop="once",
+                                tol_iter=case.tol_iter)
+        O.run_ref(spec, d, threads=threads, timeout=timeout)
+        rows = O.read_ref_steps(d)
+        with open(os.path.join(d, "steps.txt")) as f:
+            head = f.readline()
+        setup = float(re.search(r"setup_s ([0-9.]+)", head).group(1))
+        return rows, setup
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def cpu_baseline(case, cg_cap):
+    """The reference's CPU path on this host: one SolverStatic::solveProblemStep call on the
+    same problem, one Newton solve with CG capped at cg_cap iterations (bounded sample).  Falls
+    back to the single-threaded C restatement when the reference build is absent."""
+    from oracle import oracle as O
+    ndof = case.n * case.dim
+    threads = os.cpu_count() or 1
+    if O.ref_available():
+        rows, setup = _ref_sample(case, 1, cg_cap, threads)
+        it = sum(r["cg_iters"] for r in rows)
+        wall = sum(r["wall_s"] for r in rows)
+        return {"value": ndof * it / wall, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": f"1 solveProblemStep call of the same workload, 1 Newton solve, CG capped at {cg_cap} "
+                          f"iterations ({it} iterations, {wall:.1f} s; setup {setup:.1f} s untimed); "
+                          "LPM-CPP headers compiled unmodified, MKL replaced by the oracle/shim stand-in",
+                "cg_spmv_s_per_iter": sum(r["spmv_s"] for r in rows) / max(it, 1)}
+    mat = O.Material(ptype="j2" if int(case.ptype) == 2 else "elastic", plane_stress=case.material.plane_stress,
+                     E=case.material.E, mu=case.material.mu, critical_bstrain=case.material.critical_bstrain)
+    lat = {0: "sq2d", 1: "hex2d", 2: "sc3d", 3: "fcc3d", 4: "bcc3d"}[int(case.lattice)]
+    o = O.OracleProblem(lat, case.radius, case.xyz, mat, types=case.types, cg_maxit=cg_cap)
+    o.update_geometry()
+    o.update_force_state()
+    flag = {"x": 0, "y": 1, "z": 2}
+    disp = [(case.groups[g], flag[f], v) for g, f, v in case.steps[0][0]]
+    o.apply_bc(disp, [])
+    t0 = time.perf_counter()
+    o.assemble(True)
+    o.update_geometry()
+    o.update_force_state()
+    o.update_rr()
+    _, it = o.cg()
+    wall = time.perf_counter() - t0
+    return {"value": ndof * it / wall, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"C restatement: assembly + 1 CG solve capped at {cg_cap} iterations"}
+
+
+def run_reference(a):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    case, desc = workload(a.config, a.size)
+    ndof = case.n * case.dim
+    threads = os.cpu_count() or 1
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/lpm_ref was not built on this machine"}))
+        return
+    W, K = a.warmup, a.steps
+    cap = max(50, a.cpu_cg_cap // 2)
+    rows, setup = _ref_sample(case, W + K, cap, threads, timeout=3600)
+    timed = rows[W:W + K]
+    it = sum(r["cg_iters"] for r in timed)
+    wall = sum(r["wall_s"] for r in timed)
+    value = ndof * it / wall
+    sample = (f"{K} timed of {W + K} solveProblemStep calls (1 Newton solve each, CG capped at {cap} iterations) "
+              f"of the same workload; setup {setup:.1f} s untimed; LPM-CPP headers compiled unmodified, MKL "
+              "replaced by the oracle/shim stand-in")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": wall / K * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference lattice generator)",
+        "config": {"workload": desc, "particles": case.n, "dof": ndof, "parallelism": "host OpenMP"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    a = args_()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -176,6 +176,20 @@ int32_t lpmgpu_set_xyz(lpmgpu_solver *h, const double *xyz);
  * [2] linear solves, [3] other */
 int32_t lpmgpu_get_phase_times(const lpmgpu_solver *h, double *t4);
 
+/* Cumulative counters of the handle since creation. */
+typedef struct
+{
+    int64_t kernel_launches;   /* device kernels this handle launched */
+    int64_t cg_launches;       /* persistent CG kernel launches */
+    int64_t cg_iters;          /* CG iterations over all launches */
+    double cg_kernel_seconds;  /* device time inside the CG kernel launches (CUDA events) */
+    double assembly_seconds;   /* device time of stiffness assembly + BC elimination */
+    double force_seconds;      /* device time of geometry / force / residual passes */
+} lpmgpu_counters;
+int32_t lpmgpu_get_counters(const lpmgpu_solver *h, lpmgpu_counters *out);
+/* The CUDA stream (cudaStream_t) the handle launches on, for callers that time with events. */
+int32_t lpmgpu_get_stream(const lpmgpu_solver *h, void **stream);
+
 #ifdef __cplusplus
 }
 #endif

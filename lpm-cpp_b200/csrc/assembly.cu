@@ -1,4 +1,5 @@
-// Global stiffness assembly: one CTA per particle row, deterministic, no atomics.
+// Global stiffness assembly: one CTA per particle row, deterministic, no atomics.  The
+// output is the sliced-ELL layout described in lpm_internal.cuh.
 //
 // The reference (include/stiffness.h:198-361) evaluates localStiffnessANA(pi, pj) for every
 // pj in conns(pi) by re-walking bond lists (include/derivative.h:8-239), then scatters
@@ -29,6 +30,8 @@ struct AsmArgs
     int n, dim, mb;
     const int *__restrict__ bstart, *__restrict__ nb0, *__restrict__ bp2, *__restrict__ brev;
     const int *__restrict__ cstart, *__restrict__ conns, *__restrict__ cons;
+    const int *__restrict__ perm;
+    const int64_t *__restrict__ slice_off;
     const double *__restrict__ cs, *__restrict__ Kn, *__restrict__ Tv, *__restrict__ bdamage;
     const double *__restrict__ cs_sum, *__restrict__ damage_visual;
     double *__restrict__ K, *__restrict__ diag_raw;
@@ -162,7 +165,12 @@ __device__ __forceinline__ void add_direct(double acc[3][3], int d, double D, do
 __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int i = blockIdx.x;
+    // CTAs run in sliced-ELL order, so the rows of one slice (whose entries interleave in
+    // memory) are written at about the same time and their partial sectors merge in L2
+    const int pos = blockIdx.x;
+    const int i = a.perm[pos];
+    const int lane = pos % kSlice;
+    const int64_t sbase = a.slice_off[pos / kSlice];
     const int tid = threadIdx.x;
     const int mb = a.mb, d = a.dim;
     AsmSmem s = carve(smem_raw, mb);
@@ -361,10 +369,10 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs a)
                     out[r][q] = (ci[r] || cj[q]) ? 0.0 : v;
                 }
         }
-        double *dst = a.K + ((int64_t)c0 + sl) * d * d;
+        double *dst = a.K + (sbase + sl) * d * d * kSlice + lane;
         for (int r = 0; r < d; ++r)
             for (int q = 0; q < d; ++q)
-                dst[r * d + q] = out[r][q];
+                dst[(r * d + q) * kSlice] = out[r][q];
     }
 }
 
@@ -395,34 +403,23 @@ __global__ void k_diag_norm(int64_t m, const double *__restrict__ diag, Scalars 
     }
 }
 
-__global__ void k_bc_diag(int n, int dim, const int *__restrict__ cstart, const int *__restrict__ conns,
-                          const int *__restrict__ cons, const double *__restrict__ damage_visual,
-                          const Scalars *__restrict__ scal, double *__restrict__ K)
+// the self block is connection slot nconn - nconn_largeq (conns >= i are the last nlq entries)
+__global__ void k_bc_diag(int n, int dim, const int *__restrict__ perm, const int64_t *__restrict__ slice_off,
+                          const int *__restrict__ cstart, const int *__restrict__ nlq, const int *__restrict__ cons,
+                          const double *__restrict__ damage_visual, const Scalars *__restrict__ scal,
+                          double *__restrict__ K)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n)
         return;
+    const int i = perm[pos];
     const bool dmg = fabs(damage_visual[i] - 1.0) < kEps;
-    int lo = cstart[i], hi = cstart[i + 1] - 1, self = -1;
-    while (lo <= hi)
-    {
-        const int mid = (lo + hi) >> 1;
-        if (conns[mid] == i)
-        {
-            self = mid;
-            break;
-        }
-        if (conns[mid] < i)
-            lo = mid + 1;
-        else
-            hi = mid - 1;
-    }
-    if (self < 0)
-        return;
+    const int self = (cstart[i + 1] - cstart[i]) - nlq[i];
+    const int64_t b = slice_off[pos / kSlice] + self;
     const double nd = scal->norm_diag;
     for (int k = 0; k < dim; ++k)
         if (cons[3 * i + k] == 1 || dmg)
-            K[(int64_t)self * dim * dim + k * dim + k] = nd;
+            K[(b * dim * dim + k * dim + k) * kSlice + pos % kSlice] = nd;
 }
 
 cudaError_t launch_assemble(Problem &p, bool apply_bc)
@@ -444,6 +441,8 @@ cudaError_t launch_assemble(Problem &p, bool apply_bc)
     a.bdamage = p.bdamage;
     a.cs_sum = p.cs_sum;
     a.damage_visual = p.damage_visual;
+    a.perm = p.perm;
+    a.slice_off = p.slice_off;
     a.K = p.K;
     a.diag_raw = p.diag_raw;
     a.apply_bc = apply_bc ? 1 : 0;
@@ -452,13 +451,15 @@ cudaError_t launch_assemble(Problem &p, bool apply_bc)
     if (e != cudaSuccess)
         return e;
     k_assemble<<<p.n, kAsmThreads, smem, p.stream>>>(a);
+    p.ctr.kernel_launches++;
     if ((e = cudaGetLastError()) != cudaSuccess)
         return e;
     if (apply_bc)
     {
         k_diag_norm<<<1, 1024, 0, p.stream>>>((int64_t)p.n * p.dim, p.diag_raw, p.scal);
-        k_bc_diag<<<div_up(p.n, 256), 256, 0, p.stream>>>(p.n, p.dim, p.cstart, p.conns, p.cons, p.damage_visual,
-                                                          p.scal, p.K);
+        k_bc_diag<<<div_up(p.n, 256), 256, 0, p.stream>>>(p.n, p.dim, p.perm, p.slice_off, p.cstart, p.nlq, p.cons,
+                                                          p.damage_visual, p.scal, p.K);
+        p.ctr.kernel_launches += 2;
         e = cudaGetLastError();
     }
     return e;
@@ -467,7 +468,8 @@ cudaError_t launch_assemble(Problem &p, bool apply_bc)
 // Reference layout (stiffness.h:24-26, 198-361): row (i, r) starts at
 // K_pointer[i] + r*dim*nlq - r(r-1)/2; self block entries c >= r, then the blocks of conns >= i.
 __global__ void k_export_ref(int n, int dim, const int *__restrict__ cstart, const int *__restrict__ conns,
-                             const int *__restrict__ nlq, const int64_t *__restrict__ kp, const double *__restrict__ K,
+                             const int *__restrict__ nlq, const int64_t *__restrict__ kp, const int *__restrict__ iperm,
+                             const int64_t *__restrict__ slice_off, const double *__restrict__ K,
                              int64_t *__restrict__ IK, int64_t *__restrict__ JK, double *__restrict__ V)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -475,19 +477,21 @@ __global__ void k_export_ref(int n, int dim, const int *__restrict__ cstart, con
         return;
     const int i = t / dim, r = t % dim;
     const int c0 = cstart[i], nc = cstart[i + 1] - c0, m = nlq[i];
-    const int first = c0 + (nc - m); // self slot
+    const int self = nc - m;
+    const int pos = iperm[i], lane = pos % kSlice;
+    const int64_t sbase = slice_off[pos / kSlice];
     const int64_t start = kp[i] + (int64_t)r * dim * m - (int64_t)r * (r - 1) / 2;
     IK[(int64_t)dim * i + r] = start + 1;
-    int64_t pos = start;
+    int64_t out = start;
     for (int num = 0; num < m; ++num)
     {
-        const int sl = first + num, j = conns[sl];
-        const double *blk = K + (int64_t)sl * dim * dim;
+        const int sl = self + num, j = conns[c0 + sl];
+        const double *blk = K + (sbase + sl) * dim * dim * kSlice + lane;
         for (int c = (num == 0 ? r : 0); c < dim; ++c)
         {
-            JK[pos] = (int64_t)dim * j + c + 1;
-            V[pos] = blk[r * dim + c];
-            pos++;
+            JK[out] = (int64_t)dim * j + c + 1;
+            V[out] = blk[(r * dim + c) * kSlice];
+            out++;
         }
     }
     if (t == 0)
@@ -497,7 +501,7 @@ __global__ void k_export_ref(int n, int dim, const int *__restrict__ cstart, con
 cudaError_t launch_export_ref(const Problem &p, int64_t *IK, int64_t *JK, double *K)
 {
     k_export_ref<<<div_up((int64_t)p.n * p.dim, 256), 256, 0, p.stream>>>(p.n, p.dim, p.cstart, p.conns, p.nlq,
-                                                                          p.kp_ref, p.K, IK, JK, K);
+                                                                          p.kp_ref, p.iperm, p.slice_off, p.K, IK, JK, K);
     return cudaGetLastError();
 }
 

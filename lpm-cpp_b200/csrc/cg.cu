@@ -14,9 +14,10 @@
 // barrier is a sense-counting barrier with a time limit: a wait that exceeds it records
 // LPMGPU_ERR_TIMEOUT and the kernel returns.
 //
-// The block-CSR SpMV assigns one warp per particle row: the row's d*d*nconn values are
-// contiguous, so lanes stream them coalesced (cache-streaming loads, the matrix is read once
-// per iteration) while x gathers hit L2, where the vectors stay resident.
+// The SpMV runs on the sliced-ELL layout (lpm_internal.cuh): one thread per particle row, a
+// warp per slice of 32 rows.  For block column k every matrix plane load is 256 contiguous
+// bytes (cache-streaming: the matrix is read once per iteration) and the x gathers of the 32
+// rows hit neighbouring particles, so they coalesce and stay in L2 with the vectors.
 //
 // Mixed precision (LPMGPU_MIXED): the same kernel on an FP32 copy of K with FP32 Krylov
 // vectors (dot products in FP64), inside an FP64 iterative refinement that recomputes the
@@ -30,15 +31,19 @@
 namespace lpm
 {
 
-constexpr int kCGThreads = 512;
+constexpr int kCGThreads = 256;
+constexpr int kCGMinBlocks = 3;
 constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull; // 4 s
 
 struct CGState
 {
     int n;              // particle rows
+    int nslices;
     int64_t ndof;
-    const int *__restrict__ rowptr;
-    const int *__restrict__ cols;
+    const int *__restrict__ rowptr;     // connection CSR (row lengths)
+    const int *__restrict__ perm;       // slice position -> particle
+    const int64_t *__restrict__ slice_off;
+    const int *__restrict__ col_sell;
     double rtol, atol, abs_stop; // abs_stop >= 0 overrides rtol/atol
     int64_t maxit;
     unsigned *bar;      // [0] arrivals, [1] generation
@@ -156,47 +161,53 @@ __device__ __forceinline__ T ldstream(const T *p)
     return __ldcs(p);
 }
 
-// q_i = sum_j K_ij (r_j + beta p_old_j) for particle row i, warp-cooperative; lane 0 returns
+// q_i = sum_j K_ij (r_j + beta p_old_j) for the row at this lane of slice sl; returns the
+// particle id (-1 past the end).  Blocks in ascending connection order, entries row-major.
 template <typename TK, typename TV, int D>
-__device__ __forceinline__ void spmv_row(int row, const int *__restrict__ rowptr, const int *__restrict__ cols,
-                                         const TK *__restrict__ K, const TV *__restrict__ r,
-                                         const TV *__restrict__ pold, TV beta, TV acc[D])
+__device__ __forceinline__ int spmv_slice(int sl, int n, const int *__restrict__ rowptr, const int *__restrict__ perm,
+                                          const int64_t *__restrict__ slice_off, const int *__restrict__ col_sell,
+                                          const TK *__restrict__ K, const TV *__restrict__ r,
+                                          const TV *__restrict__ pold, TV beta, TV acc[D])
 {
     constexpr int E = D * D;
     const int lane = threadIdx.x & 31;
-    const int start = rowptr[row], nblk = rowptr[row + 1] - start;
-    const int nval = nblk * E;
-    const TK *Kr = K + (int64_t)start * E;
-    const int *cr = cols + start;
-    TV a[D];
+    const int pos = sl * kSlice + lane;
+    const bool valid = pos < n;
+    const int i = valid ? perm[pos] : -1;
+    const int myn = valid ? (rowptr[i + 1] - rowptr[i]) : 0;
+    const int64_t off = slice_off[sl];
+    const int w = (int)(slice_off[sl + 1] - off);
+    const int *cp = col_sell + off * kSlice + lane;
+    const TK *kp = K + off * E * kSlice + lane;
 #pragma unroll
     for (int k = 0; k < D; ++k)
-        a[k] = TV(0);
-#pragma unroll 4
-    for (int v = lane; v < nval; v += 32)
+        acc[k] = TV(0);
+    for (int k = 0; k < w; ++k)
     {
-        const int blk = v / E, e = v - blk * E, rr = e / D, cc = e - rr * D;
-        const int j = ldstream(cr + blk);
-        const int64_t xi = (int64_t)j * D + cc;
-        const TV xv = r[xi] + beta * pold[xi];
-        const TV prod = (TV)ldstream(Kr + v) * xv;
+        if (k < myn)
+        {
+            const int j = ldstream(cp + (int64_t)k * kSlice);
+            TV xv[D];
 #pragma unroll
-        for (int k = 0; k < D; ++k)
-            if (rr == k)
-                a[k] += prod;
-    }
+            for (int c = 0; c < D; ++c)
+                xv[c] = r[(int64_t)j * D + c] + beta * pold[(int64_t)j * D + c];
+            const TK *kb = kp + (int64_t)k * E * kSlice;
+            TK kv[E];
 #pragma unroll
-    for (int k = 0; k < D; ++k)
-    {
-        TV v = a[k];
-        for (int o = 16; o > 0; o >>= 1)
-            v += __shfl_xor_sync(0xffffffffu, v, o);
-        acc[k] = v;
+            for (int e = 0; e < E; ++e)
+                kv[e] = ldstream(kb + e * kSlice);
+#pragma unroll
+            for (int rr = 0; rr < D; ++rr)
+#pragma unroll
+                for (int c = 0; c < D; ++c)
+                    acc[rr] += (TV)kv[rr * D + c] * xv[c];
+        }
     }
+    return i;
 }
 
 template <typename TK, typename TV, int D>
-__global__ void __launch_bounds__(kCGThreads) k_cg(CGState s, const TK *__restrict__ K, const TV *__restrict__ b,
+__global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg(CGState s, const TK *__restrict__ K, const TV *__restrict__ b,
                                                    TV *__restrict__ x, TV *__restrict__ r, TV *__restrict__ pa,
                                                    TV *__restrict__ pb, TV *__restrict__ q)
 {
@@ -209,7 +220,6 @@ __global__ void __launch_bounds__(kCGThreads) k_cg(CGState s, const TK *__restri
     const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int W = (int)(T >> 5);
     const int gw = (int)(gt >> 5);
-    const int lane = threadIdx.x & 31;
 
     double loc = 0;
     for (int64_t k = gt; k < s.ndof; k += T)
@@ -238,22 +248,22 @@ __global__ void __launch_bounds__(kCGThreads) k_cg(CGState s, const TK *__restri
     for (int64_t it = 1;; ++it)
     {
         double lpq = 0;
-        for (int row = gw; row < s.n; row += W)
+        for (int sl = gw; sl < s.nslices; sl += W)
         {
             TV acc[D];
-            spmv_row<TK, TV, D>(row, s.rowptr, s.cols, K, r, pold, beta, acc);
-            if (lane < D)
+            const int i = spmv_slice<TK, TV, D>(sl, s.n, s.rowptr, s.perm, s.slice_off, s.col_sell, K, r, pold, beta,
+                                                acc);
+            if (i >= 0)
             {
-                const int64_t k = (int64_t)row * D + lane;
-                const TV pn = r[k] + beta * pold[k];
-                pnew[k] = pn;
-                TV qv = acc[0];
 #pragma unroll
-                for (int c = 1; c < D; ++c)
-                    if (lane == c)
-                        qv = acc[c];
-                q[k] = qv;
-                lpq += (double)pn * (double)qv;
+                for (int c = 0; c < D; ++c)
+                {
+                    const int64_t k = (int64_t)i * D + c;
+                    const TV pn = r[k] + beta * pold[k];
+                    pnew[k] = pn;
+                    q[k] = acc[c];
+                    lpq += (double)pn * (double)acc[c];
+                }
             }
         }
         block_partial(lpq, s.part, 1, sh);
@@ -321,30 +331,28 @@ __global__ void k_add_f32(int64_t m, const float *__restrict__ d, double *__rest
 
 // r = b - K x (FP64), partial ||r||^2 per block
 template <int D>
-__global__ void __launch_bounds__(256) k_residual64(int n, const int *__restrict__ rowptr, const int *__restrict__ cols,
-                                                    const double *__restrict__ K, const double *__restrict__ b,
-                                                    const double *__restrict__ x, double *__restrict__ r,
-                                                    double *__restrict__ part)
+__global__ void __launch_bounds__(256) k_residual64(int n, int nslices, const int *__restrict__ rowptr,
+                                                    const int *__restrict__ perm, const int64_t *__restrict__ slice_off,
+                                                    const int *__restrict__ col_sell, const double *__restrict__ K,
+                                                    const double *__restrict__ b, const double *__restrict__ x,
+                                                    double *__restrict__ r, double *__restrict__ part)
 {
     __shared__ double sh[32];
     const int W = (gridDim.x * blockDim.x) >> 5;
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     double loc = 0;
-    for (int row = gw; row < n; row += W)
+    for (int sl = gw; sl < nslices; sl += W)
     {
         double acc[D];
-        spmv_row<double, double, D>(row, rowptr, cols, K, x, x, 0.0, acc);
-        if (lane < D)
-        {
-            double qv = acc[0];
-            for (int c = 1; c < D; ++c)
-                if (lane == c)
-                    qv = acc[c];
-            const int64_t k = (int64_t)row * D + lane;
-            const double v = b[k] - qv;
-            r[k] = v;
-            loc += v * v;
-        }
+        const int i = spmv_slice<double, double, D>(sl, n, rowptr, perm, slice_off, col_sell, K, x, x, 0.0, acc);
+        if (i >= 0)
+            for (int c = 0; c < D; ++c)
+            {
+                const int64_t k = (int64_t)i * D + c;
+                const double v = b[k] - acc[c];
+                r[k] = v;
+                loc += v * v;
+            }
     }
     block_partial(loc, part, 0, sh);
 }
@@ -383,17 +391,20 @@ static cudaError_t run_cg(Problem &p, const TK *K, const TV *b, TV *x, TV *r, TV
         if (occ < 1)
             occ = 1;
     }
-    int grid = p.num_sms * std::min(occ, 2);
-    const int64_t rows_warps = ((int64_t)p.n + 0) / ((kCGThreads / 32)) + 1;
-    if (grid > rows_warps)
-        grid = (int)std::max<int64_t>(1, rows_warps);
+    int grid = p.num_sms * std::min(occ, kCGMinBlocks);
+    const int64_t slice_blocks = (int64_t)p.nslices / (kCGThreads / 32) + 1;
+    if (grid > slice_blocks)
+        grid = (int)std::max<int64_t>(1, slice_blocks);
     if (grid > kMaxGridBlocks)
         grid = kMaxGridBlocks;
     CGState s;
     s.n = p.n;
+    s.nslices = p.nslices;
     s.ndof = (int64_t)p.n * D;
     s.rowptr = p.cstart;
-    s.cols = p.conns;
+    s.perm = p.perm;
+    s.slice_off = p.slice_off;
+    s.col_sell = p.col_sell;
     s.rtol = rtol;
     s.atol = atol;
     s.abs_stop = abs_stop;
@@ -406,15 +417,27 @@ static cudaError_t run_cg(Problem &p, const TK *K, const TV *b, TV *x, TV *r, TV
     if ((e = cudaMemsetAsync(p.cg_info, 0, 4 * sizeof(int64_t), p.stream)) != cudaSuccess)
         return e;
     void *args[] = {&s, &K, &b, &x, &r, &pa, &pb, &q};
+    if ((e = cudaEventRecord(p.cg_ev[0], p.stream)) != cudaSuccess)
+        return e;
     e = cudaLaunchCooperativeKernel((const void *)k_cg<TK, TV, D>, dim3(grid), dim3(kCGThreads), args, 0, p.stream);
     if (e != cudaSuccess)
         return e;
+    if ((e = cudaEventRecord(p.cg_ev[1], p.stream)) != cudaSuccess)
+        return e;
+    p.ctr.kernel_launches++;
+    p.ctr.cg_launches++;
     if ((e = cudaMemcpyAsync(p.cg_info_host, p.cg_info, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, p.stream)) !=
         cudaSuccess)
         return e;
     if ((e = cudaStreamSynchronize(p.stream)) != cudaSuccess)
         return e;
     out.iters += p.cg_info_host[0];
+    p.ctr.cg_iters += p.cg_info_host[0];
+    {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, p.cg_ev[0], p.cg_ev[1]) == cudaSuccess)
+            p.ctr.cg_kernel_seconds += ms * 1e-3;
+    }
     if (p.cg_info_host[1] & 1)
         out.maxit_hits++;
     if (p.cg_info_host[1] & 2)
@@ -440,8 +463,10 @@ static cudaError_t solve_dim(Problem &p, CGResult &out)
         return e;
     double rr0 = 0, rr = 0;
     auto true_residual = [&](double &val) -> cudaError_t {
-        k_residual64<D><<<nb_res, 256, 0, p.stream>>>(p.n, p.cstart, p.conns, p.K, p.res, p.x, p.r, p.partials);
+        k_residual64<D><<<nb_res, 256, 0, p.stream>>>(p.n, p.nslices, p.cstart, p.perm, p.slice_off, p.col_sell, p.K,
+                                                      p.res, p.x, p.r, p.partials);
         k_sum_partials<<<1, 256, 0, p.stream>>>(nb_res, p.partials, reinterpret_cast<double *>(p.cg_info) + 3);
+        p.ctr.kernel_launches += 2;
         cudaError_t e2 = cudaMemcpyAsync(&val, reinterpret_cast<double *>(p.cg_info) + 3, sizeof(double),
                                          cudaMemcpyDeviceToHost, p.stream);
         if (e2 != cudaSuccess)
@@ -456,6 +481,7 @@ static cudaError_t solve_dim(Problem &p, CGResult &out)
     for (int ref = 0; ref < 30 && !(rr <= stop); ++ref)
     {
         k_convert<double, float><<<gconv, 256, 0, p.stream>>>(ndof, p.r, p.b32);
+        p.ctr.kernel_launches++;
         // the inner solve aims a little below the outer target, measured on its own residual
         CGResult inner;
         double rr_in = 0;
@@ -469,6 +495,7 @@ static cudaError_t solve_dim(Problem &p, CGResult &out)
         if (inner.timeout)
             break;
         k_add_f32<<<gconv, 256, 0, p.stream>>>(ndof, p.x32, p.x);
+        p.ctr.kernel_launches++;
         if ((e = true_residual(rr)) != cudaSuccess)
             return e;
         if (inner.iters == 0)
@@ -485,8 +512,9 @@ __global__ void k_to_f32(int64_t m, const double *__restrict__ a, float *__restr
 
 cudaError_t launch_k_to_f32(Problem &p)
 {
-    const int64_t m = p.nnzb * p.dim * p.dim;
+    const int64_t m = p.nsb * p.dim * p.dim * kSlice;
     k_to_f32<<<std::min(div_up(m, 256), 16 * p.num_sms), 256, 0, p.stream>>>(m, p.K, p.K32);
+    p.ctr.kernel_launches++;
     return cudaGetLastError();
 }
 

@@ -18,6 +18,7 @@ constexpr int kMaxBonds = 32;    // bonds per particle supported by the fixed-si
 constexpr int kMaxConns = 128;   // connections per particle (SC 61, FCC/BCC below 100)
 constexpr int kMaxCand = 512;    // connection candidates per particle before sort-unique
 constexpr double kEps = 1e-6;    // include/lpm.h:41
+constexpr int kSlice = 32;       // rows per slice of the sliced-ELL stiffness layout
 
 // std::max semantics ((a < b) ? b : a), which keeps the first argument when b is NaN
 __host__ __device__ inline double std_max(double a, double b) { return (a < b) ? b : a; }
@@ -48,8 +49,16 @@ struct Scalars
 
 // Device state of one problem.  Particles are indexed by id; bonds are owner-major CSR
 // (bstart), each particle's layer-0 list first then its layer-1 list, both ascending in the
-// partner id (assembly.h:218-229).  The stiffness is a full symmetric block-CSR (row i holds
-// the blocks of conns(i), ascending), d x d row-major doubles per block.
+// partner id (assembly.h:218-229).
+//
+// The stiffness is full symmetric and stored sliced-ELL: particle rows are ordered by
+// descending connection count (perm: position -> id, stable, so equal counts keep id order),
+// grouped in slices of kSlice rows; slice s holds width(s) = its longest row's count of block
+// columns starting at block slot slice_off[s].  Block slot b, entry e = r*d + c (row-major d x d)
+// of the row at lane l lives at K[(b*d*d + e)*kSlice + l]; its particle column at
+// col_sell[b*kSlice + l].  A row's k-th block is its k-th connection (ascending id).  A warp
+// streams 32 rows in lockstep: every matrix load is 256 contiguous bytes and the x gathers of
+// interior rows hit 32 consecutive particles.
 struct Problem
 {
     lpmgpu_desc desc{};
@@ -75,7 +84,12 @@ struct Problem
     // connections and matrices
     int *cstart = nullptr, *conns = nullptr, *nlq = nullptr;
     int64_t *kp_ref = nullptr;        // reference K_pointer (n+1)
-    double *K = nullptr;              // nnzb * d*d
+    int *perm = nullptr, *iperm = nullptr; // sliced-ELL row order: position -> id, id -> position
+    int64_t *slice_off = nullptr;     // nslices+1 block-slot offsets
+    int *col_sell = nullptr;          // nsb * kSlice particle columns
+    int nslices = 0;
+    int64_t nsb = 0;                  // block slots of the sliced-ELL layout (>= nnzb / kSlice)
+    double *K = nullptr;              // nsb * d*d * kSlice
     float *K32 = nullptr;             // mixed precision copy
     double *diag_raw = nullptr;       // n*d unmodified diagonal (for norm_diag)
     // vectors (n*d)
@@ -91,6 +105,8 @@ struct Problem
     // timing
     cudaEvent_t ev[8];
     double phase_s[4] = {0, 0, 0, 0};
+    lpmgpu_counters ctr{};
+    cudaEvent_t cg_ev[2] = {nullptr, nullptr};
     int64_t device_bytes = 0;
     std::vector<void *> allocs;
 };

@@ -236,6 +236,7 @@ cudaError_t launch_geometry_force(Problem &p)
     a.cs_sum = p.cs_sum;
     a.damage = p.damage;
     k_geometry_force<<<div_up(p.n, 128), 128, 0, p.stream>>>(a);
+    p.ctr.kernel_launches++;
     return cudaGetLastError();
 }
 
@@ -265,6 +266,7 @@ cudaError_t launch_update_rr_impl(Problem &p, bool accumulate_reaction)
     const int nblk = div_up(p.n, kForceThreads);
     k_internal_force<<<nblk, kForceThreads, 0, p.stream>>>(a);
     k_finalize_rr<<<1, 256, 0, p.stream>>>(nblk, p.partials, p.scal, accumulate_reaction ? 1 : 0);
+    p.ctr.kernel_launches += 2;
     return cudaGetLastError();
 }
 
@@ -325,6 +327,7 @@ cudaError_t launch_update_state_var(Problem &p)
     k_j2_update<<<div_up(p.n, 128), 128, 0, p.stream>>>(p.n, p.desc.E, p.desc.mu, p.desc.sigmay, p.desc.xi, p.desc.H,
                                                         p.desc.A, p.bstart, p.stress, p.dis, p.cs, p.sv, p.dLp,
                                                         p.ddot_local);
+    p.ctr.kernel_launches++;
     return cudaGetLastError();
 }
 
@@ -371,6 +374,7 @@ cudaError_t launch_static_damage(Problem &p)
     k_static_damage<<<div_up(p.n, 128), 128, 0, p.stream>>>(p.n, p.desc.ptype, p.desc.undamaged_type,
                                                             p.desc.critical_bstrain, p.type, p.bstart, p.bstrain,
                                                             p.bdamage, p.damage, p.damage_last, p.scal);
+    p.ctr.kernel_launches++;
     return cudaGetLastError();
 }
 
@@ -387,6 +391,7 @@ __global__ void k_add_disp(int n, int dim, const double *__restrict__ x, double 
 cudaError_t launch_add_disp(Problem &p)
 {
     k_add_disp<<<div_up(p.n, 256), 256, 0, p.stream>>>(p.n, p.dim, p.x, p.xyz);
+    p.ctr.kernel_launches++;
     return cudaGetLastError();
 }
 
@@ -442,14 +447,20 @@ cudaError_t launch_apply_bc(Problem &p, const lpmgpu_load_step &s)
     {
         const auto &b = s.force[f];
         if (b.count > 0)
+        {
             k_force_bc<<<div_up(b.count, 256), 256, 0, p.stream>>>(b.count, dids + o, b.fx, b.fy, b.fz, p.pex);
+            p.ctr.kernel_launches++;
+        }
         o += b.count;
     }
     for (int d = 0; d < s.ndisp && e == cudaSuccess; ++d)
     {
         const auto &b = s.disp[d];
         if (b.count > 0)
+        {
             k_disp_bc<<<div_up(b.count, 256), 256, 0, p.stream>>>(b.count, dids + o, b.flag, b.step, p.xyz, p.cons);
+            p.ctr.kernel_launches++;
+        }
         o += b.count;
     }
     if (e == cudaSuccess)

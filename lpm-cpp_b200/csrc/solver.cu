@@ -69,6 +69,7 @@ static int32_t force_state(Problem &p, bool with_rr)
     float ms = 0;
     cudaEventElapsedTime(&ms, p.ev[0], p.ev[1]);
     p.phase_s[0] += ms * 1e-3;
+    p.ctr.force_seconds += ms * 1e-3;
     return LPMGPU_OK;
 }
 
@@ -83,6 +84,7 @@ static int32_t assemble(Problem &p, bool apply_bc)
     float ms = 0;
     cudaEventElapsedTime(&ms, p.ev[2], p.ev[3]);
     p.phase_s[1] += ms * 1e-3;
+    p.ctr.assembly_seconds += ms * 1e-3;
     return LPMGPU_OK;
 }
 
@@ -428,6 +430,9 @@ static void free_problem(Problem &p)
     for (auto &e : p.ev)
         if (e)
             cudaEventDestroy(e);
+    for (auto &e : p.cg_ev)
+        if (e)
+            cudaEventDestroy(e);
     if (p.stream)
         cudaStreamDestroy(p.stream);
 }
@@ -469,6 +474,8 @@ int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
     CKF(cudaDeviceGetAttribute(&p.num_sms, cudaDevAttrMultiProcessorCount, p.device));
     for (auto &e : p.ev)
         CKF(cudaEventCreate(&e));
+    for (auto &e : p.cg_ev)
+        CKF(cudaEventCreate(&e));
     p.cell = make_cell(d->lattice, d->radius);
     p.n = d->n;
     p.dim = p.cell.dim;
@@ -509,7 +516,7 @@ int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
         return fail(topo_err);
     }
     const size_t ndof = n * p.dim;
-    CKF(dalloc(p, &p.K, (size_t)p.nnzb * p.dim * p.dim));
+    CKF(dalloc(p, &p.K, (size_t)p.nsb * p.dim * p.dim * kSlice));
     CKF(dalloc(p, &p.diag_raw, ndof));
     CKF(dalloc(p, &p.res, ndof));
     CKF(dalloc(p, &p.x, ndof));
@@ -519,7 +526,7 @@ int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
     CKF(dalloc(p, &p.q, ndof));
     if (d->precision == LPMGPU_MIXED)
     {
-        CKF(dalloc(p, &p.K32, (size_t)p.nnzb * p.dim * p.dim));
+        CKF(dalloc(p, &p.K32, (size_t)p.nsb * p.dim * p.dim * kSlice));
         CKF(dalloc(p, &p.x32, ndof));
         CKF(dalloc(p, &p.r32, ndof));
         CKF(dalloc(p, &p.pa32, ndof));
@@ -816,6 +823,22 @@ int32_t lpmgpu_set_xyz(lpmgpu_solver *h, const double *xyz)
     CK(cudaSetDevice(p.device));
     CK(cudaMemcpyAsync(p.xyz, xyz, sizeof(double) * 3 * p.n, cudaMemcpyHostToDevice, p.stream));
     CK(cudaStreamSynchronize(p.stream));
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_get_counters(const lpmgpu_solver *h, lpmgpu_counters *out)
+{
+    if (!h || !out)
+        return LPMGPU_ERR_INVALID_ARG;
+    *out = h->p.ctr;
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_get_stream(const lpmgpu_solver *h, void **stream)
+{
+    if (!h || !stream)
+        return LPMGPU_ERR_INVALID_ARG;
+    *stream = (void *)h->p.stream;
     return LPMGPU_OK;
 }
 

@@ -1,6 +1,6 @@
 // Device construction of the particle topology: bonds, opposite-bond index, connection
-// lists and both stiffness patterns (full block-CSR for the solver, 1-based upper CSR
-// pointers of the reference).  Restates, on the device:
+// lists, the sliced-ELL row order and column slots of the solver's stiffness, and the 1-based
+// upper-CSR pointers of the reference.  Restates, on the device:
 //   Bond(p1,p2,layer,dis)          include/bond.h:59-72
 //   Assembly::createBonds          include/assembly.h:213-234  (O(N^2) in the reference;
 //                                  here a radix-sorted cell grid, same lists, same order)
@@ -406,6 +406,52 @@ __global__ void k_kp_counts(int n, int dim, const int *__restrict__ nlq, int64_t
         v[i] = 0;
 }
 
+// ---- sliced-ELL row order and column slots
+__global__ void k_sell_keys(int n, const int *__restrict__ cstart, int *__restrict__ key, int *__restrict__ ids)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    key[i] = kMaxConns - (cstart[i + 1] - cstart[i]);
+    ids[i] = i;
+}
+
+__global__ void k_sell_width(int n, int nslices, const int *__restrict__ perm, const int *__restrict__ cstart,
+                             const int *__restrict__ iperm_unused, int64_t *__restrict__ width)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nslices)
+    {
+        const int i = perm[s * kSlice]; // rows are sorted by descending count
+        width[s] = cstart[i + 1] - cstart[i];
+    }
+    if (s == nslices)
+        width[s] = 0;
+}
+
+__global__ void k_sell_fill(int n, int nslices, const int *__restrict__ perm, const int *__restrict__ cstart,
+                            const int *__restrict__ conns, const int64_t *__restrict__ off, int *__restrict__ iperm,
+                            int *__restrict__ col_sell)
+{
+    const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= nslices * kSlice)
+        return;
+    const int s = pos / kSlice, lane = pos % kSlice;
+    const int64_t o = off[s];
+    const int w = (int)(off[s + 1] - o);
+    if (pos >= n)
+    {
+        for (int k = 0; k < w; ++k)
+            col_sell[(o + k) * kSlice + lane] = 0;
+        return;
+    }
+    const int i = perm[pos];
+    iperm[i] = pos;
+    const int c0 = cstart[i], m = cstart[i + 1] - c0;
+    for (int k = 0; k < w; ++k)
+        col_sell[(o + k) * kSlice + lane] = (k < m) ? conns[c0 + k] : i;
+}
+
 template <typename T>
 static cudaError_t exclusive_scan(Problem &p, const T *in, T *out, int count)
 {
@@ -603,6 +649,43 @@ cudaError_t build_topology(Problem &p, const double *xyz_host, int *err_code)
     LPM_TRY(reduce_max(p, p.nb, n, &p.max_bonds));
     cudaFreeAsync(pad_c, p.stream);
     cudaFreeAsync(ncx, p.stream);
+
+    // sliced-ELL layout: rows by descending connection count (stable radix sort), slices of 32
+    {
+        int *key = nullptr, *ids = nullptr, *skey = nullptr;
+        LPM_TRY(cudaMallocAsync(&key, sizeof(int) * n, p.stream));
+        LPM_TRY(cudaMallocAsync(&ids, sizeof(int) * n, p.stream));
+        LPM_TRY(cudaMallocAsync(&skey, sizeof(int) * n, p.stream));
+        LPM_TRY(dalloc(p, &p.perm, n));
+        LPM_TRY(dalloc(p, &p.iperm, n));
+        k_sell_keys<<<div_up(n, T), T, 0, p.stream>>>(n, p.cstart, key, ids);
+        size_t bytes = 0;
+        int bits = 1;
+        while ((1 << bits) <= kMaxConns)
+            bits++;
+        LPM_TRY(cub::DeviceRadixSort::SortPairs(nullptr, bytes, key, skey, ids, p.perm, n, 0, bits, p.stream));
+        void *tmp = nullptr;
+        LPM_TRY(cudaMallocAsync(&tmp, bytes + 16, p.stream));
+        LPM_TRY(cub::DeviceRadixSort::SortPairs(tmp, bytes, key, skey, ids, p.perm, n, 0, bits, p.stream));
+        cudaFreeAsync(tmp, p.stream);
+        p.nslices = div_up(n, kSlice);
+        int64_t *width = nullptr;
+        LPM_TRY(cudaMallocAsync(&width, sizeof(int64_t) * (p.nslices + 1), p.stream));
+        LPM_TRY(dalloc(p, &p.slice_off, (size_t)p.nslices + 1));
+        k_sell_width<<<div_up(p.nslices + 1, T), T, 0, p.stream>>>(n, p.nslices, p.perm, p.cstart, nullptr, width);
+        LPM_TRY(exclusive_scan(p, width, p.slice_off, p.nslices + 1));
+        LPM_TRY(cudaMemcpyAsync(&p.nsb, p.slice_off + p.nslices, sizeof(int64_t), cudaMemcpyDeviceToHost, p.stream));
+        LPM_TRY(cudaStreamSynchronize(p.stream));
+        LPM_TRY(dalloc(p, &p.col_sell, (size_t)p.nsb * kSlice));
+        k_sell_fill<<<div_up((int64_t)p.nslices * kSlice, T), T, 0, p.stream>>>(n, p.nslices, p.perm, p.cstart,
+                                                                                p.conns, p.slice_off, p.iperm,
+                                                                                p.col_sell);
+        LPM_TRY(cudaGetLastError());
+        cudaFreeAsync(width, p.stream);
+        cudaFreeAsync(key, p.stream);
+        cudaFreeAsync(ids, p.stream);
+        cudaFreeAsync(skey, p.stream);
+    }
 
     // reference K_pointer
     int64_t *kv = nullptr;

@@ -111,6 +111,14 @@ class Stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Counters(C.Structure):
+    _fields_ = [("kernel_launches", C.c_int64), ("cg_launches", C.c_int64), ("cg_iters", C.c_int64),
+                ("cg_kernel_seconds", C.c_double), ("assembly_seconds", C.c_double), ("force_seconds", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class Sizes(C.Structure):
     _fields_ = [("n", C.c_int32), ("dim", C.c_int32), ("nbonds", C.c_int64), ("nnzb", C.c_int64),
                 ("nnz_upper", C.c_int64), ("max_bonds", C.c_int32), ("max_conns", C.c_int32),
@@ -127,6 +135,7 @@ EXPORTS = [
     "lpmgpu_export_ref_csr", "lpmgpu_solve_linear", "lpmgpu_apply_load_step",
     "lpmgpu_solve_problem_step", "lpmgpu_solve_load_step", "lpmgpu_store_state", "lpmgpu_reset_state",
     "lpmgpu_read_state", "lpmgpu_read_residual", "lpmgpu_set_xyz", "lpmgpu_get_phase_times",
+    "lpmgpu_get_counters", "lpmgpu_get_stream",
 ]
 
 
@@ -163,6 +172,8 @@ def lib():
         "lpmgpu_read_residual": (C.c_int32, [vp, dp]),
         "lpmgpu_set_xyz": (C.c_int32, [vp, dp]),
         "lpmgpu_get_phase_times": (C.c_int32, [vp, dp]),
+        "lpmgpu_get_counters": (C.c_int32, [vp, C.POINTER(Counters)]),
+        "lpmgpu_get_stream": (C.c_int32, [vp, C.POINTER(vp)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -475,6 +486,20 @@ class GpuProblem:
         r = np.zeros(self.dim * self.n)
         _check(lib().lpmgpu_read_residual(self._h, _dp(r)), "lpmgpu_read_residual")
         return r
+
+    def counters(self):
+        c = Counters()
+        _check(lib().lpmgpu_get_counters(self._h, C.byref(c)), "lpmgpu_get_counters")
+        return c.as_dict()
+
+    def stream_ptr(self) -> int:
+        s = C.c_void_p()
+        _check(lib().lpmgpu_get_stream(self._h, C.byref(s)), "lpmgpu_get_stream")
+        return s.value or 0
+
+    def read_xyz_into(self, out: np.ndarray):
+        """Device-to-host copy of the positions into a caller buffer (n x 3, float64)."""
+        _check(lib().lpmgpu_read_state(self._h, _dp(out), None, None, None, None, None, None), "lpmgpu_read_state")
 
     def phase_times(self):
         t = np.zeros(4)

@@ -301,3 +301,48 @@ def read_ref_steps(outdir: str):
 
 def read_bin(outdir: str, name: str, dtype) -> np.ndarray:
     return np.fromfile(os.path.join(outdir, name), dtype=dtype)
+
+
+def write_ref_spec(case, outdir: str, steps=None, max_iter=None, tol_iter=None, cg_tol=None, cg_maxit_cap=0,
+                   dump_k=(), loop="step", use_generator=True) -> str:
+    """Spec text for oracle/_ref/lpm_ref describing a product-side ``Case`` (duck-typed):
+    groups and particle types are passed as raw int32 id files so both sides see the same sets.
+    With use_generator the reference generates the lattice itself (its ids must then equal
+    case.xyz, which the tests check); otherwise case.xyz is passed as a coordinate file."""
+    os.makedirs(outdir, exist_ok=True)
+    lat = {0: "sq2d", 1: "hex2d", 2: "sc3d", 3: "fcc3d", 4: "bcc3d"}[int(case.lattice)]
+    m = case.material
+    lines = [f"lattice {lat}", f"radius {case.radius!r}", "box " + " ".join(repr(float(v)) for v in case.box),
+             f"euler {case.euler[0]} " + " ".join(repr(float(a)) for a in case.euler[1]),
+             f"ptype {'j2' if int(case.ptype) == 2 else 'elastic'}", f"plane_stress {int(m.plane_stress)}",
+             f"E {m.E!r}", f"mu {m.mu!r}", f"critical_bstrain {m.critical_bstrain!r}",
+             f"j2 {m.sigmay!r} {m.xi!r} {m.H!r} {m.A!r}", f"nonlocal_L {m.nonlocal_L!r}",
+             f"undamaged_type {case.undamaged_type}",
+             f"max_iter {case.max_iter if max_iter is None else max_iter}",
+             f"tol_iter {(case.tol_iter if tol_iter is None else tol_iter)!r}", f"loop {loop}"]
+    if cg_maxit_cap:
+        lines.append(f"cg_maxit_cap {int(cg_maxit_cap)}")
+    if cg_tol is not None:
+        lines.append(f"cg_tol {cg_tol[0]!r} {cg_tol[1]!r}")
+    if not use_generator or lat == "bcc3d":
+        p = os.path.join(outdir, "xyz_in.f64")
+        np.ascontiguousarray(case.xyz, dtype=np.float64).tofile(p)
+        lines.append(f"xyz_file {p}")
+    p = os.path.join(outdir, "types_in.i32")
+    np.ascontiguousarray(case.types, dtype=np.int32).tofile(p)
+    lines.append(f"typefile {p}")
+    for name, ids in case.groups.items():
+        p = os.path.join(outdir, f"group_{name}.i32")
+        np.ascontiguousarray(ids, dtype=np.int32).tofile(p)
+        lines.append(f"groupfile {name} {p}")
+    nsteps = len(case.steps) if steps is None else steps
+    lines.append(f"steps {nsteps}")
+    for s in range(nsteps):
+        disp, force = case.steps[s % len(case.steps)]
+        for g, flag, v in disp:
+            lines.append(f"dispbc {g} {flag} {float(v)!r} {s} {s + 1}")
+        for g, fx, fy, fz in force:
+            lines.append(f"forcebc {g} {float(fx)!r} {float(fy)!r} {float(fz)!r} {s} {s + 1}")
+    for k in dump_k:
+        lines.append(f"dumpK {int(k)}")
+    return "\n".join(lines) + "\n"

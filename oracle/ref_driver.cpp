@@ -27,7 +27,7 @@
  *   dispbc NAME FLAG STEP [FROM TO]              (FLAG x|y|z, steps FROM..TO-1)
  *   forcebc NAME FX FY FZ [FROM TO]
  *   dumpK STEP   (write the reference CSR after that load step; may repeat)
- *   loop ref|step   out DIR   xyz_file PATH (optional: particle coordinates instead of a generator)
+ *   loop ref|step|once   out DIR   xyz_file PATH (optional: particle coordinates instead of a generator)
  *   groupfile NAME PATH   (group from raw int32 particle ids)   typefile PATH (raw int32 types)
  *   cg_tol RTOL ATOL      (overrides the squared-norm tolerances the reference sets at
  *                          solver.h:312-313; applied inside the MKL stand-in, test use only)
@@ -419,7 +419,13 @@ int main(int argc, char **argv)
         lpm_shim_stats st0 = lpm_shim_stats_g;
         double t0 = wall();
         int cuts = 0;
-        if (sp.loop == "ref")
+        if (sp.loop == "once")
+        {
+            /* one SolverStatic::solveProblemStep call, no retry: a bounded sample of the step */
+            double dt = 1;
+            cuts = solv.solveProblemStep(load[s], dt) ? 0 : -1;
+        }
+        else if (sp.loop == "ref")
         {
             std::vector<LoadStep<NL>> one{load[s]};
             solv.solveProblem(one, start_index);

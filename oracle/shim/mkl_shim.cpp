@@ -7,8 +7,10 @@
  *    uses); each output is alpha * (in-order dot product) + beta * old value (beta term
  *    skipped when beta == 0).
  *  - mkl_sparse_d_create_csr + mkl_sparse_d_mv: the reference passes a 1-based upper-triangular
- *    CSR with a SYMMETRIC/UPPER descriptor (include/solver.h:287-296).  The handle expands it
- *    once into full symmetric CSR so the product is an OpenMP row-parallel gather.
+ *    CSR with a SYMMETRIC/UPPER descriptor (include/solver.h:287-296).  The handle references the
+ *    caller's arrays; the product reads the upper triangle once (OpenMP, per-thread scatter
+ *    buffers for the transposed half).  The reference never destroys its handles (solver.h:296);
+ *    with no copy inside, that leaks only the small handle, as with MKL.
  *  - dcg_*: the RCI state machine of unpreconditioned Hestenes-Stiefel CG.  With ipar[8] != 0
  *    the residual test is ||r||^2 <= dpar[0] * ||r0||^2 + dpar[1] (squared norms, as the
  *    public documentation of dpar[2..4] states); ipar[4] is the iteration cap, ipar[3] the
@@ -91,90 +93,86 @@ void cblas_dgemv(const CBLAS_LAYOUT layout, const CBLAS_TRANSPOSE trans, const M
 struct lpm_shim_sparse_matrix
 {
     MKL_INT n;
-    std::vector<long long> rp;  /* full symmetric CSR, 0-based */
-    std::vector<long long> ci;
-    std::vector<double> v;
+    long long base;
+    const MKL_INT *rs, *re, *ci; /* caller's arrays, as MKL's handle references them */
+    const double *v;
+    std::vector<double> scratch; /* per-thread partial products of the transposed half */
 };
 
-/* The reference creates a handle per linear solve and never destroys it (include/solver.h:296).
- * MKL's handle only references the caller's arrays, but this stand-in holds an expanded copy,
- * so the previous handle is released when a new one is created (one live handle at a time,
- * which is how the reference uses the API). */
-static lpm_shim_sparse_matrix *g_last_handle = nullptr;
-
+/* The handle references the caller's upper-triangular CSR without copying (as MKL's does). */
 sparse_status_t mkl_sparse_d_create_csr(sparse_matrix_t *A, const sparse_index_base_t indexing, const MKL_INT rows,
                                         const MKL_INT cols, MKL_INT *rows_start, MKL_INT *rows_end,
                                         MKL_INT *col_indx, double *values)
 {
     double t0 = now_s();
-    if (g_last_handle)
-    {
-        delete g_last_handle;
-        g_last_handle = nullptr;
-    }
     if (rows != cols)
         return SPARSE_STATUS_NOT_SUPPORTED;
-    const long long base = (indexing == SPARSE_INDEX_BASE_ONE) ? 1 : 0;
     auto *M = new lpm_shim_sparse_matrix;
     M->n = rows;
-    const long long n = rows;
-    std::vector<long long> cnt(n + 1, 0);
-    for (long long i = 0; i < n; ++i)
-        for (long long p = rows_start[i] - base; p < rows_end[i] - base; ++p)
-        {
-            long long j = col_indx[p] - base;
-            cnt[i]++;
-            if (j != i)
-                cnt[j]++;
-        }
-    M->rp.assign(n + 1, 0);
-    for (long long i = 0; i < n; ++i)
-        M->rp[i + 1] = M->rp[i] + cnt[i];
-    M->ci.resize(M->rp[n]);
-    M->v.resize(M->rp[n]);
-    std::vector<long long> fill(M->rp.begin(), M->rp.end() - 1);
-    /* lower-triangle entries of row j (from upper rows i < j) land before row j's own upper entries */
-    for (long long i = 0; i < n; ++i)
-        for (long long p = rows_start[i] - base; p < rows_end[i] - base; ++p)
-        {
-            long long j = col_indx[p] - base;
-            if (j != i)
-            {
-                M->ci[fill[j]] = i;
-                M->v[fill[j]++] = values[p];
-            }
-        }
-    for (long long i = 0; i < n; ++i)
-        for (long long p = rows_start[i] - base; p < rows_end[i] - base; ++p)
-        {
-            M->ci[fill[i]] = col_indx[p] - base;
-            M->v[fill[i]++] = values[p];
-        }
+    M->base = (indexing == SPARSE_INDEX_BASE_ONE) ? 1 : 0;
+    M->rs = rows_start;
+    M->re = rows_end;
+    M->ci = col_indx;
+    M->v = values;
     *A = M;
-    g_last_handle = M;
     lpm_shim_stats_g.create_seconds += now_s() - t0;
     return SPARSE_STATUS_SUCCESS;
 }
 
+/* y = alpha*A*x + beta*y for A = U + U^T - diag(U) given the upper triangle U (the SYMMETRIC /
+ * UPPER descriptor of solver.h:287-289).  Row-parallel gather for U x; the U^T x part is a
+ * scatter, accumulated in per-thread buffers and summed afterwards. */
 sparse_status_t mkl_sparse_d_mv(const sparse_operation_t operation, const double alpha, const sparse_matrix_t A,
                                 const struct matrix_descr descr, const double *x, const double beta, double *y)
 {
     (void)operation;
-    (void)descr;
     if (!A)
         return SPARSE_STATUS_NOT_INITIALIZED;
     double t0 = now_s();
-    const long long n = A->n;
-    const long long *rp = A->rp.data();
-    const long long *ci = A->ci.data();
-    const double *v = A->v.data();
-#pragma omp parallel for schedule(static)
-    for (long long i = 0; i < n; ++i)
+    const long long n = A->n, b = A->base;
+    const bool sym = descr.type == SPARSE_MATRIX_TYPE_SYMMETRIC;
+    int nt = 1;
+#ifdef _OPENMP
+    nt = omp_get_max_threads();
+#endif
+    if (sym)
+        A->scratch.assign((size_t)nt * n, 0.0);
+    double *scr = sym ? A->scratch.data() : nullptr;
+#pragma omp parallel num_threads(nt)
     {
-        double s = 0.0;
-        for (long long p = rp[i]; p < rp[i + 1]; ++p)
-            s += v[p] * x[ci[p]];
-        y[i] = (beta == 0.0) ? alpha * s : alpha * s + beta * y[i];
+        int t = 0;
+#ifdef _OPENMP
+        t = omp_get_thread_num();
+#endif
+        double *yt = sym ? scr + (size_t)t * n : nullptr;
+#pragma omp for schedule(static)
+        for (long long i = 0; i < n; ++i)
+        {
+            double s = 0.0;
+            const double xi = x[i];
+            for (long long p = A->rs[i] - b; p < A->re[i] - b; ++p)
+            {
+                const long long j = A->ci[p] - b;
+                s += A->v[p] * x[j];
+                if (sym && j != i)
+                    yt[j] += A->v[p] * xi;
+            }
+            if (sym)
+                yt[i] += s;
+            else
+                y[i] = (beta == 0.0) ? alpha * s : alpha * s + beta * y[i];
+        }
+        if (sym)
+        {
+#pragma omp for schedule(static)
+            for (long long i = 0; i < n; ++i)
+            {
+                double s = 0.0;
+                for (int q = 0; q < nt; ++q)
+                    s += scr[(size_t)q * n + i];
+                y[i] = (beta == 0.0) ? alpha * s : alpha * s + beta * y[i];
+            }
+        }
     }
     lpm_shim_stats_g.spmv_calls++;
     lpm_shim_stats_g.spmv_seconds += now_s() - t0;
@@ -183,8 +181,6 @@ sparse_status_t mkl_sparse_d_mv(const sparse_operation_t operation, const double
 
 sparse_status_t mkl_sparse_destroy(sparse_matrix_t A)
 {
-    if (A == g_last_handle)
-        g_last_handle = nullptr;
     delete A;
     return SPARSE_STATUS_SUCCESS;
 }

@@ -1,0 +1,72 @@
+"""The C-ABI library (no compute without a GPU): it loads, exports every symbol that
+include/lpmgpu.h declares, rejects bad input with status codes, and refuses to run without a
+CUDA device instead of falling back to the CPU."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from _util import CFG, LPM, ROOT
+from conftest import cuda_available
+
+HEADER = os.path.join(ROOT, "include", "lpmgpu.h")
+
+
+def declared():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[\w]+\s*\*?\s*(lpmgpu_\w+)\s*\(", txt, flags=re.M)))
+
+
+def test_header_declares_entry_points():
+    names = declared()
+    assert "lpmgpu_create" in names and "lpmgpu_solve_load_step" in names
+    assert len(names) >= 20
+
+
+def test_library_exports_every_declared_symbol():
+    lib = C.CDLL(LPM.LIB_PATH)
+    missing = [n for n in declared() if not hasattr(lib, n)]
+    assert not missing, missing
+    assert sorted(LPM.EXPORTS) == declared(), "lpm.py binds exactly the declared symbols"
+
+
+def test_version_and_status_strings():
+    L = LPM.lib()
+    assert b"sm_100a" in L.lpmgpu_version()
+    assert L.lpmgpu_status_string(0) == b"ok"
+    assert L.lpmgpu_status_string(4).startswith(b"Newton")
+
+
+def test_invalid_arguments_are_rejected():
+    L = LPM.lib()
+    h = C.c_void_p()
+    assert L.lpmgpu_create(None, C.byref(h)) == 1
+    d = LPM.Desc()
+    d.n = 0
+    assert L.lpmgpu_create(C.byref(d), C.byref(h)) == 1
+    cnt = C.c_int64()
+    box = np.zeros(6)
+    ang = np.zeros(3)
+    assert L.lpmgpu_generate_lattice(9, 0.1, box.ctypes.data_as(C.POINTER(C.c_double)), 0,
+                                     ang.ctypes.data_as(C.POINTER(C.c_double)), None, 0, C.byref(cnt)) == 1
+    assert L.lpmgpu_destroy(None) == 1
+    assert L.lpmgpu_solve_load_step(None, None, None) == 1
+
+
+@pytest.mark.skipif(cuda_available(), reason="checks the no-device path")
+def test_no_device_fails_loudly():
+    case = CFG.hex_plate(size=1.0, radius=0.1, steps=1)
+    with pytest.raises(LPM.LpmGpuError) as e:
+        LPM.GpuProblem(case.assembly())
+    assert e.value.status in (2, 11)
+
+
+def test_generators_are_host_side():
+    """Lattice generation needs no device (utilities.h restated on the host)."""
+    cell = LPM.UnitCell(LPM.LatticeType.SimpleCubic3D, 0.2)
+    x = LPM.createCuboidSC3D([0, 2, 0, 2, 0, 2], cell)
+    from oracle import oracle as O
+    assert len(x) > 100 and np.array_equal(x, O.generate("sc3d", 0.2, [0, 2, 0, 2, 0, 2]))
