@@ -31,8 +31,10 @@
 namespace lpm
 {
 
-constexpr int kCGThreads = 256;
-constexpr int kCGMinBlocks = 3;
+// one 32-warp block per SM: with <= 64 registers every slice of the 382,500-DOF cube gets its
+// own warp (3,985 slices, 4,736 resident warps) and each grid barrier takes 148 arrivals
+constexpr int kCGThreads = 1024;
+constexpr int kCGMinBlocks = 1;
 constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull; // 4 s
 
 struct CGState
@@ -48,6 +50,7 @@ struct CGState
     int64_t maxit;
     unsigned *bar;      // [0] arrivals, [1] generation
     double *part;       // [grid][2]
+    double *tot;        // [2] reduced totals published by the last block at each barrier
     int64_t *info;      // [0] iterations, [1] status bits (1 maxit, 2 timeout, 4 breakdown), [2..3] rr0/rr bits
 };
 
@@ -65,22 +68,24 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
     return v;
 }
 
-// returns false when the wait timed out (the flag is then also set in info[1])
-__device__ bool grid_barrier(unsigned *bar, int64_t *info, volatile int *s_fail)
+__device__ __forceinline__ double wsum(double v);
+
+// Grid barrier fused with the reduction of the per-block partials part[2*b + slot]: the last
+// block to arrive sums them (fixed order: thread t takes b = t, t + blockDim, ..., then a fixed
+// tree), publishes the total in tot[slot] and releases the others.  Every block returns the
+// same total.  Returns false when the wait timed out.
+__device__ bool grid_reduce(unsigned *bar, int64_t *info, volatile int *s_fail, const double *part, int slot,
+                            double *tot, double *sh, double *out)
 {
+    __shared__ int s_last;
     __syncthreads();
     if (threadIdx.x == 0)
     {
         const unsigned gen = ld_acquire(bar + 1);
         __threadfence();
         const unsigned arrived = atomicAdd(bar, 1u);
-        if (arrived == gridDim.x - 1)
-        {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        }
-        else
+        s_last = (arrived == gridDim.x - 1);
+        if (!s_last)
         {
             const unsigned long long t0 = gtimer();
             unsigned ns = 32;
@@ -93,17 +98,49 @@ __device__ bool grid_barrier(unsigned *bar, int64_t *info, volatile int *s_fail)
                     break;
                 }
                 __nanosleep(ns);
-                if (ns < 256)
+                if (ns < 128)
                     ns <<= 1;
             }
+            __threadfence();
         }
-        __threadfence();
-        // a block that sees another block's timeout stops too
-        if (*reinterpret_cast<volatile long long *>(info + 1) & 2)
-            *s_fail = 1;
+        else
+            __threadfence();
     }
     __syncthreads();
-    return *s_fail == 0;
+    if (s_last)
+    {
+        double v = 0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+            v += __ldcg(part + 2 * b + slot);
+        v = wsum(v);
+        const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+        if (l == 0)
+            sh[w] = v;
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            double t = 0;
+            for (int q = 0; q < (int)(blockDim.x >> 5); ++q)
+                t += sh[q];
+            __stcg(tot + slot, t);
+            __threadfence();
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+    {
+        if (*reinterpret_cast<volatile long long *>(info + 1) & 2)
+            *s_fail = 1;
+        sh[0] = __ldcg(tot + slot);
+    }
+    __syncthreads();
+    *out = sh[0];
+    const bool ok = *s_fail == 0;
+    __syncthreads();
+    return ok;
 }
 
 __device__ __forceinline__ double wsum(double v)
@@ -137,28 +174,59 @@ __device__ __forceinline__ void block_partial(double v, double *part, int slot, 
     __syncthreads();
 }
 
-// the same fixed-order sum of all blocks' partials, computed by every block
-__device__ __forceinline__ double grid_total(const double *part, int slot, double *sh)
+// L2 cache policies: the matrix and its columns are streamed once per iteration (evict-first,
+// no L1 allocation, read-only path); the Krylov vectors are gathered many times per iteration
+// and must stay in L2 (evict-last on their loads and stores).
+__device__ __forceinline__ uint64_t l2_evict_first()
 {
-    if (threadIdx.x < 32)
-    {
-        double v = 0;
-        for (int b = threadIdx.x; b < (int)gridDim.x; b += 32)
-            v += __ldcg(part + 2 * b + slot);
-        v = wsum(v);
-        if (threadIdx.x == 0)
-            sh[0] = v;
-    }
-    __syncthreads();
-    const double r = sh[0];
-    __syncthreads();
-    return r;
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
 }
-
-template <typename T>
-__device__ __forceinline__ T ldstream(const T *p)
+__device__ __forceinline__ uint64_t l2_evict_last()
 {
-    return __ldcs(p);
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ double ld_stream(const double *a, uint64_t pol)
+{
+    double v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float ld_stream(const float *a, uint64_t pol)
+{
+    float v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int ld_stream(const int *a, uint64_t pol)
+{
+    int v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+    return v;
+}
+// vectors change between phases: volatile keeps these loads where the code puts them
+__device__ __forceinline__ double ld_keep(const double *a, uint64_t pol)
+{
+    double v;
+    asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol) : "memory");
+    return v;
+}
+__device__ __forceinline__ float ld_keep(const float *a, uint64_t pol)
+{
+    float v;
+    asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_keep(double *a, double v, uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_keep(float *a, float v, uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(pol) : "memory");
 }
 
 // q_i = sum_j K_ij (r_j + beta p_old_j) for the row at this lane of slice sl; returns the
@@ -167,7 +235,8 @@ template <typename TK, typename TV, int D>
 __device__ __forceinline__ int spmv_slice(int sl, int n, const int *__restrict__ rowptr, const int *__restrict__ perm,
                                           const int64_t *__restrict__ slice_off, const int *__restrict__ col_sell,
                                           const TK *__restrict__ K, const TV *__restrict__ r,
-                                          const TV *__restrict__ pold, TV beta, TV acc[D])
+                                          const TV *__restrict__ pold, TV beta, TV acc[D], uint64_t pf,
+                                          uint64_t pl)
 {
     constexpr int E = D * D;
     const int lane = threadIdx.x & 31;
@@ -182,20 +251,25 @@ __device__ __forceinline__ int spmv_slice(int sl, int n, const int *__restrict__
 #pragma unroll
     for (int k = 0; k < D; ++k)
         acc[k] = TV(0);
+    // the column of step k+1 is fetched during step k, so the x gathers never wait on it
+    int jn = (myn > 0) ? ld_stream(cp, pf) : 0;
+#pragma unroll 2
     for (int k = 0; k < w; ++k)
     {
+        const int j = jn;
+        if (k + 1 < myn)
+            jn = ld_stream(cp + (int64_t)(k + 1) * kSlice, pf);
         if (k < myn)
         {
-            const int j = ldstream(cp + (int64_t)k * kSlice);
             TV xv[D];
 #pragma unroll
             for (int c = 0; c < D; ++c)
-                xv[c] = r[(int64_t)j * D + c] + beta * pold[(int64_t)j * D + c];
+                xv[c] = ld_keep(r + (int64_t)j * D + c, pl) + beta * ld_keep(pold + (int64_t)j * D + c, pl);
             const TK *kb = kp + (int64_t)k * E * kSlice;
             TK kv[E];
 #pragma unroll
             for (int e = 0; e < E; ++e)
-                kv[e] = ldstream(kb + e * kSlice);
+                kv[e] = ld_stream(kb + e * kSlice, pf);
 #pragma unroll
             for (int rr = 0; rr < D; ++rr)
 #pragma unroll
@@ -218,22 +292,25 @@ __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg(CGState s, cons
     __syncthreads();
     const int64_t T = (int64_t)gridDim.x * blockDim.x;
     const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int W = (int)(T >> 5);
-    const int gw = (int)(gt >> 5);
+    // each block owns a contiguous, equal share of the slices (balanced, neighbours share L1)
+    const int s0 = (int)((int64_t)blockIdx.x * s.nslices / gridDim.x);
+    const int s1 = (int)((int64_t)(blockIdx.x + 1) * s.nslices / gridDim.x);
+    const int warp = threadIdx.x >> 5;
+    const uint64_t pf = l2_evict_first(), pl = l2_evict_last();
 
     double loc = 0;
     for (int64_t k = gt; k < s.ndof; k += T)
     {
         const TV v = b[k];
-        r[k] = v;
-        x[k] = TV(0);
-        pa[k] = TV(0);
+        st_keep(r + k, v, pl);
+        st_keep(x + k, TV(0), pl);
+        st_keep(pa + k, TV(0), pl);
         loc += (double)v * (double)v;
     }
     block_partial(loc, s.part, 0, sh);
-    if (!grid_barrier(s.bar, s.info, &s_fail))
+    double rr;
+    if (!grid_reduce(s.bar, s.info, &s_fail, s.part, 0, s.tot, sh, &rr))
         return;
-    double rr = grid_total(s.part, 0, sh);
     const double stop = (s.abs_stop >= 0) ? s.abs_stop : s.rtol * rr + s.atol;
     if (blockIdx.x == 0 && threadIdx.x == 0)
     {
@@ -248,28 +325,28 @@ __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg(CGState s, cons
     for (int64_t it = 1;; ++it)
     {
         double lpq = 0;
-        for (int sl = gw; sl < s.nslices; sl += W)
+        for (int sl = s0 + warp; sl < s1; sl += (int)(blockDim.x >> 5))
         {
             TV acc[D];
             const int i = spmv_slice<TK, TV, D>(sl, s.n, s.rowptr, s.perm, s.slice_off, s.col_sell, K, r, pold, beta,
-                                                acc);
+                                                acc, pf, pl);
             if (i >= 0)
             {
 #pragma unroll
                 for (int c = 0; c < D; ++c)
                 {
                     const int64_t k = (int64_t)i * D + c;
-                    const TV pn = r[k] + beta * pold[k];
-                    pnew[k] = pn;
-                    q[k] = acc[c];
+                    const TV pn = ld_keep(r + k, pl) + beta * ld_keep(pold + k, pl);
+                    st_keep(pnew + k, pn, pl);
+                    st_keep(q + k, acc[c], pl);
                     lpq += (double)pn * (double)acc[c];
                 }
             }
         }
         block_partial(lpq, s.part, 1, sh);
-        if (!grid_barrier(s.bar, s.info, &s_fail))
+        double pq;
+        if (!grid_reduce(s.bar, s.info, &s_fail, s.part, 1, s.tot, sh, &pq))
             return;
-        const double pq = grid_total(s.part, 1, sh);
         if (pq == 0.0)
         {
             if (blockIdx.x == 0 && threadIdx.x == 0)
@@ -284,16 +361,16 @@ __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg(CGState s, cons
         double lrr = 0;
         for (int64_t k = gt; k < s.ndof; k += T)
         {
-            const TV pn = pnew[k];
-            x[k] = x[k] + al * pn;
-            const TV rv = r[k] - al * q[k];
-            r[k] = rv;
+            const TV pn = ld_keep(pnew + k, pl);
+            st_keep(x + k, ld_keep(x + k, pl) + al * pn, pl);
+            const TV rv = ld_keep(r + k, pl) - al * ld_keep(q + k, pl);
+            st_keep(r + k, rv, pl);
             lrr += (double)rv * (double)rv;
         }
         block_partial(lrr, s.part, 0, sh);
-        if (!grid_barrier(s.bar, s.info, &s_fail))
+        double rn;
+        if (!grid_reduce(s.bar, s.info, &s_fail, s.part, 0, s.tot, sh, &rn))
             return;
-        const double rn = grid_total(s.part, 0, sh);
         const bool done = rn <= stop;
         const bool capped = it >= s.maxit;
         if (done || capped)
@@ -344,7 +421,8 @@ __global__ void __launch_bounds__(256) k_residual64(int n, int nslices, const in
     for (int sl = gw; sl < nslices; sl += W)
     {
         double acc[D];
-        const int i = spmv_slice<double, double, D>(sl, n, rowptr, perm, slice_off, col_sell, K, x, x, 0.0, acc);
+        const int i = spmv_slice<double, double, D>(sl, n, rowptr, perm, slice_off, col_sell, K, x, x, 0.0, acc,
+                                                    l2_evict_first(), l2_evict_last());
         if (i >= 0)
             for (int c = 0; c < D; ++c)
             {
@@ -392,9 +470,8 @@ static cudaError_t run_cg(Problem &p, const TK *K, const TV *b, TV *x, TV *r, TV
             occ = 1;
     }
     int grid = p.num_sms * std::min(occ, kCGMinBlocks);
-    const int64_t slice_blocks = (int64_t)p.nslices / (kCGThreads / 32) + 1;
-    if (grid > slice_blocks)
-        grid = (int)std::max<int64_t>(1, slice_blocks);
+    if (grid > p.nslices)
+        grid = std::max(1, p.nslices);
     if (grid > kMaxGridBlocks)
         grid = kMaxGridBlocks;
     CGState s;
@@ -411,6 +488,7 @@ static cudaError_t run_cg(Problem &p, const TK *K, const TV *b, TV *x, TV *r, TV
     s.maxit = maxit;
     s.bar = p.barrier;
     s.part = p.partials;
+    s.tot = p.partials + 2 * kMaxGridBlocks;
     s.info = p.cg_info;
     if ((e = cudaMemsetAsync(p.barrier, 0, 2 * sizeof(unsigned), p.stream)) != cudaSuccess)
         return e;
