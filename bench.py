@@ -324,6 +324,9 @@ def run_ours(a):
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "newton_per_step": sum(st["newton_solves"] for st in stats) / K,
             "cg_iters_per_step": iters / K,
+            "phases_ms_per_step": {"assembly": (c1["assembly_seconds"] - c0["assembly_seconds"]) * 1e3 / K,
+                                   "force": (c1["force_seconds"] - c0["force_seconds"]) * 1e3 / K,
+                                   "cg_kernel": cg_s * 1e3 / K},
             "roofline": roof, "e2e": e2e, "gpu_launches": counters_total, "clocks": clocks,
             "mixed": mixed, "cpu_baseline": cpu,
         }

@@ -23,11 +23,11 @@
 namespace lpm
 {
 
-constexpr int kAsmThreads = 64;
+
 
 struct AsmArgs
 {
-    int n, dim, mb;
+    int n, mb, mrec;
     const int *__restrict__ bstart, *__restrict__ nb0, *__restrict__ bp2, *__restrict__ brev;
     const int *__restrict__ cstart, *__restrict__ conns, *__restrict__ cons;
     const int *__restrict__ perm;
@@ -38,30 +38,31 @@ struct AsmArgs
     int apply_bc;
 };
 
-// shared-memory staging of particle i's neighbourhood
+// Shared-memory staging of particle i's neighbourhood.  Own bonds a (i -> k) keep their full
+// record; every same-layer bond of every neighbour k (k -> x) is a "record" holding its cosines,
+// T = (1 - D) Tv (the product the reference forms inline, same rounding), its partner x, the
+// slot of x in conns(i), and the cosines and T of the opposite bond x -> k.
 struct AsmSmem
 {
-    int *conns;                      // [kMaxConns]
-    int *o_p2, *o_revpos, *o_L, *n_off; // own bonds [mb], n_off [mb+1]
-    double *o_cs, *o_Kn, *o_Tv, *o_D, *o_S; // [mb*3], [mb], [mb], [mb], [mb*3]
-    int *n_p2, *n_slot, *n_rev;      // neighbour (same-layer) bonds [mb*mb]
-    double *n_cs, *n_Kn, *n_Tv, *n_D; // [mb*mb*3], [mb*mb] ...
-    signed char *dir;                // [2][kMaxConns]
-    signed char *hop;                // [mb][kMaxConns]
+    double *o_cs, *o_Kn, *o_Tv, *o_D, *o_S; // own bonds [mb*3], [mb], [mb], [mb], [mb*3] (S of k)
+    double *o_rKn, *o_rTv, *o_rD;            // the opposite bond k -> i of own bond a
+    double *n_cs, *n_T, *r_cs, *r_T;          // records [mrec*3], [mrec], [mrec*3], [mrec]
+    int *conns;                               // [kMaxConns]
+    int *o_p2, *o_revpos, *o_L, *n_off;       // [mb], [mb], [mb], [mb+1]
+    int *n_p2, *n_slot;                       // [mrec]
+    signed char *dir, *hop;                   // [2][kMaxConns], [mb][kMaxConns]
 };
 
-__host__ __device__ inline size_t asm_smem_bytes(int mb)
+__host__ __device__ inline size_t asm_smem_bytes(int mb, int mrec)
 {
-    const size_t m2 = (size_t)mb * mb;
-    return sizeof(int) * (kMaxConns + 4 * (size_t)mb + 1 + 3 * m2) +
-           sizeof(double) * (3 * (size_t)mb + 3 * (size_t)mb + 3 * (size_t)mb + 3 * m2 + 3 * m2) +
+    return sizeof(double) * (12 * (size_t)mb + 8 * (size_t)mrec) +
+           sizeof(int) * (kMaxConns + 4 * (size_t)mb + 1 + 2 * (size_t)mrec) +
            sizeof(signed char) * ((2 + (size_t)mb) * kMaxConns) + 64;
 }
 
-__device__ inline AsmSmem carve(void *base, int mb)
+__device__ inline AsmSmem carve(void *base, int mb, int mrec)
 {
     AsmSmem s;
-    const size_t m2 = (size_t)mb * mb;
     double *d = static_cast<double *>(base);
     s.o_cs = d;
     d += 3 * mb;
@@ -73,14 +74,20 @@ __device__ inline AsmSmem carve(void *base, int mb)
     d += mb;
     s.o_S = d;
     d += 3 * mb;
+    s.o_rKn = d;
+    d += mb;
+    s.o_rTv = d;
+    d += mb;
+    s.o_rD = d;
+    d += mb;
     s.n_cs = d;
-    d += 3 * m2;
-    s.n_Kn = d;
-    d += m2;
-    s.n_Tv = d;
-    d += m2;
-    s.n_D = d;
-    d += m2;
+    d += 3 * mrec;
+    s.n_T = d;
+    d += mrec;
+    s.r_cs = d;
+    d += 3 * mrec;
+    s.r_T = d;
+    d += mrec;
     int *q = reinterpret_cast<int *>(d);
     s.conns = q;
     q += kMaxConns;
@@ -93,11 +100,9 @@ __device__ inline AsmSmem carve(void *base, int mb)
     s.n_off = q;
     q += mb + 1;
     s.n_p2 = q;
-    q += m2;
+    q += mrec;
     s.n_slot = q;
-    q += m2;
-    s.n_rev = q;
-    q += m2;
+    q += mrec;
     signed char *c = reinterpret_cast<signed char *>(q);
     s.dir = c;
     c += 2 * kMaxConns;
@@ -122,47 +127,142 @@ __device__ __forceinline__ int find_slot(const int *conns, int nc, int x)
     return -1;
 }
 
-// (Kn+Tv) * cs_r * cs_c as the reference writes it: pow(cs, 2) on the diagonal,
-// cs_hi * cs_lo (coordinate order x < y < z) off the diagonal (derivative.h:17-33, 62-87)
-__device__ __forceinline__ double pkt(double kt, const double *c, int r, int q)
+// A thread owns output row R of block (i, j): row R of K(i, j) and column R of K(j, i).
+// fr[c] accumulates K(i,j)[R][c] and gc[c] accumulates K(j,i)[c][R], each entry through the
+// operations derivative.h applies to it:
+//   other bond (derivative.h:91-99):  -= 0.5*((1-D1)Tv1 + (1-D2)Tv2) * cs2[row] * cs1[col]
+//   two-hop    (derivative.h:105-113, 128-136): -= 0.5*(T_B + T_A) * csA[row] * csB[col]
+//   direct     (derivative.h:62-87):  += (1-D)((-Kn cs[col] + Tv S_j[col]) cs[row] - (Kn+Tv) cs.cs)
+// where (Kn+Tv) cs.cs is (Kn+Tv)*(cs[r]*cs[r]) on the diagonal (pow(cs,2)) and
+// (Kn+Tv)*cs[hi]*cs[lo] off it (coordinate order x < y < z), as the reference writes them.
+template <int D>
+__device__ __forceinline__ void sub_other_row(double fr[D], int R, double T1, const double *c1, double T2,
+                                              const double *c2)
+{
+    const double t = 0.5 * (T1 + T2);
+#pragma unroll
+    for (int c = 0; c < D; ++c)
+        fr[c] -= t * c2[R] * c1[c];
+}
+template <int D>
+__device__ __forceinline__ void sub_other_col(double gc[D], int R, double T1, const double *c1, double T2,
+                                              const double *c2)
+{
+    const double t = 0.5 * (T1 + T2);
+#pragma unroll
+    for (int c = 0; c < D; ++c)
+        gc[c] -= t * c2[c] * c1[R];
+}
+template <int D>
+__device__ __forceinline__ void sub_hop_row(double fr[D], int R, double TA, const double *cA, double TB,
+                                            const double *cB)
+{
+    const double t = 0.5 * (TB + TA);
+#pragma unroll
+    for (int c = 0; c < D; ++c)
+        fr[c] -= t * cA[R] * cB[c];
+}
+template <int D>
+__device__ __forceinline__ void sub_hop_col(double gc[D], int R, double TA, const double *cA, double TB,
+                                            const double *cB)
+{
+    const double t = 0.5 * (TB + TA);
+#pragma unroll
+    for (int c = 0; c < D; ++c)
+        gc[c] -= t * cA[c] * cB[R];
+}
+// (Kn+Tv) cs_r cs_q in the reference's operator order
+__device__ __forceinline__ double pkt_rt(double kt, const double *c, int r, int q)
 {
     if (r == q)
         return kt * (c[r] * c[r]);
-    const int hi = r > q ? r : q, lo = r > q ? q : r;
-    return kt * c[hi] * c[lo];
+    return kt * c[r > q ? r : q] * c[r > q ? q : r];
 }
-
-// the "other bond" term of derivative.h:91-99: bond 1 gives the column cosine, bond 2 the row
-__device__ __forceinline__ void sub_other(double acc[3][3], int d, double D1, double Tv1, const double *c1, double D2,
-                                          double Tv2, const double *c2)
-{
-    const double t = 0.5 * ((1 - D1) * Tv1 + (1 - D2) * Tv2);
-    for (int r = 0; r < d; ++r)
-        for (int c = 0; c < d; ++c)
-            acc[r][c] -= t * c2[r] * c1[c];
-}
-
-// the two-hop term i->k (bond A), k->j (bond B) of derivative.h:105-113 / 128-136
-__device__ __forceinline__ void sub_hop(double acc[3][3], int d, double DA, double TvA, const double *cA, double DB,
-                                        double TvB, const double *cB)
-{
-    const double t = 0.5 * ((1 - DB) * TvB + (1 - DA) * TvA);
-    for (int r = 0; r < d; ++r)
-        for (int c = 0; c < d; ++c)
-            acc[r][c] -= t * cA[r] * cB[c];
-}
-
-// the direct term of derivative.h:62-87: bond i->j with the cosine sum S of particle j
-__device__ __forceinline__ void add_direct(double acc[3][3], int d, double D, double Kn, double Tv, const double *c,
-                                           const double *S)
+template <int D>
+__device__ __forceinline__ void add_direct_row(double fr[D], int R, double Dm, double Kn, double Tv, const double *c,
+                                               const double *S)
 {
     const double kt = Kn + Tv;
-    for (int r = 0; r < d; ++r)
-        for (int q = 0; q < d; ++q)
-            acc[r][q] += (1 - D) * ((-Kn * c[q] + Tv * S[q]) * c[r] - pkt(kt, c, r, q));
+#pragma unroll
+    for (int q = 0; q < D; ++q)
+        fr[q] += (1 - Dm) * ((-Kn * c[q] + Tv * S[q]) * c[R] - pkt_rt(kt, c, R, q));
+}
+template <int D>
+__device__ __forceinline__ void add_direct_col(double gc[D], int R, double Dm, double Kn, double Tv, const double *c,
+                                               const double *S)
+{
+    const double kt = Kn + Tv;
+#pragma unroll
+    for (int r = 0; r < D; ++r)
+        gc[r] += (1 - Dm) * ((-Kn * c[R] + Tv * S[R]) * c[r] - pkt_rt(kt, c, r, R));
 }
 
-__global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs a)
+// row R of K_L(i, j) and column R of K_L(j, i) (j's orientation) for slot sl, layer L
+template <int D, int L>
+__device__ __forceinline__ void layer_rows(const AsmSmem &s, int sl, int R, int olo, int ohi, const double *Si,
+                                           double fr[D], double gc[D])
+{
+    const int aj = s.dir[L * kMaxConns + sl];
+    for (int o = olo; o < ohi; ++o)
+    {
+        const double *co = s.o_cs + 3 * o;
+        const double To = (1 - s.o_D[o]) * s.o_Tv[o];
+        const int hb = s.hop[o * kMaxConns + sl];
+        if (aj >= 0)
+        {
+            if (o == aj)
+            {
+                add_direct_row<D>(fr, R, s.o_D[o], s.o_Kn[o], s.o_Tv[o], co, s.o_S + 3 * o);
+                continue;
+            }
+            sub_other_row<D>(fr, R, (1 - s.o_D[aj]) * s.o_Tv[aj], s.o_cs + 3 * aj, To, co);
+        }
+        if (hb >= 0)
+        {
+            const int q = s.n_off[o] + hb;
+            sub_hop_row<D>(fr, R, To, co, s.n_T[q], s.n_cs + 3 * q);
+        }
+    }
+    if (aj >= 0)
+    {
+        const int jlo = s.n_off[aj], jhi = s.n_off[aj + 1];
+        const int rji = jlo + s.o_revpos[aj];
+        const double Tji = s.n_T[rji];
+        const double *cji = s.n_cs + 3 * rji;
+        for (int q = jlo; q < jhi; ++q)
+        {
+            const double *cq = s.n_cs + 3 * q;
+            if (q == rji)
+            {
+                add_direct_col<D>(gc, R, s.o_rD[aj], s.o_rKn[aj], s.o_rTv[aj], cq, Si);
+                continue;
+            }
+            sub_other_col<D>(gc, R, Tji, cji, s.n_T[q], cq);
+            const int xs = s.n_slot[q];
+            const int ax = (xs >= 0) ? s.dir[L * kMaxConns + xs] : -1;
+            if (ax >= 0)
+            {
+                const int rxi = s.n_off[ax] + s.o_revpos[ax];
+                sub_hop_col<D>(gc, R, s.n_T[q], cq, s.n_T[rxi], s.n_cs + 3 * rxi);
+            }
+        }
+    }
+    else
+    {
+        for (int o = olo; o < ohi; ++o)
+        {
+            const int hb = s.hop[o * kMaxConns + sl];
+            if (hb < 0)
+                continue;
+            const int q = s.n_off[o] + hb;
+            const int rki = s.n_off[o] + s.o_revpos[o];
+            sub_hop_col<D>(gc, R, s.r_T[q], s.r_cs + 3 * q, s.n_T[rki], s.n_cs + 3 * rki);
+        }
+    }
+}
+
+template <int D>
+__global__ void __launch_bounds__(256) k_assemble(AsmArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     // CTAs run in sliced-ELL order, so the rows of one slice (whose entries interleave in
@@ -172,26 +272,25 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs a)
     const int lane = pos % kSlice;
     const int64_t sbase = a.slice_off[pos / kSlice];
     const int tid = threadIdx.x;
-    const int mb = a.mb, d = a.dim;
-    AsmSmem s = carve(smem_raw, mb);
+    AsmSmem s = carve(smem_raw, a.mb, a.mrec);
 
     const int b0 = a.bstart[i], nbi = a.bstart[i + 1] - b0, n0 = a.nb0[i];
     const int c0 = a.cstart[i], nc = a.cstart[i + 1] - c0;
-    for (int q = tid; q < nc; q += kAsmThreads)
+    for (int q = tid; q < nc; q += blockDim.x)
         s.conns[q] = a.conns[c0 + q];
-    for (int q = tid; q < 2 * kMaxConns; q += kAsmThreads)
+    for (int q = tid; q < 2 * kMaxConns; q += blockDim.x)
         s.dir[q] = -1;
-    for (int q = tid; q < nbi * kMaxConns; q += kAsmThreads)
+    for (int q = tid; q < nbi * kMaxConns; q += blockDim.x)
         s.hop[q] = -1;
-    // own bonds
-    for (int o = tid; o < nbi; o += kAsmThreads)
+    for (int o = tid; o < nbi; o += blockDim.x)
     {
         const int b = b0 + o, k = a.bp2[b], L = (o < n0) ? 0 : 1;
         const int klo = (L == 0) ? a.bstart[k] : a.bstart[k] + a.nb0[k];
         const int khi = (L == 0) ? a.bstart[k] + a.nb0[k] : a.bstart[k + 1];
+        const int rb = a.brev[b];
         s.o_p2[o] = k;
         s.o_L[o] = L;
-        s.o_revpos[o] = a.brev[b] - klo;
+        s.o_revpos[o] = rb - klo;
         s.n_off[o + 1] = khi - klo; // counts, scanned below
         for (int c = 0; c < 3; ++c)
         {
@@ -201,6 +300,9 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs a)
         s.o_Kn[o] = a.Kn[b];
         s.o_Tv[o] = a.Tv[b];
         s.o_D[o] = a.bdamage[b];
+        s.o_rKn[o] = a.Kn[rb];
+        s.o_rTv[o] = a.Tv[rb];
+        s.o_rD[o] = a.bdamage[rb];
     }
     __syncthreads();
     if (tid == 0)
@@ -211,8 +313,7 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs a)
     }
     __syncthreads();
     const int ntot = s.n_off[nbi];
-    // neighbours' same-layer bonds
-    for (int q = tid; q < ntot; q += kAsmThreads)
+    for (int q = tid; q < ntot; q += blockDim.x)
     {
         int o = 0;
         while (s.n_off[o + 1] <= q)
@@ -221,158 +322,99 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs a)
         const int klo = (L == 0) ? a.bstart[k] : a.bstart[k] + a.nb0[k];
         const int b = klo + (q - s.n_off[o]);
         const int x = a.bp2[b];
+        const int rb = a.brev[b];
         s.n_p2[q] = x;
-        s.n_rev[q] = a.brev[b];
-        s.n_slot[q] = find_slot(s.conns, nc, x);
+        const int sl = find_slot(s.conns, nc, x);
+        s.n_slot[q] = sl;
         for (int c = 0; c < 3; ++c)
+        {
             s.n_cs[3 * q + c] = a.cs[3 * (int64_t)b + c];
-        s.n_Kn[q] = a.Kn[b];
-        s.n_Tv[q] = a.Tv[b];
-        s.n_D[q] = a.bdamage[b];
+            s.r_cs[3 * q + c] = a.cs[3 * (int64_t)rb + c];
+        }
+        s.n_T[q] = (1 - a.bdamage[b]) * a.Tv[b];
+        s.r_T[q] = (1 - a.bdamage[rb]) * a.Tv[rb];
+        if (sl >= 0)
+            s.hop[o * kMaxConns + sl] = (signed char)(q - s.n_off[o]);
     }
-    __syncthreads();
-    for (int o = tid; o < nbi; o += kAsmThreads)
+    for (int o = tid; o < nbi; o += blockDim.x)
     {
         const int sl = find_slot(s.conns, nc, s.o_p2[o]);
         if (sl >= 0)
             s.dir[s.o_L[o] * kMaxConns + sl] = (signed char)o;
-    }
-    for (int q = tid; q < ntot; q += kAsmThreads)
-    {
-        int o = 0;
-        while (s.n_off[o + 1] <= q)
-            ++o;
-        const int sl = s.n_slot[q];
-        if (sl >= 0)
-            s.hop[o * kMaxConns + sl] = (signed char)(q - s.n_off[o]);
     }
     __syncthreads();
 
     const int selfslot = find_slot(s.conns, nc, i);
     const double dvi = a.damage_visual[i];
     bool ci[3];
+#pragma unroll
     for (int k = 0; k < 3; ++k)
-        ci[k] = a.apply_bc && (k < d) && (a.cons[3 * i + k] == 1 || fabs(dvi - 1.0) < kEps);
+        ci[k] = a.apply_bc && (k < D) && (a.cons[3 * i + k] == 1 || fabs(dvi - 1.0) < kEps);
+    const double *Si0 = a.cs_sum + 6 * (int64_t)i, *Si1 = Si0 + 3;
 
-    for (int sl = tid; sl < nc; sl += kAsmThreads)
+    for (int t = tid; t < nc * D; t += blockDim.x)
     {
+        const int sl = t / D, R = t - sl * D;
         const int j = s.conns[sl];
-        double out[3][3];
+        double out[D];
         if (sl == selfslot)
         {
-            // fdu2dxyz (derivative.h:8-45): one accumulator over both layers, upper part
-            double acc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            // fdu2dxyz (derivative.h:8-45): one accumulator over both layers; row R of the upper
+            // part is acc[R][q >= R], the mirrored entries come from the rows above
+            double acc[D];
+#pragma unroll
+            for (int q = 0; q < D; ++q)
+                acc[q] = 0.0;
             for (int o = 0; o < nbi; ++o)
             {
-                const int L = s.o_L[o];
                 const double *c = s.o_cs + 3 * o;
-                const double D = s.o_D[o], Kn = s.o_Kn[o], Tv = s.o_Tv[o], kt = Kn + Tv;
-                const double *S = a.cs_sum + 6 * (int64_t)i + 3 * L;
-                for (int r = 0; r < d; ++r)
-                    for (int q = r; q < d; ++q)
-                        acc[r][q] += (1 - D) * ((Kn * c[q] + Tv * S[q]) * c[r] + pkt(kt, c, r, q));
+                const double Dm = s.o_D[o], Kn = s.o_Kn[o], Tv = s.o_Tv[o], kt = Kn + Tv;
+                const double *S = (s.o_L[o] == 0) ? Si0 : Si1;
+#pragma unroll
+                for (int q = 0; q < D; ++q)
+                {
+                    // entry (min(R,q), max(R,q)) of the upper triangle
+                    const int rr = R < q ? R : q, cc = R < q ? q : R;
+                    acc[q] += (1 - Dm) * ((Kn * c[cc] + Tv * S[cc]) * c[rr] + pkt_rt(kt, c, rr, cc));
+                }
             }
-            for (int r = 0; r < d; ++r)
-                for (int q = 0; q < d; ++q)
-                    out[r][q] = (q >= r) ? acc[r][q] : acc[q][r];
-            for (int r = 0; r < d; ++r)
-                a.diag_raw[(int64_t)d * i + r] = out[r][r];
-            for (int r = 0; r < d; ++r)
-                for (int q = 0; q < d; ++q)
-                    if (r != q && (ci[r] || ci[q]))
-                        out[r][q] = 0.0;
+#pragma unroll
+            for (int q = 0; q < D; ++q)
+                out[q] = acc[q];
+            a.diag_raw[(int64_t)D * i + R] = out[R];
+#pragma unroll
+            for (int q = 0; q < D; ++q)
+                if (R != q && (ci[R] || ci[q]))
+                    out[q] = 0.0;
         }
         else
         {
-            double f[2][3][3], g[2][3][3];
-            for (int L = 0; L < 2; ++L)
-                for (int r = 0; r < 3; ++r)
-                    for (int q = 0; q < 3; ++q)
-                    {
-                        f[L][r][q] = 0.0;
-                        g[L][r][q] = 0.0;
-                    }
-            for (int L = 0; L < 2; ++L)
+            double f0[D], f1[D], g0[D], g1[D];
+#pragma unroll
+            for (int q = 0; q < D; ++q)
             {
-                const int aj = s.dir[L * kMaxConns + sl];
-                const int olo = (L == 0) ? 0 : n0, ohi = (L == 0) ? n0 : nbi;
-                // K_L(i, j): fdu2dxyz1/2(pi = i, pj = j)
-                for (int o = olo; o < ohi; ++o)
-                {
-                    const double *co = s.o_cs + 3 * o;
-                    const int hb = s.hop[o * kMaxConns + sl];
-                    if (aj >= 0)
-                    {
-                        if (o == aj)
-                        {
-                            add_direct(f[L], d, s.o_D[o], s.o_Kn[o], s.o_Tv[o], co, s.o_S + 3 * o);
-                            continue;
-                        }
-                        sub_other(f[L], d, s.o_D[aj], s.o_Tv[aj], s.o_cs + 3 * aj, s.o_D[o], s.o_Tv[o], co);
-                    }
-                    if (hb >= 0)
-                    {
-                        const int q = s.n_off[o] + hb;
-                        sub_hop(f[L], d, s.o_D[o], s.o_Tv[o], co, s.n_D[q], s.n_Tv[q], s.n_cs + 3 * q);
-                    }
-                }
-                // K_L(j, i): fdu2dxyz1/2(pi = j, pj = i), accumulated in j's orientation
-                if (aj >= 0)
-                {
-                    const int jlo = s.n_off[aj], jhi = s.n_off[aj + 1];
-                    const int rji = jlo + s.o_revpos[aj]; // bond j -> i
-                    for (int q = jlo; q < jhi; ++q)
-                    {
-                        const double *cq = s.n_cs + 3 * q;
-                        if (s.n_p2[q] == i)
-                        {
-                            add_direct(g[L], d, s.n_D[q], s.n_Kn[q], s.n_Tv[q], cq,
-                                       a.cs_sum + 6 * (int64_t)i + 3 * L);
-                            continue;
-                        }
-                        sub_other(g[L], d, s.n_D[rji], s.n_Tv[rji], s.n_cs + 3 * rji, s.n_D[q], s.n_Tv[q], cq);
-                        const int xs = s.n_slot[q];
-                        const int ax = (xs >= 0) ? s.dir[L * kMaxConns + xs] : -1;
-                        if (ax >= 0)
-                        {
-                            const int rxi = s.n_off[ax] + s.o_revpos[ax]; // bond x -> i
-                            sub_hop(g[L], d, s.n_D[q], s.n_Tv[q], cq, s.n_D[rxi], s.n_Tv[rxi], s.n_cs + 3 * rxi);
-                        }
-                    }
-                }
-                else
-                {
-                    for (int o = olo; o < ohi; ++o)
-                    {
-                        const int hb = s.hop[o * kMaxConns + sl];
-                        if (hb < 0)
-                            continue;
-                        const int q = s.n_off[o] + hb;      // bond k -> j
-                        const int bjk = s.n_rev[q];          // bond j -> k (global)
-                        const int rki = s.n_off[o] + s.o_revpos[o]; // bond k -> i
-                        const double cjk[3] = {a.cs[3 * (int64_t)bjk], a.cs[3 * (int64_t)bjk + 1],
-                                               a.cs[3 * (int64_t)bjk + 2]};
-                        sub_hop(g[L], d, a.bdamage[bjk], a.Tv[bjk], cjk, s.n_D[rki], s.n_Tv[rki], s.n_cs + 3 * rki);
-                    }
-                }
+                f0[q] = 0.0;
+                f1[q] = 0.0;
+                g0[q] = 0.0;
+                g1[q] = 0.0;
             }
-            bool cj[3];
+            layer_rows<D, 0>(s, sl, R, 0, n0, Si0, f0, g0);
+            layer_rows<D, 1>(s, sl, R, n0, nbi, Si1, f1, g1);
             const double dvj = a.damage_visual[j];
-            for (int k = 0; k < 3; ++k)
-                cj[k] = a.apply_bc && (k < d) && (a.cons[3 * j + k] == 1 || fabs(dvj - 1.0) < kEps);
-            for (int r = 0; r < d; ++r)
-                for (int q = 0; q < d; ++q)
-                {
-                    const double kij = f[0][r][q] + f[1][r][q];
-                    const double kji = g[0][q][r] + g[1][q][r];
-                    const double v = 0.5 * kij + 0.5 * kji;
-                    out[r][q] = (ci[r] || cj[q]) ? 0.0 : v;
-                }
+#pragma unroll
+            for (int q = 0; q < D; ++q)
+            {
+                const bool cjq = a.apply_bc && (a.cons[3 * j + q] == 1 || fabs(dvj - 1.0) < kEps);
+                const double kij = f0[q] + f1[q];
+                const double kji = g0[q] + g1[q];
+                const double v = 0.5 * kij + 0.5 * kji;
+                out[q] = (ci[R] || cjq) ? 0.0 : v;
+            }
         }
-        double *dst = a.K + (sbase + sl) * d * d * kSlice + lane;
-        for (int r = 0; r < d; ++r)
-            for (int q = 0; q < d; ++q)
-                dst[(r * d + q) * kSlice] = out[r][q];
+        double *dst = a.K + (sbase + sl) * D * D * kSlice + lane;
+#pragma unroll
+        for (int q = 0; q < D; ++q)
+            dst[(R * D + q) * kSlice] = out[q];
     }
 }
 
@@ -426,8 +468,8 @@ cudaError_t launch_assemble(Problem &p, bool apply_bc)
 {
     AsmArgs a;
     a.n = p.n;
-    a.dim = p.dim;
     a.mb = p.max_bonds;
+    a.mrec = p.max_records;
     a.bstart = p.bstart;
     a.nb0 = p.nb0;
     a.bp2 = p.bp2;
@@ -446,11 +488,24 @@ cudaError_t launch_assemble(Problem &p, bool apply_bc)
     a.K = p.K;
     a.diag_raw = p.diag_raw;
     a.apply_bc = apply_bc ? 1 : 0;
-    const size_t smem = asm_smem_bytes(a.mb);
-    cudaError_t e = cudaFuncSetAttribute(k_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess)
-        return e;
-    k_assemble<<<p.n, kAsmThreads, smem, p.stream>>>(a);
+    const size_t smem = asm_smem_bytes(a.mb, a.mrec);
+    // one thread per (connection slot, block row)
+    const int threads = std::min(256, std::max(32, ((p.max_conns * p.dim + 31) / 32) * 32));
+    cudaError_t e;
+    if (p.dim == 2)
+    {
+        if ((e = cudaFuncSetAttribute(k_assemble<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+            cudaSuccess)
+            return e;
+        k_assemble<2><<<p.n, threads, smem, p.stream>>>(a);
+    }
+    else
+    {
+        if ((e = cudaFuncSetAttribute(k_assemble<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+            cudaSuccess)
+            return e;
+        k_assemble<3><<<p.n, threads, smem, p.stream>>>(a);
+    }
     p.ctr.kernel_launches++;
     if ((e = cudaGetLastError()) != cudaSuccess)
         return e;

@@ -66,6 +66,7 @@ struct Problem
     int n = 0, dim = 2, nsv = 1;
     int64_t nbonds = 0, nnzb = 0, nnz_upper = 0;
     int max_bonds = 0, max_conns = 0;
+    int max_records = 0; // largest sum over a particle's bonds of the partner's same-layer bond count
     double kntv[3] = {0, 0, 0};
     cudaStream_t stream = nullptr;
     int device = 0, num_sms = 0;

@@ -385,6 +385,22 @@ __global__ void k_conns(int n, const int *__restrict__ bstart, const int *__rest
     }
 }
 
+// per particle: sum over its bonds of the partner's same-layer bond count (assembly staging size)
+__global__ void k_records(int n, const int *__restrict__ bstart, const int *__restrict__ nb0,
+                          const int *__restrict__ bp2, int *__restrict__ nrec)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    int t = 0;
+    for (int b = bstart[i]; b < bstart[i + 1]; ++b)
+    {
+        const int k = bp2[b];
+        t += (b < bstart[i] + nb0[i]) ? nb0[k] : (bstart[k + 1] - bstart[k] - nb0[k]);
+    }
+    nrec[i] = t;
+}
+
 __global__ void k_conns_fill(int n, const int *__restrict__ pad_c, const int *__restrict__ cstart,
                              int *__restrict__ conns)
 {
@@ -647,6 +663,8 @@ cudaError_t build_topology(Problem &p, const double *xyz_host, int *err_code)
     LPM_TRY(cudaGetLastError());
     LPM_TRY(reduce_max(p, ncx, n, &p.max_conns));
     LPM_TRY(reduce_max(p, p.nb, n, &p.max_bonds));
+    k_records<<<div_up(n, T), T, 0, p.stream>>>(n, p.bstart, p.nb0, p.bp2, ncx);
+    LPM_TRY(reduce_max(p, ncx, n, &p.max_records));
     cudaFreeAsync(pad_c, p.stream);
     cudaFreeAsync(ncx, p.stream);
 
