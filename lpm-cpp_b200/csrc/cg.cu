@@ -25,6 +25,8 @@
 #include <cooperative_groups.h>
 
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 
 #include "lpm_internal.cuh"
 
@@ -515,6 +517,11 @@ static cudaError_t run_cg(Problem &p, const TK *K, const TV *b, TV *x, TV *r, TV
         float ms = 0;
         if (cudaEventElapsedTime(&ms, p.cg_ev[0], p.cg_ev[1]) == cudaSuccess)
             p.ctr.cg_kernel_seconds += ms * 1e-3;
+        static const bool log = std::getenv("LPMGPU_LOG") != nullptr;
+        if (log)
+            std::fprintf(stderr, "lpmgpu cg launch %lld: %s%s iters=%lld ms=%.3f grid=%d\n",
+                         (long long)p.ctr.cg_launches, sizeof(TK) == 8 ? "fp64" : "fp32", D == 2 ? "/2d" : "/3d",
+                         (long long)p.cg_info_host[0], ms, grid);
     }
     if (p.cg_info_host[1] & 1)
         out.maxit_hits++;
