@@ -190,6 +190,24 @@ int32_t lpmgpu_get_counters(const lpmgpu_solver *h, lpmgpu_counters *out);
 /* The CUDA stream (cudaStream_t) the handle launches on, for callers that time with events. */
 int32_t lpmgpu_get_stream(const lpmgpu_solver *h, void **stream);
 
+/* Allocation-free CG, for callers that cannot allocate device memory: code running under CUDA
+ * graph capture, where cudaMalloc is not allowed, and hosts whose device memory belongs to an
+ * external pool or arena.  No counterpart in the reference (LPM-CPP solves inside
+ * Solver::LPM_CG with MKL and allocates per call).
+ * Solves A x = b by the same unpreconditioned CG and stopping rule as lpmgpu_solve_linear
+ * (||r||^2 <= rtol*||r0||^2 + atol, x0 = 0, maxit <= 0 means rows*dim).  A is block-CSR on the
+ * device: rowptr[nrows+1] and colidx[nnzb] (int32), values[nnzb*dim*dim] row-major blocks; b and
+ * x are device vectors of rows*dim doubles; stream is a cudaStream_t (NULL = default stream);
+ * *iterations (host, may be NULL) gets the iteration count.  The call allocates nothing: its
+ * work vectors and reduction words live in a static device array that every GPU loading the
+ * library holds (about 8 MiB), so at most 262144 unknowns are accepted (larger sizes return
+ * LPMGPU_ERR_INVALID_ARG).  All calls on a device share that array, so calls that overlap on
+ * the GPU race.  The first call on a device looks the array up and should come before any
+ * stream capture.  Synchronises the stream before returning. */
+int32_t lpmgpu_cg_bsr_noalloc(int32_t dim, int32_t nrows, const int32_t *rowptr, const int32_t *colidx,
+                              const double *values, const double *b, double *x, double rtol, double atol,
+                              int64_t maxit, void *stream, int64_t *iterations);
+
 #ifdef __cplusplus
 }
 #endif

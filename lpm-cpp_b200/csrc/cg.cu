@@ -24,9 +24,12 @@
 // true residual b - K x with the FP64 matrix and stops on the same squared-norm rule.
 #include <cooperative_groups.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <mutex>
+#include <string>
 
 #include "lpm_internal.cuh"
 
@@ -609,3 +612,255 @@ cudaError_t solve_linear(Problem &p, CGResult &out)
 }
 
 } // namespace lpm
+
+// ---------------------------------------------------------------------------------------
+// Allocation-free CG on a caller-supplied block-CSR matrix.
+//
+// Some callers cannot allocate device memory: code running while a CUDA graph is being
+// captured (cudaMalloc is not capturable), and hosts whose device memory is owned by an
+// external pool or arena that forbids driver allocations behind its back.  For them the
+// solve below takes every input and output from the caller and keeps its own work vectors,
+// reduction partials and barrier words in the file-scope array g_noalloc_scratch, which
+// every GPU that loads this library holds (about 8 MiB) until the process exits.
+//
+// Limits and caveats:
+//  * at most kNoAllocMaxDof unknowns (rows * dim); larger systems are rejected;
+//  * all calls on a device share the one array, so calls that overlap on the GPU (two
+//    streams, two host threads) race; serialise them;
+//  * the first call on a device looks up the array's device address (set-up) and should
+//    come before any stream capture.
+namespace lpm
+{
+
+constexpr int64_t kNoAllocMaxDof = int64_t(1) << 18; // 262,144 unknowns
+constexpr int kNoAllocMaxBlocks = 1024;
+// r, p_a, p_b, q | per-block partials [2*blocks] | totals [2] | status words [4] | barrier [2]
+constexpr int64_t kNoAllocDoubles = 4 * kNoAllocMaxDof + 2 * kNoAllocMaxBlocks + 2 + 4 + 2;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+struct CGBsr
+{
+    int nrows;
+    int64_t ndof;
+    const int *__restrict__ rowptr;
+    const int *__restrict__ col;
+    const double *__restrict__ val; // row-major d x d blocks
+    double rtol, atol;
+    int64_t maxit;
+    unsigned *bar;
+    double *part;
+    double *tot;
+    int64_t *info;
+};
+
+template <int D>
+__global__ void __launch_bounds__(kCGThreads, kCGMinBlocks)
+    k_cg_bsr_noalloc(CGBsr s, const double *__restrict__ b, double *__restrict__ x, double *__restrict__ r,
+                     double *__restrict__ pa, double *__restrict__ pb, double *__restrict__ q)
+{
+    constexpr int E = D * D;
+    __shared__ double sh[32];
+    __shared__ int s_fail;
+    if (threadIdx.x == 0)
+        s_fail = 0;
+    __syncthreads();
+    const int64_t T = (int64_t)gridDim.x * blockDim.x;
+    const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double loc = 0;
+    for (int64_t k = gt; k < s.ndof; k += T)
+    {
+        const double v = b[k];
+        r[k] = v;
+        x[k] = 0.0;
+        pa[k] = 0.0;
+        loc += v * v;
+    }
+    block_partial(loc, s.part, 0, sh);
+    double rr;
+    if (!grid_reduce(s.bar, s.info, &s_fail, s.part, 0, s.tot, sh, &rr))
+        return;
+    const double stop = s.rtol * rr + s.atol;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        s.info[0] = 0;
+    if (rr <= stop)
+        return;
+    double beta = 0.0;
+    double *pold = pa, *pnew = pb;
+    for (int64_t it = 1;; ++it)
+    {
+        double lpq = 0;
+        for (int64_t row = gt; row < s.nrows; row += T)
+        {
+            double acc[D];
+#pragma unroll
+            for (int c = 0; c < D; ++c)
+                acc[c] = 0.0;
+            for (int bk = s.rowptr[row]; bk < s.rowptr[row + 1]; ++bk)
+            {
+                const int64_t j = s.col[bk];
+                double xv[D];
+#pragma unroll
+                for (int c = 0; c < D; ++c)
+                    xv[c] = r[j * D + c] + beta * pold[j * D + c];
+                const double *v = s.val + (int64_t)bk * E;
+#pragma unroll
+                for (int rr2 = 0; rr2 < D; ++rr2)
+#pragma unroll
+                    for (int c = 0; c < D; ++c)
+                        acc[rr2] += v[rr2 * D + c] * xv[c];
+            }
+#pragma unroll
+            for (int c = 0; c < D; ++c)
+            {
+                const int64_t k = row * D + c;
+                const double pn = r[k] + beta * pold[k];
+                pnew[k] = pn;
+                q[k] = acc[c];
+                lpq += pn * acc[c];
+            }
+        }
+        block_partial(lpq, s.part, 1, sh);
+        double pq;
+        if (!grid_reduce(s.bar, s.info, &s_fail, s.part, 1, s.tot, sh, &pq))
+            return;
+        if (pq == 0.0)
+        {
+            if (blockIdx.x == 0 && threadIdx.x == 0)
+            {
+                s.info[0] = it - 1;
+                atomicOr(reinterpret_cast<unsigned long long *>(s.info + 1), 4ull);
+            }
+            return;
+        }
+        const double alpha = rr / pq;
+        double lrr = 0;
+        for (int64_t k = gt; k < s.ndof; k += T)
+        {
+            x[k] = x[k] + alpha * pnew[k];
+            const double rv = r[k] - alpha * q[k];
+            r[k] = rv;
+            lrr += rv * rv;
+        }
+        block_partial(lrr, s.part, 0, sh);
+        double rn;
+        if (!grid_reduce(s.bar, s.info, &s_fail, s.part, 0, s.tot, sh, &rn))
+            return;
+        if (rn <= stop || it >= s.maxit)
+        {
+            if (blockIdx.x == 0 && threadIdx.x == 0)
+            {
+                s.info[0] = it;
+                if (!(rn <= stop))
+                    atomicOr(reinterpret_cast<unsigned long long *>(s.info + 1), 1ull);
+            }
+            return;
+        }
+        beta = rn / rr;
+        rr = rn;
+        double *t = pold;
+        pold = pnew;
+        pnew = t;
+    }
+}
+
+static std::mutex g_noalloc_mu;
+static double *g_noalloc_dev[64] = {nullptr};
+
+// Set-up, once per device, with that device current: the device address of the array.
+static cudaError_t noalloc_scratch(int dev, double **out)
+{
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (dev < 0 || dev >= 64)
+        return cudaErrorInvalidDevice;
+    if (!g_noalloc_dev[dev])
+    {
+        double *ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            return e;
+        g_noalloc_dev[dev] = ptr;
+    }
+    *out = g_noalloc_dev[dev];
+    return cudaSuccess;
+}
+
+template <int D>
+static cudaError_t noalloc_launch(double *scr, int grid, const CGBsr &s0, const double *b, double *x,
+                                  cudaStream_t stream, int64_t *status)
+{
+    CGBsr s = s0;
+    double *r = scr, *pa = scr + kNoAllocMaxDof, *pb = scr + 2 * kNoAllocMaxDof, *q = scr + 3 * kNoAllocMaxDof;
+    s.part = scr + 4 * kNoAllocMaxDof;
+    s.tot = s.part + 2 * kNoAllocMaxBlocks;
+    s.info = reinterpret_cast<int64_t *>(s.tot + 2);
+    s.bar = reinterpret_cast<unsigned *>(s.tot + 6);
+    // the barrier words and status must start at zero; the vectors are written before use
+    cudaError_t e = cudaMemsetAsync(s.info, 0, 4 * sizeof(int64_t) + 2 * sizeof(double), stream);
+    if (e != cudaSuccess)
+        return e;
+    void *args[] = {&s, &b, &x, &r, &pa, &pb, &q};
+    e = cudaLaunchCooperativeKernel((const void *)k_cg_bsr_noalloc<D>, dim3(grid), dim3(kCGThreads), args, 0, stream);
+    if (e != cudaSuccess)
+        return e;
+    e = cudaMemcpyAsync(status, s.info, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, stream);
+    if (e != cudaSuccess)
+        return e;
+    return cudaStreamSynchronize(stream);
+}
+
+} // namespace lpm
+
+extern "C" int32_t lpmgpu_cg_bsr_noalloc(int32_t dim, int32_t nrows, const int32_t *rowptr, const int32_t *colidx,
+                                         const double *values, const double *b, double *x, double rtol, double atol,
+                                         int64_t maxit, void *stream, int64_t *iterations)
+{
+    using namespace lpm;
+    if ((dim != 2 && dim != 3) || nrows <= 0 || !rowptr || !colidx || !values || !b || !x)
+        return LPMGPU_ERR_INVALID_ARG;
+    if ((int64_t)nrows * dim > kNoAllocMaxDof)
+    {
+        set_last_error("lpmgpu_cg_bsr_noalloc: more than 262144 unknowns (the size of its static scratch)");
+        return LPMGPU_ERR_INVALID_ARG;
+    }
+    int dev = 0, sms = 0, occ = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    double *scr = nullptr;
+    if (e == cudaSuccess)
+        e = noalloc_scratch(dev, &scr);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+        e = (dim == 2) ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg_bsr_noalloc<2>, kCGThreads, 0)
+                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg_bsr_noalloc<3>, kCGThreads, 0);
+    if (e != cudaSuccess)
+    {
+        set_last_error(std::string("lpmgpu_cg_bsr_noalloc: ") + cudaGetErrorString(e));
+        return e == cudaErrorNoDevice ? LPMGPU_ERR_NO_DEVICE : LPMGPU_ERR_CUDA;
+    }
+    int grid = sms * std::max(1, std::min(occ, kCGMinBlocks));
+    grid = std::min(grid, kNoAllocMaxBlocks);
+    grid = (int)std::min<int64_t>(grid, (nrows + kCGThreads - 1) / kCGThreads);
+    grid = std::max(grid, 1);
+    CGBsr s{};
+    s.nrows = nrows;
+    s.ndof = (int64_t)nrows * dim;
+    s.rowptr = rowptr;
+    s.col = colidx;
+    s.val = values;
+    s.rtol = rtol;
+    s.atol = atol;
+    s.maxit = maxit > 0 ? maxit : s.ndof;
+    int64_t status[2] = {0, 0};
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    e = (dim == 2) ? noalloc_launch<2>(scr, grid, s, b, x, st, status) : noalloc_launch<3>(scr, grid, s, b, x, st, status);
+    if (e != cudaSuccess)
+    {
+        set_last_error(std::string("lpmgpu_cg_bsr_noalloc: ") + cudaGetErrorString(e));
+        return LPMGPU_ERR_CUDA;
+    }
+    if (iterations)
+        *iterations = status[0];
+    if (status[1] & 2)
+        return LPMGPU_ERR_TIMEOUT;
+    return LPMGPU_OK;
+}

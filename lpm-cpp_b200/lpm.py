@@ -135,7 +135,7 @@ EXPORTS = [
     "lpmgpu_export_ref_csr", "lpmgpu_solve_linear", "lpmgpu_apply_load_step",
     "lpmgpu_solve_problem_step", "lpmgpu_solve_load_step", "lpmgpu_store_state", "lpmgpu_reset_state",
     "lpmgpu_read_state", "lpmgpu_read_residual", "lpmgpu_set_xyz", "lpmgpu_get_phase_times",
-    "lpmgpu_get_counters", "lpmgpu_get_stream",
+    "lpmgpu_get_counters", "lpmgpu_get_stream", "lpmgpu_cg_bsr_noalloc",
 ]
 
 
@@ -174,6 +174,8 @@ def lib():
         "lpmgpu_get_phase_times": (C.c_int32, [vp, dp]),
         "lpmgpu_get_counters": (C.c_int32, [vp, C.POINTER(Counters)]),
         "lpmgpu_get_stream": (C.c_int32, [vp, C.POINTER(vp)]),
+        "lpmgpu_cg_bsr_noalloc": (C.c_int32, [C.c_int32, C.c_int32, vp, vp, vp, vp, vp, C.c_double, C.c_double,
+                                              C.c_int64, vp, C.POINTER(C.c_int64)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
