@@ -69,6 +69,14 @@ typedef struct
     int64_t cg_maxit;        /* CG cap, 0 = problem size (solver.h:308) */
     int32_t precision;       /* LPMGPU_FP64 or LPMGPU_MIXED */
     int32_t device;          /* CUDA device ordinal */
+    /* Optional inputs (NULL = derive them as the reference's Assembly constructor would).
+     * bond_nb0/bond_nb1/bond_p2: the bond lists (per particle its layer-0 partners then its
+     * layer-1 partners), e.g. from Assembly::readBond (assembly.h:391-424) or with bonds left
+     * out along a pre-crack; every bond needs its opposite.  bond_kn/bond_tv: per-bond
+     * coefficients in the same order (what setParticleProperty stored), overriding E/mu.
+     * bond_damage: initial bond damage in the same order (1 = broken). */
+    const int32_t *bond_nb0, *bond_nb1, *bond_p2;
+    const double *bond_kn, *bond_tv, *bond_damage;
 } lpmgpu_desc;
 
 /* Displacement / force boundary condition of one load step (boundary.h:10-44, Relative mode). */

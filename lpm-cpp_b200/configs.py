@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import math
 from dataclasses import dataclass, field
-from typing import Dict, List, Tuple
+from typing import Callable, Dict, List, Optional, Tuple
 
 import numpy as np
 
@@ -36,6 +36,11 @@ class Case:
     tol_iter: float = 1e-5
     euler: Tuple[int, Tuple[float, float, float]] = (0, (0.0, 0.0, 0.0))
     meta: dict = field(default_factory=dict)
+    # explicit bond lists (nb0, nb1, p2) as Assembly::readBond builds them; None -> bond search
+    bonds: Optional[Tuple[np.ndarray, np.ndarray, np.ndarray]] = None
+    # per-bond (Kn, Tv, bdamage) in bond order, written into the bonds before the first force
+    # update (a heterogeneous material, initial damage); None -> setParticleProperty's values
+    bond_props: Optional[Tuple[np.ndarray, np.ndarray, np.ndarray]] = None
 
     @property
     def n(self):
@@ -58,7 +63,55 @@ class Case:
         a = L.Assembly(self.xyz, self.box, L.UnitCell(self.lattice, self.radius), self.ptype)
         a.type = self.types.copy()
         a.material = self.material
+        a.bonds = self.bonds
+        if self.bond_props is not None:
+            a.bond_kn, a.bond_tv, a.bond_damage = self.bond_props
         return a
+
+
+def bond_lists(xyz: np.ndarray, cell: L.UnitCell,
+               exclude: Optional[Callable[[np.ndarray, np.ndarray], np.ndarray]] = None):
+    """Bond lists of Assembly::createBonds (include/assembly.h:213-234) built on the host, for
+    problems whose bonds are prepared before the solver sees them: a bond i-j for every pair with
+    distance < 1.01*cutoff[1], layer 0 below 1.01*cutoff[0]; per particle the layer-0 partners,
+    then the layer-1 partners, each in ascending id.  ``exclude(i, j)`` (arrays, i < j) marks
+    bonds to leave out, as the reference's geometry tools do for notches and cracks
+    (geometry/geo1_CT_configuration.cpp:79-134); the decision is taken once per pair, so the
+    lists stay symmetric.  Returns (nb0, nb1, p2) in int32."""
+    from scipy.spatial import cKDTree
+
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    n = len(xyz)
+    rc0, rc1 = 1.01 * cell.neighbor_cutoff[0], 1.01 * cell.neighbor_cutoff[1]
+    pairs = cKDTree(xyz).query_pairs(rc1, output_type="ndarray").astype(np.int64)
+    i, j = pairs[:, 0], pairs[:, 1]
+    dv = xyz[i] - xyz[j]
+    d = np.sqrt(dv[:, 0] * dv[:, 0] + dv[:, 1] * dv[:, 1] + dv[:, 2] * dv[:, 2])
+    keep = d < rc1
+    if exclude is not None:
+        keep &= ~np.asarray(exclude(i, j), dtype=bool)
+    i, j, d = i[keep], j[keep], d[keep]
+    layer = np.where(d < rc0, 0, 1)
+    p1, p2, ly = np.concatenate([i, j]), np.concatenate([j, i]), np.concatenate([layer, layer])
+    order = np.lexsort((p2, ly, p1))
+    nb0 = np.bincount(p1[ly == 0], minlength=n).astype(np.int32)
+    nb1 = np.bincount(p1[ly == 1], minlength=n).astype(np.int32)
+    return nb0, nb1, p2[order].astype(np.int32)
+
+
+def slit_exclusion(xyz: np.ndarray, y_slit: float, x_from: float, x_to: float):
+    """exclude(i, j) for a zero-width straight slit on y = y_slit between x_from and x_to: a
+    bond is cut when its segment crosses the slit line inside that span."""
+    xyz = np.asarray(xyz)
+
+    def exclude(i, j):
+        yi, yj = xyz[i, 1] - y_slit, xyz[j, 1] - y_slit
+        cross = yi * yj < 0
+        t = np.where(cross, yi / np.where(cross, yi - yj, 1.0), 0.0)
+        xc = xyz[i, 0] + t * (xyz[j, 0] - xyz[i, 0])
+        return cross & (xc >= x_from) & (xc <= x_to)
+
+    return exclude
 
 
 def _gen(lattice, radius, box, euler=(0, (0.0, 0.0, 0.0))):
@@ -139,10 +192,10 @@ def fcc_bar(size=(4.0, 4.0, 8.0), radius=0.2, E=110e3, mu=0.34, steps=10, strain
 
 def notched_plate(size=4.0, radius=0.1, crack=0.3, E=69e3, mu=0.3, critical_bstrain=2e-3, steps=40,
                   total_disp=None, tol_iter=1e-5, max_iter=30) -> Case:
-    """Config 4 member: single-edge-notched hexagonal plate, brittle bonds.  The pre-crack is a
-    straight slit from the left edge at mid-height, made by leaving out the bonds that cross
-    it (the bond-exclusion pattern of geometry/geo1_CT_configuration.cpp:79-134), realised here
-    by giving the particles on the two faces of the slit broken bonds across it."""
+    """Single-edge-notched hexagonal plate with brittle bonds, pulled in y.  The pre-crack is a
+    straight slit from the left edge, ``crack`` x the width long, between the two particle rows
+    nearest mid-height; the bonds crossing it are left out of the bond lists (the bond-exclusion
+    of geometry/geo1_CT_configuration.cpp:79-134, read back through Assembly::readBond)."""
     box = [0.0, size, 0.0, size, 0.0, 1.0]
     xyz = _gen(L.LatticeType.Hexagon2D, radius, box)
     top = np.nonzero(xyz[:, 1] > box[3] - 2 * radius)[0].astype(np.int32)
@@ -157,5 +210,11 @@ def notched_plate(size=4.0, radius=0.1, crack=0.3, E=69e3, mu=0.3, critical_bstr
     st = [([("bottom", "x", 0.0), ("bottom", "y", 0.0), ("top", "y", dstep)], []) for _ in range(steps)]
     c = Case(f"sen_hex_{size:g}mm", L.LatticeType.Hexagon2D, radius, box, xyz, L.ParticleType.Elastic, mat, types,
              {"top": top, "bottom": bot}, st, tol_iter=tol_iter, max_iter=max_iter)
-    c.meta["crack"] = (crack * size, 0.5 * size)
+    ys = np.unique(np.round(xyz[:, 1], 9))
+    k = int(np.searchsorted(ys, 0.5 * size)) - 1
+    k = min(max(k, 0), len(ys) - 2)
+    y_slit = 0.5 * (ys[k] + ys[k + 1])
+    c.bonds = bond_lists(xyz, L.UnitCell(L.LatticeType.Hexagon2D, radius),
+                         slit_exclusion(xyz, y_slit, box[0] - 1.0, box[0] + crack * size))
+    c.meta["crack"] = (crack * size, y_slit)
     return c

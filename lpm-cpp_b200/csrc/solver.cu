@@ -452,8 +452,6 @@ int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
     auto *h = new lpmgpu_solver();
     Problem &p = h->p;
     p.desc = *d;
-    p.desc.xyz = nullptr;
-    p.desc.type = nullptr;
     p.device = d->device;
     for (auto &e : p.ev)
         e = nullptr;
@@ -508,8 +506,21 @@ int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
     CKF(cudaMemcpyAsync(p.xyz_last, d->xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, p.stream));
     if (d->type)
         CKF(cudaMemcpyAsync(p.type, d->type, sizeof(int) * n, cudaMemcpyHostToDevice, p.stream));
+    if ((d->bond_nb0 || d->bond_nb1 || d->bond_p2) && !(d->bond_nb0 && d->bond_nb1 && d->bond_p2))
+        return fail(LPMGPU_ERR_INVALID_ARG);
+    if ((d->bond_kn || d->bond_tv || d->bond_damage) && !d->bond_p2)
+    {
+        set_last_error("per-bond arrays need the bond lists they refer to (bond_nb0/bond_nb1/bond_p2)");
+        return fail(LPMGPU_ERR_INVALID_ARG);
+    }
     int topo_err = 0;
     CKF(build_topology(p, d->xyz, &topo_err));
+    CKF(cudaStreamSynchronize(p.stream));
+    // the host pointers of the description are only read during creation
+    p.desc.xyz = nullptr;
+    p.desc.type = nullptr;
+    p.desc.bond_nb0 = p.desc.bond_nb1 = p.desc.bond_p2 = nullptr;
+    p.desc.bond_kn = p.desc.bond_tv = p.desc.bond_damage = nullptr;
     if (topo_err)
     {
         set_last_error("a particle has no bonds, or more bonds / connections than supported");

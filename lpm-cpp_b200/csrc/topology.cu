@@ -229,6 +229,20 @@ __global__ void k_bonds_find(int n, const double *__restrict__ xyz, Grid g, cons
     nb0[i] = c0;
 }
 
+// distances of caller-supplied bonds (Assembly::readBond computes them the same way, assembly.h:416)
+__global__ void k_bonds_dist(int n, const double *__restrict__ xyz, const int *__restrict__ pad_id,
+                             const int *__restrict__ nb, double *__restrict__ pad_d)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    for (int q = 0; q < nb[i]; ++q)
+    {
+        const int j = pad_id[(int64_t)i * kMaxBonds + q];
+        pad_d[(int64_t)i * kMaxBonds + q] = pdist(xyz + 3 * i, xyz + 3 * j);
+    }
+}
+
 // Bond(p1,p2,layer,dis) (bond.h:59-72) and setParticleProperty's Kn/Tv assignment
 // (particle_elastic.h:92-107): hexagonal lattices use Kn = KnTv[0], Tv = KnTv[1] for both layers
 __global__ void k_bonds_fill(int n, const double *__restrict__ xyz, const int *__restrict__ pad_id,
@@ -516,6 +530,7 @@ cudaError_t build_topology(Problem &p, const double *xyz_host, int *err_code)
 {
     const int n = p.n;
     *err_code = 0;
+    const bool user_bonds = p.desc.bond_nb0 && p.desc.bond_nb1 && p.desc.bond_p2;
     // grid of cells no smaller than the largest search radius
     const double rc0 = 1.01 * p.cell.cutoff[0], rc1 = 1.01 * p.cell.cutoff[1];
     Grid g;
@@ -583,8 +598,41 @@ cudaError_t build_topology(Problem &p, const double *xyz_host, int *err_code)
     LPM_TRY(dalloc(p, &p.nb, n));
     LPM_TRY(dalloc(p, &p.nb0, n));
     LPM_TRY(dalloc(p, &p.bstart, (size_t)n + 1));
-    k_bonds_find<<<div_up(n, 128), 128, 0, p.stream>>>(n, p.xyz, g, sid, cbeg, cend, rc0, rc1, pad_id, pad_d, p.nb,
-                                                       p.nb0, p.scal);
+    if (user_bonds)
+    {
+        // caller-supplied lists (bond file / pre-crack): padded copy, distances computed here
+        std::vector<int> hnb(n), hnb0(n), hpad((size_t)n * kMaxBonds, 0);
+        size_t o = 0;
+        for (int i = 0; i < n; ++i)
+        {
+            const int a0 = p.desc.bond_nb0[i], a1 = p.desc.bond_nb1[i];
+            if (a0 < 0 || a1 < 0 || a0 + a1 > kMaxBonds)
+            {
+                *err_code = LPMGPU_ERR_TOPOLOGY;
+                return cudaSuccess;
+            }
+            hnb0[i] = a0;
+            hnb[i] = a0 + a1;
+            for (int q = 0; q < a0 + a1; ++q)
+            {
+                const int j = p.desc.bond_p2[o++];
+                if (j < 0 || j >= n || j == i)
+                {
+                    *err_code = LPMGPU_ERR_TOPOLOGY;
+                    return cudaSuccess;
+                }
+                hpad[(size_t)i * kMaxBonds + q] = j;
+            }
+        }
+        LPM_TRY(cudaMemcpyAsync(p.nb, hnb.data(), sizeof(int) * n, cudaMemcpyHostToDevice, p.stream));
+        LPM_TRY(cudaMemcpyAsync(p.nb0, hnb0.data(), sizeof(int) * n, cudaMemcpyHostToDevice, p.stream));
+        LPM_TRY(cudaMemcpyAsync(pad_id, hpad.data(), sizeof(int) * hpad.size(), cudaMemcpyHostToDevice, p.stream));
+        k_bonds_dist<<<div_up(n, 128), 128, 0, p.stream>>>(n, p.xyz, pad_id, p.nb, pad_d);
+        LPM_TRY(cudaStreamSynchronize(p.stream)); // the host vectors above must outlive the copies
+    }
+    else
+        k_bonds_find<<<div_up(n, 128), 128, 0, p.stream>>>(n, p.xyz, g, sid, cbeg, cend, rc0, rc1, pad_id, pad_d,
+                                                           p.nb, p.nb0, p.scal);
     LPM_TRY(cudaGetLastError());
     // bstart = exclusive scan of nb (n+1 entries: the appended zero yields the total)
     int *nbx = nullptr;
@@ -624,6 +672,16 @@ cudaError_t build_topology(Problem &p, const double *xyz_host, int *err_code)
                                                    p.kntv[2], p.bp2, p.dis0, p.dis, p.dis_last, p.cs, p.Kn, p.Tv);
     k_bonds_rev<<<div_up(n, T), T, 0, p.stream>>>(n, p.bstart, p.nb0, p.bp2, p.brev, p.scal);
     LPM_TRY(cudaGetLastError());
+    if (p.desc.bond_kn)
+        LPM_TRY(cudaMemcpyAsync(p.Kn, p.desc.bond_kn, sizeof(double) * nb, cudaMemcpyHostToDevice, p.stream));
+    if (p.desc.bond_tv)
+        LPM_TRY(cudaMemcpyAsync(p.Tv, p.desc.bond_tv, sizeof(double) * nb, cudaMemcpyHostToDevice, p.stream));
+    if (p.desc.bond_damage)
+    {
+        LPM_TRY(cudaMemcpyAsync(p.bdamage, p.desc.bond_damage, sizeof(double) * nb, cudaMemcpyHostToDevice, p.stream));
+        LPM_TRY(cudaMemcpyAsync(p.bdamage_last, p.desc.bond_damage, sizeof(double) * nb, cudaMemcpyHostToDevice,
+                                p.stream));
+    }
     cudaFreeAsync(pad_id, p.stream);
     cudaFreeAsync(pad_d, p.stream);
     cudaFreeAsync(key, p.stream);

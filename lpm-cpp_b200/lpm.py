@@ -84,6 +84,9 @@ class Desc(C.Structure):
         ("nonlocal_L", C.c_double), ("undamaged_type", C.c_int32), ("max_iter", C.c_int32),
         ("tol_iter", C.c_double), ("cg_rtol", C.c_double), ("cg_atol", C.c_double),
         ("cg_maxit", C.c_int64), ("precision", C.c_int32), ("device", C.c_int32),
+        ("bond_nb0", C.POINTER(C.c_int32)), ("bond_nb1", C.POINTER(C.c_int32)), ("bond_p2", C.POINTER(C.c_int32)),
+        ("bond_kn", C.POINTER(C.c_double)), ("bond_tv", C.POINTER(C.c_double)),
+        ("bond_damage", C.POINTER(C.c_double)),
     ]
 
 
@@ -274,6 +277,22 @@ class Material:
     nonlocal_L: float = 0.0
 
 
+def _read_dump(path: str):
+    """LAMMPS-style dump as Assembly::readDump reads it (include/assembly.h:338-388): three
+    header lines, the particle count, one line, three box lines, one line, then
+    "id type x y z" records."""
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"'{path}' does not exist!")
+    with open(path) as f:
+        lines = f.read().splitlines()
+    n = int(lines[3].split()[0])
+    box = [float(v) for k in (5, 6, 7) for v in lines[k].split()[:2]]
+    rec = np.array([ln.split()[:5] for ln in lines[9:9 + n] if ln.strip()], dtype=np.float64).reshape(-1, 5)
+    if len(rec) != n or not np.array_equal(rec[:, 0], np.arange(n)):
+        raise ValueError(f"{path}: expected {n} particles with ids 0..{n - 1} in file order")
+    return box, rec[:, 1].astype(np.int32), np.ascontiguousarray(rec[:, 2:5])
+
+
 class Assembly:
     """Particle system built from coordinates (include/assembly.h:98-106).  The bonds and
     connections are built on the device when the solver is constructed."""
@@ -286,6 +305,51 @@ class Assembly:
         self.nparticle = len(self.xyz)
         self.type = np.zeros(self.nparticle, dtype=np.int32)
         self.material = Material()
+        # optional explicit bonds (Assembly(dumpFile, bondFile) / pre-cracks), per-bond
+        # coefficients and initial bond damage, all in (particle, layer-0 then layer-1) order
+        self.bonds = None          # (nb0[n], nb1[n], p2[nbonds])
+        self.bond_kn = self.bond_tv = self.bond_damage = None
+
+    @classmethod
+    def fromDump(cls, dumpFile: str, cell: UnitCell, ptype: ParticleType = ParticleType.Elastic,
+                 bondFile: str = None) -> "Assembly":
+        """Assembly(dumpFile, cell, ptype) and Assembly(dumpFile, bondFile, cell, ptype)
+        (include/assembly.h:74-95): ids, types and coordinates from a LAMMPS-style dump
+        (readDump, assembly.h:338-388); bonds from the bond file (readBond) or, without one, from
+        the device's bond search (createBonds).  Particle ids must run 0..n-1 in file order."""
+        box, types, xyz = _read_dump(dumpFile)
+        a = cls(xyz, box, cell, ptype)
+        a.type = types
+        if bondFile is not None:
+            a.readBond(bondFile)
+        return a
+
+    def readBond(self, bondFile: str):
+        """Assembly::readBond (include/assembly.h:391-424): one "id layer p1 p2" line per bond;
+        each bond joins p1's list of its layer in file order."""
+        if not os.path.exists(bondFile):
+            raise FileNotFoundError(f"'{bondFile}' does not exist!")
+        rows = np.loadtxt(bondFile, dtype=np.int64, ndmin=2).reshape(-1, 4)
+        layer, p1, p2 = rows[:, 1], rows[:, 2], rows[:, 3]
+        n = self.nparticle
+        if rows.size and (layer.min() < 0 or layer.max() > 1 or p1.min() < 0 or p1.max() >= n
+                          or p2.min() < 0 or p2.max() >= n):
+            raise ValueError(f"{bondFile}: layer outside 0..1 or particle id outside 0..{n - 1}")
+        order = np.lexsort((layer, p1))  # stable: file order inside each (p1, layer) list
+        nb0 = np.bincount(p1[layer == 0], minlength=n).astype(np.int32)
+        nb1 = np.bincount(p1[layer == 1], minlength=n).astype(np.int32)
+        self.bonds = (nb0, nb1, p2[order].astype(np.int32))
+
+    def writeBond(self, bondFile: str):
+        """Assembly::writeBond (include/assembly.h:269-283) for explicit bond lists."""
+        if self.bonds is None:
+            raise ValueError("writeBond needs explicit bond lists (readBond or Assembly.bonds)")
+        nb0, nb1, p2 = (np.asarray(a, dtype=np.int64) for a in self.bonds)
+        nb = nb0 + nb1
+        start = np.concatenate([[0], np.cumsum(nb)[:-1]]).astype(np.int64)
+        layer = (np.arange(len(p2)) - np.repeat(start, nb) >= np.repeat(nb0, nb)).astype(np.int64)
+        rows = np.stack([np.arange(len(p2)), layer, np.repeat(np.arange(len(nb)), nb), p2], axis=1)
+        np.savetxt(bondFile, rows, fmt="%d")
 
     def setParticleProperty(self, nonlocal_L, is_plane_stress, E, mu, *rest):
         """Elastic: (nonlocal_L, is_plane_stress, E, mu, critical_bstrain);
@@ -385,6 +449,17 @@ class GpuProblem:
         d.undamaged_type, d.max_iter, d.tol_iter = int(undamaged_pt_type), int(max_iter), float(tol_iter)
         d.cg_rtol, d.cg_atol, d.cg_maxit = float(cg_rtol), float(cg_atol), int(cg_maxit)
         d.precision, d.device = int(precision), int(device)
+        self._keep = []
+        if ass.bonds is not None:
+            nb0, nb1, p2 = (np.ascontiguousarray(a, dtype=np.int32) for a in ass.bonds)
+            self._keep += [nb0, nb1, p2]
+            d.bond_nb0, d.bond_nb1, d.bond_p2 = _ip(nb0), _ip(nb1), _ip(p2)
+        for name in ("bond_kn", "bond_tv", "bond_damage"):
+            arr = getattr(ass, name)
+            if arr is not None:
+                a = np.ascontiguousarray(arr, dtype=np.float64)
+                self._keep.append(a)
+                setattr(d, name, _dp(a))
         h = C.c_void_p()
         _check(L.lpmgpu_create(C.byref(d), C.byref(h)), "lpmgpu_create")
         self._h = h

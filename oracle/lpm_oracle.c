@@ -463,6 +463,38 @@ static int build_bonds(lpmo_problem *p)
     return 0;
 }
 
+/* Assembly::readBond (assembly.h:391-424): the caller's lists in their own order, each bond
+ * with dis = Particle::distanceTo (particle.h) and the layer it is listed under */
+static void build_bonds_user(lpmo_problem *p, const lpmo_desc *d)
+{
+    const int n = p->n;
+    long tot = 0;
+    for (int i = 0; i < n; ++i)
+        tot += d->bond_nb0[i] + d->bond_nb1[i];
+    p->bstart = (int *)malloc(sizeof(int) * (n + 1));
+    p->nb = (int *)malloc(sizeof(int) * n);
+    p->nb0 = (int *)malloc(sizeof(int) * n);
+    p->bp2 = (int *)malloc(sizeof(int) * (tot + 1));
+    p->blayer = (int *)malloc(sizeof(int) * (tot + 1));
+    p->dis0 = (double *)malloc(sizeof(double) * (tot + 1));
+    long b = 0;
+    for (int i = 0; i < n; ++i)
+    {
+        p->bstart[i] = (int)b;
+        p->nb0[i] = d->bond_nb0[i];
+        p->nb[i] = d->bond_nb0[i] + d->bond_nb1[i];
+        for (int q = 0; q < p->nb[i]; ++q, ++b)
+        {
+            const int j = d->bond_p2[b];
+            p->bp2[b] = j;
+            p->blayer[b] = (q < d->bond_nb0[i]) ? 0 : 1;
+            p->dis0[b] = dist(p->xyz0 + 3 * i, p->xyz0 + 3 * j);
+        }
+    }
+    p->bstart[n] = (int)b;
+    p->nbonds = b;
+}
+
 #define B0(p, i) ((p)->bstart[i])
 #define B1(p, i) ((p)->bstart[i] + (p)->nb0[i])
 #define BE(p, i) ((p)->bstart[(i) + 1])
@@ -602,7 +634,10 @@ lpmo_problem *lpmo_create(const lpmo_desc *d)
     if (d->type)
         memcpy(p->type, d->type, sizeof(int) * n);
 
-    build_bonds(p);
+    if (d->bond_nb0 && d->bond_nb1 && d->bond_p2)
+        build_bonds_user(p, d);
+    else
+        build_bonds(p);
     build_conns(p);
     build_rev(p);
     const long nb = p->nbonds;
@@ -1586,4 +1621,22 @@ void lpmo_read_state(const lpmo_problem *p, double *xyz, double *pin, double *st
 void lpmo_set_xyz(lpmo_problem *p, const double *xyz)
 {
     memcpy(p->xyz, xyz, sizeof(double) * 3 * p->n);
+}
+
+void lpmo_get_bond_kntv(const lpmo_problem *p, double *kn, double *tv)
+{
+    memcpy(kn, p->Kn, sizeof(double) * p->nbonds);
+    memcpy(tv, p->Tv, sizeof(double) * p->nbonds);
+}
+
+void lpmo_set_bond_kntv(lpmo_problem *p, const double *kn, const double *tv)
+{
+    memcpy(p->Kn, kn, sizeof(double) * p->nbonds);
+    memcpy(p->Tv, tv, sizeof(double) * p->nbonds);
+}
+
+void lpmo_set_bond_damage(lpmo_problem *p, const double *bdamage)
+{
+    memcpy(p->bdamage, bdamage, sizeof(double) * p->nbonds);
+    memcpy(p->bdamage_last, bdamage, sizeof(double) * p->nbonds);
 }

@@ -34,6 +34,10 @@ typedef struct
     double tol_iter;
     double cg_rtol, cg_atol;   /* squared-norm tolerances of the RCI CG (solver.h:312-313) */
     long long cg_maxit;        /* 0 -> problem size (solver.h:308) */
+    /* optional bond lists in place of the search: per particle nb0[i] layer-0 partners then
+     * nb1[i] layer-1 partners, concatenated in p2 (Assembly(dumpFile, bondFile, ...) and
+     * Assembly::readBond, assembly.h:84-95, 391-424); NULL -> Assembly::createBonds */
+    const int *bond_nb0, *bond_nb1, *bond_p2;
 } lpmo_desc;
 
 typedef struct
@@ -114,6 +118,13 @@ void lpmo_read_state(const lpmo_problem *p, double *xyz, double *pin, double *st
 int lpmo_nstate_var(const lpmo_problem *p);
 void lpmo_read_residual(const lpmo_problem *p, double *res);
 void lpmo_set_xyz(lpmo_problem *p, const double *xyz);
+/* per-bond coefficients and damage, in bond order (owner, layer 0 then layer 1).  An LPM-CPP
+ * example sets them by writing Bond::Kn / Tv / bdamage (bond.h:25-27) after setParticleProperty
+ * and before the first updateForceState: a heterogeneous material or a pre-crack.  Setting the
+ * damage also sets bdamage_last, so resetStateVar(true) (particle.h:141) restores it. */
+void lpmo_get_bond_kntv(const lpmo_problem *p, double *kn, double *tv);
+void lpmo_set_bond_kntv(lpmo_problem *p, const double *kn, const double *tv);
+void lpmo_set_bond_damage(lpmo_problem *p, const double *bdamage);
 
 #ifdef __cplusplus
 }

@@ -16,6 +16,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblpm_oracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "lpm_ref")
+# the same driver built with SolverStaticGPU (lpm-cpp_b200/cpp/solver_static_gpu.h) in place of
+# SolverStatic: the reference's Assembly and LoadStep code calling the device library
+REF_GPU_BIN = os.path.join(HERE, "_ref", "lpm_ref_gpu")
 
 LATTICES = {"sq2d": 0, "hex2d": 1, "sc3d": 2, "fcc3d": 3, "bcc3d": 4}
 PTYPES = {"elastic": 0, "j2": 2}
@@ -31,6 +34,7 @@ class _Desc(C.Structure):
         ("nonlocal_L", C.c_double), ("nonlocal_cutoff_ratio", C.c_double),
         ("undamaged_type", C.c_int), ("max_iter", C.c_int), ("tol_iter", C.c_double),
         ("cg_rtol", C.c_double), ("cg_atol", C.c_double), ("cg_maxit", C.c_longlong),
+        ("bond_nb0", C.POINTER(C.c_int)), ("bond_nb1", C.POINTER(C.c_int)), ("bond_p2", C.POINTER(C.c_int)),
     ]
 
 
@@ -95,6 +99,9 @@ def lib():
         L.lpmo_read_state.argtypes = [C.c_void_p, dp, dp, dp, dp, dp, dp, dp]
         L.lpmo_read_residual.argtypes = [C.c_void_p, dp]
         L.lpmo_set_xyz.argtypes = [C.c_void_p, dp]
+        L.lpmo_get_bond_kntv.argtypes = [C.c_void_p, dp, dp]
+        L.lpmo_set_bond_kntv.argtypes = [C.c_void_p, dp, dp]
+        L.lpmo_set_bond_damage.argtypes = [C.c_void_p, dp]
         _lib = L
     return _lib
 
@@ -167,7 +174,9 @@ class OracleProblem:
 
     def __init__(self, lattice: str, radius: float, xyz: np.ndarray, mat: Material, types=None,
                  undamaged_type=-1, max_iter=30, tol_iter=1e-5, cg_rtol=1e-12, cg_atol=1e-12, cg_maxit=0,
-                 nonlocal_cutoff_ratio=0.0):
+                 nonlocal_cutoff_ratio=0.0, bonds=None):
+        """bonds: optional (nb0, nb1, p2) lists as Assembly::readBond builds them; None runs the
+        reference's bond search."""
         self.xyz0 = np.ascontiguousarray(xyz, dtype=np.float64)
         self.n = len(self.xyz0)
         self.types = np.ascontiguousarray(types if types is not None else np.zeros(self.n), dtype=np.int32)
@@ -180,6 +189,9 @@ class OracleProblem:
         d.nonlocal_L, d.nonlocal_cutoff_ratio = mat.nonlocal_L, nonlocal_cutoff_ratio
         d.undamaged_type, d.max_iter, d.tol_iter = undamaged_type, max_iter, tol_iter
         d.cg_rtol, d.cg_atol, d.cg_maxit = cg_rtol, cg_atol, cg_maxit
+        if bonds is not None:
+            self._bonds = [np.ascontiguousarray(a, dtype=np.int32) for a in bonds]
+            d.bond_nb0, d.bond_nb1, d.bond_p2 = (_ip(a) for a in self._bonds)
         self._h = lib().lpmo_create(C.byref(d))
         self.dim = lib().lpmo_dim(self._h)
         self.nsv = lib().lpmo_nstate_var(self._h)
@@ -257,6 +269,20 @@ class OracleProblem:
         a = np.ascontiguousarray(xyz, dtype=np.float64)
         lib().lpmo_set_xyz(self._h, _dp(a))
 
+    def bond_kntv(self):
+        nb = lib().lpmo_nbonds(self._h)
+        kn, tv = np.zeros(nb), np.zeros(nb)
+        lib().lpmo_get_bond_kntv(self._h, _dp(kn), _dp(tv))
+        return kn, tv
+
+    def set_bond_kntv(self, kn, tv):
+        a, b = (np.ascontiguousarray(v, dtype=np.float64) for v in (kn, tv))
+        lib().lpmo_set_bond_kntv(self._h, _dp(a), _dp(b))
+
+    def set_bond_damage(self, bdamage):
+        a = np.ascontiguousarray(bdamage, dtype=np.float64)
+        lib().lpmo_set_bond_damage(self._h, _dp(a))
+
     def state(self):
         L = lib()
         n = self.n
@@ -273,16 +299,16 @@ def ref_available() -> bool:
     return os.path.exists(REF_BIN)
 
 
-def run_ref(spec_text: str, outdir: str, threads: int = 1, timeout: float = 600.0) -> str:
+def run_ref(spec_text: str, outdir: str, threads: int = 1, timeout: float = 600.0, binary: str = REF_BIN) -> str:
     """Runs the reference's own build on a spec (see oracle/ref_driver.cpp); returns stdout."""
     os.makedirs(outdir, exist_ok=True)
     path = os.path.join(outdir, "spec.txt")
     with open(path, "w") as f:
         f.write(spec_text + f"\nout {outdir}\n")
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
-    r = subprocess.run([REF_BIN, path], env=env, capture_output=True, text=True, timeout=timeout)
+    r = subprocess.run([binary, path], env=env, capture_output=True, text=True, timeout=timeout)
     if r.returncode != 0:
-        raise RuntimeError(f"lpm_ref failed ({r.returncode}): {r.stderr[-2000:]}")
+        raise RuntimeError(f"{os.path.basename(binary)} failed ({r.returncode}): {r.stderr[-2000:]}")
     return r.stdout
 
 
@@ -301,6 +327,18 @@ def read_ref_steps(outdir: str):
 
 def read_bin(outdir: str, name: str, dtype) -> np.ndarray:
     return np.fromfile(os.path.join(outdir, name), dtype=dtype)
+
+
+def write_bond_file(path: str, nb0, nb1, p2):
+    """Bond lists in the reference's text format, one "id layer p1 p2" line per bond in
+    (particle, layer-0 then layer-1) order, as Assembly::writeBond prints them (assembly.h:269-283)."""
+    nb0, nb1, p2 = (np.asarray(a, dtype=np.int64) for a in (nb0, nb1, p2))
+    nb = nb0 + nb1
+    p1 = np.repeat(np.arange(len(nb)), nb)
+    start = np.concatenate([[0], np.cumsum(nb)[:-1]])
+    layer = (np.arange(len(p2)) - np.repeat(start, nb) >= np.repeat(nb0, nb)).astype(np.int64)
+    rows = np.stack([np.arange(len(p2)), layer, p1, p2], axis=1)
+    np.savetxt(path, rows, fmt="%d")
 
 
 def write_ref_spec(case, outdir: str, steps=None, max_iter=None, tol_iter=None, cg_tol=None, cg_maxit_cap=0,
@@ -328,6 +366,14 @@ def write_ref_spec(case, outdir: str, steps=None, max_iter=None, tol_iter=None, 
         p = os.path.join(outdir, "xyz_in.f64")
         np.ascontiguousarray(case.xyz, dtype=np.float64).tofile(p)
         lines.append(f"xyz_file {p}")
+    if getattr(case, "bonds", None) is not None:
+        p = os.path.join(outdir, "bonds_in.txt")
+        write_bond_file(p, *case.bonds)
+        lines.append(f"bondfile {p}")
+    if getattr(case, "bond_props", None) is not None:
+        p = os.path.join(outdir, "bondprops_in.f64")
+        np.concatenate([np.asarray(a, dtype=np.float64) for a in case.bond_props]).tofile(p)
+        lines.append(f"bondprops {p}")
     p = os.path.join(outdir, "types_in.i32")
     np.ascontiguousarray(case.types, dtype=np.int32).tofile(p)
     lines.append(f"typefile {p}")

@@ -31,6 +31,13 @@
  *   groupfile NAME PATH   (group from raw int32 particle ids)   typefile PATH (raw int32 types)
  *   cg_tol RTOL ATOL      (overrides the squared-norm tolerances the reference sets at
  *                          solver.h:312-313; applied inside the MKL stand-in, test use only)
+ *   bondfile PATH         (bond list in the reference's text format "id layer p1 p2": the
+ *                          Assembly is then built by Assembly(dumpFile, bondFile, cell, ptype),
+ *                          include/assembly.h:84-95, from a dump of the coordinates written
+ *                          at full precision; pre-cracks by bond exclusion)
+ *   bondprops PATH        (raw f64: Kn[nb], Tv[nb], bdamage[nb] in bond order, written into
+ *                          Bond::Kn / Tv / bdamage and bdamage_last (include/bond.h:25-27) after
+ *                          setParticleProperty: a heterogeneous material or initial damage)
  */
 #include <cstdio>
 #include <cstdlib>
@@ -49,6 +56,13 @@
 #include "stiffness.h"
 #include "load_step.h"
 #include "solver_static.h"
+#ifdef LPM_USE_GPU
+/* the one-line switch of an example's run(): SolverStatic -> SolverStaticGPU (lpm-cpp_b200/cpp) */
+#include "solver_static_gpu.h"
+#define LPM_SOLVER SolverStaticGPU
+#else
+#define LPM_SOLVER SolverStatic
+#endif
 
 static const int NL = 2;
 
@@ -108,6 +122,8 @@ struct Spec
     std::string xyz_file;
     std::vector<std::pair<std::string, std::string>> groupfiles;
     std::string typefile;
+    std::string bondfile;
+    std::string bondprops;
     double cg_rtol = -1, cg_atol = -1;
 };
 
@@ -221,6 +237,8 @@ static Spec parse(const char *path)
         }
         else if (k == "typefile") is >> s.typefile;
         else if (k == "cg_tol") is >> s.cg_rtol >> s.cg_atol;
+        else if (k == "bondfile") is >> s.bondfile;
+        else if (k == "bondprops") is >> s.bondprops;
         else
         {
             std::fprintf(stderr, "unknown spec directive '%s'\n", k.c_str());
@@ -258,6 +276,31 @@ static LatticeType lattice_of(const std::string &s)
     if (s == "bcc3d") return LatticeType::BCC3D_1Slip;
     std::fprintf(stderr, "unknown lattice %s\n", s.c_str());
     std::exit(2);
+}
+
+/* Assembly(xyz, box, cell, ptype) (assembly.h:98-106), or with a bond file the reference's
+ * file constructor: readDump (assembly.h:338-388) of a dump holding the same coordinates, then
+ * readBond (assembly.h:391-424). */
+static Assembly<NL> make_assembly(std::vector<std::array<double, NDIM>> &xyz, std::array<double, 2 * NDIM> &box,
+                                  UnitCell &cell, ParticleType pt, const Spec &sp)
+{
+    if (sp.bondfile.empty())
+        return Assembly<NL>{xyz, box, cell, pt};
+    const std::string dump = sp.out + "/assembly_in.dump";
+    FILE *f = std::fopen(dump.c_str(), "w");
+    if (!f)
+    {
+        std::fprintf(stderr, "cannot write %s\n", dump.c_str());
+        std::exit(3);
+    }
+    std::fprintf(f, "ITEM: TIMESTEP\n0\nITEM: NUMBER OF ATOMS\n%zu\nITEM: BOX BOUNDS pp pp pp\n", xyz.size());
+    for (int k = 0; k < 3; ++k)
+        std::fprintf(f, "%.17g %.17g\n", box[2 * k], box[2 * k + 1]);
+    std::fprintf(f, "ITEM: ATOMS id type x y z\n");
+    for (size_t i = 0; i < xyz.size(); ++i)
+        std::fprintf(f, "%zu 0 %.17g %.17g %.17g\n", i, xyz[i][0], xyz[i][1], xyz[i][2]);
+    std::fclose(f);
+    return Assembly<NL>{dump, sp.bondfile, cell, pt};
 }
 
 int main(int argc, char **argv)
@@ -301,7 +344,7 @@ int main(int argc, char **argv)
     }
 
     ParticleType pt = (sp.ptype == "j2") ? ParticleType::J2Plasticity : ParticleType::Elastic;
-    Assembly<NL> ass{xyz, box, cell, pt};
+    Assembly<NL> ass = make_assembly(xyz, box, cell, pt, sp);
     const int N = ass.nparticle;
     const int dim = cell.dim;
 
@@ -346,6 +389,40 @@ int main(int argc, char **argv)
                                                                         sp.mu, sp.critical_bstrain);
     }
 
+    if (!sp.bondprops.empty())
+    {
+        std::vector<double> v;
+        FILE *f = std::fopen(sp.bondprops.c_str(), "rb");
+        if (!f)
+        {
+            std::fprintf(stderr, "cannot open %s\n", sp.bondprops.c_str());
+            return 2;
+        }
+        double x;
+        while (std::fread(&x, sizeof(double), 1, f) == 1)
+            v.push_back(x);
+        std::fclose(f);
+        size_t nb = 0;
+        for (Particle<NL> *p : ass.pt_sys)
+            for (int l = 0; l < NL; ++l)
+                nb += p->bond_layers[l].size();
+        if (v.size() != 3 * nb)
+        {
+            std::fprintf(stderr, "bondprops holds %zu values, expected 3 x %zu bonds\n", v.size(), nb);
+            return 2;
+        }
+        size_t k = 0;
+        for (Particle<NL> *p : ass.pt_sys)
+            for (int l = 0; l < NL; ++l)
+                for (Bond<NL> *b : p->bond_layers[l])
+                {
+                    b->Kn = v[k];
+                    b->Tv = v[nb + k];
+                    b->bdamage = b->bdamage_last = v[2 * nb + k];
+                    ++k;
+                }
+    }
+
     std::vector<LoadStep<NL>> load;
     for (int s = 0; s < sp.steps; ++s)
     {
@@ -366,8 +443,12 @@ int main(int argc, char **argv)
     if (sp.init_state_var)
         ass.updateStateVar();
 
-    SolverStatic<NL> solv{sp.undamaged_type, ass, StiffnessMode::Analytical, SolverMode::CG, "/dev/null",
-                          sp.max_iter, sp.tol_iter};
+    LPM_SOLVER<NL> solv{sp.undamaged_type, ass, StiffnessMode::Analytical, SolverMode::CG, "/dev/null",
+                        sp.max_iter, sp.tol_iter};
+#ifdef LPM_USE_GPU
+    if (sp.cg_rtol >= 0 || sp.cg_atol >= 0)
+        solv.setCGTolerance(sp.cg_rtol >= 0 ? sp.cg_rtol : 1e-12, sp.cg_atol >= 0 ? sp.cg_atol : 1e-12);
+#endif
     const double t_setup1 = wall();
 
     /* setup outputs: coordinates, bonds (per particle: layer-0 list then layer-1 list), conns */
@@ -417,6 +498,9 @@ int main(int argc, char **argv)
     for (int s = 0; s < sp.steps; ++s)
     {
         lpm_shim_stats st0 = lpm_shim_stats_g;
+#ifdef LPM_USE_GPU
+        const long long gpu_newton0 = solv.totals.newton_solves, gpu_cg0 = solv.totals.cg_iters;
+#endif
         double t0 = wall();
         int cuts = 0;
         if (sp.loop == "once")
@@ -442,7 +526,11 @@ int main(int argc, char **argv)
                 bool ok = solv.solveProblemStep(one[i], dt);
                 if (!ok)
                 {
+#ifdef LPM_USE_GPU
+                    lpmgpu_reset_state(solv.handle());
+#else
                     solv.ass.resetStateVar(true);
+#endif
                     one[i].loadCutHalf();
                     one.insert(one.begin() + i, one[i]);
                     ++n_step;
@@ -459,6 +547,11 @@ int main(int argc, char **argv)
         }
         double t1 = wall();
         lpm_shim_stats st1 = lpm_shim_stats_g;
+#ifdef LPM_USE_GPU
+        /* the device solver counts its own linear solves and CG iterations */
+        st1.cg_solves = st0.cg_solves + (solv.totals.newton_solves - gpu_newton0);
+        st1.cg_iterations = st0.cg_iterations + (solv.totals.cg_iters - gpu_cg0);
+#endif
         double rn = cblas_dnrm2((MKL_INT)solv.reaction_force.size(), solv.reaction_force.data(), 1);
         std::fprintf(log, "%d %lld %lld %.6f %.6f %.6f %.6f %d %.17g %lld\n", s, st1.cg_solves - st0.cg_solves,
                      st1.cg_iterations - st0.cg_iterations, t1 - t0, st1.spmv_seconds - st0.spmv_seconds,

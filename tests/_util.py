@@ -22,10 +22,36 @@ def oracle_problem(case, cg_rtol=1e-12, cg_atol=1e-12, tol_iter=None, max_iter=N
     mat = O.Material(ptype="j2" if int(case.ptype) == 2 else "elastic", plane_stress=m.plane_stress, E=m.E, mu=m.mu,
                      critical_bstrain=m.critical_bstrain, sigmay=m.sigmay, xi=m.xi, H=m.H, A=m.A,
                      nonlocal_L=m.nonlocal_L)
-    return O.OracleProblem(LAT_NAME[int(case.lattice)], case.radius, case.xyz, mat, types=case.types,
-                           undamaged_type=case.undamaged_type,
-                           max_iter=case.max_iter if max_iter is None else max_iter,
-                           tol_iter=case.tol_iter if tol_iter is None else tol_iter, cg_rtol=cg_rtol, cg_atol=cg_atol)
+    o = O.OracleProblem(LAT_NAME[int(case.lattice)], case.radius, case.xyz, mat, types=case.types,
+                        undamaged_type=case.undamaged_type,
+                        max_iter=case.max_iter if max_iter is None else max_iter,
+                        tol_iter=case.tol_iter if tol_iter is None else tol_iter, cg_rtol=cg_rtol, cg_atol=cg_atol,
+                        bonds=getattr(case, "bonds", None))
+    if getattr(case, "bond_props", None) is not None:
+        kn, tv, dmg = case.bond_props
+        o.set_bond_kntv(kn, tv)
+        o.set_bond_damage(dmg)
+    return o
+
+
+def hetero_plate(size=2.4, steps=3, total_disp=0.003, seed=3):
+    """Hexagonal plate whose bonds carry their own Kn/Tv, drawn in [0.6, 1.4] x the values
+    setParticleProperty gives (one factor per particle pair), with 3% of the pairs broken before
+    loading: the per-bond properties an LPM-CPP example writes into its bonds (bond.h:25-27)."""
+    case = CFG.hex_plate(size=size, radius=0.1, steps=steps, total_disp=total_disp, tol_iter=1e-9)
+    o = oracle_problem(case)
+    nb0, nb1, p2 = o.bonds()
+    owner = np.repeat(np.arange(case.n), nb0 + nb1)
+    key = np.minimum(owner, p2).astype(np.int64) * case.n + np.maximum(owner, p2)
+    uniq, inv = np.unique(key, return_inverse=True)
+    rng = np.random.default_rng(seed)
+    factor = rng.uniform(0.6, 1.4, len(uniq))[inv]
+    broken = (rng.random(len(uniq)) < 0.03)[inv].astype(np.float64)
+    kn, tv = o.bond_kntv()
+    case.bonds = (nb0, nb1, p2)  # per-bond arrays are sized and ordered by explicit lists
+    case.bond_props = (kn * factor, tv * factor, broken)
+    case.name = "hex_hetero"
+    return case
 
 
 def gpu_problem(case, precision=0, cg_rtol=1e-12, cg_atol=1e-12, tol_iter=None, max_iter=None):

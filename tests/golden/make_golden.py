@@ -28,6 +28,9 @@ sys.path.insert(0, ROOT)
 
 from oracle import oracle as O  # noqa: E402
 
+sys.path.insert(0, os.path.dirname(HERE))
+from _util import hetero_plate  # noqa: E402
+
 CFG = importlib.import_module("lpm-cpp_b200.configs")
 LPM = importlib.import_module("lpm-cpp_b200.lpm")
 
@@ -68,6 +71,11 @@ def cases():
                                       ptype=LPM.ParticleType.J2Plasticity, j2=(200.0, 0.0, 38714.0, 10.0)), {}),
         "hex_damage": (lambda: CFG.hex_plate(size=2.0, radius=0.1, steps=3, total_disp=0.024, critical_bstrain=3e-3,
                                              tol_iter=1e-9), {"cg_tol": (1e-24, 0.0)}),
+        # pre-crack by bond exclusion, built by the reference through readDump + readBond
+        "hex_crack": (lambda: CFG.notched_plate(size=2.0, radius=0.1, crack=0.3, steps=8, total_disp=0.008,
+                                                tol_iter=1e-9), {"cg_tol": (1e-24, 0.0), "dump_k": (0,)}),
+        # per-bond Kn/Tv and initially broken bonds written into the bonds (bond.h:25-27)
+        "hex_hetero": (hetero_plate, {"cg_tol": (1e-24, 0.0), "dump_k": (0,)}),
     }
 
 
@@ -95,7 +103,7 @@ def make(name, build, opts):
             out[f"pin_{s}"] = rb(f"pin_{tag}.f64", np.float64).reshape(-1, 3)
             if int(case.ptype) == 2:
                 out[f"state_var_{s}"] = rb(f"state_var_{tag}.f64", np.float64).reshape(-1, 7)
-            if case.material.critical_bstrain < 1.0:
+            if case.material.critical_bstrain < 1.0 or case.bond_props is not None:
                 out[f"bdamage_{s}"] = rb(f"bdamage_{tag}.f64", np.float64)
         out["meta"] = np.array(json.dumps({"name": name, "opts": {k: list(v) for k, v in opts.items()},
                                            "n": int(case.n), "spec": spec}))

@@ -8,7 +8,7 @@ solving tightly) and 1e-6 relative (mixed path).
 import numpy as np
 import pytest
 
-from _util import CFG, LPM, O, gpu_problem, oracle_problem, oracle_step_args, rel
+from _util import CFG, LPM, O, gpu_problem, hetero_plate, oracle_problem, oracle_step_args, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -25,6 +25,8 @@ def small_cases():
         "fcc_j2": CFG.fcc_bar(size=(1.6, 1.6, 2.4), radius=0.2, steps=3, strain=0.02),
         "sc_j2": CFG.sc_cube(size=2.0, radius=0.25, steps=3, total_disp=0.06, ptype=LPM.ParticleType.J2Plasticity,
                              j2=(200.0, 0.0, 38714.0, 10.0)),
+        # pre-cracked plate (explicit bond lists), loaded below the first bond break
+        "hex_crack": CFG.notched_plate(size=2.0, radius=0.1, crack=0.3, steps=2, total_disp=0.001),
     }
 
 
@@ -192,3 +194,79 @@ def test_cut_back_matches():
     assert stg["cuts"] == sto["cuts"]
     if okg:
         assert rel(g.state()["xyz"] - case.xyz, o.state()["xyz"] - case.xyz) <= FP64_DISP_TOL
+
+
+def test_precrack_grows_like_oracle():
+    """The slit of a notched plate (bond exclusion, explicit bond lists) grows under tension:
+    the same bonds break in the same load steps as in the oracle."""
+    case = CFG.notched_plate(size=2.0, radius=0.1, crack=0.3, steps=8, total_disp=0.008)
+    kw = dict(cg_rtol=1e-24, cg_atol=0.0, tol_iter=1e-9)
+    g = gpu_problem(case, **kw)
+    o = oracle_problem(case, **kw)
+    o.update_geometry()
+    o.update_force_state()
+    for s in range(len(case.steps)):
+        okg, stg = g.solve_load_step(case.load_step(s))
+        oko, sto = o.solve_load_step(*oracle_step_args(case, s))
+        assert okg == oko and stg["cuts"] == sto["cuts"]
+        assert stg["newton_solves"] == sto["newton_solves"], f"step {s}"
+        bg, bo = g.state()["bdamage"], o.state()["bdamage"]
+        assert np.array_equal(bg == 1.0, bo == 1.0), f"step {s}: broken bond sets differ"
+        assert rel(g.state()["xyz"] - case.xyz, o.state()["xyz"] - case.xyz) <= FP64_DISP_TOL
+    assert (bo == 1.0).sum() > 100, "the crack should grow"
+
+
+def _shuffled_bonds(case, seed):
+    """The bond search's lists with each particle's layer-0 and layer-1 lists shuffled: bond
+    files need not list partners in id order (Assembly::readBond keeps file order)."""
+    nb0, nb1, p2 = CFG.bond_lists(case.xyz, LPM.UnitCell(case.lattice, case.radius))
+    rng = np.random.default_rng(seed)
+    p2 = p2.copy()
+    start = 0
+    for a, b in zip(nb0, nb1):
+        p2[start:start + a] = rng.permutation(p2[start:start + a])
+        p2[start + a:start + a + b] = rng.permutation(p2[start + a:start + a + b])
+        start += a + b
+    return nb0, nb1, p2
+
+
+@pytest.mark.parametrize("lat", ["hex", "sc"])
+def test_user_bond_order_is_kept(lat):
+    """Explicit bond lists in arbitrary order: the device keeps the caller's order, so every
+    bond-ordered sum (forces, stiffness) matches the oracle given the same lists bit for bit."""
+    case = CASES[lat]
+    case = CFG.Case(**{**case.__dict__, "bonds": _shuffled_bonds(case, 7)})
+    g = gpu_problem(case)
+    o = oracle_problem(case)
+    t = g.topology()
+    nb0, nb1, p2 = case.bonds
+    assert np.array_equal(t["bond_p2"], p2) and np.array_equal(t["nb0"], nb0)
+    assert np.array_equal(t["conns"], o.conns()[2])
+    o.update_geometry()
+    o.update_force_state()
+    assert np.array_equal(g.state()["pin"], o.state()["pin"])
+    disp, force = oracle_step_args(case, 0)
+    o.apply_bc(disp, force)
+    g.apply_load_step(case.load_step(0))
+    o.assemble(False)
+    g.assemble(False)
+    assert np.array_equal(g.export_csr()[3], o.export_csr()[3])
+
+
+def test_bond_coefficients_and_initial_damage():
+    """Per-bond Kn/Tv (a heterogeneous material) and initially broken bonds, passed through
+    the optional per-bond arrays of the descriptor: forces bit-exact, load steps as the oracle."""
+    case = hetero_plate()
+    kw = dict(cg_rtol=1e-24, cg_atol=0.0, tol_iter=1e-9)
+    o = oracle_problem(case, **kw)
+    o.update_geometry()
+    o.update_force_state()
+    g = gpu_problem(case, **kw)
+    assert np.array_equal(g.state()["pin"], o.state()["pin"])
+    assert np.array_equal(g.state()["damage_visual"], o.state()["damage_visual"])
+    for s in range(len(case.steps)):
+        okg, _ = g.solve_load_step(case.load_step(s))
+        oko, _ = o.solve_load_step(*oracle_step_args(case, s))
+        assert okg and oko
+        assert rel(g.state()["xyz"] - case.xyz, o.state()["xyz"] - case.xyz) <= FP64_DISP_TOL
+    assert np.array_equal(g.state()["bdamage"], o.state()["bdamage"])
