@@ -216,6 +216,52 @@ int32_t lpmgpu_cg_bsr_noalloc(int32_t dim, int32_t nrows, const int32_t *rowptr,
                               const double *values, const double *b, double *x, double rtol, double atol,
                               int64_t maxit, void *stream, int64_t *iterations);
 
+/* ---- Batches: many independent problems advanced together on one GPU (the batched,
+ * served form of SolverStatic::solveProblem).  A member is an lpmgpu_solver handle (not owned
+ * by the batch) plus its whole load path, copied at lpmgpu_batch_add.  Each member follows
+ * exactly the steps of lpmgpu_solve_load_step, load step by load step (halving included); a
+ * round advances every member by one piece of device work and solves all members' pending
+ * Newton systems in one persistent CG launch.  Members may be added between rounds; finished
+ * members may be removed.  A handle must not be used by other calls while it is a running
+ * member.  Not thread-safe: one host thread per batch. */
+typedef struct lpmgpu_batch lpmgpu_batch;
+
+typedef struct
+{
+    int32_t state;      /* 0 running, 1 done, 2 failed */
+    int32_t status;     /* LPMGPU_OK, or the error that stopped the member */
+    int32_t steps_done; /* finished load steps */
+    int32_t nsteps;
+    lpmgpu_stats total; /* summed over the finished load steps */
+    int64_t dof_iters;  /* sum over the member's CG iterations of its unknown count */
+    double seconds;     /* wall time from lpmgpu_batch_add to completion (or to now) */
+} lpmgpu_member_info;
+
+typedef struct
+{
+    int64_t rounds, cg_launches, members_done, members_failed;
+    int64_t cg_iters, dof_iters; /* over members still held by the batch */
+    double seconds;              /* wall time inside lpmgpu_batch_run */
+    double cg_kernel_seconds;    /* device time of the batched CG launches */
+} lpmgpu_batch_stats;
+
+int32_t lpmgpu_batch_create(int32_t device, lpmgpu_batch **out);
+int32_t lpmgpu_batch_destroy(lpmgpu_batch *b);
+/* adds a problem with its load path (steps[0..nsteps)); *member receives its id */
+int32_t lpmgpu_batch_add(lpmgpu_batch *b, lpmgpu_solver *h, const lpmgpu_load_step *steps, int32_t nsteps,
+                         int32_t *member);
+/* one round; *running receives the number of members not yet finished */
+int32_t lpmgpu_batch_round(lpmgpu_batch *b, int32_t *running);
+/* rounds until every member finished */
+int32_t lpmgpu_batch_run(lpmgpu_batch *b);
+int32_t lpmgpu_batch_member(const lpmgpu_batch *b, int32_t member, lpmgpu_member_info *info);
+/* per-load-step statistics of a member (the lpmgpu_stats of each lpmgpu_solve_load_step) */
+int32_t lpmgpu_batch_member_steps(const lpmgpu_batch *b, int32_t member, lpmgpu_stats *steps, int32_t cap,
+                                  int32_t *count);
+/* forgets a finished member (its handle stays with the caller) */
+int32_t lpmgpu_batch_remove(lpmgpu_batch *b, int32_t member);
+int32_t lpmgpu_batch_get_stats(const lpmgpu_batch *b, lpmgpu_batch_stats *st);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,1283 @@
+// Many independent problems on one GPU: the batched persistent CG and the runtime that advances
+// every problem's load path in rounds.
+//
+// Batched CG.  One cooperative launch solves the Newton systems of many problems (any mix of
+// 2D and 3D, each with its own sliced-ELL matrix and Krylov vectors), each with its own
+// stopping test, iteration cap and scalars: the unpreconditioned CG of Solver::LPM_CG
+// (include/solver.h:277-354, MKL RCI dcg on the squared-norm test) per problem.
+//   * Every active problem gets g >= 1 "virtual blocks", g proportional to its matrix size; a
+//     virtual block owns a contiguous share of the problem's slices (SpMV phase) and of its
+//     unknowns (update phase).  The physical blocks (one 32-warp block per SM) stride over
+//     the virtual blocks, so a problem of any size, alone or with others, keeps every SM busy.
+//   * Each virtual block writes one partial per reduction.  At the grid barrier the last block
+//     to arrive sums each problem's partials (a fixed tree: 32-wide warp sums in order), takes
+//     the per-problem decisions (alpha; converged, capped or broken down) and, when a problem
+//     leaves, re-partitions the remaining ones over the virtual blocks before it releases the
+//     barrier.  The tail of a batch (the largest problems) therefore runs on the whole GPU.
+//   * All waits are bounded (4 s); a timeout sets a flag and every block returns.
+//
+// Runtime.  Each member follows SolverStatic::solveProblem / solveProblemStep
+// (include/solver_static.h:65-152) exactly as lpmgpu_solve_load_step does: apply the load
+// step, assemble, modified Newton with K fixed, J2 state + static damage, the damage loop, and
+// on Newton failure reset + halve + run both halves.  A round issues every member's next piece
+// of device work on the member's stream, one batched CG for all members that need a linear
+// solve, and then waits once for all of them before the host takes the members' decisions.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "cg_device.cuh"
+
+namespace lpm
+{
+
+constexpr int kMaxBatch = 1024;                      // problems in one batched launch
+constexpr int kMaxVirt = kMaxGridBlocks + kMaxBatch; // virtual blocks
+
+struct BInst
+{
+    int dim, n, nslices, pad;
+    int64_t ndof, cost; // cost: matrix entries (slots x d^2), the split weight
+    const int *rowptr, *perm;
+    const int64_t *slice_off;
+    const int *col_sell;
+    const void *K, *b;
+    void *x, *r, *pa, *pb, *q;
+    double rtol, atol, abs_stop;
+    int64_t maxit;
+};
+
+struct BState
+{
+    double rr, stop, alpha, beta, rr0, rr_final;
+    int64_t it, status; // status bits: 1 iteration cap, 4 breakdown (p.Ap == 0)
+};
+
+struct BCtl
+{
+    unsigned bar[2]; // arrivals, generation
+    int nvirt, nact;
+    int fail, pad;
+};
+
+struct BArgs
+{
+    const BInst *inst;
+    BState *st;
+    BCtl *ctl;
+    int *act, *gcnt, *vstart; // per active rank [kMaxBatch]
+    int *vinst, *vk, *vg;     // per virtual block [kMaxVirt]
+    double *part;             // per virtual block [kMaxVirt]
+};
+
+// virtual blocks of one problem: its share of G by matrix size, at least 1, at most its slices
+__host__ __device__ inline int vblocks_for(int64_t G, int64_t cost, int64_t C, int nslices)
+{
+    int64_t g = C > 0 ? (G * cost) / C : 1;
+    if (g > nslices)
+        g = nslices;
+    if (g < 1)
+        g = 1;
+    return (int)g;
+}
+
+// ---- block-wide integer scans / sums (1024 threads, deterministic)
+__device__ int block_exscan(int v, int *total, int *sh)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o)
+            x += y;
+    }
+    if (lane == 31)
+        sh[w] = x;
+    __syncthreads();
+    if (w == 0)
+    {
+        int t = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o)
+                t += y;
+        }
+        sh[lane] = t; // inclusive prefix of warp totals
+    }
+    __syncthreads();
+    const int before = (w > 0 ? sh[w - 1] : 0) + x - v;
+    *total = sh[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return before;
+}
+
+__device__ int64_t block_sum_i64(int64_t v, long long *sh)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0)
+        sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    int64_t t = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q)
+        t += sh[q];
+    __syncthreads();
+    return t;
+}
+
+// The last block's work at a barrier: reduce each active problem's partials, decide, and
+// re-partition when problems left.  mode 0: initial ||r||^2; 1: p.Ap -> alpha; 2: ||r||^2 ->
+// beta / convergence / cap.
+__device__ void batch_decide(const BArgs &a, int mode, int64_t it)
+{
+    __shared__ int s_keep[kMaxBatch];
+    __shared__ int s_act[kMaxBatch];
+    __shared__ int s_scan[32];
+    __shared__ long long s_sum[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nact = *reinterpret_cast<volatile int *>(&a.ctl->nact);
+    for (int r = warp; r < nact; r += (int)(blockDim.x >> 5))
+    {
+        const int m = __ldcg(a.act + r), g = __ldcg(a.gcnt + r), vs = __ldcg(a.vstart + r);
+        double tot = 0;
+        for (int c = 0; c < g; c += 32)
+        {
+            double v = (c + lane < g) ? __ldcg(a.part + vs + c + lane) : 0.0;
+            tot += wsum(v);
+        }
+        if (lane == 0)
+        {
+            // written by whichever block arrived last before: read past L1
+            volatile BState *S = a.st + m;
+            const BInst &I = a.inst[m];
+            int keep = 1;
+            if (mode == 0)
+            {
+                const double stop = (I.abs_stop >= 0) ? I.abs_stop : I.rtol * tot + I.atol;
+                S->rr = tot;
+                S->rr0 = tot;
+                S->stop = stop;
+                S->beta = 0.0;
+                S->it = 0;
+                S->rr_final = tot;
+                keep = !(tot <= stop);
+            }
+            else if (mode == 1)
+            {
+                if (tot == 0.0)
+                {
+                    S->it = it - 1;
+                    S->status |= 4;
+                    S->rr_final = S->rr;
+                    keep = 0;
+                }
+                else
+                    S->alpha = S->rr / tot;
+            }
+            else
+            {
+                const bool done = tot <= S->stop;
+                const bool capped = it >= I.maxit;
+                if (done || capped)
+                {
+                    S->it = it;
+                    S->rr_final = tot;
+                    if (!done)
+                        S->status |= 1;
+                    keep = 0;
+                }
+                else
+                {
+                    S->beta = tot / S->rr;
+                    S->rr = tot;
+                }
+            }
+            s_keep[r] = keep;
+        }
+    }
+    __syncthreads();
+    const int t = threadIdx.x;
+    const int keep = (t < nact) ? s_keep[t] : 1;
+    if (!__syncthreads_or(keep == 0))
+        return;
+    // compaction of the still-active ranks (order kept), then the new split
+    const int mine = (t < nact) ? __ldcg(a.act + t) : -1;
+    int nnew = 0;
+    const int pos = block_exscan((t < nact && keep) ? 1 : 0, &nnew, s_scan);
+    if (t < nact && keep)
+        s_act[pos] = mine;
+    __syncthreads();
+    const int m = (t < nnew) ? s_act[t] : -1;
+    const int64_t cost = (m >= 0) ? a.inst[m].cost : 0;
+    const int64_t C = block_sum_i64(cost, s_sum);
+    const int g = (m >= 0) ? vblocks_for(gridDim.x, cost, C, a.inst[m].nslices) : 0;
+    int V = 0;
+    const int vs = block_exscan(g, &V, s_scan);
+    if (m >= 0)
+    {
+        __stcg(a.act + t, m);
+        __stcg(a.gcnt + t, g);
+        __stcg(a.vstart + t, vs);
+        for (int q = 0; q < g; ++q)
+        {
+            __stcg(a.vinst + vs + q, m);
+            __stcg(a.vk + vs + q, q);
+            __stcg(a.vg + vs + q, g);
+        }
+    }
+    if (t == 0)
+    {
+        a.ctl->nact = nnew;
+        a.ctl->nvirt = V;
+    }
+    __syncthreads();
+}
+
+// Grid barrier whose last arrival runs batch_decide before releasing the others.  Returns false
+// when a wait timed out (every block then returns).
+__device__ bool batch_sync(const BArgs &a, int mode, int64_t it, volatile int *s_fail)
+{
+    __shared__ int s_last;
+    unsigned *bar = a.ctl->bar;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        const unsigned gen = ld_acquire(bar + 1);
+        __threadfence();
+        const unsigned arrived = atomicAdd(bar, 1u);
+        s_last = (arrived == gridDim.x - 1);
+        if (!s_last)
+        {
+            const unsigned long long t0 = gtimer();
+            unsigned ns = 32;
+            while (ld_acquire(bar + 1) == gen)
+            {
+                if (gtimer() - t0 > kBarrierTimeoutNs)
+                {
+                    atomicExch(&a.ctl->fail, 1);
+                    *s_fail = 1;
+                    break;
+                }
+                __nanosleep(ns);
+                if (ns < 128)
+                    ns <<= 1;
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    if (s_last)
+    {
+        batch_decide(a, mode, it);
+        if (threadIdx.x == 0)
+        {
+            __threadfence();
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && *reinterpret_cast<volatile int *>(&a.ctl->fail))
+        *s_fail = 1;
+    __syncthreads();
+    return *s_fail == 0;
+}
+
+// phase A for one slice: q = K p_new, p_new = r + beta p_old written, returns the slice's p.q
+template <typename TK, typename TV, int D>
+__device__ __forceinline__ double phase_a_slice(const BInst &I, int sl, TV beta, const TV *pold, TV *pnew, uint64_t pf,
+                                                uint64_t pl)
+{
+    TV acc[D];
+    const TV *r = static_cast<const TV *>(I.r);
+    const int i = spmv_slice<TK, TV, D>(sl, I.n, I.rowptr, I.perm, I.slice_off, I.col_sell,
+                                        static_cast<const TK *>(I.K), r, pold, beta, acc, pf, pl);
+    double lpq = 0;
+    if (i >= 0)
+    {
+        TV *q = static_cast<TV *>(I.q);
+#pragma unroll
+        for (int c = 0; c < D; ++c)
+        {
+            const int64_t k = (int64_t)i * D + c;
+            const TV pn = ld_keep(r + k, pl) + beta * ld_keep(pold + k, pl);
+            st_keep(pnew + k, pn, pl);
+            st_keep(q + k, acc[c], pl);
+            lpq += (double)pn * (double)acc[c];
+        }
+    }
+    return lpq;
+}
+
+template <typename TK, typename TV>
+__global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg_batch(BArgs a)
+{
+    __shared__ double sh[32];
+    __shared__ int s_fail;
+    if (threadIdx.x == 0)
+        s_fail = 0;
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const uint64_t pf = l2_evict_first(), pl = l2_evict_last();
+
+    // r = b, x = 0, p_old = 0; partial ||b||^2
+    int nvirt = *reinterpret_cast<volatile int *>(&a.ctl->nvirt);
+    for (int v = blockIdx.x; v < nvirt; v += gridDim.x)
+    {
+        const int m = __ldcg(a.vinst + v), k = __ldcg(a.vk + v), g = __ldcg(a.vg + v);
+        const BInst &I = a.inst[m];
+        const int64_t lo = k * I.ndof / g, hi = (k + 1) * I.ndof / g;
+        const TV *b = static_cast<const TV *>(I.b);
+        TV *x = static_cast<TV *>(I.x), *r = static_cast<TV *>(I.r), *pa = static_cast<TV *>(I.pa);
+        double loc = 0;
+        for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x)
+        {
+            const TV bv = b[j];
+            st_keep(r + j, bv, pl);
+            st_keep(x + j, TV(0), pl);
+            st_keep(pa + j, TV(0), pl);
+            loc += (double)bv * (double)bv;
+        }
+        block_partial_at(loc, a.part + v, sh);
+    }
+    if (!batch_sync(a, 0, 0, &s_fail))
+        return;
+
+    for (int64_t it = 1;; ++it)
+    {
+        if (*reinterpret_cast<volatile int *>(&a.ctl->nact) == 0)
+            return;
+        const bool odd = (it & 1) != 0;
+        // phase A: q = K p_new over this block's virtual blocks
+        nvirt = *reinterpret_cast<volatile int *>(&a.ctl->nvirt);
+        for (int v = blockIdx.x; v < nvirt; v += gridDim.x)
+        {
+            const int m = __ldcg(a.vinst + v), k = __ldcg(a.vk + v), g = __ldcg(a.vg + v);
+            const BInst &I = a.inst[m];
+            const TV beta = (TV)__ldcg(&a.st[m].beta);
+            const TV *pold = static_cast<const TV *>(odd ? I.pa : I.pb);
+            TV *pnew = static_cast<TV *>(odd ? I.pb : I.pa);
+            const int s0 = (int)((int64_t)k * I.nslices / g), s1 = (int)((int64_t)(k + 1) * I.nslices / g);
+            double lpq = 0;
+            if (I.dim == 2)
+            {
+                for (int sl = s0 + warp; sl < s1; sl += nwarp)
+                    lpq += phase_a_slice<TK, TV, 2>(I, sl, beta, pold, pnew, pf, pl);
+            }
+            else
+            {
+                for (int sl = s0 + warp; sl < s1; sl += nwarp)
+                    lpq += phase_a_slice<TK, TV, 3>(I, sl, beta, pold, pnew, pf, pl);
+            }
+            block_partial_at(lpq, a.part + v, sh);
+        }
+        if (!batch_sync(a, 1, it, &s_fail))
+            return;
+        // phase B: x += alpha p_new, r -= alpha q
+        nvirt = *reinterpret_cast<volatile int *>(&a.ctl->nvirt);
+        for (int v = blockIdx.x; v < nvirt; v += gridDim.x)
+        {
+            const int m = __ldcg(a.vinst + v), k = __ldcg(a.vk + v), g = __ldcg(a.vg + v);
+            const BInst &I = a.inst[m];
+            const TV al = (TV)__ldcg(&a.st[m].alpha);
+            const TV *pnew = static_cast<const TV *>(odd ? I.pb : I.pa);
+            TV *x = static_cast<TV *>(I.x), *r = static_cast<TV *>(I.r);
+            const TV *q = static_cast<const TV *>(I.q);
+            const int64_t lo = k * I.ndof / g, hi = (k + 1) * I.ndof / g;
+            double lrr = 0;
+            for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x)
+            {
+                st_keep(x + j, ld_keep(x + j, pl) + al * ld_keep(pnew + j, pl), pl);
+                const TV rv = ld_keep(r + j, pl) - al * ld_keep(q + j, pl);
+                st_keep(r + j, rv, pl);
+                lrr += (double)rv * (double)rv;
+            }
+            block_partial_at(lrr, a.part + v, sh);
+        }
+        if (!batch_sync(a, 2, it, &s_fail))
+            return;
+    }
+}
+
+// ---- host side of the batched CG
+struct BatchItem
+{
+    Problem *p;
+    bool fp32;
+    double rtol, atol, abs_stop;
+    int64_t maxit;
+};
+
+struct BatchCtx
+{
+    int device = 0, num_sms = 0, grid = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_done = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
+    std::vector<cudaEvent_t> ev_in; // one per item slot
+    BInst *d_inst = nullptr, *h_inst = nullptr;
+    BState *d_st = nullptr, *h_st = nullptr;
+    BCtl *d_ctl = nullptr, *h_ctl = nullptr;
+    int *d_tab = nullptr, *h_tab = nullptr; // act|gcnt|vstart [3*kMaxBatch] + vinst|vk|vg [3*kMaxVirt]
+    double *d_part = nullptr;
+    int64_t launches = 0;
+    double kernel_seconds = 0;
+    bool timing_pending = false;
+
+    cudaError_t init(int dev)
+    {
+        device = dev;
+        cudaError_t e;
+        if ((e = cudaSetDevice(dev)) != cudaSuccess)
+            return e;
+        if ((e = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+            return e;
+        int occ64 = 0, occ32 = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ64, k_cg_batch<double, double>, kCGThreads, 0)) !=
+            cudaSuccess)
+            return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ32, k_cg_batch<float, float>, kCGThreads, 0)) !=
+            cudaSuccess)
+            return e;
+        grid = std::min(kMaxGridBlocks, num_sms * std::max(1, std::min({occ64, occ32, kCGMinBlocks})));
+        if ((e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)) != cudaSuccess)
+            return e;
+        if ((e = cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming)) != cudaSuccess)
+            return e;
+        if ((e = cudaEventCreate(&ev_t0)) != cudaSuccess || (e = cudaEventCreate(&ev_t1)) != cudaSuccess)
+            return e;
+        const size_t ntab = 3 * (size_t)kMaxBatch + 3 * (size_t)kMaxVirt;
+        if ((e = cudaMalloc(&d_inst, sizeof(BInst) * kMaxBatch)) != cudaSuccess ||
+            (e = cudaMalloc(&d_st, sizeof(BState) * kMaxBatch)) != cudaSuccess ||
+            (e = cudaMalloc(&d_ctl, sizeof(BCtl))) != cudaSuccess ||
+            (e = cudaMalloc(&d_tab, sizeof(int) * ntab)) != cudaSuccess ||
+            (e = cudaMalloc(&d_part, sizeof(double) * kMaxVirt)) != cudaSuccess)
+            return e;
+        if ((e = cudaMallocHost(&h_inst, sizeof(BInst) * kMaxBatch)) != cudaSuccess ||
+            (e = cudaMallocHost(&h_st, sizeof(BState) * kMaxBatch)) != cudaSuccess ||
+            (e = cudaMallocHost(&h_ctl, sizeof(BCtl))) != cudaSuccess ||
+            (e = cudaMallocHost(&h_tab, sizeof(int) * ntab)) != cudaSuccess)
+            return e;
+        return cudaSuccess;
+    }
+
+    void release()
+    {
+        cudaSetDevice(device);
+        for (auto ev : ev_in)
+            cudaEventDestroy(ev);
+        ev_in.clear();
+        if (ev_done)
+            cudaEventDestroy(ev_done);
+        if (ev_t0)
+            cudaEventDestroy(ev_t0);
+        if (ev_t1)
+            cudaEventDestroy(ev_t1);
+        if (stream)
+            cudaStreamDestroy(stream);
+        cudaFree(d_inst);
+        cudaFree(d_st);
+        cudaFree(d_ctl);
+        cudaFree(d_tab);
+        cudaFree(d_part);
+        cudaFreeHost(h_inst);
+        cudaFreeHost(h_st);
+        cudaFreeHost(h_ctl);
+        cudaFreeHost(h_tab);
+        ev_done = ev_t0 = ev_t1 = nullptr;
+        stream = nullptr;
+        d_inst = h_inst = nullptr;
+        d_st = h_st = nullptr;
+        d_ctl = h_ctl = nullptr;
+        d_tab = h_tab = nullptr;
+        d_part = nullptr;
+    }
+
+    // Enqueues one batched solve after each item's pending work on its own stream; each item's
+    // stream then waits for the solve.  Results (h_st, h_ctl) are valid once `stream` is
+    // synchronised.  All items must share one precision.
+    cudaError_t launch(const std::vector<BatchItem> &items)
+    {
+        if (items.empty())
+            return cudaSuccess;
+        if (items.size() > (size_t)kMaxBatch)
+            return cudaErrorInvalidValue;
+        const int ni = (int)items.size();
+        const bool fp32 = items[0].fp32;
+        cudaError_t e;
+        while ((int)ev_in.size() < ni)
+        {
+            cudaEvent_t ev;
+            if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
+                return e;
+            ev_in.push_back(ev);
+        }
+        int64_t C = 0;
+        for (int m = 0; m < ni; ++m)
+        {
+            const Problem &p = *items[m].p;
+            BInst &I = h_inst[m];
+            std::memset(&I, 0, sizeof(I));
+            I.dim = p.dim;
+            I.n = p.n;
+            I.nslices = p.nslices;
+            I.ndof = (int64_t)p.n * p.dim;
+            I.cost = p.nsb * p.dim * p.dim;
+            I.rowptr = p.cstart;
+            I.perm = p.perm;
+            I.slice_off = p.slice_off;
+            I.col_sell = p.col_sell;
+            if (fp32)
+            {
+                I.K = p.K32;
+                I.b = p.b32;
+                I.x = p.x32;
+                I.r = p.r32;
+                I.pa = p.pa32;
+                I.pb = p.pb32;
+                I.q = p.q32;
+            }
+            else
+            {
+                I.K = p.K;
+                I.b = p.res;
+                I.x = p.x;
+                I.r = p.r;
+                I.pa = p.p0;
+                I.pb = p.p1;
+                I.q = p.q;
+            }
+            I.rtol = items[m].rtol;
+            I.atol = items[m].atol;
+            I.abs_stop = items[m].abs_stop;
+            I.maxit = items[m].maxit;
+            C += I.cost;
+        }
+        // initial split over all items (the same integer rule the kernel uses when problems leave)
+        int *act = h_tab, *gcnt = h_tab + kMaxBatch, *vstart = h_tab + 2 * kMaxBatch;
+        int *vinst = h_tab + 3 * kMaxBatch, *vk = vinst + kMaxVirt, *vg = vk + kMaxVirt;
+        int V = 0;
+        for (int m = 0; m < ni; ++m)
+        {
+            const int g = vblocks_for(grid, h_inst[m].cost, C, h_inst[m].nslices);
+            act[m] = m;
+            gcnt[m] = g;
+            vstart[m] = V;
+            for (int q = 0; q < g; ++q)
+            {
+                vinst[V + q] = m;
+                vk[V + q] = q;
+                vg[V + q] = g;
+            }
+            V += g;
+        }
+        std::memset(h_st, 0, sizeof(BState) * items.size());
+        std::memset(h_ctl, 0, sizeof(BCtl));
+        h_ctl->nvirt = V;
+        h_ctl->nact = ni;
+        for (int m = 0; m < ni; ++m)
+        {
+            if ((e = cudaEventRecord(ev_in[m], items[m].p->stream)) != cudaSuccess)
+                return e;
+            if ((e = cudaStreamWaitEvent(stream, ev_in[m], 0)) != cudaSuccess)
+                return e;
+        }
+        if ((e = cudaMemcpyAsync(d_inst, h_inst, sizeof(BInst) * ni, cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(d_st, h_st, sizeof(BState) * ni, cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(d_ctl, h_ctl, sizeof(BCtl), cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(d_tab, h_tab, sizeof(int) * 3 * kMaxBatch, cudaMemcpyHostToDevice, stream)) !=
+                cudaSuccess ||
+            (e = cudaMemcpyAsync(d_tab + 3 * kMaxBatch, vinst, sizeof(int) * V, cudaMemcpyHostToDevice, stream)) !=
+                cudaSuccess ||
+            (e = cudaMemcpyAsync(d_tab + 3 * kMaxBatch + kMaxVirt, vk, sizeof(int) * V, cudaMemcpyHostToDevice,
+                                 stream)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(d_tab + 3 * kMaxBatch + 2 * kMaxVirt, vg, sizeof(int) * V, cudaMemcpyHostToDevice,
+                                 stream)) != cudaSuccess)
+            return e;
+        BArgs a;
+        a.inst = d_inst;
+        a.st = d_st;
+        a.ctl = d_ctl;
+        a.act = d_tab;
+        a.gcnt = d_tab + kMaxBatch;
+        a.vstart = d_tab + 2 * kMaxBatch;
+        a.vinst = d_tab + 3 * kMaxBatch;
+        a.vk = a.vinst + kMaxVirt;
+        a.vg = a.vk + kMaxVirt;
+        a.part = d_part;
+        void *args[] = {&a};
+        if ((e = cudaEventRecord(ev_t0, stream)) != cudaSuccess)
+            return e;
+        e = fp32 ? cudaLaunchCooperativeKernel((const void *)k_cg_batch<float, float>, dim3(grid), dim3(kCGThreads),
+                                               args, 0, stream)
+                 : cudaLaunchCooperativeKernel((const void *)k_cg_batch<double, double>, dim3(grid),
+                                               dim3(kCGThreads), args, 0, stream);
+        if (e != cudaSuccess)
+            return e;
+        if ((e = cudaEventRecord(ev_t1, stream)) != cudaSuccess)
+            return e;
+        launches++;
+        timing_pending = true;
+        if ((e = cudaMemcpyAsync(h_st, d_st, sizeof(BState) * ni, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(h_ctl, d_ctl, sizeof(BCtl), cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
+            return e;
+        if ((e = cudaEventRecord(ev_done, stream)) != cudaSuccess)
+            return e;
+        for (int m = 0; m < ni; ++m)
+        {
+            items[m].p->ctr.kernel_launches++;
+            items[m].p->ctr.cg_launches++;
+            if ((e = cudaStreamWaitEvent(items[m].p->stream, ev_done, 0)) != cudaSuccess)
+                return e;
+        }
+        return cudaSuccess;
+    }
+
+    // after `stream` was synchronised: accumulate the kernel time of the last launch
+    void account()
+    {
+        if (!timing_pending)
+            return;
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, ev_t0, ev_t1) == cudaSuccess)
+            kernel_seconds += ms * 1e-3;
+        timing_pending = false;
+    }
+};
+
+} // namespace lpm
+
+// ======================================================================================
+// The batch runtime and its C ABI.
+using namespace lpm;
+
+namespace
+{
+
+struct StepCopy
+{
+    std::vector<std::vector<int32_t>> dids, fids;
+    std::vector<lpmgpu_dispbc> d;
+    std::vector<lpmgpu_forcebc> f;
+
+    explicit StepCopy(const lpmgpu_load_step &s)
+    {
+        for (int k = 0; k < s.ndisp; ++k)
+        {
+            dids.emplace_back(s.disp[k].ids, s.disp[k].ids + s.disp[k].count);
+            d.push_back(s.disp[k]);
+        }
+        for (int k = 0; k < s.nforce; ++k)
+        {
+            fids.emplace_back(s.force[k].ids, s.force[k].ids + s.force[k].count);
+            f.push_back(s.force[k]);
+        }
+        for (size_t k = 0; k < d.size(); ++k)
+            d[k].ids = dids[k].data();
+        for (size_t k = 0; k < f.size(); ++k)
+            f[k].ids = fids[k].data();
+    }
+};
+
+enum class Ph
+{
+    Start,       // next sub-step (or next load step) to begin
+    NewtonFirst, // force state of the first Newton check in flight
+    Newton,      // force state after a Newton update in flight
+    NeedCG,      // needs a linear solve this round
+    DamageCheck, // J2 state + static damage in flight
+    Done,
+    Failed
+};
+
+struct Member
+{
+    lpmgpu_solver *h = nullptr;
+    std::vector<StepCopy> steps;
+    size_t next = 0;
+    std::vector<std::pair<double, int>> stack; // pending sub-steps of the current load step
+    double scale = 1.0;
+    int depth = 0;
+    Ph ph = Ph::Start;
+    bool pending = false; // device work whose scalars the next synchronisation delivers
+    int k = 0;
+    double tol_mult = 0, nres = 0;
+    lpmgpu_stats cur{};
+    std::vector<lpmgpu_stats> step_stats;
+    lpmgpu_stats total{};
+    int64_t dof_iters = 0;
+    int32_t status = LPMGPU_OK;
+    std::chrono::steady_clock::time_point t_add, t_done;
+    // mixed-precision refinement of the current linear solve
+    double ir_stop = 0, ir_rr = 0;
+    int ir_ref = 0;
+};
+
+int32_t cuda_status(cudaError_t e, const char *what)
+{
+    set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? LPMGPU_ERR_OUT_OF_MEMORY : LPMGPU_ERR_CUDA;
+}
+
+} // namespace
+
+struct lpmgpu_batch
+{
+    BatchCtx ctx;
+    std::vector<std::unique_ptr<Member>> members; // index = member id; removed -> null
+    lpmgpu_batch_stats stats{};
+    std::chrono::steady_clock::time_point t_create;
+
+    Problem &P(Member &m) { return m.h->p; }
+
+    // one sub-step begins: scaled load step (solver_static.h:78-87 halving), assembly, first
+    // force state of the Newton loop.  Returns false when the member has finished its path.
+    int32_t begin_substep(Member &m)
+    {
+        if (m.stack.empty())
+        {
+            if (m.next >= m.steps.size())
+            {
+                finish(m, LPMGPU_OK);
+                return LPMGPU_OK;
+            }
+            m.stack.push_back({1.0, 0});
+            m.next++;
+            m.cur = lpmgpu_stats{};
+        }
+        auto sd = m.stack.back();
+        m.stack.pop_back();
+        m.scale = sd.first;
+        m.depth = sd.second;
+        const StepCopy &s = m.steps[m.next - 1];
+        std::vector<lpmgpu_dispbc> db(s.d);
+        std::vector<lpmgpu_forcebc> fb(s.f);
+        for (auto &d : db)
+            d.step *= m.scale;
+        for (auto &f : fb)
+        {
+            f.fx *= m.scale;
+            f.fy *= m.scale;
+            f.fz *= m.scale;
+        }
+        lpmgpu_load_step ls{db.data(), (int32_t)db.size(), fb.data(), (int32_t)fb.size()};
+        Problem &p = P(m);
+        cudaError_t e = launch_apply_bc(p, ls);
+        if (e == cudaSuccess)
+            e = enqueue_assemble(p, true);
+        if (e == cudaSuccess)
+            e = enqueue_force_state(p, true);
+        if (e != cudaSuccess)
+            return fail_member(m, cuda_status(e, "batch sub-step"));
+        m.cur.damage_iters++;
+        m.ph = Ph::NewtonFirst;
+        m.pending = true;
+        return LPMGPU_OK;
+    }
+
+    int32_t fail_member(Member &m, int32_t code)
+    {
+        m.status = code;
+        m.ph = Ph::Failed;
+        m.pending = false;
+        m.t_done = std::chrono::steady_clock::now();
+        stats.members_failed++;
+        return LPMGPU_OK;
+    }
+
+    void finish(Member &m, int32_t code)
+    {
+        m.status = code;
+        m.ph = Ph::Done;
+        m.pending = false;
+        m.t_done = std::chrono::steady_clock::now();
+        stats.members_done++;
+    }
+
+    // after the Newton loop of one damage iteration (solver_static.h:119-121)
+    int32_t after_newton(Member &m, int n_newton)
+    {
+        Problem &p = P(m);
+        m.cur.residual_norm = m.nres;
+        if (n_newton >= p.desc.max_iter)
+            return fail_substep(m);
+        cudaError_t e = enqueue_damage_update(p);
+        if (e != cudaSuccess)
+            return fail_member(m, cuda_status(e, "batch damage update"));
+        m.ph = Ph::DamageCheck;
+        m.pending = true;
+        return LPMGPU_OK;
+    }
+
+    // Newton failure: reset to the last converged state and run two halves (solver_static.h:78-87)
+    int32_t fail_substep(Member &m)
+    {
+        if (m.depth >= 30)
+            return fail_member(m, LPMGPU_ERR_CUTS);
+        cudaError_t e = enqueue_reset_state(P(m));
+        if (e != cudaSuccess)
+            return fail_member(m, cuda_status(e, "batch reset"));
+        m.cur.cuts++;
+        m.stack.push_back({m.scale / 2.0, m.depth + 1});
+        m.stack.push_back({m.scale / 2.0, m.depth + 1});
+        m.ph = Ph::Start;
+        return LPMGPU_OK;
+    }
+
+    void substep_done(Member &m)
+    {
+        Problem &p = P(m);
+        m.cur.reaction_norm = std::sqrt(p.scal_host->reaction_sq);
+        if (m.stack.empty())
+        {
+            m.cur.converged = 1;
+            m.step_stats.push_back(m.cur);
+            m.total.converged = 1;
+            m.total.newton_solves += m.cur.newton_solves;
+            m.total.cuts += m.cur.cuts;
+            m.total.damage_iters += m.cur.damage_iters;
+            m.total.cg_iters += m.cur.cg_iters;
+            m.total.cg_maxit_hits += m.cur.cg_maxit_hits;
+            m.total.refinements += m.cur.refinements;
+            m.total.reaction_norm = m.cur.reaction_norm;
+            m.total.residual_norm = m.cur.residual_norm;
+            if (m.next >= m.steps.size())
+            {
+                finish(m, LPMGPU_OK);
+                return;
+            }
+        }
+        m.ph = Ph::Start;
+    }
+
+    // Solver::NewtonIteration's test (solver.h:55-90) after a force state arrived
+    int32_t newton_check(Member &m)
+    {
+        Problem &p = P(m);
+        if (m.nres <= p.desc.tol_iter * m.tol_mult)
+            return after_newton(m, m.k);
+        if (++m.k > p.desc.max_iter)
+            return after_newton(m, p.desc.max_iter);
+        m.ph = Ph::NeedCG;
+        return LPMGPU_OK;
+    }
+
+    int32_t resolve(Member &m)
+    {
+        Problem &p = P(m);
+        m.pending = false;
+        if (p.scal_host->err)
+            return fail_member(m, LPMGPU_ERR_TOPOLOGY);
+        switch (m.ph)
+        {
+        case Ph::NewtonFirst:
+        {
+            m.nres = std::sqrt(p.scal_host->res_sq);
+            const double nreac = std::sqrt(p.scal_host->reaction_sq);
+            m.tol_mult = std_max(m.nres, nreac);
+            m.k = 0;
+            return newton_check(m);
+        }
+        case Ph::Newton:
+            m.nres = std::sqrt(p.scal_host->res_sq);
+            return newton_check(m);
+        case Ph::DamageCheck:
+        {
+            const bool new_damaged = p.scal_host->any_flag != 0;
+            cudaError_t e = enqueue_store_state(p);
+            if (e == cudaSuccess && new_damaged)
+            {
+                // damage loop (solver_static.h:126-139): force state, then assemble + Newton again
+                e = enqueue_force_state(p, false);
+                if (e == cudaSuccess)
+                    e = enqueue_assemble(p, true);
+                if (e == cudaSuccess)
+                    e = enqueue_force_state(p, true);
+                if (e == cudaSuccess)
+                {
+                    m.cur.damage_iters++;
+                    m.ph = Ph::NewtonFirst;
+                    m.pending = true;
+                    return LPMGPU_OK;
+                }
+            }
+            if (e != cudaSuccess)
+                return fail_member(m, cuda_status(e, "batch damage loop"));
+            substep_done(m);
+            return LPMGPU_OK;
+        }
+        default:
+            return LPMGPU_OK;
+        }
+    }
+
+    cudaError_t sync_members(const std::vector<Member *> &ms)
+    {
+        for (Member *m : ms)
+        {
+            cudaError_t e = cudaStreamSynchronize(P(*m).stream);
+            if (e != cudaSuccess)
+                return e;
+        }
+        return cudaSuccess;
+    }
+
+    // the linear solves of this round: FP64 members in one batched launch; mixed members in
+    // FP32 batched launches inside their own FP64 refinements (the rule of solve_dim)
+    int32_t linear_solves(std::vector<Member *> &cg64, std::vector<Member *> &cgmix)
+    {
+        cudaError_t e;
+        if (!cg64.empty())
+        {
+            std::vector<BatchItem> items;
+            for (Member *m : cg64)
+            {
+                Problem &p = P(*m);
+                const int64_t ndof = (int64_t)p.n * p.dim;
+                items.push_back({&p, false, p.desc.cg_rtol, p.desc.cg_atol, -1.0,
+                                 p.desc.cg_maxit > 0 ? p.desc.cg_maxit : ndof});
+            }
+            if ((e = ctx.launch(items)) != cudaSuccess)
+                return cuda_status(e, "batched CG launch");
+            if ((e = cudaStreamSynchronize(ctx.stream)) != cudaSuccess)
+                return cuda_status(e, "batched CG");
+            ctx.account();
+            const bool timeout = ctx.h_ctl->fail != 0;
+            for (size_t q = 0; q < cg64.size(); ++q)
+            {
+                Member &m = *cg64[q];
+                const BState &S = ctx.h_st[q];
+                Problem &p = P(m);
+                m.cur.newton_solves++;
+                m.cur.cg_iters += S.it;
+                m.dof_iters += S.it * (int64_t)p.n * p.dim;
+                p.ctr.cg_iters += S.it;
+                if (S.status & 1)
+                    m.cur.cg_maxit_hits++;
+                if (timeout)
+                {
+                    set_last_error("a device-side barrier wait timed out in the batched CG kernel");
+                    fail_member(m, LPMGPU_ERR_TIMEOUT);
+                }
+            }
+            stats.cg_launches++;
+        }
+        if (!cgmix.empty())
+        {
+            // x = 0, r = b, rr0 = ||b||^2 for every member
+            for (Member *m : cgmix)
+            {
+                Problem &p = P(*m);
+                if ((e = cudaMemsetAsync(p.x, 0, sizeof(double) * (size_t)p.n * p.dim, p.stream)) != cudaSuccess ||
+                    (e = enqueue_true_residual(p)) != cudaSuccess)
+                    return cuda_status(e, "batched refinement");
+            }
+            if ((e = sync_members(cgmix)) != cudaSuccess)
+                return cuda_status(e, "batched refinement");
+            std::vector<Member *> act;
+            for (Member *m : cgmix)
+            {
+                Problem &p = P(*m);
+                m->ir_rr = true_residual_result(p);
+                m->ir_stop = p.desc.cg_rtol * m->ir_rr + p.desc.cg_atol;
+                m->ir_ref = 0;
+                m->cur.newton_solves++;
+                if (!(m->ir_rr <= m->ir_stop))
+                    act.push_back(m);
+            }
+            while (!act.empty())
+            {
+                std::vector<BatchItem> items;
+                for (Member *m : act)
+                {
+                    Problem &p = P(*m);
+                    if ((e = enqueue_r_to_b32(p)) != cudaSuccess)
+                        return cuda_status(e, "batched refinement");
+                    const int64_t ndof = (int64_t)p.n * p.dim;
+                    items.push_back({&p, true, 0.0, 0.0, 0.25 * m->ir_stop,
+                                     p.desc.cg_maxit > 0 ? p.desc.cg_maxit : ndof});
+                }
+                if ((e = ctx.launch(items)) != cudaSuccess)
+                    return cuda_status(e, "batched CG launch");
+                stats.cg_launches++;
+                for (Member *m : act)
+                    if ((e = enqueue_add_x32(P(*m))) != cudaSuccess || (e = enqueue_true_residual(P(*m))) != cudaSuccess)
+                        return cuda_status(e, "batched refinement");
+                if ((e = cudaStreamSynchronize(ctx.stream)) != cudaSuccess || (e = sync_members(act)) != cudaSuccess)
+                    return cuda_status(e, "batched refinement");
+                ctx.account();
+                const bool timeout = ctx.h_ctl->fail != 0;
+                std::vector<Member *> next;
+                for (size_t q = 0; q < act.size(); ++q)
+                {
+                    Member &m = *act[q];
+                    Problem &p = P(m);
+                    const BState &S = ctx.h_st[q];
+                    m.cur.cg_iters += S.it;
+                    m.dof_iters += S.it * (int64_t)p.n * p.dim;
+                    p.ctr.cg_iters += S.it;
+                    m.cur.refinements++;
+                    if (S.status & 1)
+                        m.cur.cg_maxit_hits++;
+                    m.ir_rr = true_residual_result(p);
+                    m.ir_ref++;
+                    if (timeout)
+                    {
+                        set_last_error("a device-side barrier wait timed out in the batched CG kernel");
+                        fail_member(m, LPMGPU_ERR_TIMEOUT);
+                        continue;
+                    }
+                    if (!(m.ir_rr <= m.ir_stop) && S.it > 0 && m.ir_ref < 30)
+                        next.push_back(&m);
+                }
+                act.swap(next);
+            }
+        }
+        // Newton update and the next force state
+        for (auto *list : {&cg64, &cgmix})
+            for (Member *m : *list)
+            {
+                if (m->ph == Ph::Failed)
+                    continue;
+                Problem &p = P(*m);
+                cudaError_t e2 = launch_add_disp(p);
+                if (e2 == cudaSuccess)
+                    e2 = enqueue_force_state(p, true);
+                if (e2 != cudaSuccess)
+                {
+                    fail_member(*m, cuda_status(e2, "batch Newton update"));
+                    continue;
+                }
+                m->ph = Ph::Newton;
+                m->pending = true;
+            }
+        return LPMGPU_OK;
+    }
+
+    int32_t round(int32_t *running)
+    {
+        stats.rounds++;
+        // A: members that can start their next sub-step
+        for (auto &up : members)
+        {
+            if (!up)
+                continue;
+            Member &m = *up;
+            if (m.ph == Ph::Start)
+            {
+                cudaSetDevice(P(m).device);
+                begin_substep(m);
+            }
+        }
+        // B: linear solves
+        std::vector<Member *> cg64, cgmix;
+        for (auto &up : members)
+            if (up && up->ph == Ph::NeedCG)
+                (P(*up).desc.precision == LPMGPU_MIXED ? cgmix : cg64).push_back(up.get());
+        int32_t r = linear_solves(cg64, cgmix);
+        if (r != LPMGPU_OK)
+            return r;
+        // C: one wait for every member's scalars, then the host decisions
+        std::vector<Member *> pend;
+        for (auto &up : members)
+            if (up && up->pending)
+                pend.push_back(up.get());
+        cudaError_t e = sync_members(pend);
+        if (e != cudaSuccess)
+            return cuda_status(e, "batch round");
+        for (Member *m : pend)
+            resolve(*m);
+        int32_t live = 0;
+        for (auto &up : members)
+            if (up && up->ph != Ph::Done && up->ph != Ph::Failed)
+                live++;
+        if (running)
+            *running = live;
+        return LPMGPU_OK;
+    }
+};
+
+extern "C" {
+
+int32_t lpmgpu_batch_create(int32_t device, lpmgpu_batch **out)
+{
+    if (!out)
+        return LPMGPU_ERR_INVALID_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    {
+        set_last_error("no CUDA device visible; liblpmgpu has no CPU path");
+        return LPMGPU_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev)
+        return LPMGPU_ERR_INVALID_ARG;
+    auto *b = new lpmgpu_batch();
+    cudaError_t e = b->ctx.init(device);
+    if (e != cudaSuccess)
+    {
+        int32_t s = cuda_status(e, "lpmgpu_batch_create");
+        b->ctx.release();
+        delete b;
+        return s;
+    }
+    b->t_create = std::chrono::steady_clock::now();
+    *out = b;
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_batch_destroy(lpmgpu_batch *b)
+{
+    if (!b)
+        return LPMGPU_ERR_INVALID_ARG;
+    b->ctx.release();
+    delete b;
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_batch_add(lpmgpu_batch *b, lpmgpu_solver *h, const lpmgpu_load_step *steps, int32_t nsteps,
+                         int32_t *member)
+{
+    if (!b || !h || nsteps < 0 || (nsteps > 0 && !steps))
+        return LPMGPU_ERR_INVALID_ARG;
+    if (h->p.device != b->ctx.device)
+    {
+        set_last_error("the problem lives on another device than the batch");
+        return LPMGPU_ERR_INVALID_ARG;
+    }
+    int live = 0;
+    for (auto &up : b->members)
+    {
+        if (up && up->h == h && up->ph != Ph::Done && up->ph != Ph::Failed)
+        {
+            set_last_error("the problem is already a running member of this batch");
+            return LPMGPU_ERR_INVALID_ARG;
+        }
+        if (up && up->ph != Ph::Done && up->ph != Ph::Failed)
+            live++;
+    }
+    if (live >= kMaxBatch)
+    {
+        set_last_error("a batch runs at most 1024 problems at once");
+        return LPMGPU_ERR_BUDGET;
+    }
+    for (int32_t s = 0; s < nsteps; ++s)
+        for (int k = 0; k < steps[s].ndisp; ++k)
+            if (steps[s].disp[k].flag < 0 || steps[s].disp[k].flag >= h->p.dim || steps[s].disp[k].count < 0 ||
+                (steps[s].disp[k].count > 0 && !steps[s].disp[k].ids))
+                return LPMGPU_ERR_INVALID_ARG;
+    auto m = std::make_unique<Member>();
+    m->h = h;
+    for (int32_t s = 0; s < nsteps; ++s)
+        m->steps.emplace_back(steps[s]);
+    m->t_add = std::chrono::steady_clock::now();
+    if (nsteps == 0)
+    {
+        m->ph = Ph::Done;
+        m->t_done = m->t_add;
+        b->stats.members_done++;
+    }
+    b->members.push_back(std::move(m));
+    if (member)
+        *member = (int32_t)b->members.size() - 1;
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_batch_round(lpmgpu_batch *b, int32_t *running)
+{
+    if (!b)
+        return LPMGPU_ERR_INVALID_ARG;
+    if (cudaSetDevice(b->ctx.device) != cudaSuccess)
+        return LPMGPU_ERR_CUDA;
+    return b->round(running);
+}
+
+int32_t lpmgpu_batch_run(lpmgpu_batch *b)
+{
+    if (!b)
+        return LPMGPU_ERR_INVALID_ARG;
+    if (cudaSetDevice(b->ctx.device) != cudaSuccess)
+        return LPMGPU_ERR_CUDA;
+    const auto t0 = std::chrono::steady_clock::now();
+    int32_t running = 1;
+    while (running > 0)
+    {
+        int32_t r = b->round(&running);
+        if (r != LPMGPU_OK)
+            return r;
+    }
+    b->stats.seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_batch_member(const lpmgpu_batch *b, int32_t member, lpmgpu_member_info *info)
+{
+    if (!b || !info || member < 0 || member >= (int32_t)b->members.size() || !b->members[member])
+        return LPMGPU_ERR_INVALID_ARG;
+    const Member &m = *b->members[member];
+    std::memset(info, 0, sizeof(*info));
+    info->state = m.ph == Ph::Done ? 1 : (m.ph == Ph::Failed ? 2 : 0);
+    info->status = m.status;
+    info->steps_done = (int32_t)m.step_stats.size();
+    info->nsteps = (int32_t)m.steps.size();
+    info->total = m.total;
+    info->dof_iters = m.dof_iters;
+    const auto end = (info->state != 0) ? m.t_done : std::chrono::steady_clock::now();
+    info->seconds = std::chrono::duration<double>(end - m.t_add).count();
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_batch_member_steps(const lpmgpu_batch *b, int32_t member, lpmgpu_stats *steps, int32_t cap,
+                                  int32_t *count)
+{
+    if (!b || member < 0 || member >= (int32_t)b->members.size() || !b->members[member] || cap < 0 ||
+        (cap > 0 && !steps))
+        return LPMGPU_ERR_INVALID_ARG;
+    const Member &m = *b->members[member];
+    const int32_t n = (int32_t)m.step_stats.size();
+    for (int32_t k = 0; k < std::min(n, cap); ++k)
+        steps[k] = m.step_stats[k];
+    if (count)
+        *count = n;
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_batch_remove(lpmgpu_batch *b, int32_t member)
+{
+    if (!b || member < 0 || member >= (int32_t)b->members.size() || !b->members[member])
+        return LPMGPU_ERR_INVALID_ARG;
+    const Member &m = *b->members[member];
+    if (m.ph != Ph::Done && m.ph != Ph::Failed)
+    {
+        set_last_error("only finished members can be removed");
+        return LPMGPU_ERR_NOT_READY;
+    }
+    b->members[member].reset();
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_batch_get_stats(const lpmgpu_batch *b, lpmgpu_batch_stats *st)
+{
+    if (!b || !st)
+        return LPMGPU_ERR_INVALID_ARG;
+    *st = b->stats;
+    st->cg_kernel_seconds = b->ctx.kernel_seconds;
+    int64_t it = 0, di = 0;
+    for (auto &up : b->members)
+        if (up)
+        {
+            it += up->total.cg_iters;
+            di += up->dof_iters;
+        }
+    st->cg_iters = it;
+    st->dof_iters = di;
+    return LPMGPU_OK;
+}
+
+} // extern "C"

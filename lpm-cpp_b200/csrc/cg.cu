@@ -31,16 +31,10 @@
 #include <mutex>
 #include <string>
 
-#include "lpm_internal.cuh"
+#include "cg_device.cuh"
 
 namespace lpm
 {
-
-// one 32-warp block per SM: with <= 64 registers every slice of the 382,500-DOF cube gets its
-// own warp (3,985 slices, 4,736 resident warps) and each grid barrier takes 148 arrivals
-constexpr int kCGThreads = 1024;
-constexpr int kCGMinBlocks = 1;
-constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull; // 4 s
 
 struct CGState
 {
@@ -59,21 +53,6 @@ struct CGState
     int64_t *info;      // [0] iterations, [1] status bits (1 maxit, 2 timeout, 4 breakdown), [2..3] rr0/rr bits
 };
 
-__device__ __forceinline__ unsigned long long gtimer()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
-{
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ double wsum(double v);
 
 // Grid barrier fused with the reduction of the per-block partials part[2*b + slot]: the last
 // block to arrive sums them (fixed order: thread t takes b = t, t + blockDim, ..., then a fixed
@@ -146,143 +125,6 @@ __device__ bool grid_reduce(unsigned *bar, int64_t *info, volatile int *s_fail, 
     const bool ok = *s_fail == 0;
     __syncthreads();
     return ok;
-}
-
-__device__ __forceinline__ double wsum(double v)
-{
-    for (int o = 16; o > 0; o >>= 1)
-        v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-__device__ __forceinline__ float wsumf(float v)
-{
-    for (int o = 16; o > 0; o >>= 1)
-        v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// block partial of v into part[blockIdx*2 + slot] (fixed tree)
-__device__ __forceinline__ void block_partial(double v, double *part, int slot, double *sh)
-{
-    v = wsum(v);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0)
-        sh[w] = v;
-    __syncthreads();
-    if (w == 0)
-    {
-        double r = (l < (int)(blockDim.x >> 5)) ? sh[l] : 0.0;
-        r = wsum(r);
-        if (l == 0)
-            part[2 * blockIdx.x + slot] = r;
-    }
-    __syncthreads();
-}
-
-// L2 cache policies: the matrix and its columns are streamed once per iteration (evict-first,
-// no L1 allocation, read-only path); the Krylov vectors are gathered many times per iteration
-// and must stay in L2 (evict-last on their loads and stores).
-__device__ __forceinline__ uint64_t l2_evict_first()
-{
-    uint64_t p;
-    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-__device__ __forceinline__ uint64_t l2_evict_last()
-{
-    uint64_t p;
-    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-__device__ __forceinline__ double ld_stream(const double *a, uint64_t pol)
-{
-    double v;
-    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
-    return v;
-}
-__device__ __forceinline__ float ld_stream(const float *a, uint64_t pol)
-{
-    float v;
-    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
-    return v;
-}
-__device__ __forceinline__ int ld_stream(const int *a, uint64_t pol)
-{
-    int v;
-    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
-    return v;
-}
-// vectors change between phases: volatile keeps these loads where the code puts them
-__device__ __forceinline__ double ld_keep(const double *a, uint64_t pol)
-{
-    double v;
-    asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol) : "memory");
-    return v;
-}
-__device__ __forceinline__ float ld_keep(const float *a, uint64_t pol)
-{
-    float v;
-    asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_keep(double *a, double v, uint64_t pol)
-{
-    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol) : "memory");
-}
-__device__ __forceinline__ void st_keep(float *a, float v, uint64_t pol)
-{
-    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(pol) : "memory");
-}
-
-// q_i = sum_j K_ij (r_j + beta p_old_j) for the row at this lane of slice sl; returns the
-// particle id (-1 past the end).  Blocks in ascending connection order, entries row-major.
-template <typename TK, typename TV, int D>
-__device__ __forceinline__ int spmv_slice(int sl, int n, const int *__restrict__ rowptr, const int *__restrict__ perm,
-                                          const int64_t *__restrict__ slice_off, const int *__restrict__ col_sell,
-                                          const TK *__restrict__ K, const TV *__restrict__ r,
-                                          const TV *__restrict__ pold, TV beta, TV acc[D], uint64_t pf,
-                                          uint64_t pl)
-{
-    constexpr int E = D * D;
-    const int lane = threadIdx.x & 31;
-    const int pos = sl * kSlice + lane;
-    const bool valid = pos < n;
-    const int i = valid ? perm[pos] : -1;
-    const int myn = valid ? (rowptr[i + 1] - rowptr[i]) : 0;
-    const int64_t off = slice_off[sl];
-    const int w = (int)(slice_off[sl + 1] - off);
-    const int *cp = col_sell + off * kSlice + lane;
-    const TK *kp = K + off * E * kSlice + lane;
-#pragma unroll
-    for (int k = 0; k < D; ++k)
-        acc[k] = TV(0);
-    // the column of step k+1 is fetched during step k, so the x gathers never wait on it
-    int jn = (myn > 0) ? ld_stream(cp, pf) : 0;
-#pragma unroll 2
-    for (int k = 0; k < w; ++k)
-    {
-        const int j = jn;
-        if (k + 1 < myn)
-            jn = ld_stream(cp + (int64_t)(k + 1) * kSlice, pf);
-        if (k < myn)
-        {
-            TV xv[D];
-#pragma unroll
-            for (int c = 0; c < D; ++c)
-                xv[c] = ld_keep(r + (int64_t)j * D + c, pl) + beta * ld_keep(pold + (int64_t)j * D + c, pl);
-            const TK *kb = kp + (int64_t)k * E * kSlice;
-            TK kv[E];
-#pragma unroll
-            for (int e = 0; e < E; ++e)
-                kv[e] = ld_stream(kb + e * kSlice, pf);
-#pragma unroll
-            for (int rr = 0; rr < D; ++rr)
-#pragma unroll
-                for (int c = 0; c < D; ++c)
-                    acc[rr] += (TV)kv[rr * D + c] * xv[c];
-        }
-    }
-    return i;
 }
 
 template <typename TK, typename TV, int D>
@@ -545,31 +387,25 @@ static cudaError_t solve_dim(Problem &p, CGResult &out)
                                          -1.0, maxit, out, nullptr);
     // FP32 Krylov solve inside FP64 iterative refinement on the same stopping rule
     cudaError_t e;
-    const int nb_res = std::min(div_up(ndof, 256), 4 * p.num_sms);
     // rr0 = ||b||^2 via r = b - K*0
     if ((e = cudaMemsetAsync(p.x, 0, sizeof(double) * ndof, p.stream)) != cudaSuccess)
         return e;
-    double rr0 = 0, rr = 0;
     auto true_residual = [&](double &val) -> cudaError_t {
-        k_residual64<D><<<nb_res, 256, 0, p.stream>>>(p.n, p.nslices, p.cstart, p.perm, p.slice_off, p.col_sell, p.K,
-                                                      p.res, p.x, p.r, p.partials);
-        k_sum_partials<<<1, 256, 0, p.stream>>>(nb_res, p.partials, reinterpret_cast<double *>(p.cg_info) + 3);
-        p.ctr.kernel_launches += 2;
-        cudaError_t e2 = cudaMemcpyAsync(&val, reinterpret_cast<double *>(p.cg_info) + 3, sizeof(double),
-                                         cudaMemcpyDeviceToHost, p.stream);
-        if (e2 != cudaSuccess)
-            return e2;
-        return cudaStreamSynchronize(p.stream);
+        cudaError_t e2 = enqueue_true_residual(p);
+        if (e2 == cudaSuccess)
+            e2 = cudaStreamSynchronize(p.stream);
+        val = true_residual_result(p);
+        return e2;
     };
+    double rr0 = 0, rr = 0;
     if ((e = true_residual(rr0)) != cudaSuccess)
         return e;
     const double stop = p.desc.cg_rtol * rr0 + p.desc.cg_atol;
     rr = rr0;
-    const int gconv = std::min(div_up(ndof, 256), 8 * p.num_sms);
     for (int ref = 0; ref < 30 && !(rr <= stop); ++ref)
     {
-        k_convert<double, float><<<gconv, 256, 0, p.stream>>>(ndof, p.r, p.b32);
-        p.ctr.kernel_launches++;
+        if ((e = enqueue_r_to_b32(p)) != cudaSuccess)
+            return e;
         // the inner solve aims a little below the outer target, measured on its own residual
         CGResult inner;
         double rr_in = 0;
@@ -582,14 +418,55 @@ static cudaError_t solve_dim(Problem &p, CGResult &out)
         out.refinements++;
         if (inner.timeout)
             break;
-        k_add_f32<<<gconv, 256, 0, p.stream>>>(ndof, p.x32, p.x);
-        p.ctr.kernel_launches++;
+        if ((e = enqueue_add_x32(p)) != cudaSuccess)
+            return e;
         if ((e = true_residual(rr)) != cudaSuccess)
             return e;
         if (inner.iters == 0)
             break;
     }
     return cudaSuccess;
+}
+
+// r = b - K x (FP64 matrix) and ||r||^2 -> the pinned slot read by true_residual_result
+cudaError_t enqueue_true_residual(Problem &p)
+{
+    const int64_t ndof = (int64_t)p.n * p.dim;
+    const int nb_res = std::min(div_up(ndof, 256), 4 * p.num_sms);
+    double *dst = reinterpret_cast<double *>(p.cg_info) + 5;
+    if (p.dim == 2)
+        k_residual64<2><<<nb_res, 256, 0, p.stream>>>(p.n, p.nslices, p.cstart, p.perm, p.slice_off, p.col_sell, p.K,
+                                                      p.res, p.x, p.r, p.partials);
+    else
+        k_residual64<3><<<nb_res, 256, 0, p.stream>>>(p.n, p.nslices, p.cstart, p.perm, p.slice_off, p.col_sell, p.K,
+                                                      p.res, p.x, p.r, p.partials);
+    k_sum_partials<<<1, 256, 0, p.stream>>>(nb_res, p.partials, dst);
+    p.ctr.kernel_launches += 2;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return e;
+    return cudaMemcpyAsync(p.cg_info_host + 5, dst, sizeof(double), cudaMemcpyDeviceToHost, p.stream);
+}
+
+double true_residual_result(const Problem &p)
+{
+    return reinterpret_cast<const double *>(p.cg_info_host)[5];
+}
+
+cudaError_t enqueue_r_to_b32(Problem &p)
+{
+    const int64_t ndof = (int64_t)p.n * p.dim;
+    k_convert<double, float><<<std::min(div_up(ndof, 256), 8 * p.num_sms), 256, 0, p.stream>>>(ndof, p.r, p.b32);
+    p.ctr.kernel_launches++;
+    return cudaGetLastError();
+}
+
+cudaError_t enqueue_add_x32(Problem &p)
+{
+    const int64_t ndof = (int64_t)p.n * p.dim;
+    k_add_f32<<<std::min(div_up(ndof, 256), 8 * p.num_sms), 256, 0, p.stream>>>(ndof, p.x32, p.x);
+    p.ctr.kernel_launches++;
+    return cudaGetLastError();
 }
 
 __global__ void k_to_f32(int64_t m, const double *__restrict__ a, float *__restrict__ b)

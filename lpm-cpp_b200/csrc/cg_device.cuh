@@ -1,0 +1,176 @@
+// Device helpers shared by the CG kernels (cg.cu: one problem per launch; batch.cu: many
+// problems per launch): timed waits, fixed-order warp and block reductions, loads and stores
+// with L2 eviction policies, and the sliced-ELL SpMV of one slice.
+#pragma once
+
+#include <cstdint>
+
+#include "lpm_internal.cuh"
+
+namespace lpm
+{
+
+// one 32-warp block per SM: with <= 64 registers every slice of the 382,500-DOF cube gets its
+// own warp (3,985 slices, 4,736 resident warps) and each grid barrier takes 148 arrivals
+constexpr int kCGThreads = 1024;
+constexpr int kCGMinBlocks = 1;
+constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull; // 4 s
+
+__device__ __forceinline__ unsigned long long gtimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ double wsum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float wsumf(float v)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// block sum of v (fixed tree: warp butterflies, then warp 0 over the warp totals) into *dst
+__device__ __forceinline__ void block_partial_at(double v, double *dst, double *sh)
+{
+    v = wsum(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0)
+        sh[w] = v;
+    __syncthreads();
+    if (w == 0)
+    {
+        double r = (l < (int)(blockDim.x >> 5)) ? sh[l] : 0.0;
+        r = wsum(r);
+        if (l == 0)
+            *dst = r;
+    }
+    __syncthreads();
+}
+
+// block partial of v into part[blockIdx*2 + slot]
+__device__ __forceinline__ void block_partial(double v, double *part, int slot, double *sh)
+{
+    block_partial_at(v, part + 2 * blockIdx.x + slot, sh);
+}
+
+// L2 cache policies: the matrix and its columns are streamed once per iteration (evict-first,
+// no L1 allocation, read-only path); the Krylov vectors are gathered many times per iteration
+// and must stay in L2 (evict-last on their loads and stores).
+__device__ __forceinline__ uint64_t l2_evict_first()
+{
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_last()
+{
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ double ld_stream(const double *a, uint64_t pol)
+{
+    double v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float ld_stream(const float *a, uint64_t pol)
+{
+    float v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int ld_stream(const int *a, uint64_t pol)
+{
+    int v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+    return v;
+}
+// vectors change between phases: volatile keeps these loads where the code puts them
+__device__ __forceinline__ double ld_keep(const double *a, uint64_t pol)
+{
+    double v;
+    asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol) : "memory");
+    return v;
+}
+__device__ __forceinline__ float ld_keep(const float *a, uint64_t pol)
+{
+    float v;
+    asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_keep(double *a, double v, uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_keep(float *a, float v, uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(a), "f"(v), "l"(pol) : "memory");
+}
+
+// q_i = sum_j K_ij (r_j + beta p_old_j) for the row at this lane of slice sl; returns the
+// particle id (-1 past the end).  Blocks in ascending connection order, entries row-major.
+template <typename TK, typename TV, int D>
+__device__ __forceinline__ int spmv_slice(int sl, int n, const int *__restrict__ rowptr, const int *__restrict__ perm,
+                                          const int64_t *__restrict__ slice_off, const int *__restrict__ col_sell,
+                                          const TK *__restrict__ K, const TV *__restrict__ r,
+                                          const TV *__restrict__ pold, TV beta, TV acc[D], uint64_t pf,
+                                          uint64_t pl)
+{
+    constexpr int E = D * D;
+    const int lane = threadIdx.x & 31;
+    const int pos = sl * kSlice + lane;
+    const bool valid = pos < n;
+    const int i = valid ? perm[pos] : -1;
+    const int myn = valid ? (rowptr[i + 1] - rowptr[i]) : 0;
+    const int64_t off = slice_off[sl];
+    const int w = (int)(slice_off[sl + 1] - off);
+    const int *cp = col_sell + off * kSlice + lane;
+    const TK *kp = K + off * E * kSlice + lane;
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+        acc[k] = TV(0);
+    // the column of step k+1 is fetched during step k, so the x gathers never wait on it
+    int jn = (myn > 0) ? ld_stream(cp, pf) : 0;
+#pragma unroll 2
+    for (int k = 0; k < w; ++k)
+    {
+        const int j = jn;
+        if (k + 1 < myn)
+            jn = ld_stream(cp + (int64_t)(k + 1) * kSlice, pf);
+        if (k < myn)
+        {
+            TV xv[D];
+#pragma unroll
+            for (int c = 0; c < D; ++c)
+                xv[c] = ld_keep(r + (int64_t)j * D + c, pl) + beta * ld_keep(pold + (int64_t)j * D + c, pl);
+            const TK *kb = kp + (int64_t)k * E * kSlice;
+            TK kv[E];
+#pragma unroll
+            for (int e = 0; e < E; ++e)
+                kv[e] = ld_stream(kb + e * kSlice, pf);
+#pragma unroll
+            for (int rr = 0; rr < D; ++rr)
+#pragma unroll
+                for (int c = 0; c < D; ++c)
+                    acc[rr] += (TV)kv[rr * D + c] * xv[c];
+        }
+    }
+    return i;
+}
+
+} // namespace lpm

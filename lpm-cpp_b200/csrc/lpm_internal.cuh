@@ -137,6 +137,24 @@ struct CGResult
 // Solves K x = res (current residual) into p.x with the reference's stopping rule.
 cudaError_t solve_linear(Problem &p, CGResult &out);
 
+// Pieces of the mixed-precision refinement, enqueued on p.stream without a host wait:
+// r = res - K x with ||r||^2 copied to a pinned slot (read after the stream is synchronised),
+// b32 = (float) r, and x += x32.
+cudaError_t enqueue_true_residual(Problem &p);
+double true_residual_result(const Problem &p);
+cudaError_t enqueue_r_to_b32(Problem &p);
+cudaError_t enqueue_add_x32(Problem &p);
+
+// Host-wait-free pieces of the load step (solver.cu), for callers that drive many problems:
+// geometry + force state (+ updateRR) with the scalar record copied to p.scal_host; assembly
+// (+ the FP32 copy in mixed precision); J2 state update + static damage with the scalar record;
+// Assembly::storeStateVar / resetStateVar(true).
+cudaError_t enqueue_force_state(Problem &p, bool with_rr);
+cudaError_t enqueue_assemble(Problem &p, bool apply_bc);
+cudaError_t enqueue_damage_update(Problem &p);
+cudaError_t enqueue_store_state(Problem &p);
+cudaError_t enqueue_reset_state(Problem &p);
+
 // error text for lpmgpu_last_error
 void set_last_error(const std::string &s);
 
@@ -157,3 +175,9 @@ cudaError_t dalloc(Problem &p, T **ptr, size_t count)
 inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
 } // namespace lpm
+
+// the opaque handle of include/lpmgpu.h
+struct lpmgpu_solver
+{
+    lpm::Problem p;
+};

@@ -13,11 +13,6 @@
 
 #include "lpm_internal.cuh"
 
-struct lpmgpu_solver
-{
-    lpm::Problem p;
-};
-
 namespace lpm
 {
 
@@ -58,14 +53,41 @@ static int32_t sync_scalars(Problem &p)
     return LPMGPU_OK;
 }
 
+cudaError_t enqueue_force_state(Problem &p, bool with_rr)
+{
+    cudaError_t e = launch_geometry_force(p);
+    if (e == cudaSuccess)
+        e = launch_update_rr_impl(p, with_rr);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(p.scal_host, p.scal, sizeof(Scalars), cudaMemcpyDeviceToHost, p.stream);
+    return e;
+}
+
+cudaError_t enqueue_assemble(Problem &p, bool apply_bc)
+{
+    cudaError_t e = launch_assemble(p, apply_bc);
+    if (e == cudaSuccess && p.desc.precision == LPMGPU_MIXED)
+        e = launch_k_to_f32(p);
+    return e;
+}
+
+cudaError_t enqueue_damage_update(Problem &p)
+{
+    cudaError_t e = launch_update_state_var(p);
+    if (e == cudaSuccess)
+        e = launch_static_damage(p);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(p.scal_host, p.scal, sizeof(Scalars), cudaMemcpyDeviceToHost, p.stream);
+    return e;
+}
+
 // Assembly::updateGeometry + updateForceState (and updateRR when with_rr)
 static int32_t force_state(Problem &p, bool with_rr)
 {
     CK(cudaEventRecord(p.ev[0], p.stream));
-    CK(launch_geometry_force(p));
-    CK(launch_update_rr_impl(p, with_rr));
+    CK(enqueue_force_state(p, with_rr));
     CK(cudaEventRecord(p.ev[1], p.stream));
-    ST(sync_scalars(p));
+    CK(cudaStreamSynchronize(p.stream));
     float ms = 0;
     cudaEventElapsedTime(&ms, p.ev[0], p.ev[1]);
     p.phase_s[0] += ms * 1e-3;
@@ -76,9 +98,7 @@ static int32_t force_state(Problem &p, bool with_rr)
 static int32_t assemble(Problem &p, bool apply_bc)
 {
     CK(cudaEventRecord(p.ev[2], p.stream));
-    CK(launch_assemble(p, apply_bc));
-    if (p.desc.precision == LPMGPU_MIXED)
-        CK(launch_k_to_f32(p));
+    CK(enqueue_assemble(p, apply_bc));
     CK(cudaEventRecord(p.ev[3], p.stream));
     CK(cudaEventSynchronize(p.ev[3]));
     float ms = 0;
@@ -142,29 +162,45 @@ static int32_t newton(Problem &p, lpmgpu_stats *st, int *ni)
     return LPMGPU_OK;
 }
 
-static int32_t store_state(Problem &p)
+cudaError_t enqueue_store_state(Problem &p)
 {
     const size_t n = p.n, nb = (size_t)p.nbonds;
-    CK(cudaMemcpyAsync(p.xyz_last, p.xyz, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, p.stream));
-    CK(cudaMemcpyAsync(p.damage_last, p.damage, sizeof(double) * n, cudaMemcpyDeviceToDevice, p.stream));
-    CK(cudaMemcpyAsync(p.sv_last, p.sv, sizeof(double) * p.nsv * n, cudaMemcpyDeviceToDevice, p.stream));
-    CK(cudaMemcpyAsync(p.dis_last, p.dis, sizeof(double) * nb, cudaMemcpyDeviceToDevice, p.stream));
-    CK(cudaMemcpyAsync(p.bdamage_last, p.bdamage, sizeof(double) * nb, cudaMemcpyDeviceToDevice, p.stream));
-    CK(cudaMemcpyAsync(p.bforce_last, p.bforce, sizeof(double) * nb, cudaMemcpyDeviceToDevice, p.stream));
-    CK(cudaMemcpyAsync(p.dLp_last, p.dLp, sizeof(double) * nb, cudaMemcpyDeviceToDevice, p.stream));
+    cudaError_t e = cudaSuccess;
+    const std::pair<void *, const void *> cp[] = {{p.xyz_last, p.xyz},   {p.damage_last, p.damage},
+                                                  {p.sv_last, p.sv},     {p.dis_last, p.dis},
+                                                  {p.bdamage_last, p.bdamage}, {p.bforce_last, p.bforce},
+                                                  {p.dLp_last, p.dLp}};
+    const size_t bytes[] = {sizeof(double) * 3 * n, sizeof(double) * n, sizeof(double) * p.nsv * n,
+                            sizeof(double) * nb,    sizeof(double) * nb, sizeof(double) * nb, sizeof(double) * nb};
+    for (int k = 0; k < 7 && e == cudaSuccess; ++k)
+        e = cudaMemcpyAsync(cp[k].first, cp[k].second, bytes[k], cudaMemcpyDeviceToDevice, p.stream);
+    return e;
+}
+
+cudaError_t enqueue_reset_state(Problem &p)
+{
+    const size_t n = p.n, nb = (size_t)p.nbonds;
+    cudaError_t e = cudaSuccess;
+    const std::pair<void *, const void *> cp[] = {{p.xyz, p.xyz_last},   {p.damage, p.damage_last},
+                                                  {p.sv, p.sv_last},     {p.dis, p.dis_last},
+                                                  {p.bdamage, p.bdamage_last}, {p.bforce, p.bforce_last},
+                                                  {p.dLp, p.dLp_last}};
+    const size_t bytes[] = {sizeof(double) * 3 * n, sizeof(double) * n, sizeof(double) * p.nsv * n,
+                            sizeof(double) * nb,    sizeof(double) * nb, sizeof(double) * nb, sizeof(double) * nb};
+    for (int k = 0; k < 7 && e == cudaSuccess; ++k)
+        e = cudaMemcpyAsync(cp[k].first, cp[k].second, bytes[k], cudaMemcpyDeviceToDevice, p.stream);
+    return e;
+}
+
+static int32_t store_state(Problem &p)
+{
+    CK(enqueue_store_state(p));
     return LPMGPU_OK;
 }
 
 static int32_t reset_state(Problem &p)
 {
-    const size_t n = p.n, nb = (size_t)p.nbonds;
-    CK(cudaMemcpyAsync(p.xyz, p.xyz_last, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, p.stream));
-    CK(cudaMemcpyAsync(p.damage, p.damage_last, sizeof(double) * n, cudaMemcpyDeviceToDevice, p.stream));
-    CK(cudaMemcpyAsync(p.sv, p.sv_last, sizeof(double) * p.nsv * n, cudaMemcpyDeviceToDevice, p.stream));
-    CK(cudaMemcpyAsync(p.dis, p.dis_last, sizeof(double) * nb, cudaMemcpyDeviceToDevice, p.stream));
-    CK(cudaMemcpyAsync(p.bdamage, p.bdamage_last, sizeof(double) * nb, cudaMemcpyDeviceToDevice, p.stream));
-    CK(cudaMemcpyAsync(p.bforce, p.bforce_last, sizeof(double) * nb, cudaMemcpyDeviceToDevice, p.stream));
-    CK(cudaMemcpyAsync(p.dLp, p.dLp_last, sizeof(double) * nb, cudaMemcpyDeviceToDevice, p.stream));
+    CK(enqueue_reset_state(p));
     return LPMGPU_OK;
 }
 
@@ -481,11 +517,11 @@ int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
     kntv(p.cell, d->plane_stress, d->E, d->mu, p.kntv);
     const size_t n = p.n;
     CKF(cudaMallocHost(&p.scal_host, sizeof(Scalars)));
-    CKF(cudaMallocHost(&p.cg_info_host, 4 * sizeof(int64_t)));
+    CKF(cudaMallocHost(&p.cg_info_host, 8 * sizeof(int64_t)));
     CKF(dalloc(p, &p.scal, 1));
     CKF(dalloc(p, &p.partials, 2 * std::max<size_t>((size_t)kMaxGridBlocks, n / 64 + 1) + 16));
     CKF(dalloc(p, &p.barrier, 4));
-    CKF(dalloc(p, &p.cg_info, 4));
+    CKF(dalloc(p, &p.cg_info, 8));
     CKF(dalloc(p, &p.xyz, 3 * n));
     CKF(dalloc(p, &p.xyz_last, 3 * n));
     CKF(dalloc(p, &p.pin, 3 * n));

@@ -128,6 +128,20 @@ class Sizes(C.Structure):
                 ("device_bytes", C.c_int64)]
 
 
+class MemberInfo(C.Structure):
+    _fields_ = [("state", C.c_int32), ("status", C.c_int32), ("steps_done", C.c_int32), ("nsteps", C.c_int32),
+                ("total", Stats), ("dof_iters", C.c_int64), ("seconds", C.c_double)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("rounds", C.c_int64), ("cg_launches", C.c_int64), ("members_done", C.c_int64),
+                ("members_failed", C.c_int64), ("cg_iters", C.c_int64), ("dof_iters", C.c_int64),
+                ("seconds", C.c_double), ("cg_kernel_seconds", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib = None
 
 # every symbol declared in include/lpmgpu.h
@@ -139,6 +153,8 @@ EXPORTS = [
     "lpmgpu_solve_problem_step", "lpmgpu_solve_load_step", "lpmgpu_store_state", "lpmgpu_reset_state",
     "lpmgpu_read_state", "lpmgpu_read_residual", "lpmgpu_set_xyz", "lpmgpu_get_phase_times",
     "lpmgpu_get_counters", "lpmgpu_get_stream", "lpmgpu_cg_bsr_noalloc",
+    "lpmgpu_batch_create", "lpmgpu_batch_destroy", "lpmgpu_batch_add", "lpmgpu_batch_round", "lpmgpu_batch_run",
+    "lpmgpu_batch_member", "lpmgpu_batch_member_steps", "lpmgpu_batch_remove", "lpmgpu_batch_get_stats",
 ]
 
 
@@ -179,6 +195,15 @@ def lib():
         "lpmgpu_get_stream": (C.c_int32, [vp, C.POINTER(vp)]),
         "lpmgpu_cg_bsr_noalloc": (C.c_int32, [C.c_int32, C.c_int32, vp, vp, vp, vp, vp, C.c_double, C.c_double,
                                               C.c_int64, vp, C.POINTER(C.c_int64)]),
+        "lpmgpu_batch_create": (C.c_int32, [C.c_int32, C.POINTER(vp)]),
+        "lpmgpu_batch_destroy": (C.c_int32, [vp]),
+        "lpmgpu_batch_add": (C.c_int32, [vp, vp, C.POINTER(CLoadStep), C.c_int32, ip]),
+        "lpmgpu_batch_round": (C.c_int32, [vp, ip]),
+        "lpmgpu_batch_run": (C.c_int32, [vp]),
+        "lpmgpu_batch_member": (C.c_int32, [vp, C.c_int32, C.POINTER(MemberInfo)]),
+        "lpmgpu_batch_member_steps": (C.c_int32, [vp, C.c_int32, C.POINTER(Stats), C.c_int32, ip]),
+        "lpmgpu_batch_remove": (C.c_int32, [vp, C.c_int32]),
+        "lpmgpu_batch_get_stats": (C.c_int32, [vp, C.POINTER(BatchStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -582,6 +607,69 @@ class GpuProblem:
         t = np.zeros(4)
         _check(lib().lpmgpu_get_phase_times(self._h, _dp(t)), "lpmgpu_get_phase_times")
         return {"force_s": t[0], "assembly_s": t[1], "linear_s": t[2], "other_s": t[3]}
+
+
+class Batch:
+    """Many problems advanced together (lpmgpu_batch_*): each member runs its whole load path
+    as repeated GpuProblem.solve_load_step calls would, and all members' Newton systems of a
+    round go through one persistent CG launch."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().lpmgpu_batch_create(int(device), C.byref(h)), "lpmgpu_batch_create")
+        self._h = h
+        self._problems = {}
+
+    def add(self, problem: "GpuProblem", steps: Sequence[LoadStep]) -> int:
+        cs = [_CStep(s) for s in steps]
+        arr = (CLoadStep * max(len(cs), 1))(*[c.s for c in cs])
+        mid = C.c_int32(-1)
+        _check(lib().lpmgpu_batch_add(self._h, problem._h, arr, len(cs), C.byref(mid)), "lpmgpu_batch_add")
+        self._problems[mid.value] = problem
+        return mid.value
+
+    def round(self) -> int:
+        running = C.c_int32(0)
+        _check(lib().lpmgpu_batch_round(self._h, C.byref(running)), "lpmgpu_batch_round")
+        return running.value
+
+    def run(self):
+        _check(lib().lpmgpu_batch_run(self._h), "lpmgpu_batch_run")
+
+    def member(self, mid: int) -> dict:
+        info = MemberInfo()
+        _check(lib().lpmgpu_batch_member(self._h, int(mid), C.byref(info)), "lpmgpu_batch_member")
+        d = {k: getattr(info, k) for k, _ in MemberInfo._fields_ if k != "total"}
+        d["total"] = info.total.as_dict()
+        return d
+
+    def member_steps(self, mid: int) -> list:
+        cnt = C.c_int32(0)
+        _check(lib().lpmgpu_batch_member_steps(self._h, int(mid), None, 0, C.byref(cnt)), "lpmgpu_batch_member_steps")
+        arr = (Stats * max(cnt.value, 1))()
+        _check(lib().lpmgpu_batch_member_steps(self._h, int(mid), arr, cnt.value, C.byref(cnt)),
+               "lpmgpu_batch_member_steps")
+        return [arr[k].as_dict() for k in range(cnt.value)]
+
+    def remove(self, mid: int):
+        _check(lib().lpmgpu_batch_remove(self._h, int(mid)), "lpmgpu_batch_remove")
+        self._problems.pop(mid, None)
+
+    def stats(self) -> dict:
+        st = BatchStats()
+        _check(lib().lpmgpu_batch_get_stats(self._h, C.byref(st)), "lpmgpu_batch_get_stats")
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lpmgpu_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class _StiffnessView:

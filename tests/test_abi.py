@@ -54,6 +54,10 @@ def test_invalid_arguments_are_rejected():
                                      ang.ctypes.data_as(C.POINTER(C.c_double)), None, 0, C.byref(cnt)) == 1
     assert L.lpmgpu_destroy(None) == 1
     assert L.lpmgpu_solve_load_step(None, None, None) == 1
+    assert L.lpmgpu_batch_create(0, None) == 1
+    assert L.lpmgpu_batch_destroy(None) == 1
+    assert L.lpmgpu_batch_add(None, None, None, 0, None) == 1
+    assert L.lpmgpu_batch_round(None, None) == 1
 
 
 @pytest.mark.skipif(cuda_available(), reason="checks the no-device path")
@@ -61,6 +65,9 @@ def test_no_device_fails_loudly():
     case = CFG.hex_plate(size=1.0, radius=0.1, steps=1)
     with pytest.raises(LPM.LpmGpuError) as e:
         LPM.GpuProblem(case.assembly())
+    assert e.value.status in (2, 11)
+    with pytest.raises(LPM.LpmGpuError) as e:
+        LPM.Batch()
     assert e.value.status in (2, 11)
 
 

@@ -1,0 +1,133 @@
+"""Batched solving (lpmgpu_batch_*): every member gives the result it gives alone.
+
+Each case builds twin handles of the same problems.  One twin of each runs alone, load step by
+load step, through lpmgpu_solve_load_step (the plain path); the others run together as members
+of one batch, whose rounds send all pending Newton systems through one persistent CG launch.
+The CG partition differs between the two (the batched kernel splits the GPU among the members),
+so the two agree to rounding, not bit for bit.  Bars, with both sides solving tightly (CG
+squared-norm test 1e-24 relative, Newton 1e-9):
+  * FP64 members: per load step the same Newton solve count and cuts, the same broken bonds,
+    displacements within 1e-8 relative of the member alone;
+  * mixed-precision members: displacements within 1e-6 relative of the FP64 member alone;
+  * members added while others are running give the same results as well.
+"""
+import numpy as np
+import pytest
+
+from _util import CFG, LPM, gpu_problem, hetero_plate, rel
+
+pytestmark = pytest.mark.gpu
+
+TIGHT = dict(cg_rtol=1e-24, cg_atol=0.0, tol_iter=1e-9)
+FP64_TOL = 1e-8
+MIXED_TOL = 1e-6
+
+
+def _cases():
+    return [
+        CFG.hex_plate(size=3.0, radius=0.1, steps=3, total_disp=0.003),
+        CFG.sc_cube(size=2.4, radius=0.2, steps=3, total_disp=0.003),
+        CFG.sc_cube(size=2.0, radius=0.25, steps=3, total_disp=0.06, ptype=LPM.ParticleType.J2Plasticity,
+                    j2=(200.0, 0.0, 38714.0, 10.0)),
+        CFG.notched_plate(size=2.0, radius=0.1, crack=0.3, steps=6, total_disp=0.006),
+        hetero_plate(size=2.0, steps=2, total_disp=0.002),
+    ]
+
+
+def _cut_case():
+    # a Newton cap of 5 makes the full step fail, so it is halved (solver_static.h:78-87)
+    return CFG.hex_plate(size=2.0, radius=0.1, steps=1, total_disp=0.01)
+
+
+def _alone(case, precision=0, max_iter=None):
+    g = gpu_problem(case, precision=precision, max_iter=max_iter, **TIGHT)
+    steps = []
+    for s in range(len(case.steps)):
+        ok, st = g.solve_load_step(case.load_step(s))
+        assert ok
+        steps.append(st)
+    out = g.state()
+    g.close()
+    return out, steps
+
+
+def _check_member(case, batch, mid, g, ref_state, ref_steps, tol, compare_counts=True):
+    info = batch.member(mid)
+    assert info["state"] == 1 and info["status"] == 0, info
+    assert info["steps_done"] == len(case.steps)
+    steps = batch.member_steps(mid)
+    if compare_counts:
+        for s, (a, b) in enumerate(zip(steps, ref_steps)):
+            assert a["newton_solves"] == b["newton_solves"], (case.name, s, a, b)
+            assert a["cuts"] == b["cuts"], (case.name, s)
+    st = g.state()
+    e = rel(st["xyz"] - case.xyz, ref_state["xyz"] - case.xyz)
+    assert e <= tol, f"{case.name}: displacement rel err {e}"
+    if compare_counts:
+        assert np.array_equal(st["bdamage"] == 1.0, ref_state["bdamage"] == 1.0), case.name
+    return info
+
+
+def test_batch_fp64_members_match_alone():
+    cases = _cases() + [_cut_case()]
+    max_iters = [None] * (len(cases) - 1) + [5]
+    refs = [_alone(c, max_iter=mi) for c, mi in zip(cases, max_iters)]
+    batch = LPM.Batch()
+    gs, mids = [], []
+    for c, mi in zip(cases, max_iters):
+        g = gpu_problem(c, max_iter=mi, **TIGHT)
+        gs.append(g)
+        mids.append(batch.add(g, [c.load_step(s) for s in range(len(c.steps))]))
+    batch.run()
+    for c, g, mid, (ref_state, ref_steps) in zip(cases, gs, mids, refs):
+        _check_member(c, batch, mid, g, ref_state, ref_steps, FP64_TOL)
+    assert batch.member_steps(mids[-1])[0]["cuts"] > 0
+    st = batch.stats()
+    assert st["members_done"] == len(cases) and st["members_failed"] == 0
+    assert st["cg_launches"] > 0 and st["dof_iters"] > 0
+    batch.close()
+    for g in gs:
+        g.close()
+
+
+def test_batch_mixed_members_match_fp64_alone():
+    cases = _cases()[:3]
+    refs = [_alone(c) for c in cases]
+    batch = LPM.Batch()
+    gs, mids = [], []
+    for c in cases:
+        g = gpu_problem(c, precision=1, **TIGHT)
+        gs.append(g)
+        mids.append(batch.add(g, [c.load_step(s) for s in range(len(c.steps))]))
+    batch.run()
+    for c, g, mid, (ref_state, ref_steps) in zip(cases, gs, mids, refs):
+        info = _check_member(c, batch, mid, g, ref_state, ref_steps, MIXED_TOL, compare_counts=False)
+        assert info["total"]["refinements"] > 0
+    batch.close()
+    for g in gs:
+        g.close()
+
+
+def test_batch_members_join_while_others_run():
+    """Continuous batching: members added between rounds, while earlier members are mid-path."""
+    cases = _cases()
+    refs = [_alone(c) for c in cases]
+    batch = LPM.Batch()
+    gs = [gpu_problem(c, **TIGHT) for c in cases]
+    mids = [None] * len(cases)
+    mids[0] = batch.add(gs[0], [cases[0].load_step(s) for s in range(len(cases[0].steps))])
+    nxt, rounds = 1, 0
+    running = 1
+    while running > 0 or nxt < len(cases):
+        if nxt < len(cases) and rounds % 3 == 2:
+            mids[nxt] = batch.add(gs[nxt], [cases[nxt].load_step(s) for s in range(len(cases[nxt].steps))])
+            nxt += 1
+        running = batch.round()
+        rounds += 1
+        assert rounds < 100000
+    for c, g, mid, (ref_state, ref_steps) in zip(cases, gs, mids, refs):
+        _check_member(c, batch, mid, g, ref_state, ref_steps, FP64_TOL)
+        batch.remove(mid)
+    batch.close()
+    for g in gs:
+        g.close()
