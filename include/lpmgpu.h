@@ -261,6 +261,10 @@ int32_t lpmgpu_batch_member_steps(const lpmgpu_batch *b, int32_t member, lpmgpu_
 /* forgets a finished member (its handle stays with the caller) */
 int32_t lpmgpu_batch_remove(lpmgpu_batch *b, int32_t member);
 int32_t lpmgpu_batch_get_stats(const lpmgpu_batch *b, lpmgpu_batch_stats *st);
+/* CG iterations one batched launch runs before the solves still unfinished pause (they resume
+ * in the next round, so one long solve does not hold the other members); 0 = no limit.
+ * Default 512. */
+int32_t lpmgpu_batch_set_slice(lpmgpu_batch *b, int64_t iterations);
 
 #ifdef __cplusplus
 }

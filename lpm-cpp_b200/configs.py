@@ -218,3 +218,34 @@ def notched_plate(size=4.0, radius=0.1, crack=0.3, E=69e3, mu=0.3, critical_bstr
                          slit_exclusion(xyz, y_slit, box[0] - 1.0, box[0] + crack * size))
     c.meta["crack"] = (crack * size, y_slit)
     return c
+
+
+def batched_notched_plates(count=64, seed=20240604, steps=40, radius=0.1, side=(4.0, 25.0), crack=(0.2, 0.5),
+                           E=(60e3, 120e3), critical_bstrain=(1e-3, 3e-3), opening=0.45, crack_ref=1.5,
+                           tol_iter=1e-5, max_iter=30) -> List[Case]:
+    """Batched 2D damage workload: ``count`` single-edge-notched hexagonal plates of uneven size.
+    Per plate (seeded): side L log-uniform in ``side`` mm at radius 0.1 mm, slit length a uniform
+    in ``crack`` x L, E uniform in ``E`` MPa, nu = 0.3, critical bond stretch c uniform in
+    ``critical_bstrain``.  Mode I: bottom edge fixed, top edge pulled in y in ``steps`` equal
+    steps to a total opening of ``opening`` x c x L x min(1, sqrt(crack_ref / a)).
+    The square-root factor keeps the slit tip's loading (stress intensity ~ strain x sqrt(a))
+    about equal across sizes: the tip breaks bonds and the crack starts to grow in every plate,
+    but does not run through.  Larger loads (checked with the oracle and the plain GPU path)
+    leave particles hanging on single bonds or split the plate; K is then singular, CG runs to
+    its iteration cap and the reference's own path ends in NaN."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        L = float(np.exp(rng.uniform(np.log(side[0]), np.log(side[1]))))
+        L = round(L / (2 * radius)) * 2 * radius
+        a = float(rng.uniform(*crack))
+        e = float(rng.uniform(*E))
+        cs = float(rng.uniform(*critical_bstrain))
+        scale = min(1.0, math.sqrt(crack_ref / (a * L)))
+        c = notched_plate(size=L, radius=radius, crack=a, E=e, mu=0.3, critical_bstrain=cs, steps=steps,
+                          total_disp=opening * cs * L * scale, tol_iter=tol_iter, max_iter=max_iter)
+        c.name = f"sen{k:02d}_L{L:.1f}"
+        c.meta.update({"seed": seed, "index": k, "side": L, "crack_ratio": a, "E": e, "critical_bstrain": cs,
+                       "opening_scale": scale})
+        out.append(c)
+    return out

@@ -25,6 +25,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -40,8 +42,10 @@ constexpr int kMaxVirt = kMaxGridBlocks + kMaxBatch; // virtual blocks
 
 struct BInst
 {
-    int dim, n, nslices, pad;
+    int dim, n, nslices;
+    int fresh;          // 1: the solve starts here (r = b, x = 0); 0: it resumes a paused solve
     int64_t ndof, cost; // cost: matrix entries (slots x d^2), the split weight
+    int64_t it0;        // iterations the solve had done before this launch
     const int *rowptr, *perm;
     const int64_t *slice_off;
     const int *col_sell;
@@ -54,7 +58,8 @@ struct BInst
 struct BState
 {
     double rr, stop, alpha, beta, rr0, rr_final;
-    int64_t it, status; // status bits: 1 iteration cap, 4 breakdown (p.Ap == 0)
+    int64_t it, status; // iterations of the solve; status bits: 1 iteration cap, 4 breakdown
+                        // (p.Ap == 0), 8 paused at the end of the launch's iteration slice
 };
 
 struct BCtl
@@ -72,6 +77,7 @@ struct BArgs
     int *act, *gcnt, *vstart; // per active rank [kMaxBatch]
     int *vinst, *vk, *vg;     // per virtual block [kMaxVirt]
     double *part;             // per virtual block [kMaxVirt]
+    int64_t slice;            // iterations per launch; unfinished solves pause and resume later
 };
 
 // virtual blocks of one problem: its share of G by matrix size, at least 1, at most its slices
@@ -157,7 +163,9 @@ __device__ void batch_decide(const BArgs &a, int mode, int64_t it)
             volatile BState *S = a.st + m;
             const BInst &I = a.inst[m];
             int keep = 1;
-            if (mode == 0)
+            if (mode == 0 && !I.fresh)
+                keep = 1; // resumed: rr, beta, stop carried over from the pause
+            else if (mode == 0)
             {
                 const double stop = (I.abs_stop >= 0) ? I.abs_stop : I.rtol * tot + I.atol;
                 S->rr = tot;
@@ -172,7 +180,7 @@ __device__ void batch_decide(const BArgs &a, int mode, int64_t it)
             {
                 if (tot == 0.0)
                 {
-                    S->it = it - 1;
+                    S->it = I.it0 + it - 1;
                     S->status |= 4;
                     S->rr_final = S->rr;
                     keep = 0;
@@ -182,11 +190,12 @@ __device__ void batch_decide(const BArgs &a, int mode, int64_t it)
             }
             else
             {
+                const int64_t itg = I.it0 + it;
                 const bool done = tot <= S->stop;
-                const bool capped = it >= I.maxit;
+                const bool capped = itg >= I.maxit;
                 if (done || capped)
                 {
-                    S->it = it;
+                    S->it = itg;
                     S->rr_final = tot;
                     if (!done)
                         S->status |= 1;
@@ -196,6 +205,13 @@ __device__ void batch_decide(const BArgs &a, int mode, int64_t it)
                 {
                     S->beta = tot / S->rr;
                     S->rr = tot;
+                    if (it >= a.slice)
+                    {
+                        S->it = itg;
+                        S->rr_final = tot;
+                        S->status |= 8;
+                        keep = 0;
+                    }
                 }
             }
             s_keep[r] = keep;
@@ -327,13 +343,13 @@ __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg_batch(BArgs a)
     const int warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const uint64_t pf = l2_evict_first(), pl = l2_evict_last();
 
-    // r = b, x = 0, p_old = 0; partial ||b||^2
+    // fresh solves: r = b, x = 0, p_old = 0; partial ||b||^2 (resumed solves keep their vectors)
     int nvirt = *reinterpret_cast<volatile int *>(&a.ctl->nvirt);
     for (int v = blockIdx.x; v < nvirt; v += gridDim.x)
     {
         const int m = __ldcg(a.vinst + v), k = __ldcg(a.vk + v), g = __ldcg(a.vg + v);
         const BInst &I = a.inst[m];
-        const int64_t lo = k * I.ndof / g, hi = (k + 1) * I.ndof / g;
+        const int64_t lo = I.fresh ? k * I.ndof / g : 0, hi = I.fresh ? (k + 1) * I.ndof / g : 0;
         const TV *b = static_cast<const TV *>(I.b);
         TV *x = static_cast<TV *>(I.x), *r = static_cast<TV *>(I.r), *pa = static_cast<TV *>(I.pa);
         double loc = 0;
@@ -354,13 +370,13 @@ __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg_batch(BArgs a)
     {
         if (*reinterpret_cast<volatile int *>(&a.ctl->nact) == 0)
             return;
-        const bool odd = (it & 1) != 0;
         // phase A: q = K p_new over this block's virtual blocks
         nvirt = *reinterpret_cast<volatile int *>(&a.ctl->nvirt);
         for (int v = blockIdx.x; v < nvirt; v += gridDim.x)
         {
             const int m = __ldcg(a.vinst + v), k = __ldcg(a.vk + v), g = __ldcg(a.vg + v);
             const BInst &I = a.inst[m];
+            const bool odd = ((I.it0 + it) & 1) != 0; // the solve's own iteration number
             const TV beta = (TV)__ldcg(&a.st[m].beta);
             const TV *pold = static_cast<const TV *>(odd ? I.pa : I.pb);
             TV *pnew = static_cast<TV *>(odd ? I.pb : I.pa);
@@ -386,6 +402,7 @@ __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg_batch(BArgs a)
         {
             const int m = __ldcg(a.vinst + v), k = __ldcg(a.vk + v), g = __ldcg(a.vg + v);
             const BInst &I = a.inst[m];
+            const bool odd = ((I.it0 + it) & 1) != 0;
             const TV al = (TV)__ldcg(&a.st[m].alpha);
             const TV *pnew = static_cast<const TV *>(odd ? I.pb : I.pa);
             TV *x = static_cast<TV *>(I.x), *r = static_cast<TV *>(I.r);
@@ -413,11 +430,14 @@ struct BatchItem
     bool fp32;
     double rtol, atol, abs_stop;
     int64_t maxit;
+    bool fresh;     // false: resume the paused solve whose state is `resume`
+    BState resume;
 };
 
 struct BatchCtx
 {
     int device = 0, num_sms = 0, grid = 0;
+    int64_t slice = 512; // CG iterations per launch before unfinished solves pause
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_done = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
     std::vector<cudaEvent_t> ev_in; // one per item slot
@@ -525,6 +545,8 @@ struct BatchCtx
             BInst &I = h_inst[m];
             std::memset(&I, 0, sizeof(I));
             I.dim = p.dim;
+            I.fresh = items[m].fresh ? 1 : 0;
+            I.it0 = items[m].fresh ? 0 : items[m].resume.it;
             I.n = p.n;
             I.nslices = p.nslices;
             I.ndof = (int64_t)p.n * p.dim;
@@ -577,7 +599,16 @@ struct BatchCtx
             }
             V += g;
         }
-        std::memset(h_st, 0, sizeof(BState) * items.size());
+        for (int m = 0; m < ni; ++m)
+        {
+            if (items[m].fresh)
+                std::memset(&h_st[m], 0, sizeof(BState));
+            else
+            {
+                h_st[m] = items[m].resume;
+                h_st[m].status &= ~int64_t(8);
+            }
+        }
         std::memset(h_ctl, 0, sizeof(BCtl));
         h_ctl->nvirt = V;
         h_ctl->nact = ni;
@@ -611,6 +642,7 @@ struct BatchCtx
         a.vk = a.vinst + kMaxVirt;
         a.vg = a.vk + kMaxVirt;
         a.part = d_part;
+        a.slice = slice > 0 ? slice : (int64_t(1) << 62);
         void *args[] = {&a};
         if ((e = cudaEventRecord(ev_t0, stream)) != cudaSuccess)
             return e;
@@ -690,11 +722,13 @@ enum class Ph
     Start,       // next sub-step (or next load step) to begin
     NewtonFirst, // force state of the first Newton check in flight
     Newton,      // force state after a Newton update in flight
-    NeedCG,      // needs a linear solve this round
+    NeedCG,      // a CG (FP64, or the FP32 inner solve of a refinement) to start or resume
     DamageCheck, // J2 state + static damage in flight
     Done,
-    Failed
+    Failed,
+    IRCheck      // mixed precision: x += x32 and the true residual in flight
 };
+constexpr int kPhases = 8;
 
 struct Member
 {
@@ -714,9 +748,12 @@ struct Member
     int64_t dof_iters = 0;
     int32_t status = LPMGPU_OK;
     std::chrono::steady_clock::time_point t_add, t_done;
-    // mixed-precision refinement of the current linear solve
+    // the CG in progress (it may span several launches) and the mixed-precision refinement
+    bool ls_fresh = true;
+    BState ls_state{};
     double ir_stop = 0, ir_rr = 0;
     int ir_ref = 0;
+    int64_t ir_inner_iters = 0;
 };
 
 int32_t cuda_status(cudaError_t e, const char *what)
@@ -733,6 +770,7 @@ struct lpmgpu_batch
     std::vector<std::unique_ptr<Member>> members; // index = member id; removed -> null
     lpmgpu_batch_stats stats{};
     std::chrono::steady_clock::time_point t_create;
+    int64_t round_max_it = 0; // most CG iterations one member ran in this round's launches
 
     Problem &P(Member &m) { return m.h->p; }
 
@@ -864,7 +902,58 @@ struct lpmgpu_batch
             return after_newton(m, m.k);
         if (++m.k > p.desc.max_iter)
             return after_newton(m, p.desc.max_iter);
+        return start_linear(m);
+    }
+
+    // one linear solve K x = res: FP64 CG, or (mixed) FP32 inner CGs inside an FP64 refinement
+    // on the same squared-norm rule (the loop of solve_dim in cg.cu).  With x = 0 the first true
+    // residual is res itself, whose squared norm the force state just delivered (updateRR), so
+    // the first inner solve starts at once from b32 = (float) res.
+    int32_t start_linear(Member &m)
+    {
+        Problem &p = P(m);
+        m.cur.newton_solves++;
+        m.ls_fresh = true;
+        if (p.desc.precision != LPMGPU_MIXED)
+        {
+            m.ph = Ph::NeedCG;
+            return LPMGPU_OK;
+        }
+        m.ir_ref = 0;
+        m.ir_rr = p.scal_host->res_sq;
+        m.ir_stop = p.desc.cg_rtol * m.ir_rr + p.desc.cg_atol;
+        cudaError_t e = cudaMemsetAsync(p.x, 0, sizeof(double) * (size_t)p.n * p.dim, p.stream);
+        if (e != cudaSuccess)
+            return fail_member(m, cuda_status(e, "batched refinement"));
+        if (m.ir_rr <= m.ir_stop)
+            return finish_linear(m);
+        if ((e = enqueue_res_to_b32(p)) != cudaSuccess)
+            return fail_member(m, cuda_status(e, "batched refinement"));
         m.ph = Ph::NeedCG;
+        return LPMGPU_OK;
+    }
+
+    int32_t next_inner(Member &m)
+    {
+        cudaError_t e = enqueue_r_to_b32(P(m));
+        if (e != cudaSuccess)
+            return fail_member(m, cuda_status(e, "batched refinement"));
+        m.ls_fresh = true;
+        m.ph = Ph::NeedCG;
+        return LPMGPU_OK;
+    }
+
+    // Newton update with the solution and the next force state
+    int32_t finish_linear(Member &m)
+    {
+        Problem &p = P(m);
+        cudaError_t e = launch_add_disp(p);
+        if (e == cudaSuccess)
+            e = enqueue_force_state(p, true);
+        if (e != cudaSuccess)
+            return fail_member(m, cuda_status(e, "batch Newton update"));
+        m.ph = Ph::Newton;
+        m.pending = true;
         return LPMGPU_OK;
     }
 
@@ -887,6 +976,11 @@ struct lpmgpu_batch
         case Ph::Newton:
             m.nres = std::sqrt(p.scal_host->res_sq);
             return newton_check(m);
+        case Ph::IRCheck:
+            m.ir_rr = true_residual_result(p);
+            if (m.ir_inner_iters == 0 || m.ir_rr <= m.ir_stop || m.ir_ref >= 30)
+                return finish_linear(m);
+            return next_inner(m);
         case Ph::DamageCheck:
         {
             const bool new_damaged = p.scal_host->any_flag != 0;
@@ -928,177 +1022,140 @@ struct lpmgpu_batch
         return cudaSuccess;
     }
 
-    // the linear solves of this round: FP64 members in one batched launch; mixed members in
-    // FP32 batched launches inside their own FP64 refinements (the rule of solve_dim)
-    int32_t linear_solves(std::vector<Member *> &cg64, std::vector<Member *> &cgmix)
+    // One batched launch over the members of one precision that need a CG this round (fresh
+    // solves and solves paused by the previous launch's iteration slice).
+    int32_t cg_launch(std::vector<Member *> &ms, bool fp32)
     {
-        cudaError_t e;
-        if (!cg64.empty())
+        if (ms.empty())
+            return LPMGPU_OK;
+        std::vector<BatchItem> items;
+        for (Member *m : ms)
         {
-            std::vector<BatchItem> items;
-            for (Member *m : cg64)
-            {
-                Problem &p = P(*m);
-                const int64_t ndof = (int64_t)p.n * p.dim;
-                items.push_back({&p, false, p.desc.cg_rtol, p.desc.cg_atol, -1.0,
-                                 p.desc.cg_maxit > 0 ? p.desc.cg_maxit : ndof});
-            }
-            if ((e = ctx.launch(items)) != cudaSuccess)
-                return cuda_status(e, "batched CG launch");
-            if ((e = cudaStreamSynchronize(ctx.stream)) != cudaSuccess)
-                return cuda_status(e, "batched CG");
-            ctx.account();
-            const bool timeout = ctx.h_ctl->fail != 0;
-            for (size_t q = 0; q < cg64.size(); ++q)
-            {
-                Member &m = *cg64[q];
-                const BState &S = ctx.h_st[q];
-                Problem &p = P(m);
-                m.cur.newton_solves++;
-                m.cur.cg_iters += S.it;
-                m.dof_iters += S.it * (int64_t)p.n * p.dim;
-                p.ctr.cg_iters += S.it;
-                if (S.status & 1)
-                    m.cur.cg_maxit_hits++;
-                if (timeout)
-                {
-                    set_last_error("a device-side barrier wait timed out in the batched CG kernel");
-                    fail_member(m, LPMGPU_ERR_TIMEOUT);
-                }
-            }
-            stats.cg_launches++;
+            Problem &p = P(*m);
+            const int64_t ndof = (int64_t)p.n * p.dim;
+            BatchItem it{&p, fp32, fp32 ? 0.0 : p.desc.cg_rtol, fp32 ? 0.0 : p.desc.cg_atol,
+                         fp32 ? 0.25 * m->ir_stop : -1.0, p.desc.cg_maxit > 0 ? p.desc.cg_maxit : ndof, m->ls_fresh,
+                         m->ls_state};
+            items.push_back(it);
         }
-        if (!cgmix.empty())
+        cudaError_t e = ctx.launch(items);
+        if (e != cudaSuccess)
+            return cuda_status(e, "batched CG launch");
+        if ((e = cudaStreamSynchronize(ctx.stream)) != cudaSuccess)
+            return cuda_status(e, "batched CG");
+        ctx.account();
+        stats.cg_launches++;
+        const bool timeout = ctx.h_ctl->fail != 0;
+        for (size_t q = 0; q < ms.size(); ++q)
         {
-            // x = 0, r = b, rr0 = ||b||^2 for every member
-            for (Member *m : cgmix)
+            Member &m = *ms[q];
+            Problem &p = P(m);
+            const BState &S = ctx.h_st[q];
+            const int64_t before = m.ls_fresh ? 0 : m.ls_state.it;
+            const int64_t done_now = S.it - before;
+            round_max_it = std::max(round_max_it, done_now);
+            m.cur.cg_iters += done_now;
+            m.dof_iters += done_now * (int64_t)p.n * p.dim;
+            p.ctr.cg_iters += done_now;
+            m.ls_state = S;
+            if (timeout)
             {
-                Problem &p = P(*m);
-                if ((e = cudaMemsetAsync(p.x, 0, sizeof(double) * (size_t)p.n * p.dim, p.stream)) != cudaSuccess ||
-                    (e = enqueue_true_residual(p)) != cudaSuccess)
-                    return cuda_status(e, "batched refinement");
+                set_last_error("a device-side barrier wait timed out in the batched CG kernel");
+                fail_member(m, LPMGPU_ERR_TIMEOUT);
+                continue;
             }
-            if ((e = sync_members(cgmix)) != cudaSuccess)
-                return cuda_status(e, "batched refinement");
-            std::vector<Member *> act;
-            for (Member *m : cgmix)
+            if (S.status & 8)
             {
-                Problem &p = P(*m);
-                m->ir_rr = true_residual_result(p);
-                m->ir_stop = p.desc.cg_rtol * m->ir_rr + p.desc.cg_atol;
-                m->ir_ref = 0;
-                m->cur.newton_solves++;
-                if (!(m->ir_rr <= m->ir_stop))
-                    act.push_back(m);
+                m.ls_fresh = false; // paused: resumes in the next round
+                continue;
             }
-            while (!act.empty())
+            if (S.status & 1)
+                m.cur.cg_maxit_hits++;
+            if (!fp32)
             {
-                std::vector<BatchItem> items;
-                for (Member *m : act)
-                {
-                    Problem &p = P(*m);
-                    if ((e = enqueue_r_to_b32(p)) != cudaSuccess)
-                        return cuda_status(e, "batched refinement");
-                    const int64_t ndof = (int64_t)p.n * p.dim;
-                    items.push_back({&p, true, 0.0, 0.0, 0.25 * m->ir_stop,
-                                     p.desc.cg_maxit > 0 ? p.desc.cg_maxit : ndof});
-                }
-                if ((e = ctx.launch(items)) != cudaSuccess)
-                    return cuda_status(e, "batched CG launch");
-                stats.cg_launches++;
-                for (Member *m : act)
-                    if ((e = enqueue_add_x32(P(*m))) != cudaSuccess || (e = enqueue_true_residual(P(*m))) != cudaSuccess)
-                        return cuda_status(e, "batched refinement");
-                if ((e = cudaStreamSynchronize(ctx.stream)) != cudaSuccess || (e = sync_members(act)) != cudaSuccess)
-                    return cuda_status(e, "batched refinement");
-                ctx.account();
-                const bool timeout = ctx.h_ctl->fail != 0;
-                std::vector<Member *> next;
-                for (size_t q = 0; q < act.size(); ++q)
-                {
-                    Member &m = *act[q];
-                    Problem &p = P(m);
-                    const BState &S = ctx.h_st[q];
-                    m.cur.cg_iters += S.it;
-                    m.dof_iters += S.it * (int64_t)p.n * p.dim;
-                    p.ctr.cg_iters += S.it;
-                    m.cur.refinements++;
-                    if (S.status & 1)
-                        m.cur.cg_maxit_hits++;
-                    m.ir_rr = true_residual_result(p);
-                    m.ir_ref++;
-                    if (timeout)
-                    {
-                        set_last_error("a device-side barrier wait timed out in the batched CG kernel");
-                        fail_member(m, LPMGPU_ERR_TIMEOUT);
-                        continue;
-                    }
-                    if (!(m.ir_rr <= m.ir_stop) && S.it > 0 && m.ir_ref < 30)
-                        next.push_back(&m);
-                }
-                act.swap(next);
+                finish_linear(m);
+                continue;
             }
+            // an inner solve finished: x += x32, new true residual (solve_dim's loop body)
+            m.ir_ref++;
+            m.cur.refinements++;
+            m.ir_inner_iters = S.it;
+            e = enqueue_add_x32(p);
+            if (e == cudaSuccess)
+                e = enqueue_true_residual(p);
+            if (e != cudaSuccess)
+            {
+                fail_member(m, cuda_status(e, "batched refinement"));
+                continue;
+            }
+            m.ph = Ph::IRCheck;
+            m.pending = true;
         }
-        // Newton update and the next force state
-        for (auto *list : {&cg64, &cgmix})
-            for (Member *m : *list)
-            {
-                if (m->ph == Ph::Failed)
-                    continue;
-                Problem &p = P(*m);
-                cudaError_t e2 = launch_add_disp(p);
-                if (e2 == cudaSuccess)
-                    e2 = enqueue_force_state(p, true);
-                if (e2 != cudaSuccess)
-                {
-                    fail_member(*m, cuda_status(e2, "batch Newton update"));
-                    continue;
-                }
-                m->ph = Ph::Newton;
-                m->pending = true;
-            }
         return LPMGPU_OK;
     }
 
     int32_t round(int32_t *running)
     {
+        static const bool log = std::getenv("LPMGPU_LOG") != nullptr;
+        const auto t_round = std::chrono::steady_clock::now();
+        const double k0 = ctx.kernel_seconds;
+        const int64_t l0 = stats.cg_launches;
+        round_max_it = 0;
         stats.rounds++;
-        // A: members that can start their next sub-step
-        for (auto &up : members)
-        {
-            if (!up)
-                continue;
-            Member &m = *up;
-            if (m.ph == Ph::Start)
-            {
-                cudaSetDevice(P(m).device);
-                begin_substep(m);
-            }
-        }
-        // B: linear solves
+        // A: CG launches for the members waiting for one (FP64 solves, then the FP32 inner
+        // solves of mixed members); finished solves enqueue their follow-up work
         std::vector<Member *> cg64, cgmix;
         for (auto &up : members)
             if (up && up->ph == Ph::NeedCG)
                 (P(*up).desc.precision == LPMGPU_MIXED ? cgmix : cg64).push_back(up.get());
-        int32_t r = linear_solves(cg64, cgmix);
+        int32_t r = cg_launch(cg64, false);
+        if (r == LPMGPU_OK)
+            r = cg_launch(cgmix, true);
         if (r != LPMGPU_OK)
             return r;
-        // C: one wait for every member's scalars, then the host decisions
-        std::vector<Member *> pend;
-        for (auto &up : members)
-            if (up && up->pending)
-                pend.push_back(up.get());
-        cudaError_t e = sync_members(pend);
-        if (e != cudaSuccess)
-            return cuda_status(e, "batch round");
-        for (Member *m : pend)
-            resolve(*m);
+        // B: until every member waits for a CG (or is finished): start sub-steps, wait once for
+        // all members' pending scalars, take their decisions, repeat
+        for (int pass = 0; pass < 1000; ++pass)
+        {
+            for (auto &up : members)
+                if (up && up->ph == Ph::Start)
+                {
+                    cudaSetDevice(P(*up).device);
+                    begin_substep(*up);
+                }
+            std::vector<Member *> pend;
+            for (auto &up : members)
+                if (up && up->pending)
+                    pend.push_back(up.get());
+            if (pend.empty())
+                break;
+            cudaError_t e = sync_members(pend);
+            if (e != cudaSuccess)
+                return cuda_status(e, "batch round");
+            for (Member *m : pend)
+                resolve(*m);
+        }
         int32_t live = 0;
         for (auto &up : members)
             if (up && up->ph != Ph::Done && up->ph != Ph::Failed)
                 live++;
         if (running)
             *running = live;
+        if (log)
+        {
+            const int64_t maxit = round_max_it;
+            int nph[kPhases] = {0};
+            for (auto &up : members)
+                if (up)
+                    nph[(int)up->ph]++;
+            std::fprintf(stderr,
+                         "lpmgpu batch round %lld: cg64=%zu cgmix=%zu launches=%lld max_it=%lld kernel_ms=%.3f "
+                         "round_ms=%.3f phases(start,nf,n,cg,dmg,done,fail,irc)=%d,%d,%d,%d,%d,%d,%d,%d\n",
+                         (long long)stats.rounds, cg64.size(), cgmix.size(), (long long)(stats.cg_launches - l0),
+                         (long long)maxit, (ctx.kernel_seconds - k0) * 1e3,
+                         std::chrono::duration<double>(std::chrono::steady_clock::now() - t_round).count() * 1e3,
+                         nph[0], nph[1], nph[2], nph[3], nph[4], nph[5], nph[6], nph[7]);
+        }
         return LPMGPU_OK;
     }
 };
@@ -1259,6 +1316,14 @@ int32_t lpmgpu_batch_remove(lpmgpu_batch *b, int32_t member)
         return LPMGPU_ERR_NOT_READY;
     }
     b->members[member].reset();
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_batch_set_slice(lpmgpu_batch *b, int64_t iterations)
+{
+    if (!b || iterations < 0)
+        return LPMGPU_ERR_INVALID_ARG;
+    b->ctx.slice = iterations;
     return LPMGPU_OK;
 }
 

@@ -461,6 +461,14 @@ cudaError_t enqueue_r_to_b32(Problem &p)
     return cudaGetLastError();
 }
 
+cudaError_t enqueue_res_to_b32(Problem &p)
+{
+    const int64_t ndof = (int64_t)p.n * p.dim;
+    k_convert<double, float><<<std::min(div_up(ndof, 256), 8 * p.num_sms), 256, 0, p.stream>>>(ndof, p.res, p.b32);
+    p.ctr.kernel_launches++;
+    return cudaGetLastError();
+}
+
 cudaError_t enqueue_add_x32(Problem &p)
 {
     const int64_t ndof = (int64_t)p.n * p.dim;

@@ -143,6 +143,7 @@ cudaError_t solve_linear(Problem &p, CGResult &out);
 cudaError_t enqueue_true_residual(Problem &p);
 double true_residual_result(const Problem &p);
 cudaError_t enqueue_r_to_b32(Problem &p);
+cudaError_t enqueue_res_to_b32(Problem &p); // b32 = (float) res: the first refinement, x = 0
 cudaError_t enqueue_add_x32(Problem &p);
 
 // Host-wait-free pieces of the load step (solver.cu), for callers that drive many problems:

@@ -155,6 +155,7 @@ EXPORTS = [
     "lpmgpu_get_counters", "lpmgpu_get_stream", "lpmgpu_cg_bsr_noalloc",
     "lpmgpu_batch_create", "lpmgpu_batch_destroy", "lpmgpu_batch_add", "lpmgpu_batch_round", "lpmgpu_batch_run",
     "lpmgpu_batch_member", "lpmgpu_batch_member_steps", "lpmgpu_batch_remove", "lpmgpu_batch_get_stats",
+    "lpmgpu_batch_set_slice",
 ]
 
 
@@ -204,6 +205,7 @@ def lib():
         "lpmgpu_batch_member_steps": (C.c_int32, [vp, C.c_int32, C.POINTER(Stats), C.c_int32, ip]),
         "lpmgpu_batch_remove": (C.c_int32, [vp, C.c_int32]),
         "lpmgpu_batch_get_stats": (C.c_int32, [vp, C.POINTER(BatchStats)]),
+        "lpmgpu_batch_set_slice": (C.c_int32, [vp, C.c_int64]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -627,6 +629,10 @@ class Batch:
         _check(lib().lpmgpu_batch_add(self._h, problem._h, arr, len(cs), C.byref(mid)), "lpmgpu_batch_add")
         self._problems[mid.value] = problem
         return mid.value
+
+    def set_slice(self, iterations: int):
+        """CG iterations per batched launch before unfinished solves pause (0: no limit)."""
+        _check(lib().lpmgpu_batch_set_slice(self._h, int(iterations)), "lpmgpu_batch_set_slice")
 
     def round(self) -> int:
         running = C.c_int32(0)

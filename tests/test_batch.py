@@ -131,3 +131,26 @@ def test_batch_members_join_while_others_run():
     batch.close()
     for g in gs:
         g.close()
+
+
+@pytest.mark.parametrize("precision,tol", [(0, FP64_TOL), (1, MIXED_TOL)])
+def test_batch_paused_solves_resume(precision, tol):
+    """A launch runs at most `slice` CG iterations; unfinished solves pause and resume in the
+    next round with their Krylov state.  A 7-iteration slice makes every solve pause many
+    times; the results still match the members alone."""
+    cases = _cases()[:4]
+    refs = [_alone(c) for c in cases]
+    batch = LPM.Batch()
+    batch.set_slice(7)
+    gs, mids = [], []
+    for c in cases:
+        g = gpu_problem(c, precision=precision, **TIGHT)
+        gs.append(g)
+        mids.append(batch.add(g, [c.load_step(s) for s in range(len(c.steps))]))
+    batch.run()
+    for c, g, mid, (ref_state, ref_steps) in zip(cases, gs, mids, refs):
+        _check_member(c, batch, mid, g, ref_state, ref_steps, tol, compare_counts=(precision == 0))
+    assert batch.stats()["cg_launches"] > 20
+    batch.close()
+    for g in gs:
+        g.close()
