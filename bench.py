@@ -55,6 +55,8 @@ def args_():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-cg-cap", type=int, default=400, help="CG iterations per solve in the CPU sample")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched 64-plate damage workload")
+    ap.add_argument("--plates", type=int, default=64, help="plates in the batched damage workload")
     return ap.parse_args()
 
 
@@ -307,6 +309,11 @@ def run_ours(a):
                  "speedup_vs_fp64": (ms_max / K) / (mms / K)}
         pm.close()
 
+    batched = None
+    if not a.no_batched:
+        barrier()
+        batched = batched_leg(lpm, a.plates, local, world, allreduce)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(case, a.cpu_cg_cap)
@@ -328,12 +335,88 @@ def run_ours(a):
                                    "force": (c1["force_seconds"] - c0["force_seconds"]) * 1e3 / K,
                                    "cg_kernel": cg_s * 1e3 / K},
             "roofline": roof, "e2e": e2e, "gpu_launches": counters_total, "clocks": clocks,
-            "mixed": mixed, "cpu_baseline": cpu,
+            "mixed": mixed, "batched": batched, "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def batched_leg(lpm, count, device, world, allreduce):
+    """Batched 2D damage workload (lpm-cpp_b200/configs.batched_notched_plates): `count` seeded
+    single-edge-notched hexagonal plates of uneven size, 40 Mode-I steps each, solved (1) one
+    plate at a time on the plain FP64 path, (2) all together by one batch in FP64, (3) all
+    together by one batch in mixed precision.  A solve is one plate's whole 40-step path.
+    Wall time around the host calls (the batch is host-driven); problem creation is outside
+    the timed regions.  Errors: final displacement of each plate against the plain FP64 path."""
+    import torch
+    cfg = importlib.import_module("lpm-cpp_b200.configs")
+    cases = cfg.batched_notched_plates(count=count)
+
+    def make(c, prec):
+        return lpm.GpuProblem(c.assembly(), undamaged_pt_type=c.undamaged_type, max_iter=c.max_iter,
+                              tol_iter=c.tol_iter, precision=lpm.Precision(prec), device=device)
+
+    # (1) plain FP64, one plate after another
+    plain_u, plain_s, plain_di, lat_plain = [], 0.0, 0, []
+    for c in cases:
+        g = make(c, 0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        iters = 0
+        for s in range(len(c.steps)):
+            ok, st = g.solve_load_step(c.load_step(s))
+            assert ok, f"{c.name}: step {s} failed on the plain path"
+            iters += st["cg_iters"]
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        plain_s += dt
+        lat_plain.append(dt)
+        plain_di += iters * c.n * 2
+        plain_u.append(g.state(("xyz",))["xyz"] - c.xyz)
+        g.close()
+
+    def batch_run(prec):
+        gs = [make(c, prec) for c in cases]
+        b = lpm.Batch(device)
+        mids = [b.add(g, [c.load_step(s) for s in range(len(c.steps))]) for g, c in zip(gs, cases)]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.run()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        st = b.stats()
+        errs, lat = [], []
+        for g, c, mid, u0 in zip(gs, cases, mids, plain_u):
+            info = b.member(mid)
+            assert info["state"] == 1, f"{c.name}: {info}"
+            lat.append(info["seconds"])
+            u = g.state(("xyz",))["xyz"] - c.xyz
+            errs.append(float(np.linalg.norm(u - u0) / np.linalg.norm(u0)))
+        b.close()
+        for g in gs:
+            g.close()
+        tmax = allreduce(dt, "max")
+        return {"seconds": tmax, "solves_per_s": world * count / tmax,
+                "dof_iter_per_s": allreduce(float(st["dof_iters"]), "sum") / tmax,
+                "rounds": st["rounds"], "cg_launches": st["cg_launches"],
+                "cg_kernel_seconds": st["cg_kernel_seconds"],
+                "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+                "max_rel_disp_err_vs_plain_fp64": max(errs), "median_rel_disp_err_vs_plain_fp64": float(np.median(errs))}
+
+    fp64 = batch_run(0)
+    mixed = batch_run(1)
+    pmax = allreduce(plain_s, "max")
+    plain = {"seconds": pmax, "solves_per_s": world * count / pmax,
+             "dof_iter_per_s": allreduce(float(plain_di), "sum") / pmax,
+             "latency_s": {"p50": float(np.percentile(lat_plain, 50)), "p99": float(np.percentile(lat_plain, 99))}}
+    return {"workload": f"{count} single-edge-notched hex plates, side log-uniform 4-25 mm at r=0.1 mm, "
+                        f"slit 0.2-0.5 of width, E 60-120 GPa, critical stretch 1e-3-3e-3, 40 Mode-I steps "
+                        f"({sum(c.n for c in cases)} particles, seed {cases[0].meta['seed']})",
+            "plain_fp64_one_at_a_time": plain, "batched_fp64": fp64, "batched_mixed": mixed,
+            "speedup_batched_mixed_vs_plain_fp64": mixed["solves_per_s"] / plain["solves_per_s"],
+            "speedup_batched_fp64_vs_plain_fp64": fp64["solves_per_s"] / plain["solves_per_s"]}
 
 
 # ------------------------------------------------------------------------------------ CPU legs

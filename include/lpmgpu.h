@@ -223,7 +223,7 @@ int32_t lpmgpu_cg_bsr_noalloc(int32_t dim, int32_t nrows, const int32_t *rowptr,
  * round advances every member by one piece of device work and solves all members' pending
  * Newton systems in one persistent CG launch.  Members may be added between rounds; finished
  * members may be removed.  A handle must not be used by other calls while it is a running
- * member.  Not thread-safe: one host thread per batch. */
+ * member.  Up to 4096 running members.  Not thread-safe: one host thread per batch. */
 typedef struct lpmgpu_batch lpmgpu_batch;
 
 typedef struct

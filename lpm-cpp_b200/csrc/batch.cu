@@ -37,8 +37,12 @@
 namespace lpm
 {
 
-constexpr int kMaxBatch = 1024;                      // problems in one batched launch
+constexpr int kMaxBatch = 256;                       // problems in one launch (their CG scalars live in
+                                                     // every block's shared memory)
 constexpr int kMaxVirt = kMaxGridBlocks + kMaxBatch; // virtual blocks
+constexpr int kMaxStage = 1024 + kMaxBatch;          // virtual blocks a launch may use (grid <= 1024)
+constexpr int kMaxMembers = 4096;                    // running members of one batch (launched in groups
+                                                     // of at most kMaxBatch)
 
 struct BInst
 {
@@ -64,26 +68,30 @@ struct BState
 
 struct BCtl
 {
-    unsigned bar[2]; // arrivals, generation
-    int nvirt, nact;
-    int fail, pad;
+    unsigned bar; // barrier arrivals: starts at zero, only counts up
+    int fail;     // a wait timed out
+    int nact;     // problems in the initial rank tables
+    int pad;
 };
 
 struct BArgs
 {
     const BInst *inst;
-    BState *st;
+    BState *st; // in: states of resumed solves; out (block 0, at the end): every problem's state
     BCtl *ctl;
-    int *act, *gcnt, *vstart; // per active rank [kMaxBatch]
-    int *vinst, *vk, *vg;     // per virtual block [kMaxVirt]
-    double *part;             // per virtual block [kMaxVirt]
-    int64_t slice;            // iterations per launch; unfinished solves pause and resume later
+    const int *act0, *gcnt0, *vstart0; // initial rank tables (the host's split)
+    double *part;                      // [2][kMaxVirt] per-virtual-block partials, two buffers
+    int ninst;
+    int64_t slice; // iterations per launch; unfinished solves pause and resume later
 };
 
-// virtual blocks of one problem: its share of G by matrix size, at least 1, at most its slices
-__host__ __device__ inline int vblocks_for(int64_t G, int64_t cost, int64_t C, int nslices)
+// Virtual blocks of one of `nact` problems: one each, plus its share (by matrix size) of the
+// G - nact blocks left, at most its slice count.  The total never exceeds G when nact <= G, so
+// every physical block carries at most one virtual block and the largest shares stay balanced.
+__host__ __device__ inline int vblocks_for(int64_t G, int nact, int64_t cost, int64_t C, int nslices)
 {
-    int64_t g = C > 0 ? (G * cost) / C : 1;
+    const int64_t R = G - nact;
+    int64_t g = 1 + ((R > 0 && C > 0) ? (R * cost) / C : 0);
     if (g > nslices)
         g = nslices;
     if (g < 1)
@@ -91,7 +99,7 @@ __host__ __device__ inline int vblocks_for(int64_t G, int64_t cost, int64_t C, i
     return (int)g;
 }
 
-// ---- block-wide integer scans / sums (1024 threads, deterministic)
+// ---- block-wide integer scans / sums (deterministic)
 __device__ int block_exscan(int v, int *total, int *sh)
 {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -137,290 +145,302 @@ __device__ int64_t block_sum_i64(int64_t v, long long *sh)
     return t;
 }
 
-// The last block's work at a barrier: reduce each active problem's partials, decide, and
-// re-partition when problems left.  mode 0: initial ||r||^2; 1: p.Ap -> alpha; 2: ||r||^2 ->
-// beta / convergence / cap.
-__device__ void batch_decide(const BArgs &a, int mode, int64_t it)
+// What every block keeps of the launch: the CG scalars of each problem (indexed by problem) and
+// the rank tables of the active ones (rank r: problem act[r], virtual blocks [vs[r], vs[r]+g[r])).
+// All blocks apply the same decisions to the same totals, so the copies never differ.
+struct BShared
 {
-    __shared__ int s_keep[kMaxBatch];
-    __shared__ int s_act[kMaxBatch];
-    __shared__ int s_scan[32];
-    __shared__ long long s_sum[32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nact = *reinterpret_cast<volatile int *>(&a.ctl->nact);
-    for (int r = warp; r < nact; r += (int)(blockDim.x >> 5))
+    double rr[kMaxBatch], stop[kMaxBatch], alpha[kMaxBatch], beta[kMaxBatch], rrf[kMaxBatch];
+    long long it[kMaxBatch];
+    int status[kMaxBatch];
+    int act[kMaxBatch], g[kMaxBatch], vs[kMaxBatch], keep[kMaxBatch];
+    int nact, nvirt;
+    int scan[32];
+    long long sum[32];
+};
+
+__device__ __forceinline__ int find_rank(const BShared &S, int v)
+{
+    int lo = 0, hi = S.nact - 1;
+    while (lo < hi)
     {
-        const int m = __ldcg(a.act + r), g = __ldcg(a.gcnt + r), vs = __ldcg(a.vstart + r);
+        const int mid = (lo + hi + 1) >> 1;
+        if (S.vs[mid] <= v)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// Counting grid barrier: barrier number `epoch` is passed once the word reaches
+// (epoch + 1) * gridDim.x.  Bounded wait; false when it timed out (here or in another block).
+__device__ bool batch_barrier(BCtl *ctl, unsigned &epoch, volatile int *s_fail)
+{
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        __threadfence();
+        atomicAdd(&ctl->bar, 1u);
+        const unsigned target = (epoch + 1u) * gridDim.x;
+        const unsigned long long t0 = gtimer();
+        while ((int)(ld_acquire(&ctl->bar) - target) < 0)
+        {
+            if (gtimer() - t0 > kBarrierTimeoutNs)
+            {
+                atomicExch(&ctl->fail, 1);
+                *s_fail = 1;
+                break;
+            }
+        }
+        if (*reinterpret_cast<volatile int *>(&ctl->fail))
+            *s_fail = 1;
+    }
+    epoch++;
+    __syncthreads();
+    return *s_fail == 0;
+}
+
+// After a barrier, in every block: reduce each active problem's partials (buffer `buf`; a fixed
+// tree: 32-wide warp sums in order), decide per problem, and re-partition the virtual blocks
+// when problems left.  mode 0: initial ||r||^2; 1: p.Ap -> alpha (or breakdown); 2: ||r||^2 ->
+// beta, or converged / capped / paused at the end of the slice.
+__device__ void batch_reduce_decide(const BArgs &a, BShared &S, int mode, int64_t it, int buf, double *stage)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const double *part = a.part + (size_t)buf * kMaxVirt;
+    // all partials into shared memory with one parallel load, then a warp per problem
+    for (int v = threadIdx.x; v < S.nvirt; v += blockDim.x)
+        stage[v] = __ldcg(part + v);
+    __syncthreads();
+    for (int r = warp; r < S.nact; r += nw)
+    {
+        const int m = S.act[r], g = S.g[r], vs = S.vs[r];
         double tot = 0;
         for (int c = 0; c < g; c += 32)
         {
-            double v = (c + lane < g) ? __ldcg(a.part + vs + c + lane) : 0.0;
+            const double v = (c + lane < g) ? stage[vs + c + lane] : 0.0;
             tot += wsum(v);
         }
         if (lane == 0)
         {
-            // written by whichever block arrived last before: read past L1
-            volatile BState *S = a.st + m;
             const BInst &I = a.inst[m];
             int keep = 1;
-            if (mode == 0 && !I.fresh)
-                keep = 1; // resumed: rr, beta, stop carried over from the pause
-            else if (mode == 0)
+            if (mode == 0)
             {
-                const double stop = (I.abs_stop >= 0) ? I.abs_stop : I.rtol * tot + I.atol;
-                S->rr = tot;
-                S->rr0 = tot;
-                S->stop = stop;
-                S->beta = 0.0;
-                S->it = 0;
-                S->rr_final = tot;
-                keep = !(tot <= stop);
+                if (I.fresh)
+                {
+                    const double stop = (I.abs_stop >= 0) ? I.abs_stop : I.rtol * tot + I.atol;
+                    S.rr[m] = tot;
+                    S.stop[m] = stop;
+                    S.beta[m] = 0.0;
+                    S.it[m] = 0;
+                    S.rrf[m] = tot;
+                    keep = !(tot <= stop);
+                }
             }
             else if (mode == 1)
             {
                 if (tot == 0.0)
                 {
-                    S->it = I.it0 + it - 1;
-                    S->status |= 4;
-                    S->rr_final = S->rr;
+                    S.it[m] = I.it0 + it - 1;
+                    S.status[m] |= 4;
+                    S.rrf[m] = S.rr[m];
                     keep = 0;
                 }
                 else
-                    S->alpha = S->rr / tot;
+                    S.alpha[m] = S.rr[m] / tot;
             }
             else
             {
                 const int64_t itg = I.it0 + it;
-                const bool done = tot <= S->stop;
+                const bool done = tot <= S.stop[m];
                 const bool capped = itg >= I.maxit;
                 if (done || capped)
                 {
-                    S->it = itg;
-                    S->rr_final = tot;
+                    S.it[m] = itg;
+                    S.rrf[m] = tot;
                     if (!done)
-                        S->status |= 1;
+                        S.status[m] |= 1;
                     keep = 0;
                 }
                 else
                 {
-                    S->beta = tot / S->rr;
-                    S->rr = tot;
+                    S.beta[m] = tot / S.rr[m];
+                    S.rr[m] = tot;
                     if (it >= a.slice)
                     {
-                        S->it = itg;
-                        S->rr_final = tot;
-                        S->status |= 8;
+                        S.it[m] = itg;
+                        S.rrf[m] = tot;
+                        S.status[m] |= 8;
                         keep = 0;
                     }
                 }
             }
-            s_keep[r] = keep;
+            S.keep[r] = keep;
         }
     }
     __syncthreads();
-    const int t = threadIdx.x;
-    const int keep = (t < nact) ? s_keep[t] : 1;
+    const int t = threadIdx.x, nact = S.nact;
+    const int keep = (t < nact) ? S.keep[t] : 1;
     if (!__syncthreads_or(keep == 0))
         return;
     // compaction of the still-active ranks (order kept), then the new split
-    const int mine = (t < nact) ? __ldcg(a.act + t) : -1;
+    const int mine = (t < nact) ? S.act[t] : -1;
     int nnew = 0;
-    const int pos = block_exscan((t < nact && keep) ? 1 : 0, &nnew, s_scan);
+    const int pos = block_exscan((t < nact && keep) ? 1 : 0, &nnew, S.scan);
     if (t < nact && keep)
-        s_act[pos] = mine;
+        S.keep[pos] = mine; // every thread has read its keep flag above
     __syncthreads();
-    const int m = (t < nnew) ? s_act[t] : -1;
+    const int m = (t < nnew) ? S.keep[t] : -1;
     const int64_t cost = (m >= 0) ? a.inst[m].cost : 0;
-    const int64_t C = block_sum_i64(cost, s_sum);
-    const int g = (m >= 0) ? vblocks_for(gridDim.x, cost, C, a.inst[m].nslices) : 0;
+    const int64_t C = block_sum_i64(cost, S.sum);
+    const int g = (m >= 0) ? vblocks_for(gridDim.x, nnew, cost, C, a.inst[m].nslices) : 0;
     int V = 0;
-    const int vs = block_exscan(g, &V, s_scan);
+    const int vs = block_exscan(g, &V, S.scan);
     if (m >= 0)
     {
-        __stcg(a.act + t, m);
-        __stcg(a.gcnt + t, g);
-        __stcg(a.vstart + t, vs);
-        for (int q = 0; q < g; ++q)
-        {
-            __stcg(a.vinst + vs + q, m);
-            __stcg(a.vk + vs + q, q);
-            __stcg(a.vg + vs + q, g);
-        }
+        S.act[t] = m;
+        S.g[t] = g;
+        S.vs[t] = vs;
     }
     if (t == 0)
     {
-        a.ctl->nact = nnew;
-        a.ctl->nvirt = V;
+        S.nact = nnew;
+        S.nvirt = V;
     }
     __syncthreads();
-}
-
-// Grid barrier whose last arrival runs batch_decide before releasing the others.  Returns false
-// when a wait timed out (every block then returns).
-__device__ bool batch_sync(const BArgs &a, int mode, int64_t it, volatile int *s_fail)
-{
-    __shared__ int s_last;
-    unsigned *bar = a.ctl->bar;
-    __syncthreads();
-    if (threadIdx.x == 0)
-    {
-        const unsigned gen = ld_acquire(bar + 1);
-        __threadfence();
-        const unsigned arrived = atomicAdd(bar, 1u);
-        s_last = (arrived == gridDim.x - 1);
-        if (!s_last)
-        {
-            const unsigned long long t0 = gtimer();
-            unsigned ns = 32;
-            while (ld_acquire(bar + 1) == gen)
-            {
-                if (gtimer() - t0 > kBarrierTimeoutNs)
-                {
-                    atomicExch(&a.ctl->fail, 1);
-                    *s_fail = 1;
-                    break;
-                }
-                __nanosleep(ns);
-                if (ns < 128)
-                    ns <<= 1;
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-    if (s_last)
-    {
-        batch_decide(a, mode, it);
-        if (threadIdx.x == 0)
-        {
-            __threadfence();
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0 && *reinterpret_cast<volatile int *>(&a.ctl->fail))
-        *s_fail = 1;
-    __syncthreads();
-    return *s_fail == 0;
-}
-
-// phase A for one slice: q = K p_new, p_new = r + beta p_old written, returns the slice's p.q
-template <typename TK, typename TV, int D>
-__device__ __forceinline__ double phase_a_slice(const BInst &I, int sl, TV beta, const TV *pold, TV *pnew, uint64_t pf,
-                                                uint64_t pl)
-{
-    TV acc[D];
-    const TV *r = static_cast<const TV *>(I.r);
-    const int i = spmv_slice<TK, TV, D>(sl, I.n, I.rowptr, I.perm, I.slice_off, I.col_sell,
-                                        static_cast<const TK *>(I.K), r, pold, beta, acc, pf, pl);
-    double lpq = 0;
-    if (i >= 0)
-    {
-        TV *q = static_cast<TV *>(I.q);
-#pragma unroll
-        for (int c = 0; c < D; ++c)
-        {
-            const int64_t k = (int64_t)i * D + c;
-            const TV pn = ld_keep(r + k, pl) + beta * ld_keep(pold + k, pl);
-            st_keep(pnew + k, pn, pl);
-            st_keep(q + k, acc[c], pl);
-            lpq += (double)pn * (double)acc[c];
-        }
-    }
-    return lpq;
 }
 
 template <typename TK, typename TV>
 __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg_batch(BArgs a)
 {
+    __shared__ BShared S;
     __shared__ double sh[32];
     __shared__ int s_fail;
-    if (threadIdx.x == 0)
+    // the column-split buffer of phase A and the staged partials of a reduction share storage
+    __shared__ union
+    {
+        TV red[32 * 3 * 32];
+        double stage[kMaxStage];
+    } U;
+    TV *red = U.red;
+    const int t = threadIdx.x;
+    if (t == 0)
+    {
         s_fail = 0;
+        S.nact = a.ctl->nact;
+    }
     __syncthreads();
-    const int warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int r = t; r < S.nact; r += blockDim.x)
+    {
+        S.act[r] = a.act0[r];
+        S.g[r] = a.gcnt0[r];
+        S.vs[r] = a.vstart0[r];
+    }
+    for (int m = t; m < a.ninst; m += blockDim.x)
+    {
+        const BState &B = a.st[m];
+        S.rr[m] = B.rr;
+        S.stop[m] = B.stop;
+        S.alpha[m] = B.alpha;
+        S.beta[m] = B.beta;
+        S.rrf[m] = B.rr_final;
+        S.it[m] = B.it;
+        S.status[m] = (int)B.status;
+    }
+    __syncthreads();
+    if (t == 0)
+        S.nvirt = S.nact > 0 ? S.vs[S.nact - 1] + S.g[S.nact - 1] : 0;
+    __syncthreads();
+    unsigned epoch = 0;
     const uint64_t pf = l2_evict_first(), pl = l2_evict_last();
 
     // fresh solves: r = b, x = 0, p_old = 0; partial ||b||^2 (resumed solves keep their vectors)
-    int nvirt = *reinterpret_cast<volatile int *>(&a.ctl->nvirt);
-    for (int v = blockIdx.x; v < nvirt; v += gridDim.x)
+    for (int v = blockIdx.x; v < S.nvirt; v += gridDim.x)
     {
-        const int m = __ldcg(a.vinst + v), k = __ldcg(a.vk + v), g = __ldcg(a.vg + v);
+        const int r = find_rank(S, v), m = S.act[r], k = v - S.vs[r], g = S.g[r];
         const BInst &I = a.inst[m];
         const int64_t lo = I.fresh ? k * I.ndof / g : 0, hi = I.fresh ? (k + 1) * I.ndof / g : 0;
         const TV *b = static_cast<const TV *>(I.b);
-        TV *x = static_cast<TV *>(I.x), *r = static_cast<TV *>(I.r), *pa = static_cast<TV *>(I.pa);
+        TV *x = static_cast<TV *>(I.x), *rv = static_cast<TV *>(I.r), *pa = static_cast<TV *>(I.pa);
         double loc = 0;
-        for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x)
+        for (int64_t j = lo + t; j < hi; j += blockDim.x)
         {
             const TV bv = b[j];
-            st_keep(r + j, bv, pl);
+            st_keep(rv + j, bv, pl);
             st_keep(x + j, TV(0), pl);
             st_keep(pa + j, TV(0), pl);
             loc += (double)bv * (double)bv;
         }
         block_partial_at(loc, a.part + v, sh);
     }
-    if (!batch_sync(a, 0, 0, &s_fail))
+    if (!batch_barrier(a.ctl, epoch, &s_fail))
         return;
+    batch_reduce_decide(a, S, 0, 0, 0, U.stage);
 
-    for (int64_t it = 1;; ++it)
+    for (int64_t it = 1; S.nact > 0; ++it)
     {
-        if (*reinterpret_cast<volatile int *>(&a.ctl->nact) == 0)
-            return;
-        // phase A: q = K p_new over this block's virtual blocks
-        nvirt = *reinterpret_cast<volatile int *>(&a.ctl->nvirt);
-        for (int v = blockIdx.x; v < nvirt; v += gridDim.x)
+        // phase A: q = K p_new (partials -> buffer 1)
+        for (int v = blockIdx.x; v < S.nvirt; v += gridDim.x)
         {
-            const int m = __ldcg(a.vinst + v), k = __ldcg(a.vk + v), g = __ldcg(a.vg + v);
+            const int r = find_rank(S, v), m = S.act[r], k = v - S.vs[r], g = S.g[r];
             const BInst &I = a.inst[m];
             const bool odd = ((I.it0 + it) & 1) != 0; // the solve's own iteration number
-            const TV beta = (TV)__ldcg(&a.st[m].beta);
+            const TV beta = (TV)S.beta[m];
             const TV *pold = static_cast<const TV *>(odd ? I.pa : I.pb);
             TV *pnew = static_cast<TV *>(odd ? I.pb : I.pa);
             const int s0 = (int)((int64_t)k * I.nslices / g), s1 = (int)((int64_t)(k + 1) * I.nslices / g);
-            double lpq = 0;
-            if (I.dim == 2)
-            {
-                for (int sl = s0 + warp; sl < s1; sl += nwarp)
-                    lpq += phase_a_slice<TK, TV, 2>(I, sl, beta, pold, pnew, pf, pl);
-            }
-            else
-            {
-                for (int sl = s0 + warp; sl < s1; sl += nwarp)
-                    lpq += phase_a_slice<TK, TV, 3>(I, sl, beta, pold, pnew, pf, pl);
-            }
-            block_partial_at(lpq, a.part + v, sh);
+            const TV *rv = static_cast<const TV *>(I.r);
+            TV *q = static_cast<TV *>(I.q);
+            const TK *K = static_cast<const TK *>(I.K);
+            const double lpq =
+                (I.dim == 2) ? spmv_block<TK, TV, 2>(s0, s1, I.n, I.rowptr, I.perm, I.slice_off, I.col_sell, K, rv, pold,
+                                                     pnew, q, beta, pf, pl, red)
+                             : spmv_block<TK, TV, 3>(s0, s1, I.n, I.rowptr, I.perm, I.slice_off, I.col_sell, K, rv, pold,
+                                                     pnew, q, beta, pf, pl, red);
+            block_partial_at(lpq, a.part + kMaxVirt + v, sh);
         }
-        if (!batch_sync(a, 1, it, &s_fail))
+        if (!batch_barrier(a.ctl, epoch, &s_fail))
             return;
-        // phase B: x += alpha p_new, r -= alpha q
-        nvirt = *reinterpret_cast<volatile int *>(&a.ctl->nvirt);
-        for (int v = blockIdx.x; v < nvirt; v += gridDim.x)
+        batch_reduce_decide(a, S, 1, it, 1, U.stage);
+        // phase B: x += alpha p_new, r -= alpha q (partials -> buffer 0)
+        for (int v = blockIdx.x; v < S.nvirt; v += gridDim.x)
         {
-            const int m = __ldcg(a.vinst + v), k = __ldcg(a.vk + v), g = __ldcg(a.vg + v);
+            const int r = find_rank(S, v), m = S.act[r], k = v - S.vs[r], g = S.g[r];
             const BInst &I = a.inst[m];
             const bool odd = ((I.it0 + it) & 1) != 0;
-            const TV al = (TV)__ldcg(&a.st[m].alpha);
+            const TV al = (TV)S.alpha[m];
             const TV *pnew = static_cast<const TV *>(odd ? I.pb : I.pa);
-            TV *x = static_cast<TV *>(I.x), *r = static_cast<TV *>(I.r);
+            TV *x = static_cast<TV *>(I.x), *rv = static_cast<TV *>(I.r);
             const TV *q = static_cast<const TV *>(I.q);
             const int64_t lo = k * I.ndof / g, hi = (k + 1) * I.ndof / g;
             double lrr = 0;
-            for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x)
+            for (int64_t j = lo + t; j < hi; j += blockDim.x)
             {
                 st_keep(x + j, ld_keep(x + j, pl) + al * ld_keep(pnew + j, pl), pl);
-                const TV rv = ld_keep(r + j, pl) - al * ld_keep(q + j, pl);
-                st_keep(r + j, rv, pl);
-                lrr += (double)rv * (double)rv;
+                const TV rn = ld_keep(rv + j, pl) - al * ld_keep(q + j, pl);
+                st_keep(rv + j, rn, pl);
+                lrr += (double)rn * (double)rn;
             }
             block_partial_at(lrr, a.part + v, sh);
         }
-        if (!batch_sync(a, 2, it, &s_fail))
+        if (!batch_barrier(a.ctl, epoch, &s_fail))
             return;
+        batch_reduce_decide(a, S, 2, it, 0, U.stage);
     }
+    if (blockIdx.x == 0)
+        for (int m = t; m < a.ninst; m += blockDim.x)
+        {
+            BState &B = a.st[m];
+            B.rr = S.rr[m];
+            B.stop = S.stop[m];
+            B.alpha = S.alpha[m];
+            B.beta = S.beta[m];
+            B.rr_final = S.rrf[m];
+            B.it = S.it[m];
+            B.status = S.status[m];
+        }
 }
 
 // ---- host side of the batched CG
@@ -444,7 +464,7 @@ struct BatchCtx
     BInst *d_inst = nullptr, *h_inst = nullptr;
     BState *d_st = nullptr, *h_st = nullptr;
     BCtl *d_ctl = nullptr, *h_ctl = nullptr;
-    int *d_tab = nullptr, *h_tab = nullptr; // act|gcnt|vstart [3*kMaxBatch] + vinst|vk|vg [3*kMaxVirt]
+    int *d_tab = nullptr, *h_tab = nullptr; // initial rank tables act|gcnt|vstart [3*kMaxBatch]
     double *d_part = nullptr;
     int64_t launches = 0;
     double kernel_seconds = 0;
@@ -465,19 +485,19 @@ struct BatchCtx
         if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ32, k_cg_batch<float, float>, kCGThreads, 0)) !=
             cudaSuccess)
             return e;
-        grid = std::min(kMaxGridBlocks, num_sms * std::max(1, std::min({occ64, occ32, kCGMinBlocks})));
+        grid = std::min(1024, num_sms * std::max(1, std::min({occ64, occ32, kCGMinBlocks})));
         if ((e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)) != cudaSuccess)
             return e;
         if ((e = cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming)) != cudaSuccess)
             return e;
         if ((e = cudaEventCreate(&ev_t0)) != cudaSuccess || (e = cudaEventCreate(&ev_t1)) != cudaSuccess)
             return e;
-        const size_t ntab = 3 * (size_t)kMaxBatch + 3 * (size_t)kMaxVirt;
+        const size_t ntab = 3 * (size_t)kMaxBatch;
         if ((e = cudaMalloc(&d_inst, sizeof(BInst) * kMaxBatch)) != cudaSuccess ||
             (e = cudaMalloc(&d_st, sizeof(BState) * kMaxBatch)) != cudaSuccess ||
             (e = cudaMalloc(&d_ctl, sizeof(BCtl))) != cudaSuccess ||
             (e = cudaMalloc(&d_tab, sizeof(int) * ntab)) != cudaSuccess ||
-            (e = cudaMalloc(&d_part, sizeof(double) * kMaxVirt)) != cudaSuccess)
+            (e = cudaMalloc(&d_part, sizeof(double) * 2 * kMaxVirt)) != cudaSuccess)
             return e;
         if ((e = cudaMallocHost(&h_inst, sizeof(BInst) * kMaxBatch)) != cudaSuccess ||
             (e = cudaMallocHost(&h_st, sizeof(BState) * kMaxBatch)) != cudaSuccess ||
@@ -583,20 +603,13 @@ struct BatchCtx
         }
         // initial split over all items (the same integer rule the kernel uses when problems leave)
         int *act = h_tab, *gcnt = h_tab + kMaxBatch, *vstart = h_tab + 2 * kMaxBatch;
-        int *vinst = h_tab + 3 * kMaxBatch, *vk = vinst + kMaxVirt, *vg = vk + kMaxVirt;
         int V = 0;
         for (int m = 0; m < ni; ++m)
         {
-            const int g = vblocks_for(grid, h_inst[m].cost, C, h_inst[m].nslices);
+            const int g = vblocks_for(grid, ni, h_inst[m].cost, C, h_inst[m].nslices);
             act[m] = m;
             gcnt[m] = g;
             vstart[m] = V;
-            for (int q = 0; q < g; ++q)
-            {
-                vinst[V + q] = m;
-                vk[V + q] = q;
-                vg[V + q] = g;
-            }
             V += g;
         }
         for (int m = 0; m < ni; ++m)
@@ -610,7 +623,6 @@ struct BatchCtx
             }
         }
         std::memset(h_ctl, 0, sizeof(BCtl));
-        h_ctl->nvirt = V;
         h_ctl->nact = ni;
         for (int m = 0; m < ni; ++m)
         {
@@ -623,25 +635,17 @@ struct BatchCtx
             (e = cudaMemcpyAsync(d_st, h_st, sizeof(BState) * ni, cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
             (e = cudaMemcpyAsync(d_ctl, h_ctl, sizeof(BCtl), cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
             (e = cudaMemcpyAsync(d_tab, h_tab, sizeof(int) * 3 * kMaxBatch, cudaMemcpyHostToDevice, stream)) !=
-                cudaSuccess ||
-            (e = cudaMemcpyAsync(d_tab + 3 * kMaxBatch, vinst, sizeof(int) * V, cudaMemcpyHostToDevice, stream)) !=
-                cudaSuccess ||
-            (e = cudaMemcpyAsync(d_tab + 3 * kMaxBatch + kMaxVirt, vk, sizeof(int) * V, cudaMemcpyHostToDevice,
-                                 stream)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(d_tab + 3 * kMaxBatch + 2 * kMaxVirt, vg, sizeof(int) * V, cudaMemcpyHostToDevice,
-                                 stream)) != cudaSuccess)
+                cudaSuccess)
             return e;
         BArgs a;
         a.inst = d_inst;
         a.st = d_st;
         a.ctl = d_ctl;
-        a.act = d_tab;
-        a.gcnt = d_tab + kMaxBatch;
-        a.vstart = d_tab + 2 * kMaxBatch;
-        a.vinst = d_tab + 3 * kMaxBatch;
-        a.vk = a.vinst + kMaxVirt;
-        a.vg = a.vk + kMaxVirt;
+        a.act0 = d_tab;
+        a.gcnt0 = d_tab + kMaxBatch;
+        a.vstart0 = d_tab + 2 * kMaxBatch;
         a.part = d_part;
+        a.ninst = ni;
         a.slice = slice > 0 ? slice : (int64_t(1) << 62);
         void *args[] = {&a};
         if ((e = cudaEventRecord(ev_t0, stream)) != cudaSuccess)
@@ -1024,7 +1028,19 @@ struct lpmgpu_batch
 
     // One batched launch over the members of one precision that need a CG this round (fresh
     // solves and solves paused by the previous launch's iteration slice).
-    int32_t cg_launch(std::vector<Member *> &ms, bool fp32)
+    int32_t cg_launch(std::vector<Member *> &all, bool fp32)
+    {
+        for (size_t c0 = 0; c0 < all.size(); c0 += kMaxBatch)
+        {
+            std::vector<Member *> group(all.begin() + c0, all.begin() + std::min(all.size(), c0 + kMaxBatch));
+            const int32_t r = cg_launch_group(group, fp32);
+            if (r != LPMGPU_OK)
+                return r;
+        }
+        return LPMGPU_OK;
+    }
+
+    int32_t cg_launch_group(std::vector<Member *> &ms, bool fp32)
     {
         if (ms.empty())
             return LPMGPU_OK;
@@ -1219,9 +1235,9 @@ int32_t lpmgpu_batch_add(lpmgpu_batch *b, lpmgpu_solver *h, const lpmgpu_load_st
         if (up && up->ph != Ph::Done && up->ph != Ph::Failed)
             live++;
     }
-    if (live >= kMaxBatch)
+    if (live >= kMaxMembers)
     {
-        set_last_error("a batch runs at most 1024 problems at once");
+        set_last_error("a batch runs at most 4096 problems at once");
         return LPMGPU_ERR_BUDGET;
     }
     for (int32_t s = 0; s < nsteps; ++s)

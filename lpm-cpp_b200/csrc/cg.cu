@@ -54,8 +54,8 @@ struct CGState
 };
 
 
-// Grid barrier fused with the reduction of the per-block partials part[2*b + slot]: the last
-// block to arrive sums them (fixed order: thread t takes b = t, t + blockDim, ..., then a fixed
+// Grid barrier fused with the reduction of the per-block partials part[2*b + slot] (used by the
+// allocation-free solve below): the last block to arrive sums them (fixed order: thread t takes b = t, t + blockDim, ..., then a fixed
 // tree), publishes the total in tot[slot] and releases the others.  Every block returns the
 // same total.  Returns false when the wait timed out.
 __device__ bool grid_reduce(unsigned *bar, int64_t *info, volatile int *s_fail, const double *part, int slot,
@@ -127,6 +127,59 @@ __device__ bool grid_reduce(unsigned *bar, int64_t *info, volatile int *s_fail, 
     return ok;
 }
 
+// Grid barrier + all-reduce of the per-block partials part[2*b + slot], with nothing serial on
+// the way out: the barrier word only counts arrivals (it starts at zero and is never reset, so
+// barrier number e is passed once it reaches (e + 1) * gridDim.x), and after it every block
+// sums all partials itself, in one fixed order (thread t takes b = t, t + blockDim, ..., warp
+// butterflies, then thread 0 over the warp sums in order), so every block holds the same
+// bit-identical total.  The two slots alternate between consecutive reductions, which keeps a
+// block that runs one phase ahead from overwriting partials another block is still reading.
+// Returns false when the wait timed out (the status word gets bit 2).
+__device__ bool grid_allreduce(unsigned *bar, unsigned &epoch, int64_t *info, volatile int *s_fail,
+                               const double *part, int slot, double *sh, double *out)
+{
+    __shared__ double s_tot;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        __threadfence();
+        atomicAdd(bar, 1u);
+        const unsigned target = (epoch + 1u) * gridDim.x;
+        const unsigned long long t0 = gtimer();
+        while ((int)(ld_acquire(bar) - target) < 0)
+        {
+            if (gtimer() - t0 > kBarrierTimeoutNs)
+            {
+                atomicOr(reinterpret_cast<unsigned long long *>(info + 1), 2ull);
+                *s_fail = 1;
+                break;
+            }
+        }
+    }
+    epoch++;
+    __syncthreads();
+    if (*s_fail)
+        return false;
+    double v = 0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+        v += __ldcg(part + 2 * b + slot);
+    v = wsum(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0)
+        sh[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double t = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q)
+            t += sh[q];
+        s_tot = t;
+    }
+    __syncthreads();
+    *out = s_tot;
+    return true;
+}
+
 template <typename TK, typename TV, int D>
 __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg(CGState s, const TK *__restrict__ K, const TV *__restrict__ b,
                                                    TV *__restrict__ x, TV *__restrict__ r, TV *__restrict__ pa,
@@ -134,9 +187,11 @@ __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg(CGState s, cons
 {
     __shared__ double sh[32];
     __shared__ int s_fail;
+    __shared__ TV red[32 * D * 32];
     if (threadIdx.x == 0)
         s_fail = 0;
     __syncthreads();
+    unsigned epoch = 0;
     const int64_t T = (int64_t)gridDim.x * blockDim.x;
     const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     // each block owns a contiguous, equal share of the slices (balanced, neighbours share L1)
@@ -156,7 +211,7 @@ __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg(CGState s, cons
     }
     block_partial(loc, s.part, 0, sh);
     double rr;
-    if (!grid_reduce(s.bar, s.info, &s_fail, s.part, 0, s.tot, sh, &rr))
+    if (!grid_allreduce(s.bar, epoch, s.info, &s_fail, s.part, 0, sh, &rr))
         return;
     const double stop = (s.abs_stop >= 0) ? s.abs_stop : s.rtol * rr + s.atol;
     if (blockIdx.x == 0 && threadIdx.x == 0)
@@ -171,28 +226,11 @@ __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg(CGState s, cons
     TV *pold = pa, *pnew = pb;
     for (int64_t it = 1;; ++it)
     {
-        double lpq = 0;
-        for (int sl = s0 + warp; sl < s1; sl += (int)(blockDim.x >> 5))
-        {
-            TV acc[D];
-            const int i = spmv_slice<TK, TV, D>(sl, s.n, s.rowptr, s.perm, s.slice_off, s.col_sell, K, r, pold, beta,
-                                                acc, pf, pl);
-            if (i >= 0)
-            {
-#pragma unroll
-                for (int c = 0; c < D; ++c)
-                {
-                    const int64_t k = (int64_t)i * D + c;
-                    const TV pn = ld_keep(r + k, pl) + beta * ld_keep(pold + k, pl);
-                    st_keep(pnew + k, pn, pl);
-                    st_keep(q + k, acc[c], pl);
-                    lpq += (double)pn * (double)acc[c];
-                }
-            }
-        }
+        const double lpq = spmv_block<TK, TV, D>(s0, s1, s.n, s.rowptr, s.perm, s.slice_off, s.col_sell, K, r,
+                                                   pold, pnew, q, beta, pf, pl, red);
         block_partial(lpq, s.part, 1, sh);
         double pq;
-        if (!grid_reduce(s.bar, s.info, &s_fail, s.part, 1, s.tot, sh, &pq))
+        if (!grid_allreduce(s.bar, epoch, s.info, &s_fail, s.part, 1, sh, &pq))
             return;
         if (pq == 0.0)
         {
@@ -216,7 +254,7 @@ __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg(CGState s, cons
         }
         block_partial(lrr, s.part, 0, sh);
         double rn;
-        if (!grid_reduce(s.bar, s.info, &s_fail, s.part, 0, s.tot, sh, &rn))
+        if (!grid_allreduce(s.bar, epoch, s.info, &s_fail, s.part, 0, sh, &rn))
             return;
         const bool done = rn <= stop;
         const bool capped = it >= s.maxit;

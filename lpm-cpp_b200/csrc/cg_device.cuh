@@ -129,8 +129,9 @@ __device__ __forceinline__ int spmv_slice(int sl, int n, const int *__restrict__
                                           const int64_t *__restrict__ slice_off, const int *__restrict__ col_sell,
                                           const TK *__restrict__ K, const TV *__restrict__ r,
                                           const TV *__restrict__ pold, TV beta, TV acc[D], uint64_t pf,
-                                          uint64_t pl)
+                                          uint64_t pl, int k0 = 0, int kstep = 1)
 {
+    // block columns k0, k0 + kstep, ... of the slice (all of them by default)
     constexpr int E = D * D;
     const int lane = threadIdx.x & 31;
     const int pos = sl * kSlice + lane;
@@ -144,14 +145,14 @@ __device__ __forceinline__ int spmv_slice(int sl, int n, const int *__restrict__
 #pragma unroll
     for (int k = 0; k < D; ++k)
         acc[k] = TV(0);
-    // the column of step k+1 is fetched during step k, so the x gathers never wait on it
-    int jn = (myn > 0) ? ld_stream(cp, pf) : 0;
+    // the column of the next step is fetched during this one, so the x gathers never wait on it
+    int jn = (myn > k0) ? ld_stream(cp + (int64_t)k0 * kSlice, pf) : 0;
 #pragma unroll 2
-    for (int k = 0; k < w; ++k)
+    for (int k = k0; k < w; k += kstep)
     {
         const int j = jn;
-        if (k + 1 < myn)
-            jn = ld_stream(cp + (int64_t)(k + 1) * kSlice, pf);
+        if (k + kstep < myn)
+            jn = ld_stream(cp + (int64_t)(k + kstep) * kSlice, pf);
         if (k < myn)
         {
             TV xv[D];
@@ -171,6 +172,81 @@ __device__ __forceinline__ int spmv_slice(int sl, int n, const int *__restrict__
         }
     }
     return i;
+}
+
+// Maximum warps that share one slice's block columns (the column split below).
+constexpr int kMaxColumnSplit = 16;
+
+// Phase A of a CG iteration for the rows of slices [s0, s1), run by the whole block:
+// q = K p_new with p_new = r + beta p_old formed on the fly; p_new and q are stored for those
+// rows and the thread's share of p_new . q is returned.  With at least one slice per warp each
+// warp streams whole slices.  With fewer slices than warps (small problems, or a small share
+// of one) S warps share a slice, each taking every S-th block column, so the chain of
+// dependent column/gather loads a warp walks is S times shorter; the S partial row sums are
+// added in a fixed order through `red` (shared memory, 32 * D * 32 values).  Every thread of
+// the block must call it.
+template <typename TK, typename TV, int D>
+__device__ __forceinline__ double spmv_block(int s0, int s1, int n, const int *__restrict__ rowptr,
+                                             const int *__restrict__ perm, const int64_t *__restrict__ slice_off,
+                                             const int *__restrict__ col_sell, const TK *__restrict__ K,
+                                             const TV *__restrict__ r, const TV *__restrict__ pold,
+                                             TV *__restrict__ pnew, TV *__restrict__ q, TV beta, uint64_t pf,
+                                             uint64_t pl, TV *red)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int ns = s1 - s0;
+    double lpq = 0;
+    auto epilogue = [&](int i, const TV *acc) {
+        if (i < 0)
+            return;
+#pragma unroll
+        for (int c = 0; c < D; ++c)
+        {
+            const int64_t k = (int64_t)i * D + c;
+            const TV pn = ld_keep(r + k, pl) + beta * ld_keep(pold + k, pl);
+            st_keep(pnew + k, pn, pl);
+            st_keep(q + k, acc[c], pl);
+            lpq += (double)pn * (double)acc[c];
+        }
+    };
+    if (ns <= 0)
+        return 0.0;
+    if (2 * ns > nw)
+    {
+        for (int sl = s0 + warp; sl < s1; sl += nw)
+        {
+            TV acc[D];
+            const int i = spmv_slice<TK, TV, D>(sl, n, rowptr, perm, slice_off, col_sell, K, r, pold, beta, acc, pf, pl);
+            epilogue(i, acc);
+        }
+        return lpq;
+    }
+    int S = 2;
+    while (S < kMaxColumnSplit && ns * S * 2 <= nw)
+        S *= 2;
+    const int ls = warp / S, part = warp % S;
+    TV acc[D];
+#pragma unroll
+    for (int c = 0; c < D; ++c)
+        acc[c] = TV(0);
+    int i = -1;
+    if (ls < ns)
+        i = spmv_slice<TK, TV, D>(s0 + ls, n, rowptr, perm, slice_off, col_sell, K, r, pold, beta, acc, pf, pl, part, S);
+    if (ls < ns && part > 0)
+#pragma unroll
+        for (int c = 0; c < D; ++c)
+            red[(warp * D + c) * 32 + lane] = acc[c];
+    __syncthreads();
+    if (ls < ns && part == 0)
+    {
+        for (int p = 1; p < S; ++p)
+#pragma unroll
+            for (int c = 0; c < D; ++c)
+                acc[c] += red[((warp + p) * D + c) * 32 + lane];
+        epilogue(i, acc);
+    }
+    __syncthreads();
+    return lpq;
 }
 
 } // namespace lpm
