@@ -266,6 +266,55 @@ int32_t lpmgpu_batch_get_stats(const lpmgpu_batch *b, lpmgpu_batch_stats *st);
  * Default 512. */
 int32_t lpmgpu_batch_set_slice(lpmgpu_batch *b, int64_t iterations);
 
+/* ---- Serving: LPM solves submitted while others run (continuous batching).  A request is a
+ * problem description plus its load path (both copied at submit).  An admission thread builds a
+ * request's device problem once its estimated device memory fits the HBM budget (requests are
+ * admitted in arrival order; one larger than the whole budget runs alone); a worker thread adds
+ * it to a running batch between two rounds, so its CG iterations share the batched launches of
+ * every solve in flight, and when its last load step is done copies its final positions to the
+ * host and frees its device memory.  All functions may be called from any host thread. */
+typedef struct lpmgpu_server lpmgpu_server;
+
+typedef struct
+{
+    int32_t state;        /* 0 queued, 1 running, 2 done, 3 failed */
+    int32_t status;       /* LPMGPU_OK, or the error that stopped the request */
+    int32_t n;            /* particles */
+    int32_t steps_done;   /* finished load steps (known once the request is done) */
+    int32_t nsteps;
+    lpmgpu_stats total;   /* summed over the finished load steps */
+    int64_t dof_iters;    /* sum over CG iterations of the unknown count */
+    int64_t device_bytes; /* device memory the problem held */
+    double t_submit, t_start, t_done; /* seconds since the server was created (-1: not yet) */
+} lpmgpu_request_info;
+
+typedef struct
+{
+    int64_t submitted, queued, running, done, failed, rounds;
+    int64_t bytes_in_use, bytes_budget, peak_bytes;
+    int32_t worker_status;              /* last error of the batch rounds, LPMGPU_OK if none */
+    int32_t pad;
+    double latency_p50, latency_p99;    /* seconds from submit to done, over finished requests */
+    double seconds;                     /* since the server was created */
+} lpmgpu_server_stats;
+
+/* the device memory the server's admission test expects a problem to take (an upper estimate
+ * from the particle count, lattice and precision; the problem's real size is in lpmgpu_sizes) */
+int32_t lpmgpu_estimate_bytes(const lpmgpu_desc *d, int64_t *bytes);
+int32_t lpmgpu_server_create(int32_t device, int64_t hbm_budget_bytes, lpmgpu_server **out);
+/* stops both threads; requests not yet fetched are dropped */
+int32_t lpmgpu_server_destroy(lpmgpu_server *s);
+int32_t lpmgpu_server_set_slice(lpmgpu_server *s, int64_t iterations);
+int32_t lpmgpu_server_submit(lpmgpu_server *s, const lpmgpu_desc *d, const lpmgpu_load_step *steps, int32_t nsteps,
+                             int64_t *request_id);
+int32_t lpmgpu_server_poll(lpmgpu_server *s, int64_t request_id, lpmgpu_request_info *info);
+/* blocks until the request is done or failed (LPMGPU_OK) or the timeout passed (LPMGPU_ERR_NOT_READY) */
+int32_t lpmgpu_server_wait(lpmgpu_server *s, int64_t request_id, double timeout_s, lpmgpu_request_info *info);
+/* copies the final positions (n*3 doubles, cap >= n*3) and forgets the request; a failed request
+ * returns its error and is forgotten as well */
+int32_t lpmgpu_server_result(lpmgpu_server *s, int64_t request_id, double *xyz, int64_t cap);
+int32_t lpmgpu_server_get_stats(lpmgpu_server *s, lpmgpu_server_stats *st);
+
 #ifdef __cplusplus
 }
 #endif

@@ -133,6 +133,28 @@ class MemberInfo(C.Structure):
                 ("total", Stats), ("dof_iters", C.c_int64), ("seconds", C.c_double)]
 
 
+class RequestInfo(C.Structure):
+    _fields_ = [("state", C.c_int32), ("status", C.c_int32), ("n", C.c_int32), ("steps_done", C.c_int32),
+                ("nsteps", C.c_int32), ("total", Stats), ("dof_iters", C.c_int64), ("device_bytes", C.c_int64),
+                ("t_submit", C.c_double), ("t_start", C.c_double), ("t_done", C.c_double)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "total"}
+        d["total"] = self.total.as_dict()
+        return d
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("queued", C.c_int64), ("running", C.c_int64), ("done", C.c_int64),
+                ("failed", C.c_int64), ("rounds", C.c_int64), ("bytes_in_use", C.c_int64),
+                ("bytes_budget", C.c_int64), ("peak_bytes", C.c_int64), ("worker_status", C.c_int32),
+                ("pad", C.c_int32), ("latency_p50", C.c_double), ("latency_p99", C.c_double),
+                ("seconds", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+
+
 class BatchStats(C.Structure):
     _fields_ = [("rounds", C.c_int64), ("cg_launches", C.c_int64), ("members_done", C.c_int64),
                 ("members_failed", C.c_int64), ("cg_iters", C.c_int64), ("dof_iters", C.c_int64),
@@ -156,6 +178,8 @@ EXPORTS = [
     "lpmgpu_batch_create", "lpmgpu_batch_destroy", "lpmgpu_batch_add", "lpmgpu_batch_round", "lpmgpu_batch_run",
     "lpmgpu_batch_member", "lpmgpu_batch_member_steps", "lpmgpu_batch_remove", "lpmgpu_batch_get_stats",
     "lpmgpu_batch_set_slice",
+    "lpmgpu_estimate_bytes", "lpmgpu_server_create", "lpmgpu_server_destroy", "lpmgpu_server_set_slice", "lpmgpu_server_submit",
+    "lpmgpu_server_poll", "lpmgpu_server_wait", "lpmgpu_server_result", "lpmgpu_server_get_stats",
 ]
 
 
@@ -206,6 +230,15 @@ def lib():
         "lpmgpu_batch_remove": (C.c_int32, [vp, C.c_int32]),
         "lpmgpu_batch_get_stats": (C.c_int32, [vp, C.POINTER(BatchStats)]),
         "lpmgpu_batch_set_slice": (C.c_int32, [vp, C.c_int64]),
+        "lpmgpu_estimate_bytes": (C.c_int32, [C.POINTER(Desc), lp]),
+        "lpmgpu_server_create": (C.c_int32, [C.c_int32, C.c_int64, C.POINTER(vp)]),
+        "lpmgpu_server_destroy": (C.c_int32, [vp]),
+        "lpmgpu_server_set_slice": (C.c_int32, [vp, C.c_int64]),
+        "lpmgpu_server_submit": (C.c_int32, [vp, C.POINTER(Desc), C.POINTER(CLoadStep), C.c_int32, lp]),
+        "lpmgpu_server_poll": (C.c_int32, [vp, C.c_int64, C.POINTER(RequestInfo)]),
+        "lpmgpu_server_wait": (C.c_int32, [vp, C.c_int64, C.c_double, C.POINTER(RequestInfo)]),
+        "lpmgpu_server_result": (C.c_int32, [vp, C.c_int64, dp, C.c_int64]),
+        "lpmgpu_server_get_stats": (C.c_int32, [vp, C.POINTER(ServerStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -457,6 +490,33 @@ class _CStep:
 
 
 # ---------------------------------------------------------------------------- solver
+def _pack_desc(ass: Assembly, undamaged_pt_type=-1, max_iter=30, tol_iter=1e-5, precision=0, cg_rtol=1e-12,
+               cg_atol=1e-12, cg_maxit=0, device=0):
+    """lpmgpu_desc of an Assembly and solver settings; returns (desc, arrays the desc points into)."""
+    m = ass.material
+    d = Desc()
+    keep = [np.ascontiguousarray(ass.xyz, dtype=np.float64), np.ascontiguousarray(ass.type, dtype=np.int32)]
+    d.lattice, d.ptype, d.n = int(ass.cell.lattice), int(ass.ptype), ass.nparticle
+    d.xyz, d.type = _dp(keep[0]), _ip(keep[1])
+    d.radius, d.plane_stress = ass.cell.radius, int(m.plane_stress)
+    d.E, d.mu, d.critical_bstrain = m.E, m.mu, m.critical_bstrain
+    d.sigmay, d.xi, d.H, d.A, d.nonlocal_L = m.sigmay, m.xi, m.H, m.A, m.nonlocal_L
+    d.undamaged_type, d.max_iter, d.tol_iter = int(undamaged_pt_type), int(max_iter), float(tol_iter)
+    d.cg_rtol, d.cg_atol, d.cg_maxit = float(cg_rtol), float(cg_atol), int(cg_maxit)
+    d.precision, d.device = int(precision), int(device)
+    if ass.bonds is not None:
+        nb0, nb1, p2 = (np.ascontiguousarray(a, dtype=np.int32) for a in ass.bonds)
+        keep += [nb0, nb1, p2]
+        d.bond_nb0, d.bond_nb1, d.bond_p2 = _ip(nb0), _ip(nb1), _ip(p2)
+    for name in ("bond_kn", "bond_tv", "bond_damage"):
+        arr = getattr(ass, name)
+        if arr is not None:
+            a = np.ascontiguousarray(arr, dtype=np.float64)
+            keep.append(a)
+            setattr(d, name, _dp(a))
+    return d, keep
+
+
 class GpuProblem:
     """One device-resident problem: the handle of include/lpmgpu.h."""
 
@@ -464,29 +524,8 @@ class GpuProblem:
                  precision: Precision = Precision.FP64, cg_rtol=1e-12, cg_atol=1e-12, cg_maxit=0, device=0):
         L = lib()
         self.ass = ass
-        m = ass.material
-        d = Desc()
-        d.lattice, d.ptype, d.n = int(ass.cell.lattice), int(ass.ptype), ass.nparticle
-        self._xyz = np.ascontiguousarray(ass.xyz, dtype=np.float64)
-        self._type = np.ascontiguousarray(ass.type, dtype=np.int32)
-        d.xyz, d.type = _dp(self._xyz), _ip(self._type)
-        d.radius, d.plane_stress = ass.cell.radius, int(m.plane_stress)
-        d.E, d.mu, d.critical_bstrain = m.E, m.mu, m.critical_bstrain
-        d.sigmay, d.xi, d.H, d.A, d.nonlocal_L = m.sigmay, m.xi, m.H, m.A, m.nonlocal_L
-        d.undamaged_type, d.max_iter, d.tol_iter = int(undamaged_pt_type), int(max_iter), float(tol_iter)
-        d.cg_rtol, d.cg_atol, d.cg_maxit = float(cg_rtol), float(cg_atol), int(cg_maxit)
-        d.precision, d.device = int(precision), int(device)
-        self._keep = []
-        if ass.bonds is not None:
-            nb0, nb1, p2 = (np.ascontiguousarray(a, dtype=np.int32) for a in ass.bonds)
-            self._keep += [nb0, nb1, p2]
-            d.bond_nb0, d.bond_nb1, d.bond_p2 = _ip(nb0), _ip(nb1), _ip(p2)
-        for name in ("bond_kn", "bond_tv", "bond_damage"):
-            arr = getattr(ass, name)
-            if arr is not None:
-                a = np.ascontiguousarray(arr, dtype=np.float64)
-                self._keep.append(a)
-                setattr(d, name, _dp(a))
+        d, self._keep = _pack_desc(ass, undamaged_pt_type, max_iter, tol_iter, precision, cg_rtol, cg_atol, cg_maxit,
+                                   device)
         h = C.c_void_p()
         _check(L.lpmgpu_create(C.byref(d), C.byref(h)), "lpmgpu_create")
         self._h = h
@@ -669,6 +708,74 @@ class Batch:
     def close(self):
         if getattr(self, "_h", None):
             lib().lpmgpu_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Serving loop (lpmgpu_server_*): submit LPM solves while others run; each is admitted when
+    its device memory fits the HBM budget and joins the running batch (continuous batching)."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 150 * 10**9):
+        h = C.c_void_p()
+        _check(lib().lpmgpu_server_create(int(device), int(hbm_budget_bytes), C.byref(h)), "lpmgpu_server_create")
+        self._h = h
+        self.device = int(device)
+        self._n = {}
+
+    @staticmethod
+    def estimate_bytes(ass: Assembly, precision: Precision = Precision.FP64) -> int:
+        """Device memory the admission test expects the problem to take (lpmgpu_estimate_bytes)."""
+        d, keep = _pack_desc(ass, precision=precision)
+        out = C.c_int64(0)
+        _check(lib().lpmgpu_estimate_bytes(C.byref(d), C.byref(out)), "lpmgpu_estimate_bytes")
+        return out.value
+
+    def set_slice(self, iterations: int):
+        _check(lib().lpmgpu_server_set_slice(self._h, int(iterations)), "lpmgpu_server_set_slice")
+
+    def submit(self, ass: Assembly, steps: Sequence[LoadStep], undamaged_pt_type=-1, max_iter=30, tol_iter=1e-5,
+               precision: Precision = Precision.FP64, cg_rtol=1e-12, cg_atol=1e-12, cg_maxit=0) -> int:
+        d, keep = _pack_desc(ass, undamaged_pt_type, max_iter, tol_iter, precision, cg_rtol, cg_atol, cg_maxit,
+                             self.device)
+        cs = [_CStep(s) for s in steps]
+        arr = (CLoadStep * max(len(cs), 1))(*[c.s for c in cs])
+        rid = C.c_int64(0)
+        _check(lib().lpmgpu_server_submit(self._h, C.byref(d), arr, len(cs), C.byref(rid)), "lpmgpu_server_submit")
+        self._n[rid.value] = ass.nparticle
+        return rid.value
+
+    def poll(self, rid: int) -> dict:
+        info = RequestInfo()
+        _check(lib().lpmgpu_server_poll(self._h, int(rid), C.byref(info)), "lpmgpu_server_poll")
+        return info.as_dict()
+
+    def wait(self, rid: int, timeout: float = 600.0) -> dict:
+        info = RequestInfo()
+        r = lib().lpmgpu_server_wait(self._h, int(rid), float(timeout), C.byref(info))
+        if r not in (OK, ERR_NOT_READY):
+            _check(r, "lpmgpu_server_wait")
+        return info.as_dict()
+
+    def result(self, rid: int) -> np.ndarray:
+        out = np.zeros((self._n[rid], 3))
+        _check(lib().lpmgpu_server_result(self._h, int(rid), _dp(out), out.size), "lpmgpu_server_result")
+        self._n.pop(rid, None)
+        return out
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().lpmgpu_server_get_stats(self._h, C.byref(st)), "lpmgpu_server_get_stats")
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lpmgpu_server_destroy(self._h)
             self._h = None
 
     def __del__(self):

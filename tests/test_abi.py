@@ -58,6 +58,9 @@ def test_invalid_arguments_are_rejected():
     assert L.lpmgpu_batch_destroy(None) == 1
     assert L.lpmgpu_batch_add(None, None, None, 0, None) == 1
     assert L.lpmgpu_batch_round(None, None) == 1
+    assert L.lpmgpu_server_create(0, 0, None) == 1
+    assert L.lpmgpu_server_submit(None, None, None, 0, None) == 1
+    assert L.lpmgpu_estimate_bytes(None, None) == 1
 
 
 @pytest.mark.skipif(cuda_available(), reason="checks the no-device path")
