@@ -57,6 +57,10 @@ def args_():
     ap.add_argument("--cpu-cg-cap", type=int, default=400, help="CG iterations per solve in the CPU sample")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched 64-plate damage workload")
     ap.add_argument("--plates", type=int, default=64, help="plates in the batched damage workload")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
+    ap.add_argument("--serve-requests", type=int, default=12, help="requests in the serving-stream sample")
+    ap.add_argument("--serve-max-particles", type=float, default=1e5,
+                    help="upper end of the log-uniform particle count (the stream's full range is 5e3-5e5)")
     return ap.parse_args()
 
 
@@ -313,6 +317,10 @@ def run_ours(a):
     if not a.no_batched:
         barrier()
         batched = batched_leg(lpm, a.plates, local, world, allreduce)
+    serving = None
+    if not a.no_serving:
+        barrier()
+        serving = serving_leg(lpm, a.serve_requests, a.serve_max_particles, local, world, allreduce)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -335,7 +343,7 @@ def run_ours(a):
                                    "force": (c1["force_seconds"] - c0["force_seconds"]) * 1e3 / K,
                                    "cg_kernel": cg_s * 1e3 / K},
             "roofline": roof, "e2e": e2e, "gpu_launches": counters_total, "clocks": clocks,
-            "mixed": mixed, "batched": batched, "cpu_baseline": cpu,
+            "mixed": mixed, "batched": batched, "serving": serving, "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
     if dist:
@@ -417,6 +425,90 @@ def batched_leg(lpm, count, device, world, allreduce):
             "plain_fp64_one_at_a_time": plain, "batched_fp64": fp64, "batched_mixed": mixed,
             "speedup_batched_mixed_vs_plain_fp64": mixed["solves_per_s"] / plain["solves_per_s"],
             "speedup_batched_fp64_vs_plain_fp64": fp64["solves_per_s"] / plain["solves_per_s"]}
+
+
+def serving_leg(lpm, count, nmax, device, world, allreduce):
+    """Serving stream (lpm-cpp_b200/configs.serving_requests): `count` requests with seeded
+    Poisson arrivals (mean 200/s) of elastic or J2 solves on hex-2D / SC-3D / BCC-3D lattices,
+    particle count log-uniform 5e3..`nmax`, 5-50 monotone steps each.
+      plain     the FP64 path one request at a time in arrival order (create + all steps, timed
+                per request; each request starts when it has arrived and the previous one is
+                done, so its latency includes queueing);
+      served    lpm.Server (HBM budget 150 GB, continuous batching), each request submitted at
+                its arrival time, in mixed precision and in FP64.
+    solves/s = requests / (last completion - first arrival); latency = completion - arrival.
+    Errors: each request's final displacement against the plain FP64 result."""
+    import threading
+    import torch
+    cfg = importlib.import_module("lpm-cpp_b200.configs")
+    reqs = cfg.serving_requests(count=count, n_range=(5e3, nmax))
+    steps_of = lambda c: [c.load_step(s) for s in range(len(c.steps))]  # noqa: E731
+
+    # plain FP64, one at a time
+    clock, lat_plain, u_plain, dof_iters = 0.0, [], [], 0
+    for arr, c in reqs:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g = lpm.GpuProblem(c.assembly(), undamaged_pt_type=c.undamaged_type, max_iter=c.max_iter,
+                           tol_iter=c.tol_iter, device=device)
+        for st in steps_of(c):
+            ok, s2 = g.solve_load_step(st)
+            assert ok, f"{c.name}: plain path failed"
+            dof_iters += s2["cg_iters"] * c.n * c.dim
+        u_plain.append(g.state(("xyz",))["xyz"] - c.xyz)
+        g.close()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        clock = max(clock, arr) + dt
+        lat_plain.append(clock - arr)
+    span_plain = clock - reqs[0][0]
+
+    def served(prec):
+        srv = lpm.Server(device=device, hbm_budget_bytes=150 * 10**9)
+        ids = [None] * len(reqs)
+        t_base = time.perf_counter()
+
+        def submitter():
+            for k, (arr, c) in enumerate(reqs):
+                wait = arr - (time.perf_counter() - t_base)
+                if wait > 0:
+                    time.sleep(wait)
+                ids[k] = srv.submit(c.assembly(), steps_of(c), undamaged_pt_type=c.undamaged_type,
+                                    max_iter=c.max_iter, tol_iter=c.tol_iter, precision=lpm.Precision(prec))
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        lat, errs, end, first = [], [], 0.0, float("inf")
+        for k, (arr, c) in enumerate(reqs):
+            info = srv.wait(ids[k], timeout=3600)
+            assert info["state"] == 2, f"{c.name}: {info}"
+            u = srv.result(ids[k]) - c.xyz
+            errs.append(float(np.linalg.norm(u - u_plain[k]) / np.linalg.norm(u_plain[k])))
+            # times on the server's clock; arrivals on the submitter's
+            lat.append(info["t_done"] - info["t_submit"])
+            end = max(end, info["t_done"])
+            first = min(first, info["t_submit"])
+        st = srv.stats()
+        srv.close()
+        span = end - first
+        return {"solves_per_s": world * len(reqs) / allreduce(span, "max"), "makespan_s": span,
+                "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+                "rounds": st["rounds"], "peak_device_bytes": st["peak_bytes"],
+                "max_rel_disp_err_vs_plain_fp64": max(errs), "median_rel_disp_err_vs_plain_fp64": float(np.median(errs))}
+
+    mixed = served(1)
+    fp64 = served(0)
+    plain = {"solves_per_s": world * len(reqs) / allreduce(span_plain, "max"), "makespan_s": span_plain,
+             "latency_s": {"p50": float(np.percentile(lat_plain, 50)), "p99": float(np.percentile(lat_plain, 99))},
+             "dof_iter_per_s": dof_iters / span_plain}
+    return {"workload": f"{len(reqs)} requests, Poisson arrivals 200/s (seed {reqs[0][1].meta['seed']}); hex-2D / "
+                        f"SC-3D / BCC-3D, N log-uniform 5e3-{nmax:.0e} (the stream's range is 5e3-5e5; this sample "
+                        f"is bounded so the leg ends in about a minute), E 50-250 GPa, nu 0.2-0.35, 5-50 steps to "
+                        f"0.1% strain, elastic or J2; {sum(c.n for _, c in reqs)} particles in total",
+            "plain_fp64_one_at_a_time": plain, "served_mixed": mixed, "served_fp64": fp64,
+            "speedup_served_mixed_vs_plain_fp64": mixed["solves_per_s"] / plain["solves_per_s"],
+            "hbm_budget_bytes": 150 * 10**9}
 
 
 # ------------------------------------------------------------------------------------ CPU legs

@@ -139,12 +139,13 @@ def hex_plate(size=10.0, radius=0.1, E=69e3, mu=0.3, plane_stress=True, steps=10
 
 
 def sc_cube(size=20.0, radius=0.2, E=2e5, mu=0.25, steps=20, total_disp=0.02, tol_iter=1e-5, max_iter=30,
-            ptype=L.ParticleType.Elastic, j2=None) -> Case:
+            ptype=L.ParticleType.Elastic, j2=None, lattice=L.LatticeType.SimpleCubic3D) -> Case:
     """Config 2 (ex1_isoelasticity_3d_sc): simple-cubic cube, bottom face fixed in z, one bottom
     corner pinned in x and y, and a second bottom corner fixed in y so the rotation about z is
-    removed (a single pinned corner leaves K singular); top face pulled in z."""
+    removed (a single pinned corner leaves K singular); top face pulled in z.  `lattice` may be
+    BCC3D for the same cube on a body-centred cubic lattice."""
     box = [0.0, size, 0.0, size, 0.0, size]
-    xyz = _gen(L.LatticeType.SimpleCubic3D, radius, box)
+    xyz = _gen(lattice, radius, box)
     top = np.nonzero(xyz[:, 2] > box[5] - 2 * radius)[0].astype(np.int32)
     bot = np.nonzero(xyz[:, 2] < box[4] + 2 * radius)[0].astype(np.int32)
     zb = xyz[bot]
@@ -160,7 +161,8 @@ def sc_cube(size=20.0, radius=0.2, E=2e5, mu=0.25, steps=20, total_disp=0.02, to
     groups = {"top": top, "bottom": bot, "corner0": np.array([c0], np.int32), "corner1": np.array([c1], np.int32)}
     st = [([("bottom", "z", 0.0), ("corner0", "x", 0.0), ("corner0", "y", 0.0), ("corner1", "y", 0.0),
             ("top", "z", dstep)], []) for _ in range(steps)]
-    return Case(f"sc3d_{size:g}mm_r{radius:g}", L.LatticeType.SimpleCubic3D, radius, box, xyz, ptype, mat, types,
+    tag = "sc3d" if lattice == L.LatticeType.SimpleCubic3D else "bcc3d"
+    return Case(f"{tag}_{size:g}mm_r{radius:g}", L.LatticeType(lattice), radius, box, xyz, ptype, mat, types,
                 groups, st, tol_iter=tol_iter, max_iter=max_iter)
 
 
@@ -248,4 +250,39 @@ def batched_notched_plates(count=64, seed=20240604, steps=40, radius=0.1, side=(
         c.meta.update({"seed": seed, "index": k, "side": L, "crack_ratio": a, "E": e, "critical_bstrain": cs,
                        "opening_scale": scale})
         out.append(c)
+    return out
+
+
+def serving_requests(count=16, seed=20240605, rate=200.0, n_range=(5e3, 5e5), steps_range=(5, 50), strain=1e-3,
+                     j2=(200.0, 0.0, 38714.0, 10.0)):
+    """Serving stream: `count` requests with Poisson arrivals (seeded, mean `rate` per second).
+    Per request: lattice hex-2D, SC-3D or BCC-3D (equally likely), particle count log-uniform in
+    `n_range` (the specimen side is chosen to give about that count), E uniform 50-250 GPa, nu
+    uniform 0.2-0.35, a monotone path of 5-50 equal steps to `strain` total strain, elastic or
+    (3D lattices, half of them) J2 plasticity.  Returns [(arrival seconds, Case)]."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for k in range(count):
+        t += float(rng.exponential(1.0 / rate))
+        lat = int(rng.integers(0, 3))
+        n = float(np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1]))))
+        E = float(rng.uniform(50e3, 250e3))
+        mu = float(rng.uniform(0.2, 0.35))
+        steps = int(rng.integers(steps_range[0], steps_range[1] + 1))
+        plastic = bool(rng.random() < 0.5)
+        if lat == 0:
+            side = round(math.sqrt(n / 29.0), 1)  # hexagonal plate at r = 0.1: ~29 particles per mm^2
+            c = hex_plate(size=side, radius=0.1, E=E, mu=mu, steps=steps, total_disp=strain * side)
+        else:
+            lattice = L.LatticeType.SimpleCubic3D if lat == 1 else L.LatticeType.BCC3D
+            per_edge = n ** (1.0 / 3.0) if lat == 1 else (n / 2.0) ** (1.0 / 3.0)
+            cellw = 0.4 if lat == 1 else 4 * 0.2 / math.sqrt(3.0)
+            side = round(per_edge * cellw, 1)
+            c = sc_cube(size=side, radius=0.2, E=E, mu=mu, steps=steps, total_disp=strain * side, lattice=lattice,
+                        ptype=L.ParticleType.J2Plasticity if plastic else L.ParticleType.Elastic,
+                        j2=j2 if plastic else None)
+        c.name = f"req{k:02d}_{c.name}"
+        c.meta.update({"arrival": t, "seed": seed, "index": k})
+        out.append((t, c))
     return out
