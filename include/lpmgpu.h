@@ -77,6 +77,12 @@ typedef struct
      * bond_damage: initial bond damage in the same order (1 = broken). */
     const int32_t *bond_nb0, *bond_nb1, *bond_p2;
     const double *bond_kn, *bond_tv, *bond_damage;
+    /* 1: tangent mode: K is re-assembled from the current state before every Newton linear
+     * solve (and not at the start of a damage iteration).  0: K fixed per load step, as in
+     * SolverStatic::solveProblemStep (solver_static.h:107-118).  No counterpart in
+     * SolverStatic; its Newton loop and assembly calls are those of solver.h:55-90 and
+     * stiffness.h, re-ordered. */
+    int32_t tangent;
 } lpmgpu_desc;
 
 /* Displacement / force boundary condition of one load step (boundary.h:10-44, Relative mode). */

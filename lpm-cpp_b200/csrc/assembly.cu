@@ -449,7 +449,7 @@ __global__ void k_diag_norm(int64_t m, const double *__restrict__ diag, Scalars 
 __global__ void k_bc_diag(int n, int dim, const int *__restrict__ perm, const int64_t *__restrict__ slice_off,
                           const int *__restrict__ cstart, const int *__restrict__ nlq, const int *__restrict__ cons,
                           const double *__restrict__ damage_visual, const Scalars *__restrict__ scal,
-                          double *__restrict__ K)
+                          double *__restrict__ K, double *__restrict__ res)
 {
     const int pos = blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n)
@@ -461,7 +461,10 @@ __global__ void k_bc_diag(int n, int dim, const int *__restrict__ perm, const in
     const double nd = scal->norm_diag;
     for (int k = 0; k < dim; ++k)
         if (cons[3 * i + k] == 1 || dmg)
+        {
             K[(b * dim * dim + k * dim + k) * kSlice + pos % kSlice] = nd;
+            res[(int64_t)dim * i + k] = 0.0; // updateStiffnessDispBC zeroes the residual (stiffness.h:434)
+        }
 }
 
 cudaError_t launch_assemble(Problem &p, bool apply_bc)
@@ -513,7 +516,7 @@ cudaError_t launch_assemble(Problem &p, bool apply_bc)
     {
         k_diag_norm<<<1, 1024, 0, p.stream>>>((int64_t)p.n * p.dim, p.diag_raw, p.scal);
         k_bc_diag<<<div_up(p.n, 256), 256, 0, p.stream>>>(p.n, p.dim, p.perm, p.slice_off, p.cstart, p.nlq, p.cons,
-                                                          p.damage_visual, p.scal, p.K);
+                                                          p.damage_visual, p.scal, p.K, p.res);
         p.ctr.kernel_launches += 2;
         e = cudaGetLastError();
     }

@@ -811,7 +811,7 @@ struct lpmgpu_batch
         lpmgpu_load_step ls{db.data(), (int32_t)db.size(), fb.data(), (int32_t)fb.size()};
         Problem &p = P(m);
         cudaError_t e = launch_apply_bc(p, ls);
-        if (e == cudaSuccess)
+        if (e == cudaSuccess && !p.desc.tangent) // tangent mode assembles before every solve
             e = enqueue_assemble(p, true);
         if (e == cudaSuccess)
             e = enqueue_force_state(p, true);
@@ -918,6 +918,13 @@ struct lpmgpu_batch
         Problem &p = P(m);
         m.cur.newton_solves++;
         m.ls_fresh = true;
+        if (p.desc.tangent)
+        {
+            // tangent mode: K (and its FP32 copy) from the current state before every solve
+            const cudaError_t e0 = enqueue_assemble(p, true);
+            if (e0 != cudaSuccess)
+                return fail_member(m, cuda_status(e0, "batch tangent assembly"));
+        }
         if (p.desc.precision != LPMGPU_MIXED)
         {
             m.ph = Ph::NeedCG;
@@ -993,7 +1000,7 @@ struct lpmgpu_batch
             {
                 // damage loop (solver_static.h:126-139): force state, then assemble + Newton again
                 e = enqueue_force_state(p, false);
-                if (e == cudaSuccess)
+                if (e == cudaSuccess && !p.desc.tangent)
                     e = enqueue_assemble(p, true);
                 if (e == cudaSuccess)
                     e = enqueue_force_state(p, true);

@@ -151,6 +151,8 @@ static int32_t newton(Problem &p, lpmgpu_stats *st, int *ni)
                 st->residual_norm = nres;
             return LPMGPU_OK;
         }
+        if (p.desc.tangent)
+            ST(assemble(p, true)); // tangent mode: K from the current state before every solve
         ST(linear_solve(p, st));
         CK(launch_add_disp(p));
         ST(force_state(p, true));
@@ -214,7 +216,8 @@ static int32_t problem_step(Problem &p, const lpmgpu_load_step &s, lpmgpu_stats 
     {
         if (st)
             st->damage_iters++;
-        ST(assemble(p, true));
+        if (!p.desc.tangent)
+            ST(assemble(p, true));
         ST(newton(p, st, &n_newton));
         if (n_newton >= p.desc.max_iter)
             break;

@@ -86,7 +86,7 @@ class Desc(C.Structure):
         ("cg_maxit", C.c_int64), ("precision", C.c_int32), ("device", C.c_int32),
         ("bond_nb0", C.POINTER(C.c_int32)), ("bond_nb1", C.POINTER(C.c_int32)), ("bond_p2", C.POINTER(C.c_int32)),
         ("bond_kn", C.POINTER(C.c_double)), ("bond_tv", C.POINTER(C.c_double)),
-        ("bond_damage", C.POINTER(C.c_double)),
+        ("bond_damage", C.POINTER(C.c_double)), ("tangent", C.c_int32),
     ]
 
 
@@ -491,7 +491,7 @@ class _CStep:
 
 # ---------------------------------------------------------------------------- solver
 def _pack_desc(ass: Assembly, undamaged_pt_type=-1, max_iter=30, tol_iter=1e-5, precision=0, cg_rtol=1e-12,
-               cg_atol=1e-12, cg_maxit=0, device=0):
+               cg_atol=1e-12, cg_maxit=0, device=0, tangent=False):
     """lpmgpu_desc of an Assembly and solver settings; returns (desc, arrays the desc points into)."""
     m = ass.material
     d = Desc()
@@ -504,6 +504,7 @@ def _pack_desc(ass: Assembly, undamaged_pt_type=-1, max_iter=30, tol_iter=1e-5, 
     d.undamaged_type, d.max_iter, d.tol_iter = int(undamaged_pt_type), int(max_iter), float(tol_iter)
     d.cg_rtol, d.cg_atol, d.cg_maxit = float(cg_rtol), float(cg_atol), int(cg_maxit)
     d.precision, d.device = int(precision), int(device)
+    d.tangent = int(bool(tangent))
     if ass.bonds is not None:
         nb0, nb1, p2 = (np.ascontiguousarray(a, dtype=np.int32) for a in ass.bonds)
         keep += [nb0, nb1, p2]
@@ -521,11 +522,14 @@ class GpuProblem:
     """One device-resident problem: the handle of include/lpmgpu.h."""
 
     def __init__(self, ass: Assembly, undamaged_pt_type=-1, max_iter=30, tol_iter=1e-5,
-                 precision: Precision = Precision.FP64, cg_rtol=1e-12, cg_atol=1e-12, cg_maxit=0, device=0):
+                 precision: Precision = Precision.FP64, cg_rtol=1e-12, cg_atol=1e-12, cg_maxit=0, device=0,
+                 tangent: bool = False):
+        """tangent: re-assemble K from the current state before every Newton solve (the
+        default keeps K fixed per load step, as SolverStatic does)."""
         L = lib()
         self.ass = ass
         d, self._keep = _pack_desc(ass, undamaged_pt_type, max_iter, tol_iter, precision, cg_rtol, cg_atol, cg_maxit,
-                                   device)
+                                   device, tangent)
         h = C.c_void_p()
         _check(L.lpmgpu_create(C.byref(d), C.byref(h)), "lpmgpu_create")
         self._h = h
@@ -740,9 +744,10 @@ class Server:
         _check(lib().lpmgpu_server_set_slice(self._h, int(iterations)), "lpmgpu_server_set_slice")
 
     def submit(self, ass: Assembly, steps: Sequence[LoadStep], undamaged_pt_type=-1, max_iter=30, tol_iter=1e-5,
-               precision: Precision = Precision.FP64, cg_rtol=1e-12, cg_atol=1e-12, cg_maxit=0) -> int:
+               precision: Precision = Precision.FP64, cg_rtol=1e-12, cg_atol=1e-12, cg_maxit=0,
+               tangent: bool = False) -> int:
         d, keep = _pack_desc(ass, undamaged_pt_type, max_iter, tol_iter, precision, cg_rtol, cg_atol, cg_maxit,
-                             self.device)
+                             self.device, tangent)
         cs = [_CStep(s) for s in steps]
         arr = (CLoadStep * max(len(cs), 1))(*[c.s for c in cs])
         rid = C.c_int64(0)

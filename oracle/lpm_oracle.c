@@ -40,7 +40,7 @@ struct lpmo_problem
     int *nlstart, *nlist;
     /* material */
     double E, mu, critical_bstrain, sigmay, xi, H, A, damage_threshold, nonlocal_L;
-    int undamaged_type, max_iter;
+    int undamaged_type, max_iter, tangent;
     double tol, cg_rtol, cg_atol;
     long long cg_maxit;
     /* stiffness, reference layout (stiffness.h:24-26) */
@@ -712,6 +712,7 @@ lpmo_problem *lpmo_create(const lpmo_desc *d)
     }
     p->undamaged_type = d->undamaged_type;
     p->max_iter = d->max_iter;
+    p->tangent = d->tangent;
     p->tol = d->tol_iter;
     p->cg_rtol = d->cg_rtol;
     p->cg_atol = d->cg_atol;
@@ -1437,6 +1438,8 @@ static int newton(lpmo_problem *p, lpmo_stats *st)
             free(disp);
             return p->max_iter;
         }
+        if (p->tangent)
+            lpmo_assemble(p, 1);
         long long it = lpmo_cg(p, disp);
         if (st)
         {
@@ -1543,7 +1546,8 @@ int lpmo_solve_problem_step(lpmo_problem *p, const lpmo_loadstep *s, lpmo_stats 
     int n_newton = 0, new_damaged = 0;
     do
     {
-        lpmo_assemble(p, 1);
+        if (!p->tangent)
+            lpmo_assemble(p, 1);
         n_newton = newton(p, st);
         if (n_newton >= p->max_iter)
             break;

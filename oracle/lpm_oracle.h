@@ -38,6 +38,10 @@ typedef struct
      * nb1[i] layer-1 partners, concatenated in p2 (Assembly(dumpFile, bondFile, ...) and
      * Assembly::readBond, assembly.h:84-95, 391-424); NULL -> Assembly::createBonds */
     const int *bond_nb0, *bond_nb1, *bond_p2;
+    /* 1: tangent mode, the stiffness re-assembled from the current state before every Newton
+     * solve (no assembly at the start of a damage iteration); 0: K fixed per load step as in
+     * SolverStatic::solveProblemStep (solver_static.h:107-118) */
+    int tangent;
 } lpmo_desc;
 
 typedef struct

@@ -35,6 +35,7 @@ class _Desc(C.Structure):
         ("undamaged_type", C.c_int), ("max_iter", C.c_int), ("tol_iter", C.c_double),
         ("cg_rtol", C.c_double), ("cg_atol", C.c_double), ("cg_maxit", C.c_longlong),
         ("bond_nb0", C.POINTER(C.c_int)), ("bond_nb1", C.POINTER(C.c_int)), ("bond_p2", C.POINTER(C.c_int)),
+        ("tangent", C.c_int),
     ]
 
 
@@ -174,9 +175,9 @@ class OracleProblem:
 
     def __init__(self, lattice: str, radius: float, xyz: np.ndarray, mat: Material, types=None,
                  undamaged_type=-1, max_iter=30, tol_iter=1e-5, cg_rtol=1e-12, cg_atol=1e-12, cg_maxit=0,
-                 nonlocal_cutoff_ratio=0.0, bonds=None):
+                 nonlocal_cutoff_ratio=0.0, bonds=None, tangent=False):
         """bonds: optional (nb0, nb1, p2) lists as Assembly::readBond builds them; None runs the
-        reference's bond search."""
+        reference's bond search.  tangent: re-assemble K before every Newton solve."""
         self.xyz0 = np.ascontiguousarray(xyz, dtype=np.float64)
         self.n = len(self.xyz0)
         self.types = np.ascontiguousarray(types if types is not None else np.zeros(self.n), dtype=np.int32)
@@ -189,6 +190,7 @@ class OracleProblem:
         d.nonlocal_L, d.nonlocal_cutoff_ratio = mat.nonlocal_L, nonlocal_cutoff_ratio
         d.undamaged_type, d.max_iter, d.tol_iter = undamaged_type, max_iter, tol_iter
         d.cg_rtol, d.cg_atol, d.cg_maxit = cg_rtol, cg_atol, cg_maxit
+        d.tangent = int(bool(tangent))
         if bonds is not None:
             self._bonds = [np.ascontiguousarray(a, dtype=np.int32) for a in bonds]
             d.bond_nb0, d.bond_nb1, d.bond_p2 = (_ip(a) for a in self._bonds)
@@ -342,7 +344,7 @@ def write_bond_file(path: str, nb0, nb1, p2):
 
 
 def write_ref_spec(case, outdir: str, steps=None, max_iter=None, tol_iter=None, cg_tol=None, cg_maxit_cap=0,
-                   dump_k=(), loop="step", use_generator=True) -> str:
+                   dump_k=(), loop="step", use_generator=True, tangent=False) -> str:
     """Spec text for oracle/_ref/lpm_ref describing a product-side ``Case`` (duck-typed):
     groups and particle types are passed as raw int32 id files so both sides see the same sets.
     With use_generator the reference generates the lattice itself (its ids must then equal
@@ -360,6 +362,8 @@ def write_ref_spec(case, outdir: str, steps=None, max_iter=None, tol_iter=None, 
              f"tol_iter {(case.tol_iter if tol_iter is None else tol_iter)!r}", f"loop {loop}"]
     if cg_maxit_cap:
         lines.append(f"cg_maxit_cap {int(cg_maxit_cap)}")
+    if tangent:
+        lines.append("tangent 1")
     if cg_tol is not None:
         lines.append(f"cg_tol {cg_tol[0]!r} {cg_tol[1]!r}")
     if not use_generator or lat == "bcc3d":

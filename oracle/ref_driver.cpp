@@ -35,6 +35,10 @@
  *                          Assembly is then built by Assembly(dumpFile, bondFile, cell, ptype),
  *                          include/assembly.h:84-95, from a dump of the coordinates written
  *                          at full precision; pre-cracks by bond exclusion)
+ *   tangent 1             (tangent mode: the step of SolverStatic::solveProblemStep with the
+ *                          stiffness re-assembled from the current state before every linear
+ *                          solve of Solver::NewtonIteration, and not at the start of a damage
+ *                          iteration; "loop step|once" only)
  *   bondprops PATH        (raw f64: Kn[nb], Tv[nb], bdamage[nb] in bond order, written into
  *                          Bond::Kn / Tv / bdamage and bdamage_last (include/bond.h:25-27) after
  *                          setParticleProperty: a heterogeneous material or initial damage)
@@ -124,6 +128,7 @@ struct Spec
     std::string typefile;
     std::string bondfile;
     std::string bondprops;
+    int tangent = 0;
     double cg_rtol = -1, cg_atol = -1;
 };
 
@@ -239,6 +244,7 @@ static Spec parse(const char *path)
         else if (k == "cg_tol") is >> s.cg_rtol >> s.cg_atol;
         else if (k == "bondfile") is >> s.bondfile;
         else if (k == "bondprops") is >> s.bondprops;
+        else if (k == "tangent") is >> s.tangent;
         else
         {
             std::fprintf(stderr, "unknown spec directive '%s'\n", k.c_str());
@@ -303,6 +309,64 @@ static Assembly<NL> make_assembly(std::vector<std::array<double, NDIM>> &xyz, st
     return Assembly<NL>{dump, sp.bondfile, cell, pt};
 }
 
+#ifndef LPM_USE_GPU
+/* Tangent mode: SolverStatic::solveProblemStep (include/solver_static.h:99-152) whose Newton loop
+ * (Solver::NewtonIteration, include/solver.h:55-90) re-assembles the stiffness from the current
+ * state (Stiffness::reset + calcStiffness2D/3D + updateStiffnessDispBC, include/stiffness.h)
+ * before every solveLinearSystem, instead of once per damage iteration.  Every call is the
+ * reference's own code; only the place of the assembly differs. */
+static bool tangent_step(SolverStatic<NL> &solv, LoadStep<NL> &load_step)
+{
+    solv.updateForceBC(load_step);
+    solv.updateDisplacementBC(load_step);
+    auto &pts = solv.ass.pt_sys;
+    int n_newton = 0;
+    bool new_damaged = false;
+    do
+    {
+        solv.ass.updateGeometry();
+        solv.ass.updateForceState();
+        solv.updateRR();
+        double norm_residual = cblas_dnrm2(solv.problem_size, solv.stiffness.residual, 1);
+        const double norm_reaction =
+            cblas_dnrm2((MKL_INT)solv.reaction_force.size(), solv.reaction_force.data(), 1);
+        const double tol_multiplier = std::max(norm_residual, norm_reaction);
+        int ni = 0;
+        while (norm_residual > solv.tol_NR_iter * tol_multiplier)
+        {
+            if (++ni > solv.max_NR_iter)
+            {
+                ni = solv.max_NR_iter;
+                break;
+            }
+            solv.stiffness.reset(pts);
+            if (pts[0]->cell.dim == 2)
+                solv.stiffness.calcStiffness2D(pts);
+            else
+                solv.stiffness.calcStiffness3D(pts);
+            solv.stiffness.updateStiffnessDispBC(pts);
+            solv.solveLinearSystem();
+            solv.ass.updateGeometry();
+            solv.ass.updateForceState();
+            solv.updateRR();
+            norm_residual = cblas_dnrm2(solv.problem_size, solv.stiffness.residual, 1);
+        }
+        n_newton = ni;
+        if (n_newton >= solv.max_NR_iter)
+            break;
+        solv.ass.updateStateVar();
+        new_damaged = solv.updateStaticDamage();
+        solv.ass.storeStateVar();
+        if (new_damaged)
+        {
+            solv.ass.updateGeometry();
+            solv.ass.updateForceState();
+        }
+    } while (new_damaged);
+    return n_newton < solv.max_NR_iter;
+}
+#endif
+
 int main(int argc, char **argv)
 {
     if (argc < 2)
@@ -311,6 +375,11 @@ int main(int argc, char **argv)
         return 2;
     }
     Spec sp = parse(argv[1]);
+    if (sp.tangent && sp.loop == "ref")
+    {
+        std::fprintf(stderr, "tangent mode needs loop step or once\n");
+        return 2;
+    }
     lpm_shim_stats_g.cg_maxit_override = sp.cg_maxit_cap;
     lpm_shim_stats_g.cg_rtol_override = sp.cg_rtol;
     lpm_shim_stats_g.cg_atol_override = sp.cg_atol;
@@ -507,7 +576,12 @@ int main(int argc, char **argv)
         {
             /* one SolverStatic::solveProblemStep call, no retry: a bounded sample of the step */
             double dt = 1;
-            cuts = solv.solveProblemStep(load[s], dt) ? 0 : -1;
+#ifndef LPM_USE_GPU
+            if (sp.tangent)
+                cuts = tangent_step(solv, load[s]) ? 0 : -1;
+            else
+#endif
+                cuts = solv.solveProblemStep(load[s], dt) ? 0 : -1;
         }
         else if (sp.loop == "ref")
         {
@@ -523,7 +597,11 @@ int main(int argc, char **argv)
             double dt = 1;
             for (int i = 0; i < n_step; i++)
             {
+#ifndef LPM_USE_GPU
+                bool ok = sp.tangent ? tangent_step(solv, one[i]) : solv.solveProblemStep(one[i], dt);
+#else
                 bool ok = solv.solveProblemStep(one[i], dt);
+#endif
                 if (!ok)
                 {
 #ifdef LPM_USE_GPU

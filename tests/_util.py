@@ -17,7 +17,7 @@ CFG = importlib.import_module("lpm-cpp_b200.configs")
 LAT_NAME = {0: "sq2d", 1: "hex2d", 2: "sc3d", 3: "fcc3d", 4: "bcc3d"}
 
 
-def oracle_problem(case, cg_rtol=1e-12, cg_atol=1e-12, tol_iter=None, max_iter=None):
+def oracle_problem(case, cg_rtol=1e-12, cg_atol=1e-12, tol_iter=None, max_iter=None, tangent=False):
     m = case.material
     mat = O.Material(ptype="j2" if int(case.ptype) == 2 else "elastic", plane_stress=m.plane_stress, E=m.E, mu=m.mu,
                      critical_bstrain=m.critical_bstrain, sigmay=m.sigmay, xi=m.xi, H=m.H, A=m.A,
@@ -26,7 +26,7 @@ def oracle_problem(case, cg_rtol=1e-12, cg_atol=1e-12, tol_iter=None, max_iter=N
                         undamaged_type=case.undamaged_type,
                         max_iter=case.max_iter if max_iter is None else max_iter,
                         tol_iter=case.tol_iter if tol_iter is None else tol_iter, cg_rtol=cg_rtol, cg_atol=cg_atol,
-                        bonds=getattr(case, "bonds", None))
+                        bonds=getattr(case, "bonds", None), tangent=tangent)
     if getattr(case, "bond_props", None) is not None:
         kn, tv, dmg = case.bond_props
         o.set_bond_kntv(kn, tv)
@@ -54,8 +54,8 @@ def hetero_plate(size=2.4, steps=3, total_disp=0.003, seed=3):
     return case
 
 
-def gpu_problem(case, precision=0, cg_rtol=1e-12, cg_atol=1e-12, tol_iter=None, max_iter=None):
-    return LPM.GpuProblem(case.assembly(), undamaged_pt_type=case.undamaged_type,
+def gpu_problem(case, precision=0, cg_rtol=1e-12, cg_atol=1e-12, tol_iter=None, max_iter=None, tangent=False):
+    return LPM.GpuProblem(case.assembly(), undamaged_pt_type=case.undamaged_type, tangent=tangent,
                           max_iter=case.max_iter if max_iter is None else max_iter,
                           tol_iter=case.tol_iter if tol_iter is None else tol_iter,
                           precision=LPM.Precision(precision), cg_rtol=cg_rtol, cg_atol=cg_atol)

@@ -76,6 +76,12 @@ def cases():
                                                 tol_iter=1e-9), {"cg_tol": (1e-24, 0.0), "dump_k": (0,)}),
         # per-bond Kn/Tv and initially broken bonds written into the bonds (bond.h:25-27)
         "hex_hetero": (hetero_plate, {"cg_tol": (1e-24, 0.0), "dump_k": (0,)}),
+        # tangent mode: the stiffness re-assembled before every Newton solve (driver directive
+        # "tangent 1", the reference's own Newton loop and stiffness calls re-ordered)
+        "fcc_j2_tangent": (lambda: CFG.fcc_bar(size=(1.2, 1.2, 1.6), radius=0.2, steps=3, strain=0.02),
+                           {"cg_tol": (1e-24, 0.0), "tangent": True, "dump_k": (2,)}),
+        "hex_crack_tangent": (lambda: CFG.notched_plate(size=2.0, radius=0.1, crack=0.3, steps=6, total_disp=0.006,
+                                                        tol_iter=1e-9), {"cg_tol": (1e-24, 0.0), "tangent": True}),
     }
 
 
@@ -83,7 +89,9 @@ def make(name, build, opts):
     case = build()
     d = tempfile.mkdtemp(prefix=f"golden_{name}_")
     try:
-        spec = O.write_ref_spec(case, d, cg_tol=opts.get("cg_tol"), dump_k=opts.get("dump_k", ()), loop="ref")
+        tangent = bool(opts.get("tangent", False))
+        spec = O.write_ref_spec(case, d, cg_tol=opts.get("cg_tol"), dump_k=opts.get("dump_k", ()),
+                                loop="step" if tangent else "ref", tangent=tangent)
         O.run_ref(spec, d, threads=1)
         rb = lambda f, t: O.read_bin(d, f, t)  # noqa: E731
         out = {"xyz0": rb("xyz0.f64", np.float64).reshape(-1, 3)}
@@ -105,7 +113,8 @@ def make(name, build, opts):
                 out[f"state_var_{s}"] = rb(f"state_var_{tag}.f64", np.float64).reshape(-1, 7)
             if case.material.critical_bstrain < 1.0 or case.bond_props is not None:
                 out[f"bdamage_{s}"] = rb(f"bdamage_{tag}.f64", np.float64)
-        out["meta"] = np.array(json.dumps({"name": name, "opts": {k: list(v) for k, v in opts.items()},
+        out["meta"] = np.array(json.dumps({"name": name,
+                                           "opts": {k: (list(v) if isinstance(v, tuple) else v) for k, v in opts.items()},
                                            "n": int(case.n), "spec": spec}))
         path = os.path.join(HERE, f"{name}.npz")
         np.savez_compressed(path, **out)

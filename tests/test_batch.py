@@ -154,3 +154,33 @@ def test_batch_paused_solves_resume(precision, tol):
     batch.close()
     for g in gs:
         g.close()
+
+
+@pytest.mark.parametrize("precision,tol", [(0, FP64_TOL), (1, MIXED_TOL)])
+def test_batch_tangent_members_match_alone(precision, tol):
+    """Tangent-mode members (K re-assembled before every Newton solve) in a batch give the
+    results they give alone."""
+    cases = [CFG.fcc_bar(size=(1.6, 1.6, 2.4), radius=0.2, steps=3, strain=0.02),
+             CFG.notched_plate(size=2.0, radius=0.1, crack=0.3, steps=6, total_disp=0.006)]
+    refs = []
+    for c in cases:
+        g = gpu_problem(c, tangent=True, **TIGHT)
+        st = []
+        for s in range(len(c.steps)):
+            ok, x = g.solve_load_step(c.load_step(s))
+            assert ok
+            st.append(x)
+        refs.append((g.state(), st))
+        g.close()
+    batch = LPM.Batch()
+    gs, mids = [], []
+    for c in cases:
+        g = gpu_problem(c, precision=precision, tangent=True, **TIGHT)
+        gs.append(g)
+        mids.append(batch.add(g, [c.load_step(s) for s in range(len(c.steps))]))
+    batch.run()
+    for c, g, mid, (ref_state, ref_steps) in zip(cases, gs, mids, refs):
+        _check_member(c, batch, mid, g, ref_state, ref_steps, tol, compare_counts=(precision == 0))
+    batch.close()
+    for g in gs:
+        g.close()

@@ -270,3 +270,35 @@ def test_bond_coefficients_and_initial_damage():
         assert okg and oko
         assert rel(g.state()["xyz"] - case.xyz, o.state()["xyz"] - case.xyz) <= FP64_DISP_TOL
     assert np.array_equal(g.state()["bdamage"], o.state()["bdamage"])
+
+
+TANGENT_CASES = {
+    "fcc_j2": lambda: CFG.fcc_bar(size=(1.6, 1.6, 2.4), radius=0.2, steps=3, strain=0.02),
+    "hex_crack": lambda: CFG.notched_plate(size=2.0, radius=0.1, crack=0.3, steps=6, total_disp=0.006),
+}
+
+
+@pytest.mark.parametrize("name", sorted(TANGENT_CASES))
+@pytest.mark.parametrize("precision,tol", [(0, FP64_DISP_TOL), (1, MIXED_DISP_TOL)])
+def test_tangent_mode_matches_oracle(name, precision, tol):
+    """Tangent mode (K re-assembled from the current state before every Newton solve): the
+    device against the oracle in the same mode, itself pinned to the reference's own Newton
+    loop and stiffness calls (golden fixtures fcc_j2_tangent, hex_crack_tangent)."""
+    case = TANGENT_CASES[name]()
+    kw = dict(cg_rtol=1e-24, cg_atol=0.0, tol_iter=1e-9, tangent=True)
+    g = gpu_problem(case, precision=precision, **kw)
+    o = oracle_problem(case, **kw)
+    o.update_geometry()
+    o.update_force_state()
+    for s in range(len(case.steps)):
+        okg, stg = g.solve_load_step(case.load_step(s))
+        oko, sto = o.solve_load_step(*oracle_step_args(case, s))
+        assert okg and oko
+        if precision == 0:
+            assert stg["newton_solves"] == sto["newton_solves"], f"step {s}"
+            assert np.array_equal(g.state()["bdamage"] == 1.0, o.state()["bdamage"] == 1.0)
+        e = rel(g.state()["xyz"] - case.xyz, o.state()["xyz"] - case.xyz)
+        assert e <= tol, f"step {s}: rel disp err {e}"
+    if precision == 0:
+        K, oK = g.export_csr()[3], o.export_csr()[3]
+        assert np.abs(K - oK).max() <= 1e-12 * np.abs(oK).max()
