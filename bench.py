@@ -58,6 +58,8 @@ def args_():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched 64-plate damage workload")
     ap.add_argument("--plates", type=int, default=64, help="plates in the batched damage workload")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
+    ap.add_argument("--no-tangent", action="store_true", help="skip the FCC J2 tangent-mode leg")
+    ap.add_argument("--tangent-steps", type=int, default=4, help="load steps of the FCC bar's 50-step path timed")
     ap.add_argument("--serve-requests", type=int, default=12, help="requests in the serving-stream sample")
     ap.add_argument("--serve-max-particles", type=float, default=1e5,
                     help="upper end of the log-uniform particle count (the stream's full range is 5e3-5e5)")
@@ -317,6 +319,10 @@ def run_ours(a):
     if not a.no_batched:
         barrier()
         batched = batched_leg(lpm, a.plates, local, world, allreduce)
+    tangent = None
+    if not a.no_tangent:
+        barrier()
+        tangent = tangent_leg(lpm, a.tangent_steps, local, world, allreduce)
     serving = None
     if not a.no_serving:
         barrier()
@@ -343,7 +349,7 @@ def run_ours(a):
                                    "force": (c1["force_seconds"] - c0["force_seconds"]) * 1e3 / K,
                                    "cg_kernel": cg_s * 1e3 / K},
             "roofline": roof, "e2e": e2e, "gpu_launches": counters_total, "clocks": clocks,
-            "mixed": mixed, "batched": batched, "serving": serving, "cpu_baseline": cpu,
+            "mixed": mixed, "batched": batched, "serving": serving, "tangent": tangent, "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
     if dist:
@@ -425,6 +431,50 @@ def batched_leg(lpm, count, device, world, allreduce):
             "plain_fp64_one_at_a_time": plain, "batched_fp64": fp64, "batched_mixed": mixed,
             "speedup_batched_mixed_vs_plain_fp64": mixed["solves_per_s"] / plain["solves_per_s"],
             "speedup_batched_fp64_vs_plain_fp64": fp64["solves_per_s"] / plain["solves_per_s"]}
+
+
+def tangent_leg(lpm, steps, device, world, allreduce):
+    """FCC single-crystal bar in J2 plasticity with the tangent re-assembled before every Newton
+    solve (lpm-cpp_b200/configs.fcc_bar): 16 x 16 x 32 mm at r = 0.18 mm (248,319 particles,
+    lattice constant 0.509 mm), seeded uniform orientation, E 110 GPa, nu 0.34, sigma_y = CRSS 60 MPa
+    x Taylor factor 3.06, H = 500 MPa, tension to 1% strain in 50 steps.  The first `steps` steps
+    of the path are timed (a bounded sample), in FP64 and in mixed precision (FP32 Krylov in FP64
+    refinement; the return mapping and the assembly stay FP64); device time of the library's
+    stream.  Error: the mixed displacement against FP64 after the same steps."""
+    import torch
+    cfg = importlib.import_module("lpm-cpp_b200.configs")
+    c = cfg.fcc_bar(size=(16.0, 16.0, 32.0), radius=0.18, steps=50, strain=0.01)
+    out, xyz = {}, {}
+    for prec, key in ((0, "fp64"), (1, "mixed")):
+        g = lpm.GpuProblem(c.assembly(), undamaged_pt_type=c.undamaged_type, max_iter=c.max_iter,
+                           tol_iter=NEWTON_TOL, precision=lpm.Precision(prec), device=device, tangent=True)
+        s0 = torch.cuda.ExternalStream(g.stream_ptr())
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0 = g.counters()
+        e0.record(s0)
+        newton = iters = 0
+        for s in range(steps):
+            ok, st = g.solve_load_step(c.load_step(s))
+            assert ok, f"FCC bar step {s} failed"
+            newton += st["newton_solves"]
+            iters += st["cg_iters"]
+        e1.record(s0)
+        torch.cuda.synchronize()
+        ms = allreduce(e0.elapsed_time(e1), "max")
+        c1 = g.counters()
+        xyz[key] = g.state(("xyz",))["xyz"]
+        out[key] = {"ms_per_step": ms / steps, "dof_iter_per_s": allreduce(float(iters * c.n * 3), "sum") / (ms * 1e-3),
+                    "newton_per_step": newton / steps, "cg_iters_per_step": iters / steps,
+                    "assembly_ms_per_newton": (c1["assembly_seconds"] - c0["assembly_seconds"]) * 1e3 / max(newton, 1),
+                    "assembly_share": (c1["assembly_seconds"] - c0["assembly_seconds"]) / (ms * 1e-3)}
+        g.close()
+    u64, um = xyz["fp64"] - c.xyz, xyz["mixed"] - c.xyz
+    out["mixed"]["rel_disp_err_vs_fp64"] = float(np.linalg.norm(um - u64) / np.linalg.norm(u64))
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    out["workload"] = (f"FCC J2 bar 16x16x32 mm, r=0.18 ({c.n} particles), tangent re-assembled every Newton "
+                       f"iteration, first {steps} of 50 steps to 1% strain, Newton tol {NEWTON_TOL}")
+    return out
 
 
 def serving_leg(lpm, count, nmax, device, world, allreduce):
