@@ -315,16 +315,18 @@ def run_ours(a):
                  "speedup_vs_fp64": (ms_max / K) / (mms / K)}
         pm.close()
 
+    # the batched, tangent and serving legs are one-GPU workloads: replicas (N > 1) skip them
+    single = world == 1
     batched = None
-    if not a.no_batched:
+    if single and not a.no_batched:
         barrier()
         batched = batched_leg(lpm, a.plates, local, world, allreduce)
     tangent = None
-    if not a.no_tangent:
+    if single and not a.no_tangent:
         barrier()
         tangent = tangent_leg(lpm, a.tangent_steps, local, world, allreduce)
     serving = None
-    if not a.no_serving:
+    if single and not a.no_serving:
         barrier()
         serving = serving_leg(lpm, a.serve_requests, a.serve_max_particles, local, world, allreduce)
 

@@ -302,3 +302,54 @@ def test_tangent_mode_matches_oracle(name, precision, tol):
     if precision == 0:
         K, oK = g.export_csr()[3], o.export_csr()[3]
         assert np.abs(K - oK).max() <= 1e-12 * np.abs(oK).max()
+
+
+def test_bond_list_overflow_is_a_topology_error():
+    """More bonds on one particle than the fixed per-particle staging holds (32) is rejected
+    with LPMGPU_ERR_TOPOLOGY, not truncated."""
+    c = CFG.hex_plate(size=2.0, radius=0.1, steps=1, total_disp=0.001)
+    nb0, nb1, p2 = CFG.bond_lists(c.xyz, LPM.UnitCell(c.lattice, c.radius))
+    nb0, nb1 = nb0.copy(), nb1.copy()
+    extra = np.arange(1, 34, dtype=np.int32)  # particle 0 claims 33 layer-1 partners
+    start1 = int(nb0[0])
+    p2 = np.concatenate([p2[:start1], extra, p2[int(nb0[0] + nb1[0]):]]).astype(np.int32)
+    nb1[0] = len(extra)
+    ass = c.assembly()
+    ass.bonds = (nb0, nb1, p2)
+    with pytest.raises(LPM.LpmGpuError) as e:
+        LPM.GpuProblem(ass)
+    assert e.value.status == 7
+
+
+def test_step_without_boundary_conditions_is_a_no_op():
+    """A load step with no displacement or force condition leaves a body at rest: Newton
+    converges before any linear solve, on the device and in the oracle."""
+    c = CFG.hex_plate(size=2.0, radius=0.1, steps=1, total_disp=0.001)
+    g = gpu_problem(c)
+    o = oracle_problem(c)
+    o.update_geometry()
+    o.update_force_state()
+    okg, stg = g.solve_load_step(LPM.LoadStep())
+    oko, sto = o.solve_load_step([], [])
+    assert okg and oko
+    assert stg["newton_solves"] == sto["newton_solves"] == 0
+    assert np.array_equal(g.state()["xyz"], c.xyz)
+
+
+@pytest.mark.parametrize("size", [0.4, 0.6])
+def test_tiny_plates_match_oracle(size):
+    """Plates of 4 and 12 particles (rows shorter than a slice, every particle on the boundary)."""
+    c = CFG.hex_plate(size=size, radius=0.1, steps=2, total_disp=0.002)
+    kw = dict(cg_rtol=1e-24, cg_atol=0.0, tol_iter=1e-9)
+    g = gpu_problem(c, **kw)
+    o = oracle_problem(c, **kw)
+    o.update_geometry()
+    o.update_force_state()
+    t = g.topology()
+    assert np.array_equal(t["conns"], o.conns()[2])
+    for s in range(2):
+        okg, _ = g.solve_load_step(c.load_step(s))
+        oko, _ = o.solve_load_step(*oracle_step_args(c, s))
+        assert okg == oko
+        if okg:
+            assert rel(g.state()["xyz"] - c.xyz, o.state()["xyz"] - c.xyz) <= FP64_DISP_TOL
