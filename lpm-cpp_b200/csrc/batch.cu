@@ -48,8 +48,9 @@ struct BInst
 {
     int dim, n, nslices;
     int fresh;          // 1: the solve starts here (r = b, x = 0); 0: it resumes a paused solve
-    int64_t ndof, cost; // cost: matrix entries (slots x d^2), the split weight
-    int64_t it0;        // iterations the solve had done before this launch
+    int refine;         // 1: FP32 inner solves inside an FP64 iterative refinement run in this launch
+    int pad;
+    int64_t ndof, cost; // cost: block slots x (d^2 + 1) (matrix entries + column index), the split weight
     const int *rowptr, *perm;
     const int64_t *slice_off;
     const int *col_sell;
@@ -57,20 +58,32 @@ struct BInst
     void *x, *r, *pa, *pb, *q;
     double rtol, atol, abs_stop;
     int64_t maxit;
+    // refinement (refine = 1): the FP64 system K64 x64 = res, its residual r64 and the outer
+    // squared-norm target stop64; the inner solve above works on (float) r64 with abs_stop
+    const double *K64, *res;
+    double *x64, *r64;
+    double stop64;
 };
 
+// One linear solve's CG state, kept across launches when a solve pauses.
 struct BState
 {
     double rr, stop, alpha, beta, rr0, rr_final;
-    int64_t it, status; // iterations of the solve; status bits: 1 iteration cap, 4 breakdown
-                        // (p.Ap == 0), 8 paused at the end of the launch's iteration slice
+    int64_t it;       // iterations of the current (inner) CG solve
+    int64_t it_total; // iterations of the whole linear solve (all refinements)
+    int64_t status;   // bits: 1 iteration cap, 4 breakdown (p.Ap == 0), 8 paused at the end of the launch
+    int32_t mode;     // 0 CG; refinement: 1 x64 += x32 next, 2 true residual next, 3 CG restarts next phase A
+    int32_t refs;     // refinement steps finished (inner solves)
+    int32_t caps;     // inner solves stopped by their cap
+    int32_t pad;
+    int64_t last_inner; // iterations of the last finished inner solve
 };
 
 struct BCtl
 {
     unsigned bar; // barrier arrivals: starts at zero, only counts up
     int fail;     // a wait timed out
-    int nact;     // problems in the initial rank tables
+    int nact;     // problems in the launch
     int pad;
 };
 
@@ -79,34 +92,26 @@ struct BArgs
     const BInst *inst;
     BState *st; // in: states of resumed solves; out (block 0, at the end): every problem's state
     BCtl *ctl;
-    const int *act0, *gcnt0, *vstart0; // initial rank tables (the host's split)
-    double *part;                      // [2][kMaxVirt] per-virtual-block partials, two buffers
+    // [6][kMaxVirt] per-piece partials.  CG: 1 = p.Ap (phase A), 0 = ||r||^2 (phase B and the
+    // start).  True residual of a refinement: 2, 3 in phase A and 4, 5 in phase B (||r64||^2,
+    // ||(float) r64||^2).  Consecutive phases never write the same buffer, so a block one phase
+    // ahead never overwrites partials another block still reads (the split, and with it the
+    // slot of each piece, may change between two phases).
+    double *part;
     int ninst;
-    int64_t slice; // iterations per launch; unfinished solves pause and resume later
+    int pause_left;  // pause the unfinished solves once this many problems left the launch (0: never)
+    int64_t slice;   // iterations per launch; unfinished solves pause and resume later
 };
 
-// Virtual blocks of one of `nact` problems: one each, plus its share (by matrix size) of the
-// G - nact blocks left, at most its slice count.  The total never exceeds G when nact <= G, so
-// every physical block carries at most one virtual block and the largest shares stay balanced.
-__host__ __device__ inline int vblocks_for(int64_t G, int nact, int64_t cost, int64_t C, int nslices)
-{
-    const int64_t R = G - nact;
-    int64_t g = 1 + ((R > 0 && C > 0) ? (R * cost) / C : 0);
-    if (g > nslices)
-        g = nslices;
-    if (g < 1)
-        g = 1;
-    return (int)g;
-}
-
 // ---- block-wide integer scans / sums (deterministic)
-__device__ int block_exscan(int v, int *total, int *sh)
+template <typename T>
+__device__ T block_exscan(T v, T *total, T *sh)
 {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int x = v;
+    T x = v;
     for (int o = 1; o < 32; o <<= 1)
     {
-        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        const T y = __shfl_up_sync(0xffffffffu, x, o);
         if (lane >= o)
             x += y;
     }
@@ -115,62 +120,138 @@ __device__ int block_exscan(int v, int *total, int *sh)
     __syncthreads();
     if (w == 0)
     {
-        int t = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : 0;
+        T t = (lane < (int)(blockDim.x >> 5)) ? sh[lane] : T(0);
         for (int o = 1; o < 32; o <<= 1)
         {
-            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            const T y = __shfl_up_sync(0xffffffffu, t, o);
             if (lane >= o)
                 t += y;
         }
         sh[lane] = t; // inclusive prefix of warp totals
     }
     __syncthreads();
-    const int before = (w > 0 ? sh[w - 1] : 0) + x - v;
+    const T before = (w > 0 ? sh[w - 1] : T(0)) + x - v;
     *total = sh[(blockDim.x >> 5) - 1];
     __syncthreads();
     return before;
 }
 
-__device__ int64_t block_sum_i64(int64_t v, long long *sh)
+// The split.  The active problems' costs are laid end to end (rank order) and cut into
+// gridDim.x equal segments, one per physical block: block b owns costs [b*C/G, (b+1)*C/G).
+// A problem's piece in block b is its part of that segment, rounded to whole slices by the
+// slices' starting cost (slice_off x (d^2 + 1)), so the pieces of one problem partition its
+// slices; the update phases take the rows' unknowns in proportion, [s0*ndof/ns, s1*ndof/ns).
+// Every SM carries the same matrix volume whatever the mix of sizes: a small problem shares a
+// block with its neighbours in rank order, a large one spans many blocks.
+__device__ __forceinline__ int seg_block(long long t, long long C, int G)
 {
-    for (int o = 16; o > 0; o >>= 1)
-        v += __shfl_xor_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0)
-        sh[threadIdx.x >> 5] = v;
-    __syncthreads();
-    int64_t t = 0;
-    for (int q = 0; q < (int)(blockDim.x >> 5); ++q)
-        t += sh[q];
-    __syncthreads();
-    return t;
+    // the last block b with b*C/G <= t
+    const long long b = ((t + 1) * G + C - 1) / C - 1;
+    return (int)(b < G - 1 ? b : G - 1);
+}
+__device__ __forceinline__ long long seg_bound(int b, long long C, int G) { return (long long)b * C / G; }
+
+// first slice s with slice_off[s] >= v (slice_off strictly increasing, slice_off[ns] = slots)
+__device__ __forceinline__ int slice_at(const int64_t *slice_off, int ns, long long v)
+{
+    int lo = 0, hi = ns;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(slice_off + mid) >= v)
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    return lo;
 }
 
-// What every block keeps of the launch: the CG scalars of each problem (indexed by problem) and
-// the rank tables of the active ones (rank r: problem act[r], virtual blocks [vs[r], vs[r]+g[r])).
-// All blocks apply the same decisions to the same totals, so the copies never differ.
+// What every block keeps of the launch: the CG scalars of each problem (indexed by problem), the
+// rank tables of the active ones (rank r: problem act[r], cost prefix cum[r], pieces in blocks
+// fb[r] .. fb[r] + g[r] - 1 whose partials sit at vs[r] ..) and this block's own pieces (ranks
+// pr_lo .. pr_lo + np - 1, slices [ps0[k], ps1[k])).  All blocks apply the same decisions to
+// the same totals, so the shared copies never differ.
 struct BShared
 {
     double rr[kMaxBatch], stop[kMaxBatch], alpha[kMaxBatch], beta[kMaxBatch], rrf[kMaxBatch];
-    long long it[kMaxBatch];
-    int status[kMaxBatch];
-    int act[kMaxBatch], g[kMaxBatch], vs[kMaxBatch], keep[kMaxBatch];
-    int nact, nvirt;
+    long long cit[kMaxBatch], itot[kMaxBatch], lastit[kMaxBatch];
+    long long cum[kMaxBatch + 1];
+    int status[kMaxBatch], mode[kMaxBatch], refs[kMaxBatch], caps[kMaxBatch];
+    int act[kMaxBatch], g[kMaxBatch], vs[kMaxBatch], fb[kMaxBatch], keep[kMaxBatch];
+    int ps0[kMaxBatch], ps1[kMaxBatch];
+    int nact, nvirt, np, pr_lo, left;
     int scan[32];
     long long sum[32];
 };
 
-__device__ __forceinline__ int find_rank(const BShared &S, int v)
+template <typename TV>
+union BUnion
 {
-    int lo = 0, hi = S.nact - 1;
-    while (lo < hi)
+    TV red[32 * 3 * 32];         // phase A's column-split buffer
+    double stage[3 * kMaxStage]; // the staged partials of a reduction (CG, ||r64||^2, ||(float) r64||^2)
+};
+
+constexpr size_t kBSharedBytes = ((sizeof(BShared) + 15) / 16) * 16;
+template <typename TV>
+constexpr size_t batch_smem_bytes()
+{
+    return kBSharedBytes + sizeof(BUnion<TV>);
+}
+
+// Recomputes the split over S.act[0 .. S.nact) and this block's pieces.  Whole block.
+__device__ void batch_split(const BArgs &a, BShared &S)
+{
+    const int t = threadIdx.x, nact = S.nact, G = gridDim.x, b = blockIdx.x;
+    const long long cost = (t < nact) ? a.inst[S.act[t]].cost : 0;
+    long long C = 0;
+    const long long before = block_exscan<long long>(cost, &C, S.sum);
+    if (t < nact)
+        S.cum[t] = before;
+    if (t == 0)
+        S.cum[nact] = C;
+    __syncthreads();
+    int g = 0, fb = 0;
+    bool mine = false;
+    if (t < nact)
     {
-        const int mid = (lo + hi + 1) >> 1;
-        if (S.vs[mid] <= v)
-            lo = mid;
-        else
-            hi = mid - 1;
+        fb = seg_block(S.cum[t], C, G);
+        const int lb = seg_block(S.cum[t + 1] - 1, C, G);
+        g = lb - fb + 1;
+        mine = fb <= b && b <= lb;
     }
-    return lo;
+    int V = 0;
+    const int vs = block_exscan<int>(g, &V, S.scan);
+    if (t < nact)
+    {
+        S.g[t] = g;
+        S.vs[t] = vs;
+        S.fb[t] = fb;
+    }
+    if (t == 0)
+    {
+        S.nvirt = V;
+        S.pr_lo = 0x7fffffff;
+    }
+    __syncthreads();
+    if (mine)
+        atomicMin(&S.pr_lo, t);
+    const int np = __syncthreads_count(mine);
+    if (t < np)
+    {
+        const int r = S.pr_lo + t;
+        const BInst &I = a.inst[S.act[r]];
+        const long long c0 = S.cum[r], c1 = S.cum[r + 1];
+        const long long lo = max(seg_bound(b, C, G), c0) - c0;
+        long long hi = min(seg_bound(b + 1, C, G), c1) - c0;
+        if (hi < lo)
+            hi = lo;
+        const long long e1 = (long long)I.dim * I.dim + 1;
+        S.ps0[t] = slice_at(I.slice_off, I.nslices, (lo + e1 - 1) / e1);
+        S.ps1[t] = slice_at(I.slice_off, I.nslices, (hi + e1 - 1) / e1);
+    }
+    if (t == 0)
+        S.np = np;
+    __syncthreads();
 }
 
 // Counting grid barrier: barrier number `epoch` is passed once the word reaches
@@ -201,32 +282,61 @@ __device__ bool batch_barrier(BCtl *ctl, unsigned &epoch, volatile int *s_fail)
     return *s_fail == 0;
 }
 
-// After a barrier, in every block: reduce each active problem's partials (buffer `buf`; a fixed
-// tree: 32-wide warp sums in order), decide per problem, and re-partition the virtual blocks
-// when problems left.  mode 0: initial ||r||^2; 1: p.Ap -> alpha (or breakdown); 2: ||r||^2 ->
-// beta, or converged / capped / paused at the end of the slice.
-__device__ void batch_reduce_decide(const BArgs &a, BShared &S, int mode, int64_t it, int buf, double *stage)
+// fixed-order sum of rank r's partials (32-wide warp sums in piece order); whole warp
+__device__ __forceinline__ double rank_total(const BShared &S, const double *stage, int r)
+{
+    const int lane = threadIdx.x & 31, g = S.g[r], vs = S.vs[r];
+    double tot = 0;
+    for (int c = 0; c < g; c += 32)
+    {
+        const double v = (c + lane < g) ? stage[vs + c + lane] : 0.0;
+        tot += wsum(v);
+    }
+    return tot;
+}
+
+// A finished inner solve of a refining problem hands over to x64 += x32 (the next phase).
+__device__ __forceinline__ void inner_done(BShared &S, int m, bool capped)
+{
+    S.lastit[m] = S.cit[m];
+    S.refs[m] += 1;
+    if (capped)
+        S.caps[m] += 1;
+    S.mode[m] = 1;
+}
+
+// After a barrier, in every block: reduce each active problem's partials, decide per problem,
+// and re-split when problems left.  kind 0: after the start (||r||^2 of fresh solves); 1: after
+// phase A (p.Ap -> alpha, or breakdown); 2: after phase B (||r||^2 -> beta, or converged /
+// capped / paused).  Refining problems step through their own modes at every decision.
+__device__ void batch_reduce_decide(const BArgs &a, BShared &S, int kind, int64_t it, double *stage)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const double *part = a.part + (size_t)buf * kMaxVirt;
-    // all partials into shared memory with one parallel load, then a warp per problem
+    const double *part = a.part + (size_t)(kind == 1 ? 1 : 0) * kMaxVirt;
+    const double *pr64 = a.part + (size_t)(kind == 1 ? 2 : 4) * kMaxVirt;
+    const double *pb32 = pr64 + kMaxVirt;
     for (int v = threadIdx.x; v < S.nvirt; v += blockDim.x)
+    {
         stage[v] = __ldcg(part + v);
+        if (kind != 0)
+        {
+            stage[kMaxStage + v] = __ldcg(pr64 + v);
+            stage[2 * kMaxStage + v] = __ldcg(pb32 + v);
+        }
+    }
     __syncthreads();
     for (int r = warp; r < S.nact; r += nw)
     {
-        const int m = S.act[r], g = S.g[r], vs = S.vs[r];
-        double tot = 0;
-        for (int c = 0; c < g; c += 32)
-        {
-            const double v = (c + lane < g) ? stage[vs + c + lane] : 0.0;
-            tot += wsum(v);
-        }
+        const int m = S.act[r];
+        const bool resid = kind != 0 && S.mode[m] == 2;
+        const double tot = rank_total(S, stage + (resid ? kMaxStage : 0), r);
+        const double tot2 = resid ? rank_total(S, stage + 2 * kMaxStage, r) : 0.0;
         if (lane == 0)
         {
             const BInst &I = a.inst[m];
             int keep = 1;
-            if (mode == 0)
+            const int md = S.mode[m];
+            if (kind == 0)
             {
                 if (I.fresh)
                 {
@@ -234,48 +344,84 @@ __device__ void batch_reduce_decide(const BArgs &a, BShared &S, int mode, int64_
                     S.rr[m] = tot;
                     S.stop[m] = stop;
                     S.beta[m] = 0.0;
-                    S.it[m] = 0;
+                    S.cit[m] = 0;
                     S.rrf[m] = tot;
-                    keep = !(tot <= stop);
+                    if (tot <= stop)
+                    {
+                        if (I.refine)
+                            inner_done(S, m, false);
+                        else
+                            keep = 0;
+                    }
                 }
             }
-            else if (mode == 1)
+            else if (md == 1)
+                S.mode[m] = 2; // x64 += x32 ran in this phase; the true residual is next
+            else if (md == 2)
+            {
+                // the true residual ran in this phase: tot = ||r64||^2, tot2 = ||(float) r64||^2
+                S.rrf[m] = tot;
+                if (tot <= I.stop64 || S.lastit[m] == 0 || S.refs[m] >= 30)
+                    keep = 0;
+                else
+                {
+                    S.rr[m] = tot2;
+                    S.stop[m] = I.abs_stop;
+                    S.beta[m] = 0.0;
+                    S.cit[m] = 0;
+                    S.mode[m] = (kind == 2) ? 0 : 3;
+                }
+            }
+            else if (md == 3)
+            {
+                if (kind == 2)
+                    S.mode[m] = 0;
+            }
+            else if (kind == 1)
             {
                 if (tot == 0.0)
                 {
-                    S.it[m] = I.it0 + it - 1;
                     S.status[m] |= 4;
                     S.rrf[m] = S.rr[m];
-                    keep = 0;
+                    if (I.refine)
+                        inner_done(S, m, false);
+                    else
+                        keep = 0;
                 }
                 else
                     S.alpha[m] = S.rr[m] / tot;
             }
             else
             {
-                const int64_t itg = I.it0 + it;
+                S.cit[m] += 1;
+                S.itot[m] += 1;
                 const bool done = tot <= S.stop[m];
-                const bool capped = itg >= I.maxit;
+                const bool capped = S.cit[m] >= I.maxit;
+                S.rrf[m] = tot;
                 if (done || capped)
                 {
-                    S.it[m] = itg;
-                    S.rrf[m] = tot;
-                    if (!done)
-                        S.status[m] |= 1;
-                    keep = 0;
+                    if (I.refine)
+                        inner_done(S, m, !done);
+                    else
+                    {
+                        if (!done)
+                            S.status[m] |= 1;
+                        keep = 0;
+                    }
                 }
                 else
                 {
                     S.beta[m] = tot / S.rr[m];
                     S.rr[m] = tot;
-                    if (it >= a.slice)
-                    {
-                        S.it[m] = itg;
-                        S.rrf[m] = tot;
-                        S.status[m] |= 8;
-                        keep = 0;
-                    }
                 }
+            }
+            // pause at the end of the launch's slice, or once enough problems left; only a solve
+            // in CG mode pauses (a refinement step finishes first)
+            if (keep && kind == 2 && S.mode[m] == 0 &&
+                (it >= a.slice || (a.pause_left > 0 && S.left >= a.pause_left)))
+            {
+                S.status[m] |= 8;
+                keep = 0;
             }
             S.keep[r] = keep;
         }
@@ -283,151 +429,223 @@ __device__ void batch_reduce_decide(const BArgs &a, BShared &S, int mode, int64_
     __syncthreads();
     const int t = threadIdx.x, nact = S.nact;
     const int keep = (t < nact) ? S.keep[t] : 1;
-    if (!__syncthreads_or(keep == 0))
+    const int gone = __syncthreads_count(keep == 0);
+    if (gone == 0)
         return;
     // compaction of the still-active ranks (order kept), then the new split
     const int mine = (t < nact) ? S.act[t] : -1;
     int nnew = 0;
-    const int pos = block_exscan((t < nact && keep) ? 1 : 0, &nnew, S.scan);
+    const int pos = block_exscan<int>((t < nact && keep) ? 1 : 0, &nnew, S.scan);
     if (t < nact && keep)
         S.keep[pos] = mine; // every thread has read its keep flag above
     __syncthreads();
-    const int m = (t < nnew) ? S.keep[t] : -1;
-    const int64_t cost = (m >= 0) ? a.inst[m].cost : 0;
-    const int64_t C = block_sum_i64(cost, S.sum);
-    const int g = (m >= 0) ? vblocks_for(gridDim.x, nnew, cost, C, a.inst[m].nslices) : 0;
-    int V = 0;
-    const int vs = block_exscan(g, &V, S.scan);
-    if (m >= 0)
-    {
-        S.act[t] = m;
-        S.g[t] = g;
-        S.vs[t] = vs;
-    }
+    if (t < nnew)
+        S.act[t] = S.keep[t];
     if (t == 0)
     {
         S.nact = nnew;
-        S.nvirt = V;
+        S.left += gone;
     }
     __syncthreads();
+    batch_split(a, S);
+}
+
+// Only the FP32 variant runs inner solves of a refinement (FP64 items never refine).
+template <typename TV>
+constexpr bool kRefines = sizeof(TV) == 4;
+
+// Refinement steps of a problem whose inner FP32 solve finished (the loop body of the mixed
+// solve in cg.cu: x64 += x32, then r64 = res - K64 x64 and the next inner solve's start).
+// x64 += x32 over the piece's unknowns
+template <typename TV>
+__device__ __forceinline__ void refine_add(const BInst &I, int s0, int s1)
+{
+    const int64_t lo = (int64_t)s0 * I.ndof / I.nslices, hi = (int64_t)s1 * I.ndof / I.nslices;
+    const TV *x32 = static_cast<const TV *>(I.x);
+    for (int64_t j = lo + threadIdx.x; j < hi; j += blockDim.x)
+        I.x64[j] = I.x64[j] + (double)x32[j];
+}
+
+// For the rows of slices [s0, s1): r64 = res - K64 x64, then the inner solve's fresh start
+// r32 = (float) r64, x32 = 0, p_old = 0.  Returns the thread's share of ||r64||^2 and, in *v2,
+// of ||(float) r64||^2 (the inner solve's initial ||r||^2).
+template <typename TV>
+__device__ __forceinline__ double refine_residual(const BInst &I, int s0, int s1, uint64_t pf, uint64_t pl, double *v2)
+{
+    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5, D = I.dim;
+    TV *x32 = static_cast<TV *>(I.x), *r32 = static_cast<TV *>(I.r), *pa = static_cast<TV *>(I.pa);
+    double loc = 0, loc2 = 0;
+    for (int sl = s0 + warp; sl < s1; sl += nw)
+    {
+        double acc[3];
+        const int i = (D == 2) ? spmv_slice<double, double, 2>(sl, I.n, I.rowptr, I.perm, I.slice_off, I.col_sell,
+                                                                I.K64, I.x64, I.x64, 0.0, acc, pf, pl)
+                               : spmv_slice<double, double, 3>(sl, I.n, I.rowptr, I.perm, I.slice_off, I.col_sell,
+                                                                I.K64, I.x64, I.x64, 0.0, acc, pf, pl);
+        if (i >= 0)
+            for (int c = 0; c < D; ++c)
+            {
+                const int64_t k = (int64_t)i * D + c;
+                const double v = I.res[k] - acc[c];
+                I.r64[k] = v;
+                loc += v * v;
+                const TV f = (TV)v;
+                st_keep(r32 + k, f, pl);
+                st_keep(x32 + k, TV(0), pl);
+                st_keep(pa + k, TV(0), pl);
+                loc2 += (double)f * (double)f;
+            }
+    }
+    *v2 = loc2;
+    return loc;
 }
 
 template <typename TK, typename TV>
 __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg_batch(BArgs a)
 {
-    __shared__ BShared S;
+    extern __shared__ __align__(16) unsigned char dsm[];
+    BShared &S = *reinterpret_cast<BShared *>(dsm);
+    BUnion<TV> &U = *reinterpret_cast<BUnion<TV> *>(dsm + kBSharedBytes);
     __shared__ double sh[32];
     __shared__ int s_fail;
-    // the column-split buffer of phase A and the staged partials of a reduction share storage
-    __shared__ union
-    {
-        TV red[32 * 3 * 32];
-        double stage[kMaxStage];
-    } U;
     TV *red = U.red;
     const int t = threadIdx.x;
     if (t == 0)
     {
         s_fail = 0;
-        S.nact = a.ctl->nact;
-    }
-    __syncthreads();
-    for (int r = t; r < S.nact; r += blockDim.x)
-    {
-        S.act[r] = a.act0[r];
-        S.g[r] = a.gcnt0[r];
-        S.vs[r] = a.vstart0[r];
+        S.nact = a.ninst;
+        S.left = 0;
     }
     for (int m = t; m < a.ninst; m += blockDim.x)
     {
         const BState &B = a.st[m];
+        S.act[m] = m;
         S.rr[m] = B.rr;
         S.stop[m] = B.stop;
         S.alpha[m] = B.alpha;
         S.beta[m] = B.beta;
         S.rrf[m] = B.rr_final;
-        S.it[m] = B.it;
+        S.cit[m] = B.it;
+        S.itot[m] = B.it_total;
+        S.lastit[m] = B.last_inner;
         S.status[m] = (int)B.status;
+        S.mode[m] = B.mode;
+        S.refs[m] = B.refs;
+        S.caps[m] = B.caps;
     }
     __syncthreads();
-    if (t == 0)
-        S.nvirt = S.nact > 0 ? S.vs[S.nact - 1] + S.g[S.nact - 1] : 0;
-    __syncthreads();
+    batch_split(a, S);
     unsigned epoch = 0;
     const uint64_t pf = l2_evict_first(), pl = l2_evict_last();
+    double *const part0 = a.part, *const part1 = a.part + kMaxVirt;
+    double *const partA = a.part + 2 * kMaxVirt, *const partB = a.part + 4 * kMaxVirt;
 
     // fresh solves: r = b, x = 0, p_old = 0; partial ||b||^2 (resumed solves keep their vectors)
-    for (int v = blockIdx.x; v < S.nvirt; v += gridDim.x)
+    for (int k = 0; k < S.np; ++k)
     {
-        const int r = find_rank(S, v), m = S.act[r], k = v - S.vs[r], g = S.g[r];
+        const int r = S.pr_lo + k, m = S.act[r], pidx = S.vs[r] + (int)blockIdx.x - S.fb[r];
         const BInst &I = a.inst[m];
-        const int64_t lo = I.fresh ? k * I.ndof / g : 0, hi = I.fresh ? (k + 1) * I.ndof / g : 0;
-        const TV *b = static_cast<const TV *>(I.b);
-        TV *x = static_cast<TV *>(I.x), *rv = static_cast<TV *>(I.r), *pa = static_cast<TV *>(I.pa);
         double loc = 0;
-        for (int64_t j = lo + t; j < hi; j += blockDim.x)
+        if (I.fresh)
         {
-            const TV bv = b[j];
-            st_keep(rv + j, bv, pl);
-            st_keep(x + j, TV(0), pl);
-            st_keep(pa + j, TV(0), pl);
-            loc += (double)bv * (double)bv;
+            const int64_t lo = (int64_t)S.ps0[k] * I.ndof / I.nslices, hi = (int64_t)S.ps1[k] * I.ndof / I.nslices;
+            const TV *b = static_cast<const TV *>(I.b);
+            TV *x = static_cast<TV *>(I.x), *rv = static_cast<TV *>(I.r), *pa = static_cast<TV *>(I.pa);
+            for (int64_t j = lo + t; j < hi; j += blockDim.x)
+            {
+                const TV bv = b[j];
+                st_keep(rv + j, bv, pl);
+                st_keep(x + j, TV(0), pl);
+                st_keep(pa + j, TV(0), pl);
+                loc += (double)bv * (double)bv;
+            }
         }
-        block_partial_at(loc, a.part + v, sh);
+        block_partial_at(loc, part0 + pidx, sh);
     }
     if (!batch_barrier(a.ctl, epoch, &s_fail))
         return;
-    batch_reduce_decide(a, S, 0, 0, 0, U.stage);
+    batch_reduce_decide(a, S, 0, 0, U.stage);
 
     for (int64_t it = 1; S.nact > 0; ++it)
     {
-        // phase A: q = K p_new (partials -> buffer 1)
-        for (int v = blockIdx.x; v < S.nvirt; v += gridDim.x)
+        // phase A: q = K p_new (partials -> buffer 1); refining problems take their next step
+        for (int k = 0; k < S.np; ++k)
         {
-            const int r = find_rank(S, v), m = S.act[r], k = v - S.vs[r], g = S.g[r];
+            const int r = S.pr_lo + k, m = S.act[r], pidx = S.vs[r] + (int)blockIdx.x - S.fb[r];
             const BInst &I = a.inst[m];
-            const bool odd = ((I.it0 + it) & 1) != 0; // the solve's own iteration number
-            const TV beta = (TV)S.beta[m];
-            const TV *pold = static_cast<const TV *>(odd ? I.pa : I.pb);
-            TV *pnew = static_cast<TV *>(odd ? I.pb : I.pa);
-            const int s0 = (int)((int64_t)k * I.nslices / g), s1 = (int)((int64_t)(k + 1) * I.nslices / g);
-            const TV *rv = static_cast<const TV *>(I.r);
-            TV *q = static_cast<TV *>(I.q);
-            const TK *K = static_cast<const TK *>(I.K);
-            const double lpq =
-                (I.dim == 2) ? spmv_block<TK, TV, 2>(s0, s1, I.n, I.rowptr, I.perm, I.slice_off, I.col_sell, K, rv, pold,
-                                                     pnew, q, beta, pf, pl, red)
-                             : spmv_block<TK, TV, 3>(s0, s1, I.n, I.rowptr, I.perm, I.slice_off, I.col_sell, K, rv, pold,
-                                                     pnew, q, beta, pf, pl, red);
-            block_partial_at(lpq, a.part + kMaxVirt + v, sh);
-        }
-        if (!batch_barrier(a.ctl, epoch, &s_fail))
-            return;
-        batch_reduce_decide(a, S, 1, it, 1, U.stage);
-        // phase B: x += alpha p_new, r -= alpha q (partials -> buffer 0)
-        for (int v = blockIdx.x; v < S.nvirt; v += gridDim.x)
-        {
-            const int r = find_rank(S, v), m = S.act[r], k = v - S.vs[r], g = S.g[r];
-            const BInst &I = a.inst[m];
-            const bool odd = ((I.it0 + it) & 1) != 0;
-            const TV al = (TV)S.alpha[m];
-            const TV *pnew = static_cast<const TV *>(odd ? I.pb : I.pa);
-            TV *x = static_cast<TV *>(I.x), *rv = static_cast<TV *>(I.r);
-            const TV *q = static_cast<const TV *>(I.q);
-            const int64_t lo = k * I.ndof / g, hi = (k + 1) * I.ndof / g;
-            double lrr = 0;
-            for (int64_t j = lo + t; j < hi; j += blockDim.x)
+            const int md = S.mode[m];
+            double val = 0;
+            if (md == 0)
             {
-                st_keep(x + j, ld_keep(x + j, pl) + al * ld_keep(pnew + j, pl), pl);
-                const TV rn = ld_keep(rv + j, pl) - al * ld_keep(q + j, pl);
-                st_keep(rv + j, rn, pl);
-                lrr += (double)rn * (double)rn;
+                const bool odd = ((S.cit[m] + 1) & 1) != 0; // the solve's own iteration number
+                const TV beta = (TV)S.beta[m];
+                const TV *pold = static_cast<const TV *>(odd ? I.pa : I.pb);
+                TV *pnew = static_cast<TV *>(odd ? I.pb : I.pa);
+                const TV *rv = static_cast<const TV *>(I.r);
+                TV *q = static_cast<TV *>(I.q);
+                const TK *K = static_cast<const TK *>(I.K);
+                val = (I.dim == 2) ? spmv_block<TK, TV, 2>(S.ps0[k], S.ps1[k], I.n, I.rowptr, I.perm, I.slice_off,
+                                                           I.col_sell, K, rv, pold, pnew, q, beta, pf, pl, red)
+                                   : spmv_block<TK, TV, 3>(S.ps0[k], S.ps1[k], I.n, I.rowptr, I.perm, I.slice_off,
+                                                           I.col_sell, K, rv, pold, pnew, q, beta, pf, pl, red);
             }
-            block_partial_at(lrr, a.part + v, sh);
+            else if constexpr (kRefines<TV>)
+            {
+                if (md == 1)
+                    refine_add<TV>(I, S.ps0[k], S.ps1[k]);
+                else if (md == 2)
+                {
+                    double v2 = 0;
+                    const double v1 = refine_residual<TV>(I, S.ps0[k], S.ps1[k], pf, pl, &v2);
+                    block_partial_at(v1, partA + pidx, sh);
+                    block_partial_at(v2, partA + kMaxVirt + pidx, sh);
+                }
+            }
+            block_partial_at(val, part1 + pidx, sh);
         }
         if (!batch_barrier(a.ctl, epoch, &s_fail))
             return;
-        batch_reduce_decide(a, S, 2, it, 0, U.stage);
+        batch_reduce_decide(a, S, 1, it, U.stage);
+        // phase B: x += alpha p_new, r -= alpha q (partials -> buffer 0)
+        for (int k = 0; k < S.np; ++k)
+        {
+            const int r = S.pr_lo + k, m = S.act[r], pidx = S.vs[r] + (int)blockIdx.x - S.fb[r];
+            const BInst &I = a.inst[m];
+            const int md = S.mode[m];
+            double lrr = 0;
+            if (md == 0)
+            {
+                const bool odd = ((S.cit[m] + 1) & 1) != 0;
+                const TV al = (TV)S.alpha[m];
+                const TV *pnew = static_cast<const TV *>(odd ? I.pb : I.pa);
+                TV *x = static_cast<TV *>(I.x), *rv = static_cast<TV *>(I.r);
+                const TV *q = static_cast<const TV *>(I.q);
+                const int64_t lo = (int64_t)S.ps0[k] * I.ndof / I.nslices, hi = (int64_t)S.ps1[k] * I.ndof / I.nslices;
+                for (int64_t j = lo + t; j < hi; j += blockDim.x)
+                {
+                    st_keep(x + j, ld_keep(x + j, pl) + al * ld_keep(pnew + j, pl), pl);
+                    const TV rn = ld_keep(rv + j, pl) - al * ld_keep(q + j, pl);
+                    st_keep(rv + j, rn, pl);
+                    lrr += (double)rn * (double)rn;
+                }
+            }
+            else if constexpr (kRefines<TV>)
+            {
+                if (md == 1)
+                    refine_add<TV>(I, S.ps0[k], S.ps1[k]);
+                else if (md == 2)
+                {
+                    double v2 = 0;
+                    const double v1 = refine_residual<TV>(I, S.ps0[k], S.ps1[k], pf, pl, &v2);
+                    block_partial_at(v1, partB + pidx, sh);
+                    block_partial_at(v2, partB + kMaxVirt + pidx, sh);
+                }
+            }
+            block_partial_at(lrr, part0 + pidx, sh);
+        }
+        if (!batch_barrier(a.ctl, epoch, &s_fail))
+            return;
+        batch_reduce_decide(a, S, 2, it, U.stage);
     }
     if (blockIdx.x == 0)
         for (int m = t; m < a.ninst; m += blockDim.x)
@@ -438,8 +656,13 @@ __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg_batch(BArgs a)
             B.alpha = S.alpha[m];
             B.beta = S.beta[m];
             B.rr_final = S.rrf[m];
-            B.it = S.it[m];
+            B.it = S.cit[m];
+            B.it_total = S.itot[m];
+            B.last_inner = S.lastit[m];
             B.status = S.status[m];
+            B.mode = S.mode[m];
+            B.refs = S.refs[m];
+            B.caps = S.caps[m];
         }
 }
 
@@ -452,19 +675,23 @@ struct BatchItem
     int64_t maxit;
     bool fresh;     // false: resume the paused solve whose state is `resume`
     BState resume;
+    bool refine;    // FP32 item: the FP64 refinement around it runs in the launch
+    double stop64;  // its outer squared-norm target
 };
 
 struct BatchCtx
 {
     int device = 0, num_sms = 0, grid = 0;
     int64_t slice = 512; // CG iterations per launch before unfinished solves pause
+    double pause_frac = 0.0; // > 0: pause the unfinished solves once this fraction of a launch's
+                             // problems finished (the others resume in the next launch)
+    size_t smem64 = 0, smem32 = 0; // dynamic shared memory of the two kernel variants
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_done = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
     std::vector<cudaEvent_t> ev_in; // one per item slot
     BInst *d_inst = nullptr, *h_inst = nullptr;
     BState *d_st = nullptr, *h_st = nullptr;
     BCtl *d_ctl = nullptr, *h_ctl = nullptr;
-    int *d_tab = nullptr, *h_tab = nullptr; // initial rank tables act|gcnt|vstart [3*kMaxBatch]
     double *d_part = nullptr;
     int64_t launches = 0;
     double kernel_seconds = 0;
@@ -478,12 +705,19 @@ struct BatchCtx
             return e;
         if ((e = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
             return e;
-        int occ64 = 0, occ32 = 0;
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ64, k_cg_batch<double, double>, kCGThreads, 0)) !=
-            cudaSuccess)
+        smem64 = batch_smem_bytes<double>();
+        smem32 = batch_smem_bytes<float>();
+        if ((e = cudaFuncSetAttribute(k_cg_batch<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem64)) != cudaSuccess ||
+            (e = cudaFuncSetAttribute(k_cg_batch<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem32)) != cudaSuccess)
             return e;
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ32, k_cg_batch<float, float>, kCGThreads, 0)) !=
-            cudaSuccess)
+        int occ64 = 0, occ32 = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ64, k_cg_batch<double, double>, kCGThreads,
+                                                                smem64)) != cudaSuccess)
+            return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ32, k_cg_batch<float, float>, kCGThreads,
+                                                                smem32)) != cudaSuccess)
             return e;
         grid = std::min(1024, num_sms * std::max(1, std::min({occ64, occ32, kCGMinBlocks})));
         if ((e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)) != cudaSuccess)
@@ -492,17 +726,14 @@ struct BatchCtx
             return e;
         if ((e = cudaEventCreate(&ev_t0)) != cudaSuccess || (e = cudaEventCreate(&ev_t1)) != cudaSuccess)
             return e;
-        const size_t ntab = 3 * (size_t)kMaxBatch;
         if ((e = cudaMalloc(&d_inst, sizeof(BInst) * kMaxBatch)) != cudaSuccess ||
             (e = cudaMalloc(&d_st, sizeof(BState) * kMaxBatch)) != cudaSuccess ||
             (e = cudaMalloc(&d_ctl, sizeof(BCtl))) != cudaSuccess ||
-            (e = cudaMalloc(&d_tab, sizeof(int) * ntab)) != cudaSuccess ||
-            (e = cudaMalloc(&d_part, sizeof(double) * 2 * kMaxVirt)) != cudaSuccess)
+            (e = cudaMalloc(&d_part, sizeof(double) * 6 * kMaxVirt)) != cudaSuccess)
             return e;
         if ((e = cudaMallocHost(&h_inst, sizeof(BInst) * kMaxBatch)) != cudaSuccess ||
             (e = cudaMallocHost(&h_st, sizeof(BState) * kMaxBatch)) != cudaSuccess ||
-            (e = cudaMallocHost(&h_ctl, sizeof(BCtl))) != cudaSuccess ||
-            (e = cudaMallocHost(&h_tab, sizeof(int) * ntab)) != cudaSuccess)
+            (e = cudaMallocHost(&h_ctl, sizeof(BCtl))) != cudaSuccess)
             return e;
         return cudaSuccess;
     }
@@ -524,18 +755,15 @@ struct BatchCtx
         cudaFree(d_inst);
         cudaFree(d_st);
         cudaFree(d_ctl);
-        cudaFree(d_tab);
         cudaFree(d_part);
         cudaFreeHost(h_inst);
         cudaFreeHost(h_st);
         cudaFreeHost(h_ctl);
-        cudaFreeHost(h_tab);
         ev_done = ev_t0 = ev_t1 = nullptr;
         stream = nullptr;
         d_inst = h_inst = nullptr;
         d_st = h_st = nullptr;
         d_ctl = h_ctl = nullptr;
-        d_tab = h_tab = nullptr;
         d_part = nullptr;
     }
 
@@ -558,7 +786,6 @@ struct BatchCtx
                 return e;
             ev_in.push_back(ev);
         }
-        int64_t C = 0;
         for (int m = 0; m < ni; ++m)
         {
             const Problem &p = *items[m].p;
@@ -566,11 +793,10 @@ struct BatchCtx
             std::memset(&I, 0, sizeof(I));
             I.dim = p.dim;
             I.fresh = items[m].fresh ? 1 : 0;
-            I.it0 = items[m].fresh ? 0 : items[m].resume.it;
             I.n = p.n;
             I.nslices = p.nslices;
             I.ndof = (int64_t)p.n * p.dim;
-            I.cost = p.nsb * p.dim * p.dim;
+            I.cost = p.nsb * (p.dim * p.dim + 1);
             I.rowptr = p.cstart;
             I.perm = p.perm;
             I.slice_off = p.slice_off;
@@ -599,18 +825,12 @@ struct BatchCtx
             I.atol = items[m].atol;
             I.abs_stop = items[m].abs_stop;
             I.maxit = items[m].maxit;
-            C += I.cost;
-        }
-        // initial split over all items (the same integer rule the kernel uses when problems leave)
-        int *act = h_tab, *gcnt = h_tab + kMaxBatch, *vstart = h_tab + 2 * kMaxBatch;
-        int V = 0;
-        for (int m = 0; m < ni; ++m)
-        {
-            const int g = vblocks_for(grid, ni, h_inst[m].cost, C, h_inst[m].nslices);
-            act[m] = m;
-            gcnt[m] = g;
-            vstart[m] = V;
-            V += g;
+            I.refine = (fp32 && items[m].refine) ? 1 : 0;
+            I.K64 = p.K;
+            I.res = p.res;
+            I.x64 = p.x;
+            I.r64 = p.r;
+            I.stop64 = items[m].stop64;
         }
         for (int m = 0; m < ni; ++m)
         {
@@ -633,27 +853,23 @@ struct BatchCtx
         }
         if ((e = cudaMemcpyAsync(d_inst, h_inst, sizeof(BInst) * ni, cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
             (e = cudaMemcpyAsync(d_st, h_st, sizeof(BState) * ni, cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(d_ctl, h_ctl, sizeof(BCtl), cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(d_tab, h_tab, sizeof(int) * 3 * kMaxBatch, cudaMemcpyHostToDevice, stream)) !=
-                cudaSuccess)
+            (e = cudaMemcpyAsync(d_ctl, h_ctl, sizeof(BCtl), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
             return e;
         BArgs a;
         a.inst = d_inst;
         a.st = d_st;
         a.ctl = d_ctl;
-        a.act0 = d_tab;
-        a.gcnt0 = d_tab + kMaxBatch;
-        a.vstart0 = d_tab + 2 * kMaxBatch;
         a.part = d_part;
         a.ninst = ni;
         a.slice = slice > 0 ? slice : (int64_t(1) << 62);
+        a.pause_left = (pause_frac > 0 && ni > 1) ? std::max(1, (int)std::ceil(pause_frac * ni)) : 0;
         void *args[] = {&a};
         if ((e = cudaEventRecord(ev_t0, stream)) != cudaSuccess)
             return e;
         e = fp32 ? cudaLaunchCooperativeKernel((const void *)k_cg_batch<float, float>, dim3(grid), dim3(kCGThreads),
-                                               args, 0, stream)
+                                               args, smem32, stream)
                  : cudaLaunchCooperativeKernel((const void *)k_cg_batch<double, double>, dim3(grid),
-                                               dim3(kCGThreads), args, 0, stream);
+                                               dim3(kCGThreads), args, smem64, stream);
         if (e != cudaSuccess)
             return e;
         if ((e = cudaEventRecord(ev_t1, stream)) != cudaSuccess)
@@ -729,10 +945,9 @@ enum class Ph
     NeedCG,      // a CG (FP64, or the FP32 inner solve of a refinement) to start or resume
     DamageCheck, // J2 state + static damage in flight
     Done,
-    Failed,
-    IRCheck      // mixed precision: x += x32 and the true residual in flight
+    Failed
 };
-constexpr int kPhases = 8;
+constexpr int kPhases = 7;
 
 struct Member
 {
@@ -756,8 +971,6 @@ struct Member
     bool ls_fresh = true;
     BState ls_state{};
     double ir_stop = 0, ir_rr = 0;
-    int ir_ref = 0;
-    int64_t ir_inner_iters = 0;
 };
 
 int32_t cuda_status(cudaError_t e, const char *what)
@@ -930,7 +1143,6 @@ struct lpmgpu_batch
             m.ph = Ph::NeedCG;
             return LPMGPU_OK;
         }
-        m.ir_ref = 0;
         m.ir_rr = p.scal_host->res_sq;
         m.ir_stop = p.desc.cg_rtol * m.ir_rr + p.desc.cg_atol;
         cudaError_t e = cudaMemsetAsync(p.x, 0, sizeof(double) * (size_t)p.n * p.dim, p.stream);
@@ -940,16 +1152,6 @@ struct lpmgpu_batch
             return finish_linear(m);
         if ((e = enqueue_res_to_b32(p)) != cudaSuccess)
             return fail_member(m, cuda_status(e, "batched refinement"));
-        m.ph = Ph::NeedCG;
-        return LPMGPU_OK;
-    }
-
-    int32_t next_inner(Member &m)
-    {
-        cudaError_t e = enqueue_r_to_b32(P(m));
-        if (e != cudaSuccess)
-            return fail_member(m, cuda_status(e, "batched refinement"));
-        m.ls_fresh = true;
         m.ph = Ph::NeedCG;
         return LPMGPU_OK;
     }
@@ -987,11 +1189,6 @@ struct lpmgpu_batch
         case Ph::Newton:
             m.nres = std::sqrt(p.scal_host->res_sq);
             return newton_check(m);
-        case Ph::IRCheck:
-            m.ir_rr = true_residual_result(p);
-            if (m.ir_inner_iters == 0 || m.ir_rr <= m.ir_stop || m.ir_ref >= 30)
-                return finish_linear(m);
-            return next_inner(m);
         case Ph::DamageCheck:
         {
             const bool new_damaged = p.scal_host->any_flag != 0;
@@ -1056,9 +1253,13 @@ struct lpmgpu_batch
         {
             Problem &p = P(*m);
             const int64_t ndof = (int64_t)p.n * p.dim;
-            BatchItem it{&p, fp32, fp32 ? 0.0 : p.desc.cg_rtol, fp32 ? 0.0 : p.desc.cg_atol,
-                         fp32 ? 0.25 * m->ir_stop : -1.0, p.desc.cg_maxit > 0 ? p.desc.cg_maxit : ndof, m->ls_fresh,
-                         m->ls_state};
+            BatchItem it{&p,           fp32,
+                         fp32 ? 0.0 : p.desc.cg_rtol,
+                         fp32 ? 0.0 : p.desc.cg_atol,
+                         fp32 ? 0.25 * m->ir_stop : -1.0,
+                         p.desc.cg_maxit > 0 ? p.desc.cg_maxit : ndof,
+                         m->ls_fresh,  m->ls_state,
+                         fp32,         m->ir_stop};
             items.push_back(it);
         }
         cudaError_t e = ctx.launch(items);
@@ -1074,8 +1275,8 @@ struct lpmgpu_batch
             Member &m = *ms[q];
             Problem &p = P(m);
             const BState &S = ctx.h_st[q];
-            const int64_t before = m.ls_fresh ? 0 : m.ls_state.it;
-            const int64_t done_now = S.it - before;
+            const int64_t before = m.ls_fresh ? 0 : m.ls_state.it_total;
+            const int64_t done_now = S.it_total - before;
             round_max_it = std::max(round_max_it, done_now);
             m.cur.cg_iters += done_now;
             m.dof_iters += done_now * (int64_t)p.n * p.dim;
@@ -1092,27 +1293,15 @@ struct lpmgpu_batch
                 m.ls_fresh = false; // paused: resumes in the next round
                 continue;
             }
-            if (S.status & 1)
+            if (fp32)
+            {
+                // the FP64 refinement ran to its end inside the launch (solve_dim's loop)
+                m.cur.refinements += S.refs;
+                m.cur.cg_maxit_hits += S.caps;
+            }
+            else if (S.status & 1)
                 m.cur.cg_maxit_hits++;
-            if (!fp32)
-            {
-                finish_linear(m);
-                continue;
-            }
-            // an inner solve finished: x += x32, new true residual (solve_dim's loop body)
-            m.ir_ref++;
-            m.cur.refinements++;
-            m.ir_inner_iters = S.it;
-            e = enqueue_add_x32(p);
-            if (e == cudaSuccess)
-                e = enqueue_true_residual(p);
-            if (e != cudaSuccess)
-            {
-                fail_member(m, cuda_status(e, "batched refinement"));
-                continue;
-            }
-            m.ph = Ph::IRCheck;
-            m.pending = true;
+            finish_linear(m);
         }
         return LPMGPU_OK;
     }
@@ -1173,11 +1362,11 @@ struct lpmgpu_batch
                     nph[(int)up->ph]++;
             std::fprintf(stderr,
                          "lpmgpu batch round %lld: cg64=%zu cgmix=%zu launches=%lld max_it=%lld kernel_ms=%.3f "
-                         "round_ms=%.3f phases(start,nf,n,cg,dmg,done,fail,irc)=%d,%d,%d,%d,%d,%d,%d,%d\n",
+                         "round_ms=%.3f phases(start,nf,n,cg,dmg,done,fail)=%d,%d,%d,%d,%d,%d,%d\n",
                          (long long)stats.rounds, cg64.size(), cgmix.size(), (long long)(stats.cg_launches - l0),
                          (long long)maxit, (ctx.kernel_seconds - k0) * 1e3,
                          std::chrono::duration<double>(std::chrono::steady_clock::now() - t_round).count() * 1e3,
-                         nph[0], nph[1], nph[2], nph[3], nph[4], nph[5], nph[6], nph[7]);
+                         nph[0], nph[1], nph[2], nph[3], nph[4], nph[5], nph[6]);
         }
         return LPMGPU_OK;
     }
