@@ -500,8 +500,28 @@ __device__ __forceinline__ double refine_residual(const BInst &I, int s0, int s1
     return loc;
 }
 
+// Phase A of one piece: q = K p_new for its slices.  The FP32 variant (80 registers) keeps three
+// steps of 2 x 2 blocks in flight per warp.
+template <typename TK, typename TV, int D>
+__device__ __forceinline__ double batch_spmv(const BInst *Ip, int s0, int s1, TV beta, bool odd, TV *red)
+{
+    const BInst &I = *Ip;
+    const TV *pold = static_cast<const TV *>(odd ? I.pa : I.pb);
+    TV *pnew = static_cast<TV *>(odd ? I.pb : I.pa);
+    return spmv_block<TK, TV, D, (sizeof(TV) == 4 ? 3 : 1)>(s0, s1, I.n, I.rowptr, I.perm, I.slice_off, I.col_sell,
+                                                             static_cast<const TK *>(I.K),
+                                 static_cast<const TV *>(I.r), pold, pnew, static_cast<TV *>(I.q), beta,
+                                 l2_evict_first(), l2_evict_last(), red);
+}
+
+// Threads per block: the FP32 variant runs 24 warps with up to 80 registers each, so its SpMV can
+// keep several steps' loads in flight (2 x 2 FP32 blocks move only 16 bytes per lane and step);
+// the FP64 variant keeps 32 warps at 64 registers, as the single-problem kernel does.
+template <typename TV>
+constexpr int kBatchThreads = sizeof(TV) == 4 ? 768 : kCGThreads;
+
 template <typename TK, typename TV>
-__global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg_batch(BArgs a)
+__global__ void __launch_bounds__(kBatchThreads<TV>, kCGMinBlocks) k_cg_batch(BArgs a)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
     BShared &S = *reinterpret_cast<BShared *>(dsm);
@@ -578,16 +598,8 @@ __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg_batch(BArgs a)
             if (md == 0)
             {
                 const bool odd = ((S.cit[m] + 1) & 1) != 0; // the solve's own iteration number
-                const TV beta = (TV)S.beta[m];
-                const TV *pold = static_cast<const TV *>(odd ? I.pa : I.pb);
-                TV *pnew = static_cast<TV *>(odd ? I.pb : I.pa);
-                const TV *rv = static_cast<const TV *>(I.r);
-                TV *q = static_cast<TV *>(I.q);
-                const TK *K = static_cast<const TK *>(I.K);
-                val = (I.dim == 2) ? spmv_block<TK, TV, 2>(S.ps0[k], S.ps1[k], I.n, I.rowptr, I.perm, I.slice_off,
-                                                           I.col_sell, K, rv, pold, pnew, q, beta, pf, pl, red)
-                                   : spmv_block<TK, TV, 3>(S.ps0[k], S.ps1[k], I.n, I.rowptr, I.perm, I.slice_off,
-                                                           I.col_sell, K, rv, pold, pnew, q, beta, pf, pl, red);
+                val = (I.dim == 2) ? batch_spmv<TK, TV, 2>(&I, S.ps0[k], S.ps1[k], (TV)S.beta[m], odd, red)
+                                   : batch_spmv<TK, TV, 3>(&I, S.ps0[k], S.ps1[k], (TV)S.beta[m], odd, red);
             }
             else if constexpr (kRefines<TV>)
             {
@@ -713,10 +725,10 @@ struct BatchCtx
                                       (int)smem32)) != cudaSuccess)
             return e;
         int occ64 = 0, occ32 = 0;
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ64, k_cg_batch<double, double>, kCGThreads,
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ64, k_cg_batch<double, double>, kBatchThreads<double>,
                                                                 smem64)) != cudaSuccess)
             return e;
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ32, k_cg_batch<float, float>, kCGThreads,
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ32, k_cg_batch<float, float>, kBatchThreads<float>,
                                                                 smem32)) != cudaSuccess)
             return e;
         grid = std::min(1024, num_sms * std::max(1, std::min({occ64, occ32, kCGMinBlocks})));
@@ -866,10 +878,10 @@ struct BatchCtx
         void *args[] = {&a};
         if ((e = cudaEventRecord(ev_t0, stream)) != cudaSuccess)
             return e;
-        e = fp32 ? cudaLaunchCooperativeKernel((const void *)k_cg_batch<float, float>, dim3(grid), dim3(kCGThreads),
+        e = fp32 ? cudaLaunchCooperativeKernel((const void *)k_cg_batch<float, float>, dim3(grid), dim3(kBatchThreads<float>),
                                                args, smem32, stream)
                  : cudaLaunchCooperativeKernel((const void *)k_cg_batch<double, double>, dim3(grid),
-                                               dim3(kCGThreads), args, smem64, stream);
+                                               dim3(kBatchThreads<double>), args, smem64, stream);
         if (e != cudaSuccess)
             return e;
         if ((e = cudaEventRecord(ev_t1, stream)) != cudaSuccess)

@@ -124,7 +124,8 @@ __device__ __forceinline__ void st_keep(float *a, float v, uint64_t pol)
 
 // q_i = sum_j K_ij (r_j + beta p_old_j) for the row at this lane of slice sl; returns the
 // particle id (-1 past the end).  Blocks in ascending connection order, entries row-major.
-template <typename TK, typename TV, int D>
+// U > 1 (callers with registers to spare): U steps of 2 x 2 FP32 blocks in flight at once.
+template <typename TK, typename TV, int D, int U = 1>
 __device__ __forceinline__ int spmv_slice(int sl, int n, const int *__restrict__ rowptr, const int *__restrict__ perm,
                                           const int64_t *__restrict__ slice_off, const int *__restrict__ col_sell,
                                           const TK *__restrict__ K, const TV *__restrict__ r,
@@ -145,6 +146,68 @@ __device__ __forceinline__ int spmv_slice(int sl, int n, const int *__restrict__
 #pragma unroll
     for (int k = 0; k < D; ++k)
         acc[k] = TV(0);
+    if constexpr (U > 1 && sizeof(TK) * E <= 16)
+    {
+        // Small blocks (2 x 2 FP32: 16 bytes per lane and step): one step moves too little for a
+        // warp's chain of column load -> gather to keep HBM busy, so U steps are in flight at
+        // once: their columns are fetched one group ahead, then all their gathers and matrix
+        // loads are issued before any of them is used.  The sums keep the ascending order.
+        int jn[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const int kk = k0 + u * kstep;
+            jn[u] = (kk < myn) ? ld_stream(cp + (int64_t)kk * kSlice, pf) : 0;
+        }
+        for (int k = k0; k < w; k += U * kstep)
+        {
+            int j[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+            {
+                j[u] = jn[u];
+                const int kk = k + (U + u) * kstep;
+                jn[u] = (kk < myn) ? ld_stream(cp + (int64_t)kk * kSlice, pf) : 0;
+            }
+            TV rv[U][D], pv[U][D];
+            TK kv[U][E];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+            {
+                const int kk = k + u * kstep;
+                if (kk < myn)
+                {
+#pragma unroll
+                    for (int c = 0; c < D; ++c)
+                    {
+                        rv[u][c] = ld_keep(r + (int64_t)j[u] * D + c, pl);
+                        pv[u][c] = ld_keep(pold + (int64_t)j[u] * D + c, pl);
+                    }
+                    const TK *kb = kp + (int64_t)kk * E * kSlice;
+#pragma unroll
+                    for (int e = 0; e < E; ++e)
+                        kv[u][e] = ld_stream(kb + e * kSlice, pf);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+            {
+                if (k + u * kstep < myn)
+                {
+                    TV xv[D];
+#pragma unroll
+                    for (int c = 0; c < D; ++c)
+                        xv[c] = rv[u][c] + beta * pv[u][c];
+#pragma unroll
+                    for (int rr = 0; rr < D; ++rr)
+#pragma unroll
+                        for (int c = 0; c < D; ++c)
+                            acc[rr] += (TV)kv[u][rr * D + c] * xv[c];
+                }
+            }
+        }
+        return i;
+    }
     // the column of the next step is fetched during this one, so the x gathers never wait on it
     int jn = (myn > k0) ? ld_stream(cp + (int64_t)k0 * kSlice, pf) : 0;
 #pragma unroll 2
@@ -185,7 +248,7 @@ constexpr int kMaxColumnSplit = 16;
 // dependent column/gather loads a warp walks is S times shorter; the S partial row sums are
 // added in a fixed order through `red` (shared memory, 32 * D * 32 values).  Every thread of
 // the block must call it.
-template <typename TK, typename TV, int D>
+template <typename TK, typename TV, int D, int U = 1>
 __device__ __forceinline__ double spmv_block(int s0, int s1, int n, const int *__restrict__ rowptr,
                                              const int *__restrict__ perm, const int64_t *__restrict__ slice_off,
                                              const int *__restrict__ col_sell, const TK *__restrict__ K,
@@ -216,7 +279,8 @@ __device__ __forceinline__ double spmv_block(int s0, int s1, int n, const int *_
         for (int sl = s0 + warp; sl < s1; sl += nw)
         {
             TV acc[D];
-            const int i = spmv_slice<TK, TV, D>(sl, n, rowptr, perm, slice_off, col_sell, K, r, pold, beta, acc, pf, pl);
+            const int i = spmv_slice<TK, TV, D, U>(sl, n, rowptr, perm, slice_off, col_sell, K, r, pold, beta, acc, pf,
+                                                   pl);
             epilogue(i, acc);
         }
         return lpq;
@@ -231,7 +295,8 @@ __device__ __forceinline__ double spmv_block(int s0, int s1, int n, const int *_
         acc[c] = TV(0);
     int i = -1;
     if (ls < ns)
-        i = spmv_slice<TK, TV, D>(s0 + ls, n, rowptr, perm, slice_off, col_sell, K, r, pold, beta, acc, pf, pl, part, S);
+        i = spmv_slice<TK, TV, D, U>(s0 + ls, n, rowptr, perm, slice_off, col_sell, K, r, pold, beta, acc, pf, pl,
+                                     part, S);
     if (ls < ns && part > 0)
 #pragma unroll
         for (int c = 0; c < D; ++c)
