@@ -190,6 +190,28 @@ int32_t lpmgpu_set_xyz(lpmgpu_solver *h, const double *xyz);
  * [2] linear solves, [3] other */
 int32_t lpmgpu_get_phase_times(const lpmgpu_solver *h, double *t4);
 
+/* ---- Per-step output: Assembly::writeDump (include/assembly.h:310-335), the LAMMPS text dump
+ * that SolverStatic::solveProblem appends after every load step (solver_static.h:89).
+ * lpmgpu_format_dump appends one step for host arrays: xyz, xyz_initial n*3; stress n*6 (s11 s22
+ * s33 s23 s13 s12); damage, damage_visual n; state_var n*nsv (column 0 is written); type n or NULL
+ * (all 0); box the Assembly's 6 bounds.  The file is opened "a+" as the reference opens it and
+ * the bytes are those of the reference's printf conversions for the same values.  Rows are
+ * formatted by `threads` host threads (<= 0: all cores) in contiguous chunks, written in order.
+ * Needs no device. */
+int32_t lpmgpu_format_dump(const char *path, int32_t step, int32_t n, const int32_t *type, const double box[6],
+                           const double *xyz, const double *xyz_initial, const double *stress, const double *damage,
+                           const double *damage_visual, const double *state_var, int32_t nsv, int32_t threads);
+/* The same for the handle's current state, with the coordinates and types given at lpmgpu_create
+ * as xyz_initial and type.  The fields are copied to pinned host buffers on the handle's stream
+ * after its pending work.  async = 1: the call returns at once and a writer thread of the handle
+ * formats and appends the step while the caller goes on (steps are written in call order; at
+ * most two are in flight, and a third call waits for one); errors of such steps are returned by
+ * lpmgpu_dump_flush.  async = 0: returns once the step is written.  lpmgpu_destroy flushes. */
+int32_t lpmgpu_dump_write(lpmgpu_solver *h, const char *path, int32_t step, const double box[6], int32_t threads,
+                          int32_t async);
+/* waits until every step queued by lpmgpu_dump_write is written; returns the first error among them */
+int32_t lpmgpu_dump_flush(lpmgpu_solver *h);
+
 /* Cumulative counters of the handle since creation. */
 typedef struct
 {

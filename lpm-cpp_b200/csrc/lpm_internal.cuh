@@ -110,6 +110,11 @@ struct Problem
     cudaEvent_t cg_ev[2] = {nullptr, nullptr};
     int64_t device_bytes = 0;
     std::vector<void *> allocs;
+    // host copies of the coordinates and types given at creation (Particle::xyz_initial, type)
+    // and the per-step dump writer (dump.cu), created by the first lpmgpu_dump_write
+    std::vector<double> xyz0_host;
+    std::vector<int> type_host;
+    void *dump = nullptr;
 };
 
 constexpr int kMaxGridBlocks = 4096;
@@ -158,6 +163,8 @@ cudaError_t enqueue_reset_state(Problem &p);
 
 // error text for lpmgpu_last_error
 void set_last_error(const std::string &s);
+// flushes and frees the handle's dump writer (waits for the steps it still writes)
+void release_dump_writer(Problem &p);
 
 template <typename T>
 cudaError_t dalloc(Problem &p, T **ptr, size_t count)

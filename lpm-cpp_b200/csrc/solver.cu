@@ -492,6 +492,11 @@ int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
     Problem &p = h->p;
     p.desc = *d;
     p.device = d->device;
+    p.xyz0_host.assign(d->xyz, d->xyz + 3 * (size_t)d->n);
+    if (d->type)
+        p.type_host.assign(d->type, d->type + d->n);
+    else
+        p.type_host.assign(d->n, 0);
     for (auto &e : p.ev)
         e = nullptr;
     auto fail = [&](int32_t code) {
@@ -599,6 +604,7 @@ int32_t lpmgpu_destroy(lpmgpu_solver *h)
         return LPMGPU_ERR_INVALID_ARG;
     cudaSetDevice(h->p.device);
     cudaStreamSynchronize(h->p.stream);
+    release_dump_writer(h->p);
     free_problem(h->p);
     delete h;
     return LPMGPU_OK;

@@ -175,6 +175,7 @@ EXPORTS = [
     "lpmgpu_solve_problem_step", "lpmgpu_solve_load_step", "lpmgpu_store_state", "lpmgpu_reset_state",
     "lpmgpu_read_state", "lpmgpu_read_residual", "lpmgpu_set_xyz", "lpmgpu_get_phase_times",
     "lpmgpu_get_counters", "lpmgpu_get_stream", "lpmgpu_cg_bsr_noalloc",
+    "lpmgpu_format_dump", "lpmgpu_dump_write", "lpmgpu_dump_flush",
     "lpmgpu_batch_create", "lpmgpu_batch_destroy", "lpmgpu_batch_add", "lpmgpu_batch_round", "lpmgpu_batch_run",
     "lpmgpu_batch_member", "lpmgpu_batch_member_steps", "lpmgpu_batch_remove", "lpmgpu_batch_get_stats",
     "lpmgpu_batch_set_slice",
@@ -218,6 +219,10 @@ def lib():
         "lpmgpu_get_phase_times": (C.c_int32, [vp, dp]),
         "lpmgpu_get_counters": (C.c_int32, [vp, C.POINTER(Counters)]),
         "lpmgpu_get_stream": (C.c_int32, [vp, C.POINTER(vp)]),
+        "lpmgpu_format_dump": (C.c_int32, [C.c_char_p, C.c_int32, C.c_int32, ip, dp, dp, dp, dp, dp, dp, dp,
+                                           C.c_int32, C.c_int32]),
+        "lpmgpu_dump_write": (C.c_int32, [vp, C.c_char_p, C.c_int32, dp, C.c_int32, C.c_int32]),
+        "lpmgpu_dump_flush": (C.c_int32, [vp]),
         "lpmgpu_cg_bsr_noalloc": (C.c_int32, [C.c_int32, C.c_int32, vp, vp, vp, vp, vp, C.c_double, C.c_double,
                                               C.c_int64, vp, C.POINTER(C.c_int64)]),
         "lpmgpu_batch_create": (C.c_int32, [C.c_int32, C.POINTER(vp)]),
@@ -639,6 +644,17 @@ class GpuProblem:
         _check(lib().lpmgpu_get_counters(self._h, C.byref(c)), "lpmgpu_get_counters")
         return c.as_dict()
 
+    def dump_write(self, path: str, step: int, box, threads: int = 0, async_: bool = True):
+        """lpmgpu_dump_write: appends the current state as one step of the reference's dump text
+        (Assembly::writeDump, include/assembly.h:310-335); async_ overlaps the formatting with the
+        caller's next device work (lpmgpu_dump_flush waits for it)."""
+        b = np.ascontiguousarray(box, dtype=np.float64)
+        _check(lib().lpmgpu_dump_write(self._h, os.fsencode(path), int(step), _dp(b), int(threads), int(bool(async_))),
+               "lpmgpu_dump_write")
+
+    def dump_flush(self):
+        _check(lib().lpmgpu_dump_flush(self._h), "lpmgpu_dump_flush")
+
     def stream_ptr(self) -> int:
         s = C.c_void_p()
         _check(lib().lpmgpu_get_stream(self._h, C.byref(s)), "lpmgpu_get_stream")
@@ -652,6 +668,20 @@ class GpuProblem:
         t = np.zeros(4)
         _check(lib().lpmgpu_get_phase_times(self._h, _dp(t)), "lpmgpu_get_phase_times")
         return {"force_s": t[0], "assembly_s": t[1], "linear_s": t[2], "other_s": t[3]}
+
+
+def format_dump(path: str, step: int, box, xyz, xyz_initial, stress, damage, damage_visual, state_var,
+                type=None, threads: int = 0):
+    """lpmgpu_format_dump: one step of the reference's dump text (Assembly::writeDump,
+    include/assembly.h:310-335) for host arrays, appended to path.  Needs no device."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    n = len(xyz)
+    sv = np.ascontiguousarray(state_var, dtype=np.float64).reshape(n, -1)
+    t = None if type is None else np.ascontiguousarray(type, dtype=np.int32)
+    arr = [np.ascontiguousarray(a, dtype=np.float64) for a in (box, xyz_initial, stress, damage, damage_visual)]
+    _check(lib().lpmgpu_format_dump(os.fsencode(path), int(step), n, _ip(t), _dp(arr[0]), _dp(xyz), _dp(arr[1]),
+                                    _dp(arr[2]), _dp(arr[3]), _dp(arr[4]), _dp(sv), sv.shape[1], int(threads)),
+           "lpmgpu_format_dump")
 
 
 class Batch:
@@ -840,21 +870,10 @@ class SolverStatic:
                 raise LpmGpuError(ERR_CUTS, f"load step {i + start_index}")
             if self.dumpFile:
                 self.writeDump(self.dumpFile, i + start_index)
+        self.problem.dump_flush()
         return start_index + len(load)
 
     def writeDump(self, path: str, step: int):
-        """Assembly::writeDump (include/assembly.h:310-335) text format."""
-        s = self.problem.state()
-        a = self.ass
-        with open(path, "a+") as f:
-            f.write("ITEM: TIMESTEP\n%d\nITEM: NUMBER OF ATOMS\n%d\nITEM: BOX BOUNDS pp pp pp\n" % (step, a.nparticle))
-            for k in range(3):
-                f.write("%8.8f %8.8f\n" % (a.box[2 * k], a.box[2 * k + 1]))
-            f.write("ITEM: ATOMS id type x y z dx dy dz s11 s22 s33 s23 s13 s12 damage damage_visual "
-                    "state_var[0] \n")
-            x, st, dmg, dv, sv = s["xyz"], s["stress"], s["damage"], s["damage_visual"], s["state_var"]
-            for i in range(a.nparticle):
-                u = x[i] - a.xyz[i]
-                f.write("%d %d %.4e %.4e %.4e %.4e %.4e %.4e %.4e %.4e %.4e %.4e %.4e %.4e %.4e %.4e %.4e\n" % (
-                    i, a.type[i], x[i, 0], x[i, 1], x[i, 2], u[0], u[1], u[2], st[i, 0], st[i, 1], st[i, 2],
-                    st[i, 3], st[i, 4], st[i, 5], dmg[i], dv[i], sv[i, 0]))
+        """Assembly::writeDump (include/assembly.h:310-335): the native writer, queued behind the
+        step's device work (solveProblem flushes before it returns)."""
+        self.problem.dump_write(path, step, self.ass.box, async_=True)

@@ -39,6 +39,8 @@
  *                          stiffness re-assembled from the current state before every linear
  *                          solve of Solver::NewtonIteration, and not at the start of a damage
  *                          iteration; "loop step|once" only)
+ *   dumpfile PATH         (the SolverStatic dumpFile: with "loop ref" the reference's own
+ *                          Assembly::writeDump appends every load step there; default /dev/null)
  *   bondprops PATH        (raw f64: Kn[nb], Tv[nb], bdamage[nb] in bond order, written into
  *                          Bond::Kn / Tv / bdamage and bdamage_last (include/bond.h:25-27) after
  *                          setParticleProperty: a heterogeneous material or initial damage)
@@ -128,6 +130,7 @@ struct Spec
     std::string typefile;
     std::string bondfile;
     std::string bondprops;
+    std::string dumpfile = "/dev/null";
     int tangent = 0;
     double cg_rtol = -1, cg_atol = -1;
 };
@@ -244,6 +247,7 @@ static Spec parse(const char *path)
         else if (k == "cg_tol") is >> s.cg_rtol >> s.cg_atol;
         else if (k == "bondfile") is >> s.bondfile;
         else if (k == "bondprops") is >> s.bondprops;
+        else if (k == "dumpfile") is >> s.dumpfile;
         else if (k == "tangent") is >> s.tangent;
         else
         {
@@ -512,7 +516,7 @@ int main(int argc, char **argv)
     if (sp.init_state_var)
         ass.updateStateVar();
 
-    LPM_SOLVER<NL> solv{sp.undamaged_type, ass, StiffnessMode::Analytical, SolverMode::CG, "/dev/null",
+    LPM_SOLVER<NL> solv{sp.undamaged_type, ass, StiffnessMode::Analytical, SolverMode::CG, sp.dumpfile,
                         sp.max_iter, sp.tol_iter};
 #ifdef LPM_USE_GPU
     if (sp.cg_rtol >= 0 || sp.cg_atol >= 0)
