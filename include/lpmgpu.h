@@ -42,7 +42,7 @@ typedef enum
 /* LatticeType (include/lpm.h:97-106); BCC3D covers the three BCC enum values */
 enum { LPMGPU_SQUARE2D = 0, LPMGPU_HEXAGON2D = 1, LPMGPU_SC3D = 2, LPMGPU_FCC3D = 3, LPMGPU_BCC3D = 4 };
 /* ParticleType (include/lpm.h:89-95) values on this path */
-enum { LPMGPU_ELASTIC = 0, LPMGPU_J2 = 2 };
+enum { LPMGPU_ELASTIC = 0, LPMGPU_ELASTIC_DAMAGE = 1, LPMGPU_J2 = 2 };
 /* linear-solve precision */
 enum { LPMGPU_FP64 = 0, LPMGPU_MIXED = 1 };
 
@@ -52,7 +52,7 @@ typedef struct lpmgpu_solver lpmgpu_solver;
 typedef struct
 {
     int32_t lattice;         /* LPMGPU_SQUARE2D .. LPMGPU_BCC3D */
-    int32_t ptype;           /* LPMGPU_ELASTIC or LPMGPU_J2 */
+    int32_t ptype;           /* LPMGPU_ELASTIC, LPMGPU_ELASTIC_DAMAGE or LPMGPU_J2 */
     int32_t n;               /* particles */
     const double *xyz;       /* host, n*3; row q is particle id q (generation order) */
     const int32_t *type;     /* host, n particle types, or NULL for all 0 */
@@ -61,7 +61,7 @@ typedef struct
     double E, mu;            /* Young's modulus, Poisson's ratio */
     double critical_bstrain; /* elastic bond breaking strain (particle_elastic.h:60) */
     double sigmay, xi, H, A; /* J2 parameters (particle_j2plasticity.h:155-163) */
-    double nonlocal_L;       /* nonlocal length (no nonlocal search is run: solver_static.h:37-52) */
+    double nonlocal_L;       /* Particle::nonlocal_L, the length of the nonlocal damage weight */
     int32_t undamaged_type;  /* SolverStatic undamaged_pt_type */
     int32_t max_iter;        /* Newton iteration cap (max_NR_iter) */
     double tol_iter;         /* Newton tolerance (tol_NR_iter) */
@@ -83,6 +83,15 @@ typedef struct
      * SolverStatic; its Newton loop and assembly calls are those of solver.h:55-90 and
      * stiffness.h, re-ordered. */
     int32_t tangent;
+    /* > 0: Assembly::searchNonlocalNeighbors(nonlocal_cutoff_ratio) (assembly.h:118-130) runs on the
+     * device at creation, and SolverStatic::updateStaticDamage (solver_static.h:32-62) averages the
+     * local damage rates over those neighbours.  0: no search; the nonlocal rate is then 0/0 as in
+     * the reference without the search. */
+    double nonlocal_cutoff_ratio;
+    /* LPMGPU_ELASTIC_DAMAGE (ParticleElasticDamage::setParticleProperty,
+     * particle_elastic_damage.h:183-220): damage surface k0 + k1 D on the strain energy density,
+     * the compression/tension ratio of its equivalent strain, and the damage threshold */
+    double k0, k1, comp_tensile_ratio, damage_threshold;
 } lpmgpu_desc;
 
 /* Displacement / force boundary condition of one load step (boundary.h:10-44, Relative mode). */

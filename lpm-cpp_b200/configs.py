@@ -41,6 +41,8 @@ class Case:
     # per-bond (Kn, Tv, bdamage) in bond order, written into the bonds before the first force
     # update (a heterogeneous material, initial damage); None -> setParticleProperty's values
     bond_props: Optional[Tuple[np.ndarray, np.ndarray, np.ndarray]] = None
+    # > 0: Assembly::searchNonlocalNeighbors(cutoff_ratio) before solving (nonlocal damage)
+    nonlocal_cutoff_ratio: float = 0.0
 
     @property
     def n(self):
@@ -66,6 +68,8 @@ class Case:
         a.bonds = self.bonds
         if self.bond_props is not None:
             a.bond_kn, a.bond_tv, a.bond_damage = self.bond_props
+        if self.nonlocal_cutoff_ratio > 0:
+            a.searchNonlocalNeighbors(self.nonlocal_cutoff_ratio)
         return a
 
 
@@ -219,6 +223,25 @@ def notched_plate(size=4.0, radius=0.1, crack=0.3, E=69e3, mu=0.3, critical_bstr
     c.bonds = bond_lists(xyz, L.UnitCell(L.LatticeType.Hexagon2D, radius),
                          slit_exclusion(xyz, y_slit, box[0] - 1.0, box[0] + crack * size))
     c.meta["crack"] = (crack * size, y_slit)
+    return c
+
+
+def edamage_plate(size=2.4, radius=0.1, E=69e3, mu=0.3, steps=4, total_disp=0.008, k0=0.02, k1=0.5,
+                  damage_threshold=0.9, nonlocal_L=0.3, cutoff_ratio=1.5, tol_iter=1e-9, max_iter=30) -> Case:
+    """Hexagonal plate of ParticleElasticDamage particles (include/particle_elastic_damage.h) with
+    the nonlocal damage of SolverStatic::updateStaticDamage (solver_static.h:32-62): the bottom edge
+    fixed, the top edge pulled in y (the groups of ex1_isoelasticity_2d_hex).  Damage grows once
+    the strain energy density passes k0 + k1 D; the local rates are averaged over the neighbours
+    within cutoff_ratio x nonlocal_L (Assembly::searchNonlocalNeighbors, assembly.h:118-130)."""
+    c = hex_plate(size=size, radius=radius, E=E, mu=mu, steps=steps, total_disp=total_disp, tol_iter=tol_iter,
+                  max_iter=max_iter)
+    c.name = f"edamage_hex_{size:g}mm"
+    c.ptype = L.ParticleType.ElasticDamage
+    c.material.k0, c.material.k1, c.material.damage_threshold = k0, k1, damage_threshold
+    c.material.nonlocal_L = nonlocal_L
+    c.nonlocal_cutoff_ratio = cutoff_ratio
+    c.meta.update({"k0": k0, "k1": k1, "damage_threshold": damage_threshold, "nonlocal_L": nonlocal_L,
+                   "cutoff_ratio": cutoff_ratio})
     return c
 
 

@@ -82,6 +82,11 @@ struct Problem
     double *dis0 = nullptr, *dis = nullptr, *dis_last = nullptr, *dLe = nullptr, *dLp = nullptr,
            *dLp_last = nullptr, *bstrain = nullptr, *Kn = nullptr, *Tv = nullptr, *cs = nullptr,
            *bforce = nullptr, *bforce_last = nullptr, *bdamage = nullptr, *bdamage_last = nullptr;
+    // nonlocal neighbours (Assembly::searchNonlocalNeighbors; CSR in ascending id) and the
+    // nonlocal damage rate; null when no search ran
+    int *nlstart = nullptr, *nlist = nullptr;
+    int64_t nnl = 0;
+    double *ddot_nonlocal = nullptr;
     // connections and matrices
     int *cstart = nullptr, *conns = nullptr, *nlq = nullptr;
     int64_t *kp_ref = nullptr;        // reference K_pointer (n+1)
@@ -128,6 +133,11 @@ cudaError_t launch_k_to_f32(Problem &p);        // FP32 copy of K for the mixed-
 cudaError_t launch_assemble(Problem &p, bool apply_bc);
 cudaError_t launch_update_state_var(Problem &p);
 cudaError_t launch_static_damage(Problem &p);   // sets p.scal->any_flag
+// nonlocal damage (damage.cu): the neighbour search at creation, the averaged damage rate,
+// and ParticleElasticDamage's state update
+cudaError_t build_nonlocal(Problem &p, double cutoff_ratio);
+cudaError_t launch_nonlocal_average(Problem &p);
+cudaError_t launch_edamage_update(Problem &p);
 cudaError_t launch_add_disp(Problem &p);        // xyz += x (solveLinearSystem position update)
 cudaError_t launch_export_ref(const Problem &p, int64_t *IK, int64_t *JK, double *K); // device outputs
 cudaError_t launch_apply_bc(Problem &p, const lpmgpu_load_step &s);

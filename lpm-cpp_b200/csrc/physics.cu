@@ -78,7 +78,7 @@ __global__ void k_geometry_force(PhysArgs a)
         const int L = b < b1 ? 0 : 1;
         double f = 2. * a.Kn[b] * a.dLe[b] + 2. * a.Tv[b] * dlt[L];
         double D = a.bdamage[b];
-        if (a.ptype == LPMGPU_J2)
+        if (a.ptype == LPMGPU_J2 || a.ptype == LPMGPU_ELASTIC_DAMAGE)
         {
             D = std_max(D, std_max(di, a.damage[a.bp2[b]]));
             a.bdamage[b] = D;
@@ -322,6 +322,8 @@ __global__ void k_j2_update(int n, double E, double mu, double sigmay, double xi
 
 cudaError_t launch_update_state_var(Problem &p)
 {
+    if (p.desc.ptype == LPMGPU_ELASTIC_DAMAGE)
+        return launch_edamage_update(p);
     if (p.desc.ptype != LPMGPU_J2)
         return cudaSuccess;
     k_j2_update<<<div_up(p.n, 128), 128, 0, p.stream>>>(p.n, p.desc.E, p.desc.mu, p.desc.sigmay, p.desc.xi, p.desc.H,
@@ -331,11 +333,14 @@ cudaError_t launch_update_state_var(Problem &p)
     return cudaGetLastError();
 }
 
-// SolverStatic::updateStaticDamage.  No nonlocal neighbour search is run on this path, so the
-// nonlocal rate is 0/0 (solver_static.h:39-51) exactly as in the reference when
-// searchNonlocalNeighbors was not called; elastic particles ignore it, J2 particles add it.
-__global__ void k_static_damage(int n, int ptype, int undamaged, double critical, const int *__restrict__ type,
-                                const int *__restrict__ bstart, const double *__restrict__ bstrain,
+// SolverStatic::updateStaticDamage.  The nonlocal rate comes from k_nonlocal_average when a
+// nonlocal search ran; without one it is 0/0 (solver_static.h:39-51), exactly as in the reference
+// when searchNonlocalNeighbors was not called.  Elastic particles ignore it; J2 and elastic-damage
+// particles add it to their damage and set the damage to 1 at their threshold
+// (particle_j2plasticity.h:142-152, particle_elastic_damage.h:172-181).
+__global__ void k_static_damage(int n, int ptype, int undamaged, double critical, double threshold,
+                                const int *__restrict__ type, const int *__restrict__ bstart,
+                                const double *__restrict__ bstrain, const double *__restrict__ ddot_nl,
                                 double *__restrict__ bdamage, double *__restrict__ damage,
                                 const double *__restrict__ damage_last, Scalars *scal)
 {
@@ -343,12 +348,12 @@ __global__ void k_static_damage(int n, int ptype, int undamaged, double critical
     if (i >= n || type[i] == undamaged)
         return;
     bool changed = false;
-    if (ptype == LPMGPU_J2)
+    if (ptype == LPMGPU_J2 || ptype == LPMGPU_ELASTIC_DAMAGE)
     {
         volatile double zero = 0.0;
-        const double ddot_nonlocal = zero / zero;
+        const double ddot_nonlocal = ddot_nl ? ddot_nl[i] : zero / zero;
         double d = damage[i] + ddot_nonlocal;
-        if (d >= 0.0) // damage_threshold is never assigned (particle_j2plasticity.h:22,148)
+        if (d >= threshold)
             d = 1;
         damage[i] = d;
         changed = fabs(d - damage_last[i]) > 1e-3;
@@ -371,9 +376,14 @@ cudaError_t launch_static_damage(Problem &p)
     cudaError_t e = cudaMemsetAsync(&p.scal->any_flag, 0, sizeof(int), p.stream);
     if (e != cudaSuccess)
         return e;
+    if (p.desc.ptype != LPMGPU_ELASTIC && (e = launch_nonlocal_average(p)) != cudaSuccess)
+        return e;
+    // damage_threshold is never assigned for J2 (particle_j2plasticity.h:22): 0
+    const double threshold = (p.desc.ptype == LPMGPU_ELASTIC_DAMAGE) ? p.desc.damage_threshold : 0.0;
     k_static_damage<<<div_up(p.n, 128), 128, 0, p.stream>>>(p.n, p.desc.ptype, p.desc.undamaged_type,
-                                                            p.desc.critical_bstrain, p.type, p.bstart, p.bstrain,
-                                                            p.bdamage, p.damage, p.damage_last, p.scal);
+                                                            p.desc.critical_bstrain, threshold, p.type, p.bstart,
+                                                            p.bstrain, p.ddot_nonlocal, p.bdamage, p.damage,
+                                                            p.damage_last, p.scal);
     p.ctr.kernel_launches++;
     return cudaGetLastError();
 }

@@ -479,7 +479,8 @@ static void free_problem(Problem &p)
 int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
 {
     if (!d || !out || !d->xyz || d->n <= 0 || d->lattice < 0 || d->lattice > LPMGPU_BCC3D ||
-        (d->ptype != LPMGPU_ELASTIC && d->ptype != LPMGPU_J2) || !(d->radius > 0) || d->max_iter < 0)
+        (d->ptype != LPMGPU_ELASTIC && d->ptype != LPMGPU_ELASTIC_DAMAGE && d->ptype != LPMGPU_J2) ||
+        !(d->radius > 0) || d->max_iter < 0 || d->nonlocal_cutoff_ratio < 0)
         return LPMGPU_ERR_INVALID_ARG;
     *out = nullptr;
     int ndev = 0;
@@ -559,6 +560,8 @@ int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
     }
     int topo_err = 0;
     CKF(build_topology(p, d->xyz, &topo_err));
+    if (d->nonlocal_cutoff_ratio > 0)
+        CKF(build_nonlocal(p, d->nonlocal_cutoff_ratio));
     CKF(cudaStreamSynchronize(p.stream));
     // the host pointers of the description are only read during creation
     p.desc.xyz = nullptr;

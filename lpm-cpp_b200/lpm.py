@@ -33,6 +33,7 @@ class LatticeType(enum.IntEnum):
 
 class ParticleType(enum.IntEnum):
     Elastic = 0
+    ElasticDamage = 1
     J2Plasticity = 2
 
 
@@ -87,6 +88,8 @@ class Desc(C.Structure):
         ("bond_nb0", C.POINTER(C.c_int32)), ("bond_nb1", C.POINTER(C.c_int32)), ("bond_p2", C.POINTER(C.c_int32)),
         ("bond_kn", C.POINTER(C.c_double)), ("bond_tv", C.POINTER(C.c_double)),
         ("bond_damage", C.POINTER(C.c_double)), ("tangent", C.c_int32),
+        ("nonlocal_cutoff_ratio", C.c_double), ("k0", C.c_double), ("k1", C.c_double),
+        ("comp_tensile_ratio", C.c_double), ("damage_threshold", C.c_double),
     ]
 
 
@@ -330,7 +333,8 @@ def createCuboidBCC3D(box, cell, R=None):
 # ---------------------------------------------------------------------------- assembly and loads
 @dataclass
 class Material:
-    """Arguments of setParticleProperty (particle_elastic.h:70, particle_j2plasticity.h:155)."""
+    """Arguments of setParticleProperty (particle_elastic.h:70, particle_j2plasticity.h:155,
+    particle_elastic_damage.h:183)."""
     plane_stress: bool = False
     E: float = 69e3
     mu: float = 0.3
@@ -340,6 +344,12 @@ class Material:
     H: float = 0.0
     A: float = 0.0
     nonlocal_L: float = 0.0
+    # ParticleElasticDamage: damage surface k0 + k1 D on the strain energy density, the
+    # compression/tension ratio and the damage threshold
+    k0: float = 0.0
+    k1: float = 1.0
+    comp_tensile_ratio: float = 10.0
+    damage_threshold: float = 1.0
 
 
 def _read_dump(path: str):
@@ -374,6 +384,13 @@ class Assembly:
         # coefficients and initial bond damage, all in (particle, layer-0 then layer-1) order
         self.bonds = None          # (nb0[n], nb1[n], p2[nbonds])
         self.bond_kn = self.bond_tv = self.bond_damage = None
+        self.nonlocal_cutoff_ratio = 0.0  # > 0 once searchNonlocalNeighbors ran
+
+    def searchNonlocalNeighbors(self, cutoff_ratio: float):
+        """Assembly::searchNonlocalNeighbors (include/assembly.h:118-130): every particle within
+        cutoff_ratio x nonlocal_L of a particle is its nonlocal neighbour.  The search runs on the
+        device when the solver is constructed."""
+        self.nonlocal_cutoff_ratio = float(cutoff_ratio)
 
     @classmethod
     def fromDump(cls, dumpFile: str, cell: UnitCell, ptype: ParticleType = ParticleType.Elastic,
@@ -510,6 +527,8 @@ def _pack_desc(ass: Assembly, undamaged_pt_type=-1, max_iter=30, tol_iter=1e-5, 
     d.cg_rtol, d.cg_atol, d.cg_maxit = float(cg_rtol), float(cg_atol), int(cg_maxit)
     d.precision, d.device = int(precision), int(device)
     d.tangent = int(bool(tangent))
+    d.nonlocal_cutoff_ratio = float(getattr(ass, "nonlocal_cutoff_ratio", 0.0))
+    d.k0, d.k1, d.comp_tensile_ratio, d.damage_threshold = m.k0, m.k1, m.comp_tensile_ratio, m.damage_threshold
     if ass.bonds is not None:
         nb0, nb1, p2 = (np.ascontiguousarray(a, dtype=np.int32) for a in ass.bonds)
         keep += [nb0, nb1, p2]

@@ -40,6 +40,7 @@ struct lpmo_problem
     int *nlstart, *nlist;
     /* material */
     double E, mu, critical_bstrain, sigmay, xi, H, A, damage_threshold, nonlocal_L;
+    double k0, k1; /* ParticleElasticDamage damage surface (particle_elastic_damage.h:27) */
     int undamaged_type, max_iter, tangent;
     double tol, cg_rtol, cg_atol;
     long long cg_maxit;
@@ -674,7 +675,11 @@ lpmo_problem *lpmo_create(const lpmo_desc *d)
     p->xi = d->xi;
     p->H = d->H;
     p->A = d->A;
-    p->damage_threshold = 0; /* never assigned in the reference (particle_j2plasticity.h:22) */
+    /* never assigned for J2 in the reference (particle_j2plasticity.h:22); ParticleElasticDamage
+     * takes it from setParticleProperty (particle_elastic_damage.h:186) */
+    p->damage_threshold = (d->ptype == LPMO_ELASTIC_DAMAGE) ? d->damage_threshold : 0;
+    p->k0 = d->k0;
+    p->k1 = d->k1;
     p->nonlocal_L = d->nonlocal_L;
     double E = d->E, mu = d->mu, Ce[3], KnTv[3];
     if (!d->plane_stress)
@@ -815,13 +820,15 @@ void lpmo_update_force_state(lpmo_problem *p)
 {
     const int n = p->n;
     /* ParticleElastic::updateBondsForce (particle_elastic.h:38-50);
-     * ParticleJ2Plasticity::updateBondsForce (particle_j2plasticity.h:63-76) */
+     * ParticleJ2Plasticity::updateBondsForce (particle_j2plasticity.h:63-76) and
+     * ParticleElasticDamage::updateBondsForce (particle_elastic_damage.h:80-91): bond damage is
+     * the largest of its own and its two particles' */
     for (int i = 0; i < n; ++i)
         for (int b = B0(p, i); b < BE(p, i); ++b)
         {
             int L = p->blayer[b];
             double f = 2. * p->Kn[b] * p->dLe[b] + 2. * p->Tv[b] * p->dLe_total[2 * i + L];
-            if (p->ptype == LPMO_J2)
+            if (p->ptype == LPMO_J2 || p->ptype == LPMO_ELASTIC_DAMAGE)
                 p->bdamage[b] = std_max(p->bdamage[b], std_max(p->damage[i], p->damage[p->bp2[b]]));
             f *= (1.0 - p->bdamage[b]);
             p->bforce[b] = f;
@@ -867,6 +874,29 @@ void lpmo_update_force_state(lpmo_problem *p)
  * Particle::updateParticleStateVariables is a no-op for elastic particles (particle.h:62) */
 void lpmo_update_state_var(lpmo_problem *p)
 {
+    if (p->ptype == LPMO_ELASTIC_DAMAGE)
+    {
+        /* ParticleElasticDamage::updateParticleStateVariables (particle_elastic_damage.h:159-170)
+         * with calcStrainEnergyDensity (:93-108): state_var[0] = strain energy density, the
+         * local damage rate from its increase past the damage surface */
+        for (int i = 0; i < p->n; ++i)
+        {
+            const double V_m = p->pvol * p->nb[i] / p->nneighbors;
+            double energy = 0;
+            for (int L = 0; L < 2; ++L)
+            {
+                const int lo = L == 0 ? B0(p, i) : B0(p, i) + p->nb0[i], hi = L == 0 ? B0(p, i) + p->nb0[i] : BE(p, i);
+                for (int b = lo; b < hi; ++b)
+                    energy += 0.5 * (p->Kn[b] * p->dLe[b] * p->dLe[b]) / V_m;
+                energy += 0.5 * p->TdLe_total[2 * i + L] * p->dLe_total[2 * i + L] / V_m;
+            }
+            p->sv[i] = energy;
+            const double delta = p->sv[i] - p->sv_last[i];
+            const double f = p->sv[i] - p->k1 * p->damage[i] - p->k0;
+            p->ddot_local[i] = (f > 0 && delta > 0) ? (1 / p->k1) * delta : 0;
+        }
+        return;
+    }
     if (p->ptype != LPMO_J2)
         return;
     for (int i = 0; i < p->n; ++i)
@@ -1492,9 +1522,10 @@ static int update_static_damage(lpmo_problem *p)
         if (p->type[i] == p->undamaged_type)
             continue;
         int changed = 0;
-        if (p->ptype == LPMO_J2)
+        if (p->ptype == LPMO_J2 || p->ptype == LPMO_ELASTIC_DAMAGE)
         {
-            /* ParticleJ2Plasticity::updateParticleStaticDamage (particle_j2plasticity.h:142-152) */
+            /* ParticleJ2Plasticity::updateParticleStaticDamage (particle_j2plasticity.h:142-152),
+             * ParticleElasticDamage::updateParticleStaticDamage (particle_elastic_damage.h:172-181) */
             p->damage[i] += p->ddot_nonlocal[i];
             if (p->damage[i] >= p->damage_threshold)
                 p->damage[i] = 1;

@@ -13,8 +13,8 @@ extern "C" {
 
 /* LatticeType order of include/lpm.h:97-106 */
 enum { LPMO_SQUARE2D = 0, LPMO_HEXAGON2D = 1, LPMO_SC3D = 2, LPMO_FCC3D = 3, LPMO_BCC3D = 4 };
-/* ParticleType order of include/lpm.h:89-95 (ElasticDamage / FatigueHCF are not on the path) */
-enum { LPMO_ELASTIC = 0, LPMO_J2 = 2 };
+/* ParticleType order of include/lpm.h:89-95 (FatigueHCF is not on the path) */
+enum { LPMO_ELASTIC = 0, LPMO_ELASTIC_DAMAGE = 1, LPMO_J2 = 2 };
 
 typedef struct
 {
@@ -42,6 +42,8 @@ typedef struct
      * solve (no assembly at the start of a damage iteration); 0: K fixed per load step as in
      * SolverStatic::solveProblemStep (solver_static.h:107-118) */
     int tangent;
+    /* ParticleElasticDamage only (setParticleProperty, particle_elastic_damage.h:183-220) */
+    double k0, k1, comp_tensile_ratio, damage_threshold;
 } lpmo_desc;
 
 typedef struct

@@ -21,7 +21,7 @@ REF_BIN = os.path.join(HERE, "_ref", "lpm_ref")
 REF_GPU_BIN = os.path.join(HERE, "_ref", "lpm_ref_gpu")
 
 LATTICES = {"sq2d": 0, "hex2d": 1, "sc3d": 2, "fcc3d": 3, "bcc3d": 4}
-PTYPES = {"elastic": 0, "j2": 2}
+PTYPES = {"elastic": 0, "elastic_damage": 1, "j2": 2}
 
 
 class _Desc(C.Structure):
@@ -36,6 +36,7 @@ class _Desc(C.Structure):
         ("cg_rtol", C.c_double), ("cg_atol", C.c_double), ("cg_maxit", C.c_longlong),
         ("bond_nb0", C.POINTER(C.c_int)), ("bond_nb1", C.POINTER(C.c_int)), ("bond_p2", C.POINTER(C.c_int)),
         ("tangent", C.c_int),
+        ("k0", C.c_double), ("k1", C.c_double), ("comp_tensile_ratio", C.c_double), ("damage_threshold", C.c_double),
     ]
 
 
@@ -148,6 +149,11 @@ class Material:
     H: float = 0.0
     A: float = 0.0
     nonlocal_L: float = 0.0
+    # ParticleElasticDamage (particle_elastic_damage.h:183-220)
+    k0: float = 0.0
+    k1: float = 1.0
+    comp_tensile_ratio: float = 10.0
+    damage_threshold: float = 1.0
 
 
 class _StepHolder:
@@ -191,6 +197,7 @@ class OracleProblem:
         d.undamaged_type, d.max_iter, d.tol_iter = undamaged_type, max_iter, tol_iter
         d.cg_rtol, d.cg_atol, d.cg_maxit = cg_rtol, cg_atol, cg_maxit
         d.tangent = int(bool(tangent))
+        d.k0, d.k1, d.comp_tensile_ratio, d.damage_threshold = mat.k0, mat.k1, mat.comp_tensile_ratio, mat.damage_threshold
         if bonds is not None:
             self._bonds = [np.ascontiguousarray(a, dtype=np.int32) for a in bonds]
             d.bond_nb0, d.bond_nb1, d.bond_p2 = (_ip(a) for a in self._bonds)
@@ -354,7 +361,11 @@ def write_ref_spec(case, outdir: str, steps=None, max_iter=None, tol_iter=None, 
     m = case.material
     lines = [f"lattice {lat}", f"radius {case.radius!r}", "box " + " ".join(repr(float(v)) for v in case.box),
              f"euler {case.euler[0]} " + " ".join(repr(float(a)) for a in case.euler[1]),
-             f"ptype {'j2' if int(case.ptype) == 2 else 'elastic'}", f"plane_stress {int(m.plane_stress)}",
+             f"ptype {({2: 'j2', 1: 'elastic_damage'}).get(int(case.ptype), 'elastic')}",
+             f"plane_stress {int(m.plane_stress)}",
+             f"edamage {getattr(m, 'k0', 0.0)!r} {getattr(m, 'k1', 1.0)!r} {getattr(m, 'comp_tensile_ratio', 10.0)!r} "
+             f"{getattr(m, 'damage_threshold', 1.0)!r}",
+             f"nonlocal_cutoff_ratio {float(getattr(case, 'nonlocal_cutoff_ratio', 0.0))!r}",
              f"E {m.E!r}", f"mu {m.mu!r}", f"critical_bstrain {m.critical_bstrain!r}",
              f"j2 {m.sigmay!r} {m.xi!r} {m.H!r} {m.A!r}", f"nonlocal_L {m.nonlocal_L!r}",
              f"undamaged_type {case.undamaged_type}",

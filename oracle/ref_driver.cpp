@@ -17,7 +17,9 @@
  *
  * Spec format: one directive per line, '#' starts a comment.
  *   lattice hex2d|sq2d|sc3d|fcc3d      radius R       box x0 x1 y0 y1 z0 z1
- *   euler FLAG A1 A2 A3 (radians)      ptype elastic|j2
+ *   euler FLAG A1 A2 A3 (radians)      ptype elastic|j2|elastic_damage
+ *   edamage K0 K1 CT_RATIO D_THRES    (ParticleElasticDamage::setParticleProperty,
+ *                                       include/particle_elastic_damage.h:183-220)
  *   plane_stress 0|1  E v  mu v  critical_bstrain v  j2 sigmay xi H A
  *   nonlocal_L v  nonlocal_cutoff_ratio v  undamaged_type t  init_state_var 0|1
  *   max_iter n  tol_iter v  cg_maxit_cap n
@@ -108,6 +110,7 @@ struct Spec
     int euler_flag = 0;
     double angles[3] = {0, 0, 0};
     std::string ptype = "elastic";
+    double k0 = 0, k1 = 1, ct_ratio = 10, d_thres = 1;
     int plane_stress = 0;
     double E = 69e3, mu = 0.3, critical_bstrain = 1.0;
     double sigmay = 200, xi = 0, H = 0, A = 0;
@@ -175,6 +178,7 @@ static Spec parse(const char *path)
         else if (k == "box") for (int i = 0; i < 6; ++i) is >> s.box[i];
         else if (k == "euler") is >> s.euler_flag >> s.angles[0] >> s.angles[1] >> s.angles[2];
         else if (k == "ptype") is >> s.ptype;
+        else if (k == "edamage") is >> s.k0 >> s.k1 >> s.ct_ratio >> s.d_thres;
         else if (k == "plane_stress") is >> s.plane_stress;
         else if (k == "E") is >> s.E;
         else if (k == "mu") is >> s.mu;
@@ -416,7 +420,9 @@ int main(int argc, char **argv)
         return 2;
     }
 
-    ParticleType pt = (sp.ptype == "j2") ? ParticleType::J2Plasticity : ParticleType::Elastic;
+    ParticleType pt = (sp.ptype == "j2")               ? ParticleType::J2Plasticity
+                      : (sp.ptype == "elastic_damage") ? ParticleType::ElasticDamage
+                                                       : ParticleType::Elastic;
     Assembly<NL> ass = make_assembly(xyz, box, cell, pt, sp);
     const int N = ass.nparticle;
     const int dim = cell.dim;
@@ -457,6 +463,9 @@ int main(int argc, char **argv)
         if (pt == ParticleType::J2Plasticity)
             dynamic_cast<ParticleJ2Plasticity<NL> *>(p)->setParticleProperty(
                 sp.nonlocal_L, sp.plane_stress != 0, sp.E, sp.mu, sp.sigmay, sp.xi, sp.H, sp.A, sp.critical_bstrain);
+        else if (pt == ParticleType::ElasticDamage)
+            dynamic_cast<ParticleElasticDamage<NL> *>(p)->setParticleProperty(
+                sp.nonlocal_L, sp.plane_stress != 0, sp.E, sp.mu, sp.k0, sp.k1, sp.ct_ratio, sp.d_thres);
         else
             dynamic_cast<ParticleElastic<NL> *>(p)->setParticleProperty(sp.nonlocal_L, sp.plane_stress != 0, sp.E,
                                                                         sp.mu, sp.critical_bstrain);

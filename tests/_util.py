@@ -19,14 +19,17 @@ LAT_NAME = {0: "sq2d", 1: "hex2d", 2: "sc3d", 3: "fcc3d", 4: "bcc3d"}
 
 def oracle_problem(case, cg_rtol=1e-12, cg_atol=1e-12, tol_iter=None, max_iter=None, tangent=False):
     m = case.material
-    mat = O.Material(ptype="j2" if int(case.ptype) == 2 else "elastic", plane_stress=m.plane_stress, E=m.E, mu=m.mu,
+    mat = O.Material(ptype={2: "j2", 1: "elastic_damage"}.get(int(case.ptype), "elastic"),
+                     plane_stress=m.plane_stress, E=m.E, mu=m.mu,
                      critical_bstrain=m.critical_bstrain, sigmay=m.sigmay, xi=m.xi, H=m.H, A=m.A,
-                     nonlocal_L=m.nonlocal_L)
+                     nonlocal_L=m.nonlocal_L, k0=m.k0, k1=m.k1, comp_tensile_ratio=m.comp_tensile_ratio,
+                     damage_threshold=m.damage_threshold)
     o = O.OracleProblem(LAT_NAME[int(case.lattice)], case.radius, case.xyz, mat, types=case.types,
                         undamaged_type=case.undamaged_type,
                         max_iter=case.max_iter if max_iter is None else max_iter,
                         tol_iter=case.tol_iter if tol_iter is None else tol_iter, cg_rtol=cg_rtol, cg_atol=cg_atol,
-                        bonds=getattr(case, "bonds", None), tangent=tangent)
+                        bonds=getattr(case, "bonds", None), tangent=tangent,
+                        nonlocal_cutoff_ratio=getattr(case, "nonlocal_cutoff_ratio", 0.0))
     if getattr(case, "bond_props", None) is not None:
         kn, tv, dmg = case.bond_props
         o.set_bond_kntv(kn, tv)

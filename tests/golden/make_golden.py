@@ -82,6 +82,9 @@ def cases():
                            {"cg_tol": (1e-24, 0.0), "tangent": True, "dump_k": (2,)}),
         "hex_crack_tangent": (lambda: CFG.notched_plate(size=2.0, radius=0.1, crack=0.3, steps=6, total_disp=0.006,
                                                         tol_iter=1e-9), {"cg_tol": (1e-24, 0.0), "tangent": True}),
+        # ParticleElasticDamage with the nonlocal damage rate (searchNonlocalNeighbors + the
+        # averaging of SolverStatic::updateStaticDamage): damage grows in every step
+        "hex_edamage": (lambda: CFG.edamage_plate(), {"cg_tol": (1e-24, 0.0), "dump_k": (1,)}),
     }
 
 
@@ -111,6 +114,10 @@ def make(name, build, opts):
             out[f"pin_{s}"] = rb(f"pin_{tag}.f64", np.float64).reshape(-1, 3)
             if int(case.ptype) == 2:
                 out[f"state_var_{s}"] = rb(f"state_var_{tag}.f64", np.float64).reshape(-1, 7)
+            if int(case.ptype) == 1:
+                out[f"state_var_{s}"] = rb(f"state_var_{tag}.f64", np.float64).reshape(-1, 1)
+                out[f"damage_{s}"] = rb(f"damage_{tag}.f64", np.float64)
+                out[f"bdamage_{s}"] = rb(f"bdamage_{tag}.f64", np.float64)
             if case.material.critical_bstrain < 1.0 or case.bond_props is not None:
                 out[f"bdamage_{s}"] = rb(f"bdamage_{tag}.f64", np.float64)
         out["meta"] = np.array(json.dumps({"name": name,
