@@ -99,7 +99,6 @@ struct BArgs
     // slot of each piece, may change between two phases).
     double *part;
     int ninst;
-    int pause_left;  // pause the unfinished solves once this many problems left the launch (0: never)
     int64_t slice;   // iterations per launch; unfinished solves pause and resume later
 };
 
@@ -179,7 +178,7 @@ struct BShared
     int status[kMaxBatch], mode[kMaxBatch], refs[kMaxBatch], caps[kMaxBatch];
     int act[kMaxBatch], g[kMaxBatch], vs[kMaxBatch], fb[kMaxBatch], keep[kMaxBatch];
     int ps0[kMaxBatch], ps1[kMaxBatch];
-    int nact, nvirt, np, pr_lo, left;
+    int nact, nvirt, np, pr_lo;
     int scan[32];
     long long sum[32];
 };
@@ -416,10 +415,9 @@ __device__ void batch_reduce_decide(const BArgs &a, BShared &S, int kind, int64_
                     S.rr[m] = tot;
                 }
             }
-            // pause at the end of the launch's slice, or once enough problems left; only a solve
-            // in CG mode pauses (a refinement step finishes first)
-            if (keep && kind == 2 && S.mode[m] == 0 &&
-                (it >= a.slice || (a.pause_left > 0 && S.left >= a.pause_left)))
+            // pause at the end of the launch's slice; only a solve in CG mode pauses (a refinement
+            // step finishes first)
+            if (keep && kind == 2 && S.mode[m] == 0 && it >= a.slice)
             {
                 S.status[m] |= 8;
                 keep = 0;
@@ -443,10 +441,7 @@ __device__ void batch_reduce_decide(const BArgs &a, BShared &S, int kind, int64_
     if (t < nnew)
         S.act[t] = S.keep[t];
     if (t == 0)
-    {
         S.nact = nnew;
-        S.left += gone;
-    }
     __syncthreads();
     batch_split(a, S);
 }
@@ -584,7 +579,6 @@ __global__ void __launch_bounds__(kBatchThreads<TV>, kCGMinBlocks) k_cg_batch(BA
     {
         s_fail = 0;
         S.nact = a.ninst;
-        S.left = 0;
     }
     for (int m = t; m < a.ninst; m += blockDim.x)
     {
@@ -791,8 +785,6 @@ struct BatchCtx
 {
     int device = 0, num_sms = 0, grid = 0;
     int64_t slice = 512; // CG iterations per launch before unfinished solves pause
-    double pause_frac = 0.0; // > 0: pause the unfinished solves once this fraction of a launch's
-                             // problems finished (the others resume in the next launch)
     size_t smem64 = 0, smem32 = 0; // dynamic shared memory of the two kernel variants
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_done = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
@@ -970,7 +962,6 @@ struct BatchCtx
         a.part = d_part;
         a.ninst = ni;
         a.slice = slice > 0 ? slice : (int64_t(1) << 62);
-        a.pause_left = (pause_frac > 0 && ni > 1) ? std::max(1, (int)std::ceil(pause_frac * ni)) : 0;
         void *args[] = {&a};
         if ((e = cudaEventRecord(ev_t0, stream)) != cudaSuccess)
             return e;
