@@ -59,6 +59,7 @@ def args_():
     ap.add_argument("--plates", type=int, default=64, help="plates in the batched damage workload")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
     ap.add_argument("--no-tangent", action="store_true", help="skip the FCC J2 tangent-mode leg")
+    ap.add_argument("--no-dump", action="store_true", help="skip the per-step dump output leg")
     ap.add_argument("--tangent-steps", type=int, default=4, help="load steps of the FCC bar's 50-step path timed")
     ap.add_argument("--serve-requests", type=int, default=12, help="requests in the serving-stream sample")
     ap.add_argument("--serve-max-particles", type=float, default=1e5,
@@ -325,6 +326,10 @@ def run_ours(a):
     if single and not a.no_tangent:
         barrier()
         tangent = tangent_leg(lpm, a.tangent_steps, local, world, allreduce)
+    dump = None
+    if single and not a.no_dump:
+        barrier()
+        dump = dump_leg(lpm, case, W, local)
     serving = None
     if single and not a.no_serving:
         barrier()
@@ -351,12 +356,56 @@ def run_ours(a):
                                    "force": (c1["force_seconds"] - c0["force_seconds"]) * 1e3 / K,
                                    "cg_kernel": cg_s * 1e3 / K},
             "roofline": roof, "e2e": e2e, "gpu_launches": counters_total, "clocks": clocks,
-            "mixed": mixed, "batched": batched, "serving": serving, "tangent": tangent, "cpu_baseline": cpu,
+            "mixed": mixed, "batched": batched, "serving": serving, "tangent": tangent, "dump": dump,
+            "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def dump_leg(lpm, case, first_step, device, steps=3):
+    """Per-step output on the headline cube: lpmgpu_dump_write appends each load step's state in
+    the reference's dump text (Assembly::writeDump, include/assembly.h:310-335), formatted on all
+    host cores.  Three arms of `steps` FP64 load steps each, wall time: the steps alone, each step
+    followed by a synchronous dump, and each step's dump written by the writer thread while the
+    next step runs (flushed at the end).  Errors are reported in the line, not raised."""
+    import shutil
+    import tempfile
+    import torch
+    d = tempfile.mkdtemp(prefix="lpm_dump_")
+    try:
+        prob = lpm.GpuProblem(case.assembly(), undamaged_pt_type=case.undamaged_type, max_iter=case.max_iter,
+                              tol_iter=case.tol_iter, precision=lpm.Precision.FP64, device=device)
+        s = first_step
+        ok, _ = prob.solve_load_step(step_of(case, s))
+        s += 1
+        arms = {}
+        for arm in ("steps_only", "sync_dump", "async_dump"):
+            path = os.path.join(d, arm + ".dump")
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                ok, _ = prob.solve_load_step(step_of(case, s))
+                if not ok:
+                    raise RuntimeError(f"load step {s} did not converge")
+                if arm != "steps_only":
+                    prob.dump_write(path, s, case.box, threads=0, async_=(arm == "async_dump"))
+                s += 1
+            prob.dump_flush()
+            torch.cuda.synchronize()
+            arms[arm] = (time.perf_counter() - t0) * 1e3 / steps
+        size = os.path.getsize(os.path.join(d, "sync_dump.dump")) / steps
+        prob.close()
+        return {"particles": case.n, "bytes_per_step": size, "host_threads": os.cpu_count(),
+                "ms_per_step": arms,
+                "dump_ms_sync": arms["sync_dump"] - arms["steps_only"],
+                "dump_ms_exposed_async": arms["async_dump"] - arms["steps_only"]}
+    except Exception as ex:  # the leg must not cost the bench line
+        return {"error": f"{type(ex).__name__}: {ex}"}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
 
 
 def batched_leg(lpm, count, device, world, allreduce):
