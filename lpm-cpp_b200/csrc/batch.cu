@@ -5,15 +5,18 @@
 // 2D and 3D, each with its own sliced-ELL matrix and Krylov vectors), each with its own
 // stopping test, iteration cap and scalars: the unpreconditioned CG of Solver::LPM_CG
 // (include/solver.h:277-354, MKL RCI dcg on the squared-norm test) per problem.
-//   * Every active problem gets g >= 1 "virtual blocks", g proportional to its matrix size; a
-//     virtual block owns a contiguous share of the problem's slices (SpMV phase) and of its
-//     unknowns (update phase).  The physical blocks (one 32-warp block per SM) stride over
-//     the virtual blocks, so a problem of any size, alone or with others, keeps every SM busy.
-//   * Each virtual block writes one partial per reduction.  At the grid barrier the last block
-//     to arrive sums each problem's partials (a fixed tree: 32-wide warp sums in order), takes
-//     the per-problem decisions (alpha; converged, capped or broken down) and, when a problem
-//     leaves, re-partitions the remaining ones over the virtual blocks before it releases the
-//     barrier.  The tail of a batch (the largest problems) therefore runs on the whole GPU.
+//   * The split: the active problems' matrix costs are laid end to end and cut into one equal
+//     segment per physical block (one block per SM); a problem's piece in a block is its part of
+//     that segment in whole slices (SpMV phase) and, in proportion, of its unknowns (update
+//     phase).  Small problems share a block, large ones span many; every SM carries the same
+//     matrix volume whatever the mix.
+//   * Each piece writes one partial per reduction.  After the counting grid barrier every block
+//     sums each problem's partials in the same fixed order (32-wide warp sums in piece order),
+//     takes the same per-problem decisions (alpha; converged, capped or broken down; the mixed
+//     solves' refinement steps) and, when problems leave, re-splits the GPU over the rest, so
+//     the tail of a batch runs on the whole GPU.
+//   * Mixed members run their FP64 refinement inside the launch: x64 += x32, the true FP64
+//     residual and the restart of the next inner FP32 solve, while the others keep iterating.
 //   * All waits are bounded (4 s); a timeout sets a flag and every block returns.
 //
 // Runtime.  Each member follows SolverStatic::solveProblem / solveProblemStep
@@ -22,6 +25,7 @@
 // on Newton failure reset + halve + run both halves.  A round issues every member's next piece
 // of device work on the member's stream, one batched CG for all members that need a linear
 // solve, and then waits once for all of them before the host takes the members' decisions.
+// Also the nonlocal damage and elastic-damage particles, through the same per-member kernels.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
