@@ -3,6 +3,7 @@
 //   Particle::updateBondsGeometry / Bond::updatebGeometry  include/particle.h:164-181, bond.h:30-39
 //   ParticleElastic::updateBondsForce                      include/particle_elastic.h:38-50
 //   ParticleJ2Plasticity::updateBondsForce                 include/particle_j2plasticity.h:63-76
+//   ParticleElasticDamage::updateBondsForce                include/particle_elastic_damage.h:80-91
 //   Particle::updateParticleForce / Stress / DamageVisual  include/particle.h:151-240
 //   Solver::updateRR                                       include/solver.h:112-126
 //   ParticleJ2Plasticity::updateParticleStateVariables     include/particle_j2plasticity.h:78-140
