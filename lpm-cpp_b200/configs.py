@@ -226,6 +226,32 @@ def notched_plate(size=4.0, radius=0.1, crack=0.3, E=69e3, mu=0.3, critical_bstr
     return c
 
 
+def cantilever_beam(radius=0.12, length=30.0, depth=10.0, force=2.0, E=69e3, mu=0.33, tol_iter=1e-5,
+                    max_iter=30) -> Case:
+    """The known-answer case of examples/ex7_convergence_beam.cpp: a plane-strain hexagonal beam,
+    box {0, length, -depth/2, depth/2}, its right edge (x > xmax - EPS) fixed in x and y and its
+    left edge (x < xmin + EPS) loaded by `force` in y, shared by its particles, in one step.  The
+    example's nonlocal search (cutoff 1.5 x nonlocal_L = EPS) finds each particle alone and the
+    undamaged type 4 matches no particle; neither changes an elastic solve."""
+    box = [0.0, length, -depth / 2, depth / 2, 0.0, 1.0]
+    xyz = _gen(L.LatticeType.Hexagon2D, radius, box)
+    eps = 1e-6  # EPS, include/lpm.h:41
+    xmin, xmax = float(xyz[:, 0].min()), float(xyz[:, 0].max())
+    left = np.nonzero(xyz[:, 0] < xmin + eps)[0].astype(np.int32)
+    right = np.nonzero(xyz[:, 0] > xmax - eps)[0].astype(np.int32)
+    types = np.zeros(len(xyz), np.int32)
+    types[left] = 2
+    types[right] = 1
+    mat = L.Material(plane_stress=False, E=E, mu=mu, critical_bstrain=1.0, nonlocal_L=eps)
+    st = [([("right", "x", 0.0), ("right", "y", 0.0)], [("left", 0.0, force, 0.0)])]
+    c = Case(f"beam_{length:g}x{depth:g}_r{radius:g}", L.LatticeType.Hexagon2D, radius, box, xyz,
+             L.ParticleType.Elastic, mat, types, {"left": left, "right": right}, st, undamaged_type=4,
+             tol_iter=tol_iter, max_iter=max_iter)
+    c.nonlocal_cutoff_ratio = 1.5
+    c.meta.update({"length": box[1] - box[0], "depth": box[3] - box[2], "force": force})
+    return c
+
+
 def edamage_plate(size=2.4, radius=0.1, E=69e3, mu=0.3, steps=4, total_disp=0.008, k0=0.02, k1=0.5,
                   damage_threshold=0.9, nonlocal_L=0.3, cutoff_ratio=1.5, tol_iter=1e-9, max_iter=30) -> Case:
     """Hexagonal plate of ParticleElasticDamage particles (include/particle_elastic_damage.h) with
