@@ -13,6 +13,7 @@
 // Clients submit, poll, wait and fetch results from any thread.
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -90,7 +91,17 @@ int64_t estimate_bytes(const lpmgpu_desc &d)
     default: nc = 80; nb = 14; dim = 3; break;
     }
     const int64_t per_block = (int64_t)dim * dim * (8 + (d.precision == LPMGPU_MIXED ? 4 : 0)) + 4;
-    const int64_t per_particle = (int64_t)(1.25 * nc * per_block) + (int64_t)nb * 20 * 8 + 40 * 8 * dim + 512;
+    int64_t per_particle = (int64_t)(1.25 * nc * per_block) + (int64_t)nb * 20 * 8 + 40 * 8 * dim + 512;
+    if (d.nonlocal_cutoff_ratio > 0 && d.radius > 0)
+    {
+        // nonlocal lists: the particles within cutoff_ratio x nonlocal_L, counted for the densest
+        // packing of the dimension (hexagonal: 2 sqrt(3) r^2 per particle; FCC: 4 sqrt(2) r^3),
+        // 4 bytes each, plus the list offset and the nonlocal rate of the particle
+        const double R = d.nonlocal_cutoff_ratio * d.nonlocal_L, r = d.radius, pi = 3.14159265358979;
+        const double m = (dim == 2) ? pi * R * R / (2 * std::sqrt(3.0) * r * r)
+                                    : 4.0 / 3.0 * pi * R * R * R / (4 * std::sqrt(2.0) * r * r * r);
+        per_particle += 4 * (int64_t)(1.2 * m + 8) + 12;
+    }
     return (int64_t)d.n * per_particle + (8 << 20);
 }
 

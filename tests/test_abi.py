@@ -80,3 +80,18 @@ def test_generators_are_host_side():
     x = LPM.createCuboidSC3D([0, 2, 0, 2, 0, 2], cell)
     from oracle import oracle as O
     assert len(x) > 100 and np.array_equal(x, O.generate("sc3d", 0.2, [0, 2, 0, 2, 0, 2]))
+
+
+def test_estimate_counts_the_nonlocal_lists():
+    """The admission estimate (lpmgpu_estimate_bytes, host arithmetic) grows by at least the
+    device bytes of the nonlocal neighbour lists the search will hold: 4 per neighbour (the
+    particle itself included) plus an offset and a rate per particle."""
+    from scipy.spatial import cKDTree
+    for c in (CFG.edamage_plate(), CFG.edamage_plate(size=3.0, cutoff_ratio=3.0)):
+        a = c.assembly()
+        with_nl = LPM.Server.estimate_bytes(a)
+        a.nonlocal_cutoff_ratio = 0.0
+        without = LPM.Server.estimate_bytes(a)
+        R = c.nonlocal_cutoff_ratio * c.material.nonlocal_L
+        pairs = sum(len(v) for v in cKDTree(c.xyz).query_ball_point(c.xyz, R * (1 - 1e-12)))
+        assert with_nl - without >= 4 * pairs + 12 * c.n
