@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import ctypes as C
 import enum
+import math
 import os
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
@@ -35,6 +36,7 @@ class ParticleType(enum.IntEnum):
     Elastic = 0
     ElasticDamage = 1
     J2Plasticity = 2
+    FatigueHCF = 3
 
 
 class LoadMode(enum.IntEnum):
@@ -350,6 +352,12 @@ class Material:
     k1: float = 1.0
     comp_tensile_ratio: float = 10.0
     damage_threshold: float = 1.0
+    # ParticleFatigueHCF (particle_fatigue_hcf.h:163-205): damage rate A pow(max energy, B)
+    # pow(energy range, d); the fatigue limit ratio is kept but unused, as in the reference
+    fatigue_A: float = 0.0
+    fatigue_B: float = 0.0
+    fatigue_d: float = 0.0
+    fatigue_limit_ratio: float = 1.108
 
 
 def _read_dump(path: str):
@@ -485,6 +493,73 @@ class LoadStep:
             d.cutHalf()
         for f in self.forceBCs:
             f.cutHalf()
+
+
+# ---------------------------------------------------------------------------- fatigue loading
+class FatigueLoadType(enum.IntEnum):
+    """include/load_step_fatigue.h:14-20"""
+    LoadUniaxialDisp = 0
+    LoadUniaxialForce = 1
+    LoadDogBoneDisp = 2
+    LoadCTForce = 3
+
+
+class TimeMapMode(enum.IntEnum):
+    """include/lpm.h:85-89"""
+    Linear = 0
+    Exponential = 1
+
+
+def LoadUniaxialForce(fy, left_group, top_group, bottom_group) -> LoadStep:
+    """include/load_step_fatigue.h:23-36"""
+    return LoadStep([DispBC(left_group, LoadMode.Relative, "x", 0.0), DispBC(bottom_group, LoadMode.Relative, "y", 0.0)],
+                    [ForceBC(top_group, LoadMode.Relative, 0.0, fy, 0.0)])
+
+
+def LoadUniaxialDisp(dy, left_group, top_group, bottom_group) -> LoadStep:
+    """include/load_step_fatigue.h:38-51"""
+    return LoadStep([DispBC(left_group, LoadMode.Relative, "x", 0.0), DispBC(top_group, LoadMode.Relative, "y", dy),
+                     DispBC(bottom_group, LoadMode.Relative, "y", 0.0)], [])
+
+
+def LoadDogBoneDisp(x, y, z, group1, group2) -> LoadStep:
+    """include/load_step_fatigue.h:53-69"""
+    return LoadStep([DispBC(group1, LoadMode.Relative, "x", x), DispBC(group1, LoadMode.Relative, "y", y),
+                     DispBC(group1, LoadMode.Relative, "z", z), DispBC(group2, LoadMode.Relative, "x", 0.0),
+                     DispBC(group2, LoadMode.Relative, "y", 0.0), DispBC(group2, LoadMode.Relative, "z", 0.0)], [])
+
+
+def LoadCTForce(fy, mid_group, top_group, bottom_group) -> LoadStep:
+    """include/load_step_fatigue.h:71-87"""
+    return LoadStep([DispBC(mid_group, LoadMode.Relative, "y", 0.0), DispBC(top_group, LoadMode.Relative, "x", 0.0),
+                     DispBC(bottom_group, LoadMode.Relative, "x", 0.0)],
+                    [ForceBC(top_group, LoadMode.Relative, 0.0, fy, 0.0),
+                     ForceBC(bottom_group, LoadMode.Relative, 0.0, -fy, 0.0)])
+
+
+def func_dNdt_linear(tau: float) -> int:
+    """include/solver_fatigue.h:60-63: (int)(1 / tau)"""
+    return int(1 / tau)
+
+
+def func_dNdt_exponental(tau: float, t: float) -> int:
+    """include/solver_fatigue.h:65-68: (int)(1 / tau * exp(t / tau))"""
+    return int(1 / tau * math.exp(t / tau))
+
+
+def generateLoadCycle(ltype: FatigueLoadType, load_spectrum: Sequence[float], N: int, n_interval: int,
+                      pt_groups: Sequence[np.ndarray]) -> List[LoadStep]:
+    """SolverFatigue::generateLoadCycle (include/solver_fatigue.h:128-180): the cycle from
+    spectrum values f0 = [2N], f1 = [2N+1], f2 = [2N+2] as n_interval steps of (f1 - f0) / n_interval
+    then n_interval steps of (f2 - f1) / n_interval."""
+    f0, f1, f2 = (float(load_spectrum[2 * N + k]) for k in range(3))
+    g = list(pt_groups)
+    make = {FatigueLoadType.LoadUniaxialDisp: lambda v: LoadUniaxialDisp(v, g[0], g[1], g[2]),
+            FatigueLoadType.LoadUniaxialForce: lambda v: LoadUniaxialForce(v, g[0], g[1], g[2]),
+            FatigueLoadType.LoadDogBoneDisp: lambda v: LoadDogBoneDisp(0, v, 0, g[0], g[1]),
+            FatigueLoadType.LoadCTForce: lambda v: LoadCTForce(v, g[0], g[1], g[2])}[FatigueLoadType(ltype)]
+    return ([make((f1 - f0) / n_interval) for _ in range(n_interval)] +
+            [make((f2 - f1) / n_interval) for _ in range(n_interval)])
 
 
 class _CStep:

@@ -41,6 +41,7 @@ struct lpmo_problem
     /* material */
     double E, mu, critical_bstrain, sigmay, xi, H, A, damage_threshold, nonlocal_L;
     double k0, k1; /* ParticleElasticDamage damage surface (particle_elastic_damage.h:27) */
+    double fA, fB, fd; /* ParticleFatigueHCF rate law (particle_fatigue_hcf.h:19) */
     int undamaged_type, max_iter, tangent;
     double tol, cg_rtol, cg_atol;
     long long cg_maxit;
@@ -610,7 +611,9 @@ lpmo_problem *lpmo_create(const lpmo_desc *d)
     p->nlayer = 2;
     p->ptype = d->ptype;
     set_cell(p, d->lattice, d->radius);
-    p->nsv = (d->ptype == LPMO_J2) ? 7 : 1;
+    /* J2: 7 (particle_j2plasticity.h); fatigue HCF: [0] largest energy so far, [1] / [2] the
+     * smallest / largest energy of the current cycle (particle_fatigue_hcf.h:16) */
+    p->nsv = (d->ptype == LPMO_J2) ? 7 : (d->ptype == LPMO_FATIGUE_HCF) ? 3 : 1;
     ALLOCD(p->xyz, 3 * n);
     ALLOCD(p->xyz0, 3 * n);
     ALLOCD(p->xyz_last, 3 * n);
@@ -634,6 +637,12 @@ lpmo_problem *lpmo_create(const lpmo_desc *d)
     memcpy(p->xyz_last, d->xyz, sizeof(double) * 3 * n);
     if (d->type)
         memcpy(p->type, d->type, sizeof(int) * n);
+    if (d->ptype == LPMO_FATIGUE_HCF)
+        for (int i = 0; i < n; ++i) /* state_var = state_var_last = {0, INT_MAX, 0} (particle_fatigue_hcf.h:27-28) */
+        {
+            p->sv[3 * i + 1] = 2147483647.0;
+            p->sv_last[3 * i + 1] = 2147483647.0;
+        }
 
     if (d->bond_nb0 && d->bond_nb1 && d->bond_p2)
         build_bonds_user(p, d);
@@ -677,7 +686,11 @@ lpmo_problem *lpmo_create(const lpmo_desc *d)
     p->A = d->A;
     /* never assigned for J2 in the reference (particle_j2plasticity.h:22); ParticleElasticDamage
      * takes it from setParticleProperty (particle_elastic_damage.h:186) */
-    p->damage_threshold = (d->ptype == LPMO_ELASTIC_DAMAGE) ? d->damage_threshold : 0;
+    p->damage_threshold =
+        (d->ptype == LPMO_ELASTIC_DAMAGE || d->ptype == LPMO_FATIGUE_HCF) ? d->damage_threshold : 0;
+    p->fA = d->fatigue_A;
+    p->fB = d->fatigue_B;
+    p->fd = d->fatigue_d;
     p->k0 = d->k0;
     p->k1 = d->k1;
     p->nonlocal_L = d->nonlocal_L;
@@ -821,14 +834,15 @@ void lpmo_update_force_state(lpmo_problem *p)
     const int n = p->n;
     /* ParticleElastic::updateBondsForce (particle_elastic.h:38-50);
      * ParticleJ2Plasticity::updateBondsForce (particle_j2plasticity.h:63-76) and
-     * ParticleElasticDamage::updateBondsForce (particle_elastic_damage.h:80-91): bond damage is
-     * the largest of its own and its two particles' */
+     * ParticleElasticDamage::updateBondsForce (particle_elastic_damage.h:80-91) and
+     * ParticleFatigueHCF::updateBondsForce (particle_fatigue_hcf.h:66-80): bond damage is the
+     * largest of its own and its two particles' */
     for (int i = 0; i < n; ++i)
         for (int b = B0(p, i); b < BE(p, i); ++b)
         {
             int L = p->blayer[b];
             double f = 2. * p->Kn[b] * p->dLe[b] + 2. * p->Tv[b] * p->dLe_total[2 * i + L];
-            if (p->ptype == LPMO_J2 || p->ptype == LPMO_ELASTIC_DAMAGE)
+            if (p->ptype == LPMO_J2 || p->ptype == LPMO_ELASTIC_DAMAGE || p->ptype == LPMO_FATIGUE_HCF)
                 p->bdamage[b] = std_max(p->bdamage[b], std_max(p->damage[i], p->damage[p->bp2[b]]));
             f *= (1.0 - p->bdamage[b]);
             p->bforce[b] = f;
@@ -874,6 +888,34 @@ void lpmo_update_force_state(lpmo_problem *p)
  * Particle::updateParticleStateVariables is a no-op for elastic particles (particle.h:62) */
 void lpmo_update_state_var(lpmo_problem *p)
 {
+    if (p->ptype == LPMO_FATIGUE_HCF)
+    {
+        /* ParticleFatigueHCF::updateParticleStateVariables (particle_fatigue_hcf.h:128-145) with
+         * calcEqEnergy (:83-125), which returns the total energy: the spring energy of each bond
+         * plus the volumetric term of each layer, per modified volume (its split into
+         * dilatational and distortional parts does not reach the result) */
+        for (int i = 0; i < p->n; ++i)
+        {
+            const double V_m = p->pvol * p->nb[i] / p->nneighbors;
+            double energy = 0;
+            for (int L = 0; L < 2; ++L)
+            {
+                const int lo = L == 0 ? B0(p, i) : B0(p, i) + p->nb0[i], hi = L == 0 ? B0(p, i) + p->nb0[i] : BE(p, i);
+                for (int b = lo; b < hi; ++b)
+                    energy += 0.5 * (p->Kn[b] * p->dLe[b] * p->dLe[b]) / V_m;
+                energy += 0.5 * p->TdLe_total[2 * i + L] * p->dLe_total[2 * i + L] / V_m;
+            }
+            double *sv = p->sv + 3 * i;
+            sv[1] = (sv[1] < energy) ? sv[1] : energy; /* std::min(curr, sv[1]) */
+            sv[2] = (energy < sv[2]) ? sv[2] : energy; /* std::max(curr, sv[2]) */
+            sv[0] = (sv[2] < sv[0]) ? sv[0] : sv[2];   /* std::max(sv[2], sv[0]) */
+            if (sv[2] - sv[1] > 0)
+                p->ddot_local[i] = p->fA * pow(sv[0], p->fB) * pow(sv[2] - sv[1], p->fd);
+            else
+                p->ddot_local[i] = 0;
+        }
+        return;
+    }
     if (p->ptype == LPMO_ELASTIC_DAMAGE)
     {
         /* ParticleElasticDamage::updateParticleStateVariables (particle_elastic_damage.h:159-170)
@@ -1493,8 +1535,9 @@ static int newton(lpmo_problem *p, lpmo_stats *st)
     return ni;
 }
 
-/* SolverStatic::updateStaticDamage (solver_static.h:32-62) with func_phi (lpm.h:48-52) */
-static int update_static_damage(lpmo_problem *p)
+/* the nonlocal damage rate of SolverStatic::updateStaticDamage (solver_static.h:35-52) and
+ * SolverFatigue::updateFatigueDamage (solver_fatigue.h:79-115), with func_phi (lpm.h:48-52) */
+static void nonlocal_rate(lpmo_problem *p)
 {
     const int n = p->n;
     for (int i = 0; i < n; ++i)
@@ -1516,6 +1559,13 @@ static int update_static_damage(lpmo_problem *p)
         }
         p->ddot_nonlocal[i] /= A;
     }
+}
+
+/* SolverStatic::updateStaticDamage (solver_static.h:32-62) */
+static int update_static_damage(lpmo_problem *p)
+{
+    const int n = p->n;
+    nonlocal_rate(p);
     int any = 0;
     for (int i = 0; i < n; ++i)
     {
@@ -1531,9 +1581,11 @@ static int update_static_damage(lpmo_problem *p)
                 p->damage[i] = 1;
             changed = fabs(p->damage[i] - p->damage_last[i]) > 1e-3;
         }
-        else
+        else if (p->ptype == LPMO_ELASTIC)
         {
-            /* ParticleElastic::updateParticleStaticDamage (particle_elastic.h:52-68) */
+            /* ParticleElastic::updateParticleStaticDamage (particle_elastic.h:52-68); fatigue
+             * particles keep Particle::updateParticleStaticDamage, which changes nothing
+             * (particle.h:63) */
             for (int b = B0(p, i); b < BE(p, i); ++b)
                 if (p->bstrain[b] >= p->critical_bstrain && fabs(p->bdamage[b] - 1.0) > EPS)
                 {
@@ -1674,4 +1726,127 @@ void lpmo_set_bond_damage(lpmo_problem *p, const double *bdamage)
 {
     memcpy(p->bdamage, bdamage, sizeof(double) * p->nbonds);
     memcpy(p->bdamage_last, bdamage, sizeof(double) * p->nbonds);
+}
+
+/* ------------------------------------------------------------------ SolverFatigue (solver_fatigue.h) */
+
+/* SolverFatigue::solveProblemStep (solver_fatigue.h:278-302): BCs, the stiffness from the
+ * current state, Newton; no damage loop */
+int lpmo_fatigue_solve_step(lpmo_problem *p, const lpmo_loadstep *s, lpmo_stats *st)
+{
+    lpmo_apply_bc(p, s);
+    if (!p->tangent)
+        lpmo_assemble(p, 1);
+    const int n_newton = newton(p, st);
+    if (st)
+        st->reaction_norm = sqrt(p->reaction_sq);
+    return n_newton < p->max_iter;
+}
+
+/* SolverFatigue::updateFatigueDamage (solver_fatigue.h:76-126) with
+ * ParticleFatigueHCF::updateParticleFatigueDamage (particle_fatigue_hcf.h:148-160); the other
+ * particle types keep Particle::updateParticleFatigueDamage, which changes nothing
+ * (particle.h:64) */
+int lpmo_fatigue_update_damage(lpmo_problem *p, double dNdt)
+{
+    nonlocal_rate(p);
+    int any = 0;
+    for (int i = 0; i < p->n; ++i)
+    {
+        if (p->type[i] == p->undamaged_type)
+            continue;
+        int changed = 0;
+        if (p->ptype == LPMO_FATIGUE_HCF)
+        {
+            p->damage[i] += p->ddot_nonlocal[i] * dNdt;
+            if (p->damage[i] >= p->damage_threshold)
+                p->damage[i] = 1;
+            p->sv[3 * i + 1] = 2147483647.0; /* INT_MAX */
+            p->sv[3 * i + 2] = 0;
+            changed = fabs(p->damage[i] - p->damage_last[i]) > 1e-3;
+        }
+        any = changed || any;
+    }
+    return any;
+}
+
+/* SolverFatigue::solveProblemOneCycle (solver_fatigue.h:221-241) */
+int lpmo_fatigue_cycle(lpmo_problem *p, const lpmo_loadstep *steps, int nsteps, double dNdt, lpmo_stats *st)
+{
+    if (st)
+        memset(st, 0, sizeof *st);
+    int all_converged = 1;
+    for (int k = 0; k < nsteps; ++k)
+    {
+        /* the reference ignores a step that did not converge (is_converged is unused) */
+        if (!lpmo_fatigue_solve_step(p, &steps[k], st))
+        {
+            all_converged = 0;
+            if (st)
+                st->cuts++;
+        }
+        lpmo_update_state_var(p);
+    }
+    const int any = lpmo_fatigue_update_damage(p, dNdt);
+    store_state(p);
+    lpmo_update_geometry(p);
+    lpmo_update_force_state(p);
+    if (st)
+    {
+        st->converged = all_converged;
+        st->reaction_norm = sqrt(p->reaction_sq);
+    }
+    return any;
+}
+
+/* one load step of SolverFatigue::solveProblemStatic (solver_fatigue.h:244-275): on failure reset
+ * the state, halve the step and run the two halves; every converged (sub)step is followed by
+ * updateStateVar and storeStateVar */
+static int fatigue_static_rec(lpmo_problem *p, const lpmo_loadstep *s, double scale, lpmo_stats *st, int depth)
+{
+    lpmo_dispbc db[64];
+    lpmo_forcebc fb[64];
+    lpmo_loadstep sc = *s;
+    if (s->ndisp > 64 || s->nforce > 64)
+        return 0;
+    for (int d = 0; d < s->ndisp; ++d)
+    {
+        db[d] = s->disp[d];
+        db[d].step = s->disp[d].step * scale;
+    }
+    for (int f = 0; f < s->nforce; ++f)
+    {
+        fb[f] = s->force[f];
+        fb[f].fx = s->force[f].fx * scale;
+        fb[f].fy = s->force[f].fy * scale;
+        fb[f].fz = s->force[f].fz * scale;
+    }
+    sc.disp = db;
+    sc.force = fb;
+    if (lpmo_fatigue_solve_step(p, &sc, st))
+    {
+        lpmo_update_state_var(p);
+        store_state(p);
+        return 1;
+    }
+    if (depth >= 30)
+        return 0;
+    reset_state(p);
+    if (st)
+        st->cuts++;
+    return fatigue_static_rec(p, s, scale / 2.0, st, depth + 1) &&
+           fatigue_static_rec(p, s, scale / 2.0, st, depth + 1);
+}
+
+int lpmo_fatigue_static_step(lpmo_problem *p, const lpmo_loadstep *s, lpmo_stats *st)
+{
+    if (st)
+        memset(st, 0, sizeof *st);
+    const int ok = fatigue_static_rec(p, s, 1.0, st, 0);
+    if (st)
+    {
+        st->converged = ok;
+        st->reaction_norm = sqrt(p->reaction_sq);
+    }
+    return ok;
 }

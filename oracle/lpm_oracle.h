@@ -13,8 +13,8 @@ extern "C" {
 
 /* LatticeType order of include/lpm.h:97-106 */
 enum { LPMO_SQUARE2D = 0, LPMO_HEXAGON2D = 1, LPMO_SC3D = 2, LPMO_FCC3D = 3, LPMO_BCC3D = 4 };
-/* ParticleType order of include/lpm.h:89-95 (FatigueHCF is not on the path) */
-enum { LPMO_ELASTIC = 0, LPMO_ELASTIC_DAMAGE = 1, LPMO_J2 = 2 };
+/* ParticleType order of include/lpm.h:89-95 */
+enum { LPMO_ELASTIC = 0, LPMO_ELASTIC_DAMAGE = 1, LPMO_J2 = 2, LPMO_FATIGUE_HCF = 3 };
 
 typedef struct
 {
@@ -44,6 +44,11 @@ typedef struct
     int tangent;
     /* ParticleElasticDamage only (setParticleProperty, particle_elastic_damage.h:183-220) */
     double k0, k1, comp_tensile_ratio, damage_threshold;
+    /* ParticleFatigueHCF only (setParticleProperty, particle_fatigue_hcf.h:163-205): the damage
+     * rate A * pow(max energy, B) * pow(energy range, d); damage_threshold above is its p_d_thres.
+     * The fatigue limit ratio is stored by the reference but unused (calcEqEnergy returns the
+     * total energy, particle_fatigue_hcf.h:123). */
+    double fatigue_A, fatigue_B, fatigue_d, fatigue_limit_ratio;
 } lpmo_desc;
 
 typedef struct
@@ -117,6 +122,24 @@ void lpmo_apply_bc(lpmo_problem *p, const lpmo_loadstep *s);
 int lpmo_solve_problem_step(lpmo_problem *p, const lpmo_loadstep *s, lpmo_stats *st);
 /* one entry of solver_static.h:72-93: solve, and on failure reset, halve, retry */
 int lpmo_solve_load_step(lpmo_problem *p, const lpmo_loadstep *s, lpmo_stats *st);
+
+/* SolverFatigue (include/solver_fatigue.h).  One fatigue step: updateForceBC,
+ * updateDisplacementBC, the stiffness from the current state, NewtonIteration; no damage loop
+ * (solver_fatigue.h:278-302).  Returns 1 when Newton converged. */
+int lpmo_fatigue_solve_step(lpmo_problem *p, const lpmo_loadstep *s, lpmo_stats *st);
+/* SolverFatigue::updateFatigueDamage (solver_fatigue.h:76-126): the nonlocal average of the
+ * local rates, then damage += rate * dNdt per damageable particle; returns any_damaged */
+int lpmo_fatigue_update_damage(lpmo_problem *p, double dNdt);
+/* SolverFatigue::solveProblemOneCycle (solver_fatigue.h:221-241): every step of the cycle
+ * (fatigue step + updateStateVar, failures ignored as in the reference), then
+ * updateFatigueDamage(dNdt), storeStateVar, updateGeometry, updateForceState.  Returns
+ * updateFatigueDamage's flag; st sums the steps' Newton solves and counts unconverged steps
+ * in st->cuts. */
+int lpmo_fatigue_cycle(lpmo_problem *p, const lpmo_loadstep *steps, int nsteps, double dNdt, lpmo_stats *st);
+/* one entry of SolverFatigue::solveProblemStatic (solver_fatigue.h:244-275): the fatigue step,
+ * on failure reset, halve and retry; after each converged (sub)step updateStateVar and
+ * storeStateVar.  Returns 1 when every (sub)step converged. */
+int lpmo_fatigue_static_step(lpmo_problem *p, const lpmo_loadstep *s, lpmo_stats *st);
 
 /* state read-back (n*3 / n*6 / n / n*nsv / nbonds) */
 void lpmo_read_state(const lpmo_problem *p, double *xyz, double *pin, double *stress, double *damage,

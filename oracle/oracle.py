@@ -21,7 +21,7 @@ REF_BIN = os.path.join(HERE, "_ref", "lpm_ref")
 REF_GPU_BIN = os.path.join(HERE, "_ref", "lpm_ref_gpu")
 
 LATTICES = {"sq2d": 0, "hex2d": 1, "sc3d": 2, "fcc3d": 3, "bcc3d": 4}
-PTYPES = {"elastic": 0, "elastic_damage": 1, "j2": 2}
+PTYPES = {"elastic": 0, "elastic_damage": 1, "j2": 2, "fatigue_hcf": 3}
 
 
 class _Desc(C.Structure):
@@ -37,6 +37,8 @@ class _Desc(C.Structure):
         ("bond_nb0", C.POINTER(C.c_int)), ("bond_nb1", C.POINTER(C.c_int)), ("bond_p2", C.POINTER(C.c_int)),
         ("tangent", C.c_int),
         ("k0", C.c_double), ("k1", C.c_double), ("comp_tensile_ratio", C.c_double), ("damage_threshold", C.c_double),
+        ("fatigue_A", C.c_double), ("fatigue_B", C.c_double), ("fatigue_d", C.c_double),
+        ("fatigue_limit_ratio", C.c_double),
     ]
 
 
@@ -98,6 +100,13 @@ def lib():
         L.lpmo_solve_problem_step.argtypes = [C.c_void_p, C.POINTER(_LoadStep), C.POINTER(_Stats)]
         L.lpmo_solve_load_step.restype = C.c_int
         L.lpmo_solve_load_step.argtypes = [C.c_void_p, C.POINTER(_LoadStep), C.POINTER(_Stats)]
+        for f in ("lpmo_fatigue_solve_step", "lpmo_fatigue_static_step"):
+            getattr(L, f).restype = C.c_int
+            getattr(L, f).argtypes = [C.c_void_p, C.POINTER(_LoadStep), C.POINTER(_Stats)]
+        L.lpmo_fatigue_update_damage.restype = C.c_int
+        L.lpmo_fatigue_update_damage.argtypes = [C.c_void_p, C.c_double]
+        L.lpmo_fatigue_cycle.restype = C.c_int
+        L.lpmo_fatigue_cycle.argtypes = [C.c_void_p, C.POINTER(_LoadStep), C.c_int, C.c_double, C.POINTER(_Stats)]
         L.lpmo_read_state.argtypes = [C.c_void_p, dp, dp, dp, dp, dp, dp, dp]
         L.lpmo_read_residual.argtypes = [C.c_void_p, dp]
         L.lpmo_set_xyz.argtypes = [C.c_void_p, dp]
@@ -154,6 +163,11 @@ class Material:
     k1: float = 1.0
     comp_tensile_ratio: float = 10.0
     damage_threshold: float = 1.0
+    # ParticleFatigueHCF (particle_fatigue_hcf.h:163-205)
+    fatigue_A: float = 0.0
+    fatigue_B: float = 0.0
+    fatigue_d: float = 0.0
+    fatigue_limit_ratio: float = 1.108
 
 
 class _StepHolder:
@@ -198,6 +212,8 @@ class OracleProblem:
         d.cg_rtol, d.cg_atol, d.cg_maxit = cg_rtol, cg_atol, cg_maxit
         d.tangent = int(bool(tangent))
         d.k0, d.k1, d.comp_tensile_ratio, d.damage_threshold = mat.k0, mat.k1, mat.comp_tensile_ratio, mat.damage_threshold
+        d.fatigue_A, d.fatigue_B = getattr(mat, "fatigue_A", 0.0), getattr(mat, "fatigue_B", 0.0)
+        d.fatigue_d, d.fatigue_limit_ratio = getattr(mat, "fatigue_d", 0.0), getattr(mat, "fatigue_limit_ratio", 1.108)
         if bonds is not None:
             self._bonds = [np.ascontiguousarray(a, dtype=np.int32) for a in bonds]
             d.bond_nb0, d.bond_nb1, d.bond_p2 = (_ip(a) for a in self._bonds)
@@ -277,6 +293,31 @@ class OracleProblem:
     def set_xyz(self, xyz):
         a = np.ascontiguousarray(xyz, dtype=np.float64)
         lib().lpmo_set_xyz(self._h, _dp(a))
+
+    # ---- SolverFatigue (include/solver_fatigue.h)
+    @staticmethod
+    def _stats(st):
+        return {"newton_solves": st.newton_solves, "cg_iters": st.cg_iters, "cuts": st.cuts,
+                "converged": bool(st.converged), "reaction_norm": st.reaction_norm}
+
+    def fatigue_static_step(self, disp=(), force=()):
+        """One entry of SolverFatigue::solveProblemStatic (solver_fatigue.h:244-275)."""
+        h = _StepHolder(disp, force)
+        st = _Stats()
+        ok = lib().lpmo_fatigue_static_step(self._h, C.byref(h.s), C.byref(st))
+        return bool(ok), self._stats(st)
+
+    def fatigue_cycle(self, steps, dNdt):
+        """SolverFatigue::solveProblemOneCycle (solver_fatigue.h:221-241); steps: [(disp, force)].
+        Returns (any_damaged, stats) with stats["cuts"] = the steps that did not converge."""
+        hs = [_StepHolder(d, f) for d, f in steps]
+        arr = (_LoadStep * max(len(hs), 1))(*[h.s for h in hs])
+        st = _Stats()
+        any_d = lib().lpmo_fatigue_cycle(self._h, arr, len(hs), float(dNdt), C.byref(st))
+        return bool(any_d), self._stats(st)
+
+    def fatigue_update_damage(self, dNdt):
+        return bool(lib().lpmo_fatigue_update_damage(self._h, float(dNdt)))
 
     def bond_kntv(self):
         nb = lib().lpmo_nbonds(self._h)
@@ -361,8 +402,10 @@ def write_ref_spec(case, outdir: str, steps=None, max_iter=None, tol_iter=None, 
     m = case.material
     lines = [f"lattice {lat}", f"radius {case.radius!r}", "box " + " ".join(repr(float(v)) for v in case.box),
              f"euler {case.euler[0]} " + " ".join(repr(float(a)) for a in case.euler[1]),
-             f"ptype {({2: 'j2', 1: 'elastic_damage'}).get(int(case.ptype), 'elastic')}",
+             f"ptype {({2: 'j2', 1: 'elastic_damage', 3: 'fatigue_hcf'}).get(int(case.ptype), 'elastic')}",
              f"plane_stress {int(m.plane_stress)}",
+             f"hcf {getattr(m, 'fatigue_A', 0.0)!r} {getattr(m, 'fatigue_B', 0.0)!r} {getattr(m, 'fatigue_d', 0.0)!r} "
+             f"{getattr(m, 'damage_threshold', 1.0)!r} {getattr(m, 'fatigue_limit_ratio', 1.108)!r}",
              f"edamage {getattr(m, 'k0', 0.0)!r} {getattr(m, 'k1', 1.0)!r} {getattr(m, 'comp_tensile_ratio', 10.0)!r} "
              f"{getattr(m, 'damage_threshold', 1.0)!r}",
              f"nonlocal_cutoff_ratio {float(getattr(case, 'nonlocal_cutoff_ratio', 0.0))!r}",
@@ -406,4 +449,12 @@ def write_ref_spec(case, outdir: str, steps=None, max_iter=None, tol_iter=None, 
             lines.append(f"forcebc {g} {float(fx)!r} {float(fy)!r} {float(fz)!r} {s} {s + 1}")
     for k in dump_k:
         lines.append(f"dumpK {int(k)}")
+    fat = getattr(case, "meta", {}).get("fatigue")
+    if fat is not None:
+        p = os.path.join(outdir, "fatigue_load.txt")
+        with open(p, "w") as f:
+            f.write("\n".join(repr(float(v)) for v in fat["spectrum"]) + "\n")
+        lines.append(f"fatigue {fat['load_type']} {int(fat['n_interval'])} {fat['tmode']} {float(fat['tau'])!r}")
+        lines.append("fatigue_groups " + " ".join(fat["groups"]))
+        lines.append(f"fatigue_load {p}")
     return "\n".join(lines) + "\n"

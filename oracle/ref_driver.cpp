@@ -46,6 +46,17 @@
  *   bondprops PATH        (raw f64: Kn[nb], Tv[nb], bdamage[nb] in bond order, written into
  *                          Bond::Kn / Tv / bdamage and bdamage_last (include/bond.h:25-27) after
  *                          setParticleProperty: a heterogeneous material or initial damage)
+ *   ptype fatigue_hcf + hcf A B D D_THRES F_LMT_RATIO
+ *                         (ParticleFatigueHCF::setParticleProperty, include/particle_fatigue_hcf.h:163-205)
+ *   fatigue TYPE N_INTERVAL TMODE TAU   (SolverFatigue, include/solver_fatigue.h: TYPE uniaxial_disp|
+ *                          uniaxial_force|dogbone_disp|ct_force (include/load_step_fatigue.h),
+ *                          TMODE linear|exponential).  The load steps then run through
+ *                          SolverFatigue::solveProblemStatic one at a time, followed by the cycles of
+ *                          SolverFatigue::solveProblemCyclic, with the state written after each
+ *                          static step and each cycle (outputs numbered on); cycles.txt holds the
+ *                          cycle count N and dNdt after each cycle.
+ *   fatigue_groups G0 G1 [G2]   (the pt_groups of solveProblemCyclic)
+ *   fatigue_load PATH     (the load spectrum, SolverFatigue::readLoad)
  */
 #include <cstdio>
 #include <cstdlib>
@@ -64,6 +75,10 @@
 #include "stiffness.h"
 #include "load_step.h"
 #include "solver_static.h"
+#ifndef LPM_USE_GPU
+#include "solver_fatigue.h"
+#include "load_step_fatigue.h"
+#endif
 #ifdef LPM_USE_GPU
 /* the one-line switch of an example's run(): SolverStatic -> SolverStaticGPU (lpm-cpp_b200/cpp) */
 #include "solver_static_gpu.h"
@@ -136,6 +151,11 @@ struct Spec
     std::string dumpfile = "/dev/null";
     int tangent = 0;
     double cg_rtol = -1, cg_atol = -1;
+    double hcf_A = 0, hcf_B = 0, hcf_d = 0, hcf_thres = 1, hcf_flr = 1.108;
+    std::string fatigue_type, fatigue_tmode = "linear", fatigue_load;
+    int fatigue_interval = 1;
+    double fatigue_tau = 1;
+    std::vector<std::string> fatigue_groups;
 };
 
 static std::vector<int> read_i32(const std::string &path)
@@ -253,6 +273,15 @@ static Spec parse(const char *path)
         else if (k == "bondprops") is >> s.bondprops;
         else if (k == "dumpfile") is >> s.dumpfile;
         else if (k == "tangent") is >> s.tangent;
+        else if (k == "hcf") is >> s.hcf_A >> s.hcf_B >> s.hcf_d >> s.hcf_thres >> s.hcf_flr;
+        else if (k == "fatigue") is >> s.fatigue_type >> s.fatigue_interval >> s.fatigue_tmode >> s.fatigue_tau;
+        else if (k == "fatigue_load") is >> s.fatigue_load;
+        else if (k == "fatigue_groups")
+        {
+            std::string g;
+            while (is >> g)
+                s.fatigue_groups.push_back(g);
+        }
         else
         {
             std::fprintf(stderr, "unknown spec directive '%s'\n", k.c_str());
@@ -317,6 +346,44 @@ static Assembly<NL> make_assembly(std::vector<std::array<double, NDIM>> &xyz, st
     return Assembly<NL>{dump, sp.bondfile, cell, pt};
 }
 
+/* the particle and bond state after a load step or cycle, as raw binaries tagged by its index */
+static void write_state(Assembly<NL> &ass, const Spec &sp, const char *tag, int N)
+{
+    std::vector<double> x(3 * (size_t)N), pin(3 * (size_t)N), stress(6 * (size_t)N), dmg(N), dmgv(N), sv,
+        bdmg, dlp;
+    int nsv = (int)ass.pt_sys[0]->state_var.size();
+    sv.resize((size_t)nsv * N);
+    for (Particle<NL> *p : ass.pt_sys)
+    {
+        for (int k = 0; k < 3; ++k)
+        {
+            x[3 * p->id + k] = p->xyz[k];
+            pin[3 * p->id + k] = p->Pin[k];
+        }
+        for (int k = 0; k < 6; ++k)
+            stress[6 * p->id + k] = p->stress[k];
+        dmg[p->id] = p->damage;
+        dmgv[p->id] = p->damage_visual;
+        for (int k = 0; k < nsv; ++k)
+            sv[(size_t)nsv * p->id + k] = p->state_var[k];
+    }
+    for (Particle<NL> *p : ass.pt_sys)
+        for (int l = 0; l < NL; ++l)
+            for (Bond<NL> *b : p->bond_layers[l])
+            {
+                bdmg.push_back(b->bdamage);
+                dlp.push_back(b->dLp);
+            }
+    write_bin(sp.out + "/xyz_" + tag + ".f64", x.data(), x.size());
+    write_bin(sp.out + "/pin_" + tag + ".f64", pin.data(), pin.size());
+    write_bin(sp.out + "/stress_" + tag + ".f64", stress.data(), stress.size());
+    write_bin(sp.out + "/damage_" + tag + ".f64", dmg.data(), dmg.size());
+    write_bin(sp.out + "/damage_visual_" + tag + ".f64", dmgv.data(), dmgv.size());
+    write_bin(sp.out + "/state_var_" + tag + ".f64", sv.data(), sv.size());
+    write_bin(sp.out + "/bdamage_" + tag + ".f64", bdmg.data(), bdmg.size());
+    write_bin(sp.out + "/dlp_" + tag + ".f64", dlp.data(), dlp.size());
+}
+
 #ifndef LPM_USE_GPU
 /* Tangent mode: SolverStatic::solveProblemStep (include/solver_static.h:99-152) whose Newton loop
  * (Solver::NewtonIteration, include/solver.h:55-90) re-assembles the stiffness from the current
@@ -375,6 +442,88 @@ static bool tangent_step(SolverStatic<NL> &solv, LoadStep<NL> &load_step)
 }
 #endif
 
+#ifndef LPM_USE_GPU
+static FatigueLoadType fatigue_type_of(const std::string &s)
+{
+    if (s == "uniaxial_disp") return FatigueLoadType::LoadUniaxialDisp;
+    if (s == "uniaxial_force") return FatigueLoadType::LoadUniaxialForce;
+    if (s == "dogbone_disp") return FatigueLoadType::LoadDogBoneDisp;
+    if (s == "ct_force") return FatigueLoadType::LoadCTForce;
+    std::fprintf(stderr, "unknown fatigue load type %s\n", s.c_str());
+    std::exit(2);
+}
+
+static void log_line(FILE *log, int s, const lpm_shim_stats &st0, const lpm_shim_stats &st1, double wall_s, int cuts,
+                     double rn)
+{
+    std::fprintf(log, "%d %lld %lld %.6f %.6f %.6f %.6f %d %.17g %lld\n", s, st1.cg_solves - st0.cg_solves,
+                 st1.cg_iterations - st0.cg_iterations, wall_s, st1.spmv_seconds - st0.spmv_seconds,
+                 st1.cg_seconds - st0.cg_seconds, st1.create_seconds - st0.create_seconds, cuts, rn,
+                 st1.cg_failures - st0.cg_failures);
+    std::fflush(log);
+}
+
+/* SolverFatigue (include/solver_fatigue.h): the spec's load steps through solveProblemStatic one at
+ * a time, then the cycles of solveProblemCyclic.  The cycle loop is the reference's
+ * (solver_fatigue.h:183-218: generateLoadCycle, the dN/dt time map, solveProblemOneCycle,
+ * N += (int)dNdt while N < n_cycles) with the state written after each cycle in place of its
+ * printout and dump. */
+static int run_fatigue(Assembly<NL> &ass, std::map<std::string, std::vector<Particle<NL> *>> &groups,
+                       std::vector<LoadStep<NL>> &load, const Spec &sp, int N, int dim, double setup_s)
+{
+    const TimeMapMode tm = (sp.fatigue_tmode == "exponential") ? TimeMapMode::Exponential : TimeMapMode::Linear;
+    SolverFatigue<NL> solv{sp.undamaged_type, ass, StiffnessMode::Analytical, SolverMode::CG, tm, sp.fatigue_tau,
+                           sp.dumpfile, sp.max_iter, sp.tol_iter};
+    FILE *log = std::fopen((sp.out + "/steps.txt").c_str(), "w");
+    std::fprintf(log, "# N %d dim %d setup_s %.6f threads %d\n", N, dim, setup_s, omp_get_max_threads());
+    std::fprintf(log, "# step newton_solves cg_iters wall_s spmv_s cg_s create_s cuts reaction_norm cg_fail\n");
+    int start_index = 0, idx = 0;
+    char tag[32];
+    for (int s = 0; s < sp.steps; ++s, ++idx)
+    {
+        lpm_shim_stats st0 = lpm_shim_stats_g;
+        const double t0 = wall();
+        std::vector<LoadStep<NL>> one{load[s]};
+        solv.solveProblemStatic(one, start_index);
+        lpm_shim_stats st1 = lpm_shim_stats_g;
+        log_line(log, idx, st0, st1, wall() - t0, (int)one.size() - 1,
+                 cblas_dnrm2((MKL_INT)solv.reaction_force.size(), solv.reaction_force.data(), 1));
+        std::snprintf(tag, sizeof tag, "%03d", idx);
+        write_state(ass, sp, tag, N);
+    }
+    if (!sp.fatigue_load.empty())
+    {
+        const FatigueLoadType lt = fatigue_type_of(sp.fatigue_type);
+        std::vector<std::vector<Particle<NL> *>> pg;
+        for (const std::string &g : sp.fatigue_groups)
+            pg.push_back(groups[g]);
+        solv.readLoad(sp.fatigue_load);
+        FILE *cyc = std::fopen((sp.out + "/cycles.txt").c_str(), "w");
+        const double n_cycles = 0.5 * (solv.load_spectrum.size() - 1);
+        double t = 0, dNdt = 1;
+        int Nc = 0;
+        do
+        {
+            lpm_shim_stats st0 = lpm_shim_stats_g;
+            const double t0 = wall();
+            std::vector<LoadStep<NL>> load_cycle = solv.generateLoadCycle(lt, Nc, sp.fatigue_interval, pg);
+            dNdt = (tm == TimeMapMode::Linear) ? func_dNdt_linear(sp.fatigue_tau) : func_dNdt_exponental(sp.fatigue_tau, t++);
+            solv.solveProblemOneCycle(load_cycle, dNdt);
+            Nc += (int)dNdt;
+            lpm_shim_stats st1 = lpm_shim_stats_g;
+            log_line(log, idx, st0, st1, wall() - t0, 0,
+                     cblas_dnrm2((MKL_INT)solv.reaction_force.size(), solv.reaction_force.data(), 1));
+            std::fprintf(cyc, "%d %.17g\n", Nc, dNdt);
+            std::snprintf(tag, sizeof tag, "%03d", idx++);
+            write_state(ass, sp, tag, N);
+        } while (Nc < n_cycles);
+        std::fclose(cyc);
+    }
+    std::fclose(log);
+    return 0;
+}
+#endif
+
 int main(int argc, char **argv)
 {
     if (argc < 2)
@@ -422,6 +571,7 @@ int main(int argc, char **argv)
 
     ParticleType pt = (sp.ptype == "j2")               ? ParticleType::J2Plasticity
                       : (sp.ptype == "elastic_damage") ? ParticleType::ElasticDamage
+                      : (sp.ptype == "fatigue_hcf")    ? ParticleType::FatigueHCF
                                                        : ParticleType::Elastic;
     Assembly<NL> ass = make_assembly(xyz, box, cell, pt, sp);
     const int N = ass.nparticle;
@@ -466,6 +616,9 @@ int main(int argc, char **argv)
         else if (pt == ParticleType::ElasticDamage)
             dynamic_cast<ParticleElasticDamage<NL> *>(p)->setParticleProperty(
                 sp.nonlocal_L, sp.plane_stress != 0, sp.E, sp.mu, sp.k0, sp.k1, sp.ct_ratio, sp.d_thres);
+        else if (pt == ParticleType::FatigueHCF)
+            dynamic_cast<ParticleFatigueHCF<NL> *>(p)->setParticleProperty(
+                sp.nonlocal_L, sp.plane_stress != 0, sp.E, sp.mu, sp.hcf_A, sp.hcf_B, sp.hcf_d, sp.hcf_thres, sp.hcf_flr);
         else
             dynamic_cast<ParticleElastic<NL> *>(p)->setParticleProperty(sp.nonlocal_L, sp.plane_stress != 0, sp.E,
                                                                         sp.mu, sp.critical_bstrain);
@@ -572,6 +725,16 @@ int main(int argc, char **argv)
         write_bin(sp.out + "/pin_init.f64", pin0.data(), pin0.size());
     }
 
+#ifndef LPM_USE_GPU
+    if (!sp.fatigue_type.empty())
+        return run_fatigue(ass, groups, load, sp, N, dim, t_setup1 - t_setup0);
+#else
+    if (!sp.fatigue_type.empty())
+    {
+        std::fprintf(stderr, "the fatigue driver is not part of this build\n");
+        return 2;
+    }
+#endif
     FILE *log = std::fopen((sp.out + "/steps.txt").c_str(), "w");
     std::fprintf(log, "# N %d dim %d setup_s %.6f threads %d\n", N, dim, t_setup1 - t_setup0, omp_get_max_threads());
     std::fprintf(log, "# step newton_solves cg_iters wall_s spmv_s cg_s create_s cuts reaction_norm cg_fail\n");
@@ -652,39 +815,7 @@ int main(int argc, char **argv)
 
         char tag[32];
         std::snprintf(tag, sizeof tag, "%03d", s);
-        std::vector<double> x(3 * (size_t)N), pin(3 * (size_t)N), stress(6 * (size_t)N), dmg(N), dmgv(N), sv,
-            bdmg, dlp;
-        int nsv = (int)ass.pt_sys[0]->state_var.size();
-        sv.resize((size_t)nsv * N);
-        for (Particle<NL> *p : ass.pt_sys)
-        {
-            for (int k = 0; k < 3; ++k)
-            {
-                x[3 * p->id + k] = p->xyz[k];
-                pin[3 * p->id + k] = p->Pin[k];
-            }
-            for (int k = 0; k < 6; ++k)
-                stress[6 * p->id + k] = p->stress[k];
-            dmg[p->id] = p->damage;
-            dmgv[p->id] = p->damage_visual;
-            for (int k = 0; k < nsv; ++k)
-                sv[(size_t)nsv * p->id + k] = p->state_var[k];
-        }
-        for (Particle<NL> *p : ass.pt_sys)
-            for (int l = 0; l < NL; ++l)
-                for (Bond<NL> *b : p->bond_layers[l])
-                {
-                    bdmg.push_back(b->bdamage);
-                    dlp.push_back(b->dLp);
-                }
-        write_bin(sp.out + "/xyz_" + tag + ".f64", x.data(), x.size());
-        write_bin(sp.out + "/pin_" + tag + ".f64", pin.data(), pin.size());
-        write_bin(sp.out + "/stress_" + tag + ".f64", stress.data(), stress.size());
-        write_bin(sp.out + "/damage_" + tag + ".f64", dmg.data(), dmg.size());
-        write_bin(sp.out + "/damage_visual_" + tag + ".f64", dmgv.data(), dmgv.size());
-        write_bin(sp.out + "/state_var_" + tag + ".f64", sv.data(), sv.size());
-        write_bin(sp.out + "/bdamage_" + tag + ".f64", bdmg.data(), bdmg.size());
-        write_bin(sp.out + "/dlp_" + tag + ".f64", dlp.data(), dlp.size());
+        write_state(ass, sp, tag, N);
 
         bool dump = false;
         for (int d : sp.dumpK)

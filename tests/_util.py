@@ -19,11 +19,12 @@ LAT_NAME = {0: "sq2d", 1: "hex2d", 2: "sc3d", 3: "fcc3d", 4: "bcc3d"}
 
 def oracle_problem(case, cg_rtol=1e-12, cg_atol=1e-12, tol_iter=None, max_iter=None, tangent=False):
     m = case.material
-    mat = O.Material(ptype={2: "j2", 1: "elastic_damage"}.get(int(case.ptype), "elastic"),
+    mat = O.Material(ptype={2: "j2", 1: "elastic_damage", 3: "fatigue_hcf"}.get(int(case.ptype), "elastic"),
                      plane_stress=m.plane_stress, E=m.E, mu=m.mu,
                      critical_bstrain=m.critical_bstrain, sigmay=m.sigmay, xi=m.xi, H=m.H, A=m.A,
                      nonlocal_L=m.nonlocal_L, k0=m.k0, k1=m.k1, comp_tensile_ratio=m.comp_tensile_ratio,
-                     damage_threshold=m.damage_threshold)
+                     damage_threshold=m.damage_threshold, fatigue_A=m.fatigue_A, fatigue_B=m.fatigue_B,
+                     fatigue_d=m.fatigue_d, fatigue_limit_ratio=m.fatigue_limit_ratio)
     o = O.OracleProblem(LAT_NAME[int(case.lattice)], case.radius, case.xyz, mat, types=case.types,
                         undamaged_type=case.undamaged_type,
                         max_iter=case.max_iter if max_iter is None else max_iter,
@@ -74,3 +75,35 @@ def oracle_step_args(case, s):
 def rel(a, b):
     nb = np.linalg.norm(b)
     return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def oracle_load_args(step):
+    """A product-side LoadStep as the oracle's (disp, force) tuples."""
+    flag = {"x": 0, "y": 1, "z": 2}
+    return ([(np.asarray(b.group, np.int32), flag[b.flag], b.step) for b in step.dispBCs],
+            [(np.asarray(b.group, np.int32), b.fx, b.fy, b.fz) for b in step.forceBCs])
+
+
+def fatigue_cycles(case):
+    """The cycles of SolverFatigue::solveProblemCyclic (solver_fatigue.h:183-218) for a fatigue
+    case: yields (cycle count N after the cycle, dNdt, the cycle's LoadSteps)."""
+    fat = case.meta["fatigue"]
+    spec = fat["spectrum"]
+    groups = [case.groups[g] for g in fat["groups"]]
+    ltype = {"uniaxial_disp": LPM.FatigueLoadType.LoadUniaxialDisp,
+             "uniaxial_force": LPM.FatigueLoadType.LoadUniaxialForce,
+             "dogbone_disp": LPM.FatigueLoadType.LoadDogBoneDisp,
+             "ct_force": LPM.FatigueLoadType.LoadCTForce}[fat["load_type"]]
+    n_cycles = 0.5 * (len(spec) - 1)
+    t, N = 0.0, 0
+    while True:
+        steps = LPM.generateLoadCycle(ltype, spec, N, fat["n_interval"], groups)
+        if fat["tmode"] == "linear":
+            dNdt = LPM.func_dNdt_linear(fat["tau"])
+        else:
+            dNdt = LPM.func_dNdt_exponental(fat["tau"], t)
+            t += 1
+        N += int(dNdt)
+        yield N, dNdt, steps
+        if not N < n_cycles:
+            break

@@ -5,11 +5,13 @@
 Each case is a small problem from lpm-cpp_b200/configs.py.  The reference (LPM-CPP headers
 compiled unmodified against the oracle/shim MKL stand-in, run single-threaded so every sum has
 one order) generates the lattice itself, builds bonds and connections, assembles, and runs
-SolverStatic::solveProblem's step loop; its outputs are stored as compressed .npz:
+SolverStatic::solveProblem's step loop (fatigue cases: SolverFatigue::solveProblemStatic for the
+load steps, then the cycles of solveProblemCyclic); its outputs are stored as compressed .npz:
   xyz0, nb0, nb1, bond_p2, nconn, nlq, conns          topology
   K_pointer, IK, JK, K                                the reference CSR after load step 0 (dump_k)
-  xyz_<s>, pin_<s>, state_var_<s>, bdamage_<s>        state after each load step
+  xyz_<s>, pin_<s>, state_var_<s>, bdamage_<s>        state after each load step (or cycle)
   steps                                               [newton_solves, cg_iters, cuts, reaction_norm]
+  cycles                                              fatigue: [N, dNdt] after each cycle
 """
 from __future__ import annotations
 
@@ -85,6 +87,8 @@ def cases():
         # ParticleElasticDamage with the nonlocal damage rate (searchNonlocalNeighbors + the
         # averaging of SolverStatic::updateStaticDamage): damage grows in every step
         "hex_edamage": (lambda: CFG.edamage_plate(), {"cg_tol": (1e-24, 0.0), "dump_k": (1,)}),
+        # SolverFatigue: one static step, then four cycles (two steps up, two down) of HCF damage
+        "hex_fatigue": (lambda: CFG.fatigue_plate(), {"cg_tol": (1e-24, 0.0), "fatigue": True}),
     }
 
 
@@ -114,12 +118,19 @@ def make(name, build, opts):
             out[f"pin_{s}"] = rb(f"pin_{tag}.f64", np.float64).reshape(-1, 3)
             if int(case.ptype) == 2:
                 out[f"state_var_{s}"] = rb(f"state_var_{tag}.f64", np.float64).reshape(-1, 7)
+            if int(case.ptype) == 3:
+                out[f"state_var_{s}"] = rb(f"state_var_{tag}.f64", np.float64).reshape(-1, 3)
+                out[f"damage_{s}"] = rb(f"damage_{tag}.f64", np.float64)
+                out[f"bdamage_{s}"] = rb(f"bdamage_{tag}.f64", np.float64)
             if int(case.ptype) == 1:
                 out[f"state_var_{s}"] = rb(f"state_var_{tag}.f64", np.float64).reshape(-1, 1)
                 out[f"damage_{s}"] = rb(f"damage_{tag}.f64", np.float64)
                 out[f"bdamage_{s}"] = rb(f"bdamage_{tag}.f64", np.float64)
             if case.material.critical_bstrain < 1.0 or case.bond_props is not None:
                 out[f"bdamage_{s}"] = rb(f"bdamage_{tag}.f64", np.float64)
+        if opts.get("fatigue"):
+            # cycle count N and dNdt after each cycle of SolverFatigue::solveProblemCyclic
+            out["cycles"] = np.loadtxt(os.path.join(d, "cycles.txt"), ndmin=2)
         out["meta"] = np.array(json.dumps({"name": name,
                                            "opts": {k: (list(v) if isinstance(v, tuple) else v) for k, v in opts.items()},
                                            "n": int(case.n), "spec": spec}))

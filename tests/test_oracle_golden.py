@@ -13,7 +13,7 @@ import os
 import numpy as np
 import pytest
 
-from _util import O, oracle_problem, oracle_step_args, rel
+from _util import O, fatigue_cycles, oracle_load_args, oracle_problem, oracle_step_args, rel
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden")
@@ -27,6 +27,9 @@ def _load_builders():
 
 CASES = _load_builders()
 NAMES = sorted(CASES)
+# cases run by SolverStatic; the fatigue cases run SolverFatigue's static steps and cycles
+STATIC = [n for n in NAMES if not CASES[n][1].get("fatigue")]
+FATIGUE = [n for n in NAMES if CASES[n][1].get("fatigue")]
 
 
 def fixture(name):
@@ -54,7 +57,7 @@ def test_oracle_topology_bit_exact(name):
         assert np.array_equal(v, g[k]), k
 
 
-@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("name", STATIC)
 def test_oracle_load_steps(name):
     build, opts = CASES[name]
     case = build()
@@ -100,6 +103,45 @@ def test_oracle_load_steps(name):
                 assert np.abs(so["bdamage"] - g[f"bdamage_{s}"]).max() <= 1e-10
             else:
                 assert np.array_equal(so["bdamage"], g[f"bdamage_{s}"])
+
+
+@pytest.mark.parametrize("name", FATIGUE)
+def test_oracle_fatigue_cycles(name):
+    """SolverFatigue (solver_fatigue.h): the static step of solveProblemStatic, then each cycle of
+    solveProblemCyclic (generateLoadCycle, the dN/dt map, solveProblemOneCycle).  Per cycle: the
+    same Newton solve count, the cycle count N, damage and the HCF state variables within 1e-12
+    (bit-exact here; the nonlocal weights are pow() sums), the reaction history's norm within
+    1e-12 relative.  Displacements are compared in absolute terms against the load amplitude:
+    at a cycle's end the plate is unloaded and u is a residual of the CG's rounding."""
+    build, opts = CASES[name]
+    case = build()
+    g = fixture(name)
+    o = oracle_problem(case, cg_rtol=opts["cg_tol"][0], cg_atol=opts["cg_tol"][1])
+    o.update_geometry()
+    o.update_force_state()
+    amp = max(abs(v) for v in case.meta["fatigue"]["spectrum"])
+    steps = g["steps"]
+    results = []
+    for s in range(len(case.steps)):
+        ok, st = o.fatigue_static_step(*oracle_step_args(case, s))
+        assert ok
+        results.append(st)
+    cyc = list(fatigue_cycles(case))
+    assert len(case.steps) + len(cyc) == len(steps)
+    for c, (N, dNdt, cycle) in enumerate(cyc):
+        assert [N, dNdt] == list(g["cycles"][c])
+        _, st = o.fatigue_cycle([oracle_load_args(x) for x in cycle], dNdt)
+        results.append(st)
+        s = len(case.steps) + c
+        so = o.state()
+        assert st["newton_solves"] == int(steps[s][0]), s
+        assert np.abs(so["damage"] - g[f"damage_{s}"]).max() <= 1e-12, s
+        assert np.abs(so["state_var"] - g[f"state_var_{s}"]).max() <= 1e-12 * np.abs(g[f"state_var_{s}"][:, 0]).max()
+        assert np.abs(so["bdamage"] - g[f"bdamage_{s}"]).max() <= 1e-12, s
+        du = np.abs((so["xyz"] - case.xyz) - (g[f"xyz_{s}"] - g["xyz0"])).max()
+        assert du <= 1e-8 * amp, (s, du)
+        assert abs(st["reaction_norm"] - steps[s][3]) <= 1e-12 * steps[s][3]
+    assert g[f"damage_{len(steps) - 1}"].max() > 0.5, "damage must grow over the cycles"
 
 
 def test_oracle_forces_bit_exact():
