@@ -42,7 +42,7 @@ typedef enum
 /* LatticeType (include/lpm.h:97-106); BCC3D covers the three BCC enum values */
 enum { LPMGPU_SQUARE2D = 0, LPMGPU_HEXAGON2D = 1, LPMGPU_SC3D = 2, LPMGPU_FCC3D = 3, LPMGPU_BCC3D = 4 };
 /* ParticleType (include/lpm.h:89-95) values on this path */
-enum { LPMGPU_ELASTIC = 0, LPMGPU_ELASTIC_DAMAGE = 1, LPMGPU_J2 = 2 };
+enum { LPMGPU_ELASTIC = 0, LPMGPU_ELASTIC_DAMAGE = 1, LPMGPU_J2 = 2, LPMGPU_FATIGUE_HCF = 3 };
 /* linear-solve precision */
 enum { LPMGPU_FP64 = 0, LPMGPU_MIXED = 1 };
 
@@ -52,7 +52,7 @@ typedef struct lpmgpu_solver lpmgpu_solver;
 typedef struct
 {
     int32_t lattice;         /* LPMGPU_SQUARE2D .. LPMGPU_BCC3D */
-    int32_t ptype;           /* LPMGPU_ELASTIC, LPMGPU_ELASTIC_DAMAGE or LPMGPU_J2 */
+    int32_t ptype;           /* LPMGPU_ELASTIC, LPMGPU_ELASTIC_DAMAGE, LPMGPU_J2 or LPMGPU_FATIGUE_HCF */
     int32_t n;               /* particles */
     const double *xyz;       /* host, n*3; row q is particle id q (generation order) */
     const int32_t *type;     /* host, n particle types, or NULL for all 0 */
@@ -92,6 +92,18 @@ typedef struct
      * particle_elastic_damage.h:183-220): damage surface k0 + k1 D on the strain energy density,
      * the compression/tension ratio of its equivalent strain, and the damage threshold */
     double k0, k1, comp_tensile_ratio, damage_threshold;
+    /* LPMGPU_FATIGUE_HCF (ParticleFatigueHCF::setParticleProperty, particle_fatigue_hcf.h:163-205):
+     * the damage rate fatigue_A * pow(largest energy, fatigue_B) * pow(energy range of the cycle,
+     * fatigue_d); damage_threshold above is its damage threshold.  fatigue_limit_ratio is kept for
+     * the interface but, as in the reference, does not enter the result (calcEqEnergy returns the
+     * total energy, particle_fatigue_hcf.h:123). */
+    double fatigue_A, fatigue_B, fatigue_d, fatigue_limit_ratio;
+    /* Optional nonlocal neighbour lists in place of the search (NULL = none given): particle i's
+     * list is nonlocal_count[i] ids, the lists concatenated in nonlocal_ids, each in the order of
+     * Particle::neighbors_nonlocal (particle.h:37), which the averaging sums in.  An Assembly on
+     * which searchNonlocalNeighbors ran (assembly.h:118-130) holds them.  Not together with
+     * nonlocal_cutoff_ratio > 0. */
+    const int32_t *nonlocal_count, *nonlocal_ids;
 } lpmgpu_desc;
 
 /* Displacement / force boundary condition of one load step (boundary.h:10-44, Relative mode). */
@@ -167,7 +179,8 @@ int32_t lpmgpu_get_topology(const lpmgpu_solver *h, int32_t *nb0, int32_t *nb1, 
 
 /* Assembly::updateGeometry + updateForceState (assembly.h:133-138, 179-191) */
 int32_t lpmgpu_update_force_state(lpmgpu_solver *h);
-/* Assembly::updateStateVar (assembly.h:162-166): the J2 return map */
+/* Assembly::updateStateVar (assembly.h:162-166): the J2 return map, the elastic-damage or the
+ * fatigue particles' energy update */
 int32_t lpmgpu_update_state_var(lpmgpu_solver *h);
 /* Solver::updateRR (solver.h:112-126); *norm gets ||residual|| */
 int32_t lpmgpu_update_rr(lpmgpu_solver *h, double *norm);
@@ -188,8 +201,31 @@ int32_t lpmgpu_solve_load_step(lpmgpu_solver *h, const lpmgpu_load_step *step, l
 int32_t lpmgpu_store_state(lpmgpu_solver *h);
 int32_t lpmgpu_reset_state(lpmgpu_solver *h);
 
+/* SolverFatigue (include/solver_fatigue.h) on the device.  The cycle loop itself
+ * (solveProblemCyclic: readLoad, generateLoadCycle, the dN/dt time map) is host logic and stays
+ * with the caller; these are the device steps it calls.
+ * lpmgpu_fatigue_solve_step: SolverFatigue::solveProblemStep (solver_fatigue.h:278-302), the BCs,
+ *   K from the current state, Newton, no damage loop; LPMGPU_ERR_NEWTON when Newton failed.
+ * lpmgpu_fatigue_static_step: one load step of SolverFatigue::solveProblemStatic
+ *   (solver_fatigue.h:244-275): the fatigue step with halve-and-retry, and updateStateVar +
+ *   storeStateVar after every converged (sub)step.
+ * lpmgpu_fatigue_update_damage: SolverFatigue::updateFatigueDamage (solver_fatigue.h:76-126): the
+ *   nonlocal average of the local rates, then each damageable particle's damage += rate * dNdt
+ *   (ParticleFatigueHCF::updateParticleFatigueDamage, particle_fatigue_hcf.h:148-160);
+ *   *any_damaged (may be NULL) gets its return value.
+ * lpmgpu_fatigue_cycle: SolverFatigue::solveProblemOneCycle (solver_fatigue.h:221-241): each step
+ *   (fatigue step + updateStateVar; a step whose Newton failed is carried on from, as in the
+ *   reference, and counted in stats->cuts), then updateFatigueDamage(dNdt), storeStateVar,
+ *   updateGeometry, updateForceState. */
+int32_t lpmgpu_fatigue_solve_step(lpmgpu_solver *h, const lpmgpu_load_step *step, lpmgpu_stats *stats);
+int32_t lpmgpu_fatigue_static_step(lpmgpu_solver *h, const lpmgpu_load_step *step, lpmgpu_stats *stats);
+int32_t lpmgpu_fatigue_update_damage(lpmgpu_solver *h, double dNdt, int32_t *any_damaged);
+int32_t lpmgpu_fatigue_cycle(lpmgpu_solver *h, const lpmgpu_load_step *steps, int32_t nsteps, double dNdt,
+                             lpmgpu_stats *stats, int32_t *any_damaged);
+
 /* Device state back to host (any pointer may be NULL): xyz n*3, Pin n*3, stress n*6 (s11 s22
- * s33 s23 s13 s12), damage n, damage_visual n, state_var n*nsv (nsv = 7 for J2, else 1),
+ * s33 s23 s13 s12), damage n, damage_visual n, state_var n*nsv (nsv = 7 for J2, 3 for fatigue
+ * HCF, else 1),
  * bdamage nbonds, residual dim*n. */
 int32_t lpmgpu_read_state(const lpmgpu_solver *h, double *xyz, double *pin, double *stress, double *damage,
                           double *damage_visual, double *state_var, double *bdamage);

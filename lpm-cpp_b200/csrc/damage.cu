@@ -3,6 +3,10 @@
 //   SolverStatic::updateStaticDamage (nonlocal rate)   include/solver_static.h:32-52, func_phi lpm.h:49-53
 //   ParticleElasticDamage::updateParticleStateVariables include/particle_elastic_damage.h:159-170
 //     with calcStrainEnergyDensity                     include/particle_elastic_damage.h:93-108
+//   ParticleFatigueHCF::updateParticleStateVariables    include/particle_fatigue_hcf.h:128-145
+//     with calcEqEnergy                                include/particle_fatigue_hcf.h:83-125
+//   SolverFatigue::updateFatigueDamage                 include/solver_fatigue.h:76-126
+//     with updateParticleFatigueDamage                 include/particle_fatigue_hcf.h:148-160
 // The search keeps the reference's neighbour order (ascending id, the order of its inner loop),
 // so the weighted sums of the averaging add in the reference's order.
 #include <cub/cub.cuh>
@@ -83,6 +87,30 @@ cudaError_t build_nonlocal(Problem &p, double cutoff_ratio)
     return cudaGetLastError();
 }
 
+// The caller's nonlocal lists (Particle::neighbors_nonlocal of an Assembly on which
+// searchNonlocalNeighbors ran), already checked on the host: counts >= 0, ids in [0, n).
+cudaError_t build_nonlocal_lists(Problem &p, const int32_t *count, const int32_t *ids)
+{
+    const int n = p.n;
+    std::vector<int> start((size_t)n + 1, 0);
+    for (int i = 0; i < n; ++i)
+        start[i + 1] = start[i] + count[i];
+    const int total = start[n];
+    cudaError_t e = dalloc(p, &p.nlstart, (size_t)n + 1);
+    if (e == cudaSuccess)
+        e = dalloc(p, &p.nlist, (size_t)total);
+    if (e == cudaSuccess)
+        e = dalloc(p, &p.ddot_nonlocal, (size_t)n);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(p.nlstart, start.data(), sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice, p.stream);
+    if (e == cudaSuccess && total > 0)
+        e = cudaMemcpyAsync(p.nlist, ids, sizeof(int) * (size_t)total, cudaMemcpyHostToDevice, p.stream);
+    p.nnl = total;
+    // the host offsets must outlive the copies
+    const cudaError_t s = cudaStreamSynchronize(p.stream);
+    return e != cudaSuccess ? e : s;
+}
+
 // SolverStatic::updateStaticDamage, first loop (solver_static.h:35-52): the nonlocal damage rate
 // of each damageable particle, the func_phi- and volume-weighted mean of its nonlocal neighbours'
 // local rates, at the current positions
@@ -159,6 +187,123 @@ cudaError_t launch_edamage_update(Problem &p)
     k_edamage_update<<<div_up(p.n, 128), 128, 0, p.stream>>>(p.n, p.cell.pvol, p.cell.nneighbors, p.desc.k0, p.desc.k1,
                                                              p.bstart, p.nb0, p.nb, p.Kn, p.dLe, p.dLe_total,
                                                              p.TdLe_total, p.damage, p.sv_last, p.sv, p.ddot_local);
+    p.ctr.kernel_launches++;
+    return cudaGetLastError();
+}
+
+// The strain energy density of particle i: each bond's spring energy, then the layer's
+// volumetric term, per modified volume, layer by layer in bond order.  It is
+// calcStrainEnergyDensity (particle_elastic_damage.h:93-108) and the energy_total that
+// calcEqEnergy returns (particle_fatigue_hcf.h:98-123).
+__device__ __forceinline__ double energy_density(int i, double pvol, int nneighbors, const int *__restrict__ bstart,
+                                                 const int *__restrict__ nb0, const int *__restrict__ nb,
+                                                 const double *__restrict__ Kn, const double *__restrict__ dLe,
+                                                 const double *__restrict__ dLe_total,
+                                                 const double *__restrict__ TdLe_total)
+{
+    const double V_m = pvol * nb[i] / nneighbors;
+    const int b0 = bstart[i], b1 = b0 + nb0[i], be = bstart[i + 1];
+    double energy = 0;
+    for (int L = 0; L < 2; ++L)
+    {
+        const int lo = L == 0 ? b0 : b1, hi = L == 0 ? b1 : be;
+        for (int b = lo; b < hi; ++b)
+            energy += 0.5 * (Kn[b] * dLe[b] * dLe[b]) / V_m;
+        energy += 0.5 * TdLe_total[2 * i + L] * dLe_total[2 * i + L] / V_m;
+    }
+    return energy;
+}
+
+// ParticleFatigueHCF state variables: [0] the largest energy so far, [1] / [2] the smallest /
+// largest energy of the current cycle.  Initial value {0, INT_MAX, 0} (particle_fatigue_hcf.h:27-28).
+constexpr double kHcfMinStart = 2147483647.0;
+
+__global__ void k_hcf_init(int n, double *__restrict__ sv, double *__restrict__ sv_last)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    sv[3 * (int64_t)i] = sv_last[3 * (int64_t)i] = 0;
+    sv[3 * (int64_t)i + 1] = sv_last[3 * (int64_t)i + 1] = kHcfMinStart;
+    sv[3 * (int64_t)i + 2] = sv_last[3 * (int64_t)i + 2] = 0;
+}
+
+cudaError_t launch_hcf_init(Problem &p)
+{
+    k_hcf_init<<<div_up(p.n, 128), 128, 0, p.stream>>>(p.n, p.sv, p.sv_last);
+    p.ctr.kernel_launches++;
+    return cudaGetLastError();
+}
+
+// ParticleFatigueHCF::updateParticleStateVariables: the cycle's smallest and largest energy,
+// the largest so far, and the local damage rate A pow(largest so far, B) pow(range, d) when the
+// cycle's energy range is positive.  std::min(a, b) is (b < a) ? b : a, std::max(a, b) is
+// (a < b) ? b : a.
+__global__ void k_hcf_update(int n, double pvol, int nneighbors, double fA, double fB, double fd,
+                             const int *__restrict__ bstart, const int *__restrict__ nb0, const int *__restrict__ nb,
+                             const double *__restrict__ Kn, const double *__restrict__ dLe,
+                             const double *__restrict__ dLe_total, const double *__restrict__ TdLe_total,
+                             double *__restrict__ sv, double *__restrict__ ddot_local)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const double e = energy_density(i, pvol, nneighbors, bstart, nb0, nb, Kn, dLe, dLe_total, TdLe_total);
+    double *s = sv + 3 * (int64_t)i;
+    const double s1 = (s[1] < e) ? s[1] : e;
+    const double s2 = (e < s[2]) ? s[2] : e;
+    const double s0 = (s2 < s[0]) ? s[0] : s2;
+    s[0] = s0;
+    s[1] = s1;
+    s[2] = s2;
+    ddot_local[i] = (s2 - s1 > 0) ? fA * pow(s0, fB) * pow(s2 - s1, fd) : 0;
+}
+
+cudaError_t launch_hcf_update(Problem &p)
+{
+    k_hcf_update<<<div_up(p.n, 128), 128, 0, p.stream>>>(p.n, p.cell.pvol, p.cell.nneighbors, p.desc.fatigue_A,
+                                                         p.desc.fatigue_B, p.desc.fatigue_d, p.bstart, p.nb0, p.nb,
+                                                         p.Kn, p.dLe, p.dLe_total, p.TdLe_total, p.sv, p.ddot_local);
+    p.ctr.kernel_launches++;
+    return cudaGetLastError();
+}
+
+// SolverFatigue::updateFatigueDamage, second loop, with
+// ParticleFatigueHCF::updateParticleFatigueDamage: damage += nonlocal rate x dNdt, set to 1 at
+// the threshold, the cycle's energy extremes cleared, and the flag raised when the damage moved
+// by more than 1e-3 since the last stored state.  Without a nonlocal search the rate is 0/0, as
+// in the reference.  Other particle types keep the base class's no-op.
+__global__ void k_fatigue_damage(int n, int hcf, int undamaged, double threshold, double dNdt,
+                                 const int *__restrict__ type, const double *__restrict__ ddot_nl,
+                                 double *__restrict__ damage, const double *__restrict__ damage_last,
+                                 double *__restrict__ sv, Scalars *scal)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || type[i] == undamaged || !hcf)
+        return;
+    volatile double zero = 0.0;
+    const double rate = ddot_nl ? ddot_nl[i] : zero / zero;
+    double d = damage[i] + rate * dNdt;
+    if (d >= threshold)
+        d = 1;
+    damage[i] = d;
+    sv[3 * (int64_t)i + 1] = kHcfMinStart;
+    sv[3 * (int64_t)i + 2] = 0;
+    if (fabs(d - damage_last[i]) > 1e-3)
+        atomicExch(&scal->any_flag, 1);
+}
+
+cudaError_t launch_fatigue_damage(Problem &p, double dNdt)
+{
+    cudaError_t e = cudaMemsetAsync(&p.scal->any_flag, 0, sizeof(int), p.stream);
+    if (e != cudaSuccess)
+        return e;
+    if ((e = launch_nonlocal_average(p)) != cudaSuccess)
+        return e;
+    k_fatigue_damage<<<div_up(p.n, 128), 128, 0, p.stream>>>(p.n, p.desc.ptype == LPMGPU_FATIGUE_HCF ? 1 : 0,
+                                                             p.desc.undamaged_type, p.desc.damage_threshold, dNdt,
+                                                             p.type, p.ddot_nonlocal, p.damage, p.damage_last, p.sv,
+                                                             p.scal);
     p.ctr.kernel_launches++;
     return cudaGetLastError();
 }

@@ -136,8 +136,14 @@ cudaError_t launch_static_damage(Problem &p);   // sets p.scal->any_flag
 // nonlocal damage (damage.cu): the neighbour search at creation, the averaged damage rate,
 // and ParticleElasticDamage's state update
 cudaError_t build_nonlocal(Problem &p, double cutoff_ratio);
+cudaError_t build_nonlocal_lists(Problem &p, const int32_t *count, const int32_t *ids);
 cudaError_t launch_nonlocal_average(Problem &p);
 cudaError_t launch_edamage_update(Problem &p);
+// fatigue (damage.cu): ParticleFatigueHCF's initial state variables and state update, and
+// SolverFatigue::updateFatigueDamage (sets p.scal->any_flag)
+cudaError_t launch_hcf_init(Problem &p);
+cudaError_t launch_hcf_update(Problem &p);
+cudaError_t launch_fatigue_damage(Problem &p, double dNdt);
 cudaError_t launch_add_disp(Problem &p);        // xyz += x (solveLinearSystem position update)
 cudaError_t launch_export_ref(const Problem &p, int64_t *IK, int64_t *JK, double *K); // device outputs
 cudaError_t launch_apply_bc(Problem &p, const lpmgpu_load_step &s);

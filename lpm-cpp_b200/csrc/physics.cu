@@ -79,7 +79,7 @@ __global__ void k_geometry_force(PhysArgs a)
         const int L = b < b1 ? 0 : 1;
         double f = 2. * a.Kn[b] * a.dLe[b] + 2. * a.Tv[b] * dlt[L];
         double D = a.bdamage[b];
-        if (a.ptype == LPMGPU_J2 || a.ptype == LPMGPU_ELASTIC_DAMAGE)
+        if (a.ptype == LPMGPU_J2 || a.ptype == LPMGPU_ELASTIC_DAMAGE || a.ptype == LPMGPU_FATIGUE_HCF)
         {
             D = std_max(D, std_max(di, a.damage[a.bp2[b]]));
             a.bdamage[b] = D;
@@ -325,6 +325,8 @@ cudaError_t launch_update_state_var(Problem &p)
 {
     if (p.desc.ptype == LPMGPU_ELASTIC_DAMAGE)
         return launch_edamage_update(p);
+    if (p.desc.ptype == LPMGPU_FATIGUE_HCF)
+        return launch_hcf_update(p);
     if (p.desc.ptype != LPMGPU_J2)
         return cudaSuccess;
     k_j2_update<<<div_up(p.n, 128), 128, 0, p.stream>>>(p.n, p.desc.E, p.desc.mu, p.desc.sigmay, p.desc.xi, p.desc.H,
@@ -377,6 +379,10 @@ cudaError_t launch_static_damage(Problem &p)
     cudaError_t e = cudaMemsetAsync(&p.scal->any_flag, 0, sizeof(int), p.stream);
     if (e != cudaSuccess)
         return e;
+    // fatigue particles keep Particle::updateParticleStaticDamage, which changes nothing
+    // (particle.h:63): their damage moves only in SolverFatigue::updateFatigueDamage
+    if (p.desc.ptype == LPMGPU_FATIGUE_HCF)
+        return cudaSuccess;
     if (p.desc.ptype != LPMGPU_ELASTIC && (e = launch_nonlocal_average(p)) != cudaSuccess)
         return e;
     // damage_threshold is never assigned for J2 (particle_j2plasticity.h:22): 0

@@ -65,7 +65,7 @@ struct Request
     int32_t status = LPMGPU_OK;
     lpmgpu_desc desc{};
     std::vector<double> xyz, kn, tv, bdmg;
-    std::vector<int32_t> type, nb0, nb1, p2;
+    std::vector<int32_t> type, nb0, nb1, p2, nl_count, nl_ids;
     std::vector<OwnedStep> steps;
     int64_t est_bytes = 0, bytes = 0;
     lpmgpu_solver *h = nullptr;
@@ -102,7 +102,15 @@ int64_t estimate_bytes(const lpmgpu_desc &d)
                                     : 4.0 / 3.0 * pi * R * R * R / (4 * std::sqrt(2.0) * r * r * r);
         per_particle += 4 * (int64_t)(1.2 * m + 8) + 12;
     }
-    return (int64_t)d.n * per_particle + (8 << 20);
+    int64_t lists = 0;
+    if (d.nonlocal_count && d.nonlocal_ids)
+    {
+        // the caller's nonlocal lists, counted exactly: 4 bytes an entry, an offset and a rate
+        for (int i = 0; i < d.n; ++i)
+            lists += 4 * (int64_t)std::max(0, d.nonlocal_count[i]);
+        per_particle += 12;
+    }
+    return (int64_t)d.n * per_particle + lists + (8 << 20);
 }
 
 } // namespace
@@ -436,6 +444,16 @@ int32_t lpmgpu_server_submit(lpmgpu_server *s, const lpmgpu_desc *d, const lpmgp
             r->bdmg.assign(d->bond_damage, d->bond_damage + nb);
             r->desc.bond_damage = r->bdmg.data();
         }
+    }
+    if (d->nonlocal_count && d->nonlocal_ids)
+    {
+        r->nl_count.assign(d->nonlocal_count, d->nonlocal_count + n);
+        size_t nl = 0;
+        for (size_t i = 0; i < n; ++i)
+            nl += (size_t)std::max(0, d->nonlocal_count[i]);
+        r->nl_ids.assign(d->nonlocal_ids, d->nonlocal_ids + nl);
+        r->desc.nonlocal_count = r->nl_count.data();
+        r->desc.nonlocal_ids = r->nl_ids.data();
     }
     for (int32_t k = 0; k < nsteps; ++k)
         r->steps.emplace_back(steps[k]);

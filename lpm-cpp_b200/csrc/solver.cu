@@ -260,6 +260,63 @@ static int32_t scaled_step(Problem &p, const lpmgpu_load_step &s, double scale, 
     return scaled_step(p, s, scale / 2.0, st, depth + 1);
 }
 
+// SolverFatigue::solveProblemStep (solver_fatigue.h:278-302): BCs, K from the current state, Newton
+static int32_t fatigue_step(Problem &p, const lpmgpu_load_step &s, lpmgpu_stats *st)
+{
+    CK(launch_apply_bc(p, s));
+    if (!p.desc.tangent)
+        ST(assemble(p, true));
+    int n_newton = 0;
+    ST(newton(p, st, &n_newton));
+    if (st)
+        st->reaction_norm = std::sqrt(p.scal_host->reaction_sq);
+    return n_newton < p.desc.max_iter ? LPMGPU_OK : LPMGPU_ERR_NEWTON;
+}
+
+// one load step of SolverFatigue::solveProblemStatic (solver_fatigue.h:244-275): on failure reset
+// to the last stored state, halve, run both halves; each converged (sub)step is followed by
+// updateStateVar and storeStateVar
+static int32_t fatigue_static_rec(Problem &p, const lpmgpu_load_step &s, double scale, lpmgpu_stats *st, int depth)
+{
+    std::vector<lpmgpu_dispbc> db(s.disp, s.disp + s.ndisp);
+    std::vector<lpmgpu_forcebc> fb(s.force, s.force + s.nforce);
+    for (auto &d : db)
+        d.step *= scale;
+    for (auto &f : fb)
+    {
+        f.fx *= scale;
+        f.fy *= scale;
+        f.fz *= scale;
+    }
+    lpmgpu_load_step sc{db.data(), s.ndisp, fb.data(), s.nforce};
+    int32_t r = fatigue_step(p, sc, st);
+    if (r == LPMGPU_OK)
+    {
+        CK(launch_update_state_var(p));
+        ST(store_state(p));
+        return LPMGPU_OK;
+    }
+    if (r != LPMGPU_ERR_NEWTON)
+        return r;
+    if (depth >= 30)
+        return LPMGPU_ERR_CUTS;
+    ST(reset_state(p));
+    if (st)
+        st->cuts++;
+    ST(fatigue_static_rec(p, s, scale / 2.0, st, depth + 1));
+    return fatigue_static_rec(p, s, scale / 2.0, st, depth + 1);
+}
+
+// SolverFatigue::updateFatigueDamage (solver_fatigue.h:76-126)
+static int32_t fatigue_damage(Problem &p, double dNdt, int32_t *any)
+{
+    CK(launch_fatigue_damage(p, dNdt));
+    ST(sync_scalars(p));
+    if (any)
+        *any = p.scal_host->any_flag != 0;
+    return LPMGPU_OK;
+}
+
 // ---- lattice generators (include/utilities.h:93-310), host side
 static void rmatrix(int f, const double a[3], double R[9])
 {
@@ -479,7 +536,8 @@ static void free_problem(Problem &p)
 int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
 {
     if (!d || !out || !d->xyz || d->n <= 0 || d->lattice < 0 || d->lattice > LPMGPU_BCC3D ||
-        (d->ptype != LPMGPU_ELASTIC && d->ptype != LPMGPU_ELASTIC_DAMAGE && d->ptype != LPMGPU_J2) ||
+        (d->ptype != LPMGPU_ELASTIC && d->ptype != LPMGPU_ELASTIC_DAMAGE && d->ptype != LPMGPU_J2 &&
+         d->ptype != LPMGPU_FATIGUE_HCF) ||
         !(d->radius > 0) || d->max_iter < 0 || d->nonlocal_cutoff_ratio < 0)
         return LPMGPU_ERR_INVALID_ARG;
     *out = nullptr;
@@ -522,7 +580,7 @@ int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
     p.cell = make_cell(d->lattice, d->radius);
     p.n = d->n;
     p.dim = p.cell.dim;
-    p.nsv = (d->ptype == LPMGPU_J2) ? 7 : 1;
+    p.nsv = (d->ptype == LPMGPU_J2) ? 7 : (d->ptype == LPMGPU_FATIGUE_HCF) ? 3 : 1;
     kntv(p.cell, d->plane_stress, d->E, d->mu, p.kntv);
     const size_t n = p.n;
     CKF(cudaMallocHost(&p.scal_host, sizeof(Scalars)));
@@ -542,6 +600,8 @@ int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
     CKF(dalloc(p, &p.ddot_local, n));
     CKF(dalloc(p, &p.sv, p.nsv * n));
     CKF(dalloc(p, &p.sv_last, p.nsv * n));
+    if (d->ptype == LPMGPU_FATIGUE_HCF)
+        CKF(launch_hcf_init(p));
     CKF(dalloc(p, &p.cons, 3 * n));
     CKF(dalloc(p, &p.type, n));
     CKF(dalloc(p, &p.dLe_total, 2 * n));
@@ -558,16 +618,43 @@ int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
         set_last_error("per-bond arrays need the bond lists they refer to (bond_nb0/bond_nb1/bond_p2)");
         return fail(LPMGPU_ERR_INVALID_ARG);
     }
+    if ((d->nonlocal_count != nullptr) != (d->nonlocal_ids != nullptr) ||
+        (d->nonlocal_count && d->nonlocal_cutoff_ratio > 0))
+    {
+        set_last_error("nonlocal lists need both nonlocal_count and nonlocal_ids, and no nonlocal_cutoff_ratio");
+        return fail(LPMGPU_ERR_INVALID_ARG);
+    }
+    if (d->nonlocal_count)
+    {
+        int64_t total = 0;
+        for (int i = 0; i < d->n; ++i)
+        {
+            if (d->nonlocal_count[i] < 0)
+                return fail(LPMGPU_ERR_INVALID_ARG);
+            total += d->nonlocal_count[i];
+        }
+        if (total >= ((int64_t)1 << 31))
+        {
+            set_last_error("more than 2^31 - 1 nonlocal neighbour pairs");
+            return fail(LPMGPU_ERR_INVALID_ARG);
+        }
+        for (int64_t q = 0; q < total; ++q)
+            if (d->nonlocal_ids[q] < 0 || d->nonlocal_ids[q] >= d->n)
+                return fail(LPMGPU_ERR_INVALID_ARG);
+    }
     int topo_err = 0;
     CKF(build_topology(p, d->xyz, &topo_err));
     if (d->nonlocal_cutoff_ratio > 0)
         CKF(build_nonlocal(p, d->nonlocal_cutoff_ratio));
+    else if (d->nonlocal_count)
+        CKF(build_nonlocal_lists(p, d->nonlocal_count, d->nonlocal_ids));
     CKF(cudaStreamSynchronize(p.stream));
     // the host pointers of the description are only read during creation
     p.desc.xyz = nullptr;
     p.desc.type = nullptr;
     p.desc.bond_nb0 = p.desc.bond_nb1 = p.desc.bond_p2 = nullptr;
     p.desc.bond_kn = p.desc.bond_tv = p.desc.bond_damage = nullptr;
+    p.desc.nonlocal_count = p.desc.nonlocal_ids = nullptr;
     if (topo_err)
     {
         set_last_error("a particle has no bonds, or more bonds / connections than supported");
@@ -815,6 +902,86 @@ int32_t lpmgpu_solve_load_step(lpmgpu_solver *h, const lpmgpu_load_step *s, lpmg
     S->converged = (r == LPMGPU_OK);
     S->reaction_norm = std::sqrt(p.scal_host->reaction_sq);
     return r;
+}
+
+static int32_t begin_call(lpmgpu_solver *h, lpmgpu_stats *st)
+{
+    if (st)
+        *st = lpmgpu_stats{};
+    for (double &t : h->p.phase_s)
+        t = 0;
+    CK(cudaSetDevice(h->p.device));
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_fatigue_solve_step(lpmgpu_solver *h, const lpmgpu_load_step *s, lpmgpu_stats *st)
+{
+    if (!h || !s)
+        return LPMGPU_ERR_INVALID_ARG;
+    ST(check_step(h->p, s));
+    ST(begin_call(h, st));
+    const int32_t r = fatigue_step(h->p, *s, st);
+    if (st)
+        st->converged = r == LPMGPU_OK;
+    return r;
+}
+
+int32_t lpmgpu_fatigue_static_step(lpmgpu_solver *h, const lpmgpu_load_step *s, lpmgpu_stats *st)
+{
+    if (!h || !s)
+        return LPMGPU_ERR_INVALID_ARG;
+    ST(check_step(h->p, s));
+    ST(begin_call(h, st));
+    const int32_t r = fatigue_static_rec(h->p, *s, 1.0, st, 0);
+    if (st)
+    {
+        st->converged = r == LPMGPU_OK;
+        st->reaction_norm = std::sqrt(h->p.scal_host->reaction_sq);
+    }
+    return r;
+}
+
+int32_t lpmgpu_fatigue_update_damage(lpmgpu_solver *h, double dNdt, int32_t *any_damaged)
+{
+    if (!h)
+        return LPMGPU_ERR_INVALID_ARG;
+    CK(cudaSetDevice(h->p.device));
+    return fatigue_damage(h->p, dNdt, any_damaged);
+}
+
+int32_t lpmgpu_fatigue_cycle(lpmgpu_solver *h, const lpmgpu_load_step *steps, int32_t nsteps, double dNdt,
+                             lpmgpu_stats *st, int32_t *any_damaged)
+{
+    if (!h || nsteps < 0 || (nsteps > 0 && !steps))
+        return LPMGPU_ERR_INVALID_ARG;
+    for (int32_t k = 0; k < nsteps; ++k)
+        ST(check_step(h->p, &steps[k]));
+    ST(begin_call(h, st));
+    Problem &p = h->p;
+    bool all = true;
+    for (int32_t k = 0; k < nsteps; ++k)
+    {
+        // solver_fatigue.h:227-236: the step's convergence is not acted on
+        const int32_t r = fatigue_step(p, steps[k], st);
+        if (r == LPMGPU_ERR_NEWTON)
+        {
+            all = false;
+            if (st)
+                st->cuts++;
+        }
+        else if (r != LPMGPU_OK)
+            return r;
+        CK(launch_update_state_var(p));
+    }
+    ST(fatigue_damage(p, dNdt, any_damaged));
+    ST(store_state(p));
+    ST(force_state(p, false));
+    if (st)
+    {
+        st->converged = all;
+        st->reaction_norm = std::sqrt(p.scal_host->reaction_sq);
+    }
+    return LPMGPU_OK;
 }
 
 int32_t lpmgpu_store_state(lpmgpu_solver *h)

@@ -92,6 +92,9 @@ class Desc(C.Structure):
         ("bond_damage", C.POINTER(C.c_double)), ("tangent", C.c_int32),
         ("nonlocal_cutoff_ratio", C.c_double), ("k0", C.c_double), ("k1", C.c_double),
         ("comp_tensile_ratio", C.c_double), ("damage_threshold", C.c_double),
+        ("fatigue_A", C.c_double), ("fatigue_B", C.c_double), ("fatigue_d", C.c_double),
+        ("fatigue_limit_ratio", C.c_double),
+        ("nonlocal_count", C.POINTER(C.c_int32)), ("nonlocal_ids", C.POINTER(C.c_int32)),
     ]
 
 
@@ -178,6 +181,7 @@ EXPORTS = [
     "lpmgpu_update_force_state", "lpmgpu_update_state_var", "lpmgpu_update_rr", "lpmgpu_assemble",
     "lpmgpu_export_ref_csr", "lpmgpu_solve_linear", "lpmgpu_apply_load_step",
     "lpmgpu_solve_problem_step", "lpmgpu_solve_load_step", "lpmgpu_store_state", "lpmgpu_reset_state",
+    "lpmgpu_fatigue_solve_step", "lpmgpu_fatigue_static_step", "lpmgpu_fatigue_update_damage", "lpmgpu_fatigue_cycle",
     "lpmgpu_read_state", "lpmgpu_read_residual", "lpmgpu_set_xyz", "lpmgpu_get_phase_times",
     "lpmgpu_get_counters", "lpmgpu_get_stream", "lpmgpu_cg_bsr_noalloc",
     "lpmgpu_format_dump", "lpmgpu_dump_write", "lpmgpu_dump_flush",
@@ -216,6 +220,10 @@ def lib():
         "lpmgpu_apply_load_step": (C.c_int32, [vp, C.POINTER(CLoadStep)]),
         "lpmgpu_solve_problem_step": (C.c_int32, [vp, C.POINTER(CLoadStep), C.POINTER(Stats)]),
         "lpmgpu_solve_load_step": (C.c_int32, [vp, C.POINTER(CLoadStep), C.POINTER(Stats)]),
+        "lpmgpu_fatigue_solve_step": (C.c_int32, [vp, C.POINTER(CLoadStep), C.POINTER(Stats)]),
+        "lpmgpu_fatigue_static_step": (C.c_int32, [vp, C.POINTER(CLoadStep), C.POINTER(Stats)]),
+        "lpmgpu_fatigue_update_damage": (C.c_int32, [vp, C.c_double, ip]),
+        "lpmgpu_fatigue_cycle": (C.c_int32, [vp, C.POINTER(CLoadStep), C.c_int32, C.c_double, C.POINTER(Stats), ip]),
         "lpmgpu_store_state": (C.c_int32, [vp]),
         "lpmgpu_reset_state": (C.c_int32, [vp]),
         "lpmgpu_read_state": (C.c_int32, [vp, dp, dp, dp, dp, dp, dp, dp]),
@@ -604,6 +612,8 @@ def _pack_desc(ass: Assembly, undamaged_pt_type=-1, max_iter=30, tol_iter=1e-5, 
     d.tangent = int(bool(tangent))
     d.nonlocal_cutoff_ratio = float(getattr(ass, "nonlocal_cutoff_ratio", 0.0))
     d.k0, d.k1, d.comp_tensile_ratio, d.damage_threshold = m.k0, m.k1, m.comp_tensile_ratio, m.damage_threshold
+    d.fatigue_A, d.fatigue_B, d.fatigue_d = m.fatigue_A, m.fatigue_B, m.fatigue_d
+    d.fatigue_limit_ratio = m.fatigue_limit_ratio
     if ass.bonds is not None:
         nb0, nb1, p2 = (np.ascontiguousarray(a, dtype=np.int32) for a in ass.bonds)
         keep += [nb0, nb1, p2]
@@ -636,7 +646,7 @@ class GpuProblem:
         _check(L.lpmgpu_get_sizes(h, C.byref(s)), "lpmgpu_get_sizes")
         self.sizes = {k: getattr(s, k) for k, _ in s._fields_}
         self.n, self.dim = s.n, s.dim
-        self.nsv = 7 if ass.ptype == ParticleType.J2Plasticity else 1
+        self.nsv = {ParticleType.J2Plasticity: 7, ParticleType.FatigueHCF: 3}.get(ass.ptype, 1)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -707,6 +717,42 @@ class GpuProblem:
         if r not in (OK, ERR_CUTS):
             _check(r, "lpmgpu_solve_load_step")
         return r == OK, st.as_dict()
+
+    # ---- SolverFatigue steps (include/solver_fatigue.h)
+    def fatigue_solve_step(self, step: LoadStep):
+        """SolverFatigue::solveProblemStep: (converged, stats)."""
+        cs = _CStep(step)
+        st = Stats()
+        r = lib().lpmgpu_fatigue_solve_step(self._h, C.byref(cs.s), C.byref(st))
+        if r not in (OK, ERR_NEWTON):
+            _check(r, "lpmgpu_fatigue_solve_step")
+        return r == OK, st.as_dict()
+
+    def fatigue_static_step(self, step: LoadStep):
+        """One load step of SolverFatigue::solveProblemStatic: (converged, stats)."""
+        cs = _CStep(step)
+        st = Stats()
+        r = lib().lpmgpu_fatigue_static_step(self._h, C.byref(cs.s), C.byref(st))
+        if r not in (OK, ERR_CUTS):
+            _check(r, "lpmgpu_fatigue_static_step")
+        return r == OK, st.as_dict()
+
+    def fatigue_update_damage(self, dNdt: float) -> bool:
+        """SolverFatigue::updateFatigueDamage: True when some damage moved by more than 1e-3."""
+        flag = C.c_int32(0)
+        _check(lib().lpmgpu_fatigue_update_damage(self._h, float(dNdt), C.byref(flag)), "lpmgpu_fatigue_update_damage")
+        return bool(flag.value)
+
+    def fatigue_cycle(self, steps: Sequence[LoadStep], dNdt: float):
+        """SolverFatigue::solveProblemOneCycle: (any_damaged, stats); stats["cuts"] counts the
+        steps whose Newton iteration did not converge (the reference carries on from them)."""
+        cs = [_CStep(x) for x in steps]
+        arr = (CLoadStep * max(len(cs), 1))(*[c.s for c in cs])
+        st = Stats()
+        flag = C.c_int32(0)
+        _check(lib().lpmgpu_fatigue_cycle(self._h, arr, len(cs), float(dNdt), C.byref(st), C.byref(flag)),
+               "lpmgpu_fatigue_cycle")
+        return bool(flag.value), st.as_dict()
 
     def store_state(self):
         _check(lib().lpmgpu_store_state(self._h), "lpmgpu_store_state")
@@ -971,3 +1017,86 @@ class SolverStatic:
         """Assembly::writeDump (include/assembly.h:310-335): the native writer, queued behind the
         step's device work (solveProblem flushes before it returns)."""
         self.problem.dump_write(path, step, self.ass.box, async_=True)
+
+
+class SolverFatigue:
+    """SolverFatigue<nlayer> (include/solver_fatigue.h:19-38) on the GPU: the same constructor
+    arguments and methods.  Each cycle's steps, the energy updates and the fatigue damage run on
+    the device; the cycle loop, the load spectrum and the dN/dt time map are host logic, as in
+    the reference."""
+
+    def __init__(self, undamaged_pt_type: int, ass: Assembly, stiff_mode=StiffnessMode.Analytical,
+                 sol_mode=SolverMode.CG, t_mode: TimeMapMode = TimeMapMode.Linear, tau: float = 1.0,
+                 dumpFile: str = "", max_iter: int = 30, tol: float = 1e-5, *,
+                 precision: Precision = Precision.FP64, cg_rtol=1e-12, cg_atol=1e-12, cg_maxit=0, device=0):
+        if StiffnessMode(stiff_mode) != StiffnessMode.Analytical:
+            raise ValueError("only StiffnessMode.Analytical is on the device path")
+        self.undamaged_pt_type = undamaged_pt_type
+        self.ass = ass
+        self.t_mode, self.tau = TimeMapMode(t_mode), float(tau)
+        self.dumpFile = dumpFile
+        self.load_spectrum: List[float] = []
+        self.problem = GpuProblem(ass, undamaged_pt_type, max_iter, tol, precision, cg_rtol, cg_atol, cg_maxit,
+                                  device)
+        self.stiffness = _StiffnessView(self.problem)
+        self.history: List[dict] = []
+
+    def readLoad(self, loadFile: str):
+        """SolverFatigue::readLoad (solver_fatigue.h:40-57): every number in the file, in order
+        (f_min, then f_max, f_min, ... pairs)."""
+        if not os.path.exists(loadFile):
+            raise FileNotFoundError(f"'{loadFile}' does not exist!")
+        with open(loadFile) as f:
+            self.load_spectrum += [float(v) for v in f.read().split()]
+
+    def generateLoadCycle(self, ltype: FatigueLoadType, N: int, n_interval: int, pt_groups) -> List[LoadStep]:
+        return generateLoadCycle(ltype, self.load_spectrum, N, n_interval, pt_groups)
+
+    def updateFatigueDamage(self, dNdt: float) -> bool:
+        return self.problem.fatigue_update_damage(dNdt)
+
+    def solveProblemStep(self, load_step: LoadStep) -> bool:
+        ok, st = self.problem.fatigue_solve_step(load_step)
+        self.history.append(st)
+        return ok
+
+    def solveProblemOneCycle(self, load: List[LoadStep], dNdt: float) -> bool:
+        any_d, st = self.problem.fatigue_cycle(load, dNdt)
+        self.history.append(st)
+        return any_d
+
+    def solveProblemStatic(self, load: List[LoadStep], start_index: int = 0) -> int:
+        """SolverFatigue::solveProblemStatic (solver_fatigue.h:244-275) with its halve-and-retry;
+        returns the new start_index."""
+        for i, step in enumerate(load):
+            ok, st = self.problem.fatigue_static_step(step)
+            st["step"] = i + start_index
+            self.history.append(st)
+            if not ok:
+                raise LpmGpuError(ERR_CUTS, f"load step {i + start_index}")
+            if self.dumpFile:
+                self.problem.dump_write(self.dumpFile, i, self.ass.box, async_=True)
+        self.problem.dump_flush()
+        return start_index + len(load)
+
+    def solveProblemCyclic(self, loadType: FatigueLoadType, n_interval: int, pt_groups) -> int:
+        """SolverFatigue::solveProblemCyclic (solver_fatigue.h:183-218): one simulated cycle per
+        pass, each standing for dN/dt real cycles, until the spectrum's cycle count is reached;
+        the dump after each cycle is tagged with the cycle count N.  Returns N."""
+        n_cycles = 0.5 * (len(self.load_spectrum) - 1)
+        t, N = 0.0, 0
+        while True:
+            load_cycle = self.generateLoadCycle(loadType, N, n_interval, pt_groups)
+            if self.t_mode == TimeMapMode.Linear:
+                dNdt = func_dNdt_linear(self.tau)
+            else:
+                dNdt = func_dNdt_exponental(self.tau, t)
+                t += 1
+            self.solveProblemOneCycle(load_cycle, dNdt)
+            N += int(dNdt)
+            if self.dumpFile:
+                self.problem.dump_write(self.dumpFile, N, self.ass.box, async_=True)
+            if not N < n_cycles:
+                break
+        self.problem.dump_flush()
+        return N

@@ -75,16 +75,17 @@
 #include "stiffness.h"
 #include "load_step.h"
 #include "solver_static.h"
-#ifndef LPM_USE_GPU
 #include "solver_fatigue.h"
 #include "load_step_fatigue.h"
-#endif
 #ifdef LPM_USE_GPU
-/* the one-line switch of an example's run(): SolverStatic -> SolverStaticGPU (lpm-cpp_b200/cpp) */
+/* the one-line switch of an example's run(): SolverStatic -> SolverStaticGPU and
+ * SolverFatigue -> SolverFatigueGPU (lpm-cpp_b200/cpp) */
 #include "solver_static_gpu.h"
 #define LPM_SOLVER SolverStaticGPU
+#define LPM_FATIGUE_SOLVER SolverFatigueGPU
 #else
 #define LPM_SOLVER SolverStatic
+#define LPM_FATIGUE_SOLVER SolverFatigue
 #endif
 
 static const int NL = 2;
@@ -442,7 +443,17 @@ static bool tangent_step(SolverStatic<NL> &solv, LoadStep<NL> &load_step)
 }
 #endif
 
-#ifndef LPM_USE_GPU
+#ifdef LPM_USE_GPU
+/* the device solver counts its own linear solves and CG iterations */
+#define DEVICE_COUNTS_BEGIN const long long gn0 = solv.totals.newton_solves, gc0 = solv.totals.cg_iters;
+#define DEVICE_COUNTS_END                                                                                             \
+    st1.cg_solves = st0.cg_solves + (solv.totals.newton_solves - gn0);                                                 \
+    st1.cg_iterations = st0.cg_iterations + (solv.totals.cg_iters - gc0);
+#else
+#define DEVICE_COUNTS_BEGIN
+#define DEVICE_COUNTS_END
+#endif
+
 static FatigueLoadType fatigue_type_of(const std::string &s)
 {
     if (s == "uniaxial_disp") return FatigueLoadType::LoadUniaxialDisp;
@@ -472,8 +483,12 @@ static int run_fatigue(Assembly<NL> &ass, std::map<std::string, std::vector<Part
                        std::vector<LoadStep<NL>> &load, const Spec &sp, int N, int dim, double setup_s)
 {
     const TimeMapMode tm = (sp.fatigue_tmode == "exponential") ? TimeMapMode::Exponential : TimeMapMode::Linear;
-    SolverFatigue<NL> solv{sp.undamaged_type, ass, StiffnessMode::Analytical, SolverMode::CG, tm, sp.fatigue_tau,
-                           sp.dumpfile, sp.max_iter, sp.tol_iter};
+    LPM_FATIGUE_SOLVER<NL> solv{sp.undamaged_type, ass, StiffnessMode::Analytical, SolverMode::CG, tm, sp.fatigue_tau,
+                                sp.dumpfile, sp.max_iter, sp.tol_iter};
+#ifdef LPM_USE_GPU
+    if (sp.cg_rtol >= 0 || sp.cg_atol >= 0)
+        solv.setCGTolerance(sp.cg_rtol >= 0 ? sp.cg_rtol : 1e-12, sp.cg_atol >= 0 ? sp.cg_atol : 1e-12);
+#endif
     FILE *log = std::fopen((sp.out + "/steps.txt").c_str(), "w");
     std::fprintf(log, "# N %d dim %d setup_s %.6f threads %d\n", N, dim, setup_s, omp_get_max_threads());
     std::fprintf(log, "# step newton_solves cg_iters wall_s spmv_s cg_s create_s cuts reaction_norm cg_fail\n");
@@ -482,10 +497,12 @@ static int run_fatigue(Assembly<NL> &ass, std::map<std::string, std::vector<Part
     for (int s = 0; s < sp.steps; ++s, ++idx)
     {
         lpm_shim_stats st0 = lpm_shim_stats_g;
+        DEVICE_COUNTS_BEGIN
         const double t0 = wall();
         std::vector<LoadStep<NL>> one{load[s]};
         solv.solveProblemStatic(one, start_index);
         lpm_shim_stats st1 = lpm_shim_stats_g;
+        DEVICE_COUNTS_END
         log_line(log, idx, st0, st1, wall() - t0, (int)one.size() - 1,
                  cblas_dnrm2((MKL_INT)solv.reaction_force.size(), solv.reaction_force.data(), 1));
         std::snprintf(tag, sizeof tag, "%03d", idx);
@@ -505,12 +522,14 @@ static int run_fatigue(Assembly<NL> &ass, std::map<std::string, std::vector<Part
         do
         {
             lpm_shim_stats st0 = lpm_shim_stats_g;
+            DEVICE_COUNTS_BEGIN
             const double t0 = wall();
             std::vector<LoadStep<NL>> load_cycle = solv.generateLoadCycle(lt, Nc, sp.fatigue_interval, pg);
             dNdt = (tm == TimeMapMode::Linear) ? func_dNdt_linear(sp.fatigue_tau) : func_dNdt_exponental(sp.fatigue_tau, t++);
             solv.solveProblemOneCycle(load_cycle, dNdt);
             Nc += (int)dNdt;
             lpm_shim_stats st1 = lpm_shim_stats_g;
+            DEVICE_COUNTS_END
             log_line(log, idx, st0, st1, wall() - t0, 0,
                      cblas_dnrm2((MKL_INT)solv.reaction_force.size(), solv.reaction_force.data(), 1));
             std::fprintf(cyc, "%d %.17g\n", Nc, dNdt);
@@ -522,7 +541,6 @@ static int run_fatigue(Assembly<NL> &ass, std::map<std::string, std::vector<Part
     std::fclose(log);
     return 0;
 }
-#endif
 
 int main(int argc, char **argv)
 {
@@ -725,16 +743,8 @@ int main(int argc, char **argv)
         write_bin(sp.out + "/pin_init.f64", pin0.data(), pin0.size());
     }
 
-#ifndef LPM_USE_GPU
     if (!sp.fatigue_type.empty())
         return run_fatigue(ass, groups, load, sp, N, dim, t_setup1 - t_setup0);
-#else
-    if (!sp.fatigue_type.empty())
-    {
-        std::fprintf(stderr, "the fatigue driver is not part of this build\n");
-        return 2;
-    }
-#endif
     FILE *log = std::fopen((sp.out + "/steps.txt").c_str(), "w");
     std::fprintf(log, "# N %d dim %d setup_s %.6f threads %d\n", N, dim, t_setup1 - t_setup0, omp_get_max_threads());
     std::fprintf(log, "# step newton_solves cg_iters wall_s spmv_s cg_s create_s cuts reaction_norm cg_fail\n");

@@ -89,6 +89,9 @@ def cases():
         "hex_edamage": (lambda: CFG.edamage_plate(), {"cg_tol": (1e-24, 0.0), "dump_k": (1,)}),
         # SolverFatigue: one static step, then four cycles (two steps up, two down) of HCF damage
         "hex_fatigue": (lambda: CFG.fatigue_plate(), {"cg_tol": (1e-24, 0.0), "fatigue": True}),
+        # the exponential time map: dN/dt = (int)(1/tau exp(t/tau)) is 0, 0, 1, 2, 3 at tau = 2
+        "hex_fatigue_exp": (lambda: CFG.fatigue_plate(cycles=4, tmode="exponential", tau=2.0, A=40.0),
+                            {"cg_tol": (1e-24, 0.0), "fatigue": True}),
     }
 
 
