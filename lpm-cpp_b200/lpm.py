@@ -344,7 +344,7 @@ def createCuboidBCC3D(box, cell, R=None):
 @dataclass
 class Material:
     """Arguments of setParticleProperty (particle_elastic.h:70, particle_j2plasticity.h:155,
-    particle_elastic_damage.h:183)."""
+    particle_elastic_damage.h:176, particle_fatigue_hcf.h:163)."""
     plane_stress: bool = False
     E: float = 69e3
     mu: float = 0.3
@@ -450,11 +450,21 @@ class Assembly:
         np.savetxt(bondFile, rows, fmt="%d")
 
     def setParticleProperty(self, nonlocal_L, is_plane_stress, E, mu, *rest):
-        """Elastic: (nonlocal_L, is_plane_stress, E, mu, critical_bstrain);
-        J2: (nonlocal_L, is_plane_stress, E, mu, sigmay, xi, H, A, critical_bstrain)."""
+        """The isotropic setParticleProperty of the assembly's particle type:
+        Elastic: (nonlocal_L, is_plane_stress, E, mu, critical_bstrain) (particle_elastic.h:71);
+        J2: (nonlocal_L, is_plane_stress, E, mu, sigmay, xi, H, A, critical_bstrain)
+        (particle_j2plasticity.h:155);
+        ElasticDamage: (nonlocal_L, is_plane_stress, E, mu, k0, k1, ct_ratio, d_thres)
+        (particle_elastic_damage.h:176);
+        FatigueHCF: (nonlocal_L, is_plane_stress, E, mu, A, B, d, d_thres, f_lmt_ratio)
+        (particle_fatigue_hcf.h:163)."""
         m = Material(plane_stress=bool(is_plane_stress), E=float(E), mu=float(mu), nonlocal_L=float(nonlocal_L))
         if self.ptype == ParticleType.J2Plasticity:
             m.sigmay, m.xi, m.H, m.A, m.critical_bstrain = map(float, rest)
+        elif self.ptype == ParticleType.ElasticDamage:
+            m.k0, m.k1, m.comp_tensile_ratio, m.damage_threshold = map(float, rest)
+        elif self.ptype == ParticleType.FatigueHCF:
+            m.fatigue_A, m.fatigue_B, m.fatigue_d, m.damage_threshold, m.fatigue_limit_ratio = map(float, rest)
         else:
             (m.critical_bstrain,) = map(float, rest)
         self.material = m

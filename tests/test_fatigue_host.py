@@ -77,3 +77,18 @@ def test_fatigue_desc_fields_reach_the_c_struct():
     assert d.ptype == int(LPM.ParticleType.FatigueHCF) == 3
     assert (d.fatigue_A, d.fatigue_B, d.fatigue_d) == (7.0, 2.5, 0.75)
     assert LPM.Desc.fatigue_A.offset > LPM.Desc.damage_threshold.offset
+
+
+def test_set_particle_property_per_type():
+    """Assembly.setParticleProperty takes each particle type's isotropic argument list."""
+    c = CFG.fatigue_plate()
+    a = c.assembly()
+    a.setParticleProperty(6.0, True, 71.7e3, 0.306, 2.003e-5, 2.833, 0.5, 1.0, 1.108)
+    m = a.material
+    assert (m.nonlocal_L, m.plane_stress, m.E, m.mu) == (6.0, True, 71.7e3, 0.306)
+    assert (m.fatigue_A, m.fatigue_B, m.fatigue_d, m.damage_threshold, m.fatigue_limit_ratio) == \
+        (2.003e-5, 2.833, 0.5, 1.0, 1.108)
+    e = CFG.edamage_plate().assembly()
+    e.setParticleProperty(0.3, True, 69e3, 0.3, 0.02, 0.5, 10.0, 0.9)
+    assert (e.material.k0, e.material.k1, e.material.comp_tensile_ratio, e.material.damage_threshold) == \
+        (0.02, 0.5, 10.0, 0.9)
