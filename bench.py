@@ -60,6 +60,8 @@ def args_():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
     ap.add_argument("--no-tangent", action="store_true", help="skip the FCC J2 tangent-mode leg")
     ap.add_argument("--no-dump", action="store_true", help="skip the per-step dump output leg")
+    ap.add_argument("--autotune", action="store_true",
+                    help="tune the CG grid of the headline problem after the first warm-up step (lpmgpu_autotune)")
     ap.add_argument("--tangent-steps", type=int, default=4, help="load steps of the FCC bar's 50-step path timed")
     ap.add_argument("--serve-requests", type=int, default=12, help="requests in the serving-stream sample")
     ap.add_argument("--serve-max-particles", type=float, default=1e5,
@@ -208,9 +210,12 @@ def run_ours(a):
     n, dim, nnzb = sizes["n"], sizes["dim"], sizes["nnzb"]
     ndof = n * dim
     stream = torch.cuda.ExternalStream(prob.stream_ptr())
+    tune = None
     for s in range(W):
         ok, _ = prob.solve_load_step(step_of(case, s))
         assert ok, f"warm-up step {s} did not converge"
+        if s == 0 and a.autotune:
+            tune = prob.autotune(iterations=50)
     barrier()
     torch.cuda.synchronize()
     c0 = prob.counters()
@@ -347,7 +352,8 @@ def run_ours(a):
             "config": {"workload": desc, "particles": n, "dof": ndof, "block_nnz": nnzb,
                        "nnz_upper_ref_csr": sizes["nnz_upper"], "newton_tol": NEWTON_TOL,
                        "cg_test": "||r||^2 <= 1e-12 ||r0||^2 + 1e-12 (reference)",
-                       "l2": "stiffness larger than L2 (126 MB); no flush", "parallelism": f"replicas x{world}"},
+                       "l2": "stiffness larger than L2 (126 MB); no flush", "parallelism": f"replicas x{world}",
+                       "cg_grid": tune if tune is not None else "default (one block per SM)"},
             "solves_per_s": world * K / (ms_max * 1e-3),
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "newton_per_step": sum(st["newton_solves"] for st in stats) / K,

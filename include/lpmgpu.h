@@ -223,6 +223,26 @@ int32_t lpmgpu_fatigue_update_damage(lpmgpu_solver *h, double dNdt, int32_t *any
 int32_t lpmgpu_fatigue_cycle(lpmgpu_solver *h, const lpmgpu_load_step *steps, int32_t nsteps, double dNdt,
                              lpmgpu_stats *stats, int32_t *any_damaged);
 
+/* Autotuner of the CG launch shape (no counterpart in the reference; the reference's MKL CG has no
+ * launch shape).  lpmgpu_autotune re-assembles K from the current state (call it between load
+ * steps, after the first, so that the displacement BCs make K definite), then times `iterations` CG iterations of this problem's matrix (the FP32 inner solve in
+ * mixed precision) for each candidate grid size: the default (one block per SM, at most one per
+ * slice) and 3/4, 1/2, 1/4, 1/8, 1/16 of it.  The fastest stays in force for this handle's later
+ * solves; results then differ from the default grid's only by the rounding of the reductions.
+ * lpmgpu_set_cg_grid sets the grid directly (0 = the default; values above the default are
+ * clamped to it). */
+#define LPMGPU_TUNE_MAX 8
+typedef struct
+{
+    int32_t precision;                    /* the precision that was tuned */
+    int32_t grid_default, grid_chosen;    /* blocks per CG launch */
+    int32_t ncandidates;
+    int32_t grid[LPMGPU_TUNE_MAX];        /* candidates, in the order tried */
+    double us_per_iter[LPMGPU_TUNE_MAX];  /* their time per CG iteration, microseconds */
+} lpmgpu_tune_result;
+int32_t lpmgpu_autotune(lpmgpu_solver *h, int32_t iterations, lpmgpu_tune_result *out);
+int32_t lpmgpu_set_cg_grid(lpmgpu_solver *h, int32_t grid);
+
 /* Device state back to host (any pointer may be NULL): xyz n*3, Pin n*3, stress n*6 (s11 s22
  * s33 s23 s13 s12), damage n, damage_visual n, state_var n*nsv (nsv = 7 for J2, 3 for fatigue
  * HCF, else 1),

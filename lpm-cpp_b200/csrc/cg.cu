@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <vector>
 #include <mutex>
 #include <string>
 
@@ -339,16 +340,16 @@ __global__ void k_sum_partials(int nblk, const double *__restrict__ part, double
     }
 }
 
+// The default CG grid: one block per SM (kCGMinBlocks per SM when they fit), at most one block per
+// slice.  Every grid up to it is co-resident, as the cooperative launch needs.
 template <typename TK, typename TV, int D>
-static cudaError_t run_cg(Problem &p, const TK *K, const TV *b, TV *x, TV *r, TV *pa, TV *pb, TV *q, double rtol,
-                          double atol, double abs_stop, int64_t maxit, CGResult &out, double *rr_final)
+static cudaError_t cg_grid_rule(const Problem &p, int *grid_out)
 {
     static int occ_cache[2][2][4] = {};
     int &occ = occ_cache[sizeof(TK) == 8][sizeof(TV) == 8][D];
-    cudaError_t e;
     if (occ == 0)
     {
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg<TK, TV, D>, kCGThreads, 0);
+        const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_cg<TK, TV, D>, kCGThreads, 0);
         if (e != cudaSuccess)
             return e;
         if (occ < 1)
@@ -359,6 +360,20 @@ static cudaError_t run_cg(Problem &p, const TK *K, const TV *b, TV *x, TV *r, TV
         grid = std::max(1, p.nslices);
     if (grid > kMaxGridBlocks)
         grid = kMaxGridBlocks;
+    *grid_out = grid;
+    return cudaSuccess;
+}
+
+template <typename TK, typename TV, int D>
+static cudaError_t run_cg(Problem &p, const TK *K, const TV *b, TV *x, TV *r, TV *pa, TV *pb, TV *q, double rtol,
+                          double atol, double abs_stop, int64_t maxit, CGResult &out, double *rr_final)
+{
+    cudaError_t e;
+    int grid = 0;
+    if ((e = cg_grid_rule<TK, TV, D>(p, &grid)) != cudaSuccess)
+        return e;
+    if (p.cg_grid > 0 && p.cg_grid < grid)
+        grid = p.cg_grid; // a tuned grid only ever lowers the default, so it stays co-resident
     CGState s;
     s.n = p.n;
     s.nslices = p.nslices;
@@ -534,7 +549,122 @@ cudaError_t solve_linear(Problem &p, CGResult &out)
     return p.dim == 2 ? solve_dim<2>(p, out) : solve_dim<3>(p, out);
 }
 
+// ---- autotuner of the CG launch shape (no counterpart in the reference)
+//
+// The persistent CG kernel's cost per iteration is the matrix stream plus two grid barriers.  On
+// large problems every SM streams and the default grid (one block per SM) is best; on small ones
+// the barriers dominate and fewer, fuller blocks can be faster.  The tuner times `iterations` CG
+// iterations of this problem's own matrix for each candidate grid (the default and its 3/4, 1/2,
+// 1/4, 1/8, 1/16), twice each, and keeps the fastest by its second timing.  Candidates are never
+// above the default, so every one is co-resident.
+template <typename TK, typename TV, int D>
+static cudaError_t tune_dim(Problem &p, int iterations, lpmgpu_tune_result *res, const TK *K, const TV *b, TV *x,
+                            TV *r, TV *pa, TV *pb, TV *q)
+{
+    int g0 = 0;
+    cudaError_t e = cg_grid_rule<TK, TV, D>(p, &g0);
+    if (e != cudaSuccess)
+        return e;
+    std::vector<int> cand;
+    for (int f : {16, 12, 8, 4, 2, 1}) // 16/16, 12/16, ... of the default
+    {
+        const int g = std::max(1, g0 * f / 16);
+        if (std::find(cand.begin(), cand.end(), g) == cand.end() && (int)cand.size() < LPMGPU_TUNE_MAX)
+            cand.push_back(g);
+    }
+    const int saved = p.cg_grid;
+    const lpmgpu_counters ctr = p.ctr;
+    int best = g0;
+    double best_us = 0;
+    res->ncandidates = (int32_t)cand.size();
+    for (size_t k = 0; k < cand.size(); ++k)
+    {
+        p.cg_grid = cand[k];
+        double us = 0;
+        for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep)
+        {
+            CGResult cr;
+            e = run_cg<TK, TV, D>(p, K, b, x, r, pa, pb, q, 0.0, 0.0, 0.0, iterations, cr, nullptr);
+            float ms = 0;
+            if (e == cudaSuccess && (e = cudaEventElapsedTime(&ms, p.cg_ev[0], p.cg_ev[1])) == cudaSuccess)
+                us = cr.iters > 0 ? 1e3 * ms / (double)cr.iters : 0.0;
+            if (cr.timeout)
+            {
+                set_last_error("a device-side barrier wait timed out while tuning the CG kernel");
+                e = cudaErrorLaunchTimeout;
+            }
+        }
+        if (e != cudaSuccess)
+            break;
+        res->grid[k] = cand[k];
+        res->us_per_iter[k] = us;
+        if (us > 0 && (best_us == 0 || us < best_us))
+        {
+            best_us = us;
+            best = cand[k];
+        }
+    }
+    p.ctr = ctr; // tuning launches do not count as solves
+    p.cg_grid = (e == cudaSuccess) ? (best == g0 ? 0 : best) : saved;
+    res->grid_default = g0;
+    res->grid_chosen = best;
+    return e;
+}
+
 } // namespace lpm
+
+extern "C" {
+
+int32_t lpmgpu_set_cg_grid(lpmgpu_solver *h, int32_t grid)
+{
+    if (!h || grid < 0)
+        return LPMGPU_ERR_INVALID_ARG;
+    h->p.cg_grid = grid;
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_autotune(lpmgpu_solver *h, int32_t iterations, lpmgpu_tune_result *out)
+{
+    using namespace lpm;
+    if (!h || !out || iterations < 1 || iterations > 100000)
+        return LPMGPU_ERR_INVALID_ARG;
+    *out = lpmgpu_tune_result{};
+    Problem &p = h->p;
+    cudaError_t e = cudaSetDevice(p.device);
+    // K from the current state, as the next load step assembles it; the right-hand side is the
+    // diagonal before the BC elimination, which is nonzero for every row
+    if (e == cudaSuccess)
+        e = enqueue_assemble(p, true);
+    const int64_t ndof = (int64_t)p.n * p.dim;
+    if (e == cudaSuccess && p.desc.precision == LPMGPU_MIXED)
+    {
+        k_convert<double, float><<<std::min(div_up(ndof, 256), 8 * p.num_sms), 256, 0, p.stream>>>(ndof, p.diag_raw,
+                                                                                                   p.b32);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+    {
+        out->precision = p.desc.precision;
+        if (p.desc.precision == LPMGPU_MIXED)
+            e = p.dim == 2 ? tune_dim<float, float, 2>(p, iterations, out, p.K32, p.b32, p.x32, p.r32, p.pa32, p.pb32,
+                                                       p.q32)
+                           : tune_dim<float, float, 3>(p, iterations, out, p.K32, p.b32, p.x32, p.r32, p.pa32, p.pb32,
+                                                       p.q32);
+        else
+            e = p.dim == 2 ? tune_dim<double, double, 2>(p, iterations, out, p.K, p.diag_raw, p.x, p.r, p.p0, p.p1, p.q)
+                           : tune_dim<double, double, 3>(p, iterations, out, p.K, p.diag_raw, p.x, p.r, p.p0, p.p1, p.q);
+    }
+    if (e == cudaErrorLaunchTimeout)
+        return LPMGPU_ERR_TIMEOUT;
+    if (e != cudaSuccess)
+    {
+        set_last_error(std::string("lpmgpu_autotune: ") + cudaGetErrorString(e));
+        return LPMGPU_ERR_CUDA;
+    }
+    return LPMGPU_OK;
+}
+
+} // extern "C"
 
 // ---------------------------------------------------------------------------------------
 // Allocation-free CG on a caller-supplied block-CSR matrix.

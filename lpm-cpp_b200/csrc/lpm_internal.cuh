@@ -94,6 +94,7 @@ struct Problem
     int64_t *slice_off = nullptr;     // nslices+1 block-slot offsets
     int *col_sell = nullptr;          // nsb * kSlice particle columns
     int nslices = 0;
+    int cg_grid = 0;                  // > 0: blocks per CG launch (lpmgpu_autotune / lpmgpu_set_cg_grid)
     int64_t nsb = 0;                  // block slots of the sliced-ELL layout (>= nnzb / kSlice)
     double *K = nullptr;              // nsb * d*d * kSlice
     float *K32 = nullptr;             // mixed precision copy

@@ -163,6 +163,16 @@ class ServerStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("grid_default", C.c_int32), ("grid_chosen", C.c_int32),
+                ("ncandidates", C.c_int32), ("grid", C.c_int32 * 8), ("us_per_iter", C.c_double * 8)]
+
+    def as_dict(self):
+        k = self.ncandidates
+        return {"precision": self.precision, "grid_default": self.grid_default, "grid_chosen": self.grid_chosen,
+                "candidates": list(self.grid[:k]), "us_per_iter": list(self.us_per_iter[:k])}
+
+
 class BatchStats(C.Structure):
     _fields_ = [("rounds", C.c_int64), ("cg_launches", C.c_int64), ("members_done", C.c_int64),
                 ("members_failed", C.c_int64), ("cg_iters", C.c_int64), ("dof_iters", C.c_int64),
@@ -183,7 +193,7 @@ EXPORTS = [
     "lpmgpu_solve_problem_step", "lpmgpu_solve_load_step", "lpmgpu_store_state", "lpmgpu_reset_state",
     "lpmgpu_fatigue_solve_step", "lpmgpu_fatigue_static_step", "lpmgpu_fatigue_update_damage", "lpmgpu_fatigue_cycle",
     "lpmgpu_read_state", "lpmgpu_read_residual", "lpmgpu_set_xyz", "lpmgpu_get_phase_times",
-    "lpmgpu_get_counters", "lpmgpu_get_stream", "lpmgpu_cg_bsr_noalloc",
+    "lpmgpu_get_counters", "lpmgpu_get_stream", "lpmgpu_cg_bsr_noalloc", "lpmgpu_autotune", "lpmgpu_set_cg_grid",
     "lpmgpu_format_dump", "lpmgpu_dump_write", "lpmgpu_dump_flush",
     "lpmgpu_batch_create", "lpmgpu_batch_destroy", "lpmgpu_batch_add", "lpmgpu_batch_round", "lpmgpu_batch_run",
     "lpmgpu_batch_member", "lpmgpu_batch_member_steps", "lpmgpu_batch_remove", "lpmgpu_batch_get_stats",
@@ -236,6 +246,8 @@ def lib():
                                            C.c_int32, C.c_int32]),
         "lpmgpu_dump_write": (C.c_int32, [vp, C.c_char_p, C.c_int32, dp, C.c_int32, C.c_int32]),
         "lpmgpu_dump_flush": (C.c_int32, [vp]),
+        "lpmgpu_autotune": (C.c_int32, [vp, C.c_int32, C.POINTER(TuneResult)]),
+        "lpmgpu_set_cg_grid": (C.c_int32, [vp, C.c_int32]),
         "lpmgpu_cg_bsr_noalloc": (C.c_int32, [C.c_int32, C.c_int32, vp, vp, vp, vp, vp, C.c_double, C.c_double,
                                               C.c_int64, vp, C.POINTER(C.c_int64)]),
         "lpmgpu_batch_create": (C.c_int32, [C.c_int32, C.POINTER(vp)]),
@@ -763,6 +775,17 @@ class GpuProblem:
         _check(lib().lpmgpu_fatigue_cycle(self._h, arr, len(cs), float(dNdt), C.byref(st), C.byref(flag)),
                "lpmgpu_fatigue_cycle")
         return bool(flag.value), st.as_dict()
+
+    def autotune(self, iterations: int = 50) -> dict:
+        """Times the CG kernel on this problem for several grid sizes and keeps the fastest
+        (lpmgpu_autotune).  Call between load steps: it re-assembles K from the current state."""
+        r = TuneResult()
+        _check(lib().lpmgpu_autotune(self._h, int(iterations), C.byref(r)), "lpmgpu_autotune")
+        return r.as_dict()
+
+    def set_cg_grid(self, grid: int):
+        """Blocks per CG launch; 0 restores the default (one block per SM, at most one per slice)."""
+        _check(lib().lpmgpu_set_cg_grid(self._h, int(grid)), "lpmgpu_set_cg_grid")
 
     def store_state(self):
         _check(lib().lpmgpu_store_state(self._h), "lpmgpu_store_state")

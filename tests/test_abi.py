@@ -61,6 +61,8 @@ def test_invalid_arguments_are_rejected():
     assert L.lpmgpu_server_create(0, 0, None) == 1
     assert L.lpmgpu_server_submit(None, None, None, 0, None) == 1
     assert L.lpmgpu_estimate_bytes(None, None) == 1
+    assert L.lpmgpu_autotune(None, 10, None) == 1
+    assert L.lpmgpu_set_cg_grid(None, 4) == 1
 
 
 @pytest.mark.skipif(cuda_available(), reason="checks the no-device path")
@@ -95,3 +97,12 @@ def test_estimate_counts_the_nonlocal_lists():
         R = c.nonlocal_cutoff_ratio * c.material.nonlocal_L
         pairs = sum(len(v) for v in cKDTree(c.xyz).query_ball_point(c.xyz, R * (1 - 1e-12)))
         assert with_nl - without >= 4 * pairs + 12 * c.n
+
+
+def test_tune_result_layout_matches_the_header():
+    """lpmgpu_tune_result: four int32 then LPMGPU_TUNE_MAX int32 grids and doubles."""
+    txt = open(HEADER).read()
+    m = re.search(r"#define LPMGPU_TUNE_MAX (\d+)", txt)
+    assert m and int(m.group(1)) == 8
+    assert LPM.TuneResult.us_per_iter.offset == 4 * 4 + 8 * 4
+    assert C.sizeof(LPM.TuneResult) == 4 * 4 + 8 * 4 + 8 * 8
