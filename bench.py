@@ -60,6 +60,7 @@ def args_():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
     ap.add_argument("--no-tangent", action="store_true", help="skip the FCC J2 tangent-mode leg")
     ap.add_argument("--no-dump", action="store_true", help="skip the per-step dump output leg")
+    ap.add_argument("--no-fatigue", action="store_true", help="skip the fatigue (SolverFatigue) leg")
     ap.add_argument("--autotune", action="store_true",
                     help="tune the CG grid of the headline problem after the first warm-up step (lpmgpu_autotune)")
     ap.add_argument("--tangent-steps", type=int, default=4, help="load steps of the FCC bar's 50-step path timed")
@@ -343,6 +344,10 @@ def run_ours(a):
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(case, a.cpu_cg_cap)
+    # last, after every other measurement: the newest device path
+    fatigue = None
+    if single and not a.no_fatigue:
+        fatigue = fatigue_leg(lpm, local)
 
     if rank == 0:
         line = {
@@ -363,6 +368,7 @@ def run_ours(a):
                                    "cg_kernel": cg_s * 1e3 / K},
             "roofline": roof, "e2e": e2e, "gpu_launches": counters_total, "clocks": clocks,
             "mixed": mixed, "batched": batched, "serving": serving, "tangent": tangent, "dump": dump,
+            "fatigue": fatigue,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -412,6 +418,73 @@ def dump_leg(lpm, case, first_step, device, steps=3):
         return {"error": f"{type(ex).__name__}: {ex}"}
     finally:
         shutil.rmtree(d, ignore_errors=True)
+
+
+def fatigue_leg(lpm, device, size=25.0, cycles=4):
+    """Fatigue (SolverFatigue, include/solver_fatigue.h) on a hexagonal plate of fatigue HCF
+    particles (lpm-cpp_b200/configs.fatigue_plate): `size` mm at r = 0.1, nonlocal averaging over
+    1.5 x 0.3 mm, one static step of solveProblemStatic, then `cycles` displacement cycles of
+    solveProblemCyclic (LoadUniaxialDisp, two steps up and two down, the amplitude scaled to the
+    plate so that the strain is that of the 2.4 mm test plate; dN/dt = 2), at the example's Newton
+    tolerance 1e-5 and the reference's CG test.  GPU: the C ABI steps, wall time around the
+    host-driven calls (creation and the nonlocal search untimed).  Reference: the reference's own
+    SolverFatigue (oracle/_ref/lpm_ref) on all host cores, the same spec, wall time of the same
+    static step and cycles.  Error: the final damage and displacements against the reference run
+    (both stop at the loose tolerance, and the reference's assembly races at several threads)."""
+    try:
+        import torch
+        from oracle import oracle as O
+        cfg = importlib.import_module("lpm-cpp_b200.configs")
+        c = cfg.fatigue_plate(size=size, radius=0.1, cycles=cycles, amplitude=0.004 * size / 2.4, tol_iter=1e-5)
+        fat = c.meta["fatigue"]
+        amp = max(abs(v) for v in fat["spectrum"])
+        groups = [c.groups[g] for g in fat["groups"]]
+        g = lpm.GpuProblem(c.assembly(), undamaged_pt_type=c.undamaged_type, max_iter=c.max_iter,
+                           tol_iter=c.tol_iter, device=device)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ok, st = g.fatigue_static_step(c.load_step(0))
+        assert ok, "static step did not converge"
+        newton, ncyc, N = st["newton_solves"], 0, 0
+        n_cycles = 0.5 * (len(fat["spectrum"]) - 1)
+        while True:  # solveProblemCyclic's loop (solver_fatigue.h:183-218)
+            steps = lpm.generateLoadCycle(lpm.FatigueLoadType.LoadUniaxialDisp, fat["spectrum"], N, fat["n_interval"],
+                                          groups)
+            dNdt = lpm.func_dNdt_linear(fat["tau"])
+            _, st = g.fatigue_cycle(steps, dNdt)
+            newton += st["newton_solves"]
+            ncyc += 1
+            N += dNdt
+            if not N < n_cycles:
+                break
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        sg = g.state(("xyz", "damage"))
+        g.close()
+        out = {"workload": f"fatigue HCF hex plate {size:g} mm, r=0.1 ({c.n} particles), 1 static step + {ncyc} "
+                           f"cycles x 4 steps, dN/dt={dNdt}, Newton tol 1e-5",
+               "gpu": {"seconds": wall, "cycles_per_s": ncyc / wall, "newton_solves": newton,
+                       "max_damage": float(sg["damage"].max())}}
+        if O.ref_available():
+            threads = os.cpu_count() or 1
+            d = tempfile.mkdtemp(prefix="lpmref_fatigue_")
+            try:
+                O.run_ref(O.write_ref_spec(c, d, loop="ref"), d, threads=threads, timeout=1800)
+                rows = O.read_ref_steps(d)
+                last = len(rows) - 1
+                xr = O.read_bin(d, f"xyz_{last:03d}.f64", np.float64).reshape(-1, 3)
+                dr = O.read_bin(d, f"damage_{last:03d}.f64", np.float64)
+            finally:
+                shutil.rmtree(d, ignore_errors=True)
+            wall_r = sum(r["wall_s"] for r in rows)
+            out["reference"] = {"seconds": wall_r, "cycles_per_s": ncyc / wall_r, "cores": threads,
+                                "kind": "reference", "newton_solves": int(sum(r["newton_solves"] for r in rows))}
+            out["speedup_vs_reference"] = wall_r / wall
+            out["max_abs_damage_diff_vs_reference"] = float(np.abs(sg["damage"] - dr).max())
+            out["max_abs_disp_diff_vs_reference_over_amplitude"] = float(np.abs(sg["xyz"] - xr).max() / amp)
+        return out
+    except Exception as ex:  # the leg must not cost the bench line
+        return {"error": f"{type(ex).__name__}: {ex}"}
 
 
 def batched_leg(lpm, count, device, world, allreduce):
