@@ -121,6 +121,11 @@ struct Problem
     std::vector<double> xyz0_host;
     std::vector<int> type_host;
     void *dump = nullptr;
+    // the force-state sequence (geometry + bond forces, particle forces + residual, the scalar
+    // record's copy) as CUDA graphs, without / with the reaction accumulation of updateRR;
+    // captured at first use, replayed afterwards (graphs_off: capture failed or LPMGPU_NO_GRAPHS)
+    cudaGraphExec_t fs_graph[2] = {nullptr, nullptr};
+    bool graphs_off = false;
 };
 
 constexpr int kMaxGridBlocks = 4096;

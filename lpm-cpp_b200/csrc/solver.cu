@@ -7,6 +7,7 @@
 //   Assembly::storeStateVar / resetStateVar  include/assembly.h:141-159
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -53,7 +54,7 @@ static int32_t sync_scalars(Problem &p)
     return LPMGPU_OK;
 }
 
-cudaError_t enqueue_force_state(Problem &p, bool with_rr)
+static cudaError_t enqueue_force_state_direct(Problem &p, bool with_rr)
 {
     cudaError_t e = launch_geometry_force(p);
     if (e == cudaSuccess)
@@ -61,6 +62,52 @@ cudaError_t enqueue_force_state(Problem &p, bool with_rr)
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(p.scal_host, p.scal, sizeof(Scalars), cudaMemcpyDeviceToHost, p.stream);
     return e;
+}
+
+// Captures the force-state sequence of enqueue_force_state_direct into an executable graph.  Its
+// kernels read only the problem's fixed device buffers and constants, so one capture per value of
+// with_rr serves every later call.  On any failure the problem goes back to direct launches.
+static void capture_force_state(Problem &p, bool with_rr)
+{
+    const int64_t launches = p.ctr.kernel_launches;
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(p.stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess)
+    {
+        const cudaError_t e1 = enqueue_force_state_direct(p, with_rr);
+        e = cudaStreamEndCapture(p.stream, &graph);
+        if (e == cudaSuccess)
+            e = e1;
+    }
+    p.ctr.kernel_launches = launches;
+    cudaGraphExec_t exec = nullptr;
+    if (e == cudaSuccess && graph)
+        e = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph)
+        cudaGraphDestroy(graph);
+    if (e != cudaSuccess || !exec)
+    {
+        p.graphs_off = true;
+        (void)cudaGetLastError(); // the failed capture's error is not the caller's
+        return;
+    }
+    p.fs_graph[with_rr ? 1 : 0] = exec;
+}
+
+// Assembly::updateGeometry + updateForceState (and updateRR when with_rr), with the scalar record
+// copied to p.scal_host: a graph launch once captured, else the three launches and the copy
+cudaError_t enqueue_force_state(Problem &p, bool with_rr)
+{
+    if (!p.graphs_off && !p.fs_graph[with_rr ? 1 : 0])
+        capture_force_state(p, with_rr);
+    if (cudaGraphExec_t g = p.graphs_off ? nullptr : p.fs_graph[with_rr ? 1 : 0])
+    {
+        const cudaError_t e = cudaGraphLaunch(g, p.stream);
+        if (e == cudaSuccess)
+            p.ctr.kernel_launches += 3; // k_geometry_force, k_internal_force, k_finalize_rr
+        return e;
+    }
+    return enqueue_force_state_direct(p, with_rr);
 }
 
 cudaError_t enqueue_assemble(Problem &p, bool apply_bc)
@@ -516,6 +563,12 @@ int32_t lpmgpu_generate_lattice(int32_t lattice, double radius, const double box
 
 static void free_problem(Problem &p)
 {
+    for (auto &g : p.fs_graph)
+        if (g)
+        {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
     for (void *v : p.allocs)
         cudaFree(v);
     p.allocs.clear();
@@ -577,6 +630,7 @@ int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
         CKF(cudaEventCreate(&e));
     for (auto &e : p.cg_ev)
         CKF(cudaEventCreate(&e));
+    p.graphs_off = std::getenv("LPMGPU_NO_GRAPHS") != nullptr;
     p.cell = make_cell(d->lattice, d->radius);
     p.n = d->n;
     p.dim = p.cell.dim;
