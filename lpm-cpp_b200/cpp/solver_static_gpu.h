@@ -108,7 +108,14 @@ public:
         : undamaged_pt_type{p_undamaged}, max_NR_iter{p_niter}, tol_NR_iter{p_tol}, dumpFile{p_dumpFile},
           ass(p_ass)
     {
-        (void)p_sol_mode; // CG and PARDISO are both replaced by the device CG
+        // CG and PARDISO are both replaced by the device CG.  For PARDISO, the direct solve of
+        // Solver::LPM_PARDISO (solver.h:191-274), it runs to a relative residual of 1e-12
+        // (squared-norm test 1e-24) instead of the reference CG's 1e-6.
+        if (p_sol_mode == SolverMode::PARDISO)
+        {
+            cg_rtol_ = 1e-24;
+            cg_atol_ = 0.0;
+        }
         if (p_stiff_mode != StiffnessMode::Analytical)
             throw std::runtime_error("SolverStaticGPU supports StiffnessMode::Analytical only");
         create(precision, device);

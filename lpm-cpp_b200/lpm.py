@@ -1009,16 +1009,27 @@ class _StiffnessView:
         raise AttributeError(name)
 
 
+def _cg_tolerances(sol_mode, rtol, atol):
+    """The device CG's squared-norm test for a solver mode: the reference CG's 1e-12 / 1e-12
+    (solver.h:312-313), or for PARDISO (a direct solve, solver.h:191-274) 1e-24 relative."""
+    pardiso = SolverMode(sol_mode) == SolverMode.PARDISO
+    return (rtol if rtol is not None else (1e-24 if pardiso else 1e-12),
+            atol if atol is not None else (0.0 if pardiso else 1e-12))
+
+
 class SolverStatic:
     """SolverStatic<nlayer> (include/solver_static.h:17-29) on the GPU: same constructor
     arguments, same solveProblem(load, start_index) contract; extra keyword arguments choose
-    the precision and CG tolerances."""
+    the precision and CG tolerances.  Both solver modes run the device CG; SolverMode.PARDISO,
+    the reference's direct solve, runs it to a relative residual of 1e-12 unless tolerances are
+    given."""
 
     def __init__(self, undamaged_pt_type: int, ass: Assembly, stiff_mode=StiffnessMode.Analytical,
                  sol_mode=SolverMode.CG, dumpFile: str = "", max_iter: int = 30, tol: float = 1e-5, *,
-                 precision: Precision = Precision.FP64, cg_rtol=1e-12, cg_atol=1e-12, cg_maxit=0, device=0):
+                 precision: Precision = Precision.FP64, cg_rtol=None, cg_atol=None, cg_maxit=0, device=0):
         if StiffnessMode(stiff_mode) != StiffnessMode.Analytical:
             raise ValueError("only StiffnessMode.Analytical is on the device path")
+        cg_rtol, cg_atol = _cg_tolerances(sol_mode, cg_rtol, cg_atol)
         self.ass = ass
         self.dumpFile = dumpFile
         self.max_NR_iter, self.tol_NR_iter = max_iter, tol
@@ -1061,9 +1072,10 @@ class SolverFatigue:
     def __init__(self, undamaged_pt_type: int, ass: Assembly, stiff_mode=StiffnessMode.Analytical,
                  sol_mode=SolverMode.CG, t_mode: TimeMapMode = TimeMapMode.Linear, tau: float = 1.0,
                  dumpFile: str = "", max_iter: int = 30, tol: float = 1e-5, *,
-                 precision: Precision = Precision.FP64, cg_rtol=1e-12, cg_atol=1e-12, cg_maxit=0, device=0):
+                 precision: Precision = Precision.FP64, cg_rtol=None, cg_atol=None, cg_maxit=0, device=0):
         if StiffnessMode(stiff_mode) != StiffnessMode.Analytical:
             raise ValueError("only StiffnessMode.Analytical is on the device path")
+        cg_rtol, cg_atol = _cg_tolerances(sol_mode, cg_rtol, cg_atol)
         self.undamaged_pt_type = undamaged_pt_type
         self.ass = ass
         self.t_mode, self.tau = TimeMapMode(t_mode), float(tau)

@@ -92,3 +92,11 @@ def test_set_particle_property_per_type():
     e.setParticleProperty(0.3, True, 69e3, 0.3, 0.02, 0.5, 10.0, 0.9)
     assert (e.material.k0, e.material.k1, e.material.comp_tensile_ratio, e.material.damage_threshold) == \
         (0.02, 0.5, 10.0, 0.9)
+
+
+def test_solver_modes_map_to_cg_tolerances():
+    """SolverMode.CG keeps the reference CG's test; PARDISO (a direct solve) runs the device CG
+    to 1e-12 relative; explicit tolerances win."""
+    assert LPM._cg_tolerances(LPM.SolverMode.CG, None, None) == (1e-12, 1e-12)
+    assert LPM._cg_tolerances(LPM.SolverMode.PARDISO, None, None) == (1e-24, 0.0)
+    assert LPM._cg_tolerances(LPM.SolverMode.PARDISO, 1e-20, 1e-30) == (1e-20, 1e-30)
