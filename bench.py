@@ -61,6 +61,7 @@ def args_():
     ap.add_argument("--no-tangent", action="store_true", help="skip the FCC J2 tangent-mode leg")
     ap.add_argument("--no-dump", action="store_true", help="skip the per-step dump output leg")
     ap.add_argument("--no-fatigue", action="store_true", help="skip the fatigue (SolverFatigue) leg")
+    ap.add_argument("--no-direct", action="store_true", help="skip the direct-solver (SolverMode::PARDISO) leg")
     ap.add_argument("--autotune", action="store_true",
                     help="tune the CG grid of the headline problem after the first warm-up step (lpmgpu_autotune)")
     ap.add_argument("--tangent-steps", type=int, default=4, help="load steps of the FCC bar's 50-step path timed")
@@ -348,6 +349,9 @@ def run_ours(a):
     fatigue = None
     if single and not a.no_fatigue:
         fatigue = fatigue_leg(lpm, local)
+    direct = None
+    if single and not a.no_direct:
+        direct = direct_leg(lpm, local)
 
     if rank == 0:
         line = {
@@ -368,7 +372,7 @@ def run_ours(a):
                                    "cg_kernel": cg_s * 1e3 / K},
             "roofline": roof, "e2e": e2e, "gpu_launches": counters_total, "clocks": clocks,
             "mixed": mixed, "batched": batched, "serving": serving, "tangent": tangent, "dump": dump,
-            "fatigue": fatigue,
+            "fatigue": fatigue, "direct": direct,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -418,6 +422,44 @@ def dump_leg(lpm, case, first_step, device, steps=3):
         return {"error": f"{type(ex).__name__}: {ex}"}
     finally:
         shutil.rmtree(d, ignore_errors=True)
+
+
+def direct_leg(lpm, device, sizes=(10.0, 20.0), steps=3):
+    """The direct solver (SolverMode::PARDISO's role; lpmgpu_desc.direct = 1) against the CG on
+    the hexagonal plate of config 1 (r = 0.1 mm, 10 x 10 mm: 2,900 particles; 20 x 20 mm: 11,500),
+    `steps` load steps of 0.001 mm at Newton tolerance 1e-8, the CG at 1e-24 on squared norms.
+    Device time of the library's stream per load step; the first step of the direct path includes
+    the ordering and the band's allocation.  Error: the direct displacements against the CG's."""
+    try:
+        import torch
+        cfg = importlib.import_module("lpm-cpp_b200.configs")
+        out = {}
+        for size in sizes:
+            c = cfg.hex_plate(size=size, radius=0.1, steps=steps, total_disp=0.001 * steps, tol_iter=NEWTON_TOL)
+            row, xyz = {}, {}
+            for key, mode in (("cg", 0), ("direct", 1)):
+                g = lpm.GpuProblem(c.assembly(), undamaged_pt_type=c.undamaged_type, max_iter=c.max_iter,
+                                   tol_iter=c.tol_iter, cg_rtol=1e-24, cg_atol=0.0, device=device, direct=mode)
+                s0 = torch.cuda.ExternalStream(g.stream_ptr())
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(s0)
+                newton = 0
+                for s in range(steps):
+                    ok, st = g.solve_load_step(c.load_step(s))
+                    assert ok, f"{key} step {s} failed"
+                    newton += st["newton_solves"]
+                e1.record(s0)
+                torch.cuda.synchronize()
+                row[key] = {"ms_per_step": e0.elapsed_time(e1) / steps, "newton_per_step": newton / steps}
+                xyz[key] = g.state(("xyz",))["xyz"] - c.xyz
+                g.close()
+            row["rel_disp_diff_direct_vs_cg"] = float(np.linalg.norm(xyz["direct"] - xyz["cg"]) /
+                                                      np.linalg.norm(xyz["cg"]))
+            out[f"hex_{size:g}mm_{c.n}"] = row
+        return out
+    except Exception as ex:  # the leg must not cost the bench line
+        return {"error": f"{type(ex).__name__}: {ex}"}
 
 
 def fatigue_leg(lpm, device, size=25.0, cycles=4):

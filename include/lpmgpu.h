@@ -36,7 +36,8 @@ typedef enum
     LPMGPU_ERR_BUDGET = 8,        /* request larger than the server's HBM budget */
     LPMGPU_ERR_CUTS = 9,          /* a load step was halved more than 30 times */
     LPMGPU_ERR_NOT_READY = 10,    /* server: result not available yet */
-    LPMGPU_ERR_NO_DEVICE = 11     /* no CUDA device; the library has no CPU fallback */
+    LPMGPU_ERR_NO_DEVICE = 11,    /* no CUDA device; the library has no CPU fallback */
+    LPMGPU_ERR_NOT_SPD = 12       /* direct solve: the stiffness is not positive definite */
 } lpmgpu_status;
 
 /* LatticeType (include/lpm.h:97-106); BCC3D covers the three BCC enum values */
@@ -104,6 +105,11 @@ typedef struct
      * which searchNonlocalNeighbors ran (assembly.h:118-130) holds them.  Not together with
      * nonlocal_cutoff_ratio > 0. */
     const int32_t *nonlocal_count, *nonlocal_ids;
+    /* Linear solver of the Newton iterations.  0: the CG (Solver::LPM_CG).  1: the direct band
+     * Cholesky (lpmgpu_solve_direct; Solver::LPM_PARDISO's role, solver.h:191-274).  2: the
+     * direct solve when its band fits (at most 32 GiB), else the CG; the C++ and Python drop-ins
+     * use 2 for SolverMode::PARDISO.  The direct solve is FP64 whatever the precision. */
+    int32_t direct;
 } lpmgpu_desc;
 
 /* Displacement / force boundary condition of one load step (boundary.h:10-44, Relative mode). */
@@ -200,6 +206,18 @@ int32_t lpmgpu_solve_load_step(lpmgpu_solver *h, const lpmgpu_load_step *step, l
 /* Assembly::storeStateVar / resetStateVar(true) (assembly.h:141-159) */
 int32_t lpmgpu_store_state(lpmgpu_solver *h);
 int32_t lpmgpu_reset_state(lpmgpu_solver *h);
+
+/* Direct solve of the current K and residual into disp (host, dim*n; may be NULL), whatever
+ * desc.direct says: reverse Cuthill-McKee ordering of the particles (once), the BC-eliminated K
+ * into a band, a blocked band Cholesky (once per assembled K) and the two substitutions on the
+ * device.  The replacement of Solver::LPM_PARDISO (solver.h:191-274), which refactors the
+ * matrix at every call.  LPMGPU_ERR_OUT_OF_MEMORY when the band exceeds 32 GiB (wide 3D
+ * problems), LPMGPU_ERR_NOT_SPD for a pivot that is not positive. */
+int32_t lpmgpu_solve_direct(lpmgpu_solver *h, double *disp, lpmgpu_stats *stats);
+/* The ordering the direct solve uses, on any graph in CSR (host only, no device): rank[i] is
+ * vertex i's position under reverse Cuthill-McKee, *bandwidth the largest |rank(i) - rank(j)|
+ * over the edges. */
+int32_t lpmgpu_band_order(int32_t n, const int32_t *start, const int32_t *adj, int32_t *rank, int64_t *bandwidth);
 
 /* SolverFatigue (include/solver_fatigue.h) on the device.  The cycle loop itself
  * (solveProblemCyclic: readLoad, generateLoadCycle, the dN/dt time map) is host logic and stays

@@ -108,11 +108,12 @@ public:
         : undamaged_pt_type{p_undamaged}, max_NR_iter{p_niter}, tol_NR_iter{p_tol}, dumpFile{p_dumpFile},
           ass(p_ass)
     {
-        // CG and PARDISO are both replaced by the device CG.  For PARDISO, the direct solve of
-        // Solver::LPM_PARDISO (solver.h:191-274), it runs to a relative residual of 1e-12
-        // (squared-norm test 1e-24) instead of the reference CG's 1e-6.
+        // SolverMode::PARDISO, the direct solve of Solver::LPM_PARDISO (solver.h:191-274): the
+        // device's band Cholesky where its band fits, else the device CG to a relative residual
+        // of 1e-12 (squared-norm test 1e-24) instead of the reference CG's 1e-6.
         if (p_sol_mode == SolverMode::PARDISO)
         {
+            direct_ = 2;
             cg_rtol_ = 1e-24;
             cg_atol_ = 0.0;
         }
@@ -189,6 +190,7 @@ protected:
     lpmgpu_solver *h_{nullptr};
     int precision_{LPMGPU_FP64}, device_{0};
     double cg_rtol_{1e-12}, cg_atol_{1e-12};
+    int direct_{0}; // lpmgpu_desc.direct
     bool rebuild_needed_{false};
 
     struct CStep
@@ -322,6 +324,7 @@ protected:
         d.cg_atol = cg_atol_;
         d.precision = precision_;
         d.device = device_;
+        d.direct = direct_;
         d.bond_nb0 = nb0.data();
         d.bond_nb1 = nb1.data();
         d.bond_p2 = p2.data();

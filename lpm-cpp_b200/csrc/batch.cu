@@ -1523,6 +1523,11 @@ int32_t lpmgpu_batch_add(lpmgpu_batch *b, lpmgpu_solver *h, const lpmgpu_load_st
         set_last_error("the problem lives on another device than the batch");
         return LPMGPU_ERR_INVALID_ARG;
     }
+    if (h->p.desc.direct == 1)
+    {
+        set_last_error("the batch solves its members by the batched CG; a problem with desc.direct = 1 cannot join");
+        return LPMGPU_ERR_INVALID_ARG;
+    }
     int live = 0;
     for (auto &up : b->members)
     {

@@ -126,6 +126,13 @@ struct Problem
     // captured at first use, replayed afterwards (graphs_off: capture failed or LPMGPU_NO_GRAPHS)
     cudaGraphExec_t fs_graph[2] = {nullptr, nullptr};
     bool graphs_off = false;
+    // K's version, raised by every assembly; the direct solver's band factor is valid for one
+    int64_t k_version = 0;
+    // direct solver (direct.cu): RCM rank of each particle, the band (factor) and its workspace
+    int *band_rank = nullptr, *band_fail = nullptr;
+    double *band_ab = nullptr, *band_y = nullptr;
+    int64_t band_kd = 0, band_factored = -1;
+    bool direct_off = false; // desc.direct == 2 and the band did not fit: the CG solves
 };
 
 constexpr int kMaxGridBlocks = 4096;
@@ -163,6 +170,8 @@ struct CGResult
 };
 // Solves K x = res (current residual) into p.x with the reference's stopping rule.
 cudaError_t solve_linear(Problem &p, CGResult &out);
+// The same system by the band Cholesky (direct.cu); returns an LPMGPU status.
+int32_t solve_direct(Problem &p);
 
 // Pieces of the mixed-precision refinement, enqueued on p.stream without a host wait:
 // r = res - K x with ||r||^2 copied to a pinned slot (read after the stream is synchronised),

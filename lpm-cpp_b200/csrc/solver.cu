@@ -112,6 +112,7 @@ cudaError_t enqueue_force_state(Problem &p, bool with_rr)
 
 cudaError_t enqueue_assemble(Problem &p, bool apply_bc)
 {
+    p.k_version++;
     cudaError_t e = launch_assemble(p, apply_bc);
     if (e == cudaSuccess && p.desc.precision == LPMGPU_MIXED)
         e = launch_k_to_f32(p);
@@ -155,8 +156,37 @@ static int32_t assemble(Problem &p, bool apply_bc)
     return LPMGPU_OK;
 }
 
+// The direct solve in place of the CG (desc.direct 1, or 2 while its band fits)
+static int32_t linear_solve_direct(Problem &p, lpmgpu_stats *st, bool *used)
+{
+    *used = false;
+    if (!p.desc.direct || p.direct_off)
+        return LPMGPU_OK;
+    CK(cudaEventRecord(p.ev[4], p.stream));
+    const int32_t r = solve_direct(p);
+    if (r == LPMGPU_ERR_OUT_OF_MEMORY && p.desc.direct == 2 && !p.band_ab)
+    {
+        p.direct_off = true; // the band does not fit: the CG from now on
+        return LPMGPU_OK;
+    }
+    ST(r);
+    CK(cudaEventRecord(p.ev[5], p.stream));
+    CK(cudaEventSynchronize(p.ev[5]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, p.ev[4], p.ev[5]);
+    p.phase_s[2] += ms * 1e-3;
+    if (st)
+        st->newton_solves++;
+    *used = true;
+    return LPMGPU_OK;
+}
+
 static int32_t linear_solve(Problem &p, lpmgpu_stats *st)
 {
+    bool direct = false;
+    ST(linear_solve_direct(p, st, &direct));
+    if (direct)
+        return LPMGPU_OK;
     CGResult r;
     CK(cudaEventRecord(p.ev[4], p.stream));
     CK(solve_linear(p, r));
@@ -544,6 +574,7 @@ const char *lpmgpu_status_string(int32_t s)
     case LPMGPU_ERR_CUTS: return "load step halved too many times";
     case LPMGPU_ERR_NOT_READY: return "result not ready";
     case LPMGPU_ERR_NO_DEVICE: return "no CUDA device";
+    case LPMGPU_ERR_NOT_SPD: return "stiffness not positive definite";
     default: return "unknown status";
     }
 }
@@ -591,7 +622,7 @@ int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
     if (!d || !out || !d->xyz || d->n <= 0 || d->lattice < 0 || d->lattice > LPMGPU_BCC3D ||
         (d->ptype != LPMGPU_ELASTIC && d->ptype != LPMGPU_ELASTIC_DAMAGE && d->ptype != LPMGPU_J2 &&
          d->ptype != LPMGPU_FATIGUE_HCF) ||
-        !(d->radius > 0) || d->max_iter < 0 || d->nonlocal_cutoff_ratio < 0)
+        !(d->radius > 0) || d->max_iter < 0 || d->nonlocal_cutoff_ratio < 0 || d->direct < 0 || d->direct > 2)
         return LPMGPU_ERR_INVALID_ARG;
     *out = nullptr;
     int ndev = 0;
@@ -880,6 +911,31 @@ int32_t lpmgpu_solve_linear(lpmgpu_solver *h, double *disp, lpmgpu_stats *st)
     if (st)
         std::memset(st, 0, sizeof *st);
     ST(linear_solve(p, st));
+    if (disp)
+        CK(cudaMemcpy(disp, p.x, sizeof(double) * p.n * p.dim, cudaMemcpyDeviceToHost));
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_solve_direct(lpmgpu_solver *h, double *disp, lpmgpu_stats *st)
+{
+    if (!h)
+        return LPMGPU_ERR_INVALID_ARG;
+    Problem &p = h->p;
+    CK(cudaSetDevice(p.device));
+    if (st)
+        std::memset(st, 0, sizeof *st);
+    CK(cudaEventRecord(p.ev[4], p.stream));
+    ST(solve_direct(p));
+    CK(cudaEventRecord(p.ev[5], p.stream));
+    CK(cudaEventSynchronize(p.ev[5]));
+    if (st)
+    {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p.ev[4], p.ev[5]);
+        st->newton_solves = 1;
+        st->converged = 1;
+        st->seconds = ms * 1e-3;
+    }
     if (disp)
         CK(cudaMemcpy(disp, p.x, sizeof(double) * p.n * p.dim, cudaMemcpyDeviceToHost));
     return LPMGPU_OK;

@@ -62,7 +62,8 @@ class Precision(enum.IntEnum):
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory",
           4: "Newton iteration did not converge", 5: "CG reached its iteration cap",
           6: "device wait timed out", 7: "unsupported particle topology", 8: "HBM budget exceeded",
-          9: "load step halved too many times", 10: "result not ready", 11: "no CUDA device"}
+          9: "load step halved too many times", 10: "result not ready", 11: "no CUDA device",
+          12: "stiffness not positive definite"}
 OK, ERR_NEWTON, ERR_CUTS, ERR_NOT_READY = 0, 4, 9, 10
 
 
@@ -95,6 +96,7 @@ class Desc(C.Structure):
         ("fatigue_A", C.c_double), ("fatigue_B", C.c_double), ("fatigue_d", C.c_double),
         ("fatigue_limit_ratio", C.c_double),
         ("nonlocal_count", C.POINTER(C.c_int32)), ("nonlocal_ids", C.POINTER(C.c_int32)),
+        ("direct", C.c_int32),
     ]
 
 
@@ -194,6 +196,7 @@ EXPORTS = [
     "lpmgpu_fatigue_solve_step", "lpmgpu_fatigue_static_step", "lpmgpu_fatigue_update_damage", "lpmgpu_fatigue_cycle",
     "lpmgpu_read_state", "lpmgpu_read_residual", "lpmgpu_set_xyz", "lpmgpu_get_phase_times",
     "lpmgpu_get_counters", "lpmgpu_get_stream", "lpmgpu_cg_bsr_noalloc", "lpmgpu_autotune", "lpmgpu_set_cg_grid",
+    "lpmgpu_solve_direct", "lpmgpu_band_order",
     "lpmgpu_format_dump", "lpmgpu_dump_write", "lpmgpu_dump_flush",
     "lpmgpu_batch_create", "lpmgpu_batch_destroy", "lpmgpu_batch_add", "lpmgpu_batch_round", "lpmgpu_batch_run",
     "lpmgpu_batch_member", "lpmgpu_batch_member_steps", "lpmgpu_batch_remove", "lpmgpu_batch_get_stats",
@@ -247,6 +250,8 @@ def lib():
         "lpmgpu_dump_write": (C.c_int32, [vp, C.c_char_p, C.c_int32, dp, C.c_int32, C.c_int32]),
         "lpmgpu_dump_flush": (C.c_int32, [vp]),
         "lpmgpu_autotune": (C.c_int32, [vp, C.c_int32, C.POINTER(TuneResult)]),
+        "lpmgpu_solve_direct": (C.c_int32, [vp, dp, C.POINTER(Stats)]),
+        "lpmgpu_band_order": (C.c_int32, [C.c_int32, ip, ip, ip, lp]),
         "lpmgpu_set_cg_grid": (C.c_int32, [vp, C.c_int32]),
         "lpmgpu_cg_bsr_noalloc": (C.c_int32, [C.c_int32, C.c_int32, vp, vp, vp, vp, vp, C.c_double, C.c_double,
                                               C.c_int64, vp, C.POINTER(C.c_int64)]),
@@ -618,7 +623,7 @@ class _CStep:
 
 # ---------------------------------------------------------------------------- solver
 def _pack_desc(ass: Assembly, undamaged_pt_type=-1, max_iter=30, tol_iter=1e-5, precision=0, cg_rtol=1e-12,
-               cg_atol=1e-12, cg_maxit=0, device=0, tangent=False):
+               cg_atol=1e-12, cg_maxit=0, device=0, tangent=False, direct=0):
     """lpmgpu_desc of an Assembly and solver settings; returns (desc, arrays the desc points into)."""
     m = ass.material
     d = Desc()
@@ -632,6 +637,7 @@ def _pack_desc(ass: Assembly, undamaged_pt_type=-1, max_iter=30, tol_iter=1e-5, 
     d.cg_rtol, d.cg_atol, d.cg_maxit = float(cg_rtol), float(cg_atol), int(cg_maxit)
     d.precision, d.device = int(precision), int(device)
     d.tangent = int(bool(tangent))
+    d.direct = int(direct)
     d.nonlocal_cutoff_ratio = float(getattr(ass, "nonlocal_cutoff_ratio", 0.0))
     d.k0, d.k1, d.comp_tensile_ratio, d.damage_threshold = m.k0, m.k1, m.comp_tensile_ratio, m.damage_threshold
     d.fatigue_A, d.fatigue_B, d.fatigue_d = m.fatigue_A, m.fatigue_B, m.fatigue_d
@@ -654,13 +660,15 @@ class GpuProblem:
 
     def __init__(self, ass: Assembly, undamaged_pt_type=-1, max_iter=30, tol_iter=1e-5,
                  precision: Precision = Precision.FP64, cg_rtol=1e-12, cg_atol=1e-12, cg_maxit=0, device=0,
-                 tangent: bool = False):
+                 tangent: bool = False, direct: int = 0):
         """tangent: re-assemble K from the current state before every Newton solve (the
-        default keeps K fixed per load step, as SolverStatic does)."""
+        default keeps K fixed per load step, as SolverStatic does).  direct: the linear solver
+        of the Newton iterations, 0 the CG, 1 the band Cholesky, 2 the band Cholesky when its
+        band fits, else the CG (lpmgpu_desc.direct)."""
         L = lib()
         self.ass = ass
         d, self._keep = _pack_desc(ass, undamaged_pt_type, max_iter, tol_iter, precision, cg_rtol, cg_atol, cg_maxit,
-                                   device, tangent)
+                                   device, tangent, direct)
         h = C.c_void_p()
         _check(L.lpmgpu_create(C.byref(d), C.byref(h)), "lpmgpu_create")
         self._h = h
@@ -713,6 +721,14 @@ class GpuProblem:
 
     def assemble(self, apply_bc=True):
         _check(lib().lpmgpu_assemble(self._h, int(apply_bc)), "lpmgpu_assemble")
+
+    def solve_direct(self):
+        """The band Cholesky solve of the current K and residual (lpmgpu_solve_direct): the
+        displacement increment."""
+        disp = np.zeros(self.dim * self.n)
+        st = Stats()
+        _check(lib().lpmgpu_solve_direct(self._h, _dp(disp), C.byref(st)), "lpmgpu_solve_direct")
+        return disp, st.as_dict()
 
     def solve_linear(self):
         disp = np.zeros(self.dim * self.n)
@@ -1009,6 +1025,12 @@ class _StiffnessView:
         raise AttributeError(name)
 
 
+def _direct_mode(sol_mode) -> int:
+    """SolverMode.PARDISO (the reference's direct solve, solver.h:191-274): the band Cholesky
+    where its band fits, else the CG (lpmgpu_desc.direct = 2); SolverMode.CG: the CG."""
+    return 2 if SolverMode(sol_mode) == SolverMode.PARDISO else 0
+
+
 def _cg_tolerances(sol_mode, rtol, atol):
     """The device CG's squared-norm test for a solver mode: the reference CG's 1e-12 / 1e-12
     (solver.h:312-313), or for PARDISO (a direct solve, solver.h:191-274) 1e-24 relative."""
@@ -1020,9 +1042,9 @@ def _cg_tolerances(sol_mode, rtol, atol):
 class SolverStatic:
     """SolverStatic<nlayer> (include/solver_static.h:17-29) on the GPU: same constructor
     arguments, same solveProblem(load, start_index) contract; extra keyword arguments choose
-    the precision and CG tolerances.  Both solver modes run the device CG; SolverMode.PARDISO,
-    the reference's direct solve, runs it to a relative residual of 1e-12 unless tolerances are
-    given."""
+    the precision and CG tolerances.  SolverMode.PARDISO, the reference's direct solve, runs the
+    device's band Cholesky where its band fits, else the CG to a relative residual of 1e-12
+    (unless tolerances are given)."""
 
     def __init__(self, undamaged_pt_type: int, ass: Assembly, stiff_mode=StiffnessMode.Analytical,
                  sol_mode=SolverMode.CG, dumpFile: str = "", max_iter: int = 30, tol: float = 1e-5, *,
@@ -1034,7 +1056,7 @@ class SolverStatic:
         self.dumpFile = dumpFile
         self.max_NR_iter, self.tol_NR_iter = max_iter, tol
         self.problem = GpuProblem(ass, undamaged_pt_type, max_iter, tol, precision, cg_rtol, cg_atol, cg_maxit,
-                                  device)
+                                  device, direct=_direct_mode(sol_mode))
         self.stiffness = _StiffnessView(self.problem)
         self.history: List[dict] = []
 
@@ -1082,7 +1104,7 @@ class SolverFatigue:
         self.dumpFile = dumpFile
         self.load_spectrum: List[float] = []
         self.problem = GpuProblem(ass, undamaged_pt_type, max_iter, tol, precision, cg_rtol, cg_atol, cg_maxit,
-                                  device)
+                                  device, direct=_direct_mode(sol_mode))
         self.stiffness = _StiffnessView(self.problem)
         self.history: List[dict] = []
 
