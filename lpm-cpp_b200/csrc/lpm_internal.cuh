@@ -125,6 +125,8 @@ struct Problem
     // record's copy) as CUDA graphs, without / with the reaction accumulation of updateRR;
     // captured at first use, replayed afterwards (graphs_off: capture failed or LPMGPU_NO_GRAPHS)
     cudaGraphExec_t fs_graph[2] = {nullptr, nullptr};
+    // Assembly::storeStateVar / resetStateVar(true) (seven copies each) as graphs
+    cudaGraphExec_t state_graph[2] = {nullptr, nullptr};
     bool graphs_off = false;
     // K's version, raised by every assembly; the direct solver's band factor is valid for one
     int64_t k_version = 0;

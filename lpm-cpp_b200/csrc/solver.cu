@@ -64,50 +64,55 @@ static cudaError_t enqueue_force_state_direct(Problem &p, bool with_rr)
     return e;
 }
 
-// Captures the force-state sequence of enqueue_force_state_direct into an executable graph.  Its
-// kernels read only the problem's fixed device buffers and constants, so one capture per value of
-// with_rr serves every later call.  On any failure the problem goes back to direct launches.
-static void capture_force_state(Problem &p, bool with_rr)
+// A fixed sequence of the problem's work, captured into an executable graph at its first call and
+// replayed afterwards.  The sequences given here read and write only the problem's own device
+// buffers with constant arguments, so one capture serves every later call.  On any failure of the
+// capture the problem goes back to direct launches for good.
+template <typename F>
+static cudaError_t run_graph(Problem &p, cudaGraphExec_t &slot, int kernels, F enqueue_direct)
 {
-    const int64_t launches = p.ctr.kernel_launches;
-    cudaGraph_t graph = nullptr;
-    cudaError_t e = cudaStreamBeginCapture(p.stream, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess)
+    if (!p.graphs_off && !slot)
     {
-        const cudaError_t e1 = enqueue_force_state_direct(p, with_rr);
-        e = cudaStreamEndCapture(p.stream, &graph);
+        const int64_t launches = p.ctr.kernel_launches;
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(p.stream, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess)
-            e = e1;
+        {
+            const cudaError_t e1 = enqueue_direct(p);
+            e = cudaStreamEndCapture(p.stream, &graph);
+            if (e == cudaSuccess)
+                e = e1;
+        }
+        p.ctr.kernel_launches = launches;
+        cudaGraphExec_t exec = nullptr;
+        if (e == cudaSuccess && graph)
+            e = cudaGraphInstantiate(&exec, graph, 0);
+        if (graph)
+            cudaGraphDestroy(graph);
+        if (e != cudaSuccess || !exec)
+        {
+            p.graphs_off = true;
+            (void)cudaGetLastError(); // the failed capture's error is not the caller's
+        }
+        else
+            slot = exec;
     }
-    p.ctr.kernel_launches = launches;
-    cudaGraphExec_t exec = nullptr;
-    if (e == cudaSuccess && graph)
-        e = cudaGraphInstantiate(&exec, graph, 0);
-    if (graph)
-        cudaGraphDestroy(graph);
-    if (e != cudaSuccess || !exec)
+    if (!p.graphs_off && slot)
     {
-        p.graphs_off = true;
-        (void)cudaGetLastError(); // the failed capture's error is not the caller's
-        return;
+        const cudaError_t e = cudaGraphLaunch(slot, p.stream);
+        if (e == cudaSuccess)
+            p.ctr.kernel_launches += kernels;
+        return e;
     }
-    p.fs_graph[with_rr ? 1 : 0] = exec;
+    return enqueue_direct(p);
 }
 
 // Assembly::updateGeometry + updateForceState (and updateRR when with_rr), with the scalar record
-// copied to p.scal_host: a graph launch once captured, else the three launches and the copy
+// copied to p.scal_host: k_geometry_force, k_internal_force, k_finalize_rr and the copy
 cudaError_t enqueue_force_state(Problem &p, bool with_rr)
 {
-    if (!p.graphs_off && !p.fs_graph[with_rr ? 1 : 0])
-        capture_force_state(p, with_rr);
-    if (cudaGraphExec_t g = p.graphs_off ? nullptr : p.fs_graph[with_rr ? 1 : 0])
-    {
-        const cudaError_t e = cudaGraphLaunch(g, p.stream);
-        if (e == cudaSuccess)
-            p.ctr.kernel_launches += 3; // k_geometry_force, k_internal_force, k_finalize_rr
-        return e;
-    }
-    return enqueue_force_state_direct(p, with_rr);
+    return run_graph(p, p.fs_graph[with_rr ? 1 : 0], 3,
+                     [with_rr](Problem &q) { return enqueue_force_state_direct(q, with_rr); });
 }
 
 cudaError_t enqueue_assemble(Problem &p, bool apply_bc)
@@ -241,7 +246,7 @@ static int32_t newton(Problem &p, lpmgpu_stats *st, int *ni)
     return LPMGPU_OK;
 }
 
-cudaError_t enqueue_store_state(Problem &p)
+static cudaError_t enqueue_store_state_direct(Problem &p)
 {
     const size_t n = p.n, nb = (size_t)p.nbonds;
     cudaError_t e = cudaSuccess;
@@ -256,7 +261,7 @@ cudaError_t enqueue_store_state(Problem &p)
     return e;
 }
 
-cudaError_t enqueue_reset_state(Problem &p)
+static cudaError_t enqueue_reset_state_direct(Problem &p)
 {
     const size_t n = p.n, nb = (size_t)p.nbonds;
     cudaError_t e = cudaSuccess;
@@ -269,6 +274,16 @@ cudaError_t enqueue_reset_state(Problem &p)
     for (int k = 0; k < 7 && e == cudaSuccess; ++k)
         e = cudaMemcpyAsync(cp[k].first, cp[k].second, bytes[k], cudaMemcpyDeviceToDevice, p.stream);
     return e;
+}
+
+cudaError_t enqueue_store_state(Problem &p)
+{
+    return run_graph(p, p.state_graph[0], 0, enqueue_store_state_direct);
+}
+
+cudaError_t enqueue_reset_state(Problem &p)
+{
+    return run_graph(p, p.state_graph[1], 0, enqueue_reset_state_direct);
 }
 
 static int32_t store_state(Problem &p)
@@ -594,12 +609,13 @@ int32_t lpmgpu_generate_lattice(int32_t lattice, double radius, const double box
 
 static void free_problem(Problem &p)
 {
-    for (auto &g : p.fs_graph)
-        if (g)
-        {
-            cudaGraphExecDestroy(g);
-            g = nullptr;
-        }
+    for (auto *slots : {p.fs_graph, p.state_graph})
+        for (int k = 0; k < 2; ++k)
+            if (slots[k])
+            {
+                cudaGraphExecDestroy(slots[k]);
+                slots[k] = nullptr;
+            }
     for (void *v : p.allocs)
         cudaFree(v);
     p.allocs.clear();
