@@ -69,7 +69,7 @@ static cudaError_t enqueue_force_state_direct(Problem &p, bool with_rr)
 // buffers with constant arguments, so one capture serves every later call.  On any failure of the
 // capture the problem goes back to direct launches for good.
 template <typename F>
-static cudaError_t run_graph(Problem &p, cudaGraphExec_t &slot, int kernels, F enqueue_direct)
+static void capture_graph(Problem &p, cudaGraphExec_t &slot, F enqueue_direct)
 {
     if (!p.graphs_off && !slot)
     {
@@ -97,6 +97,12 @@ static cudaError_t run_graph(Problem &p, cudaGraphExec_t &slot, int kernels, F e
         else
             slot = exec;
     }
+}
+
+template <typename F>
+static cudaError_t run_graph(Problem &p, cudaGraphExec_t &slot, int kernels, F enqueue_direct)
+{
+    capture_graph(p, slot, enqueue_direct);
     if (!p.graphs_off && slot)
     {
         const cudaError_t e = cudaGraphLaunch(slot, p.stream);
@@ -284,6 +290,16 @@ cudaError_t enqueue_store_state(Problem &p)
 cudaError_t enqueue_reset_state(Problem &p)
 {
     return run_graph(p, p.state_graph[1], 0, enqueue_reset_state_direct);
+}
+
+// Captures every graph of the problem while nothing else uses its stream (at creation), so no
+// capture later overlaps another thread's work on this problem (the dump writer's waits)
+static void prepare_graphs(Problem &p)
+{
+    for (int rr = 0; rr < 2; ++rr)
+        capture_graph(p, p.fs_graph[rr], [rr](Problem &q) { return enqueue_force_state_direct(q, rr != 0); });
+    capture_graph(p, p.state_graph[0], enqueue_store_state_direct);
+    capture_graph(p, p.state_graph[1], enqueue_reset_state_direct);
 }
 
 static int32_t store_state(Problem &p)
@@ -784,6 +800,7 @@ int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
     CKF(launch_geometry_force(p));
     CKF(launch_update_rr_impl(p, false));
     CKF(cudaStreamSynchronize(p.stream));
+    prepare_graphs(p);
 #undef CKF
     *out = h;
     return LPMGPU_OK;

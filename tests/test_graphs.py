@@ -1,6 +1,6 @@
 """The force-state sequence of every Newton iteration (geometry and bond forces, particle forces
 and the residual, the scalar record's copy) and the state store / reset copies are replayed from
-CUDA graphs captured at first use.
+CUDA graphs captured when the problem is created.
 The graph holds the same kernels with the same arguments as the direct launches, so a load path
 solved with it is bit-identical to one solved with LPMGPU_NO_GRAPHS set, with the same kernel
 count."""
