@@ -273,13 +273,15 @@ def edamage_plate(size=2.4, radius=0.1, E=69e3, mu=0.3, steps=4, total_disp=0.00
 
 def fatigue_plate(size=2.4, radius=0.1, E=69e3, mu=0.3, amplitude=0.004, cycles=8, n_interval=2, tau=0.5,
                   tmode="linear", A=15.0, B=2.833, d=0.5, damage_threshold=1.0, fatigue_limit_ratio=1.108,
-                  nonlocal_L=0.3, cutoff_ratio=1.5, tol_iter=1e-9, max_iter=30) -> Case:
+                  nonlocal_L=0.3, cutoff_ratio=1.5, tol_iter=1e-9, max_iter=30, load_type="uniaxial_disp") -> Case:
     """Hexagonal plate of ParticleFatigueHCF particles (include/particle_fatigue_hcf.h) under the
     constant-amplitude displacement cycles of SolverFatigue (include/solver_fatigue.h) with the
     LoadUniaxialDisp cycle (include/load_step_fatigue.h:39-50): left edge fixed in x, bottom edge
     in y, top edge moved in y.  One static step first (solveProblemStatic at f_min = 0, which
     sets the constraints, as ex5_isoelasticity_2d_fatigue.cpp does before its cycles), then the
-    spectrum 0, amplitude, 0, amplitude, ..., 0 of `cycles` cycles.  Each simulated cycle stands
+    spectrum 0, amplitude, 0, amplitude, ..., 0 of `cycles` cycles.  load_type "uniaxial_force"
+    takes the LoadUniaxialForce cycle instead (load_step_fatigue.h:23-36): the top edge pulled by a
+    force of `amplitude` N shared by its particles.  Each simulated cycle stands
     for dN/dt = (int)(1 / tau) real cycles (TimeMapMode::Linear, solver_fatigue.h:60-63); the
     damage rate per cycle is A * pow(largest energy, B) * pow(energy range, d), averaged over the
     nonlocal neighbours within cutoff_ratio x nonlocal_L."""
@@ -289,13 +291,16 @@ def fatigue_plate(size=2.4, radius=0.1, E=69e3, mu=0.3, amplitude=0.004, cycles=
     c.ptype = L.ParticleType.FatigueHCF
     x = c.xyz[:, 0]
     c.groups["left"] = np.nonzero(x < x.min() + 1.5 * radius)[0].astype(np.int32)
-    c.steps = [([("left", "x", 0.0), ("top", "y", 0.0), ("bottom", "y", 0.0)], [])]
+    if load_type == "uniaxial_force":  # the top edge stays free in y: the force moves it
+        c.steps = [([("left", "x", 0.0), ("bottom", "y", 0.0)], [])]
+    else:
+        c.steps = [([("left", "x", 0.0), ("top", "y", 0.0), ("bottom", "y", 0.0)], [])]
     m = c.material
     m.fatigue_A, m.fatigue_B, m.fatigue_d = A, B, d
     m.damage_threshold, m.fatigue_limit_ratio, m.nonlocal_L = damage_threshold, fatigue_limit_ratio, nonlocal_L
     c.nonlocal_cutoff_ratio = cutoff_ratio
     spectrum = [0.0] + [v for _ in range(cycles) for v in (amplitude, 0.0)]
-    c.meta["fatigue"] = {"load_type": "uniaxial_disp", "n_interval": n_interval, "tmode": tmode, "tau": tau,
+    c.meta["fatigue"] = {"load_type": load_type, "n_interval": n_interval, "tmode": tmode, "tau": tau,
                          "spectrum": spectrum, "groups": ["left", "top", "bottom"]}
     return c
 

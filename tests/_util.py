@@ -84,6 +84,15 @@ def oracle_load_args(step):
             [(np.asarray(b.group, np.int32), b.fx, b.fy, b.fz) for b in step.forceBCs])
 
 
+def fatigue_disp_scale(case):
+    """A displacement scale for comparing fatigue states: the spectrum's amplitude for a
+    displacement-driven cycle, the particle radius for a force-driven one."""
+    fat = case.meta["fatigue"]
+    if fat["load_type"].endswith("disp"):
+        return max(abs(v) for v in fat["spectrum"])
+    return case.radius
+
+
 def fatigue_cycles(case):
     """The cycles of SolverFatigue::solveProblemCyclic (solver_fatigue.h:183-218) for a fatigue
     case: yields (cycle count N after the cycle, dNdt, the cycle's LoadSteps)."""

@@ -13,7 +13,7 @@ import os
 import numpy as np
 import pytest
 
-from _util import O, fatigue_cycles, oracle_load_args, oracle_problem, oracle_step_args, rel
+from _util import O, fatigue_cycles, fatigue_disp_scale, oracle_load_args, oracle_problem, oracle_step_args, rel
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden")
@@ -119,7 +119,7 @@ def test_oracle_fatigue_cycles(name):
     o = oracle_problem(case, cg_rtol=opts["cg_tol"][0], cg_atol=opts["cg_tol"][1])
     o.update_geometry()
     o.update_force_state()
-    amp = max(abs(v) for v in case.meta["fatigue"]["spectrum"])
+    amp = fatigue_disp_scale(case)
     steps = g["steps"]
     results = []
     for s in range(len(case.steps)):
@@ -141,7 +141,7 @@ def test_oracle_fatigue_cycles(name):
         du = np.abs((so["xyz"] - case.xyz) - (g[f"xyz_{s}"] - g["xyz0"])).max()
         assert du <= 1e-8 * amp, (s, du)
         assert abs(st["reaction_norm"] - steps[s][3]) <= 1e-12 * steps[s][3]
-    assert g[f"damage_{len(steps) - 1}"].max() > 0.5, "damage must grow over the cycles"
+    assert g[f"damage_{len(steps) - 1}"].max() > 0.1, "damage must grow over the cycles"
 
 
 def test_oracle_forces_bit_exact():
