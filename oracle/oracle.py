@@ -392,7 +392,7 @@ def write_bond_file(path: str, nb0, nb1, p2):
 
 
 def write_ref_spec(case, outdir: str, steps=None, max_iter=None, tol_iter=None, cg_tol=None, cg_maxit_cap=0,
-                   dump_k=(), loop="step", use_generator=True, tangent=False) -> str:
+                   dump_k=(), loop="step", use_generator=True, tangent=False, solver="cg") -> str:
     """Spec text for oracle/_ref/lpm_ref describing a product-side ``Case`` (duck-typed):
     groups and particle types are passed as raw int32 id files so both sides see the same sets.
     With use_generator the reference generates the lattice itself (its ids must then equal
@@ -418,6 +418,8 @@ def write_ref_spec(case, outdir: str, steps=None, max_iter=None, tol_iter=None, 
         lines.append(f"cg_maxit_cap {int(cg_maxit_cap)}")
     if tangent:
         lines.append("tangent 1")
+    if solver != "cg":
+        lines.append(f"solver {solver}")
     if cg_tol is not None:
         lines.append(f"cg_tol {cg_tol[0]!r} {cg_tol[1]!r}")
     if not use_generator or lat == "bcc3d":

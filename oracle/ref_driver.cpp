@@ -57,6 +57,8 @@
  *                          cycle count N and dNdt after each cycle.
  *   fatigue_groups G0 G1 [G2]   (the pt_groups of solveProblemCyclic)
  *   fatigue_load PATH     (the load spectrum, SolverFatigue::readLoad)
+ *   solver cg|pardiso     (the SolverMode of the solver: Solver::LPM_CG or Solver::LPM_PARDISO,
+ *                          include/solver.h:191-354; default cg)
  */
 #include <cstdio>
 #include <cstdlib>
@@ -157,6 +159,7 @@ struct Spec
     int fatigue_interval = 1;
     double fatigue_tau = 1;
     std::vector<std::string> fatigue_groups;
+    std::string solver = "cg";
 };
 
 static std::vector<int> read_i32(const std::string &path)
@@ -277,6 +280,7 @@ static Spec parse(const char *path)
         else if (k == "hcf") is >> s.hcf_A >> s.hcf_B >> s.hcf_d >> s.hcf_thres >> s.hcf_flr;
         else if (k == "fatigue") is >> s.fatigue_type >> s.fatigue_interval >> s.fatigue_tmode >> s.fatigue_tau;
         else if (k == "fatigue_load") is >> s.fatigue_load;
+        else if (k == "solver") is >> s.solver;
         else if (k == "fatigue_groups")
         {
             std::string g;
@@ -483,7 +487,8 @@ static int run_fatigue(Assembly<NL> &ass, std::map<std::string, std::vector<Part
                        std::vector<LoadStep<NL>> &load, const Spec &sp, int N, int dim, double setup_s)
 {
     const TimeMapMode tm = (sp.fatigue_tmode == "exponential") ? TimeMapMode::Exponential : TimeMapMode::Linear;
-    LPM_FATIGUE_SOLVER<NL> solv{sp.undamaged_type, ass, StiffnessMode::Analytical, SolverMode::CG, tm, sp.fatigue_tau,
+    const SolverMode sm = (sp.solver == "pardiso") ? SolverMode::PARDISO : SolverMode::CG;
+    LPM_FATIGUE_SOLVER<NL> solv{sp.undamaged_type, ass, StiffnessMode::Analytical, sm, tm, sp.fatigue_tau,
                                 sp.dumpfile, sp.max_iter, sp.tol_iter};
 #ifdef LPM_USE_GPU
     if (sp.cg_rtol >= 0 || sp.cg_atol >= 0)
@@ -696,7 +701,8 @@ int main(int argc, char **argv)
     if (sp.init_state_var)
         ass.updateStateVar();
 
-    LPM_SOLVER<NL> solv{sp.undamaged_type, ass, StiffnessMode::Analytical, SolverMode::CG, sp.dumpfile,
+    const SolverMode sm = (sp.solver == "pardiso") ? SolverMode::PARDISO : SolverMode::CG;
+    LPM_SOLVER<NL> solv{sp.undamaged_type, ass, StiffnessMode::Analytical, sm, sp.dumpfile,
                         sp.max_iter, sp.tol_iter};
 #ifdef LPM_USE_GPU
     if (sp.cg_rtol >= 0 || sp.cg_atol >= 0)

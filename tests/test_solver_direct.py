@@ -84,3 +84,34 @@ def test_solver_static_pardiso_mode_uses_the_direct_solve():
     u = solv.problem.state(("xyz",))["xyz"] - case.xyz
     assert rel(u, g.state(("xyz",))["xyz"] - case.xyz) <= 1e-9
     g.close()
+
+
+@pytest.mark.parametrize("name", ["hex", "hex_damage"])
+def test_solver_static_gpu_pardiso_matches_the_reference(name, tmp_path):
+    """SolverStaticGPU with SolverMode::PARDISO (the device's band Cholesky) against the
+    reference's SolverStatic with SolverMode::PARDISO (Solver::LPM_PARDISO; the MKL stand-in's
+    PARDISO solves to 1e-14): the same driver built both ways.  Per step: displacements within
+    1e-8 relative and the same broken bonds."""
+    import os
+    from _util import O
+    for b in (O.REF_BIN, O.REF_GPU_BIN):
+        if not os.path.exists(b):
+            pytest.skip(f"{os.path.basename(b)} not built (make -C oracle ref ref-gpu)")
+    case = _cases()[name]
+    out = {}
+    for tag, binary in (("cpu", O.REF_BIN), ("gpu", O.REF_GPU_BIN)):
+        d = str(tmp_path / tag)
+        O.run_ref(O.write_ref_spec(case, d, loop="ref", solver="pardiso"), d, threads=1, timeout=900, binary=binary)
+        out[tag] = d
+    x0 = O.read_bin(out["cpu"], "xyz0.f64", np.float64)
+    rc, rg = O.read_ref_steps(out["cpu"]), O.read_ref_steps(out["gpu"])
+    assert len(rc) == len(rg) == len(case.steps)
+    for s in range(len(case.steps)):
+        t = f"{s:03d}"
+        uc = O.read_bin(out["cpu"], f"xyz_{t}.f64", np.float64) - x0
+        ug = O.read_bin(out["gpu"], f"xyz_{t}.f64", np.float64) - x0
+        assert rel(ug, uc) <= 1e-8, s
+        bc = O.read_bin(out["cpu"], f"bdamage_{t}.f64", np.float64)
+        bg = O.read_bin(out["gpu"], f"bdamage_{t}.f64", np.float64)
+        assert np.array_equal(bc == 1.0, bg == 1.0), s
+        assert rc[s]["cuts"] == rg[s]["cuts"] == 0
