@@ -362,6 +362,16 @@ int32_t lpmgpu_batch_destroy(lpmgpu_batch *b);
 int32_t lpmgpu_batch_add(lpmgpu_batch *b, lpmgpu_solver *h, const lpmgpu_load_step *steps, int32_t nsteps,
                          int32_t *member);
 /* one round; *running receives the number of members not yet finished */
+/* A fatigue member (the reference's SolverFatigue runs one specimen; no batch counterpart): the
+ * nstatic static_steps run as SolverFatigue::solveProblemStatic's steps (solver_fatigue.h:244-275:
+ * halve-and-retry, then updateStateVar + storeStateVar), then ncycles cycles of cycle_len steps
+ * each (cycle_steps, cycle by cycle) as solveProblemOneCycle runs them (:221-241), cycle c with
+ * dN/dt = dndt[c].  Its Newton systems join the batched CG of every round with the other members.
+ * Member results: lpmgpu_batch_member_steps gives one record per step; `cuts` of a cycle step
+ * counts a Newton failure that was carried on from. */
+int32_t lpmgpu_batch_add_fatigue(lpmgpu_batch *b, lpmgpu_solver *h, const lpmgpu_load_step *static_steps,
+                                 int32_t nstatic, const lpmgpu_load_step *cycle_steps, int32_t cycle_len,
+                                 int32_t ncycles, const double *dndt, int32_t *member);
 int32_t lpmgpu_batch_round(lpmgpu_batch *b, int32_t *running);
 /* rounds until every member finished */
 int32_t lpmgpu_batch_run(lpmgpu_batch *b);

@@ -1074,6 +1074,11 @@ struct Member
     bool ls_fresh = true;
     BState ls_state{};
     double ir_stop = 0, ir_rr = 0;
+    // fatigue members (SolverFatigue, include/solver_fatigue.h): steps [0, nstatic) run as
+    // solveProblemStatic's steps, the rest as cycle steps; cycle_end[s] = (closes a cycle, dN/dt)
+    bool fatigue = false;
+    size_t nstatic = 0;
+    std::vector<std::pair<bool, double>> cycle_end;
 };
 
 int32_t cuda_status(cudaError_t e, const char *what)
@@ -1158,11 +1163,48 @@ struct lpmgpu_batch
         stats.members_done++;
     }
 
+    // after the Newton loop of a fatigue member's step (SolverFatigue::solveProblemStep has no
+    // damage loop, solver_fatigue.h:278-302).  A static step (solveProblemStatic, :244-275) that
+    // failed is reset and halved, and a converged one is followed by updateStateVar and
+    // storeStateVar.  A cycle step (solveProblemOneCycle, :221-241) is followed by updateStateVar
+    // whether it converged or not; the cycle's last step adds updateFatigueDamage(dN/dt),
+    // storeStateVar, updateGeometry and updateForceState.
+    int32_t after_newton_fatigue(Member &m, int n_newton)
+    {
+        Problem &p = P(m);
+        const size_t si = m.next - 1;
+        const bool is_static = si < m.nstatic, failed = n_newton >= p.desc.max_iter;
+        if (is_static && failed)
+            return fail_substep(m);
+        cudaError_t e = launch_update_state_var(p);
+        if (e == cudaSuccess && is_static)
+            e = enqueue_store_state(p);
+        if (e == cudaSuccess && !is_static)
+        {
+            if (failed)
+                m.cur.cuts++; // a cycle step whose Newton failed, carried on from
+            if (m.cycle_end[si].first)
+            {
+                e = launch_fatigue_damage(p, m.cycle_end[si].second);
+                if (e == cudaSuccess)
+                    e = enqueue_store_state(p);
+                if (e == cudaSuccess)
+                    e = enqueue_force_state(p, false);
+            }
+        }
+        if (e != cudaSuccess)
+            return fail_member(m, cuda_status(e, "batch fatigue step"));
+        substep_done(m);
+        return LPMGPU_OK;
+    }
+
     // after the Newton loop of one damage iteration (solver_static.h:119-121)
     int32_t after_newton(Member &m, int n_newton)
     {
         Problem &p = P(m);
         m.cur.residual_norm = m.nres;
+        if (m.fatigue)
+            return after_newton_fatigue(m, n_newton);
         if (n_newton >= p.desc.max_iter)
             return fail_substep(m);
         cudaError_t e = enqueue_damage_update(p);
@@ -1513,11 +1555,9 @@ int32_t lpmgpu_batch_destroy(lpmgpu_batch *b)
     return LPMGPU_OK;
 }
 
-int32_t lpmgpu_batch_add(lpmgpu_batch *b, lpmgpu_solver *h, const lpmgpu_load_step *steps, int32_t nsteps,
-                         int32_t *member)
+// Checks a problem that is to join the batch; LPMGPU_OK when it may.
+static int32_t check_joiner(lpmgpu_batch *b, lpmgpu_solver *h)
 {
-    if (!b || !h || nsteps < 0 || (nsteps > 0 && !steps))
-        return LPMGPU_ERR_INVALID_ARG;
     if (h->p.device != b->ctx.device)
     {
         set_last_error("the problem lives on another device than the batch");
@@ -1544,17 +1584,13 @@ int32_t lpmgpu_batch_add(lpmgpu_batch *b, lpmgpu_solver *h, const lpmgpu_load_st
         set_last_error("a batch runs at most 4096 problems at once");
         return LPMGPU_ERR_BUDGET;
     }
-    for (int32_t s = 0; s < nsteps; ++s)
-        for (int k = 0; k < steps[s].ndisp; ++k)
-            if (steps[s].disp[k].flag < 0 || steps[s].disp[k].flag >= h->p.dim || steps[s].disp[k].count < 0 ||
-                (steps[s].disp[k].count > 0 && !steps[s].disp[k].ids))
-                return LPMGPU_ERR_INVALID_ARG;
-    auto m = std::make_unique<Member>();
-    m->h = h;
-    for (int32_t s = 0; s < nsteps; ++s)
-        m->steps.emplace_back(steps[s]);
+    return LPMGPU_OK;
+}
+
+static int32_t push_member(lpmgpu_batch *b, std::unique_ptr<Member> m, int32_t *member)
+{
     m->t_add = std::chrono::steady_clock::now();
-    if (nsteps == 0)
+    if (m->steps.empty())
     {
         m->ph = Ph::Done;
         m->t_done = m->t_add;
@@ -1564,6 +1600,71 @@ int32_t lpmgpu_batch_add(lpmgpu_batch *b, lpmgpu_solver *h, const lpmgpu_load_st
     if (member)
         *member = (int32_t)b->members.size() - 1;
     return LPMGPU_OK;
+}
+
+int32_t lpmgpu_batch_add(lpmgpu_batch *b, lpmgpu_solver *h, const lpmgpu_load_step *steps, int32_t nsteps,
+                         int32_t *member)
+{
+    if (!b || !h || nsteps < 0 || (nsteps > 0 && !steps))
+        return LPMGPU_ERR_INVALID_ARG;
+    const int32_t c = check_joiner(b, h);
+    if (c != LPMGPU_OK)
+        return c;
+    for (int32_t s = 0; s < nsteps; ++s)
+        for (int k = 0; k < steps[s].ndisp; ++k)
+            if (steps[s].disp[k].flag < 0 || steps[s].disp[k].flag >= h->p.dim || steps[s].disp[k].count < 0 ||
+                (steps[s].disp[k].count > 0 && !steps[s].disp[k].ids))
+                return LPMGPU_ERR_INVALID_ARG;
+    auto m = std::make_unique<Member>();
+    m->h = h;
+    for (int32_t s = 0; s < nsteps; ++s)
+        m->steps.emplace_back(steps[s]);
+    return push_member(b, std::move(m), member);
+}
+
+int32_t lpmgpu_batch_add_fatigue(lpmgpu_batch *b, lpmgpu_solver *h, const lpmgpu_load_step *static_steps,
+                                 int32_t nstatic, const lpmgpu_load_step *cycle_steps, int32_t cycle_len,
+                                 int32_t ncycles, const double *dndt, int32_t *member)
+{
+    if (!b || !h || nstatic < 0 || (nstatic > 0 && !static_steps) || cycle_len < 0 || ncycles < 0 ||
+        (ncycles > 0 && (cycle_len == 0 || !cycle_steps || !dndt)))
+        return LPMGPU_ERR_INVALID_ARG;
+    const int32_t c = check_joiner(b, h);
+    if (c != LPMGPU_OK)
+        return c;
+    auto check = [&](const lpmgpu_load_step &st) {
+        for (int k = 0; k < st.ndisp; ++k)
+            if (st.disp[k].flag < 0 || st.disp[k].flag > 2 || st.disp[k].count < 0 ||
+                (st.disp[k].count > 0 && !st.disp[k].ids))
+                return false;
+        for (int k = 0; k < st.nforce; ++k)
+            if (st.force[k].count < 0 || (st.force[k].count > 0 && !st.force[k].ids))
+                return false;
+        return true;
+    };
+    const int64_t ncs = (int64_t)cycle_len * ncycles;
+    for (int32_t s = 0; s < nstatic; ++s)
+        if (!check(static_steps[s]))
+            return LPMGPU_ERR_INVALID_ARG;
+    for (int64_t s = 0; s < ncs; ++s)
+        if (!check(cycle_steps[s]))
+            return LPMGPU_ERR_INVALID_ARG;
+    auto m = std::make_unique<Member>();
+    m->h = h;
+    m->fatigue = true;
+    m->nstatic = (size_t)nstatic;
+    for (int32_t s = 0; s < nstatic; ++s)
+    {
+        m->steps.emplace_back(static_steps[s]);
+        m->cycle_end.push_back({false, 0.0});
+    }
+    for (int64_t s = 0; s < ncs; ++s)
+    {
+        m->steps.emplace_back(cycle_steps[s]);
+        const bool end = (s + 1) % cycle_len == 0;
+        m->cycle_end.push_back({end, end ? dndt[s / cycle_len] : 0.0});
+    }
+    return push_member(b, std::move(m), member);
 }
 
 int32_t lpmgpu_batch_round(lpmgpu_batch *b, int32_t *running)

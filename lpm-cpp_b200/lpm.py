@@ -198,7 +198,8 @@ EXPORTS = [
     "lpmgpu_get_counters", "lpmgpu_get_stream", "lpmgpu_cg_bsr_noalloc", "lpmgpu_autotune", "lpmgpu_set_cg_grid",
     "lpmgpu_solve_direct", "lpmgpu_band_order",
     "lpmgpu_format_dump", "lpmgpu_dump_write", "lpmgpu_dump_flush",
-    "lpmgpu_batch_create", "lpmgpu_batch_destroy", "lpmgpu_batch_add", "lpmgpu_batch_round", "lpmgpu_batch_run",
+    "lpmgpu_batch_create", "lpmgpu_batch_destroy", "lpmgpu_batch_add", "lpmgpu_batch_add_fatigue",
+    "lpmgpu_batch_round", "lpmgpu_batch_run",
     "lpmgpu_batch_member", "lpmgpu_batch_member_steps", "lpmgpu_batch_remove", "lpmgpu_batch_get_stats",
     "lpmgpu_batch_set_slice",
     "lpmgpu_estimate_bytes", "lpmgpu_server_create", "lpmgpu_server_destroy", "lpmgpu_server_set_slice", "lpmgpu_server_submit",
@@ -258,6 +259,8 @@ def lib():
         "lpmgpu_batch_create": (C.c_int32, [C.c_int32, C.POINTER(vp)]),
         "lpmgpu_batch_destroy": (C.c_int32, [vp]),
         "lpmgpu_batch_add": (C.c_int32, [vp, vp, C.POINTER(CLoadStep), C.c_int32, ip]),
+        "lpmgpu_batch_add_fatigue": (C.c_int32, [vp, vp, C.POINTER(CLoadStep), C.c_int32, C.POINTER(CLoadStep),
+                                                 C.c_int32, C.c_int32, dp, ip]),
         "lpmgpu_batch_round": (C.c_int32, [vp, ip]),
         "lpmgpu_batch_run": (C.c_int32, [vp]),
         "lpmgpu_batch_member": (C.c_int32, [vp, C.c_int32, C.POINTER(MemberInfo)]),
@@ -889,6 +892,24 @@ class Batch:
         arr = (CLoadStep * max(len(cs), 1))(*[c.s for c in cs])
         mid = C.c_int32(-1)
         _check(lib().lpmgpu_batch_add(self._h, problem._h, arr, len(cs), C.byref(mid)), "lpmgpu_batch_add")
+        self._problems[mid.value] = problem
+        return mid.value
+
+    def add_fatigue(self, problem: "GpuProblem", static_steps: Sequence[LoadStep],
+                    cycles: Sequence[Sequence[LoadStep]], dndt: Sequence[float]) -> int:
+        """A fatigue member (lpmgpu_batch_add_fatigue): the static steps as
+        SolverFatigue::solveProblemStatic runs them, then each cycle (equal lengths) as
+        solveProblemOneCycle with its dN/dt."""
+        if len(cycles) != len(dndt) or len({len(c) for c in cycles}) > 1:
+            raise ValueError("one dN/dt per cycle, and cycles of equal length")
+        cs = [_CStep(s) for s in static_steps]
+        cc = [_CStep(s) for cyc in cycles for s in cyc]
+        a_s = (CLoadStep * max(len(cs), 1))(*[c.s for c in cs])
+        a_c = (CLoadStep * max(len(cc), 1))(*[c.s for c in cc])
+        d = np.ascontiguousarray(dndt, dtype=np.float64) if len(dndt) else np.zeros(1)
+        mid = C.c_int32(-1)
+        _check(lib().lpmgpu_batch_add_fatigue(self._h, problem._h, a_s, len(cs), a_c, len(cycles[0]) if cycles else 0,
+                                              len(cycles), _dp(d), C.byref(mid)), "lpmgpu_batch_add_fatigue")
         self._problems[mid.value] = problem
         return mid.value
 

@@ -179,3 +179,45 @@ def test_solver_static_gpu_passes_the_assembly_nonlocal_lists(tmp_path):
         dg = O.read_bin(out["gpu"], f"damage_{t}.f64", np.float64)
         assert np.abs(dg - dc).max() <= 1e-9, s
     assert dc.max() > 0.5
+
+
+def test_batch_fatigue_members_match_alone():
+    """Two fatigue plates (displacement- and force-driven) as fatigue members of one batch
+    (lpmgpu_batch_add_fatigue), their Newton systems solved by the batched CG with the other
+    member's: each ends as it does alone through lpmgpu_fatigue_static_step / _cycle (damage
+    within 1e-9, displacements within 1e-8 x the scale, the same Newton count)."""
+    cases = [CFG.fatigue_plate(),
+             CFG.fatigue_plate(size=2.0, load_type="uniaxial_force", amplitude=200.0, cycles=4, tol_iter=1e-7)]
+    alone = []
+    for c in cases:
+        g = gpu_problem(c, **TIGHT)
+        newton = 0
+        for s in range(len(c.steps)):
+            ok, st = g.fatigue_static_step(c.load_step(s))
+            assert ok
+            newton += st["newton_solves"]
+        for N, dNdt, steps in fatigue_cycles(c):
+            _, st = g.fatigue_cycle(steps, dNdt)
+            newton += st["newton_solves"]
+        alone.append((g.state(("xyz", "damage")), newton))
+        g.close()
+    gs = [gpu_problem(c, **TIGHT) for c in cases]
+    b = LPM.Batch(0)
+    mids = []
+    for g, c in zip(gs, cases):
+        cyc = list(fatigue_cycles(c))
+        mids.append(b.add_fatigue(g, [c.load_step(s) for s in range(len(c.steps))], [x[2] for x in cyc],
+                                  [x[1] for x in cyc]))
+    b.run()
+    for g, c, mid, (st0, n0) in zip(gs, cases, mids, alone):
+        info = b.member(mid)
+        assert info["state"] == 1, info
+        assert sum(s["newton_solves"] for s in b.member_steps(mid)) == n0
+        st = g.state(("xyz", "damage"))
+        scale = fatigue_disp_scale(c)
+        assert np.abs((st["xyz"] - c.xyz) - (st0["xyz"] - c.xyz)).max() <= 1e-8 * scale
+        assert np.abs(st["damage"] - st0["damage"]).max() <= 1e-9
+    assert max(alone[0][0]["damage"].max(), alone[1][0]["damage"].max()) > 0.1
+    b.close()
+    for g in gs:
+        g.close()
