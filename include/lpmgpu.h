@@ -428,6 +428,12 @@ int32_t lpmgpu_server_destroy(lpmgpu_server *s);
 int32_t lpmgpu_server_set_slice(lpmgpu_server *s, int64_t iterations);
 int32_t lpmgpu_server_submit(lpmgpu_server *s, const lpmgpu_desc *d, const lpmgpu_load_step *steps, int32_t nsteps,
                              int64_t *request_id);
+/* A fatigue request: the problem and a SolverFatigue run as lpmgpu_batch_add_fatigue takes it
+ * (static steps, then ncycles cycles of cycle_len steps with dN/dt dndt[c]), admitted and batched
+ * like any request (no counterpart in the reference). */
+int32_t lpmgpu_server_submit_fatigue(lpmgpu_server *s, const lpmgpu_desc *d, const lpmgpu_load_step *static_steps,
+                                     int32_t nstatic, const lpmgpu_load_step *cycle_steps, int32_t cycle_len,
+                                     int32_t ncycles, const double *dndt, int64_t *id);
 int32_t lpmgpu_server_poll(lpmgpu_server *s, int64_t request_id, lpmgpu_request_info *info);
 /* blocks until the request is done or failed (LPMGPU_OK) or the timeout passed (LPMGPU_ERR_NOT_READY) */
 int32_t lpmgpu_server_wait(lpmgpu_server *s, int64_t request_id, double timeout_s, lpmgpu_request_info *info);

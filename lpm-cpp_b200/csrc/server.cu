@@ -67,6 +67,11 @@ struct Request
     std::vector<double> xyz, kn, tv, bdmg;
     std::vector<int32_t> type, nb0, nb1, p2, nl_count, nl_ids;
     std::vector<OwnedStep> steps;
+    // a fatigue request (lpmgpu_server_submit_fatigue): steps = nstatic static steps, then
+    // ncycles cycles of cycle_len steps, cycle c with dN/dt dndt[c]
+    bool fatigue = false;
+    int32_t nstatic = 0, cycle_len = 0, ncycles = 0;
+    std::vector<double> dndt;
     int64_t est_bytes = 0, bytes = 0;
     lpmgpu_solver *h = nullptr;
     int32_t member = -1;
@@ -259,7 +264,10 @@ struct lpmgpu_server
                 for (auto &s : r->steps)
                     v.push_back(s.view);
                 int32_t mid = -1;
-                const int32_t s = lpmgpu_batch_add(batch, r->h, v.data(), (int32_t)v.size(), &mid);
+                const int32_t s =
+                    r->fatigue ? lpmgpu_batch_add_fatigue(batch, r->h, v.data(), r->nstatic, v.data() + r->nstatic,
+                                                          r->cycle_len, r->ncycles, r->dndt.data(), &mid)
+                               : lpmgpu_batch_add(batch, r->h, v.data(), (int32_t)v.size(), &mid);
                 std::lock_guard<std::mutex> lk(mu);
                 if (s != LPMGPU_OK)
                 {
@@ -398,8 +406,16 @@ int32_t lpmgpu_server_set_slice(lpmgpu_server *s, int64_t iterations)
     return LPMGPU_OK;
 }
 
-int32_t lpmgpu_server_submit(lpmgpu_server *s, const lpmgpu_desc *d, const lpmgpu_load_step *steps, int32_t nsteps,
-                             int64_t *id)
+struct FatigueSpec
+{
+    int32_t nstatic, cycle_len, ncycles;
+    const double *dndt;
+};
+
+// The request: a deep copy of the problem description and its steps (all static, or for a
+// fatigue request the static steps followed by the cycles' steps)
+static int32_t submit_impl(lpmgpu_server *s, const lpmgpu_desc *d, const lpmgpu_load_step *steps, int32_t nsteps,
+                           int64_t *id, const FatigueSpec *f)
 {
     if (!s || !d || !d->xyz || d->n <= 0 || nsteps < 0 || (nsteps > 0 && !steps))
         return LPMGPU_ERR_INVALID_ARG;
@@ -457,6 +473,16 @@ int32_t lpmgpu_server_submit(lpmgpu_server *s, const lpmgpu_desc *d, const lpmgp
     }
     for (int32_t k = 0; k < nsteps; ++k)
         r->steps.emplace_back(steps[k]);
+    if (f)
+    {
+        r->fatigue = true;
+        r->nstatic = f->nstatic;
+        r->cycle_len = f->cycle_len;
+        r->ncycles = f->ncycles;
+        r->dndt.assign(f->dndt, f->dndt + f->ncycles);
+        if (r->dndt.empty())
+            r->dndt.push_back(0.0);
+    }
     r->est_bytes = estimate_bytes(r->desc);
     r->t_submit = Clock::now();
     std::lock_guard<std::mutex> lk(s->mu);
@@ -468,6 +494,25 @@ int32_t lpmgpu_server_submit(lpmgpu_server *s, const lpmgpu_desc *d, const lpmgp
     s->submitted++;
     s->cv_admit.notify_all();
     return LPMGPU_OK;
+}
+
+int32_t lpmgpu_server_submit(lpmgpu_server *s, const lpmgpu_desc *d, const lpmgpu_load_step *steps, int32_t nsteps,
+                             int64_t *id)
+{
+    return submit_impl(s, d, steps, nsteps, id, nullptr);
+}
+
+int32_t lpmgpu_server_submit_fatigue(lpmgpu_server *s, const lpmgpu_desc *d, const lpmgpu_load_step *static_steps,
+                                     int32_t nstatic, const lpmgpu_load_step *cycle_steps, int32_t cycle_len,
+                                     int32_t ncycles, const double *dndt, int64_t *id)
+{
+    if (nstatic < 0 || cycle_len < 0 || ncycles < 0 || (nstatic > 0 && !static_steps) ||
+        (ncycles > 0 && (cycle_len == 0 || !cycle_steps || !dndt)))
+        return LPMGPU_ERR_INVALID_ARG;
+    std::vector<lpmgpu_load_step> all(static_steps, static_steps + nstatic);
+    all.insert(all.end(), cycle_steps, cycle_steps + (size_t)cycle_len * ncycles);
+    const FatigueSpec f{nstatic, cycle_len, ncycles, dndt};
+    return submit_impl(s, d, all.data(), (int32_t)all.size(), id, &f);
 }
 
 static void fill_info(const lpmgpu_server *s, const Request &r, lpmgpu_request_info *info)

@@ -203,6 +203,7 @@ EXPORTS = [
     "lpmgpu_batch_member", "lpmgpu_batch_member_steps", "lpmgpu_batch_remove", "lpmgpu_batch_get_stats",
     "lpmgpu_batch_set_slice",
     "lpmgpu_estimate_bytes", "lpmgpu_server_create", "lpmgpu_server_destroy", "lpmgpu_server_set_slice", "lpmgpu_server_submit",
+    "lpmgpu_server_submit_fatigue",
     "lpmgpu_server_poll", "lpmgpu_server_wait", "lpmgpu_server_result", "lpmgpu_server_get_stats",
 ]
 
@@ -273,6 +274,8 @@ def lib():
         "lpmgpu_server_destroy": (C.c_int32, [vp]),
         "lpmgpu_server_set_slice": (C.c_int32, [vp, C.c_int64]),
         "lpmgpu_server_submit": (C.c_int32, [vp, C.POINTER(Desc), C.POINTER(CLoadStep), C.c_int32, lp]),
+        "lpmgpu_server_submit_fatigue": (C.c_int32, [vp, C.POINTER(Desc), C.POINTER(CLoadStep), C.c_int32,
+                                                     C.POINTER(CLoadStep), C.c_int32, C.c_int32, dp, lp]),
         "lpmgpu_server_poll": (C.c_int32, [vp, C.c_int64, C.POINTER(RequestInfo)]),
         "lpmgpu_server_wait": (C.c_int32, [vp, C.c_int64, C.c_double, C.POINTER(RequestInfo)]),
         "lpmgpu_server_result": (C.c_int32, [vp, C.c_int64, dp, C.c_int64]),
@@ -992,6 +995,27 @@ class Server:
         arr = (CLoadStep * max(len(cs), 1))(*[c.s for c in cs])
         rid = C.c_int64(0)
         _check(lib().lpmgpu_server_submit(self._h, C.byref(d), arr, len(cs), C.byref(rid)), "lpmgpu_server_submit")
+        self._n[rid.value] = ass.nparticle
+        return rid.value
+
+    def submit_fatigue(self, ass: Assembly, static_steps: Sequence[LoadStep], cycles: Sequence[Sequence[LoadStep]],
+                       dndt: Sequence[float], undamaged_pt_type=-1, max_iter=30, tol_iter=1e-5,
+                       precision: Precision = Precision.FP64, cg_rtol=1e-12, cg_atol=1e-12, cg_maxit=0) -> int:
+        """A SolverFatigue run as a request (lpmgpu_server_submit_fatigue): the static steps, then
+        the cycles (equal lengths) with their dN/dt."""
+        if len(cycles) != len(dndt) or len({len(c) for c in cycles}) > 1:
+            raise ValueError("one dN/dt per cycle, and cycles of equal length")
+        d, keep = _pack_desc(ass, undamaged_pt_type, max_iter, tol_iter, precision, cg_rtol, cg_atol, cg_maxit,
+                             self.device, False)
+        cs = [_CStep(s) for s in static_steps]
+        cc = [_CStep(s) for cyc in cycles for s in cyc]
+        a_s = (CLoadStep * max(len(cs), 1))(*[c.s for c in cs])
+        a_c = (CLoadStep * max(len(cc), 1))(*[c.s for c in cc])
+        dd = np.ascontiguousarray(dndt, dtype=np.float64) if len(dndt) else np.zeros(1)
+        rid = C.c_int64(0)
+        _check(lib().lpmgpu_server_submit_fatigue(self._h, C.byref(d), a_s, len(cs), a_c,
+                                                  len(cycles[0]) if cycles else 0, len(cycles), _dp(dd),
+                                                  C.byref(rid)), "lpmgpu_server_submit_fatigue")
         self._n[rid.value] = ass.nparticle
         return rid.value
 

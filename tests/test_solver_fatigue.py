@@ -221,3 +221,29 @@ def test_batch_fatigue_members_match_alone():
     b.close()
     for g in gs:
         g.close()
+
+
+def test_served_fatigue_request_matches_alone():
+    """A fatigue run submitted to the server (lpmgpu_server_submit_fatigue) while a static
+    request runs: its final positions are those of the same run alone within 1e-8 x the scale."""
+    c = CFG.fatigue_plate()
+    g = gpu_problem(c, **TIGHT)
+    for s in range(len(c.steps)):
+        g.fatigue_static_step(c.load_step(s))
+    cyc = list(fatigue_cycles(c))
+    for N, dNdt, steps in cyc:
+        g.fatigue_cycle(steps, dNdt)
+    x_alone = g.state(("xyz",))["xyz"]
+    g.close()
+    other = CFG.hex_plate(size=3.0, radius=0.1, steps=3, total_disp=0.003, tol_iter=1e-9)
+    srv = LPM.Server(0, hbm_budget_bytes=8 * 10**9)
+    r0 = srv.submit(other.assembly(), [other.load_step(s) for s in range(3)], tol_iter=other.tol_iter, **TIGHT)
+    r1 = srv.submit_fatigue(c.assembly(), [c.load_step(s) for s in range(len(c.steps))], [x[2] for x in cyc],
+                            [x[1] for x in cyc], undamaged_pt_type=c.undamaged_type, max_iter=c.max_iter,
+                            tol_iter=c.tol_iter, **TIGHT)
+    for rid in (r0, r1):
+        info = srv.wait(rid, timeout=300)
+        assert info["state"] == 2, info
+    x = srv.result(r1).reshape(-1, 3)
+    assert np.abs((x - c.xyz) - (x_alone - c.xyz)).max() <= 1e-8 * fatigue_disp_scale(c)
+    srv.close()
