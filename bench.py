@@ -519,8 +519,10 @@ def fatigue_leg(lpm, device, size=25.0, cycles=4):
             finally:
                 shutil.rmtree(d, ignore_errors=True)
             wall_r = sum(r["wall_s"] for r in rows)
-            out["reference"] = {"seconds": wall_r, "cycles_per_s": ncyc / wall_r, "cores": threads,
-                                "kind": "reference", "newton_solves": int(sum(r["newton_solves"] for r in rows))}
+            # the leg's CPU baseline and checker: the reference's own SolverFatigue on the host cores
+            out["cpu_baseline"] = {"seconds": wall_r, "cycles_per_s": ncyc / wall_r, "cores": threads,
+                                   "kind": "reference", "newton_solves": int(sum(r["newton_solves"] for r in rows)),
+                                   "sample": "the same static step and cycles"}
             out["speedup_vs_reference"] = wall_r / wall
             out["max_abs_damage_diff_vs_reference"] = float(np.abs(sg["damage"] - dr).max())
             out["max_abs_disp_diff_vs_reference_over_amplitude"] = float(np.abs(sg["xyz"] - xr).max() / amp)
