@@ -11,7 +11,11 @@
 // so the weighted sums of the averaging add in the reference's order.
 #include <cub/cub.cuh>
 
+#include <cstdlib>
+#include <vector>
+
 #include "lpm_internal.cuh"
+#include "nonlocal_grid.cuh"
 
 namespace lpm
 {
@@ -47,10 +51,126 @@ __global__ void k_nonlocal_search(int n, const double *__restrict__ xyz, double 
         cnt[i] = c;
 }
 
+// Cell-grid search: one thread per particle collects its neighbours from the cells around it
+// (nonlocal_grid.cuh); pass 0 counts, pass 1 writes them unsorted at start[i].
+template <int PASS>
+__global__ void k_nonlocal_grid(int n, const double *__restrict__ xyz, double rc, const int *__restrict__ cxyz, int d0,
+                                int d1, int d2, const int *__restrict__ cell_start, const int *__restrict__ cell_ids,
+                                int *__restrict__ cnt, const int *__restrict__ start, int *__restrict__ list)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const int dims[3] = {d0, d1, d2};
+    if (PASS == 0)
+        cnt[i] = nlgrid::candidates(i, xyz, rc, cxyz + 3 * (int64_t)i, dims, cell_start, cell_ids, nullptr);
+    else
+        nlgrid::candidates(i, xyz, rc, cxyz + 3 * (int64_t)i, dims, cell_start, cell_ids, list + start[i]);
+}
+
+// Above this many particles the search bins them into cells instead of testing all pairs
+// (LPMGPU_NL_GRID=1 / =0 forces either).
+constexpr int kNlAllPairsMax = 16384;
+
+static bool use_grid(int n)
+{
+    const char *f = std::getenv("LPMGPU_NL_GRID");
+    if (f && f[0] == '1')
+        return true;
+    if (f && f[0] == '0')
+        return false;
+    return n > kNlAllPairsMax;
+}
+
+// The cell-grid search: the same lists as the all-pairs search (the same distance test; each list
+// sorted to ascending id by a segmented sort), in O(n x neighbours) instead of O(n^2).
+static cudaError_t build_nonlocal_grid(Problem &p, double rc)
+{
+    const int n = p.n;
+    int dims[3];
+    std::vector<int> cxyz, cell_start, cell_ids;
+    if (!nlgrid::bin(p.xyz0_host.data(), n, rc, int64_t(1) << 26, dims, cxyz, cell_start, cell_ids))
+        return cudaErrorInvalidValue;
+    int *d_cxyz = nullptr, *d_cs = nullptr, *d_ci = nullptr, *cnt = nullptr, *unsorted = nullptr;
+    void *tmp = nullptr;
+    cudaError_t e = dalloc(p, &p.nlstart, (size_t)n + 1);
+    auto cleanup = [&]() {
+        for (void *q : {(void *)d_cxyz, (void *)d_cs, (void *)d_ci, (void *)cnt, (void *)unsorted, tmp})
+            if (q)
+                cudaFreeAsync(q, p.stream);
+    };
+    if (e == cudaSuccess)
+        e = cudaMallocAsync(&d_cxyz, sizeof(int) * cxyz.size(), p.stream);
+    if (e == cudaSuccess)
+        e = cudaMallocAsync(&d_cs, sizeof(int) * cell_start.size(), p.stream);
+    if (e == cudaSuccess)
+        e = cudaMallocAsync(&d_ci, sizeof(int) * cell_ids.size(), p.stream);
+    if (e == cudaSuccess)
+        e = cudaMallocAsync(&cnt, sizeof(int) * ((size_t)n + 1), p.stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_cxyz, cxyz.data(), sizeof(int) * cxyz.size(), cudaMemcpyHostToDevice, p.stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_cs, cell_start.data(), sizeof(int) * cell_start.size(), cudaMemcpyHostToDevice, p.stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_ci, cell_ids.data(), sizeof(int) * cell_ids.size(), cudaMemcpyHostToDevice, p.stream);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)n + 1), p.stream);
+    if (e != cudaSuccess)
+    {
+        cleanup();
+        return e;
+    }
+    k_nonlocal_grid<0><<<div_up(n, 128), 128, 0, p.stream>>>(n, p.xyz, rc, d_cxyz, dims[0], dims[1], dims[2], d_cs,
+                                                             d_ci, cnt, nullptr, nullptr);
+    p.ctr.kernel_launches++;
+    size_t bytes = 0;
+    if ((e = cub::DeviceScan::ExclusiveSum(nullptr, bytes, cnt, p.nlstart, n + 1, p.stream)) == cudaSuccess &&
+        (e = cudaMallocAsync(&tmp, bytes ? bytes : 16, p.stream)) == cudaSuccess)
+        e = cub::DeviceScan::ExclusiveSum(tmp, bytes, cnt, p.nlstart, n + 1, p.stream);
+    if (tmp)
+    {
+        cudaFreeAsync(tmp, p.stream);
+        tmp = nullptr;
+    }
+    int total = 0;
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&total, p.nlstart + n, sizeof(int), cudaMemcpyDeviceToHost, p.stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(p.stream); // also keeps the host bins alive through their copies
+    if (e == cudaSuccess)
+    {
+        p.nnl = total;
+        e = dalloc(p, &p.nlist, (size_t)total);
+    }
+    if (e == cudaSuccess)
+        e = dalloc(p, &p.ddot_nonlocal, (size_t)n);
+    if (e == cudaSuccess)
+        e = cudaMallocAsync(&unsorted, sizeof(int) * ((size_t)total + 1), p.stream);
+    if (e == cudaSuccess)
+    {
+        k_nonlocal_grid<1><<<div_up(n, 128), 128, 0, p.stream>>>(n, p.xyz, rc, d_cxyz, dims[0], dims[1], dims[2], d_cs,
+                                                                 d_ci, nullptr, p.nlstart, unsorted);
+        p.ctr.kernel_launches++;
+        e = cudaGetLastError();
+    }
+    // each particle's list in ascending id, the order of the reference's loop
+    bytes = 0;
+    if (e == cudaSuccess &&
+        (e = cub::DeviceSegmentedSort::SortKeys(nullptr, bytes, unsorted, p.nlist, total, n, p.nlstart, p.nlstart + 1,
+                                                 p.stream)) == cudaSuccess &&
+        (e = cudaMallocAsync(&tmp, bytes ? bytes : 16, p.stream)) == cudaSuccess)
+        e = cub::DeviceSegmentedSort::SortKeys(tmp, bytes, unsorted, p.nlist, total, n, p.nlstart, p.nlstart + 1,
+                                               p.stream);
+    cleanup();
+    return e;
+}
+
 cudaError_t build_nonlocal(Problem &p, double cutoff_ratio)
 {
     const int n = p.n;
     const double rc = cutoff_ratio * p.desc.nonlocal_L; // searchNonlocalNeighbors: cutoff_ratio * nonlocal_L
+    if (use_grid(n) && rc > 0)
+        return build_nonlocal_grid(p, rc);
     cudaError_t e = dalloc(p, &p.nlstart, (size_t)n + 1);
     if (e != cudaSuccess)
         return e;

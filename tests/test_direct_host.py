@@ -1,4 +1,4 @@
-"""The direct solver's host-checkable parts (no device): the band Cholesky core of
+"""Host-checkable parts of the direct solver and the nonlocal search (no device): the band Cholesky core of
 lpm-cpp_b200/csrc/band_chol.cuh, compiled for the host by a harness that runs it in the device
 driver's order and thread decomposition (tests/native/band_check.cpp), against numpy on random
 banded SPD matrices; and the reverse Cuthill-McKee ordering (lpmgpu_band_order, host only) on
@@ -118,3 +118,35 @@ def test_rcm_order_handles_components_and_rejects_bad_graphs():
     st, rank, bw = _rcm(start, adj)
     assert st == 0 and sorted(rank) == list(range(5)) and bw == 1
     assert _rcm(np.array([0, 1], np.int32), np.array([5], np.int32))[0] == 1
+
+
+# ---- the cell-grid nonlocal search (lpm-cpp_b200/csrc/nonlocal_grid.cuh), host-compiled
+@pytest.fixture(scope="module")
+def nlgrid(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("nlgrid") / "nlgrid_check")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I", os.path.join(ROOT, "lpm-cpp_b200", "csrc"),
+                    os.path.join(HERE, "native", "nlgrid_check.cpp"), "-o", exe], check=True)
+    return exe
+
+
+@pytest.mark.parametrize("which,max_cells", [("hex", 1 << 26), ("sc", 1 << 26), ("random", 1 << 26),
+                                             ("random", 8), ("hex", 1)])
+def test_grid_nonlocal_search_finds_the_all_pairs_lists(nlgrid, tmp_path, which, max_cells):
+    """Every particle's list from the cells around it, sorted, equals the all-pairs list; also
+    when the grid is capped to a few cells (wider cells) or to one."""
+    if which == "hex":
+        xyz, rc = CFG.hex_plate(size=3.0, radius=0.1).xyz, 0.45
+    elif which == "sc":
+        xyz, rc = CFG.sc_cube(size=2.0, radius=0.2).xyz, 0.9
+    else:
+        xyz, rc = np.random.default_rng(5).uniform(-1.0, 2.0, (700, 3)), 0.37
+    p = str(tmp_path / "in.bin")
+    with open(p, "wb") as f:
+        np.array([len(xyz)], np.int64).tofile(f)
+        np.array([rc], np.float64).tofile(f)
+        np.ascontiguousarray(xyz, np.float64).tofile(f)
+    out = subprocess.run([nlgrid, p, str(max_cells)], check=True, capture_output=True, text=True).stdout.split()
+    bad, pairs = int(out[0]), int(out[1])
+    assert bad == 0
+    d = np.linalg.norm(xyz[:, None, :] - xyz[None, :, :], axis=2)
+    assert pairs == int((d < rc).sum())

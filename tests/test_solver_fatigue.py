@@ -247,3 +247,25 @@ def test_served_fatigue_request_matches_alone():
     x = srv.result(r1).reshape(-1, 3)
     assert np.abs((x - c.xyz) - (x_alone - c.xyz)).max() <= 1e-8 * fatigue_disp_scale(c)
     srv.close()
+
+
+def test_grid_nonlocal_search_gives_the_all_pairs_run():
+    """The nonlocal search by cell grid (the default above 16,384 particles) and by all pairs
+    (LPMGPU_NL_GRID forces either) give the same lists in the same order, so a fatigue run is
+    bit-identical with either."""
+    import os
+    c = CFG.fatigue_plate()
+    states = []
+    for mode in ("1", "0"):
+        os.environ["LPMGPU_NL_GRID"] = mode
+        try:
+            g = gpu_problem(c, **TIGHT)
+        finally:
+            os.environ.pop("LPMGPU_NL_GRID", None)
+        g.fatigue_static_step(c.load_step(0))
+        for N, dNdt, steps in fatigue_cycles(c):
+            g.fatigue_cycle(steps, dNdt)
+        states.append(g.state(("xyz", "damage", "state_var")))
+        g.close()
+    for k in states[0]:
+        assert np.array_equal(states[0][k], states[1][k]), k
