@@ -1,8 +1,11 @@
-"""Host-checkable parts of the direct solver and the nonlocal search (no device): the band Cholesky core of
-lpm-cpp_b200/csrc/band_chol.cuh, compiled for the host by a harness that runs it in the device
-driver's order and thread decomposition (tests/native/band_check.cpp), against numpy on random
-banded SPD matrices; and the reverse Cuthill-McKee ordering (lpmgpu_band_order, host only) on
-the particle connection graphs of the reference's lattices."""
+"""Host-checkable parts of the direct solver and of the nonlocal search (no device).
+- The band Cholesky core of lpm-cpp_b200/csrc/band_chol.cuh, compiled for the host by a harness
+  that runs it in the device driver's order and thread decomposition (tests/native/band_check.cpp),
+  against numpy on random banded SPD matrices.
+- The reverse Cuthill-McKee ordering (lpmgpu_band_order, host only) on the particle connection
+  graphs of the reference's lattices.
+- The cell-grid nonlocal search of lpm-cpp_b200/csrc/nonlocal_grid.cuh (tests/native/
+  nlgrid_check.cpp) against the all-pairs search."""
 import ctypes as C
 import os
 import subprocess
