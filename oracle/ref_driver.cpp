@@ -83,6 +83,7 @@
 /* the one-line switch of an example's run(): SolverStatic -> SolverStaticGPU and
  * SolverFatigue -> SolverFatigueGPU (lpm-cpp_b200/cpp) */
 #include "solver_static_gpu.h"
+#include "solver_fatigue_gpu.h"
 #define LPM_SOLVER SolverStaticGPU
 #define LPM_FATIGUE_SOLVER SolverFatigueGPU
 #else
