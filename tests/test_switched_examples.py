@@ -66,3 +66,18 @@ def test_hex_example_through_the_switch(tmp_path):
     uc = _dump_disp(os.path.join(dirs["cpu"], "hex_position.dump"))
     ug = _dump_disp(os.path.join(dirs["gpu"], "hex_position.dump"))
     assert np.abs(uc - ug).max() <= 1e-3 * np.abs(uc).max()
+
+
+def test_fcc_pardiso_example_through_the_switch(tmp_path):
+    """examples/ex3_singlecrystal_3d_fcc.cpp: 10,976 FCC particles, elastic with cubic constants
+    (C11, C12, C44) and a brittle bond law, solved in SolverMode::PARDISO, which the drop-in runs as
+    the device's direct solve where its band fits (else the CG to 1e-12); the reference's PARDISO
+    stand-in solves to 1e-14."""
+    dirs = {}
+    for tag in ("cpu", "gpu"):
+        dirs[tag] = str(tmp_path / tag)
+        _run("ex3_singlecrystal_3d_fcc", tag, dirs[tag])
+    uc = _dump_disp(os.path.join(dirs["cpu"], "Crystal_position.dump"))
+    ug = _dump_disp(os.path.join(dirs["gpu"], "Crystal_position.dump"))
+    assert uc.shape == ug.shape and np.abs(uc).max() > 0
+    assert np.abs(uc - ug).max() <= 1e-3 * np.abs(uc).max()
