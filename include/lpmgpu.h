@@ -110,6 +110,11 @@ typedef struct
      * direct solve when its band fits (at most 32 GiB), else the CG; the C++ and Python drop-ins
      * use 2 for SolverMode::PARDISO.  The direct solve is FP64 whatever the precision. */
     int32_t direct;
+    /* C11 > 0: the bond coefficients come from these elastic constants, as the (C11, C12, C44)
+     * overloads of setParticleProperty set them (particle_elastic.h:110-140,
+     * particle_elastic_damage.h:218-250), in place of E, mu and plane_stress; for elastic and
+     * elastic-damage particles (J2 keeps E and mu for its return map). */
+    double C11, C12, C44;
 } lpmgpu_desc;
 
 /* Displacement / force boundary condition of one load step (boundary.h:10-44, Relative mode). */

@@ -196,6 +196,20 @@ def fcc_bar(size=(4.0, 4.0, 8.0), radius=0.2, E=110e3, mu=0.34, steps=10, strain
                 types, groups, st, tol_iter=tol_iter, max_iter=max_iter, euler=euler)
 
 
+def fcc_cubic_cube(size=2.8, radius=0.244948964611159, C11=108e3, C12=61e3, C44=29e3, steps=2, total_disp=0.002,
+                   critical_bstrain=1.0, tol_iter=1e-9, max_iter=30) -> Case:
+    """An FCC cube of elastic particles with cubic elastic constants, as
+    examples/ex3_singlecrystal_3d_fcc.cpp sets them (setParticleProperty's (C11, C12, C44) overload,
+    particle_elastic.h:110-140; its radius and constants): bottom face fixed in z with two corners
+    pinned, top face moved in z."""
+    c = sc_cube(size=size, radius=radius, steps=steps, total_disp=total_disp, tol_iter=tol_iter, max_iter=max_iter,
+                lattice=L.LatticeType.FCC3D)
+    c.name = f"fcc_cubic_{size:g}mm"
+    c.material.C11, c.material.C12, c.material.C44 = C11, C12, C44
+    c.material.critical_bstrain = critical_bstrain
+    return c
+
+
 def notched_plate(size=4.0, radius=0.1, crack=0.3, E=69e3, mu=0.3, critical_bstrain=2e-3, steps=40,
                   total_disp=None, tol_iter=1e-5, max_iter=30) -> Case:
     """Single-edge-notched hexagonal plate with brittle bonds, pulled in y.  The pre-crack is a

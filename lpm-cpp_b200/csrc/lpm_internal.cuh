@@ -34,6 +34,8 @@ struct Cell
 Cell make_cell(int lattice, double radius);
 // setParticleProperty (particle_elastic.h:70-108): Kn/Tv coefficients
 void kntv(const Cell &c, int plane_stress, double E, double mu, double out[3]);
+// the same from given elastic constants C11, C12, C44 (particle_elastic.h:110-140)
+void kntv_cij(const Cell &c, const double Ce[3], double out[3]);
 
 // Reduction scratch: per-block partial sums and the scalars they reduce to.
 struct Scalars

@@ -698,7 +698,13 @@ int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
     p.n = d->n;
     p.dim = p.cell.dim;
     p.nsv = (d->ptype == LPMGPU_J2) ? 7 : (d->ptype == LPMGPU_FATIGUE_HCF) ? 3 : 1;
-    kntv(p.cell, d->plane_stress, d->E, d->mu, p.kntv);
+    if (d->C11 > 0 && d->ptype != LPMGPU_J2)
+    {
+        const double Ce[3] = {d->C11, d->C12, d->C44};
+        kntv_cij(p.cell, Ce, p.kntv);
+    }
+    else
+        kntv(p.cell, d->plane_stress, d->E, d->mu, p.kntv);
     const size_t n = p.n;
     CKF(cudaMallocHost(&p.scal_host, sizeof(Scalars)));
     CKF(cudaMallocHost(&p.cg_info_host, 8 * sizeof(int64_t)));

@@ -113,6 +113,20 @@ void kntv(const Cell &c, int plane_stress, double E, double mu, double out[3])
     }
 }
 
+// setParticleProperty's (C11, C12, C44) overload (particle_elastic.h:110-140): the same mapping
+// from given elastic constants
+void kntv_cij(const Cell &c, const double Ce[3], double out[3])
+{
+    const double alpha = (c.dim == 2) ? 1.0 : c.radius;
+    for (int r = 0; r < 3; ++r)
+    {
+        double s = 0.0;
+        for (int k = 0; k < 3; ++k)
+            s += c.el[3 * r + k] * Ce[k];
+        out[r] = alpha * s;
+    }
+}
+
 __device__ __forceinline__ double pdist(const double *a, const double *b)
 {
     const double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];

@@ -97,6 +97,7 @@ class Desc(C.Structure):
         ("fatigue_limit_ratio", C.c_double),
         ("nonlocal_count", C.POINTER(C.c_int32)), ("nonlocal_ids", C.POINTER(C.c_int32)),
         ("direct", C.c_int32),
+        ("C11", C.c_double), ("C12", C.c_double), ("C44", C.c_double),
     ]
 
 
@@ -389,6 +390,11 @@ class Material:
     fatigue_B: float = 0.0
     fatigue_d: float = 0.0
     fatigue_limit_ratio: float = 1.108
+    # setParticleProperty's (C11, C12, C44) overload (particle_elastic.h:110-140): C11 > 0 takes
+    # the bond coefficients from these constants instead of E, mu and plane_stress
+    C11: float = 0.0
+    C12: float = 0.0
+    C44: float = 0.0
 
 
 def _read_dump(path: str):
@@ -473,14 +479,29 @@ class Assembly:
         np.savetxt(bondFile, rows, fmt="%d")
 
     def setParticleProperty(self, nonlocal_L, is_plane_stress, E, mu, *rest):
-        """The isotropic setParticleProperty of the assembly's particle type:
+        """setParticleProperty of the assembly's particle type.  With a bool second argument, the
+        isotropic overloads:
         Elastic: (nonlocal_L, is_plane_stress, E, mu, critical_bstrain) (particle_elastic.h:71);
         J2: (nonlocal_L, is_plane_stress, E, mu, sigmay, xi, H, A, critical_bstrain)
         (particle_j2plasticity.h:155);
         ElasticDamage: (nonlocal_L, is_plane_stress, E, mu, k0, k1, ct_ratio, d_thres)
         (particle_elastic_damage.h:176);
         FatigueHCF: (nonlocal_L, is_plane_stress, E, mu, A, B, d, d_thres, f_lmt_ratio)
-        (particle_fatigue_hcf.h:163)."""
+        (particle_fatigue_hcf.h:163).
+        With a number there, the cubic-constant overloads: Elastic (nonlocal_L, C11, C12, C44,
+        critical_bstrain) (particle_elastic.h:111); ElasticDamage (nonlocal_L, C11, C12, C44, k0, k1,
+        ct_ratio, d_thres) (particle_elastic_damage.h:219)."""
+        if not isinstance(is_plane_stress, (bool, np.bool_)):
+            C11, C12, C44 = float(is_plane_stress), float(E), float(mu)
+            m = Material(nonlocal_L=float(nonlocal_L), C11=C11, C12=C12, C44=C44)
+            if self.ptype == ParticleType.ElasticDamage:
+                m.k0, m.k1, m.comp_tensile_ratio, m.damage_threshold = map(float, rest)
+            elif self.ptype == ParticleType.Elastic:
+                (m.critical_bstrain,) = map(float, rest)
+            else:
+                raise ValueError("the (C11, C12, C44) overload exists for elastic and elastic-damage particles")
+            self.material = m
+            return
         m = Material(plane_stress=bool(is_plane_stress), E=float(E), mu=float(mu), nonlocal_L=float(nonlocal_L))
         if self.ptype == ParticleType.J2Plasticity:
             m.sigmay, m.xi, m.H, m.A, m.critical_bstrain = map(float, rest)
@@ -648,6 +669,7 @@ def _pack_desc(ass: Assembly, undamaged_pt_type=-1, max_iter=30, tol_iter=1e-5, 
     d.k0, d.k1, d.comp_tensile_ratio, d.damage_threshold = m.k0, m.k1, m.comp_tensile_ratio, m.damage_threshold
     d.fatigue_A, d.fatigue_B, d.fatigue_d = m.fatigue_A, m.fatigue_B, m.fatigue_d
     d.fatigue_limit_ratio = m.fatigue_limit_ratio
+    d.C11, d.C12, d.C44 = m.C11, m.C12, m.C44
     if ass.bonds is not None:
         nb0, nb1, p2 = (np.ascontiguousarray(a, dtype=np.int32) for a in ass.bonds)
         keep += [nb0, nb1, p2]

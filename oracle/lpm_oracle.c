@@ -695,7 +695,13 @@ lpmo_problem *lpmo_create(const lpmo_desc *d)
     p->k1 = d->k1;
     p->nonlocal_L = d->nonlocal_L;
     double E = d->E, mu = d->mu, Ce[3], KnTv[3];
-    if (!d->plane_stress)
+    if (d->C11 > 0 && d->ptype != LPMO_J2)
+    {
+        Ce[0] = d->C11;
+        Ce[1] = d->C12;
+        Ce[2] = d->C44;
+    }
+    else if (!d->plane_stress)
     {
         Ce[0] = E * (1.0 - mu) / (1.0 + mu) / (1.0 - 2.0 * mu);
         Ce[1] = E * mu / (1.0 + mu) / (1.0 - 2.0 * mu);

@@ -49,6 +49,9 @@ typedef struct
      * The fatigue limit ratio is stored by the reference but unused (calcEqEnergy returns the
      * total energy, particle_fatigue_hcf.h:123). */
     double fatigue_A, fatigue_B, fatigue_d, fatigue_limit_ratio;
+    /* C11 > 0: the (C11, C12, C44) overloads of setParticleProperty (particle_elastic.h:110-140,
+     * particle_elastic_damage.h:218-250) in place of E, mu and plane_stress (not for J2) */
+    double C11, C12, C44;
 } lpmo_desc;
 
 typedef struct

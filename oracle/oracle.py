@@ -39,6 +39,7 @@ class _Desc(C.Structure):
         ("k0", C.c_double), ("k1", C.c_double), ("comp_tensile_ratio", C.c_double), ("damage_threshold", C.c_double),
         ("fatigue_A", C.c_double), ("fatigue_B", C.c_double), ("fatigue_d", C.c_double),
         ("fatigue_limit_ratio", C.c_double),
+        ("C11", C.c_double), ("C12", C.c_double), ("C44", C.c_double),
     ]
 
 
@@ -168,6 +169,10 @@ class Material:
     fatigue_B: float = 0.0
     fatigue_d: float = 0.0
     fatigue_limit_ratio: float = 1.108
+    # setParticleProperty's (C11, C12, C44) overload; C11 > 0 takes it (particle_elastic.h:110-140)
+    C11: float = 0.0
+    C12: float = 0.0
+    C44: float = 0.0
 
 
 class _StepHolder:
@@ -214,6 +219,7 @@ class OracleProblem:
         d.k0, d.k1, d.comp_tensile_ratio, d.damage_threshold = mat.k0, mat.k1, mat.comp_tensile_ratio, mat.damage_threshold
         d.fatigue_A, d.fatigue_B = getattr(mat, "fatigue_A", 0.0), getattr(mat, "fatigue_B", 0.0)
         d.fatigue_d, d.fatigue_limit_ratio = getattr(mat, "fatigue_d", 0.0), getattr(mat, "fatigue_limit_ratio", 1.108)
+        d.C11, d.C12, d.C44 = getattr(mat, "C11", 0.0), getattr(mat, "C12", 0.0), getattr(mat, "C44", 0.0)
         if bonds is not None:
             self._bonds = [np.ascontiguousarray(a, dtype=np.int32) for a in bonds]
             d.bond_nb0, d.bond_nb1, d.bond_p2 = (_ip(a) for a in self._bonds)
@@ -404,6 +410,7 @@ def write_ref_spec(case, outdir: str, steps=None, max_iter=None, tol_iter=None, 
              f"euler {case.euler[0]} " + " ".join(repr(float(a)) for a in case.euler[1]),
              f"ptype {({2: 'j2', 1: 'elastic_damage', 3: 'fatigue_hcf'}).get(int(case.ptype), 'elastic')}",
              f"plane_stress {int(m.plane_stress)}",
+             f"cij {getattr(m, 'C11', 0.0)!r} {getattr(m, 'C12', 0.0)!r} {getattr(m, 'C44', 0.0)!r}",
              f"hcf {getattr(m, 'fatigue_A', 0.0)!r} {getattr(m, 'fatigue_B', 0.0)!r} {getattr(m, 'fatigue_d', 0.0)!r} "
              f"{getattr(m, 'damage_threshold', 1.0)!r} {getattr(m, 'fatigue_limit_ratio', 1.108)!r}",
              f"edamage {getattr(m, 'k0', 0.0)!r} {getattr(m, 'k1', 1.0)!r} {getattr(m, 'comp_tensile_ratio', 10.0)!r} "

@@ -59,6 +59,9 @@
  *   fatigue_load PATH     (the load spectrum, SolverFatigue::readLoad)
  *   solver cg|pardiso     (the SolverMode of the solver: Solver::LPM_CG or Solver::LPM_PARDISO,
  *                          include/solver.h:191-354; default cg)
+ *   cij C11 C12 C44       (C11 > 0: the (C11, C12, C44) overload of setParticleProperty for elastic
+ *                          and elastic-damage particles, include/particle_elastic.h:110-140,
+ *                          include/particle_elastic_damage.h:218-250)
  */
 #include <cstdio>
 #include <cstdlib>
@@ -161,6 +164,7 @@ struct Spec
     double fatigue_tau = 1;
     std::vector<std::string> fatigue_groups;
     std::string solver = "cg";
+    double C11 = 0, C12 = 0, C44 = 0;
 };
 
 static std::vector<int> read_i32(const std::string &path)
@@ -282,6 +286,7 @@ static Spec parse(const char *path)
         else if (k == "fatigue") is >> s.fatigue_type >> s.fatigue_interval >> s.fatigue_tmode >> s.fatigue_tau;
         else if (k == "fatigue_load") is >> s.fatigue_load;
         else if (k == "solver") is >> s.solver;
+        else if (k == "cij") is >> s.C11 >> s.C12 >> s.C44;
         else if (k == "fatigue_groups")
         {
             std::string g;
@@ -637,12 +642,18 @@ int main(int argc, char **argv)
         if (pt == ParticleType::J2Plasticity)
             dynamic_cast<ParticleJ2Plasticity<NL> *>(p)->setParticleProperty(
                 sp.nonlocal_L, sp.plane_stress != 0, sp.E, sp.mu, sp.sigmay, sp.xi, sp.H, sp.A, sp.critical_bstrain);
+        else if (pt == ParticleType::ElasticDamage && sp.C11 > 0)
+            dynamic_cast<ParticleElasticDamage<NL> *>(p)->setParticleProperty(sp.nonlocal_L, sp.C11, sp.C12, sp.C44,
+                                                                              sp.k0, sp.k1, sp.ct_ratio, sp.d_thres);
         else if (pt == ParticleType::ElasticDamage)
             dynamic_cast<ParticleElasticDamage<NL> *>(p)->setParticleProperty(
                 sp.nonlocal_L, sp.plane_stress != 0, sp.E, sp.mu, sp.k0, sp.k1, sp.ct_ratio, sp.d_thres);
         else if (pt == ParticleType::FatigueHCF)
             dynamic_cast<ParticleFatigueHCF<NL> *>(p)->setParticleProperty(
                 sp.nonlocal_L, sp.plane_stress != 0, sp.E, sp.mu, sp.hcf_A, sp.hcf_B, sp.hcf_d, sp.hcf_thres, sp.hcf_flr);
+        else if (sp.C11 > 0)
+            dynamic_cast<ParticleElastic<NL> *>(p)->setParticleProperty(sp.nonlocal_L, sp.C11, sp.C12, sp.C44,
+                                                                        sp.critical_bstrain);
         else
             dynamic_cast<ParticleElastic<NL> *>(p)->setParticleProperty(sp.nonlocal_L, sp.plane_stress != 0, sp.E,
                                                                         sp.mu, sp.critical_bstrain);

@@ -24,7 +24,8 @@ def oracle_problem(case, cg_rtol=1e-12, cg_atol=1e-12, tol_iter=None, max_iter=N
                      critical_bstrain=m.critical_bstrain, sigmay=m.sigmay, xi=m.xi, H=m.H, A=m.A,
                      nonlocal_L=m.nonlocal_L, k0=m.k0, k1=m.k1, comp_tensile_ratio=m.comp_tensile_ratio,
                      damage_threshold=m.damage_threshold, fatigue_A=m.fatigue_A, fatigue_B=m.fatigue_B,
-                     fatigue_d=m.fatigue_d, fatigue_limit_ratio=m.fatigue_limit_ratio)
+                     fatigue_d=m.fatigue_d, fatigue_limit_ratio=m.fatigue_limit_ratio, C11=m.C11, C12=m.C12,
+                     C44=m.C44)
     o = O.OracleProblem(LAT_NAME[int(case.lattice)], case.radius, case.xyz, mat, types=case.types,
                         undamaged_type=case.undamaged_type,
                         max_iter=case.max_iter if max_iter is None else max_iter,

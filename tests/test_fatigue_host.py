@@ -100,3 +100,20 @@ def test_solver_modes_map_to_cg_tolerances():
     assert LPM._cg_tolerances(LPM.SolverMode.CG, None, None) == (1e-12, 1e-12)
     assert LPM._cg_tolerances(LPM.SolverMode.PARDISO, None, None) == (1e-24, 0.0)
     assert LPM._cg_tolerances(LPM.SolverMode.PARDISO, 1e-20, 1e-30) == (1e-20, 1e-30)
+
+
+def test_set_particle_property_cubic_overload():
+    """The (C11, C12, C44) overloads (particle_elastic.h:111, particle_elastic_damage.h:219) are
+    taken when the second argument is a number, and reach lpmgpu_desc."""
+    c = CFG.fcc_cubic_cube()
+    a = c.assembly()
+    a.setParticleProperty(0.5, 108e3, 61e3, 29e3, 0.01)
+    m = a.material
+    assert (m.C11, m.C12, m.C44, m.critical_bstrain, m.nonlocal_L) == (108e3, 61e3, 29e3, 0.01, 0.5)
+    d, _ = LPM._pack_desc(a)
+    assert (d.C11, d.C12, d.C44) == (108e3, 61e3, 29e3)
+    e = CFG.edamage_plate().assembly()
+    e.setParticleProperty(0.3, 90e3, 40e3, 25e3, 0.02, 0.5, 10.0, 0.9)
+    assert (e.material.C11, e.material.k0, e.material.damage_threshold) == (90e3, 0.02, 0.9)
+    a.setParticleProperty(0.5, False, 69e3, 0.3, 1.0)  # a bool: the isotropic overload
+    assert a.material.C11 == 0.0 and a.material.E == 69e3
