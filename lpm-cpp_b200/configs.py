@@ -319,6 +319,32 @@ def fatigue_plate(size=2.4, radius=0.1, E=69e3, mu=0.3, amplitude=0.004, cycles=
     return c
 
 
+def fatigue_cube(size=2.0, radius=0.2, E=69e3, mu=0.3, amplitude=0.004, cycles=4, n_interval=2, tau=0.5,
+                 A=15.0, B=2.833, d=0.5, damage_threshold=1.0, nonlocal_L=0.6, cutoff_ratio=1.5, tol_iter=1e-9,
+                 max_iter=30) -> Case:
+    """A simple-cubic cube of fatigue HCF particles under the LoadDogBoneDisp cycle
+    (load_step_fatigue.h:53-69), as examples/ex5_isoelasticity_3d_fatigue.cpp loads its specimen:
+    the top layer (largest y) moved in y and held in x and z, the bottom layer held in x, y and z.
+    One static step at zero load, then `cycles` cycles of the spectrum 0, amplitude, 0, ..."""
+    c = sc_cube(size=size, radius=radius, E=E, mu=mu, steps=1, total_disp=0.0, tol_iter=tol_iter, max_iter=max_iter)
+    c.name = f"fatigue_sc_{size:g}mm"
+    c.ptype = L.ParticleType.FatigueHCF
+    y = c.xyz[:, 1]
+    c.groups = {"top": np.nonzero(y > y.max() - radius)[0].astype(np.int32),
+                "bottom": np.nonzero(y < y.min() + radius)[0].astype(np.int32)}
+    c.types = np.zeros(c.n, np.int32)
+    c.steps = [([("top", "x", 0.0), ("top", "y", 0.0), ("top", "z", 0.0), ("bottom", "x", 0.0),
+                 ("bottom", "y", 0.0), ("bottom", "z", 0.0)], [])]
+    m = c.material
+    m.fatigue_A, m.fatigue_B, m.fatigue_d = A, B, d
+    m.damage_threshold, m.nonlocal_L = damage_threshold, nonlocal_L
+    c.nonlocal_cutoff_ratio = cutoff_ratio
+    spectrum = [0.0] + [v for _ in range(cycles) for v in (amplitude, 0.0)]
+    c.meta["fatigue"] = {"load_type": "dogbone_disp", "n_interval": n_interval, "tmode": "linear", "tau": tau,
+                         "spectrum": spectrum, "groups": ["top", "bottom"]}
+    return c
+
+
 def batched_notched_plates(count=64, seed=20240604, steps=40, radius=0.1, side=(4.0, 25.0), crack=(0.2, 0.5),
                            E=(60e3, 120e3), critical_bstrain=(1e-3, 3e-3), opening=0.45, crack_ref=1.5,
                            tol_iter=1e-5, max_iter=30) -> List[Case]:
