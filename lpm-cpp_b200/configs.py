@@ -307,6 +307,11 @@ def fatigue_plate(size=2.4, radius=0.1, E=69e3, mu=0.3, amplitude=0.004, cycles=
     c.groups["left"] = np.nonzero(x < x.min() + 1.5 * radius)[0].astype(np.int32)
     if load_type == "uniaxial_force":  # the top edge stays free in y: the force moves it
         c.steps = [([("left", "x", 0.0), ("bottom", "y", 0.0)], [])]
+    elif load_type == "ct_force":  # LoadCTForce (load_step_fatigue.h:71-87): mid row held in y,
+        y = c.xyz[:, 1]             # top and bottom edges held in x and pulled apart in y
+        ymid = 0.5 * (y.min() + y.max())
+        c.groups["mid"] = np.nonzero(np.abs(y - ymid) < radius)[0].astype(np.int32)
+        c.steps = [([("mid", "y", 0.0), ("top", "x", 0.0), ("bottom", "x", 0.0)], [])]
     else:
         c.steps = [([("left", "x", 0.0), ("top", "y", 0.0), ("bottom", "y", 0.0)], [])]
     m = c.material
@@ -314,8 +319,9 @@ def fatigue_plate(size=2.4, radius=0.1, E=69e3, mu=0.3, amplitude=0.004, cycles=
     m.damage_threshold, m.fatigue_limit_ratio, m.nonlocal_L = damage_threshold, fatigue_limit_ratio, nonlocal_L
     c.nonlocal_cutoff_ratio = cutoff_ratio
     spectrum = [0.0] + [v for _ in range(cycles) for v in (amplitude, 0.0)]
+    groups = ["mid", "top", "bottom"] if load_type == "ct_force" else ["left", "top", "bottom"]
     c.meta["fatigue"] = {"load_type": load_type, "n_interval": n_interval, "tmode": tmode, "tau": tau,
-                         "spectrum": spectrum, "groups": ["left", "top", "bottom"]}
+                         "spectrum": spectrum, "groups": groups}
     return c
 
 
