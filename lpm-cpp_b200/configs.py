@@ -287,7 +287,8 @@ def edamage_plate(size=2.4, radius=0.1, E=69e3, mu=0.3, steps=4, total_disp=0.00
 
 def fatigue_plate(size=2.4, radius=0.1, E=69e3, mu=0.3, amplitude=0.004, cycles=8, n_interval=2, tau=0.5,
                   tmode="linear", A=15.0, B=2.833, d=0.5, damage_threshold=1.0, fatigue_limit_ratio=1.108,
-                  nonlocal_L=0.3, cutoff_ratio=1.5, tol_iter=1e-9, max_iter=30, load_type="uniaxial_disp") -> Case:
+                  nonlocal_L=0.3, cutoff_ratio=1.5, tol_iter=1e-9, max_iter=30, load_type="uniaxial_disp",
+                  undamaged_band=0.0) -> Case:
     """Hexagonal plate of ParticleFatigueHCF particles (include/particle_fatigue_hcf.h) under the
     constant-amplitude displacement cycles of SolverFatigue (include/solver_fatigue.h) with the
     LoadUniaxialDisp cycle (include/load_step_fatigue.h:39-50): left edge fixed in x, bottom edge
@@ -295,7 +296,11 @@ def fatigue_plate(size=2.4, radius=0.1, E=69e3, mu=0.3, amplitude=0.004, cycles=
     sets the constraints, as ex5_isoelasticity_2d_fatigue.cpp does before its cycles), then the
     spectrum 0, amplitude, 0, amplitude, ..., 0 of `cycles` cycles.  load_type "uniaxial_force"
     takes the LoadUniaxialForce cycle instead (load_step_fatigue.h:23-36): the top edge pulled by a
-    force of `amplitude` N shared by its particles.  Each simulated cycle stands
+    force of `amplitude` N shared by its particles, and "ct_force" the LoadCTForce cycle (the middle
+    row held in y, the top and bottom edges held in x and pulled apart by +/- `amplitude` N).
+    undamaged_band > 0 gives the particles within that distance of the top and bottom edges type 3,
+    the undamaged type, outside the loaded edge groups (types 1 and 2), as
+    examples/ex5_isoelasticity_2d_fatigue.cpp types the grips of its specimen.  Each simulated cycle stands
     for dN/dt = (int)(1 / tau) real cycles (TimeMapMode::Linear, solver_fatigue.h:60-63); the
     damage rate per cycle is A * pow(largest energy, B) * pow(energy range, d), averaged over the
     nonlocal neighbours within cutoff_ratio x nonlocal_L."""
@@ -314,6 +319,12 @@ def fatigue_plate(size=2.4, radius=0.1, E=69e3, mu=0.3, amplitude=0.004, cycles=
         c.steps = [([("mid", "y", 0.0), ("top", "x", 0.0), ("bottom", "x", 0.0)], [])]
     else:
         c.steps = [([("left", "x", 0.0), ("top", "y", 0.0), ("bottom", "y", 0.0)], [])]
+    if undamaged_band > 0:
+        y = c.xyz[:, 1]
+        far = (y > y.max() - undamaged_band) | (y < y.min() + undamaged_band)
+        c.types = c.types.copy()
+        c.types[far & (c.types == 0)] = 3
+        c.undamaged_type = 3
     m = c.material
     m.fatigue_A, m.fatigue_B, m.fatigue_d = A, B, d
     m.damage_threshold, m.fatigue_limit_ratio, m.nonlocal_L = damage_threshold, fatigue_limit_ratio, nonlocal_L

@@ -94,6 +94,8 @@ def cases():
         # the exponential time map: dN/dt = (int)(1/tau exp(t/tau)) is 0, 0, 1, 2, 3 at tau = 2
         "hex_fatigue_exp": (lambda: CFG.fatigue_plate(cycles=4, tmode="exponential", tau=2.0, A=40.0),
                             {"cg_tol": (1e-24, 0.0), "fatigue": True}),
+        # undamaged grips (type 3 near the top and bottom edges), as ex5_isoelasticity_2d_fatigue
+        "hex_fatigue_grips": (lambda: CFG.fatigue_plate(undamaged_band=0.5), {"cg_tol": (1e-24, 0.0), "fatigue": True}),
         # the LoadCTForce cycle: middle row held in y, top and bottom edges pulled apart
         "hex_fatigue_ct": (lambda: CFG.fatigue_plate(load_type="ct_force", amplitude=250.0, cycles=4, tol_iter=1e-7),
                            {"cg_tol": (1e-24, 0.0), "fatigue": True}),

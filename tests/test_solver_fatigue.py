@@ -38,12 +38,13 @@ def _oracle_run(case):
 
 @pytest.mark.parametrize("load,precision,dtol,ktol", [("disp", 0, 1e-8, 1e-9), ("disp", 1, 1e-6, 1e-5),
                                                       ("force", 0, 1e-8, 1e-9), ("dogbone3d", 0, 1e-8, 1e-9),
-                                                      ("ct", 0, 1e-8, 1e-9)])
+                                                      ("ct", 0, 1e-8, 1e-9), ("grips", 0, 1e-8, 1e-9)])
 def test_fatigue_cycles_match_oracle(load, precision, dtol, ktol):
     case = {"disp": lambda: CFG.fatigue_plate(),
             "force": lambda: CFG.fatigue_plate(load_type="uniaxial_force", amplitude=200.0, cycles=4, tol_iter=1e-7),
             "dogbone3d": lambda: CFG.fatigue_cube(),
-            "ct": lambda: CFG.fatigue_plate(load_type="ct_force", amplitude=250.0, cycles=4, tol_iter=1e-7)}[load]()
+            "ct": lambda: CFG.fatigue_plate(load_type="ct_force", amplitude=250.0, cycles=4, tol_iter=1e-7),
+            "grips": lambda: CFG.fatigue_plate(undamaged_band=0.5)}[load]()
     amp = fatigue_disp_scale(case)
     ref = _oracle_run(case)
     g = gpu_problem(case, precision=precision, **TIGHT)
