@@ -526,9 +526,68 @@ def fatigue_leg(lpm, device, size=25.0, cycles=4):
             out["speedup_vs_reference"] = wall_r / wall
             out["max_abs_damage_diff_vs_reference"] = float(np.abs(sg["damage"] - dr).max())
             out["max_abs_disp_diff_vs_reference_over_amplitude"] = float(np.abs(sg["xyz"] - xr).max() / amp)
+        try:
+            out["batched"] = fatigue_batch_sample(lpm, device)
+        except Exception as ex:  # keeps the single-specimen numbers above
+            out["batched"] = {"error": f"{type(ex).__name__}: {ex}"}
         return out
     except Exception as ex:  # the leg must not cost the bench line
         return {"error": f"{type(ex).__name__}: {ex}"}
+
+
+def fatigue_batch_sample(lpm, device, sizes=(4.0, 5.0, 6.0, 7.0, 8.0, 9.0, 10.0, 12.0)):
+    """Eight fatigue plates of uneven size (the 2.4 mm test plate's strain and rate law, one static
+    step and two simulated cycles each): one at a time through the C ABI's fatigue steps, then all
+    as fatigue members of one batch (lpmgpu_batch_add_fatigue); wall time of each, problem
+    creation untimed, and the largest damage difference between the two."""
+    import torch
+    cfg = importlib.import_module("lpm-cpp_b200.configs")
+    cases = [cfg.fatigue_plate(size=sz, radius=0.1, cycles=4, amplitude=0.004 * sz / 2.4, tol_iter=1e-5)
+             for sz in sizes]
+    cyc = []
+    for c in cases:
+        fat, N, lst = c.meta["fatigue"], 0, []
+        while True:
+            steps = lpm.generateLoadCycle(lpm.FatigueLoadType.LoadUniaxialDisp, fat["spectrum"], N, fat["n_interval"],
+                                          [c.groups[g] for g in fat["groups"]])
+            d = lpm.func_dNdt_linear(fat["tau"])
+            lst.append((steps, d))
+            N += d
+            if not N < 0.5 * (len(fat["spectrum"]) - 1):
+                break
+        cyc.append(lst)
+
+    def make(c):
+        return lpm.GpuProblem(c.assembly(), undamaged_pt_type=c.undamaged_type, max_iter=c.max_iter,
+                              tol_iter=c.tol_iter, device=device)
+    probs = [make(c) for c in cases]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for g, c, lst in zip(probs, cases, cyc):
+        g.fatigue_static_step(c.load_step(0))
+        for steps, d in lst:
+            g.fatigue_cycle(steps, d)
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    dmg_plain = [g.state(("damage",))["damage"] for g in probs]
+    for g in probs:
+        g.close()
+    probs = [make(c) for c in cases]
+    b = lpm.Batch(device)
+    for g, c, lst in zip(probs, cases, cyc):
+        b.add_fatigue(g, [c.load_step(0)], [x[0] for x in lst], [x[1] for x in lst])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.run()
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    diff = max(float(np.abs(g.state(("damage",))["damage"] - d0).max()) for g, d0 in zip(probs, dmg_plain))
+    b.close()
+    for g in probs:
+        g.close()
+    return {"specimens": len(cases), "particles": int(sum(c.n for c in cases)),
+            "plain_s": t_plain, "batched_s": t_batch, "speedup_batched_vs_plain": t_plain / t_batch,
+            "max_damage_diff_batched_vs_plain": diff}
 
 
 def batched_leg(lpm, count, device, world, allreduce):
