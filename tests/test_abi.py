@@ -106,3 +106,21 @@ def test_tune_result_layout_matches_the_header():
     assert m and int(m.group(1)) == 8
     assert LPM.TuneResult.us_per_iter.offset == 4 * 4 + 8 * 4
     assert C.sizeof(LPM.TuneResult) == 4 * 4 + 8 * 4 + 8 * 8
+
+
+def test_estimate_counts_explicit_nonlocal_lists():
+    """Nonlocal lists handed over in lpmgpu_desc (nonlocal_count / nonlocal_ids, as the C++
+    drop-ins pass an Assembly's own) count exactly in the admission estimate: 4 bytes an entry
+    plus an offset and a rate per particle."""
+    c = CFG.hex_plate(size=2.0, radius=0.1)
+    a = c.assembly()
+    d, keep = LPM._pack_desc(a)
+    base = C.c_int64()
+    assert LPM.lib().lpmgpu_estimate_bytes(C.byref(d), C.byref(base)) == 0
+    cnt = np.full(c.n, 7, np.int32)
+    ids = np.zeros(7 * c.n, np.int32)
+    d.nonlocal_count = cnt.ctypes.data_as(C.POINTER(C.c_int32))
+    d.nonlocal_ids = ids.ctypes.data_as(C.POINTER(C.c_int32))
+    with_lists = C.c_int64()
+    assert LPM.lib().lpmgpu_estimate_bytes(C.byref(d), C.byref(with_lists)) == 0
+    assert with_lists.value - base.value == 4 * 7 * c.n + 12 * c.n
