@@ -345,6 +345,8 @@ def run_ours(a):
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(case, a.cpu_cg_cap)
+        if cpu is not None and cpu.get("kind") == "reference":
+            cpu["parity"] = reference_parity(lpm, local)
     # last, after every other measurement: the newest device path
     fatigue = None
     if single and not a.no_fatigue:
@@ -809,6 +811,43 @@ def _ref_sample(case, steps, cg_cap, threads, timeout=1800):
         return rows, setup
     finally:
         shutil.rmtree(d, ignore_errors=True)
+
+
+def reference_parity(lpm, device, size=6.0, steps=3):
+    """The errors of the device solutions against the reference's own FP64 solution: the SC cube of
+    the headline workload at `size` mm (r = 0.2), `steps` load steps, the bench's Newton tolerance
+    and the reference's CG test, solved by oracle/_ref/lpm_ref single-threaded (its multi-threaded
+    assembly races) and on the device in FP64 and mixed precision.  Per arm: the largest relative
+    displacement error over the steps and the relative error of the reaction-force norm."""
+    try:
+        from oracle import oracle as O
+        case, desc = workload("sc3d", size)
+        case.steps = case.steps[:steps]
+        d = tempfile.mkdtemp(prefix="lpmref_parity_")
+        try:
+            O.run_ref(O.write_ref_spec(case, d, steps=steps, tol_iter=NEWTON_TOL, loop="step"), d, threads=1,
+                      timeout=1800)
+            rows = O.read_ref_steps(d)
+            x0 = O.read_bin(d, "xyz0.f64", np.float64).reshape(-1, 3)
+            ref = [O.read_bin(d, f"xyz_{s:03d}.f64", np.float64).reshape(-1, 3) - x0 for s in range(steps)]
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
+        out = {"workload": f"{desc}, first {steps} steps", "reference": "oracle/_ref/lpm_ref, 1 thread"}
+        for key, prec in (("fp64", lpm.Precision.FP64), ("mixed", lpm.Precision.MIXED)):
+            g = lpm.GpuProblem(case.assembly(), undamaged_pt_type=case.undamaged_type, max_iter=case.max_iter,
+                               tol_iter=NEWTON_TOL, precision=prec, device=device)
+            disp_err, reac_err = 0.0, 0.0
+            for s in range(steps):
+                ok, st = g.solve_load_step(step_of(case, s))
+                u = g.state(("xyz",))["xyz"] - case.xyz
+                disp_err = max(disp_err, float(np.linalg.norm(u - ref[s]) / np.linalg.norm(ref[s])))
+                rn = rows[s]["reaction_norm"]
+                reac_err = max(reac_err, abs(st["reaction_norm"] - rn) / rn)
+            g.close()
+            out[key] = {"rel_disp_err_vs_reference": disp_err, "rel_reaction_err_vs_reference": reac_err}
+        return out
+    except Exception as ex:  # the parity figures must not cost the bench line
+        return {"error": f"{type(ex).__name__}: {ex}"}
 
 
 def cpu_baseline(case, cg_cap):
