@@ -267,16 +267,26 @@ def cantilever_beam(radius=0.12, length=30.0, depth=10.0, force=2.0, E=69e3, mu=
 
 
 def edamage_plate(size=2.4, radius=0.1, E=69e3, mu=0.3, steps=4, total_disp=0.008, k0=0.02, k1=0.5,
-                  damage_threshold=0.9, nonlocal_L=0.3, cutoff_ratio=1.5, tol_iter=1e-9, max_iter=30) -> Case:
+                  damage_threshold=0.9, nonlocal_L=0.3, cutoff_ratio=1.5, tol_iter=1e-9, max_iter=30,
+                  undamaged_band=0.0) -> Case:
     """Hexagonal plate of ParticleElasticDamage particles (include/particle_elastic_damage.h) with
     the nonlocal damage of SolverStatic::updateStaticDamage (solver_static.h:32-62): the bottom edge
     fixed, the top edge pulled in y (the groups of ex1_isoelasticity_2d_hex).  Damage grows once
     the strain energy density passes k0 + k1 D; the local rates are averaged over the neighbours
-    within cutoff_ratio x nonlocal_L (Assembly::searchNonlocalNeighbors, assembly.h:118-130)."""
+    within cutoff_ratio x nonlocal_L (Assembly::searchNonlocalNeighbors, assembly.h:118-130).
+    undamaged_band > 0 gives the particles within that distance of the top and bottom edges,
+    outside the loaded edge groups, type 3 and makes 3 the undamaged type: they take no damage
+    and are left out of the averaging (solver_static.h:37-57)."""
     c = hex_plate(size=size, radius=radius, E=E, mu=mu, steps=steps, total_disp=total_disp, tol_iter=tol_iter,
                   max_iter=max_iter)
     c.name = f"edamage_hex_{size:g}mm"
     c.ptype = L.ParticleType.ElasticDamage
+    if undamaged_band > 0:
+        y = c.xyz[:, 1]
+        far = (y > y.max() - undamaged_band) | (y < y.min() + undamaged_band)
+        c.types = c.types.copy()
+        c.types[far & (c.types == 0)] = 3
+        c.undamaged_type = 3
     c.material.k0, c.material.k1, c.material.damage_threshold = k0, k1, damage_threshold
     c.material.nonlocal_L = nonlocal_L
     c.nonlocal_cutoff_ratio = cutoff_ratio

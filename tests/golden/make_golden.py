@@ -87,6 +87,8 @@ def cases():
         # ParticleElasticDamage with the nonlocal damage rate (searchNonlocalNeighbors + the
         # averaging of SolverStatic::updateStaticDamage): damage grows in every step
         "hex_edamage": (lambda: CFG.edamage_plate(), {"cg_tol": (1e-24, 0.0), "dump_k": (1,)}),
+        # undamaged grips (type 3): no damage there, and left out of the nonlocal averaging
+        "hex_edamage_grips": (lambda: CFG.edamage_plate(undamaged_band=0.5), {"cg_tol": (1e-24, 0.0), "dump_k": (1,)}),
         # FCC with cubic elastic constants (setParticleProperty's (C11, C12, C44) overload, as ex3)
         "fcc_cubic": (lambda: CFG.fcc_cubic_cube(), {"cg_tol": (1e-24, 0.0), "dump_k": (0,)}),
         # SolverFatigue: one static step, then four cycles (two steps up, two down) of HCF damage
