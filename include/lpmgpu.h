@@ -188,6 +188,11 @@ int32_t lpmgpu_get_sizes(const lpmgpu_solver *h, lpmgpu_sizes *out);
 int32_t lpmgpu_get_topology(const lpmgpu_solver *h, int32_t *nb0, int32_t *nb1, int32_t *bond_p2,
                             int32_t *nconn, int32_t *nlq, int32_t *conns);
 
+/* The nonlocal neighbour lists the problem holds (Particle::neighbors_nonlocal, particle.h:37,
+ * as Assembly::searchNonlocalNeighbors builds them, assembly.h:118-130: ascending id).  count
+ * (n) and ids (the lists concatenated) may be NULL; *total gets the number of ids, 0 when the
+ * problem has no lists. */
+int32_t lpmgpu_get_nonlocal(const lpmgpu_solver *h, int32_t *count, int32_t *ids, int64_t *total);
 /* Assembly::updateGeometry + updateForceState (assembly.h:133-138, 179-191) */
 int32_t lpmgpu_update_force_state(lpmgpu_solver *h);
 /* Assembly::updateStateVar (assembly.h:162-166): the J2 return map, the elastic-damage or the

@@ -11,6 +11,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "lpm_internal.cuh"
 
@@ -867,6 +868,27 @@ int32_t lpmgpu_get_topology(const lpmgpu_solver *h, int32_t *nb0, int32_t *nb1, 
         CK(cudaMemcpy(nlq, p.nlq, sizeof(int) * n, cudaMemcpyDeviceToHost));
     if (conns)
         CK(cudaMemcpy(conns, p.conns, sizeof(int) * p.nnzb, cudaMemcpyDeviceToHost));
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_get_nonlocal(const lpmgpu_solver *h, int32_t *count, int32_t *ids, int64_t *total)
+{
+    if (!h || !total)
+        return LPMGPU_ERR_INVALID_ARG;
+    const Problem &p = h->p;
+    CK(cudaSetDevice(p.device));
+    *total = p.nlist ? p.nnl : 0;
+    if (!p.nlist)
+        return LPMGPU_OK;
+    if (count)
+    {
+        std::vector<int> start((size_t)p.n + 1);
+        CK(cudaMemcpy(start.data(), p.nlstart, sizeof(int) * ((size_t)p.n + 1), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < p.n; ++i)
+            count[i] = start[i + 1] - start[i];
+    }
+    if (ids && p.nnl > 0)
+        CK(cudaMemcpy(ids, p.nlist, sizeof(int) * (size_t)p.nnl, cudaMemcpyDeviceToHost));
     return LPMGPU_OK;
 }
 

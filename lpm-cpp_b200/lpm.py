@@ -197,7 +197,7 @@ EXPORTS = [
     "lpmgpu_fatigue_solve_step", "lpmgpu_fatigue_static_step", "lpmgpu_fatigue_update_damage", "lpmgpu_fatigue_cycle",
     "lpmgpu_read_state", "lpmgpu_read_residual", "lpmgpu_set_xyz", "lpmgpu_get_phase_times",
     "lpmgpu_get_counters", "lpmgpu_get_stream", "lpmgpu_cg_bsr_noalloc", "lpmgpu_autotune", "lpmgpu_set_cg_grid",
-    "lpmgpu_solve_direct", "lpmgpu_band_order",
+    "lpmgpu_solve_direct", "lpmgpu_band_order", "lpmgpu_get_nonlocal",
     "lpmgpu_format_dump", "lpmgpu_dump_write", "lpmgpu_dump_flush",
     "lpmgpu_batch_create", "lpmgpu_batch_destroy", "lpmgpu_batch_add", "lpmgpu_batch_add_fatigue",
     "lpmgpu_batch_round", "lpmgpu_batch_run",
@@ -255,6 +255,7 @@ def lib():
         "lpmgpu_autotune": (C.c_int32, [vp, C.c_int32, C.POINTER(TuneResult)]),
         "lpmgpu_solve_direct": (C.c_int32, [vp, dp, C.POINTER(Stats)]),
         "lpmgpu_band_order": (C.c_int32, [C.c_int32, ip, ip, ip, lp]),
+        "lpmgpu_get_nonlocal": (C.c_int32, [vp, ip, ip, lp]),
         "lpmgpu_set_cg_grid": (C.c_int32, [vp, C.c_int32]),
         "lpmgpu_cg_bsr_noalloc": (C.c_int32, [C.c_int32, C.c_int32, vp, vp, vp, vp, vp, C.c_double, C.c_double,
                                               C.c_int64, vp, C.POINTER(C.c_int64)]),
@@ -749,6 +750,18 @@ class GpuProblem:
 
     def assemble(self, apply_bc=True):
         _check(lib().lpmgpu_assemble(self._h, int(apply_bc)), "lpmgpu_assemble")
+
+    def nonlocal_lists(self):
+        """(count per particle, concatenated ids) of the nonlocal neighbour lists, or None when the
+        problem has none (lpmgpu_get_nonlocal)."""
+        total = C.c_int64(0)
+        _check(lib().lpmgpu_get_nonlocal(self._h, None, None, C.byref(total)), "lpmgpu_get_nonlocal")
+        if total.value == 0:
+            return None
+        cnt = np.zeros(self.n, np.int32)
+        ids = np.zeros(total.value, np.int32)
+        _check(lib().lpmgpu_get_nonlocal(self._h, _ip(cnt), _ip(ids), C.byref(total)), "lpmgpu_get_nonlocal")
+        return cnt, ids
 
     def solve_direct(self):
         """The band Cholesky solve of the current K and residual (lpmgpu_solve_direct): the

@@ -273,3 +273,36 @@ def test_grid_nonlocal_search_gives_the_all_pairs_run():
         g.close()
     for k in states[0]:
         assert np.array_equal(states[0][k], states[1][k]), k
+
+
+def test_device_nonlocal_lists_at_scale():
+    """The nonlocal lists of a 26 mm plate (19,500 particles: the cell-grid search) read back from
+    the device (lpmgpu_get_nonlocal) equal the all-pairs lists, both the device's own
+    (LPMGPU_NL_GRID=0) and numpy's: every particle within cutoff_ratio x nonlocal_L, by
+    Particle::distanceTo's arithmetic, in ascending id."""
+    import os
+    from scipy.spatial import cKDTree
+    c = CFG.fatigue_plate(size=26.0)
+    assert c.n > 16384
+    rc = c.nonlocal_cutoff_ratio * c.material.nonlocal_L
+    lists = []
+    for mode in (None, "0"):
+        if mode is not None:
+            os.environ["LPMGPU_NL_GRID"] = mode
+        try:
+            g = gpu_problem(c)
+        finally:
+            os.environ.pop("LPMGPU_NL_GRID", None)
+        lists.append(g.nonlocal_lists())
+        g.close()
+    (cg, ig), (ca, ia) = lists
+    assert np.array_equal(cg, ca) and np.array_equal(ig, ia)
+    x = c.xyz
+    cand = cKDTree(x).query_ball_point(x, rc * (1 + 1e-9))
+    start = np.concatenate([[0], np.cumsum(cg)])
+    for i in range(c.n):
+        js = np.array(sorted(cand[i]), dtype=np.int64)
+        d = x[i] - x[js]
+        dist = np.sqrt(d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1] + d[:, 2] * d[:, 2])
+        want = js[dist < rc]
+        assert np.array_equal(ig[start[i]:start[i + 1]], want), i
