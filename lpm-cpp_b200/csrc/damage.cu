@@ -1,4 +1,4 @@
-// Nonlocal damage and the elastic-damage particle on the device:
+// Nonlocal damage, the elastic-damage and fatigue particles on the device:
 //   Assembly::searchNonlocalNeighbors                  include/assembly.h:118-130
 //   SolverStatic::updateStaticDamage (nonlocal rate)   include/solver_static.h:32-52, func_phi lpm.h:49-53
 //   ParticleElasticDamage::updateParticleStateVariables include/particle_elastic_damage.h:159-170
@@ -8,7 +8,10 @@
 //   SolverFatigue::updateFatigueDamage                 include/solver_fatigue.h:76-126
 //     with updateParticleFatigueDamage                 include/particle_fatigue_hcf.h:148-160
 // The search keeps the reference's neighbour order (ascending id, the order of its inner loop),
-// so the weighted sums of the averaging add in the reference's order.
+// so the weighted sums of the averaging add in the reference's order.  It tests all pairs up to
+// kNlAllPairsMax particles and bins them into cells above (nonlocal_grid.cuh), with the same
+// distance test and each list sorted to ascending id; the caller may also hand over its own
+// lists (build_nonlocal_lists).
 #include <cub/cub.cuh>
 
 #include <cstdlib>
