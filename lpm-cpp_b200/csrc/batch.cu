@@ -25,7 +25,9 @@
 // on Newton failure reset + halve + run both halves.  A round issues every member's next piece
 // of device work on the member's stream, one batched CG for all members that need a linear
 // solve, and then waits once for all of them before the host takes the members' decisions.
-// Also the nonlocal damage and elastic-damage particles, through the same per-member kernels.
+// Also the nonlocal damage and elastic-damage particles, through the same per-member kernels,
+// and fatigue members (lpmgpu_batch_add_fatigue): SolverFatigue's static steps and cycles
+// (include/solver_fatigue.h:221-302), whose steps go through the same rounds.
 #include <algorithm>
 #include <chrono>
 #include <cmath>

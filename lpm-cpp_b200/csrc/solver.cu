@@ -5,6 +5,11 @@
 //   SolverStatic::solveProblemStep    include/solver_static.h:99-152
 //   SolverStatic::solveProblem        include/solver_static.h:65-96 (one load step per call)
 //   Assembly::storeStateVar / resetStateVar  include/assembly.h:141-159
+//   SolverFatigue::solveProblemStep / solveProblemStatic / solveProblemOneCycle /
+//     updateFatigueDamage             include/solver_fatigue.h:76-302 (lpmgpu_fatigue_*)
+// The force-state sequence of every Newton iteration and the state store / reset are captured
+// into CUDA graphs when a problem is created and replayed (run_graph); the linear solve is the
+// CG of cg.cu or, with desc.direct, the band Cholesky of direct.cu.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
