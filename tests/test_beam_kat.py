@@ -66,39 +66,3 @@ def test_beam_known_answer_matches_the_reference_run(tmp_path):
     assert rel(x_o - case.xyz, x_ref - case.xyz) <= 1e-8
     assert abs(beam_l2_error(case.xyz, x_o, *args) - e_ref) <= 1e-8 * e_ref
     assert abs(e_ref - BEAM_L2_REFERENCE) <= 1e-8 * BEAM_L2_REFERENCE
-
-
-@pytest.mark.gpu
-@pytest.mark.parametrize("precision,tol", [(0, 1e-8), (1, 1e-6)])
-def test_device_beam_force_bc_known_answer(precision, tol):
-    """The beam through the C ABI: its load is a force BC, shared by the left edge's particles
-    (Solver::updateForceBC, solver.h:167-188, the device's k_force_bc).  Solved tightly on both
-    sides, the device's displacements match the oracle's within 1e-8 (FP64) or 1e-6 (mixed);
-    at the example's own tolerances the device's L2 error is the known answer within 1e-6.
-    "Tightly" is Newton 1e-7: below about 1e-8 the beam's residual stops falling (rounding of the
-    force sums), Newton fails, and the halved retry keeps the failed attempt's external force (the
-    reference's resetStateVar leaves Pex alone), which doubles the load."""
-    from _util import gpu_problem
-    case = CFG.cantilever_beam()
-    m = case.meta
-    args = (m["length"], m["depth"], m["force"], case.material.E, case.material.mu)
-    tight = dict(cg_rtol=1e-24, cg_atol=0.0, tol_iter=1e-7)
-    o = oracle_problem(case, **tight)
-    o.update_geometry()
-    o.update_force_state()
-    ok, st = o.solve_load_step(*oracle_step_args(case, 0))
-    assert ok and st["cuts"] == 0
-    x_o = o.state()["xyz"]
-    g = gpu_problem(case, precision=precision, **tight)
-    ok, st = g.solve_load_step(case.load_step(0))
-    assert ok and st["cuts"] == 0
-    x_g = g.state()["xyz"]
-    g.close()
-    assert rel(x_g - case.xyz, x_o - case.xyz) <= tol
-    if precision == 0:
-        g = gpu_problem(case)
-        ok, st = g.solve_load_step(case.load_step(0))
-        assert ok and st["newton_solves"] == 2
-        e = beam_l2_error(case.xyz, g.state()["xyz"], *args)
-        g.close()
-        assert abs(e - BEAM_L2_REFERENCE) <= 1e-6 * BEAM_L2_REFERENCE
