@@ -23,8 +23,6 @@ def small_cases():
         "sc": CFG.sc_cube(size=2.4, radius=0.2, steps=3, total_disp=0.003),
         "sq": _square(),
         "fcc_j2": CFG.fcc_bar(size=(1.6, 1.6, 2.4), radius=0.2, steps=3, strain=0.02),
-        # cubic elastic constants (setParticleProperty's (C11, C12, C44) overload, as ex3)
-        "fcc_cubic": CFG.fcc_cubic_cube(steps=3, total_disp=0.003),
         "sc_j2": CFG.sc_cube(size=2.0, radius=0.25, steps=3, total_disp=0.06, ptype=LPM.ParticleType.J2Plasticity,
                              j2=(200.0, 0.0, 38714.0, 10.0)),
         # pre-cracked plate (explicit bond lists), loaded below the first bond break

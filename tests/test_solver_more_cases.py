@@ -1,9 +1,11 @@
 """Further device parity cases, through the C ABI against the CPU oracle: the known-answer beam
 of examples/ex7_convergence_beam.cpp, whose load is a force BC (Solver::updateForceBC,
-solver.h:167-188), and elastic-damage particles with undamaged grips (the undamaged type in
-SolverStatic::updateStaticDamage, solver_static.h:32-62).  Both oracles are pinned to the
-reference: the beam by its known answer (tests/test_beam_kat.py), the grips by the
-hex_edamage_grips golden fixture."""
+solver.h:167-188); elastic-damage particles with undamaged grips (the undamaged type in
+SolverStatic::updateStaticDamage, solver_static.h:32-62); and an FCC cube with cubic elastic
+constants (setParticleProperty's (C11, C12, C44) overload, particle_elastic.h:110-140, as
+examples/ex3_singlecrystal_3d_fcc.cpp sets them).  The oracles are pinned to the reference: the
+beam by its known answer (tests/test_beam_kat.py), the others by the hex_edamage_grips and
+fcc_cubic golden fixtures."""
 import numpy as np
 import pytest
 
@@ -69,4 +71,32 @@ def test_elastic_damage_with_undamaged_grips_matches_oracle():
         assert rel(sg["xyz"] - case.xyz, so["xyz"] - case.xyz) <= 1e-8, f"step {s}"
         assert np.abs(sg["damage"] - so["damage"]).max() <= 1e-9, f"step {s}"
         assert (sg["damage"][grips] == 0).all()
+    g.close()
+
+
+
+def test_cubic_constants_fcc_matches_oracle():
+    """Topology and the reference CSR pattern bit-exact, the stiffness before the BC elimination
+    bit-exact, and the load steps' Newton counts equal with displacements within 1e-8."""
+    case = CFG.fcc_cubic_cube(steps=3, total_disp=0.003)
+    tight = dict(cg_rtol=1e-24, cg_atol=0.0)
+    g = gpu_problem(case, **tight)
+    o = oracle_problem(case, **tight)
+    t = g.topology()
+    nb0, nb1, p2 = o.bonds()
+    nconn, nlq, conns = o.conns()
+    for k, v in (("nb0", nb0), ("nb1", nb1), ("bond_p2", p2), ("nconn", nconn), ("nlq", nlq), ("conns", conns)):
+        assert np.array_equal(t[k], v), k
+    o.update_geometry()
+    o.update_force_state()
+    g.assemble(False)
+    o.assemble(False)
+    for a, b in zip(g.export_csr(), o.export_csr()):
+        assert np.array_equal(a, b)
+    for s in range(len(case.steps)):
+        okg, stg = g.solve_load_step(case.load_step(s))
+        oko, sto = o.solve_load_step(*oracle_step_args(case, s))
+        assert okg and oko
+        assert stg["newton_solves"] == sto["newton_solves"], s
+        assert rel(g.state(("xyz",))["xyz"] - case.xyz, o.state()["xyz"] - case.xyz) <= 1e-8, s
     g.close()
