@@ -54,7 +54,6 @@ def args_():
     ap.add_argument("--size", type=float, default=20.0, help="specimen edge in mm (20 = the headline workload)")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-cg-cap", type=int, default=400, help="CG iterations per solve in the CPU sample")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched 64-plate damage workload")
     ap.add_argument("--plates", type=int, default=64, help="plates in the batched damage workload")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
@@ -64,23 +63,75 @@ def args_():
     ap.add_argument("--no-direct", action="store_true", help="skip the direct-solver (SolverMode::PARDISO) leg")
     ap.add_argument("--autotune", action="store_true",
                     help="tune the CG grid of the headline problem after the first warm-up step (lpmgpu_autotune)")
-    ap.add_argument("--tangent-steps", type=int, default=4, help="load steps of the FCC bar's 50-step path timed")
-    ap.add_argument("--serve-requests", type=int, default=12, help="requests in the serving-stream sample")
-    ap.add_argument("--serve-max-particles", type=float, default=1e5,
-                    help="upper end of the log-uniform particle count (the stream's full range is 5e3-5e5)")
+    ap.add_argument("--tangent-steps", type=int, default=50, help="load steps of the FCC bar's 50-step path timed")
+    ap.add_argument("--serve-requests", type=int, default=24, help="requests in the serving-stream sample")
+    ap.add_argument("--serve-max-particles", type=float, default=5e5,
+                    help="upper end of the log-uniform particle count (the stream's range is 5e3-5e5)")
     return ap.parse_args()
+
+
+def workload_desc(name, size=20.0):
+    """The workload's description and load increment, without building it (both arms use it)."""
+    if name == "hex2d":
+        return (f"hex2d {size:g}x{size:g} mm r=0.1 plane stress, E=69 GPa, 10 x 0.001 mm top-edge tension",
+                10, 0.001)
+    dstep = 0.001 * size / 20.0
+    return (f"sc3d {size:g}x{size:g}x{size:g} mm r=0.2 elastic, E=200 GPa nu=0.25, 20 x {dstep:g} mm top-face tension",
+            20, dstep)
+
+
+def workload_config(name, size, particles, dim):
+    """The `config` object of the JSON line: the same keys and values in both arms."""
+    return {"workload": workload_desc(name, size)[0], "particles": int(particles), "dof": int(particles * dim),
+            "newton_tol": NEWTON_TOL, "cg_test": "||r||^2 <= 1e-12 ||r0||^2 + 1e-12 (reference)",
+            "l2": "stiffness larger than L2 (126 MB); no flush" if name == "sc3d" and size >= 16
+            else "stiffness may fit in L2 (126 MB); no flush"}
 
 
 def workload(name, size=20.0):
     cfg = importlib.import_module("lpm-cpp_b200.configs")
+    desc, nsteps, dstep = workload_desc(name, size)
     if name == "hex2d":
-        c = cfg.hex_plate(size=size, radius=0.1, steps=10, total_disp=0.01, tol_iter=NEWTON_TOL)
-        desc = f"hex2d {size:g}x{size:g} mm r=0.1 plane stress, E=69 GPa, 10 x 0.001 mm top-edge tension"
+        c = cfg.hex_plate(size=size, radius=0.1, steps=nsteps, total_disp=dstep * nsteps, tol_iter=NEWTON_TOL)
     else:
-        c = cfg.sc_cube(size=size, radius=0.2, steps=20, total_disp=0.001 * 20 * size / 20.0, tol_iter=NEWTON_TOL)
-        desc = (f"sc3d {size:g}x{size:g}x{size:g} mm r=0.2 elastic, E=200 GPa nu=0.25, "
-                f"20 x {0.001 * size / 20.0:g} mm top-face tension")
+        c = cfg.sc_cube(size=size, radius=0.2, steps=nsteps, total_disp=dstep * nsteps, tol_iter=NEWTON_TOL)
     return c, desc
+
+
+def reference_spec(name, size, nsteps, tol_iter=NEWTON_TOL, loop="step", solve_threads=0, dump_k=()):
+    """Spec of the workload for oracle/_ref/lpm_ref written from the workload's definition alone:
+    the reference's own generator builds the lattice, and the boundary groups are coordinate
+    conditions evaluated by the driver on the reference's particles (those of
+    configs.hex_plate / configs.sc_cube: top and bottom rows within 2r of the box faces; in 3D
+    the two bottom corners at minimum y and minimum / maximum x).  Nothing of the product is
+    loaded to write it."""
+    desc, steps_path, dstep = workload_desc(name, size)
+    if name == "hex2d":
+        r = 0.1
+        lines = ["lattice hex2d", f"radius {r!r}", f"box 0.0 {size!r} 0.0 {size!r} 0.0 1.0", "euler 0 0.0 0.0 0.0",
+                 "ptype elastic", "plane_stress 1", "E 69000.0", "mu 0.3", "critical_bstrain 1.0",
+                 f"group top 1 > {size - 2 * r!r}", f"group bottom 1 < {2 * r!r}",
+                 "settype top 1", "settype bottom 2"]
+        bcs = [("bottom", "x", 0.0), ("bottom", "y", 0.0), ("top", "y", dstep)]
+    else:
+        r = 0.2
+        lines = ["lattice sc3d", f"radius {r!r}", f"box 0.0 {size!r} 0.0 {size!r} 0.0 {size!r}", "euler 0 0.0 0.0 0.0",
+                 "ptype elastic", "plane_stress 0", "E 200000.0", "mu 0.25", "critical_bstrain 1.0",
+                 f"group top 2 > {size - 2 * r!r}", f"group bottom 2 < {2 * r!r}",
+                 # the generator's first row in y lies in [0, 2r) and its x rows run from 0 to size
+                 f"group corner0 2 < {2 * r!r} 0 < {r!r} 1 < {2 * r!r}",
+                 f"group corner1 2 < {2 * r!r} 0 > {size - r!r} 1 < {2 * r!r}",
+                 "settype top 1", "settype bottom 2"]
+        bcs = [("bottom", "z", 0.0), ("corner0", "x", 0.0), ("corner0", "y", 0.0), ("corner1", "y", 0.0),
+               ("top", "z", dstep)]
+    lines += ["max_iter 30", f"tol_iter {tol_iter!r}", f"loop {loop}", f"steps {nsteps}"]
+    if solve_threads:
+        lines.append(f"solve_threads {int(solve_threads)}")
+    for g, flag, v in bcs:
+        lines.append(f"dispbc {g} {flag} {float(v)!r} 0 {nsteps}")
+    for k in dump_k:
+        lines.append(f"dumpK {int(k)}")
+    return "\n".join(lines) + "\n"
 
 
 def step_of(case, s):
@@ -344,9 +395,12 @@ def run_ours(a):
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cpu = cpu_baseline(case, a.cpu_cg_cap)
-        if cpu is not None and cpu.get("kind") == "reference":
-            cpu["parity"] = reference_parity(lpm, local)
+        try:
+            cpu = cpu_baseline(a.config, a.size)
+            if cpu.get("kind") == "reference":
+                cpu["parity"] = reference_parity(lpm, local)
+        except Exception as ex:  # the baseline must not cost the bench line
+            cpu = {"error": f"{type(ex).__name__}: {ex}"}
     # last, after every other measurement: the newest device path
     fatigue = None
     if single and not a.no_fatigue:
@@ -356,15 +410,18 @@ def run_ours(a):
         direct = direct_leg(lpm, local)
 
     if rank == 0:
+        # every leg in full on its own line first; the last line is the compact record
+        for name, leg in (("mixed", mixed), ("batched", batched), ("tangent", tangent), ("dump", dump),
+                          ("serving", serving), ("cpu_baseline", cpu), ("fatigue", fatigue), ("direct", direct)):
+            if leg is not None:
+                print(json.dumps({"leg": name, **leg}), flush=True)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (reference lattice generator)",
-            "config": {"workload": desc, "particles": n, "dof": ndof, "block_nnz": nnzb,
-                       "nnz_upper_ref_csr": sizes["nnz_upper"], "newton_tol": NEWTON_TOL,
-                       "cg_test": "||r||^2 <= 1e-12 ||r0||^2 + 1e-12 (reference)",
-                       "l2": "stiffness larger than L2 (126 MB); no flush", "parallelism": f"replicas x{world}",
-                       "cg_grid": tune if tune is not None else "default (one block per SM)"},
+            "config": workload_config(a.config, a.size, n, dim),
+            "roofline": roof, "e2e": e2e, "gpu_launches": counters_total, "clocks": clocks,
+            "cpu_baseline": _r({k: v for k, v in (cpu or {}).items() if k != "parity"}) if cpu else None,
             "solves_per_s": world * K / (ms_max * 1e-3),
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
             "newton_per_step": sum(st["newton_solves"] for st in stats) / K,
@@ -372,15 +429,75 @@ def run_ours(a):
             "phases_ms_per_step": {"assembly": (c1["assembly_seconds"] - c0["assembly_seconds"]) * 1e3 / K,
                                    "force": (c1["force_seconds"] - c0["force_seconds"]) * 1e3 / K,
                                    "cg_kernel": cg_s * 1e3 / K},
-            "roofline": roof, "e2e": e2e, "gpu_launches": counters_total, "clocks": clocks,
-            "mixed": mixed, "batched": batched, "serving": serving, "tangent": tangent, "dump": dump,
-            "fatigue": fatigue, "direct": direct,
-            "cpu_baseline": cpu,
+            "parallelism": f"replicas x{world}", "cg_grid": tune if tune is not None else "default",
+            "sizes": {"block_nnz": nnzb, "nnz_upper_ref_csr": sizes["nnz_upper"]},
+            "legs": compact_legs(mixed, batched, serving, tangent, dump, cpu, fatigue, direct),
         }
-        print(json.dumps(line), flush=True)
+        print(json.dumps(_r(line), separators=(",", ":")), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _r(o, sig=4):
+    """Floats rounded to `sig` significant digits, recursively (keeps the record short)."""
+    if isinstance(o, float):
+        return float(f"{o:.{sig}g}") if o == o and abs(o) != float("inf") else o
+    if isinstance(o, dict):
+        return {k: _r(v, sig) for k, v in o.items()}
+    if isinstance(o, (list, tuple)):
+        return [_r(v, sig) for v in o]
+    return o
+
+
+def compact_legs(mixed, batched, serving, tangent, dump, cpu, fatigue, direct):
+    """The other measurements in a few keys each (the full objects are printed above the line)."""
+    out = {}
+
+    def err(leg):
+        return {"error": leg["error"][:160]} if isinstance(leg, dict) and "error" in leg else None
+
+    if mixed:
+        out["mixed"] = {"speedup_vs_fp64": mixed["speedup_vs_fp64"], "rel_disp_err_vs_fp64": mixed["rel_disp_err_vs_fp64"],
+                        "dof_iter_per_s": mixed["dof_iter_per_s"], "ms_per_step": mixed["ms_per_step"]}
+    if batched:
+        out["batched"] = err(batched) or {
+            "specimens": batched.get("specimens"),
+            "plain_fp64_solves_per_s": batched["plain_fp64_one_at_a_time"]["solves_per_s"],
+            "batched_mixed_solves_per_s": batched["batched_mixed"]["solves_per_s"],
+            "speedup_batched_mixed_vs_plain_fp64": batched["speedup_batched_mixed_vs_plain_fp64"],
+            "speedup_batched_fp64_vs_plain_fp64": batched["speedup_batched_fp64_vs_plain_fp64"],
+            "max_rel_disp_err_mixed_vs_plain_fp64": batched["batched_mixed"]["max_rel_disp_err_vs_plain_fp64"]}
+    if serving:
+        out["serving"] = err(serving) or {
+            "requests": serving.get("requests"), "particles_range": serving.get("particles_range"),
+            "plain_fp64_solves_per_s": serving["plain_fp64_one_at_a_time"]["solves_per_s"],
+            "served_mixed_solves_per_s": serving["served_mixed"]["solves_per_s"],
+            "served_mixed_latency_s": serving["served_mixed"]["latency_s"],
+            "plain_fp64_latency_s": serving["plain_fp64_one_at_a_time"]["latency_s"],
+            "speedup_served_mixed_vs_plain_fp64": serving["speedup_served_mixed_vs_plain_fp64"],
+            "max_rel_disp_err_mixed_vs_plain_fp64": serving["served_mixed"]["max_rel_disp_err_vs_plain_fp64"]}
+    if tangent:
+        out["tangent"] = err(tangent) or {
+            "steps_timed": tangent.get("steps_timed"), "fp64_ms_per_step": tangent["fp64"]["ms_per_step"],
+            "mixed_ms_per_step": tangent["mixed"]["ms_per_step"], "speedup_mixed_vs_fp64": tangent["speedup_mixed_vs_fp64"],
+            "rel_disp_err_mixed_vs_fp64": tangent["mixed"]["rel_disp_err_vs_fp64"],
+            "assembly_share_fp64": tangent["fp64"]["assembly_share"]}
+    if cpu and isinstance(cpu.get("parity"), dict):
+        p = cpu["parity"]
+        out["parity_vs_reference"] = err(p) or {"workload": p.get("workload_short"),
+                                                "fp64_rel_disp": p["fp64"]["rel_disp_err_vs_reference"],
+                                                "mixed_rel_disp": p["mixed"]["rel_disp_err_vs_reference"]}
+    if dump:
+        out["dump"] = err(dump) or {"ms_exposed_async": dump.get("dump_ms_exposed_async"),
+                                    "ms_sync": dump.get("dump_ms_sync")}
+    if fatigue:
+        out["fatigue"] = err(fatigue) or {"speedup_vs_reference": fatigue.get("speedup_vs_reference"),
+                                          "max_abs_damage_diff": fatigue.get("max_abs_damage_diff_vs_reference")}
+    if direct:
+        out["direct"] = err(direct) or {k: {"cg_ms": v["cg"]["ms_per_step"], "direct_ms": v["direct"]["ms_per_step"]}
+                                        for k, v in direct.items() if isinstance(v, dict) and "cg" in v}
+    return out
 
 
 def dump_leg(lpm, case, first_step, device, steps=3):
@@ -708,7 +825,9 @@ def tangent_leg(lpm, steps, device, world, allreduce):
     out["mixed"]["rel_disp_err_vs_fp64"] = float(np.linalg.norm(um - u64) / np.linalg.norm(u64))
     out["speedup_mixed_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
     out["workload"] = (f"FCC J2 bar 16x16x32 mm, r=0.18 ({c.n} particles), tangent re-assembled every Newton "
-                       f"iteration, first {steps} of 50 steps to 1% strain, Newton tol {NEWTON_TOL}")
+                       f"iteration, {'all 50' if steps >= 50 else f'first {steps} of 50'} steps to 1% strain, "
+                       f"Newton tol {NEWTON_TOL}")
+    out["steps_timed"] = f"{steps}/50"
     return out
 
 
@@ -788,31 +907,16 @@ def serving_leg(lpm, count, nmax, device, world, allreduce):
              "latency_s": {"p50": float(np.percentile(lat_plain, 50)), "p99": float(np.percentile(lat_plain, 99))},
              "dof_iter_per_s": dof_iters / span_plain}
     return {"workload": f"{len(reqs)} requests, Poisson arrivals 200/s (seed {reqs[0][1].meta['seed']}); hex-2D / "
-                        f"SC-3D / BCC-3D, N log-uniform 5e3-{nmax:.0e} (the stream's range is 5e3-5e5; this sample "
-                        f"is bounded so the leg ends in about a minute), E 50-250 GPa, nu 0.2-0.35, 5-50 steps to "
+                        f"SC-3D / BCC-3D, N log-uniform 5e3-{nmax:.0e} (the stream's range is 5e3-5e5), "
+                        f"E 50-250 GPa, nu 0.2-0.35, 5-50 steps to "
                         f"0.1% strain, elastic or J2; {sum(c.n for _, c in reqs)} particles in total",
+            "requests": len(reqs), "particles_range": [int(min(c.n for _, c in reqs)), int(max(c.n for _, c in reqs))],
             "plain_fp64_one_at_a_time": plain, "served_mixed": mixed, "served_fp64": fp64,
             "speedup_served_mixed_vs_plain_fp64": mixed["solves_per_s"] / plain["solves_per_s"],
             "hbm_budget_bytes": 150 * 10**9}
 
 
 # ------------------------------------------------------------------------------------ CPU legs
-def _ref_sample(case, steps, cg_cap, threads, timeout=1800):
-    from oracle import oracle as O
-    d = tempfile.mkdtemp(prefix="lpmref_")
-    try:
-        spec = O.write_ref_spec(case, d, steps=steps, max_iter=1, cg_maxit_cap=cg_cap, loop="once",
-                                tol_iter=case.tol_iter)
-        O.run_ref(spec, d, threads=threads, timeout=timeout)
-        rows = O.read_ref_steps(d)
-        with open(os.path.join(d, "steps.txt")) as f:
-            head = f.readline()
-        setup = float(re.search(r"setup_s ([0-9.]+)", head).group(1))
-        return rows, setup
-    finally:
-        shutil.rmtree(d, ignore_errors=True)
-
-
 def reference_parity(lpm, device, size=6.0, steps=3):
     """The errors of the device solutions against the reference's own FP64 solution: the SC cube of
     the headline workload at `size` mm (r = 0.2), `steps` load steps, the bench's Newton tolerance
@@ -832,7 +936,8 @@ def reference_parity(lpm, device, size=6.0, steps=3):
             ref = [O.read_bin(d, f"xyz_{s:03d}.f64", np.float64).reshape(-1, 3) - x0 for s in range(steps)]
         finally:
             shutil.rmtree(d, ignore_errors=True)
-        out = {"workload": f"{desc}, first {steps} steps", "reference": "oracle/_ref/lpm_ref, 1 thread"}
+        out = {"workload": f"{desc}, first {steps} steps", "workload_short": f"sc3d {size:g} mm, {steps} steps",
+               "reference": "oracle/_ref/lpm_ref, 1 thread"}
         for key, prec in (("fp64", lpm.Precision.FP64), ("mixed", lpm.Precision.MIXED)):
             g = lpm.GpuProblem(case.assembly(), undamaged_pt_type=case.undamaged_type, max_iter=case.max_iter,
                                tol_iter=NEWTON_TOL, precision=prec, device=device)
@@ -850,26 +955,40 @@ def reference_parity(lpm, device, size=6.0, steps=3):
         return {"error": f"{type(ex).__name__}: {ex}"}
 
 
-def cpu_baseline(case, cg_cap):
-    """The reference's CPU path on this host: one SolverStatic::solveProblemStep call on the
-    same problem, one Newton solve with CG capped at cg_cap iterations (bounded sample).  Falls
-    back to the single-threaded C restatement when the reference build is absent."""
+def _steps_header(d):
+    with open(os.path.join(d, "steps.txt")) as f:
+        head = f.readline()
+    m = re.search(r"N (\d+) dim (\d+) setup_s ([0-9.]+)", head)
+    return int(m.group(1)), int(m.group(2)), float(m.group(3))
+
+
+def cpu_baseline(name, size):
+    """The reference's CPU path on this host, a bounded sample: the workload's first load step,
+    one converged SolverStatic::solveProblemStep call (Newton to the workload's tolerance, the
+    reference's CG test) on all host cores, from oracle/_ref/lpm_ref.  Falls back to the
+    single-threaded C restatement (assembly + one CG solve) when the reference build is absent."""
     from oracle import oracle as O
-    ndof = case.n * case.dim
     threads = os.cpu_count() or 1
     if O.ref_available():
-        rows, setup = _ref_sample(case, 1, cg_cap, threads)
+        d = tempfile.mkdtemp(prefix="lpmref_")
+        try:
+            O.run_ref(reference_spec(name, size, 1), d, threads=threads, timeout=1800)
+            rows = O.read_ref_steps(d)
+            n, dim, setup = _steps_header(d)
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
         it = sum(r["cg_iters"] for r in rows)
         wall = sum(r["wall_s"] for r in rows)
-        return {"value": ndof * it / wall, "unit": UNIT, "cores": threads, "kind": "reference",
-                "sample": f"1 solveProblemStep call of the same workload, 1 Newton solve, CG capped at {cg_cap} "
-                          f"iterations ({it} iterations, {wall:.1f} s; setup {setup:.1f} s untimed); "
-                          "LPM-CPP headers compiled unmodified, MKL replaced by the oracle/shim stand-in",
-                "cg_spmv_s_per_iter": sum(r["spmv_s"] for r in rows) / max(it, 1)}
-    mat = O.Material(ptype="j2" if int(case.ptype) == 2 else "elastic", plane_stress=case.material.plane_stress,
-                     E=case.material.E, mu=case.material.mu, critical_bstrain=case.material.critical_bstrain)
+        return {"value": n * dim * it / wall, "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": f"load step 1 of the same workload, one converged solveProblemStep ({rows[0]['newton_solves']} "
+                          f"Newton solves, {it} CG iterations, {wall:.1f} s; setup {setup:.1f} s untimed); LPM-CPP "
+                          "headers compiled unmodified, MKL replaced by the oracle/shim stand-in",
+                "s_per_step": wall, "cg_spmv_s_per_iter": sum(r["spmv_s"] for r in rows) / max(it, 1)}
+    case, _ = workload(name, size)
+    mat = O.Material(ptype="elastic", plane_stress=case.material.plane_stress, E=case.material.E, mu=case.material.mu,
+                     critical_bstrain=case.material.critical_bstrain)
     lat = {0: "sq2d", 1: "hex2d", 2: "sc3d", 3: "fcc3d", 4: "bcc3d"}[int(case.lattice)]
-    o = O.OracleProblem(lat, case.radius, case.xyz, mat, types=case.types, cg_maxit=cg_cap)
+    o = O.OracleProblem(lat, case.radius, case.xyz, mat, types=case.types, cg_maxit=400)
     o.update_geometry()
     o.update_force_state()
     flag = {"x": 0, "y": 1, "z": 2}
@@ -882,38 +1001,51 @@ def cpu_baseline(case, cg_cap):
     o.update_rr()
     _, it = o.cg()
     wall = time.perf_counter() - t0
-    return {"value": ndof * it / wall, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"C restatement: assembly + 1 CG solve capped at {cg_cap} iterations"}
+    return {"value": case.n * case.dim * it / wall, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "C restatement: assembly + 1 CG solve capped at 400 iterations"}
 
 
 def run_reference(a):
+    """The reference arm: oracle/_ref/lpm_ref (LPM-CPP's headers compiled unmodified, MKL replaced
+    by the oracle/shim stand-in) runs the same workload on all host cores, W + K converged load
+    steps of SolverStatic::solveProblemStep (the loop of solveProblem without the per-step dump),
+    the last K timed by the driver's own clock around each call.  The spec is written from the
+    workload's definition (reference_spec); nothing of the product is imported or loaded."""
     world, rank, local = dist_setup()
     if rank != 0:
         return
     from oracle import oracle as O
-    case, desc = workload(a.config, a.size)
-    ndof = case.n * case.dim
-    threads = os.cpu_count() or 1
     if not O.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/lpm_ref was not built on this machine"}))
         return
     W, K = a.warmup, a.steps
-    cap = max(50, a.cpu_cg_cap // 2)
-    rows, setup = _ref_sample(case, W + K, cap, threads, timeout=3600)
+    threads = os.cpu_count() or 1
+    d = tempfile.mkdtemp(prefix="lpmref_arm_")
+    try:
+        O.run_ref(reference_spec(a.config, a.size, W + K), d, threads=threads, timeout=3600)
+        rows = O.read_ref_steps(d)
+        n, dim, setup = _steps_header(d)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
     timed = rows[W:W + K]
     it = sum(r["cg_iters"] for r in timed)
     wall = sum(r["wall_s"] for r in timed)
+    ndof = n * dim
     value = ndof * it / wall
-    sample = (f"{K} timed of {W + K} solveProblemStep calls (1 Newton solve each, CG capped at {cap} iterations) "
-              f"of the same workload; setup {setup:.1f} s untimed; LPM-CPP headers compiled unmodified, MKL "
-              "replaced by the oracle/shim stand-in")
+    lat = sorted(r["wall_s"] * 1e3 for r in timed)
+    sample = (f"{K} timed of {W + K} converged solveProblemStep calls of the same workload "
+              f"({sum(r['newton_solves'] for r in timed) / K:.1f} Newton solves, {it / K:.0f} CG iterations per step); "
+              f"setup {setup:.1f} s untimed; LPM-CPP headers compiled unmodified, MKL replaced by the oracle/shim stand-in")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
         "warmup": W, "ms_per_step": wall / K * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference lattice generator)",
-        "config": {"workload": desc, "particles": case.n, "dof": ndof, "parallelism": "host OpenMP"},
+        "config": workload_config(a.config, a.size, n, dim),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "solves_per_s": K / wall, "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "newton_per_step": sum(r["newton_solves"] for r in timed) / K, "cg_iters_per_step": it / K,
+        "parallelism": f"host OpenMP, {threads} threads",
     }), flush=True)
 
 

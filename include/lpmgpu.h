@@ -30,14 +30,16 @@ typedef enum
     LPMGPU_ERR_OUT_OF_MEMORY = 3, /* device allocation failed */
     LPMGPU_ERR_NEWTON = 4,        /* Newton hit max_iter (solver_static.h:122, the load-cut trigger) */
     LPMGPU_ERR_CG_MAXIT = 5,      /* a CG solve reached its cap; printed and ignored by the reference
-                                     (solver.h:338-349); reported through stats, never returned */
+                                     (solver.h:338-349); the handle entry points report it through
+                                     stats, only lpmgpu_cg_bsr_noalloc returns it */
     LPMGPU_ERR_TIMEOUT = 6,       /* a bounded device-side wait gave up; the context stays usable */
     LPMGPU_ERR_TOPOLOGY = 7,      /* a particle without bonds, or more bonds/connections than supported */
     LPMGPU_ERR_BUDGET = 8,        /* request larger than the server's HBM budget */
     LPMGPU_ERR_CUTS = 9,          /* a load step was halved more than 30 times */
     LPMGPU_ERR_NOT_READY = 10,    /* server: result not available yet */
     LPMGPU_ERR_NO_DEVICE = 11,    /* no CUDA device; the library has no CPU fallback */
-    LPMGPU_ERR_NOT_SPD = 12       /* direct solve: the stiffness is not positive definite */
+    LPMGPU_ERR_NOT_SPD = 12,      /* direct solve: the stiffness is not positive definite */
+    LPMGPU_ERR_CG_BREAKDOWN = 13  /* lpmgpu_cg_bsr_noalloc: p.Ap == 0 (singular or indefinite matrix) */
 } lpmgpu_status;
 
 /* LatticeType (include/lpm.h:97-106); BCC3D covers the three BCC enum values */
@@ -270,6 +272,12 @@ typedef struct
 } lpmgpu_tune_result;
 int32_t lpmgpu_autotune(lpmgpu_solver *h, int32_t iterations, lpmgpu_tune_result *out);
 int32_t lpmgpu_set_cg_grid(lpmgpu_solver *h, int32_t grid);
+/* Time limit of each grid-barrier wait inside this handle's CG kernel (default 4 s; ns <= 0
+ * restores it).  A wait that exceeds it makes every block of the launch return and the solve
+ * report LPMGPU_ERR_TIMEOUT; the handle stays usable.  Its use is testing that path: a limit
+ * below the natural barrier wait makes the next solve time out.  No counterpart in the reference,
+ * whose CG (MKL dcg, solver.h:303-344) has no device waits. */
+int32_t lpmgpu_set_wait_limit_ns(lpmgpu_solver *h, int64_t ns);
 
 /* Device state back to host (any pointer may be NULL): xyz n*3, Pin n*3, stress n*6 (s11 s22
  * s33 s23 s13 s12), damage n, damage_visual n, state_var n*nsv (nsv = 7 for J2, 3 for fatigue
@@ -319,10 +327,10 @@ int32_t lpmgpu_get_counters(const lpmgpu_solver *h, lpmgpu_counters *out);
 /* The CUDA stream (cudaStream_t) the handle launches on, for callers that time with events. */
 int32_t lpmgpu_get_stream(const lpmgpu_solver *h, void **stream);
 
-/* Allocation-free CG, for callers that cannot allocate device memory: code running under CUDA
- * graph capture, where cudaMalloc is not allowed, and hosts whose device memory belongs to an
- * external pool or arena.  No counterpart in the reference (LPM-CPP solves inside
- * Solver::LPM_CG with MKL and allocates per call).
+/* Allocation-free CG, for callers that cannot allocate device memory: a plugin inside a host
+ * program that owns all device memory through its own pool or arena, and latency-bound loops
+ * that cannot afford cudaMalloc/cudaFree (which may synchronise the device).  No counterpart in
+ * the reference (LPM-CPP solves inside Solver::LPM_CG with MKL and allocates per call).
  * Solves A x = b by the same unpreconditioned CG and stopping rule as lpmgpu_solve_linear
  * (||r||^2 <= rtol*||r0||^2 + atol, x0 = 0, maxit <= 0 means rows*dim).  A is block-CSR on the
  * device: rowptr[nrows+1] and colidx[nnzb] (int32), values[nnzb*dim*dim] row-major blocks; b and
@@ -330,9 +338,13 @@ int32_t lpmgpu_get_stream(const lpmgpu_solver *h, void **stream);
  * *iterations (host, may be NULL) gets the iteration count.  The call allocates nothing: its
  * work vectors and reduction words live in a static device array that every GPU loading the
  * library holds (about 8 MiB), so at most 262144 unknowns are accepted (larger sizes return
- * LPMGPU_ERR_INVALID_ARG).  All calls on a device share that array, so calls that overlap on
- * the GPU race.  The first call on a device looks the array up and should come before any
- * stream capture.  Synchronises the stream before returning. */
+ * LPMGPU_ERR_INVALID_ARG).  All calls on a device share that array and it keeps the last call's
+ * contents, so calls that overlap on the GPU race.  The first call on a device looks the array
+ * up (set-up) and should come before any stream capture begins; a cudaDeviceReset invalidates
+ * that look-up.  The call waits for its stream before returning.  Returns LPMGPU_ERR_CG_MAXIT
+ * when the cap was reached without meeting the tolerance (NaN input included),
+ * LPMGPU_ERR_CG_BREAKDOWN when p.Ap == 0, LPMGPU_ERR_TIMEOUT when a device wait gave up; x then
+ * holds the last iterate. */
 int32_t lpmgpu_cg_bsr_noalloc(int32_t dim, int32_t nrows, const int32_t *rowptr, const int32_t *colidx,
                               const double *values, const double *b, double *x, double rtol, double atol,
                               int64_t maxit, void *stream, int64_t *iterations);

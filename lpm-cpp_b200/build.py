@@ -38,21 +38,42 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(d) <= t for d in deps)
 
 
+def _compile(args):
+    cmd, src = args
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    return src, r.returncode, r.stderr
+
+
 def build(debug: bool = False, force: bool = False, verbose: bool = False) -> str:
+    """Compiles every csrc/*.cu to an object in parallel (one nvcc per source, each its own
+    translation unit as before) and links them into liblpmgpu.so."""
     if not force and not debug and up_to_date():
         return OUT
-    cmd = [nvcc(), *ARCH, "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC", "-shared",
-           "-O0" if debug else "-O3", "-o", OUT + ".tmp", *sources()]
+    from concurrent.futures import ThreadPoolExecutor
+    objdir = os.path.join(HERE, "_build", "debug" if debug else "release")
+    os.makedirs(objdir, exist_ok=True)
+    flags = [*ARCH, "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC", "-O0" if debug else "-O3"]
     if debug:
-        cmd.insert(1, "-DLPM_CHECK")
+        flags.insert(0, "-DLPM_CHECK")
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    r = subprocess.run(cmd, capture_output=True, text=True)
+        flags.insert(0, "-Xptxas=-v")
+    jobs, objs = [], []
+    for src in sources():
+        obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
+        objs.append(obj)
+        jobs.append(([nvcc(), *flags, "-c", "-o", obj, src], src))
+    with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as ex:
+        results = list(ex.map(_compile, jobs))
+    errs = [f"{os.path.basename(src)}:\n{err[-4000:]}" for src, rc, err in results if rc != 0]
+    if errs:
+        raise RuntimeError("nvcc failed:\n" + "\n".join(errs))
+    if verbose:
+        for src, _, err in results:
+            sys.stderr.write(f"== {os.path.basename(src)}\n{err}")
+    r = subprocess.run([nvcc(), *ARCH, "-shared", "-o", OUT + ".tmp", *objs], capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stderr[-6000:])
+        raise RuntimeError("nvcc link failed:\n" + r.stderr[-6000:])
     os.replace(OUT + ".tmp", OUT)
-    if verbose:
-        sys.stderr.write(r.stderr)
     return OUT
 
 

@@ -52,6 +52,7 @@ struct CGState
     double *part;       // [grid][2]
     double *tot;        // [2] reduced totals published by the last block at each barrier
     int64_t *info;      // [0] iterations, [1] status bits (1 maxit, 2 timeout, 4 breakdown), [2..3] rr0/rr bits
+    unsigned long long wait_ns; // limit of each grid-barrier wait
 };
 
 
@@ -137,7 +138,8 @@ __device__ bool grid_reduce(unsigned *bar, int64_t *info, volatile int *s_fail, 
 // block that runs one phase ahead from overwriting partials another block is still reading.
 // Returns false when the wait timed out (the status word gets bit 2).
 __device__ bool grid_allreduce(unsigned *bar, unsigned &epoch, int64_t *info, volatile int *s_fail,
-                               const double *part, int slot, double *sh, double *out)
+                               const double *part, int slot, double *sh, double *out,
+                               unsigned long long wait_ns)
 {
     __shared__ double s_tot;
     __syncthreads();
@@ -149,7 +151,7 @@ __device__ bool grid_allreduce(unsigned *bar, unsigned &epoch, int64_t *info, vo
         const unsigned long long t0 = gtimer();
         while ((int)(ld_acquire(bar) - target) < 0)
         {
-            if (gtimer() - t0 > kBarrierTimeoutNs)
+            if (gtimer() - t0 > wait_ns)
             {
                 atomicOr(reinterpret_cast<unsigned long long *>(info + 1), 2ull);
                 *s_fail = 1;
@@ -212,7 +214,7 @@ __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg(CGState s, cons
     }
     block_partial(loc, s.part, 0, sh);
     double rr;
-    if (!grid_allreduce(s.bar, epoch, s.info, &s_fail, s.part, 0, sh, &rr))
+    if (!grid_allreduce(s.bar, epoch, s.info, &s_fail, s.part, 0, sh, &rr, s.wait_ns))
         return;
     const double stop = (s.abs_stop >= 0) ? s.abs_stop : s.rtol * rr + s.atol;
     if (blockIdx.x == 0 && threadIdx.x == 0)
@@ -231,7 +233,7 @@ __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg(CGState s, cons
                                                    pold, pnew, q, beta, pf, pl, red);
         block_partial(lpq, s.part, 1, sh);
         double pq;
-        if (!grid_allreduce(s.bar, epoch, s.info, &s_fail, s.part, 1, sh, &pq))
+        if (!grid_allreduce(s.bar, epoch, s.info, &s_fail, s.part, 1, sh, &pq, s.wait_ns))
             return;
         if (pq == 0.0)
         {
@@ -255,7 +257,7 @@ __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks) k_cg(CGState s, cons
         }
         block_partial(lrr, s.part, 0, sh);
         double rn;
-        if (!grid_allreduce(s.bar, epoch, s.info, &s_fail, s.part, 0, sh, &rn))
+        if (!grid_allreduce(s.bar, epoch, s.info, &s_fail, s.part, 0, sh, &rn, s.wait_ns))
             return;
         const bool done = rn <= stop;
         const bool capped = it >= s.maxit;
@@ -390,6 +392,7 @@ static cudaError_t run_cg(Problem &p, const TK *K, const TV *b, TV *x, TV *r, TV
     s.part = p.partials;
     s.tot = p.partials + 2 * kMaxGridBlocks;
     s.info = p.cg_info;
+    s.wait_ns = p.wait_ns;
     if ((e = cudaMemsetAsync(p.barrier, 0, 2 * sizeof(unsigned), p.stream)) != cudaSuccess)
         return e;
     if ((e = cudaMemsetAsync(p.cg_info, 0, 4 * sizeof(int64_t), p.stream)) != cudaSuccess)
@@ -623,6 +626,14 @@ int32_t lpmgpu_set_cg_grid(lpmgpu_solver *h, int32_t grid)
     return LPMGPU_OK;
 }
 
+int32_t lpmgpu_set_wait_limit_ns(lpmgpu_solver *h, int64_t ns)
+{
+    if (!h)
+        return LPMGPU_ERR_INVALID_ARG;
+    h->p.wait_ns = ns > 0 ? (unsigned long long)ns : lpm::kBarrierTimeoutNs;
+    return LPMGPU_OK;
+}
+
 int32_t lpmgpu_autotune(lpmgpu_solver *h, int32_t iterations, lpmgpu_tune_result *out)
 {
     using namespace lpm;
@@ -669,19 +680,23 @@ int32_t lpmgpu_autotune(lpmgpu_solver *h, int32_t iterations, lpmgpu_tune_result
 // ---------------------------------------------------------------------------------------
 // Allocation-free CG on a caller-supplied block-CSR matrix.
 //
-// Some callers cannot allocate device memory: code running while a CUDA graph is being
-// captured (cudaMalloc is not capturable), and hosts whose device memory is owned by an
-// external pool or arena that forbids driver allocations behind its back.  For them the
-// solve below takes every input and output from the caller and keeps its own work vectors,
-// reduction partials and barrier words in the file-scope array g_noalloc_scratch, which
-// every GPU that loads this library holds (about 8 MiB) until the process exits.
+// Some callers cannot allocate device memory.  A plugin that runs inside a host program which
+// owns all device memory through its own pool or arena may not call cudaMalloc behind that
+// allocator's back, and a latency-bound loop cannot afford cudaMalloc/cudaFree, which may
+// synchronise the whole device.  For them the solve below takes every input and output from
+// the caller and keeps its own work vectors, reduction partials and barrier words in the
+// file-scope array g_noalloc_scratch, which every GPU that loads this library holds (about
+// 8 MiB) until the process exits.
 //
 // Limits and caveats:
 //  * at most kNoAllocMaxDof unknowns (rows * dim); larger systems are rejected;
-//  * all calls on a device share the one array, so calls that overlap on the GPU (two
-//    streams, two host threads) race; serialise them;
+//  * all calls on a device share the one array and it keeps the last call's contents, so
+//    calls that overlap on the GPU (two streams, two host threads) race; serialise them;
 //  * the first call on a device looks up the array's device address (set-up) and should
-//    come before any stream capture.
+//    come before any stream capture begins; a cudaDeviceReset of that device invalidates the
+//    looked-up address, so the entry point must not be used after one;
+//  * the call waits for its stream before returning, and reports a solve that reached its
+//    iteration cap (LPMGPU_ERR_CG_MAXIT) or broke down with p.Ap == 0 (LPMGPU_ERR_CG_BREAKDOWN).
 namespace lpm
 {
 
@@ -913,7 +928,21 @@ extern "C" int32_t lpmgpu_cg_bsr_noalloc(int32_t dim, int32_t nrows, const int32
     }
     if (iterations)
         *iterations = status[0];
+    // status bits of k_cg_bsr_noalloc: 2 a barrier wait timed out, 4 p.Ap == 0, 1 cap reached
     if (status[1] & 2)
+    {
+        set_last_error("lpmgpu_cg_bsr_noalloc: a device-side barrier wait timed out");
         return LPMGPU_ERR_TIMEOUT;
+    }
+    if (status[1] & 4)
+    {
+        set_last_error("lpmgpu_cg_bsr_noalloc: CG broke down (p.Ap == 0: the matrix is singular or indefinite)");
+        return LPMGPU_ERR_CG_BREAKDOWN;
+    }
+    if (status[1] & 1)
+    {
+        set_last_error("lpmgpu_cg_bsr_noalloc: CG reached its iteration cap without meeting the tolerance");
+        return LPMGPU_ERR_CG_MAXIT;
+    }
     return LPMGPU_OK;
 }

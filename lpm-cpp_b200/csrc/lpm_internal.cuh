@@ -97,6 +97,7 @@ struct Problem
     int *col_sell = nullptr;          // nsb * kSlice particle columns
     int nslices = 0;
     int cg_grid = 0;                  // > 0: blocks per CG launch (lpmgpu_autotune / lpmgpu_set_cg_grid)
+    unsigned long long wait_ns = 4000000000ull; // limit of each grid-barrier wait in k_cg (lpmgpu_set_wait_limit_ns)
     int64_t nsb = 0;                  // block slots of the sliced-ELL layout (>= nnzb / kSlice)
     double *K = nullptr;              // nsb * d*d * kSlice
     float *K32 = nullptr;             // mixed precision copy

@@ -612,6 +612,7 @@ const char *lpmgpu_status_string(int32_t s)
     case LPMGPU_ERR_NOT_READY: return "result not ready";
     case LPMGPU_ERR_NO_DEVICE: return "no CUDA device";
     case LPMGPU_ERR_NOT_SPD: return "stiffness not positive definite";
+    case LPMGPU_ERR_CG_BREAKDOWN: return "CG broke down (p.Ap == 0)";
     default: return "unknown status";
     }
 }

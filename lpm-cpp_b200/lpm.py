@@ -63,8 +63,9 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device mem
           4: "Newton iteration did not converge", 5: "CG reached its iteration cap",
           6: "device wait timed out", 7: "unsupported particle topology", 8: "HBM budget exceeded",
           9: "load step halved too many times", 10: "result not ready", 11: "no CUDA device",
-          12: "stiffness not positive definite"}
+          12: "stiffness not positive definite", 13: "CG broke down (p.Ap == 0)"}
 OK, ERR_NEWTON, ERR_CUTS, ERR_NOT_READY = 0, 4, 9, 10
+ERR_CG_MAXIT, ERR_TIMEOUT, ERR_CG_BREAKDOWN = 5, 6, 13
 
 
 class LpmGpuError(RuntimeError):
@@ -197,6 +198,7 @@ EXPORTS = [
     "lpmgpu_fatigue_solve_step", "lpmgpu_fatigue_static_step", "lpmgpu_fatigue_update_damage", "lpmgpu_fatigue_cycle",
     "lpmgpu_read_state", "lpmgpu_read_residual", "lpmgpu_set_xyz", "lpmgpu_get_phase_times",
     "lpmgpu_get_counters", "lpmgpu_get_stream", "lpmgpu_cg_bsr_noalloc", "lpmgpu_autotune", "lpmgpu_set_cg_grid",
+    "lpmgpu_set_wait_limit_ns",
     "lpmgpu_solve_direct", "lpmgpu_band_order", "lpmgpu_get_nonlocal",
     "lpmgpu_format_dump", "lpmgpu_dump_write", "lpmgpu_dump_flush",
     "lpmgpu_batch_create", "lpmgpu_batch_destroy", "lpmgpu_batch_add", "lpmgpu_batch_add_fatigue",
@@ -257,6 +259,7 @@ def lib():
         "lpmgpu_band_order": (C.c_int32, [C.c_int32, ip, ip, ip, lp]),
         "lpmgpu_get_nonlocal": (C.c_int32, [vp, ip, ip, lp]),
         "lpmgpu_set_cg_grid": (C.c_int32, [vp, C.c_int32]),
+        "lpmgpu_set_wait_limit_ns": (C.c_int32, [vp, C.c_int64]),
         "lpmgpu_cg_bsr_noalloc": (C.c_int32, [C.c_int32, C.c_int32, vp, vp, vp, vp, vp, C.c_double, C.c_double,
                                               C.c_int64, vp, C.POINTER(C.c_int64)]),
         "lpmgpu_batch_create": (C.c_int32, [C.c_int32, C.POINTER(vp)]),
@@ -843,6 +846,12 @@ class GpuProblem:
     def set_cg_grid(self, grid: int):
         """Blocks per CG launch; 0 restores the default (one block per SM, at most one per slice)."""
         _check(lib().lpmgpu_set_cg_grid(self._h, int(grid)), "lpmgpu_set_cg_grid")
+
+    def set_wait_limit_ns(self, ns: int):
+        """Time limit of each grid-barrier wait in this problem's CG kernel; 0 restores the
+        default of 4 s (lpmgpu_set_wait_limit_ns).  A solve whose wait exceeds it raises
+        LpmGpuError with LPMGPU_ERR_TIMEOUT, and the problem stays usable."""
+        _check(lib().lpmgpu_set_wait_limit_ns(self._h, int(ns)), "lpmgpu_set_wait_limit_ns")
 
     def store_state(self):
         _check(lib().lpmgpu_store_state(self._h), "lpmgpu_store_state")

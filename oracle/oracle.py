@@ -355,13 +355,19 @@ def ref_available() -> bool:
     return os.path.exists(REF_BIN)
 
 
-def run_ref(spec_text: str, outdir: str, threads: int = 1, timeout: float = 600.0, binary: str = REF_BIN) -> str:
-    """Runs the reference's own build on a spec (see oracle/ref_driver.cpp); returns stdout."""
+def run_ref(spec_text: str, outdir: str, threads: int = 1, timeout: float = 600.0, binary: str = REF_BIN,
+            mkl_threads: int = 0) -> str:
+    """Runs the reference's own build on a spec (see oracle/ref_driver.cpp); returns stdout.
+    threads sets OMP_NUM_THREADS; mkl_threads > 0 sets MKL_NUM_THREADS, the team of the MKL
+    stand-in's sparse product and CG loops (otherwise it follows OMP_NUM_THREADS)."""
     os.makedirs(outdir, exist_ok=True)
     path = os.path.join(outdir, "spec.txt")
     with open(path, "w") as f:
         f.write(spec_text + f"\nout {outdir}\n")
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    env.pop("MKL_NUM_THREADS", None)
+    if mkl_threads > 0:
+        env["MKL_NUM_THREADS"] = str(int(mkl_threads))
     r = subprocess.run([binary, path], env=env, capture_output=True, text=True, timeout=timeout)
     if r.returncode != 0:
         raise RuntimeError(f"{os.path.basename(binary)} failed ({r.returncode}): {r.stderr[-2000:]}")
@@ -398,7 +404,7 @@ def write_bond_file(path: str, nb0, nb1, p2):
 
 
 def write_ref_spec(case, outdir: str, steps=None, max_iter=None, tol_iter=None, cg_tol=None, cg_maxit_cap=0,
-                   dump_k=(), loop="step", use_generator=True, tangent=False, solver="cg") -> str:
+                   dump_k=(), loop="step", use_generator=True, tangent=False, solver="cg", solve_threads=0) -> str:
     """Spec text for oracle/_ref/lpm_ref describing a product-side ``Case`` (duck-typed):
     groups and particle types are passed as raw int32 id files so both sides see the same sets.
     With use_generator the reference generates the lattice itself (its ids must then equal
@@ -423,6 +429,8 @@ def write_ref_spec(case, outdir: str, steps=None, max_iter=None, tol_iter=None, 
              f"tol_iter {(case.tol_iter if tol_iter is None else tol_iter)!r}", f"loop {loop}"]
     if cg_maxit_cap:
         lines.append(f"cg_maxit_cap {int(cg_maxit_cap)}")
+    if solve_threads:
+        lines.append(f"solve_threads {int(solve_threads)}")
     if tangent:
         lines.append("tangent 1")
     if solver != "cg":

@@ -59,6 +59,11 @@
  *   fatigue_load PATH     (the load spectrum, SolverFatigue::readLoad)
  *   solver cg|pardiso     (the SolverMode of the solver: Solver::LPM_CG or Solver::LPM_PARDISO,
  *                          include/solver.h:191-354; default cg)
+ *   solve_threads N       (N > 0: omp_set_num_threads(N) once the Assembly is built, so the
+ *                          bond and connection searches use every thread and the solve's own
+ *                          OpenMP loops use N; with N = 1 the stiffness scatter, which races
+ *                          under OpenMP (include/stiffness.h:261-276), is deterministic.  The
+ *                          MKL stand-in sizes its own loops by MKL_NUM_THREADS)
  *   cij C11 C12 C44       (C11 > 0: the (C11, C12, C44) overload of setParticleProperty for elastic
  *                          and elastic-damage particles, include/particle_elastic.h:110-140,
  *                          include/particle_elastic_damage.h:218-250)
@@ -148,6 +153,7 @@ struct Spec
     std::vector<DispSpec> disp;
     std::vector<ForceSpec> force;
     std::vector<int> dumpK;
+    int solve_threads = 0;
     std::string loop = "step";
     std::string out = ".";
     std::string xyz_file;
@@ -261,6 +267,8 @@ static Spec parse(const char *path)
             is >> d.from >> d.to;
             s.force.push_back(d);
         }
+        else if (k == "solve_threads")
+            is >> s.solve_threads;
         else if (k == "dumpK")
         {
             int st;
@@ -720,6 +728,8 @@ int main(int argc, char **argv)
     if (sp.cg_rtol >= 0 || sp.cg_atol >= 0)
         solv.setCGTolerance(sp.cg_rtol >= 0 ? sp.cg_rtol : 1e-12, sp.cg_atol >= 0 ? sp.cg_atol : 1e-12);
 #endif
+    if (sp.solve_threads > 0)
+        omp_set_num_threads(sp.solve_threads);
     const double t_setup1 = wall();
 
     /* setup outputs: coordinates, bonds (per particle: layer-0 list then layer-1 list), conns */

@@ -22,6 +22,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -119,6 +120,23 @@ sparse_status_t mkl_sparse_d_create_csr(sparse_matrix_t *A, const sparse_index_b
     return SPARSE_STATUS_SUCCESS;
 }
 
+/* Threads of the stand-in's own parallel loops.  MKL sizes its thread team by MKL_NUM_THREADS
+ * (falling back to the OpenMP setting), independently of the caller's OpenMP loops; the same
+ * rule here lets a checker run the reference's own loops on one thread (its assembly scatter
+ * races under OpenMP) while the sparse product and the CG vector updates use every core. */
+static int shim_threads()
+{
+    const char *e = std::getenv("MKL_NUM_THREADS");
+    const int v = e ? std::atoi(e) : 0;
+    if (v > 0)
+        return v;
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
 /* y = alpha*A*x + beta*y for A = U + U^T - diag(U) given the upper triangle U (the SYMMETRIC /
  * UPPER descriptor of solver.h:287-289).  Row-parallel gather for U x; the U^T x part is a
  * scatter, accumulated in per-thread buffers and summed afterwards. */
@@ -131,10 +149,7 @@ sparse_status_t mkl_sparse_d_mv(const sparse_operation_t operation, const double
     double t0 = now_s();
     const long long n = A->n, b = A->base;
     const bool sym = descr.type == SPARSE_MATRIX_TYPE_SYMMETRIC;
-    int nt = 1;
-#ifdef _OPENMP
-    nt = omp_get_max_threads();
-#endif
+    const int nt = shim_threads();
     if (sym)
         A->scratch.assign((size_t)nt * n, 0.0);
     double *scr = sym ? A->scratch.data() : nullptr;
@@ -242,7 +257,7 @@ void dcg_check(const MKL_INT *n, const double *x, const double *b, MKL_INT *rci_
 static double dotv(long long n, const double *a, const double *b)
 {
     double s = 0.0;
-#pragma omp parallel for reduction(+ : s) schedule(static)
+#pragma omp parallel for reduction(+ : s) schedule(static) num_threads(shim_threads())
     for (long long i = 0; i < n; ++i)
         s += a[i] * b[i];
     return s;
@@ -264,7 +279,7 @@ void dcg(const MKL_INT *n_, double *x, double *b, MKL_INT *rci_request, MKL_INT 
     }
     if (ipar[2] == CG_STAGE_R0)
     {
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) num_threads(shim_threads())
         for (long long i = 0; i < n; ++i)
             r[i] = b[i] - Ap[i];
         double rr = dotv(n, r, r);
@@ -294,7 +309,7 @@ void dcg(const MKL_INT *n_, double *x, double *b, MKL_INT *rci_request, MKL_INT 
     }
     const double rr = dpar[4];
     const double alpha = rr / pAp;
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) num_threads(shim_threads())
     for (long long i = 0; i < n; ++i)
     {
         x[i] += alpha * p[i];
@@ -319,7 +334,7 @@ void dcg(const MKL_INT *n_, double *x, double *b, MKL_INT *rci_request, MKL_INT 
         return;
     }
     const double beta = rr_new / rr;
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) num_threads(shim_threads())
     for (long long i = 0; i < n; ++i)
         p[i] = r[i] + beta * p[i];
     *rci_request = 1;

@@ -13,7 +13,8 @@ import pytest
 
 from _util import ROOT
 
-REF = "/root/reference"
+# the LPM-CPP checkout: $LPM_REFERENCE, else a sibling directory "reference" of this repository
+REF = os.environ.get("LPM_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
 EXAMPLES = sorted(glob.glob(os.path.join(REF, "examples", "*.cpp")) +
                   glob.glob(os.path.join(REF, "examples", "plasticity", "*.cpp")))
 LIBDIR = os.path.join(ROOT, "lpm-cpp_b200")
