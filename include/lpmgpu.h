@@ -278,6 +278,14 @@ int32_t lpmgpu_set_cg_grid(lpmgpu_solver *h, int32_t grid);
  * below the natural barrier wait makes the next solve time out.  No counterpart in the reference,
  * whose CG (MKL dcg, solver.h:303-344) has no device waits. */
 int32_t lpmgpu_set_wait_limit_ns(lpmgpu_solver *h, int64_t ns);
+/* Which stiffness kernel this handle's assemblies use.  0 (the default): the fast form, which
+ * sums the reference's terms (Stiffness::calcStiffness2D/3D over localStiffnessANA,
+ * stiffness.h:198-361, derivative.h:8-239) in closed form over precomputed 2-hop path lists, with
+ * FMA; K agrees with the reference within rounding (about 1e-15 of max|K|).  1: the bit-exact
+ * kernel, which reproduces the reference's operator order entry by entry.  The environment
+ * variable LPMGPU_ASSEMBLY_EXACT, set when a handle is created, skips building the path lists
+ * (the handle then always uses the bit-exact kernel). */
+int32_t lpmgpu_set_assembly_exact(lpmgpu_solver *h, int32_t exact);
 
 /* Device state back to host (any pointer may be NULL): xyz n*3, Pin n*3, stress n*6 (s11 s22
  * s33 s23 s13 s12), damage n, damage_visual n, state_var n*nsv (nsv = 7 for J2, 3 for fatigue

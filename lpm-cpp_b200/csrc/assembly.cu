@@ -485,7 +485,7 @@ __global__ void k_diag_norm(int64_t m, const double *__restrict__ diag, Scalars 
 __global__ void k_bc_diag(int n, int dim, const int *__restrict__ perm, const int64_t *__restrict__ slice_off,
                           const int *__restrict__ cstart, const int *__restrict__ nlq, const int *__restrict__ cons,
                           const double *__restrict__ damage_visual, const Scalars *__restrict__ scal,
-                          double *__restrict__ K, double *__restrict__ res)
+                          double *__restrict__ K, float *__restrict__ K32, double *__restrict__ res)
 {
     const int pos = blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n)
@@ -499,12 +499,37 @@ __global__ void k_bc_diag(int n, int dim, const int *__restrict__ perm, const in
         if (cons[3 * i + k] == 1 || dmg)
         {
             K[(b * dim * dim + k * dim + k) * kSlice + pos % kSlice] = nd;
+            if (K32)
+                K32[(b * dim * dim + k * dim + k) * kSlice + pos % kSlice] = (float)nd;
             res[(int64_t)dim * i + k] = 0.0; // updateStiffnessDispBC zeroes the residual (stiffness.h:434)
         }
 }
 
-cudaError_t launch_assemble(Problem &p, bool apply_bc)
+cudaError_t launch_assemble(Problem &p, bool apply_bc, bool *k32_written)
 {
+    cudaError_t e;
+    if (k32_written)
+        *k32_written = false;
+    if (p.asm_fast && !p.asm_exact)
+    {
+        // the fast form writes the FP32 copy too when the caller wants one
+        const bool k32 = k32_written != nullptr && p.K32 != nullptr;
+        if ((e = launch_assemble_fast(p, apply_bc, k32)) != cudaSuccess)
+            return e;
+        if (apply_bc)
+        {
+            k_diag_norm<<<1, 1024, 0, p.stream>>>((int64_t)p.n * p.dim, p.diag_raw, p.scal);
+            k_bc_diag<<<div_up(p.n, 256), 256, 0, p.stream>>>(p.n, p.dim, p.perm, p.slice_off, p.cstart, p.nlq,
+                                                              p.cons, p.damage_visual, p.scal, p.K,
+                                                              k32 ? p.K32 : nullptr, p.res);
+            p.ctr.kernel_launches += 2;
+            if ((e = cudaGetLastError()) != cudaSuccess)
+                return e;
+        }
+        if (k32_written)
+            *k32_written = k32;
+        return cudaSuccess;
+    }
     AsmArgs a;
     a.n = p.n;
     a.mb = p.max_bonds;
@@ -531,7 +556,6 @@ cudaError_t launch_assemble(Problem &p, bool apply_bc)
     // one thread per connection slot (more threads per block cost more in occupancy than they
     // gain in the staging: measured 3.5 ms vs 5.0 ms per SC 20 mm assembly at 128)
     const int threads = std::min(256, std::max(32, ((p.max_conns + 31) / 32) * 32));
-    cudaError_t e;
     if (p.dim == 2)
     {
         if ((e = cudaFuncSetAttribute(k_assemble<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
@@ -553,7 +577,7 @@ cudaError_t launch_assemble(Problem &p, bool apply_bc)
     {
         k_diag_norm<<<1, 1024, 0, p.stream>>>((int64_t)p.n * p.dim, p.diag_raw, p.scal);
         k_bc_diag<<<div_up(p.n, 256), 256, 0, p.stream>>>(p.n, p.dim, p.perm, p.slice_off, p.cstart, p.nlq, p.cons,
-                                                          p.damage_visual, p.scal, p.K, p.res);
+                                                          p.damage_visual, p.scal, p.K, nullptr, p.res);
         p.ctr.kernel_launches += 2;
         e = cudaGetLastError();
     }

@@ -138,6 +138,16 @@ struct Problem
     double *band_ab = nullptr, *band_y = nullptr;
     int64_t band_kd = 0, band_factored = -1;
     bool direct_off = false; // desc.direct == 2 and the band did not fit: the CG solves
+    // fast assembly (assembly_fast.cu): per-bond T and Ts = T + T_opposite, per-particle U, the
+    // 2-hop path lists (per slot counts, per row offsets, (partner bond, own bond) pairs) and the
+    // flag of a bond broken in one direction only
+    bool asm_fast = false;  // the path lists exist
+    bool asm_exact = false; // lpmgpu_set_assembly_exact: the bit-exact kernel instead
+    double *asm_T = nullptr, *asm_Ts = nullptr, *asm_U = nullptr;
+    unsigned char *asm_cnt = nullptr, *asm_pa = nullptr;
+    int64_t *asm_row = nullptr;
+    int *asm_pb = nullptr, *asm_asym = nullptr;
+    int64_t asm_paths = 0;
 };
 
 constexpr int kMaxGridBlocks = 4096;
@@ -148,7 +158,12 @@ cudaError_t launch_geometry_force(Problem &p);
 cudaError_t launch_update_rr(Problem &p);       // residual + norms into p.scal
 cudaError_t launch_update_rr_impl(Problem &p, bool accumulate_reaction);
 cudaError_t launch_k_to_f32(Problem &p);        // FP32 copy of K for the mixed-precision solve
-cudaError_t launch_assemble(Problem &p, bool apply_bc);
+// stiffness assembly with the BC elimination: the fast form (assembly_fast.cu) once its path
+// lists exist and the handle is not in exact mode, else the bit-exact kernel (assembly.cu).
+// With k32_written, the fast form also writes the FP32 copy and reports it there.
+cudaError_t launch_assemble(Problem &p, bool apply_bc, bool *k32_written = nullptr);
+cudaError_t launch_assemble_fast(Problem &p, bool apply_bc, bool write_k32);
+cudaError_t setup_fast_assembly(Problem &p); // the 2-hop path lists, once per problem
 cudaError_t launch_update_state_var(Problem &p);
 cudaError_t launch_static_damage(Problem &p);   // sets p.scal->any_flag
 // nonlocal damage (damage.cu): the neighbour search at creation, the averaged damage rate,

@@ -28,64 +28,91 @@ struct PhysArgs
     const double *__restrict__ damage;
 };
 
-// updateBondsGeometry + updateBondsForce of particle i
-__global__ void k_geometry_force(PhysArgs a)
+// Sequential sum of v over lanes 0 .. cnt-1 in lane order, the same in every lane: the bond
+// loop's own accumulation order, so the result rounds exactly as the reference's loop does.
+__device__ __forceinline__ double lane_ordered_sum(double acc, double v, int cnt)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n)
-        return;
-    const int b0 = a.bstart[i], b1 = b0 + a.nb0[i], be = a.bstart[i + 1];
-    const double xi0 = a.xyz[3 * i], xi1 = a.xyz[3 * i + 1], xi2 = a.xyz[3 * i + 2];
-    double dlt[2];
-    for (int L = 0; L < 2; ++L)
+    for (int k = 0; k < cnt; ++k)
+        acc += __shfl_sync(0xffffffffu, v, k);
+    return acc;
+}
+
+// updateBondsGeometry + updateBondsForce: one warp per particle, lane k on the k-th bond of a
+// 32-bond chunk of one layer's list.  Every per-bond array is read and written contiguously by
+// the warp (coalesced); only the partner's coordinates and damage are gathers.  The layer sums
+// (dLe, Tv*dLe, cosines) are taken in bond order through the lanes, as the reference's loop
+// takes them (particle.h:164-181).
+constexpr int kPhysWarps = 8;
+__global__ void __launch_bounds__(32 * kPhysWarps) k_geometry_force(PhysArgs a)
+{
+    const int lane = threadIdx.x & 31;
+    const int nw = gridDim.x * kPhysWarps;
+    const bool dmg_max = a.ptype == LPMGPU_J2 || a.ptype == LPMGPU_ELASTIC_DAMAGE || a.ptype == LPMGPU_FATIGUE_HCF;
+    for (int i = blockIdx.x * kPhysWarps + (threadIdx.x >> 5); i < a.n; i += nw)
     {
-        const int lo = L == 0 ? b0 : b1, hi = L == 0 ? b1 : be;
-        double s = 0, ts = 0, cx = 0, cy = 0, cz = 0;
-        for (int b = lo; b < hi; ++b)
+        const int b0 = a.bstart[i], b1 = b0 + a.nb0[i], be = a.bstart[i + 1];
+        const double xi0 = a.xyz[3 * i], xi1 = a.xyz[3 * i + 1], xi2 = a.xyz[3 * i + 2];
+        double dlt[2];
+        for (int L = 0; L < 2; ++L)
         {
-            const int j = a.bp2[b];
-            const double dx = xi0 - a.xyz[3 * j], dy = xi1 - a.xyz[3 * j + 1], dz = xi2 - a.xyz[3 * j + 2];
-            const bool broken = fabs(a.bdamage[b] - 1.0) < kEps;
-            const double dis = sqrt(dx * dx + dy * dy + dz * dz);
-            const double d0 = a.dis0[b];
-            const double dL = broken ? 0.0 : (dis - d0);
-            const double bst = broken ? 0.0 : (dL / dis);
-            const double dle = broken ? 0.0 : (dis - d0 - a.dLp[b]);
-            const double c0 = broken ? 0.0 : (dx / dis);
-            const double c1 = broken ? 0.0 : (dy / dis);
-            const double c2 = broken ? 0.0 : (dz / dis);
-            a.dis[b] = dis;
-            a.bstrain[b] = bst;
-            a.dLe[b] = dle;
-            a.cs[3 * (int64_t)b] = c0;
-            a.cs[3 * (int64_t)b + 1] = c1;
-            a.cs[3 * (int64_t)b + 2] = c2;
-            s += dle;
-            ts += a.Tv[b] * dle;
-            cx += c0;
-            cy += c1;
-            cz += c2;
+            const int lo = L == 0 ? b0 : b1, hi = L == 0 ? b1 : be;
+            double s = 0, ts = 0, cx = 0, cy = 0, cz = 0;
+            for (int c0 = lo; c0 < hi; c0 += 32)
+            {
+                const int b = c0 + lane, cnt = min(32, hi - c0);
+                double dle = 0, tdle = 0, c[3] = {0, 0, 0};
+                if (b < hi)
+                {
+                    const int j = a.bp2[b];
+                    const double dx = xi0 - a.xyz[3 * j], dy = xi1 - a.xyz[3 * j + 1], dz = xi2 - a.xyz[3 * j + 2];
+                    const bool broken = fabs(a.bdamage[b] - 1.0) < kEps;
+                    const double dis = sqrt(dx * dx + dy * dy + dz * dz);
+                    const double d0 = a.dis0[b];
+                    const double dL = broken ? 0.0 : (dis - d0);
+                    const double bst = broken ? 0.0 : (dL / dis);
+                    dle = broken ? 0.0 : (dis - d0 - a.dLp[b]);
+                    c[0] = broken ? 0.0 : (dx / dis);
+                    c[1] = broken ? 0.0 : (dy / dis);
+                    c[2] = broken ? 0.0 : (dz / dis);
+                    a.dis[b] = dis;
+                    a.bstrain[b] = bst;
+                    a.dLe[b] = dle;
+                    a.cs[3 * (int64_t)b] = c[0];
+                    a.cs[3 * (int64_t)b + 1] = c[1];
+                    a.cs[3 * (int64_t)b + 2] = c[2];
+                    tdle = a.Tv[b] * dle;
+                }
+                s = lane_ordered_sum(s, dle, cnt);
+                ts = lane_ordered_sum(ts, tdle, cnt);
+                cx = lane_ordered_sum(cx, c[0], cnt);
+                cy = lane_ordered_sum(cy, c[1], cnt);
+                cz = lane_ordered_sum(cz, c[2], cnt);
+            }
+            dlt[L] = s;
+            if (lane == 0)
+            {
+                a.dLe_total[2 * i + L] = s;
+                a.TdLe_total[2 * i + L] = ts;
+                a.cs_sum[6 * i + 3 * L] = cx;
+                a.cs_sum[6 * i + 3 * L + 1] = cy;
+                a.cs_sum[6 * i + 3 * L + 2] = cz;
+            }
         }
-        dlt[L] = s;
-        a.dLe_total[2 * i + L] = s;
-        a.TdLe_total[2 * i + L] = ts;
-        a.cs_sum[6 * i + 3 * L] = cx;
-        a.cs_sum[6 * i + 3 * L + 1] = cy;
-        a.cs_sum[6 * i + 3 * L + 2] = cz;
-    }
-    const double di = a.damage[i];
-    for (int b = b0; b < be; ++b)
-    {
-        const int L = b < b1 ? 0 : 1;
-        double f = 2. * a.Kn[b] * a.dLe[b] + 2. * a.Tv[b] * dlt[L];
-        double D = a.bdamage[b];
-        if (a.ptype == LPMGPU_J2 || a.ptype == LPMGPU_ELASTIC_DAMAGE || a.ptype == LPMGPU_FATIGUE_HCF)
+        __syncwarp(); // dLe of a bond is read below by another lane than the one that wrote it
+        const double di = a.damage[i];
+        for (int b = b0 + lane; b < be; b += 32)
         {
-            D = std_max(D, std_max(di, a.damage[a.bp2[b]]));
-            a.bdamage[b] = D;
+            const int L = b < b1 ? 0 : 1;
+            double f = 2. * a.Kn[b] * a.dLe[b] + 2. * a.Tv[b] * dlt[L];
+            double D = a.bdamage[b];
+            if (dmg_max)
+            {
+                D = std_max(D, std_max(di, a.damage[a.bp2[b]]));
+                a.bdamage[b] = D;
+            }
+            f *= (1.0 - D);
+            a.bforce[b] = f;
         }
-        f *= (1.0 - D);
-        a.bforce[b] = f;
     }
 }
 
@@ -126,68 +153,97 @@ __device__ __forceinline__ double block_sum(double v, double *sh)
     return r;
 }
 
-// updateParticleForce + updateParticleStress + updateParticleDamageVisual, then updateRR
-constexpr int kForceThreads = 256;
-__global__ void __launch_bounds__(kForceThreads) k_internal_force(ForceArgs a)
+// updateParticleForce + updateParticleStress + updateParticleDamageVisual, then updateRR: one warp
+// per particle, lanes over the bond list in 32-bond chunks (coalesced per-bond reads; the
+// opposite bond's force is a gather), sums in bond order through the lanes.  The per-block
+// partials of the residual and reaction norms are summed in a fixed order (each warp over its
+// particles in turn, then the warps in order), so every run rounds alike.
+constexpr int kForceWarps = 8;
+__global__ void __launch_bounds__(32 * kForceWarps) k_internal_force(ForceArgs a)
 {
-    __shared__ double sh[32];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double rsq = 0.0, rea = 0.0;
-    if (i < a.n)
+    __shared__ double sh[2 * kForceWarps];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int nw = gridDim.x * kForceWarps;
+    double rsq = 0.0, rea = 0.0; // this warp's sums (valid in lane 0)
+    for (int i = blockIdx.x * kForceWarps + w; i < a.n; i += nw)
     {
         const int b0 = a.bstart[i], be = a.bstart[i + 1];
-        double P0 = 0., P1 = 0., P2 = 0.;
-        for (int b = b0; b < be; ++b)
-        {
-            const double fs = a.bforce[b] + a.bforce[a.brev[b]];
-            P0 += a.cs[3 * (int64_t)b] * 0.5 * fs;
-            P1 += a.cs[3 * (int64_t)b + 1] * 0.5 * fs;
-            P2 += a.cs[3 * (int64_t)b + 2] * 0.5 * fs;
-        }
-        a.pin[3 * i] = P0;
-        a.pin[3 * i + 1] = P1;
-        a.pin[3 * i + 2] = P2;
         const int nbi = a.nb[i];
         const double V_m = a.pvol * nbi / a.nneighbors;
+        double P0 = 0., P1 = 0., P2 = 0.;
         double S0 = 0, S1 = 0, S2 = 0, S3 = 0, S4 = 0, S5 = 0, dv = 0;
-        for (int b = b0; b < be; ++b)
+        for (int c0 = b0; c0 < be; c0 += 32)
         {
-            const double fs = a.bforce[b] + a.bforce[a.brev[b]];
-            const double cx = a.cs[3 * (int64_t)b], cy = a.cs[3 * (int64_t)b + 1], cz = a.cs[3 * (int64_t)b + 2];
-            const double w = 0.5 / V_m * (a.dis[b]) * 0.5 * fs;
-            S0 += w * (cx) * (cx);
-            S1 += w * (cy) * (cy);
-            S2 += w * (cz) * (cz);
-            S3 += w * (cy) * (cz);
-            S4 += w * (cx) * (cz);
-            S5 += w * (cx) * (cy);
-            dv += a.bdamage[b];
+            const int b = c0 + lane, cnt = min(32, be - c0);
+            double p0 = 0, p1 = 0, p2 = 0, s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0, dmg = 0;
+            if (b < be)
+            {
+                const double fs = a.bforce[b] + a.bforce[a.brev[b]];
+                const double cx = a.cs[3 * (int64_t)b], cy = a.cs[3 * (int64_t)b + 1], cz = a.cs[3 * (int64_t)b + 2];
+                p0 = cx * 0.5 * fs;
+                p1 = cy * 0.5 * fs;
+                p2 = cz * 0.5 * fs;
+                const double wgt = 0.5 / V_m * (a.dis[b]) * 0.5 * fs;
+                s0 = wgt * (cx) * (cx);
+                s1 = wgt * (cy) * (cy);
+                s2 = wgt * (cz) * (cz);
+                s3 = wgt * (cy) * (cz);
+                s4 = wgt * (cx) * (cz);
+                s5 = wgt * (cx) * (cy);
+                dmg = a.bdamage[b];
+            }
+            P0 = lane_ordered_sum(P0, p0, cnt);
+            P1 = lane_ordered_sum(P1, p1, cnt);
+            P2 = lane_ordered_sum(P2, p2, cnt);
+            S0 = lane_ordered_sum(S0, s0, cnt);
+            S1 = lane_ordered_sum(S1, s1, cnt);
+            S2 = lane_ordered_sum(S2, s2, cnt);
+            S3 = lane_ordered_sum(S3, s3, cnt);
+            S4 = lane_ordered_sum(S4, s4, cnt);
+            S5 = lane_ordered_sum(S5, s5, cnt);
+            dv = lane_ordered_sum(dv, dmg, cnt);
         }
-        double *st = a.stress + 6 * (int64_t)i;
-        st[0] = S0;
-        st[1] = S1;
-        st[2] = S2;
-        st[3] = S3;
-        st[4] = S4;
-        st[5] = S5;
-        a.damage_visual[i] = dv / (double)nbi;
-        const double P[3] = {P0, P1, P2};
-        for (int k = 0; k < a.dim; ++k)
+        if (lane == 0)
         {
-            const int c = a.cons[3 * i + k];
-            const double v = (1 - c) * (a.pex[3 * i + k] - P[k]);
-            a.res[(int64_t)a.dim * i + k] = v;
-            rsq += v * v;
-            if (c == 1)
-                rea += P[k] * P[k];
+            a.pin[3 * i] = P0;
+            a.pin[3 * i + 1] = P1;
+            a.pin[3 * i + 2] = P2;
+            double *st = a.stress + 6 * (int64_t)i;
+            st[0] = S0;
+            st[1] = S1;
+            st[2] = S2;
+            st[3] = S3;
+            st[4] = S4;
+            st[5] = S5;
+            a.damage_visual[i] = dv / (double)nbi;
+            const double P[3] = {P0, P1, P2};
+            for (int k = 0; k < a.dim; ++k)
+            {
+                const int c = a.cons[3 * i + k];
+                const double v = (1 - c) * (a.pex[3 * i + k] - P[k]);
+                a.res[(int64_t)a.dim * i + k] = v;
+                rsq += v * v;
+                if (c == 1)
+                    rea += P[k] * P[k];
+            }
         }
     }
-    const double s0 = block_sum<kForceThreads>(rsq, sh);
-    const double s1 = block_sum<kForceThreads>(rea, sh);
+    if (lane == 0)
+    {
+        sh[w] = rsq;
+        sh[kForceWarps + w] = rea;
+    }
+    __syncthreads();
     if (threadIdx.x == 0)
     {
-        a.partials[2 * blockIdx.x] = s0;
-        a.partials[2 * blockIdx.x + 1] = s1;
+        double r = 0, q = 0;
+        for (int k = 0; k < kForceWarps; ++k)
+        {
+            r += sh[k];
+            q += sh[kForceWarps + k];
+        }
+        a.partials[2 * blockIdx.x] = r;
+        a.partials[2 * blockIdx.x + 1] = q;
     }
 }
 
@@ -209,6 +265,15 @@ __global__ void k_finalize_rr(int nblk, const double *__restrict__ partials, Sca
         if (accumulate)
             scal->reaction_sq += Q;
     }
+}
+
+// grid of the warp-per-particle kernels: one warp per particle up to 16 blocks of 8 warps per SM;
+// beyond that each warp takes several particles
+static int phys_grid(const Problem &p)
+{
+    // the partials buffer holds 2 x kMaxGridBlocks doubles
+    const int64_t cap = std::min<int64_t>((int64_t)p.num_sms * 16, kMaxGridBlocks);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(div_up(p.n, kPhysWarps), cap));
 }
 
 cudaError_t launch_geometry_force(Problem &p)
@@ -236,7 +301,7 @@ cudaError_t launch_geometry_force(Problem &p)
     a.TdLe_total = p.TdLe_total;
     a.cs_sum = p.cs_sum;
     a.damage = p.damage;
-    k_geometry_force<<<div_up(p.n, 128), 128, 0, p.stream>>>(a);
+    k_geometry_force<<<phys_grid(p), 32 * kPhysWarps, 0, p.stream>>>(a);
     p.ctr.kernel_launches++;
     return cudaGetLastError();
 }
@@ -264,8 +329,8 @@ cudaError_t launch_update_rr_impl(Problem &p, bool accumulate_reaction)
     a.damage_visual = p.damage_visual;
     a.res = p.res;
     a.partials = p.partials;
-    const int nblk = div_up(p.n, kForceThreads);
-    k_internal_force<<<nblk, kForceThreads, 0, p.stream>>>(a);
+    const int nblk = phys_grid(p);
+    k_internal_force<<<nblk, 32 * kForceWarps, 0, p.stream>>>(a);
     k_finalize_rr<<<1, 256, 0, p.stream>>>(nblk, p.partials, p.scal, accumulate_reaction ? 1 : 0);
     p.ctr.kernel_launches += 2;
     return cudaGetLastError();

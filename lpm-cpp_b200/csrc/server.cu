@@ -97,6 +97,9 @@ int64_t estimate_bytes(const lpmgpu_desc &d)
     }
     const int64_t per_block = (int64_t)dim * dim * (8 + (d.precision == LPMGPU_MIXED ? 4 : 0)) + 4;
     int64_t per_particle = (int64_t)(1.25 * nc * per_block) + (int64_t)nb * 20 * 8 + 40 * 8 * dim + 512;
+    // the fast assembly's lists: at most nb^2 two-hop paths of 5 bytes, a count per slot, T and
+    // Ts per bond, U and the row offset per particle
+    per_particle += (int64_t)nb * nb * 5 + nc + (int64_t)nb * 16 + 56;
     if (d.nonlocal_cutoff_ratio > 0 && d.radius > 0)
     {
         // nonlocal lists: the particles within cutoff_ratio x nonlocal_L, counted for the densest

@@ -130,8 +130,10 @@ cudaError_t enqueue_force_state(Problem &p, bool with_rr)
 cudaError_t enqueue_assemble(Problem &p, bool apply_bc)
 {
     p.k_version++;
-    cudaError_t e = launch_assemble(p, apply_bc);
-    if (e == cudaSuccess && p.desc.precision == LPMGPU_MIXED)
+    const bool mixed = p.desc.precision == LPMGPU_MIXED;
+    bool k32 = false;
+    cudaError_t e = launch_assemble(p, apply_bc, mixed ? &k32 : nullptr);
+    if (e == cudaSuccess && mixed && !k32)
         e = launch_k_to_f32(p);
     return e;
 }
@@ -809,6 +811,8 @@ int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
         CKF(dalloc(p, &p.q32, ndof));
         CKF(dalloc(p, &p.b32, ndof));
     }
+    if (!std::getenv("LPMGPU_ASSEMBLY_EXACT"))
+        CKF(setup_fast_assembly(p));
     // the examples run updateGeometry + updateForceState before constructing the solver
     CKF(launch_geometry_force(p));
     CKF(launch_update_rr_impl(p, false));
@@ -980,6 +984,14 @@ int32_t lpmgpu_solve_linear(lpmgpu_solver *h, double *disp, lpmgpu_stats *st)
     ST(linear_solve(p, st));
     if (disp)
         CK(cudaMemcpy(disp, p.x, sizeof(double) * p.n * p.dim, cudaMemcpyDeviceToHost));
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_set_assembly_exact(lpmgpu_solver *h, int32_t exact)
+{
+    if (!h || (exact != 0 && exact != 1))
+        return LPMGPU_ERR_INVALID_ARG;
+    h->p.asm_exact = exact != 0;
     return LPMGPU_OK;
 }
 

@@ -198,7 +198,7 @@ EXPORTS = [
     "lpmgpu_fatigue_solve_step", "lpmgpu_fatigue_static_step", "lpmgpu_fatigue_update_damage", "lpmgpu_fatigue_cycle",
     "lpmgpu_read_state", "lpmgpu_read_residual", "lpmgpu_set_xyz", "lpmgpu_get_phase_times",
     "lpmgpu_get_counters", "lpmgpu_get_stream", "lpmgpu_cg_bsr_noalloc", "lpmgpu_autotune", "lpmgpu_set_cg_grid",
-    "lpmgpu_set_wait_limit_ns",
+    "lpmgpu_set_wait_limit_ns", "lpmgpu_set_assembly_exact",
     "lpmgpu_solve_direct", "lpmgpu_band_order", "lpmgpu_get_nonlocal",
     "lpmgpu_format_dump", "lpmgpu_dump_write", "lpmgpu_dump_flush",
     "lpmgpu_batch_create", "lpmgpu_batch_destroy", "lpmgpu_batch_add", "lpmgpu_batch_add_fatigue",
@@ -260,6 +260,7 @@ def lib():
         "lpmgpu_get_nonlocal": (C.c_int32, [vp, ip, ip, lp]),
         "lpmgpu_set_cg_grid": (C.c_int32, [vp, C.c_int32]),
         "lpmgpu_set_wait_limit_ns": (C.c_int32, [vp, C.c_int64]),
+        "lpmgpu_set_assembly_exact": (C.c_int32, [vp, C.c_int32]),
         "lpmgpu_cg_bsr_noalloc": (C.c_int32, [C.c_int32, C.c_int32, vp, vp, vp, vp, vp, C.c_double, C.c_double,
                                               C.c_int64, vp, C.POINTER(C.c_int64)]),
         "lpmgpu_batch_create": (C.c_int32, [C.c_int32, C.POINTER(vp)]),
@@ -846,6 +847,11 @@ class GpuProblem:
     def set_cg_grid(self, grid: int):
         """Blocks per CG launch; 0 restores the default (one block per SM, at most one per slice)."""
         _check(lib().lpmgpu_set_cg_grid(self._h, int(grid)), "lpmgpu_set_cg_grid")
+
+    def set_assembly_exact(self, exact: bool = True):
+        """The bit-exact stiffness kernel (reference operator order) instead of the default fast
+        form (within rounding of the reference; lpmgpu_set_assembly_exact)."""
+        _check(lib().lpmgpu_set_assembly_exact(self._h, int(bool(exact))), "lpmgpu_set_assembly_exact")
 
     def set_wait_limit_ns(self, ns: int):
         """Time limit of each grid-barrier wait in this problem's CG kernel; 0 restores the

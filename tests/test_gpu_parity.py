@@ -77,8 +77,12 @@ def test_initial_force_bit_exact(case):
     assert np.array_equal(sg["damage_visual"], so["damage_visual"])
 
 
-def test_stiffness_matches(case):
+@pytest.mark.parametrize("exact", [True, False], ids=["exact", "fast"])
+def test_stiffness_matches(case, exact):
+    """The bit-exact kernel reproduces the reference's K before the BC elimination bit for bit;
+    the fast form (the default) agrees within K_TOL of max|K|, before and after the elimination."""
     g = gpu_problem(case)
+    g.set_assembly_exact(exact)
     o = oracle_problem(case)
     o.update_geometry()
     o.update_force_state()
@@ -94,7 +98,7 @@ def test_stiffness_matches(case):
         assert np.array_equal(JK, oJK)
         err = np.abs(K - oK).max() / np.abs(oK).max()
         assert err <= K_TOL, f"apply_bc={apply_bc}: max rel {err}"
-        if not apply_bc:
+        if not apply_bc and exact:
             assert np.array_equal(K, oK), "stiffness before the BC elimination should be bit-exact"
 
 
@@ -237,6 +241,7 @@ def test_user_bond_order_is_kept(lat):
     case = CASES[lat]
     case = CFG.Case(**{**case.__dict__, "bonds": _shuffled_bonds(case, 7)})
     g = gpu_problem(case)
+    g.set_assembly_exact(True)
     o = oracle_problem(case)
     t = g.topology()
     nb0, nb1, p2 = case.bonds
@@ -270,6 +275,51 @@ def test_bond_coefficients_and_initial_damage():
         assert okg and oko
         assert rel(g.state()["xyz"] - case.xyz, o.state()["xyz"] - case.xyz) <= FP64_DISP_TOL
     assert np.array_equal(g.state()["bdamage"], o.state()["bdamage"])
+
+
+def _asym_damage_plate():
+    """A hexagonal plate whose explicit per-bond damage breaks 4% of the directed bonds in one
+    direction only, so the opposite bonds stay intact (the case where the fast assembly takes
+    the opposite bonds' own cosines)."""
+    case = CFG.hex_plate(size=2.4, radius=0.1, steps=2, total_disp=0.002, tol_iter=1e-9)
+    o = oracle_problem(case)
+    nb0, nb1, p2 = o.bonds()
+    kn, tv = o.bond_kntv()
+    rng = np.random.default_rng(11)
+    dmg = (rng.random(len(p2)) < 0.04).astype(np.float64)
+    dmg[rng.random(len(p2)) < 0.05] = 0.5  # partial damage too
+    case.bonds = (nb0, nb1, p2)
+    case.bond_props = (kn, tv, dmg)
+    case.name = "hex_asym_damage"
+    return case
+
+
+@pytest.mark.parametrize("name", ["hex", "sc", "sq", "fcc_j2", "sc_j2", "hex_crack", "asym"])
+def test_fast_assembly_matches_exact_after_loading(name):
+    """The fast stiffness form against the bit-exact kernel on deformed, yielded and damaged
+    states: after two load steps each handle re-assembles from the same state, before and after
+    the BC elimination, within K_TOL of max|K|; the oracle's K of the same state agrees too."""
+    case = _asym_damage_plate() if name == "asym" else CASES[name]
+    kw = dict(cg_rtol=1e-24, cg_atol=0.0, tol_iter=1e-9)
+    g = gpu_problem(case, **kw)
+    o = oracle_problem(case, **kw)
+    o.update_geometry()
+    o.update_force_state()
+    for s in range(min(2, len(case.steps))):
+        assert g.solve_load_step(case.load_step(s))[0]
+        assert o.solve_load_step(*oracle_step_args(case, s))[0]
+    for apply_bc in (False, True):
+        g.set_assembly_exact(True)
+        g.assemble(apply_bc)
+        Ke = g.export_csr()[3]
+        g.set_assembly_exact(False)
+        g.assemble(apply_bc)
+        Kf = g.export_csr()[3]
+        o.assemble(apply_bc)
+        oK = o.export_csr()[3]
+        scale = np.abs(Ke).max()
+        assert np.abs(Kf - Ke).max() <= K_TOL * scale, (apply_bc, np.abs(Kf - Ke).max() / scale)
+        assert np.abs(Kf - oK).max() <= 1e-9 * scale  # the states differ by the solves' rounding
 
 
 TANGENT_CASES = {
