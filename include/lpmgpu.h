@@ -108,9 +108,11 @@ typedef struct
      * nonlocal_cutoff_ratio > 0. */
     const int32_t *nonlocal_count, *nonlocal_ids;
     /* Linear solver of the Newton iterations.  0: the CG (Solver::LPM_CG).  1: the direct band
-     * Cholesky (lpmgpu_solve_direct; Solver::LPM_PARDISO's role, solver.h:191-274).  2: the
-     * direct solve when its band fits (at most 32 GiB), else the CG; the C++ and Python drop-ins
-     * use 2 for SolverMode::PARDISO.  The direct solve is FP64 whatever the precision. */
+     * Cholesky (lpmgpu_solve_direct; Solver::LPM_PARDISO's role, solver.h:191-274).  2: the CG
+     * first, and the band Cholesky only for a system the CG could not solve (cap reached or
+     * p.Ap == 0) while its band fits (at most 32 GiB); the C++ and Python drop-ins use 2, with
+     * the CG's squared-norm test at 1e-24, for SolverMode::PARDISO.  The direct solve is FP64
+     * whatever the precision. */
     int32_t direct;
     /* C11 > 0: the bond coefficients come from these elastic constants, as the (C11, C12, C44)
      * overloads of setParticleProperty set them (particle_elastic.h:110-140,
@@ -155,6 +157,7 @@ typedef struct
     double reaction_norm;    /* ||reaction history|| (solver.h:64) */
     double residual_norm;    /* final Newton residual norm */
     double seconds;          /* device time of the call */
+    int32_t direct_solves;   /* linear solves done by the band Cholesky (lpmgpu_desc.direct) */
 } lpmgpu_stats;
 
 typedef struct

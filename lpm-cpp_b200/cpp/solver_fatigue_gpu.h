@@ -175,6 +175,7 @@ private:
         this->totals.newton_solves += st.newton_solves;
         this->totals.cg_iters += st.cg_iters;
         this->totals.cg_maxit_hits += st.cg_maxit_hits;
+        this->totals.direct_solves += st.direct_solves;
         this->reaction_force.assign(1, st.reaction_norm);
     }
 };

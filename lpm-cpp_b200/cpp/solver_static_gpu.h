@@ -109,8 +109,8 @@ public:
           ass(p_ass)
     {
         // SolverMode::PARDISO, the direct solve of Solver::LPM_PARDISO (solver.h:191-274): the
-        // device's band Cholesky where its band fits, else the device CG to a relative residual
-        // of 1e-12 (squared-norm test 1e-24) instead of the reference CG's 1e-6.
+        // device CG to a relative residual of 1e-12 (squared-norm test 1e-24) instead of the
+        // reference CG's 1e-6, and the device's band Cholesky for a system the CG cannot solve.
         if (p_sol_mode == SolverMode::PARDISO)
         {
             direct_ = 2;
@@ -152,6 +152,7 @@ public:
         totals.newton_solves += st.newton_solves;
         totals.cg_iters += st.cg_iters;
         totals.cg_maxit_hits += st.cg_maxit_hits;
+        totals.direct_solves += st.direct_solves;
         reaction_force.assign(1, st.reaction_norm);
         write_back();
         return r == LPMGPU_OK;

@@ -428,6 +428,8 @@ static cudaError_t run_cg(Problem &p, const TK *K, const TV *b, TV *x, TV *r, TV
         out.maxit_hits++;
     if (p.cg_info_host[1] & 2)
         out.timeout = true;
+    if (p.cg_info_host[1] & 4)
+        out.breakdown = true;
     if (rr_final)
         *rr_final = reinterpret_cast<double *>(p.cg_info_host)[3];
     return cudaSuccess;
@@ -471,6 +473,7 @@ static cudaError_t solve_dim(Problem &p, CGResult &out)
         out.iters += inner.iters;
         out.maxit_hits += inner.maxit_hits;
         out.timeout = out.timeout || inner.timeout;
+        out.breakdown = out.breakdown || inner.breakdown;
         out.refinements++;
         if (inner.timeout)
             break;

@@ -187,6 +187,7 @@ struct CGResult
     int64_t maxit_hits = 0;
     int refinements = 0;
     bool timeout = false;
+    bool breakdown = false; // p.Ap == 0 in some launch
 };
 // Solves K x = res (current residual) into p.x with the reference's stopping rule.
 cudaError_t solve_linear(Problem &p, CGResult &out);

@@ -175,7 +175,8 @@ static int32_t assemble(Problem &p, bool apply_bc)
     return LPMGPU_OK;
 }
 
-// The direct solve in place of the CG (desc.direct 1, or 2 while its band fits)
+// The direct solve in place of the CG (desc.direct 1), or after a CG that failed (desc.direct 2,
+// while the band fits).  *used reports whether it ran.
 static int32_t linear_solve_direct(Problem &p, lpmgpu_stats *st, bool *used)
 {
     *used = false;
@@ -185,7 +186,7 @@ static int32_t linear_solve_direct(Problem &p, lpmgpu_stats *st, bool *used)
     const int32_t r = solve_direct(p);
     if (r == LPMGPU_ERR_OUT_OF_MEMORY && p.desc.direct == 2 && !p.band_ab)
     {
-        p.direct_off = true; // the band does not fit: the CG from now on
+        p.direct_off = true; // the band does not fit: the CG's result stands from now on
         return LPMGPU_OK;
     }
     ST(r);
@@ -194,18 +195,32 @@ static int32_t linear_solve_direct(Problem &p, lpmgpu_stats *st, bool *used)
     float ms = 0;
     cudaEventElapsedTime(&ms, p.ev[4], p.ev[5]);
     p.phase_s[2] += ms * 1e-3;
-    if (st)
-        st->newton_solves++;
     *used = true;
     return LPMGPU_OK;
 }
 
+// One linear solve K x = res.  desc.direct 1: the band Cholesky.  desc.direct 2 (the drop-ins'
+// SolverMode::PARDISO): the CG at the caller's tolerance first, and the band Cholesky only when
+// the CG reached its cap or broke down.  Measured on B200 (hexagonal plates of 2,900 and 11,500
+// particles, one factorisation and three solves per load step): the band solve took 20x and 58x
+// the CG's time per load step, so the CG serves PARDISO mode and the factorisation is kept for
+// the systems the CG cannot solve.
 static int32_t linear_solve(Problem &p, lpmgpu_stats *st)
 {
     bool direct = false;
-    ST(linear_solve_direct(p, st, &direct));
-    if (direct)
-        return LPMGPU_OK;
+    if (p.desc.direct == 1)
+    {
+        ST(linear_solve_direct(p, st, &direct));
+        if (direct)
+        {
+            if (st)
+            {
+                st->newton_solves++;
+                st->direct_solves++;
+            }
+            return LPMGPU_OK;
+        }
+    }
     CGResult r;
     CK(cudaEventRecord(p.ev[4], p.stream));
     CK(solve_linear(p, r));
@@ -214,17 +229,20 @@ static int32_t linear_solve(Problem &p, lpmgpu_stats *st)
     float ms = 0;
     cudaEventElapsedTime(&ms, p.ev[4], p.ev[5]);
     p.phase_s[2] += ms * 1e-3;
+    if (r.timeout)
+    {
+        set_last_error("a device-side barrier wait timed out in the CG kernel");
+        return LPMGPU_ERR_TIMEOUT;
+    }
+    if (p.desc.direct == 2 && (r.maxit_hits > 0 || r.breakdown))
+        ST(linear_solve_direct(p, st, &direct));
     if (st)
     {
         st->newton_solves++;
         st->cg_iters += r.iters;
         st->cg_maxit_hits += r.maxit_hits;
         st->refinements += r.refinements;
-    }
-    if (r.timeout)
-    {
-        set_last_error("a device-side barrier wait timed out in the CG kernel");
-        return LPMGPU_ERR_TIMEOUT;
+        st->direct_solves += direct ? 1 : 0;
     }
     return LPMGPU_OK;
 }
@@ -1012,6 +1030,7 @@ int32_t lpmgpu_solve_direct(lpmgpu_solver *h, double *disp, lpmgpu_stats *st)
         float ms = 0;
         cudaEventElapsedTime(&ms, p.ev[4], p.ev[5]);
         st->newton_solves = 1;
+        st->direct_solves = 1;
         st->converged = 1;
         st->seconds = ms * 1e-3;
     }

@@ -120,7 +120,7 @@ class Stats(C.Structure):
     _fields_ = [("converged", C.c_int32), ("newton_solves", C.c_int32), ("cuts", C.c_int32),
                 ("damage_iters", C.c_int32), ("cg_iters", C.c_int64), ("cg_maxit_hits", C.c_int64),
                 ("refinements", C.c_int32), ("reaction_norm", C.c_double), ("residual_norm", C.c_double),
-                ("seconds", C.c_double)]
+                ("seconds", C.c_double), ("direct_solves", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -1121,8 +1121,9 @@ class _StiffnessView:
 
 
 def _direct_mode(sol_mode) -> int:
-    """SolverMode.PARDISO (the reference's direct solve, solver.h:191-274): the band Cholesky
-    where its band fits, else the CG (lpmgpu_desc.direct = 2); SolverMode.CG: the CG."""
+    """SolverMode.PARDISO (the reference's direct solve, solver.h:191-274): the CG to a relative
+    residual of 1e-12, and the band Cholesky for a system the CG cannot solve (lpmgpu_desc.direct
+    = 2); SolverMode.CG: the CG."""
     return 2 if SolverMode(sol_mode) == SolverMode.PARDISO else 0
 
 
@@ -1138,8 +1139,8 @@ class SolverStatic:
     """SolverStatic<nlayer> (include/solver_static.h:17-29) on the GPU: same constructor
     arguments, same solveProblem(load, start_index) contract; extra keyword arguments choose
     the precision and CG tolerances.  SolverMode.PARDISO, the reference's direct solve, runs the
-    device's band Cholesky where its band fits, else the CG to a relative residual of 1e-12
-    (unless tolerances are given)."""
+    device CG to a relative residual of 1e-12 (unless tolerances are given) and the band Cholesky
+    for a system the CG cannot solve."""
 
     def __init__(self, undamaged_pt_type: int, ass: Assembly, stiff_mode=StiffnessMode.Analytical,
                  sol_mode=SolverMode.CG, dumpFile: str = "", max_iter: int = 30, tol: float = 1e-5, *,

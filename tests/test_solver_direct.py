@@ -72,12 +72,15 @@ def test_direct_newton_matches_the_cg_newton(name):
     gc.close()
 
 
-def test_solver_static_pardiso_mode_uses_the_direct_solve():
+def test_solver_static_pardiso_mode_solves_by_cg_first():
+    """SolverMode.PARDISO runs the CG to a relative residual of 1e-12 (the band solve costs 20-58x
+    the CG per load step on the benchmark plates) and keeps the band Cholesky for a system the CG
+    cannot solve; the solution equals the tight CG's."""
     case = _cases()["hex"]
     solv = LPM.SolverStatic(case.undamaged_type, case.assembly(), LPM.StiffnessMode.Analytical,
                             LPM.SolverMode.PARDISO, "", case.max_iter, case.tol_iter)
     solv.solveProblem([case.load_step(s) for s in range(len(case.steps))], 0)
-    assert all(h["cg_iters"] == 0 and h["newton_solves"] > 0 for h in solv.history)
+    assert all(h["cg_iters"] > 0 and h["newton_solves"] > 0 and h["direct_solves"] == 0 for h in solv.history)
     g = gpu_problem(case, **TIGHT)
     for s in range(len(case.steps)):
         g.solve_load_step(case.load_step(s))
@@ -88,7 +91,7 @@ def test_solver_static_pardiso_mode_uses_the_direct_solve():
 
 @pytest.mark.parametrize("name", ["hex", "hex_damage"])
 def test_solver_static_gpu_pardiso_matches_the_reference(name, tmp_path):
-    """SolverStaticGPU with SolverMode::PARDISO (the device's band Cholesky) against the
+    """SolverStaticGPU with SolverMode::PARDISO (the device CG at 1e-12, the band Cholesky behind it) against the
     reference's SolverStatic with SolverMode::PARDISO (Solver::LPM_PARDISO; the MKL stand-in's
     PARDISO solves to 1e-14): the same driver built both ways.  Per step: displacements within
     1e-8 relative and the same broken bonds."""
@@ -115,3 +118,24 @@ def test_solver_static_gpu_pardiso_matches_the_reference(name, tmp_path):
         bg = O.read_bin(out["gpu"], f"bdamage_{t}.f64", np.float64)
         assert np.array_equal(bc == 1.0, bg == 1.0), s
         assert rc[s]["cuts"] == rg[s]["cuts"] == 0
+
+
+def test_pardiso_mode_falls_back_to_the_band_solve_when_the_cg_fails():
+    """desc.direct = 2 with a CG cap too small to converge: every Newton solve's CG stops at its
+    cap and the band Cholesky solves the system instead; the load path equals the direct path's."""
+    case = _cases()["hex"]
+    gf = LPM.GpuProblem(case.assembly(), undamaged_pt_type=case.undamaged_type, max_iter=case.max_iter,
+                        tol_iter=case.tol_iter, direct=2, cg_maxit=3, **TIGHT)
+    gd = LPM.GpuProblem(case.assembly(), undamaged_pt_type=case.undamaged_type, max_iter=case.max_iter,
+                        tol_iter=case.tol_iter, direct=1, **TIGHT)
+    for s in range(len(case.steps)):
+        okf, sf = gf.solve_load_step(case.load_step(s))
+        okd, sd = gd.solve_load_step(case.load_step(s))
+        assert okf and okd
+        assert sf["direct_solves"] == sf["newton_solves"] == sd["newton_solves"] == sd["direct_solves"], (s, sf, sd)
+        assert sf["cg_maxit_hits"] == sf["newton_solves"]
+        uf = gf.state(("xyz",))["xyz"] - case.xyz
+        ud = gd.state(("xyz",))["xyz"] - case.xyz
+        assert rel(uf, ud) <= 1e-12, s
+    gf.close()
+    gd.close()
