@@ -419,6 +419,13 @@ int32_t lpmgpu_batch_get_stats(const lpmgpu_batch *b, lpmgpu_batch_stats *st);
  * in the next round, so one long solve does not hold the other members); 0 = no limit.
  * Default 512. */
 int32_t lpmgpu_batch_set_slice(lpmgpu_batch *b, int64_t iterations);
+/* Lanes of the batch: its members are dealt to `lanes` groups (by matrix volume), each with its
+ * own batched CG launches on an equal share of the SMs.  Lanes progress independently, so one
+ * lane's host decisions and per-member kernels overlap the other lanes' CG kernels, and a short
+ * solve waits only for the longest solve of its own lane.  Only while no member is running;
+ * the default is 1 (LPMGPU_BATCH_LANES in the environment sets a new batch's count).  No
+ * counterpart in the reference. */
+int32_t lpmgpu_batch_set_lanes(lpmgpu_batch *b, int32_t lanes);
 
 /* ---- Serving: LPM solves submitted while others run (continuous batching).  A request is a
  * problem description plus its load path (both copied at submit).  An admission thread builds a
@@ -459,6 +466,8 @@ int32_t lpmgpu_server_create(int32_t device, int64_t hbm_budget_bytes, lpmgpu_se
 /* stops both threads; requests not yet fetched are dropped */
 int32_t lpmgpu_server_destroy(lpmgpu_server *s);
 int32_t lpmgpu_server_set_slice(lpmgpu_server *s, int64_t iterations);
+/* lpmgpu_batch_set_lanes for the server's batch, applied once no request is running */
+int32_t lpmgpu_server_set_lanes(lpmgpu_server *s, int32_t lanes);
 int32_t lpmgpu_server_submit(lpmgpu_server *s, const lpmgpu_desc *d, const lpmgpu_load_step *steps, int32_t nsteps,
                              int64_t *request_id);
 /* A fatigue request: the problem and a SolverFatigue run as lpmgpu_batch_add_fatigue takes it

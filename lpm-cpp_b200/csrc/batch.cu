@@ -49,6 +49,7 @@ constexpr int kMaxVirt = kMaxGridBlocks + kMaxBatch; // virtual blocks
 constexpr int kMaxStage = 1024 + kMaxBatch;          // virtual blocks a launch may use (grid <= 1024)
 constexpr int kMaxMembers = 4096;                    // running members of one batch (launched in groups
                                                      // of at most kMaxBatch)
+constexpr int kDefaultLanes = 1;                     // lanes of a new batch (LPMGPU_BATCH_LANES overrides)
 
 struct BInst
 {
@@ -803,7 +804,8 @@ struct BatchCtx
     double kernel_seconds = 0;
     bool timing_pending = false;
 
-    cudaError_t init(int dev)
+    // grid_cap > 0: at most that many blocks per launch (a lane's share of the SMs)
+    cudaError_t init(int dev, int grid_cap = 0)
     {
         device = dev;
         cudaError_t e;
@@ -826,6 +828,8 @@ struct BatchCtx
                                                                 smem32)) != cudaSuccess)
             return e;
         grid = std::min(1024, num_sms * std::max(1, std::min({occ64, occ32, kCGMinBlocks})));
+        if (grid_cap > 0)
+            grid = std::max(1, std::min(grid, grid_cap));
         if ((e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)) != cudaSuccess)
             return e;
         if ((e = cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming)) != cudaSuccess)
@@ -1081,6 +1085,25 @@ struct Member
     bool fatigue = false;
     size_t nstatic = 0;
     std::vector<std::pair<bool, double>> cycle_end;
+    // the lane that solves this member's linear systems, and the member's weight in its balance
+    int lane = 0;
+    int64_t cost = 0;
+};
+
+// A lane: a share of the SMs with its own batched CG launches (FP64 members, then the FP32 inner
+// solves of mixed members, one launch of each in flight at most; the FP32 launch waits for the
+// FP64 one so the lane never holds more than its share).  Lanes progress independently: while
+// one lane's members take their host decisions and run their per-member kernels, the other
+// lanes' CG kernels keep the GPU busy, and a lane's short solves wait only for its own long
+// ones.  The lanes' shares add up to at most one block per SM, so every launch in flight can
+// be resident at once, as its grid barrier needs.
+struct Lane
+{
+    BatchCtx c64, c32;
+    bool inflight = false;
+    std::vector<Member *> g64, g32; // members of the launches in flight
+    int64_t cost = 0;               // summed matrix cost of its live members
+    int64_t launches = 0;
 };
 
 int32_t cuda_status(cudaError_t e, const char *what)
@@ -1093,7 +1116,9 @@ int32_t cuda_status(cudaError_t e, const char *what)
 
 struct lpmgpu_batch
 {
-    BatchCtx ctx;
+    int device = 0;
+    int64_t slice = 512;
+    std::vector<std::unique_ptr<Lane>> lanes;
     std::vector<std::unique_ptr<Member>> members; // index = member id; removed -> null
     lpmgpu_batch_stats stats{};
     std::chrono::steady_clock::time_point t_create;
@@ -1153,6 +1178,7 @@ struct lpmgpu_batch
         m.pending = false;
         m.t_done = std::chrono::steady_clock::now();
         stats.members_failed++;
+        lanes[m.lane]->cost -= m.cost;
         return LPMGPU_OK;
     }
 
@@ -1163,6 +1189,55 @@ struct lpmgpu_batch
         m.pending = false;
         m.t_done = std::chrono::steady_clock::now();
         stats.members_done++;
+        lanes[m.lane]->cost -= m.cost;
+    }
+
+    double kernel_seconds() const
+    {
+        double t = 0;
+        for (auto &L : lanes)
+            t += L->c64.kernel_seconds + L->c32.kernel_seconds;
+        return t;
+    }
+
+    // (Re)creates the lanes; only while no member is running.  The SMs are split evenly.
+    cudaError_t make_lanes(int nl)
+    {
+        for (auto &L : lanes)
+        {
+            L->c64.release();
+            L->c32.release();
+        }
+        lanes.clear();
+        int sms = 0;
+        cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (e != cudaSuccess)
+            return e;
+        nl = std::max(1, std::min(nl, std::max(1, sms / 8)));
+        for (int l = 0; l < nl; ++l)
+        {
+            auto L = std::make_unique<Lane>();
+            const int cap = (nl == 1) ? 0 : sms / nl;
+            if ((e = L->c64.init(device, cap)) != cudaSuccess || (e = L->c32.init(device, cap)) != cudaSuccess)
+            {
+                L->c64.release();
+                L->c32.release();
+                return e;
+            }
+            L->c64.slice = L->c32.slice = slice;
+            lanes.push_back(std::move(L));
+        }
+        return cudaSuccess;
+    }
+
+    void release()
+    {
+        for (auto &L : lanes)
+        {
+            L->c64.release();
+            L->c32.release();
+        }
+        lanes.clear();
     }
 
     // after the Newton loop of a fatigue member's step (SolverFatigue::solveProblemStep has no
@@ -1377,21 +1452,9 @@ struct lpmgpu_batch
         return cudaSuccess;
     }
 
-    // One batched launch over the members of one precision that need a CG this round (fresh
-    // solves and solves paused by the previous launch's iteration slice).
-    int32_t cg_launch(std::vector<Member *> &all, bool fp32)
-    {
-        for (size_t c0 = 0; c0 < all.size(); c0 += kMaxBatch)
-        {
-            std::vector<Member *> group(all.begin() + c0, all.begin() + std::min(all.size(), c0 + kMaxBatch));
-            const int32_t r = cg_launch_group(group, fp32);
-            if (r != LPMGPU_OK)
-                return r;
-        }
-        return LPMGPU_OK;
-    }
-
-    int32_t cg_launch_group(std::vector<Member *> &ms, bool fp32)
+    // Enqueues one batched launch over members of one precision that need a CG (fresh solves and
+    // solves paused by an earlier launch's iteration slice), without waiting for it.
+    int32_t launch_group(BatchCtx &ctx, std::vector<Member *> &ms, bool fp32)
     {
         if (ms.empty())
             return LPMGPU_OK;
@@ -1412,10 +1475,20 @@ struct lpmgpu_batch
         cudaError_t e = ctx.launch(items);
         if (e != cudaSuccess)
             return cuda_status(e, "batched CG launch");
+        stats.cg_launches++;
+        return LPMGPU_OK;
+    }
+
+    // After the launch of `ctx` finished: each member's CG state, and the follow-up work of the
+    // solves that ended.
+    int32_t finish_group(BatchCtx &ctx, std::vector<Member *> &ms, bool fp32)
+    {
+        if (ms.empty())
+            return LPMGPU_OK;
+        cudaError_t e;
         if ((e = cudaStreamSynchronize(ctx.stream)) != cudaSuccess)
             return cuda_status(e, "batched CG");
         ctx.account();
-        stats.cg_launches++;
         const bool timeout = ctx.h_ctl->fail != 0;
         for (size_t q = 0; q < ms.size(); ++q)
         {
@@ -1437,7 +1510,7 @@ struct lpmgpu_batch
             }
             if (S.status & 8)
             {
-                m.ls_fresh = false; // paused: resumes in the next round
+                m.ls_fresh = false; // paused: resumes in the lane's next launch
                 continue;
             }
             if (fp32)
@@ -1450,41 +1523,73 @@ struct lpmgpu_batch
                 m.cur.cg_maxit_hits++;
             finish_linear(m);
         }
+        ms.clear();
         return LPMGPU_OK;
     }
 
-    int32_t round(int32_t *running)
+    // A lane's launches: the FP64 members waiting for a CG, then the FP32 inner solves of its
+    // mixed members (at most kMaxBatch of each per launch; the rest wait for the next one).
+    int32_t launch_lane(int l)
     {
-        static const bool log = std::getenv("LPMGPU_LOG") != nullptr;
-        const auto t_round = std::chrono::steady_clock::now();
-        const double k0 = ctx.kernel_seconds;
-        const int64_t l0 = stats.cg_launches;
-        round_max_it = 0;
-        stats.rounds++;
-        // A: CG launches for the members waiting for one (FP64 solves, then the FP32 inner
-        // solves of mixed members); finished solves enqueue their follow-up work
-        std::vector<Member *> cg64, cgmix;
+        Lane &L = *lanes[l];
+        L.g64.clear();
+        L.g32.clear();
         for (auto &up : members)
-            if (up && up->ph == Ph::NeedCG)
-                (P(*up).desc.precision == LPMGPU_MIXED ? cgmix : cg64).push_back(up.get());
-        int32_t r = cg_launch(cg64, false);
-        if (r == LPMGPU_OK)
-            r = cg_launch(cgmix, true);
+            if (up && up->lane == l && up->ph == Ph::NeedCG)
+            {
+                auto &g = P(*up).desc.precision == LPMGPU_MIXED ? L.g32 : L.g64;
+                if ((int)g.size() < kMaxBatch)
+                    g.push_back(up.get());
+            }
+        if (L.g64.empty() && L.g32.empty())
+            return LPMGPU_OK;
+        int32_t r = launch_group(L.c64, L.g64, false);
         if (r != LPMGPU_OK)
             return r;
-        // B: until every member waits for a CG (or is finished): start sub-steps, wait once for
-        // all members' pending scalars, take their decisions, repeat
+        if (!L.g64.empty() && !L.g32.empty())
+        {
+            // the FP32 launch starts after the FP64 one: the lane never holds more than its share
+            const cudaError_t e = cudaStreamWaitEvent(L.c32.stream, L.c64.ev_done, 0);
+            if (e != cudaSuccess)
+                return cuda_status(e, "batched CG launch");
+        }
+        if ((r = launch_group(L.c32, L.g32, true)) != LPMGPU_OK)
+            return r;
+        L.inflight = true;
+        L.launches++;
+        return LPMGPU_OK;
+    }
+
+    bool lane_ready(Lane &L)
+    {
+        const cudaEvent_t ev = !L.g32.empty() ? L.c32.ev_done : L.c64.ev_done;
+        return cudaEventQuery(ev) == cudaSuccess;
+    }
+
+    int32_t complete_lane(Lane &L)
+    {
+        int32_t r = finish_group(L.c64, L.g64, false);
+        if (r == LPMGPU_OK)
+            r = finish_group(L.c32, L.g32, true);
+        L.inflight = false;
+        return r;
+    }
+
+    // The host passes of one lane's members: until each waits for a CG (or is finished), start
+    // sub-steps, wait once for all their pending scalars, take their decisions, repeat.
+    int32_t host_passes(int l)
+    {
         for (int pass = 0; pass < 1000; ++pass)
         {
             for (auto &up : members)
-                if (up && up->ph == Ph::Start)
+                if (up && up->lane == l && up->ph == Ph::Start)
                 {
                     cudaSetDevice(P(*up).device);
                     begin_substep(*up);
                 }
             std::vector<Member *> pend;
             for (auto &up : members)
-                if (up && up->pending)
+                if (up && up->lane == l && up->pending)
                     pend.push_back(up.get());
             if (pend.empty())
                 break;
@@ -1494,24 +1599,92 @@ struct lpmgpu_batch
             for (Member *m : pend)
                 resolve(*m);
         }
+        return LPMGPU_OK;
+    }
+
+    // One round: every lane whose launches finished takes its members' results; every idle
+    // lane runs its members' host passes and starts its next launch.  When no lane could do
+    // anything, the round waits for the lane launched first.  With one lane this is the loop of
+    // one launch for all members followed by their host decisions.
+    int32_t round(int32_t *running)
+    {
+        static const bool log = std::getenv("LPMGPU_LOG") != nullptr;
+        const auto t_round = std::chrono::steady_clock::now();
+        const double k0 = kernel_seconds();
+        const int64_t l0 = stats.cg_launches;
+        round_max_it = 0;
+        stats.rounds++;
+        bool progressed = false;
+        for (auto &L : lanes)
+            if (L->inflight && lane_ready(*L))
+            {
+                const int32_t r = complete_lane(*L);
+                if (r != LPMGPU_OK)
+                    return r;
+                progressed = true;
+            }
+        int launched = 0;
+        for (int l = 0; l < (int)lanes.size(); ++l)
+        {
+            if (lanes[l]->inflight)
+                continue;
+            int32_t r = host_passes(l);
+            if (r == LPMGPU_OK)
+                r = launch_lane(l);
+            if (r != LPMGPU_OK)
+                return r;
+            if (lanes[l]->inflight)
+                launched++;
+        }
+        if (!progressed && launched == 0)
+        {
+            // nothing finished and nothing new to start: wait for the lane in flight longest
+            Lane *oldest = nullptr;
+            for (auto &L : lanes)
+                if (L->inflight && (!oldest || L->launches < oldest->launches))
+                    oldest = L.get();
+            if (oldest)
+            {
+                int32_t r = complete_lane(*oldest);
+                const int l = (int)(std::find_if(lanes.begin(), lanes.end(),
+                                                 [&](const std::unique_ptr<Lane> &x) { return x.get() == oldest; }) -
+                                    lanes.begin());
+                if (r == LPMGPU_OK)
+                    r = host_passes(l);
+                if (r == LPMGPU_OK)
+                    r = launch_lane(l);
+                if (r != LPMGPU_OK)
+                    return r;
+            }
+        }
         int32_t live = 0;
         for (auto &up : members)
             if (up && up->ph != Ph::Done && up->ph != Ph::Failed)
                 live++;
         if (running)
             *running = live;
+        if (live == 0)
+            for (auto &L : lanes)
+                if (L->inflight)
+                {
+                    const int32_t r = complete_lane(*L);
+                    if (r != LPMGPU_OK)
+                        return r;
+                }
         if (log)
         {
-            const int64_t maxit = round_max_it;
             int nph[kPhases] = {0};
             for (auto &up : members)
                 if (up)
                     nph[(int)up->ph]++;
+            int infl = 0;
+            for (auto &L : lanes)
+                infl += L->inflight ? 1 : 0;
             std::fprintf(stderr,
-                         "lpmgpu batch round %lld: cg64=%zu cgmix=%zu launches=%lld max_it=%lld kernel_ms=%.3f "
+                         "lpmgpu batch round %lld: lanes in flight %d/%zu launches=%lld max_it=%lld kernel_ms=%.3f "
                          "round_ms=%.3f phases(start,nf,n,cg,dmg,done,fail)=%d,%d,%d,%d,%d,%d,%d\n",
-                         (long long)stats.rounds, cg64.size(), cgmix.size(), (long long)(stats.cg_launches - l0),
-                         (long long)maxit, (ctx.kernel_seconds - k0) * 1e3,
+                         (long long)stats.rounds, infl, lanes.size(), (long long)(stats.cg_launches - l0),
+                         (long long)round_max_it, (kernel_seconds() - k0) * 1e3,
                          std::chrono::duration<double>(std::chrono::steady_clock::now() - t_round).count() * 1e3,
                          nph[0], nph[1], nph[2], nph[3], nph[4], nph[5], nph[6]);
         }
@@ -1535,11 +1708,15 @@ int32_t lpmgpu_batch_create(int32_t device, lpmgpu_batch **out)
     if (device < 0 || device >= ndev)
         return LPMGPU_ERR_INVALID_ARG;
     auto *b = new lpmgpu_batch();
-    cudaError_t e = b->ctx.init(device);
+    b->device = device;
+    const char *env = std::getenv("LPMGPU_BATCH_LANES");
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess)
+        e = b->make_lanes(env ? std::max(1, std::atoi(env)) : kDefaultLanes);
     if (e != cudaSuccess)
     {
         int32_t s = cuda_status(e, "lpmgpu_batch_create");
-        b->ctx.release();
+        b->release();
         delete b;
         return s;
     }
@@ -1552,15 +1729,37 @@ int32_t lpmgpu_batch_destroy(lpmgpu_batch *b)
 {
     if (!b)
         return LPMGPU_ERR_INVALID_ARG;
-    b->ctx.release();
+    cudaSetDevice(b->device);
+    for (auto &L : b->lanes)
+        if (L->inflight)
+            b->complete_lane(*L);
+    b->release();
     delete b;
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_batch_set_lanes(lpmgpu_batch *b, int32_t lanes)
+{
+    if (!b || lanes < 1)
+        return LPMGPU_ERR_INVALID_ARG;
+    for (auto &up : b->members)
+        if (up && up->ph != Ph::Done && up->ph != Ph::Failed)
+        {
+            set_last_error("the lanes of a batch can change only while no member is running");
+            return LPMGPU_ERR_NOT_READY;
+        }
+    if (cudaSetDevice(b->device) != cudaSuccess)
+        return LPMGPU_ERR_CUDA;
+    const cudaError_t e = b->make_lanes(lanes);
+    if (e != cudaSuccess)
+        return cuda_status(e, "lpmgpu_batch_set_lanes");
     return LPMGPU_OK;
 }
 
 // Checks a problem that is to join the batch; LPMGPU_OK when it may.
 static int32_t check_joiner(lpmgpu_batch *b, lpmgpu_solver *h)
 {
-    if (h->p.device != b->ctx.device)
+    if (h->p.device != b->device)
     {
         set_last_error("the problem lives on another device than the batch");
         return LPMGPU_ERR_INVALID_ARG;
@@ -1592,11 +1791,21 @@ static int32_t check_joiner(lpmgpu_batch *b, lpmgpu_solver *h)
 static int32_t push_member(lpmgpu_batch *b, std::unique_ptr<Member> m, int32_t *member)
 {
     m->t_add = std::chrono::steady_clock::now();
+    // the lane with the least matrix volume among its running members
+    const Problem &p = m->h->p;
+    m->cost = p.nsb * (p.dim * p.dim + 1);
+    int best = 0;
+    for (int l = 1; l < (int)b->lanes.size(); ++l)
+        if (b->lanes[l]->cost < b->lanes[best]->cost)
+            best = l;
+    m->lane = best;
+    b->lanes[best]->cost += m->cost;
     if (m->steps.empty())
     {
         m->ph = Ph::Done;
         m->t_done = m->t_add;
         b->stats.members_done++;
+        b->lanes[best]->cost -= m->cost;
     }
     b->members.push_back(std::move(m));
     if (member)
@@ -1673,7 +1882,7 @@ int32_t lpmgpu_batch_round(lpmgpu_batch *b, int32_t *running)
 {
     if (!b)
         return LPMGPU_ERR_INVALID_ARG;
-    if (cudaSetDevice(b->ctx.device) != cudaSuccess)
+    if (cudaSetDevice(b->device) != cudaSuccess)
         return LPMGPU_ERR_CUDA;
     return b->round(running);
 }
@@ -1682,7 +1891,7 @@ int32_t lpmgpu_batch_run(lpmgpu_batch *b)
 {
     if (!b)
         return LPMGPU_ERR_INVALID_ARG;
-    if (cudaSetDevice(b->ctx.device) != cudaSuccess)
+    if (cudaSetDevice(b->device) != cudaSuccess)
         return LPMGPU_ERR_CUDA;
     const auto t0 = std::chrono::steady_clock::now();
     int32_t running = 1;
@@ -1746,7 +1955,9 @@ int32_t lpmgpu_batch_set_slice(lpmgpu_batch *b, int64_t iterations)
 {
     if (!b || iterations < 0)
         return LPMGPU_ERR_INVALID_ARG;
-    b->ctx.slice = iterations;
+    b->slice = iterations;
+    for (auto &L : b->lanes)
+        L->c64.slice = L->c32.slice = iterations;
     return LPMGPU_OK;
 }
 
@@ -1755,7 +1966,7 @@ int32_t lpmgpu_batch_get_stats(const lpmgpu_batch *b, lpmgpu_batch_stats *st)
     if (!b || !st)
         return LPMGPU_ERR_INVALID_ARG;
     *st = b->stats;
-    st->cg_kernel_seconds = b->ctx.kernel_seconds;
+    st->cg_kernel_seconds = b->kernel_seconds();
     int64_t it = 0, di = 0;
     for (auto &up : b->members)
         if (up)

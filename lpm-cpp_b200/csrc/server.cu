@@ -136,6 +136,7 @@ struct lpmgpu_server
     int64_t next_id = 1, used = 0, reserved = 0, peak = 0, running = 0, done = 0, failed = 0, submitted = 0;
     int64_t rounds = 0, finished_epoch = 0;
     int64_t slice = -1; // requested CG slice, applied by the worker between rounds (-1: unchanged)
+    int32_t lanes = 0;  // requested batch lanes, applied by the worker once no request runs (0: unchanged)
     bool stop = false;
     int32_t worker_status = LPMGPU_OK;
     lpmgpu_batch *batch = nullptr;
@@ -250,6 +251,7 @@ struct lpmgpu_server
         {
             std::vector<Request *> add;
             int64_t sl = -1;
+            int32_t nl = 0;
             {
                 std::unique_lock<std::mutex> lk(mu);
                 cv_work.wait(lk, [&] { return stop || !ready.empty() || !live.empty(); });
@@ -258,9 +260,16 @@ struct lpmgpu_server
                 add.swap(ready);
                 sl = slice;
                 slice = -1;
+                if (lanes > 0 && live.empty())
+                {
+                    nl = lanes;
+                    lanes = 0;
+                }
             }
             if (sl >= 0)
                 lpmgpu_batch_set_slice(batch, sl);
+            if (nl > 0)
+                lpmgpu_batch_set_lanes(batch, nl);
             for (Request *r : add)
             {
                 std::vector<lpmgpu_load_step> v;
@@ -406,6 +415,16 @@ int32_t lpmgpu_server_set_slice(lpmgpu_server *s, int64_t iterations)
         return LPMGPU_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(s->mu);
     s->slice = iterations; // applied by the worker before its next round
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_server_set_lanes(lpmgpu_server *s, int32_t lanes)
+{
+    if (!s || lanes < 1)
+        return LPMGPU_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->lanes = lanes; // applied by the worker once no request is running
+    s->cv_work.notify_all();
     return LPMGPU_OK;
 }
 

@@ -204,8 +204,8 @@ EXPORTS = [
     "lpmgpu_batch_create", "lpmgpu_batch_destroy", "lpmgpu_batch_add", "lpmgpu_batch_add_fatigue",
     "lpmgpu_batch_round", "lpmgpu_batch_run",
     "lpmgpu_batch_member", "lpmgpu_batch_member_steps", "lpmgpu_batch_remove", "lpmgpu_batch_get_stats",
-    "lpmgpu_batch_set_slice",
-    "lpmgpu_estimate_bytes", "lpmgpu_server_create", "lpmgpu_server_destroy", "lpmgpu_server_set_slice", "lpmgpu_server_submit",
+    "lpmgpu_batch_set_slice", "lpmgpu_batch_set_lanes",
+    "lpmgpu_estimate_bytes", "lpmgpu_server_create", "lpmgpu_server_destroy", "lpmgpu_server_set_slice", "lpmgpu_server_set_lanes", "lpmgpu_server_submit",
     "lpmgpu_server_submit_fatigue",
     "lpmgpu_server_poll", "lpmgpu_server_wait", "lpmgpu_server_result", "lpmgpu_server_get_stats",
 ]
@@ -275,10 +275,12 @@ def lib():
         "lpmgpu_batch_remove": (C.c_int32, [vp, C.c_int32]),
         "lpmgpu_batch_get_stats": (C.c_int32, [vp, C.POINTER(BatchStats)]),
         "lpmgpu_batch_set_slice": (C.c_int32, [vp, C.c_int64]),
+        "lpmgpu_batch_set_lanes": (C.c_int32, [vp, C.c_int32]),
         "lpmgpu_estimate_bytes": (C.c_int32, [C.POINTER(Desc), lp]),
         "lpmgpu_server_create": (C.c_int32, [C.c_int32, C.c_int64, C.POINTER(vp)]),
         "lpmgpu_server_destroy": (C.c_int32, [vp]),
         "lpmgpu_server_set_slice": (C.c_int32, [vp, C.c_int64]),
+        "lpmgpu_server_set_lanes": (C.c_int32, [vp, C.c_int32]),
         "lpmgpu_server_submit": (C.c_int32, [vp, C.POINTER(Desc), C.POINTER(CLoadStep), C.c_int32, lp]),
         "lpmgpu_server_submit_fatigue": (C.c_int32, [vp, C.POINTER(Desc), C.POINTER(CLoadStep), C.c_int32,
                                                      C.POINTER(CLoadStep), C.c_int32, C.c_int32, dp, lp]),
@@ -970,6 +972,11 @@ class Batch:
         """CG iterations per batched launch before unfinished solves pause (0: no limit)."""
         _check(lib().lpmgpu_batch_set_slice(self._h, int(iterations)), "lpmgpu_batch_set_slice")
 
+    def set_lanes(self, lanes: int):
+        """Independent groups of members, each with its own CG launches on a share of the SMs
+        (lpmgpu_batch_set_lanes); only while no member is running."""
+        _check(lib().lpmgpu_batch_set_lanes(self._h, int(lanes)), "lpmgpu_batch_set_lanes")
+
     def round(self) -> int:
         running = C.c_int32(0)
         _check(lib().lpmgpu_batch_round(self._h, C.byref(running)), "lpmgpu_batch_round")
@@ -1035,6 +1042,10 @@ class Server:
 
     def set_slice(self, iterations: int):
         _check(lib().lpmgpu_server_set_slice(self._h, int(iterations)), "lpmgpu_server_set_slice")
+
+    def set_lanes(self, lanes: int):
+        """lpmgpu_server_set_lanes: the batch's lanes, applied once no request is running."""
+        _check(lib().lpmgpu_server_set_lanes(self._h, int(lanes)), "lpmgpu_server_set_lanes")
 
     def submit(self, ass: Assembly, steps: Sequence[LoadStep], undamaged_pt_type=-1, max_iter=30, tol_iter=1e-5,
                precision: Precision = Precision.FP64, cg_rtol=1e-12, cg_atol=1e-12, cg_maxit=0,

@@ -2,7 +2,8 @@
 
 Each case builds twin handles of the same problems.  One twin of each runs alone, load step by
 load step, through lpmgpu_solve_load_step (the plain path); the others run together as members
-of one batch, whose rounds send all pending Newton systems through one persistent CG launch.
+of one batch, whose rounds send the pending Newton systems of each lane (a group of members with
+its own share of the SMs) through one persistent CG launch.
 The CG partition differs between the two (the batched kernel splits the GPU among the members),
 so the two agree to rounding, not bit for bit.  Bars, with both sides solving tightly (CG
 squared-norm test 1e-24 relative, Newton 1e-9):
@@ -68,11 +69,15 @@ def _check_member(case, batch, mid, g, ref_state, ref_steps, tol, compare_counts
     return info
 
 
-def test_batch_fp64_members_match_alone():
+@pytest.mark.parametrize("lanes", [1, 3])
+def test_batch_fp64_members_match_alone(lanes):
+    """With one lane every round launches all members' CGs together; with three, the members are
+    dealt to three lanes whose launches run side by side on shares of the SMs."""
     cases = _cases() + [_cut_case()]
     max_iters = [None] * (len(cases) - 1) + [5]
     refs = [_alone(c, max_iter=mi) for c, mi in zip(cases, max_iters)]
     batch = LPM.Batch()
+    batch.set_lanes(lanes)
     gs, mids = [], []
     for c, mi in zip(cases, max_iters):
         g = gpu_problem(c, max_iter=mi, **TIGHT)
@@ -90,10 +95,12 @@ def test_batch_fp64_members_match_alone():
         g.close()
 
 
-def test_batch_mixed_members_match_fp64_alone():
+@pytest.mark.parametrize("lanes", [1, 2])
+def test_batch_mixed_members_match_fp64_alone(lanes):
     cases = _cases()[:3]
     refs = [_alone(c) for c in cases]
     batch = LPM.Batch()
+    batch.set_lanes(lanes)
     gs, mids = [], []
     for c in cases:
         g = gpu_problem(c, precision=1, **TIGHT)
@@ -108,11 +115,14 @@ def test_batch_mixed_members_match_fp64_alone():
         g.close()
 
 
-def test_batch_members_join_while_others_run():
-    """Continuous batching: members added between rounds, while earlier members are mid-path."""
+@pytest.mark.parametrize("lanes", [1, 2])
+def test_batch_members_join_while_others_run(lanes):
+    """Continuous batching: members added between rounds, while earlier members are mid-path
+    (with two lanes, also while the other lane's launch is in flight)."""
     cases = _cases()
     refs = [_alone(c) for c in cases]
     batch = LPM.Batch()
+    batch.set_lanes(lanes)
     gs = [gpu_problem(c, **TIGHT) for c in cases]
     mids = [None] * len(cases)
     mids[0] = batch.add(gs[0], [cases[0].load_step(s) for s in range(len(cases[0].steps))])
