@@ -12,7 +12,6 @@
 // kNlAllPairsMax particles and bins them into cells above (nonlocal_grid.cuh), with the same
 // distance test and each list sorted to ascending id; the caller may also hand over its own
 // lists (build_nonlocal_lists).
-#include <cub/cub.cuh>
 
 #include <cstdlib>
 #include <vector>
@@ -126,15 +125,7 @@ static cudaError_t build_nonlocal_grid(Problem &p, double rc)
     k_nonlocal_grid<0><<<div_up(n, 128), 128, 0, p.stream>>>(n, p.xyz, rc, d_cxyz, dims[0], dims[1], dims[2], d_cs,
                                                              d_ci, cnt, nullptr, nullptr);
     p.ctr.kernel_launches++;
-    size_t bytes = 0;
-    if ((e = cub::DeviceScan::ExclusiveSum(nullptr, bytes, cnt, p.nlstart, n + 1, p.stream)) == cudaSuccess &&
-        (e = cudaMallocAsync(&tmp, bytes ? bytes : 16, p.stream)) == cudaSuccess)
-        e = cub::DeviceScan::ExclusiveSum(tmp, bytes, cnt, p.nlstart, n + 1, p.stream);
-    if (tmp)
-    {
-        cudaFreeAsync(tmp, p.stream);
-        tmp = nullptr;
-    }
+    e = prim_exclusive_scan(p.stream, cnt, p.nlstart, (int64_t)n + 1);
     int total = 0;
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(&total, p.nlstart + n, sizeof(int), cudaMemcpyDeviceToHost, p.stream);
@@ -157,13 +148,8 @@ static cudaError_t build_nonlocal_grid(Problem &p, double rc)
         e = cudaGetLastError();
     }
     // each particle's list in ascending id, the order of the reference's loop
-    bytes = 0;
-    if (e == cudaSuccess &&
-        (e = cub::DeviceSegmentedSort::SortKeys(nullptr, bytes, unsorted, p.nlist, total, n, p.nlstart, p.nlstart + 1,
-                                                 p.stream)) == cudaSuccess &&
-        (e = cudaMallocAsync(&tmp, bytes ? bytes : 16, p.stream)) == cudaSuccess)
-        e = cub::DeviceSegmentedSort::SortKeys(tmp, bytes, unsorted, p.nlist, total, n, p.nlstart, p.nlstart + 1,
-                                               p.stream);
+    if (e == cudaSuccess)
+        e = prim_segmented_sort(p.stream, unsorted, p.nlist, total, n, p.nlstart);
     cleanup();
     return e;
 }
@@ -185,14 +171,7 @@ cudaError_t build_nonlocal(Problem &p, double cutoff_ratio)
     const int threads = 256, blocks = div_up((int64_t)n * 32, threads);
     k_nonlocal_search<0><<<blocks, threads, 0, p.stream>>>(n, p.xyz, rc, cnt, nullptr, nullptr);
     p.ctr.kernel_launches++;
-    size_t bytes = 0;
-    if ((e = cub::DeviceScan::ExclusiveSum(nullptr, bytes, cnt, p.nlstart, n + 1, p.stream)) != cudaSuccess)
-        return e;
-    void *tmp = nullptr;
-    if ((e = cudaMallocAsync(&tmp, bytes ? bytes : 16, p.stream)) != cudaSuccess)
-        return e;
-    e = cub::DeviceScan::ExclusiveSum(tmp, bytes, cnt, p.nlstart, n + 1, p.stream);
-    cudaFreeAsync(tmp, p.stream);
+    e = prim_exclusive_scan(p.stream, cnt, p.nlstart, (int64_t)n + 1);
     cudaFreeAsync(cnt, p.stream);
     if (e != cudaSuccess)
         return e;

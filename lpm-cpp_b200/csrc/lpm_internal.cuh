@@ -164,6 +164,14 @@ cudaError_t launch_k_to_f32(Problem &p);        // FP32 copy of K for the mixed-
 cudaError_t launch_assemble(Problem &p, bool apply_bc, bool *k32_written = nullptr);
 cudaError_t launch_assemble_fast(Problem &p, bool apply_bc, bool write_k32);
 cudaError_t setup_fast_assembly(Problem &p); // the 2-hop path lists, once per problem
+// device-wide primitives of the set-up paths (prims.cu), enqueued on a stream
+cudaError_t prim_exclusive_scan(cudaStream_t st, const int *in, int *out, int64_t count);
+cudaError_t prim_exclusive_scan(cudaStream_t st, const int64_t *in, int64_t *out, int64_t count);
+cudaError_t prim_max(cudaStream_t st, const int *in, int64_t count, int *dev_out);
+// stable sort of (key, val) pairs by non-negative key
+cudaError_t prim_sort_pairs(cudaStream_t st, const int *key, const int *val, int *skey, int *sval, int64_t n);
+// each segment [off[s], off[s+1]) of non-negative values sorted ascending, in -> out
+cudaError_t prim_segmented_sort(cudaStream_t st, const int *in, int *out, int64_t total, int nseg, const int *off);
 cudaError_t launch_update_state_var(Problem &p);
 cudaError_t launch_static_damage(Problem &p);   // sets p.scal->any_flag
 // nonlocal damage (damage.cu): the neighbour search at creation, the averaged damage rate,

@@ -8,7 +8,6 @@
 //   Stiffness::initialize          include/stiffness.h:55-71   (K_pointer)
 // The distance is sqrt(dx*dx + dy*dy + dz*dz) evaluated in that order (particle.h:277-280,
 // where the compiler folds pow(x, 2) into x*x), so the bond/layer decisions are identical.
-#include <cub/cub.cuh>
 
 #include <algorithm>
 #include <climits>
@@ -499,36 +498,21 @@ __global__ void k_sell_fill(int n, int nslices, const int *__restrict__ perm, co
 template <typename T>
 static cudaError_t exclusive_scan(Problem &p, const T *in, T *out, int count)
 {
-    size_t bytes = 0;
-    cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, count, p.stream);
-    if (e != cudaSuccess)
-        return e;
-    void *tmp = nullptr;
-    e = cudaMallocAsync(&tmp, bytes ? bytes : 16, p.stream);
-    if (e != cudaSuccess)
-        return e;
-    e = cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, count, p.stream);
-    cudaFreeAsync(tmp, p.stream);
-    return e;
+    return prim_exclusive_scan(p.stream, in, out, count);
 }
 
 static cudaError_t reduce_max(Problem &p, const int *in, int count, int *host_out)
 {
     int *dmax = nullptr;
-    size_t bytes = 0;
-    cudaError_t e = cub::DeviceReduce::Max(nullptr, bytes, in, dmax, count, p.stream);
+    cudaError_t e = cudaMallocAsync(&dmax, sizeof(int), p.stream);
     if (e != cudaSuccess)
         return e;
-    void *tmp = nullptr;
-    if ((e = cudaMallocAsync(&tmp, bytes + 64, p.stream)) != cudaSuccess)
-        return e;
-    dmax = reinterpret_cast<int *>(static_cast<char *>(tmp) + ((bytes + 15) / 16) * 16);
-    e = cub::DeviceReduce::Max(tmp, bytes, in, dmax, count, p.stream);
+    e = prim_max(p.stream, in, count, dmax);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(host_out, dmax, sizeof(int), cudaMemcpyDeviceToHost, p.stream);
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(p.stream);
-    cudaFreeAsync(tmp, p.stream);
+    cudaFreeAsync(dmax, p.stream);
     return e;
 }
 
@@ -593,15 +577,7 @@ cudaError_t build_topology(Problem &p, const double *xyz_host, int *err_code)
     const int T = 256;
     k_cell_keys<<<div_up(n, T), T, 0, p.stream>>>(n, p.xyz, g, key, ids);
     {
-        int bits = 1;
-        while ((1ll << bits) < ncell)
-            bits++;
-        size_t bytes = 0;
-        LPM_TRY(cub::DeviceRadixSort::SortPairs(nullptr, bytes, key, skey, ids, sid, n, 0, bits, p.stream));
-        void *tmp = nullptr;
-        LPM_TRY(cudaMallocAsync(&tmp, bytes + 16, p.stream));
-        LPM_TRY(cub::DeviceRadixSort::SortPairs(tmp, bytes, key, skey, ids, sid, n, 0, bits, p.stream));
-        cudaFreeAsync(tmp, p.stream);
+        LPM_TRY(prim_sort_pairs(p.stream, key, ids, skey, sid, n));
     }
     k_cell_bounds<<<div_up(n, T), T, 0, p.stream>>>(n, skey, cbeg, cend);
 
@@ -740,7 +716,7 @@ cudaError_t build_topology(Problem &p, const double *xyz_host, int *err_code)
     cudaFreeAsync(pad_c, p.stream);
     cudaFreeAsync(ncx, p.stream);
 
-    // sliced-ELL layout: rows by descending connection count (stable radix sort), slices of 32
+    // sliced-ELL layout: rows by descending connection count (stable sort), slices of 32
     {
         int *key = nullptr, *ids = nullptr, *skey = nullptr;
         LPM_TRY(cudaMallocAsync(&key, sizeof(int) * n, p.stream));
@@ -749,15 +725,7 @@ cudaError_t build_topology(Problem &p, const double *xyz_host, int *err_code)
         LPM_TRY(dalloc(p, &p.perm, n));
         LPM_TRY(dalloc(p, &p.iperm, n));
         k_sell_keys<<<div_up(n, T), T, 0, p.stream>>>(n, p.cstart, key, ids);
-        size_t bytes = 0;
-        int bits = 1;
-        while ((1 << bits) <= kMaxConns)
-            bits++;
-        LPM_TRY(cub::DeviceRadixSort::SortPairs(nullptr, bytes, key, skey, ids, p.perm, n, 0, bits, p.stream));
-        void *tmp = nullptr;
-        LPM_TRY(cudaMallocAsync(&tmp, bytes + 16, p.stream));
-        LPM_TRY(cub::DeviceRadixSort::SortPairs(tmp, bytes, key, skey, ids, p.perm, n, 0, bits, p.stream));
-        cudaFreeAsync(tmp, p.stream);
+        LPM_TRY(prim_sort_pairs(p.stream, key, ids, skey, p.perm, n));
         p.nslices = div_up(n, kSlice);
         int64_t *width = nullptr;
         LPM_TRY(cudaMallocAsync(&width, sizeof(int64_t) * (p.nslices + 1), p.stream));
