@@ -56,6 +56,8 @@ def args_():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched 64-plate damage workload")
     ap.add_argument("--plates", type=int, default=64, help="plates in the batched damage workload")
+    ap.add_argument("--batch-lanes", type=int, default=0,
+                    help="lanes of the batch and the server (0: the library's default)")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream leg")
     ap.add_argument("--no-tangent", action="store_true", help="skip the FCC J2 tangent-mode leg")
     ap.add_argument("--no-dump", action="store_true", help="skip the per-step dump output leg")
@@ -379,7 +381,7 @@ def run_ours(a):
     batched = None
     if single and not a.no_batched:
         barrier()
-        batched = batched_leg(lpm, a.plates, local, world, allreduce)
+        batched = batched_leg(lpm, a.plates, local, world, allreduce, a.batch_lanes)
     tangent = None
     if single and not a.no_tangent:
         barrier()
@@ -391,7 +393,7 @@ def run_ours(a):
     serving = None
     if single and not a.no_serving:
         barrier()
-        serving = serving_leg(lpm, a.serve_requests, a.serve_max_particles, local, world, allreduce)
+        serving = serving_leg(lpm, a.serve_requests, a.serve_max_particles, local, world, allreduce, a.batch_lanes)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -709,7 +711,7 @@ def fatigue_batch_sample(lpm, device, sizes=(4.0, 5.0, 6.0, 7.0, 8.0, 9.0, 10.0,
             "max_damage_diff_batched_vs_plain": diff}
 
 
-def batched_leg(lpm, count, device, world, allreduce):
+def batched_leg(lpm, count, device, world, allreduce, lanes=0):
     """Batched 2D damage workload (lpm-cpp_b200/configs.batched_notched_plates): `count` seeded
     single-edge-notched hexagonal plates of uneven size, 40 Mode-I steps each, solved (1) one
     plate at a time on the plain FP64 path, (2) all together by one batch in FP64, (3) all
@@ -746,6 +748,8 @@ def batched_leg(lpm, count, device, world, allreduce):
     def batch_run(prec):
         gs = [make(c, prec) for c in cases]
         b = lpm.Batch(device)
+        if lanes > 0:
+            b.set_lanes(lanes)
         mids = [b.add(g, [c.load_step(s) for s in range(len(c.steps))]) for g, c in zip(gs, cases)]
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -780,6 +784,7 @@ def batched_leg(lpm, count, device, world, allreduce):
     return {"workload": f"{count} single-edge-notched hex plates, side log-uniform 4-25 mm at r=0.1 mm, "
                         f"slit 0.2-0.5 of width, E 60-120 GPa, critical stretch 1e-3-3e-3, 40 Mode-I steps "
                         f"({sum(c.n for c in cases)} particles, seed {cases[0].meta['seed']})",
+            "lanes": lanes if lanes > 0 else "default",
             "plain_fp64_one_at_a_time": plain, "batched_fp64": fp64, "batched_mixed": mixed,
             "speedup_batched_mixed_vs_plain_fp64": mixed["solves_per_s"] / plain["solves_per_s"],
             "speedup_batched_fp64_vs_plain_fp64": fp64["solves_per_s"] / plain["solves_per_s"]}
@@ -831,7 +836,7 @@ def tangent_leg(lpm, steps, device, world, allreduce):
     return out
 
 
-def serving_leg(lpm, count, nmax, device, world, allreduce):
+def serving_leg(lpm, count, nmax, device, world, allreduce, lanes=0):
     """Serving stream (lpm-cpp_b200/configs.serving_requests): `count` requests with seeded
     Poisson arrivals (mean 200/s) of elastic or J2 solves on hex-2D / SC-3D / BCC-3D lattices,
     particle count log-uniform 5e3..`nmax`, 5-50 monotone steps each.
@@ -869,6 +874,8 @@ def serving_leg(lpm, count, nmax, device, world, allreduce):
 
     def served(prec):
         srv = lpm.Server(device=device, hbm_budget_bytes=150 * 10**9)
+        if lanes > 0:
+            srv.set_lanes(lanes)
         ids = [None] * len(reqs)
         t_base = time.perf_counter()
 
