@@ -63,6 +63,9 @@ struct BInst
     const int *col_sell;
     const void *K, *b;
     void *x, *r, *pa, *pb, *q;
+    // the single-reduction inner solves (k_cg_batch_sr): second buffers of r, w = A r (first: q)
+    // and s = A p (first: pb); p is pa
+    void *r1, *w1, *s1;
     double rtol, atol, abs_stop;
     int64_t maxit;
     // refinement (refine = 1): the FP64 system K64 x64 = res, its residual r64 and the outer
@@ -775,6 +778,428 @@ __global__ void __launch_bounds__(kBatchThreads<TV>, kCGMinBlocks) k_cg_batch(BA
         }
 }
 
+// ---- single-reduction inner solves (the FP32 members of a refinement)
+//
+// The textbook CG needs two grid-wide reductions per iteration (p.Ap, then r.r), and in a batch
+// whose members are small each reduction costs a grid barrier plus every block's decision pass:
+// the floor of a batched iteration.  The FP32 inner solves of mixed members therefore run the
+// Chronopoulos-Gear form of the same CG (the same iterates in exact arithmetic, one reduction
+// per iteration), with w = A r computed and s = A p kept by recurrence:
+//   p_k = r_k + beta_{k-1} p_{k-1},   s_k = w_k + beta_{k-1} s_{k-1},
+//   x_{k+1} = x_k + alpha_k p_k,      r_{k+1} = r_k - alpha_k s_k,      w_{k+1} = A r_{k+1},
+//   gamma_{k+1} = r_{k+1}.r_{k+1} and delta_{k+1} = w_{k+1}.r_{k+1} in one reduction,
+//   beta_k = gamma_{k+1} / gamma_k,   alpha_{k+1} = gamma_{k+1} / (delta_{k+1} - beta_k gamma_{k+1} / alpha_k).
+// The SpMV gathers the neighbours' r_{k+1} formed on the fly from their r_k, w_k and s_{k-1},
+// so r, w and s alternate between two buffers each (the iteration's parity).  Every inner solve
+// opens with one phase w_0 = A r_0, alpha_0 = gamma_0 / delta_0.  The FP64 refinement around it
+// (x64 += x32, the true residual, the restart) and its stopping rule are those of k_cg_batch.
+//
+// Modes of a member (S.mode): 6 open a fresh solve from b; 3 open an inner solve from r (after a
+// true residual); 0 iterate; 1 x64 += x32 next; 2 the true residual next.
+
+// q = K v for the row at this lane of slice sl, with v gathered as r (INIT) or formed on the fly
+// as r - alpha (w + beta s) from the three buffers; returns the particle id (-1 past the end).
+template <int D, int U, bool INIT>
+__device__ __forceinline__ int sr_spmv_slice(int sl, const BInst &I, const float *__restrict__ r,
+                                             const float *__restrict__ w, const float *__restrict__ sv, float alpha,
+                                             float beta, float acc[D], uint64_t pf, uint64_t pl, int k0, int kstep)
+{
+    constexpr int E = D * D;
+    const int lane = threadIdx.x & 31;
+    const int pos = sl * kSlice + lane;
+    const bool valid = pos < I.n;
+    const int i = valid ? I.perm[pos] : -1;
+    const int myn = valid ? (I.rowptr[i + 1] - I.rowptr[i]) : 0;
+    const int64_t off = I.slice_off[sl];
+    const int wd = (int)(I.slice_off[sl + 1] - off);
+    const int *cp = I.col_sell + off * kSlice + lane;
+    const float *kp = static_cast<const float *>(I.K) + off * E * kSlice + lane;
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+        acc[k] = 0.0f;
+    int jn[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+    {
+        const int kk = k0 + u * kstep;
+        jn[u] = (kk < myn) ? ld_stream(cp + (int64_t)kk * kSlice, pf) : 0;
+    }
+    for (int k = k0; k < wd; k += U * kstep)
+    {
+        int j[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            j[u] = jn[u];
+            const int kk = k + (U + u) * kstep;
+            jn[u] = (kk < myn) ? ld_stream(cp + (int64_t)kk * kSlice, pf) : 0;
+        }
+        float xv[U][D], kv[U][E];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const int kk = k + u * kstep;
+            if (kk < myn)
+            {
+#pragma unroll
+                for (int c = 0; c < D; ++c)
+                {
+                    const int64_t q = (int64_t)j[u] * D + c;
+                    if (INIT)
+                        xv[u][c] = ld_keep(r + q, pl);
+                    else
+                        xv[u][c] = ld_keep(r + q, pl) - alpha * (ld_keep(w + q, pl) + beta * ld_keep(sv + q, pl));
+                }
+                const float *kb = kp + (int64_t)kk * E * kSlice;
+#pragma unroll
+                for (int e = 0; e < E; ++e)
+                    kv[u][e] = ld_stream(kb + e * kSlice, pf);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (k + u * kstep < myn)
+#pragma unroll
+                for (int rr = 0; rr < D; ++rr)
+#pragma unroll
+                    for (int c = 0; c < D; ++c)
+                        acc[rr] += kv[u][rr * D + c] * xv[u][c];
+    }
+    return i;
+}
+
+// One phase of a member's piece (slices [s0, s1)) in mode 0 (INIT false: iteration k of parity
+// cur) or mode 3/6 (INIT: w_0 = A r_0, the solve's opening; fresh: r_0 = b).  Whole block; with
+// fewer slices than warps several warps share a slice (column split through `red`).  Returns
+// the thread's shares of gamma (r.r) and, in *ldelta, of delta (w.r).
+template <int D, bool INIT, int UV>
+__device__ __forceinline__ double sr_phase(const BInst &I, int s0, int s1, int cur, bool fresh, float alpha, float beta,
+                                           uint64_t pf, uint64_t pl, float *red, double *ldelta)
+{
+    constexpr int U = (D == 2) ? UV : 1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    float *x = static_cast<float *>(I.x), *p = static_cast<float *>(I.pa);
+    float *r0 = static_cast<float *>(I.r), *r1 = static_cast<float *>(I.r1);
+    float *w0 = static_cast<float *>(I.q), *w1 = static_cast<float *>(I.w1);
+    float *s0b = static_cast<float *>(I.pb), *s1b = static_cast<float *>(I.s1);
+    // this iteration's buffers by parity: r_k, w_k in rc, wc; s_{k-1} in sp; writes s_k to sc,
+    // r_{k+1} to rn_, w_{k+1} to wn
+    float *rc = cur ? r1 : r0, *rn_ = cur ? r0 : r1, *wc = cur ? w1 : w0, *wn = cur ? w0 : w1;
+    float *sc = cur ? s1b : s0b, *sp = cur ? s0b : s1b;
+    // gathered sources: the opening reads b (fresh) or r_0; an iteration reads r_k, w_k, s_{k-1}
+    const float *gr = INIT ? (fresh ? static_cast<const float *>(I.b) : r0) : rc;
+    const float *gw = wc, *gs = sp;
+    double lg = 0, ld = 0;
+    auto epilogue = [&](int i, const float *acc) {
+        if (i < 0)
+            return;
+#pragma unroll
+        for (int c = 0; c < D; ++c)
+        {
+            const int64_t k = (int64_t)i * D + c;
+            if (INIT)
+            {
+                const float v = ld_keep(gr + k, pl);
+                if (fresh)
+                    st_keep(r0 + k, v, pl);
+                st_keep(w0 + k, acc[c], pl);
+                st_keep(x + k, 0.0f, pl);
+                st_keep(p + k, 0.0f, pl);
+                st_keep(s1b + k, 0.0f, pl);
+                lg += (double)v * (double)v;
+                ld += (double)acc[c] * (double)v;
+            }
+            else
+            {
+                const float sk = ld_keep(gw + k, pl) + beta * ld_keep(gs + k, pl);
+                const float rk = ld_keep(gr + k, pl);
+                const float pk = rk + beta * ld_keep(p + k, pl);
+                st_keep(x + k, ld_keep(x + k, pl) + alpha * pk, pl);
+                const float rn = rk - alpha * sk;
+                st_keep(sc + k, sk, pl);
+                st_keep(p + k, pk, pl);
+                st_keep(rn_ + k, rn, pl);
+                st_keep(wn + k, acc[c], pl);
+                lg += (double)rn * (double)rn;
+                ld += (double)acc[c] * (double)rn;
+            }
+        }
+    };
+    const int ns = s1 - s0;
+    if (ns > 0)
+    {
+        if (2 * ns > nw)
+        {
+            for (int sl = s0 + warp; sl < s1; sl += nw)
+            {
+                float acc[D];
+                const int i = sr_spmv_slice<D, U, INIT>(sl, I, gr, gw, gs, alpha, beta, acc, pf, pl, 0, 1);
+                epilogue(i, acc);
+            }
+        }
+        else
+        {
+            int S = 2;
+            while (S < kMaxColumnSplit && ns * S * 2 <= nw)
+                S *= 2;
+            const int ls = warp / S, part = warp % S;
+            float acc[D];
+#pragma unroll
+            for (int c = 0; c < D; ++c)
+                acc[c] = 0.0f;
+            int i = -1;
+            if (ls < ns)
+                i = sr_spmv_slice<D, U, INIT>(s0 + ls, I, gr, gw, gs, alpha, beta, acc, pf, pl, part, S);
+            if (ls < ns && part > 0)
+#pragma unroll
+                for (int c = 0; c < D; ++c)
+                    red[(warp * D + c) * 32 + lane] = acc[c];
+            __syncthreads();
+            if (ls < ns && part == 0)
+            {
+                for (int q = 1; q < S; ++q)
+#pragma unroll
+                    for (int c = 0; c < D; ++c)
+                        acc[c] += red[((warp + q) * D + c) * 32 + lane];
+                epilogue(i, acc);
+            }
+            __syncthreads();
+        }
+    }
+    *ldelta = ld;
+    return lg;
+}
+
+// After the barrier of phase `ph`, in every block: each active member's gamma and delta (or its
+// true residual's two norms), its decision, and the compaction / re-split when members left.
+__device__ void sr_reduce_decide(const BArgs &a, BShared &S, int64_t ph, double *stage)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const double *p0 = a.part + (size_t)(2 * (ph & 1)) * kMaxVirt, *p1 = p0 + kMaxVirt;
+    for (int v = threadIdx.x; v < S.nvirt; v += blockDim.x)
+    {
+        stage[v] = __ldcg(p0 + v);
+        stage[kMaxStage + v] = __ldcg(p1 + v);
+    }
+    __syncthreads();
+    for (int r = warp; r < S.nact; r += nw)
+    {
+        const int m = S.act[r];
+        const int md = S.mode[m];
+        const bool sums = md != 1;
+        const double g = sums ? rank_total(S, stage, r) : 0.0;
+        const double d = sums ? rank_total(S, stage + kMaxStage, r) : 0.0;
+        if (lane == 0)
+        {
+            const BInst &I = a.inst[m];
+            int keep = 1;
+            if (md == 6 || md == 3)
+            {
+                // the opening phase: gamma_0 = r_0.r_0, delta_0 = (A r_0).r_0
+                if (md == 6)
+                {
+                    S.stop[m] = (I.abs_stop >= 0) ? I.abs_stop : I.rtol * g + I.atol;
+                    S.cit[m] = 0;
+                }
+                S.rr[m] = g;
+                S.rrf[m] = g;
+                S.beta[m] = 0.0;
+                if (g <= S.stop[m])
+                {
+                    if (I.refine)
+                        inner_done(S, m, false);
+                    else
+                        keep = 0;
+                }
+                else if (d == 0.0)
+                {
+                    S.status[m] |= 4;
+                    if (I.refine)
+                        inner_done(S, m, false);
+                    else
+                        keep = 0;
+                }
+                else
+                {
+                    S.alpha[m] = g / d;
+                    S.mode[m] = 0;
+                }
+            }
+            else if (md == 1)
+                S.mode[m] = 2; // x64 += x32 ran; the true residual is next
+            else if (md == 2)
+            {
+                // the true residual ran: g = ||r64||^2, d = ||(float) r64||^2 (the next r_0)
+                S.rrf[m] = g;
+                if (g <= I.stop64 || S.lastit[m] == 0 || S.refs[m] >= 30)
+                    keep = 0;
+                else
+                {
+                    S.stop[m] = I.abs_stop;
+                    S.cit[m] = 0;
+                    S.mode[m] = 3;
+                }
+            }
+            else
+            {
+                // iteration k ran: g = gamma_{k+1}, d = delta_{k+1}
+                S.cit[m] += 1;
+                S.itot[m] += 1;
+                S.rrf[m] = g;
+                const bool done = g <= S.stop[m];
+                const bool capped = S.cit[m] >= I.maxit;
+                if (done || capped)
+                {
+                    if (I.refine)
+                        inner_done(S, m, !done);
+                    else
+                    {
+                        if (!done)
+                            S.status[m] |= 1;
+                        keep = 0;
+                    }
+                }
+                else
+                {
+                    const double beta = g / S.rr[m];
+                    const double den = d - beta * g / S.alpha[m];
+                    if (den == 0.0)
+                    {
+                        S.status[m] |= 4;
+                        if (I.refine)
+                            inner_done(S, m, false);
+                        else
+                            keep = 0;
+                    }
+                    else
+                    {
+                        S.beta[m] = beta;
+                        S.alpha[m] = g / den;
+                        S.rr[m] = g;
+                    }
+                }
+            }
+            // pause at the end of the launch's slice; only an iterating solve pauses
+            if (keep && S.mode[m] == 0 && ph + 1 >= a.slice)
+            {
+                S.status[m] |= 8;
+                keep = 0;
+            }
+            S.keep[r] = keep;
+        }
+    }
+    __syncthreads();
+    const int t = threadIdx.x, nact = S.nact;
+    const int keep = (t < nact) ? S.keep[t] : 1;
+    const int gone = __syncthreads_count(keep == 0);
+    if (gone == 0)
+        return;
+    const int mine = (t < nact) ? S.act[t] : -1;
+    int nnew = 0;
+    const int pos = block_exscan<int>((t < nact && keep) ? 1 : 0, &nnew, S.scan);
+    if (t < nact && keep)
+        S.keep[pos] = mine;
+    __syncthreads();
+    if (t < nnew)
+        S.act[t] = S.keep[t];
+    if (t == 0)
+        S.nact = nnew;
+    __syncthreads();
+    batch_split(a, S);
+}
+
+// UV: 2 x 2 FP32 steps in flight per warp in the 2D SpMV (1 or 2); 2 needs 128 registers, so its
+// blocks have 512 threads, against 768 at 80 registers for 1
+template <int UV>
+constexpr int kSrThreads = UV == 2 ? 512 : 768;
+
+template <int UV>
+__global__ void __launch_bounds__(kSrThreads<UV>, kCGMinBlocks) k_cg_batch_sr(BArgs a)
+{
+    extern __shared__ __align__(16) unsigned char dsm[];
+    BShared &S = *reinterpret_cast<BShared *>(dsm);
+    BUnion<float> &Un = *reinterpret_cast<BUnion<float> *>(dsm + kBSharedBytes);
+    __shared__ double sh[32];
+    __shared__ int s_fail;
+    const int t = threadIdx.x;
+    if (t == 0)
+    {
+        s_fail = 0;
+        S.nact = a.ninst;
+    }
+    for (int m = t; m < a.ninst; m += blockDim.x)
+    {
+        const BState &B = a.st[m];
+        const BInst &I = a.inst[m];
+        S.act[m] = m;
+        S.rr[m] = B.rr;
+        S.stop[m] = B.stop;
+        S.alpha[m] = B.alpha;
+        S.beta[m] = B.beta;
+        S.rrf[m] = B.rr_final;
+        S.cit[m] = B.it;
+        S.itot[m] = B.it_total;
+        S.lastit[m] = B.last_inner;
+        S.status[m] = (int)B.status;
+        S.mode[m] = I.fresh ? 6 : B.mode;
+        S.refs[m] = B.refs;
+        S.caps[m] = B.caps;
+    }
+    __syncthreads();
+    batch_split(a, S);
+    unsigned epoch = 0;
+    const uint64_t pf = l2_evict_first(), pl = l2_evict_last();
+    for (int64_t ph = 0; S.nact > 0; ++ph)
+    {
+        double *const P0 = a.part + (size_t)(2 * (ph & 1)) * kMaxVirt, *const P1 = P0 + kMaxVirt;
+        for (int k = 0; k < S.np; ++k)
+        {
+            const int r = S.pr_lo + k, m = S.act[r], pidx = S.vs[r] + (int)blockIdx.x - S.fb[r];
+            const BInst &I = a.inst[m];
+            const int md = S.mode[m];
+            double g = 0, d = 0;
+            if (md == 1)
+                refine_add<float>(I, S.ps0[k], S.ps1[k]);
+            else if (md == 2)
+                g = refine_residual<float>(I, S.ps0[k], S.ps1[k], pf, pl, &d);
+            else
+            {
+                const bool init = md != 0;
+                const int cur = (int)(S.cit[m] & 1);
+                const float al = (float)S.alpha[m], be = (float)S.beta[m];
+                if (I.dim == 2)
+                    g = init ? sr_phase<2, true, UV>(I, S.ps0[k], S.ps1[k], 0, md == 6, 0.0f, 0.0f, pf, pl, Un.red, &d)
+                             : sr_phase<2, false, UV>(I, S.ps0[k], S.ps1[k], cur, false, al, be, pf, pl, Un.red, &d);
+                else
+                    g = init ? sr_phase<3, true, UV>(I, S.ps0[k], S.ps1[k], 0, md == 6, 0.0f, 0.0f, pf, pl, Un.red, &d)
+                             : sr_phase<3, false, UV>(I, S.ps0[k], S.ps1[k], cur, false, al, be, pf, pl, Un.red, &d);
+            }
+            block_partial_at(g, P0 + pidx, sh);
+            block_partial_at(d, P1 + pidx, sh);
+        }
+        if (!batch_barrier(a.ctl, epoch, &s_fail))
+            return;
+        sr_reduce_decide(a, S, ph, Un.stage);
+    }
+    if (blockIdx.x == 0)
+        for (int m = t; m < a.ninst; m += blockDim.x)
+        {
+            BState &B = a.st[m];
+            B.rr = S.rr[m];
+            B.stop = S.stop[m];
+            B.alpha = S.alpha[m];
+            B.beta = S.beta[m];
+            B.rr_final = S.rrf[m];
+            B.it = S.cit[m];
+            B.it_total = S.itot[m];
+            B.last_inner = S.lastit[m];
+            B.status = S.status[m];
+            B.mode = S.mode[m];
+            B.refs = S.refs[m];
+            B.caps = S.caps[m];
+        }
+}
+
 // ---- host side of the batched CG
 struct BatchItem
 {
@@ -793,6 +1218,8 @@ struct BatchCtx
     int device = 0, num_sms = 0, grid = 0;
     int64_t slice = 512; // CG iterations per launch before unfinished solves pause
     size_t smem64 = 0, smem32 = 0; // dynamic shared memory of the two kernel variants
+    int sr = 1; // FP32 inner solves: 1, 2 the single-reduction kernel with 1 or 2 SpMV steps in flight;
+                // 0 the two-reduction kernel (LPMGPU_BATCH_SR)
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_done = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
     std::vector<cudaEvent_t> ev_in; // one per item slot
@@ -815,6 +1242,17 @@ struct BatchCtx
             return e;
         smem64 = batch_smem_bytes<double>();
         smem32 = batch_smem_bytes<float>();
+        {
+            const char *env = std::getenv("LPMGPU_BATCH_SR");
+            sr = env ? std::atoi(env) : 1;
+            if (sr < 0 || sr > 2)
+                sr = 1;
+        }
+        if ((e = cudaFuncSetAttribute(k_cg_batch_sr<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32)) !=
+                cudaSuccess ||
+            (e = cudaFuncSetAttribute(k_cg_batch_sr<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32)) !=
+                cudaSuccess)
+            return e;
         if ((e = cudaFuncSetAttribute(k_cg_batch<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem64)) != cudaSuccess ||
             (e = cudaFuncSetAttribute(k_cg_batch<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -827,6 +1265,13 @@ struct BatchCtx
         if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ32, k_cg_batch<float, float>, kBatchThreads<float>,
                                                                 smem32)) != cudaSuccess)
             return e;
+        int occsr1 = 0, occsr2 = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occsr1, k_cg_batch_sr<1>, kSrThreads<1>, smem32)) !=
+                cudaSuccess ||
+            (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occsr2, k_cg_batch_sr<2>, kSrThreads<2>, smem32)) !=
+                cudaSuccess)
+            return e;
+        occ32 = std::min({occ32, occsr1, occsr2});
         grid = std::min(1024, num_sms * std::max(1, std::min({occ64, occ32, kCGMinBlocks})));
         if (grid_cap > 0)
             grid = std::max(1, std::min(grid, grid_cap));
@@ -920,6 +1365,9 @@ struct BatchCtx
                 I.pa = p.pa32;
                 I.pb = p.pb32;
                 I.q = p.q32;
+                I.r1 = p.r32b;
+                I.w1 = p.w32b;
+                I.s1 = p.s32b;
             }
             else
             {
@@ -975,7 +1423,11 @@ struct BatchCtx
         void *args[] = {&a};
         if ((e = cudaEventRecord(ev_t0, stream)) != cudaSuccess)
             return e;
-        e = fp32 ? cudaLaunchCooperativeKernel((const void *)k_cg_batch<float, float>, dim3(grid), dim3(kBatchThreads<float>),
+        e = (fp32 && sr == 1) ? cudaLaunchCooperativeKernel((const void *)k_cg_batch_sr<1>, dim3(grid),
+                                                            dim3(kSrThreads<1>), args, smem32, stream)
+            : (fp32 && sr == 2) ? cudaLaunchCooperativeKernel((const void *)k_cg_batch_sr<2>, dim3(grid),
+                                                              dim3(kSrThreads<2>), args, smem32, stream)
+            : fp32 ? cudaLaunchCooperativeKernel((const void *)k_cg_batch<float, float>, dim3(grid), dim3(kBatchThreads<float>),
                                                args, smem32, stream)
                  : cudaLaunchCooperativeKernel((const void *)k_cg_batch<double, double>, dim3(grid),
                                                dim3(kBatchThreads<double>), args, smem64, stream);

@@ -105,6 +105,7 @@ struct Problem
     // vectors (n*d)
     double *res = nullptr, *x = nullptr, *r = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr;
     float *x32 = nullptr, *r32 = nullptr, *pa32 = nullptr, *pb32 = nullptr, *q32 = nullptr, *b32 = nullptr;
+    float *r32b = nullptr, *w32b = nullptr, *s32b = nullptr; // second buffers of the batch's single-reduction CG
     // reductions
     double *partials = nullptr;       // kMaxGridBlocks * 4
     Scalars *scal = nullptr;

@@ -96,7 +96,9 @@ int64_t estimate_bytes(const lpmgpu_desc &d)
     default: nc = 80; nb = 14; dim = 3; break;
     }
     const int64_t per_block = (int64_t)dim * dim * (8 + (d.precision == LPMGPU_MIXED ? 4 : 0)) + 4;
-    int64_t per_particle = (int64_t)(1.25 * nc * per_block) + (int64_t)nb * 20 * 8 + 40 * 8 * dim + 512;
+    // mixed: the FP32 Krylov vectors, three of them doubled for the batch's single-reduction CG
+    const int64_t mixed_vec = d.precision == LPMGPU_MIXED ? (int64_t)dim * 9 * 4 : 0;
+    int64_t per_particle = (int64_t)(1.25 * nc * per_block) + (int64_t)nb * 20 * 8 + 40 * 8 * dim + 512 + mixed_vec;
     // the fast assembly's lists: at most nb^2 two-hop paths of 5 bytes, a count per slot, T and
     // Ts per bond, U and the row offset per particle
     per_particle += (int64_t)nb * nb * 5 + nc + (int64_t)nb * 16 + 56;

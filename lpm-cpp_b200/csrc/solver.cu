@@ -828,6 +828,9 @@ int32_t lpmgpu_create(const lpmgpu_desc *d, lpmgpu_solver **out)
         CKF(dalloc(p, &p.pb32, ndof));
         CKF(dalloc(p, &p.q32, ndof));
         CKF(dalloc(p, &p.b32, ndof));
+        CKF(dalloc(p, &p.r32b, ndof));
+        CKF(dalloc(p, &p.w32b, ndof));
+        CKF(dalloc(p, &p.s32b, ndof));
     }
     if (!std::getenv("LPMGPU_ASSEMBLY_EXACT"))
         CKF(setup_fast_assembly(p));
