@@ -1,5 +1,7 @@
-// Per-Newton-iteration particle physics on the device, one thread per particle, each bond
-// loop in the reference's list order so the sums round exactly as the reference does:
+// Per-Newton-iteration particle physics on the device.  The bond and force passes work on tiles of
+// particles (per-bond terms one thread per bond, per-particle sums one thread per particle in the
+// reference's bond order); the state updates run one thread per particle.  Every sum follows the
+// reference's list order, so it rounds exactly as the reference's does:
 //   Particle::updateBondsGeometry / Bond::updatebGeometry  include/particle.h:164-181, bond.h:30-39
 //   ParticleElastic::updateBondsForce                      include/particle_elastic.h:38-50
 //   ParticleJ2Plasticity::updateBondsForce                 include/particle_j2plasticity.h:63-76
@@ -28,91 +30,122 @@ struct PhysArgs
     const double *__restrict__ damage;
 };
 
-// Sequential sum of v over lanes 0 .. cnt-1 in lane order, the same in every lane: the bond
-// loop's own accumulation order, so the result rounds exactly as the reference's loop does.
-__device__ __forceinline__ double lane_ordered_sum(double acc, double v, int cnt)
+// Both per-Newton-iteration kernels work on tiles of kTileParticles consecutive particles,
+// whose bonds are one contiguous range of the bond arrays.  Phase 1 runs one thread per BOND
+// (every lane busy, every per-bond array read and written contiguously; only the partner's
+// coordinates, damage and opposite bond are gathers) and leaves the per-bond terms of the
+// particle sums in shared memory.  Phase 2 runs one thread per particle and adds its bonds'
+// terms in bond order, the order of the reference's loops, so every sum rounds exactly as the
+// reference's does.  Blocks loop over tiles, so the grid (and the per-block partials of the
+// residual norms) stay bounded.
+constexpr int kTileParticles = 32;
+constexpr int kTileThreads = 256;
+
+// owner (tile-local particle) of bond b, given the tile's bstart[p0 .. p0 + np] in shared memory
+__device__ __forceinline__ int tile_owner(const int *bs, int np, int b)
 {
-    for (int k = 0; k < cnt; ++k)
-        acc += __shfl_sync(0xffffffffu, v, k);
-    return acc;
+    int lo = 0, hi = np - 1;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi + 1) >> 1;
+        if (bs[mid] <= b)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
 }
 
-// updateBondsGeometry + updateBondsForce: one warp per particle, lane k on the k-th bond of a
-// 32-bond chunk of one layer's list.  Every per-bond array is read and written contiguously by
-// the warp (coalesced); only the partner's coordinates and damage are gathers.  The layer sums
-// (dLe, Tv*dLe, cosines) are taken in bond order through the lanes, as the reference's loop
-// takes them (particle.h:164-181).
-constexpr int kPhysWarps = 8;
-__global__ void __launch_bounds__(32 * kPhysWarps) k_geometry_force(PhysArgs a)
+// updateBondsGeometry + updateBondsForce (particle.h:164-181, bond.h:30-39, particle_elastic.h:38-50)
+__global__ void __launch_bounds__(kTileThreads) k_geometry_force(PhysArgs a, int maxb)
 {
-    const int lane = threadIdx.x & 31;
-    const int nw = gridDim.x * kPhysWarps;
+    extern __shared__ __align__(16) double tsm[];
+    // per tile bond (<= kTileParticles * maxb): dLe, Tv dLe, cs[3]; per particle: the layer sums
+    const int cap = kTileParticles * maxb;
+    double *t_dle = tsm, *t_tdle = t_dle + cap, *t_c = t_tdle + cap, *t_dlt = t_c + 3 * cap;
+    int *bs = reinterpret_cast<int *>(t_dlt + 2 * kTileParticles), *b1s = bs + kTileParticles + 1;
     const bool dmg_max = a.ptype == LPMGPU_J2 || a.ptype == LPMGPU_ELASTIC_DAMAGE || a.ptype == LPMGPU_FATIGUE_HCF;
-    for (int i = blockIdx.x * kPhysWarps + (threadIdx.x >> 5); i < a.n; i += nw)
+    const int ntiles = (a.n + kTileParticles - 1) / kTileParticles;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
     {
-        const int b0 = a.bstart[i], b1 = b0 + a.nb0[i], be = a.bstart[i + 1];
-        const double xi0 = a.xyz[3 * i], xi1 = a.xyz[3 * i + 1], xi2 = a.xyz[3 * i + 2];
-        double dlt[2];
-        for (int L = 0; L < 2; ++L)
+        const int p0 = tile * kTileParticles, np = min(kTileParticles, a.n - p0);
+        for (int q = threadIdx.x; q <= np; q += blockDim.x)
+            bs[q] = a.bstart[p0 + q];
+        for (int q = threadIdx.x; q < np; q += blockDim.x)
+            b1s[q] = a.bstart[p0 + q] + a.nb0[p0 + q];
+        __syncthreads();
+        const int bb = bs[0], be = bs[np];
+        // phase 1: one thread per bond
+        for (int b = bb + threadIdx.x; b < be; b += blockDim.x)
         {
-            const int lo = L == 0 ? b0 : b1, hi = L == 0 ? b1 : be;
-            double s = 0, ts = 0, cx = 0, cy = 0, cz = 0;
-            for (int c0 = lo; c0 < hi; c0 += 32)
+            const int o = tile_owner(bs, np, b), i = p0 + o;
+            const int j = a.bp2[b];
+            const double dx = a.xyz[3 * i] - a.xyz[3 * j], dy = a.xyz[3 * i + 1] - a.xyz[3 * j + 1],
+                         dz = a.xyz[3 * i + 2] - a.xyz[3 * j + 2];
+            const bool broken = fabs(a.bdamage[b] - 1.0) < kEps;
+            const double dis = sqrt(dx * dx + dy * dy + dz * dz);
+            const double d0 = a.dis0[b];
+            const double dL = broken ? 0.0 : (dis - d0);
+            const double bst = broken ? 0.0 : (dL / dis);
+            const double dle = broken ? 0.0 : (dis - d0 - a.dLp[b]);
+            const double c0 = broken ? 0.0 : (dx / dis);
+            const double c1 = broken ? 0.0 : (dy / dis);
+            const double c2 = broken ? 0.0 : (dz / dis);
+            a.dis[b] = dis;
+            a.bstrain[b] = bst;
+            a.dLe[b] = dle;
+            a.cs[3 * (int64_t)b] = c0;
+            a.cs[3 * (int64_t)b + 1] = c1;
+            a.cs[3 * (int64_t)b + 2] = c2;
+            const int t = b - bb;
+            t_dle[t] = dle;
+            t_tdle[t] = a.Tv[b] * dle;
+            t_c[3 * t] = c0;
+            t_c[3 * t + 1] = c1;
+            t_c[3 * t + 2] = c2;
+        }
+        __syncthreads();
+        // phase 2: one thread per particle, each layer's sums in bond order
+        if (threadIdx.x < np)
+        {
+            const int o = threadIdx.x, i = p0 + o;
+            for (int L = 0; L < 2; ++L)
             {
-                const int b = c0 + lane, cnt = min(32, hi - c0);
-                double dle = 0, tdle = 0, c[3] = {0, 0, 0};
-                if (b < hi)
+                const int lo = (L == 0 ? bs[o] : b1s[o]) - bb, hi = (L == 0 ? b1s[o] : bs[o + 1]) - bb;
+                double sd = 0, ts = 0, cx = 0, cy = 0, cz = 0;
+                for (int t = lo; t < hi; ++t)
                 {
-                    const int j = a.bp2[b];
-                    const double dx = xi0 - a.xyz[3 * j], dy = xi1 - a.xyz[3 * j + 1], dz = xi2 - a.xyz[3 * j + 2];
-                    const bool broken = fabs(a.bdamage[b] - 1.0) < kEps;
-                    const double dis = sqrt(dx * dx + dy * dy + dz * dz);
-                    const double d0 = a.dis0[b];
-                    const double dL = broken ? 0.0 : (dis - d0);
-                    const double bst = broken ? 0.0 : (dL / dis);
-                    dle = broken ? 0.0 : (dis - d0 - a.dLp[b]);
-                    c[0] = broken ? 0.0 : (dx / dis);
-                    c[1] = broken ? 0.0 : (dy / dis);
-                    c[2] = broken ? 0.0 : (dz / dis);
-                    a.dis[b] = dis;
-                    a.bstrain[b] = bst;
-                    a.dLe[b] = dle;
-                    a.cs[3 * (int64_t)b] = c[0];
-                    a.cs[3 * (int64_t)b + 1] = c[1];
-                    a.cs[3 * (int64_t)b + 2] = c[2];
-                    tdle = a.Tv[b] * dle;
+                    sd += t_dle[t];
+                    ts += t_tdle[t];
+                    cx += t_c[3 * t];
+                    cy += t_c[3 * t + 1];
+                    cz += t_c[3 * t + 2];
                 }
-                s = lane_ordered_sum(s, dle, cnt);
-                ts = lane_ordered_sum(ts, tdle, cnt);
-                cx = lane_ordered_sum(cx, c[0], cnt);
-                cy = lane_ordered_sum(cy, c[1], cnt);
-                cz = lane_ordered_sum(cz, c[2], cnt);
-            }
-            dlt[L] = s;
-            if (lane == 0)
-            {
-                a.dLe_total[2 * i + L] = s;
+                t_dlt[2 * o + L] = sd;
+                a.dLe_total[2 * i + L] = sd;
                 a.TdLe_total[2 * i + L] = ts;
                 a.cs_sum[6 * i + 3 * L] = cx;
                 a.cs_sum[6 * i + 3 * L + 1] = cy;
                 a.cs_sum[6 * i + 3 * L + 2] = cz;
             }
         }
-        __syncwarp(); // dLe of a bond is read below by another lane than the one that wrote it
-        const double di = a.damage[i];
-        for (int b = b0 + lane; b < be; b += 32)
+        __syncthreads();
+        // phase 3: one thread per bond, the bond force
+        for (int b = bb + threadIdx.x; b < be; b += blockDim.x)
         {
-            const int L = b < b1 ? 0 : 1;
-            double f = 2. * a.Kn[b] * a.dLe[b] + 2. * a.Tv[b] * dlt[L];
+            const int o = tile_owner(bs, np, b), i = p0 + o;
+            const int L = b < b1s[o] ? 0 : 1;
+            double f = 2. * a.Kn[b] * t_dle[b - bb] + 2. * a.Tv[b] * t_dlt[2 * o + L];
             double D = a.bdamage[b];
             if (dmg_max)
             {
-                D = std_max(D, std_max(di, a.damage[a.bp2[b]]));
+                D = std_max(D, std_max(a.damage[i], a.damage[a.bp2[b]]));
                 a.bdamage[b] = D;
             }
             f *= (1.0 - D);
             a.bforce[b] = f;
         }
+        __syncthreads();
     }
 }
 
@@ -153,58 +186,67 @@ __device__ __forceinline__ double block_sum(double v, double *sh)
     return r;
 }
 
-// updateParticleForce + updateParticleStress + updateParticleDamageVisual, then updateRR: one warp
-// per particle, lanes over the bond list in 32-bond chunks (coalesced per-bond reads; the
-// opposite bond's force is a gather), sums in bond order through the lanes.  The per-block
-// partials of the residual and reaction norms are summed in a fixed order (each warp over its
-// particles in turn, then the warps in order), so every run rounds alike.
-constexpr int kForceWarps = 8;
-__global__ void __launch_bounds__(32 * kForceWarps) k_internal_force(ForceArgs a)
+// updateParticleForce + updateParticleStress + updateParticleDamageVisual, then updateRR
+// (particle.h:151-240, solver.h:112-126), in the tiles of k_geometry_force.  The per-block
+// partials of the residual and reaction norms add each tile's particles in order and the tiles
+// in order, so every run rounds alike.
+__global__ void __launch_bounds__(kTileThreads) k_internal_force(ForceArgs a, int maxb)
 {
-    __shared__ double sh[2 * kForceWarps];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int nw = gridDim.x * kForceWarps;
-    double rsq = 0.0, rea = 0.0; // this warp's sums (valid in lane 0)
-    for (int i = blockIdx.x * kForceWarps + w; i < a.n; i += nw)
+    extern __shared__ __align__(16) double tsm[];
+    __shared__ double sh[2 * kTileParticles];
+    // per tile bond: the three Pin terms, the six stress terms and the bond damage
+    const int cap = kTileParticles * maxb;
+    double *t_v = tsm;
+    int *bs = reinterpret_cast<int *>(t_v + 10 * cap);
+    double rsq_blk = 0.0, rea_blk = 0.0; // valid in thread 0
+    const int ntiles = (a.n + kTileParticles - 1) / kTileParticles;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
     {
-        const int b0 = a.bstart[i], be = a.bstart[i + 1];
-        const int nbi = a.nb[i];
-        const double V_m = a.pvol * nbi / a.nneighbors;
-        double P0 = 0., P1 = 0., P2 = 0.;
-        double S0 = 0, S1 = 0, S2 = 0, S3 = 0, S4 = 0, S5 = 0, dv = 0;
-        for (int c0 = b0; c0 < be; c0 += 32)
+        const int p0 = tile * kTileParticles, np = min(kTileParticles, a.n - p0);
+        for (int q = threadIdx.x; q <= np; q += blockDim.x)
+            bs[q] = a.bstart[p0 + q];
+        __syncthreads();
+        const int bb = bs[0], be = bs[np];
+        for (int b = bb + threadIdx.x; b < be; b += blockDim.x)
         {
-            const int b = c0 + lane, cnt = min(32, be - c0);
-            double p0 = 0, p1 = 0, p2 = 0, s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0, dmg = 0;
-            if (b < be)
-            {
-                const double fs = a.bforce[b] + a.bforce[a.brev[b]];
-                const double cx = a.cs[3 * (int64_t)b], cy = a.cs[3 * (int64_t)b + 1], cz = a.cs[3 * (int64_t)b + 2];
-                p0 = cx * 0.5 * fs;
-                p1 = cy * 0.5 * fs;
-                p2 = cz * 0.5 * fs;
-                const double wgt = 0.5 / V_m * (a.dis[b]) * 0.5 * fs;
-                s0 = wgt * (cx) * (cx);
-                s1 = wgt * (cy) * (cy);
-                s2 = wgt * (cz) * (cz);
-                s3 = wgt * (cy) * (cz);
-                s4 = wgt * (cx) * (cz);
-                s5 = wgt * (cx) * (cy);
-                dmg = a.bdamage[b];
-            }
-            P0 = lane_ordered_sum(P0, p0, cnt);
-            P1 = lane_ordered_sum(P1, p1, cnt);
-            P2 = lane_ordered_sum(P2, p2, cnt);
-            S0 = lane_ordered_sum(S0, s0, cnt);
-            S1 = lane_ordered_sum(S1, s1, cnt);
-            S2 = lane_ordered_sum(S2, s2, cnt);
-            S3 = lane_ordered_sum(S3, s3, cnt);
-            S4 = lane_ordered_sum(S4, s4, cnt);
-            S5 = lane_ordered_sum(S5, s5, cnt);
-            dv = lane_ordered_sum(dv, dmg, cnt);
+            const int o = tile_owner(bs, np, b), i = p0 + o;
+            const double V_m = a.pvol * a.nb[i] / a.nneighbors;
+            const double fs = a.bforce[b] + a.bforce[a.brev[b]];
+            const double cx = a.cs[3 * (int64_t)b], cy = a.cs[3 * (int64_t)b + 1], cz = a.cs[3 * (int64_t)b + 2];
+            const double w = 0.5 / V_m * (a.dis[b]) * 0.5 * fs;
+            double *v = t_v + 10 * (b - bb);
+            v[0] = cx * 0.5 * fs;
+            v[1] = cy * 0.5 * fs;
+            v[2] = cz * 0.5 * fs;
+            v[3] = w * (cx) * (cx);
+            v[4] = w * (cy) * (cy);
+            v[5] = w * (cz) * (cz);
+            v[6] = w * (cy) * (cz);
+            v[7] = w * (cx) * (cz);
+            v[8] = w * (cx) * (cy);
+            v[9] = a.bdamage[b];
         }
-        if (lane == 0)
+        __syncthreads();
+        double rsq = 0.0, rea = 0.0;
+        if (threadIdx.x < np)
         {
+            const int o = threadIdx.x, i = p0 + o;
+            double P0 = 0., P1 = 0., P2 = 0.;
+            double S0 = 0, S1 = 0, S2 = 0, S3 = 0, S4 = 0, S5 = 0, dv = 0;
+            for (int t = bs[o] - bb; t < bs[o + 1] - bb; ++t)
+            {
+                const double *v = t_v + 10 * t;
+                P0 += v[0];
+                P1 += v[1];
+                P2 += v[2];
+                S0 += v[3];
+                S1 += v[4];
+                S2 += v[5];
+                S3 += v[6];
+                S4 += v[7];
+                S5 += v[8];
+                dv += v[9];
+            }
             a.pin[3 * i] = P0;
             a.pin[3 * i + 1] = P1;
             a.pin[3 * i + 2] = P2;
@@ -215,35 +257,37 @@ __global__ void __launch_bounds__(32 * kForceWarps) k_internal_force(ForceArgs a
             st[3] = S3;
             st[4] = S4;
             st[5] = S5;
+            const int nbi = a.nb[i];
             a.damage_visual[i] = dv / (double)nbi;
             const double P[3] = {P0, P1, P2};
             for (int k = 0; k < a.dim; ++k)
             {
                 const int c = a.cons[3 * i + k];
-                const double v = (1 - c) * (a.pex[3 * i + k] - P[k]);
-                a.res[(int64_t)a.dim * i + k] = v;
-                rsq += v * v;
+                const double rv = (1 - c) * (a.pex[3 * i + k] - P[k]);
+                a.res[(int64_t)a.dim * i + k] = rv;
+                rsq += rv * rv;
                 if (c == 1)
                     rea += P[k] * P[k];
             }
         }
+        if (threadIdx.x < kTileParticles)
+        {
+            sh[threadIdx.x] = rsq;
+            sh[kTileParticles + threadIdx.x] = rea;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int k = 0; k < np; ++k)
+            {
+                rsq_blk += sh[k];
+                rea_blk += sh[kTileParticles + k];
+            }
+        __syncthreads();
     }
-    if (lane == 0)
-    {
-        sh[w] = rsq;
-        sh[kForceWarps + w] = rea;
-    }
-    __syncthreads();
     if (threadIdx.x == 0)
     {
-        double r = 0, q = 0;
-        for (int k = 0; k < kForceWarps; ++k)
-        {
-            r += sh[k];
-            q += sh[kForceWarps + k];
-        }
-        a.partials[2 * blockIdx.x] = r;
-        a.partials[2 * blockIdx.x + 1] = q;
+        a.partials[2 * blockIdx.x] = rsq_blk;
+        a.partials[2 * blockIdx.x + 1] = rea_blk;
     }
 }
 
@@ -267,13 +311,24 @@ __global__ void k_finalize_rr(int nblk, const double *__restrict__ partials, Sca
     }
 }
 
-// grid of the warp-per-particle kernels: one warp per particle up to 16 blocks of 8 warps per SM;
-// beyond that each warp takes several particles
+// grid of the tiled kernels: one block per tile up to 8 blocks per SM, then blocks loop over
+// tiles (the per-block partials fit the 2 x kMaxGridBlocks buffer)
 static int phys_grid(const Problem &p)
 {
-    // the partials buffer holds 2 x kMaxGridBlocks doubles
-    const int64_t cap = std::min<int64_t>((int64_t)p.num_sms * 16, kMaxGridBlocks);
-    return (int)std::max<int64_t>(1, std::min<int64_t>(div_up(p.n, kPhysWarps), cap));
+    const int64_t ntiles = (p.n + kTileParticles - 1) / kTileParticles;
+    const int64_t cap = std::min<int64_t>((int64_t)p.num_sms * 8, kMaxGridBlocks);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, cap));
+}
+
+static size_t geo_smem(const Problem &p)
+{
+    return sizeof(double) * (5 * (size_t)kTileParticles * p.max_bonds + 2 * kTileParticles) +
+           sizeof(int) * (2 * kTileParticles + 1);
+}
+
+static size_t force_smem(const Problem &p)
+{
+    return sizeof(double) * 10 * (size_t)kTileParticles * p.max_bonds + sizeof(int) * (kTileParticles + 1);
 }
 
 cudaError_t launch_geometry_force(Problem &p)
@@ -301,7 +356,15 @@ cudaError_t launch_geometry_force(Problem &p)
     a.TdLe_total = p.TdLe_total;
     a.cs_sum = p.cs_sum;
     a.damage = p.damage;
-    k_geometry_force<<<phys_grid(p), 32 * kPhysWarps, 0, p.stream>>>(a);
+    const size_t smem = geo_smem(p);
+    if (smem > 48 * 1024)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(k_geometry_force, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)smem);
+        if (e != cudaSuccess)
+            return e;
+    }
+    k_geometry_force<<<phys_grid(p), kTileThreads, smem, p.stream>>>(a, p.max_bonds);
     p.ctr.kernel_launches++;
     return cudaGetLastError();
 }
@@ -330,7 +393,15 @@ cudaError_t launch_update_rr_impl(Problem &p, bool accumulate_reaction)
     a.res = p.res;
     a.partials = p.partials;
     const int nblk = phys_grid(p);
-    k_internal_force<<<nblk, 32 * kForceWarps, 0, p.stream>>>(a);
+    const size_t smem = force_smem(p);
+    if (smem > 48 * 1024)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(k_internal_force, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)smem);
+        if (e != cudaSuccess)
+            return e;
+    }
+    k_internal_force<<<nblk, kTileThreads, smem, p.stream>>>(a, p.max_bonds);
     k_finalize_rr<<<1, 256, 0, p.stream>>>(nblk, p.partials, p.scal, accumulate_reaction ? 1 : 0);
     p.ctr.kernel_launches += 2;
     return cudaGetLastError();
