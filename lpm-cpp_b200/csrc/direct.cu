@@ -138,18 +138,92 @@ __global__ void k_band_fill(int n, const int *__restrict__ rowptr, const int *__
     }
 }
 
-__global__ void k_potrf(double *AB, int64_t ldab, int64_t kd, int64_t j0, int64_t jb, int *fail)
+// The diagonal block by one warp: the block's lower triangle (inside the band) staged in shared
+// memory, lane i owning row i.  Per column jj: the pivot's square root, the column scaled, the
+// trailing entries updated, each entry receiving exactly the operations, in the order, of
+// band::potrf_block (which the host tests run), so the factor is bit for bit the same.
+__global__ void __launch_bounds__(32) k_potrf(double *AB, int64_t ldab, int64_t kd, int64_t j0, int64_t jb, int *fail)
 {
-    const int r = band::potrf_block(AB, ldab, kd, j0, jb);
-    if (r && *fail == 0)
-        *fail = (int)(j0 + r);
+    __shared__ double a[32][33];
+    __shared__ int bad;
+    const int i = threadIdx.x;
+    if (i == 0)
+        bad = 0;
+    if (i < jb)
+        for (int j = 0; j <= i; ++j)
+            a[i][j] = (i - j <= kd) ? band::at(AB, ldab, j0 + i, j0 + j) : 0.0;
+    __syncwarp();
+    for (int jj = 0; jj < jb; ++jj)
+    {
+        if (i == jj)
+        {
+            const double v = a[jj][jj];
+            if (!(v > 0.0))
+                bad = jj + 1;
+            else
+                a[jj][jj] = sqrt(v);
+        }
+        __syncwarp();
+        if (bad)
+            break;
+        const double d = a[jj][jj];
+        if (i > jj && i < jb && i - jj <= kd)
+            a[i][jj] = a[i][jj] / d;
+        __syncwarp();
+        // row i: entries (i, c), jj < c <= i, in ascending c as the one-thread loop reaches them
+        if (i > jj && i < jb && i - jj <= kd)
+            for (int c = jj + 1; c <= i; ++c)
+                if (c - jj <= kd)
+                    a[i][c] = a[i][c] - a[i][jj] * a[c][jj];
+        __syncwarp();
+    }
+    if (bad)
+    {
+        if (i == 0 && *fail == 0)
+            *fail = (int)(j0 + bad);
+        return;
+    }
+    if (i < jb)
+        for (int j = 0; j <= i; ++j)
+            if (i - j <= kd)
+                band::at(AB, ldab, j0 + i, j0 + j) = a[i][j];
 }
 
-__global__ void k_trsm(double *AB, int64_t ldab, int64_t kd, int64_t j0, int64_t jb, int64_t m2)
+// The rows below the diagonal block, one thread per row, with the factored block and the thread's
+// row staged in shared memory; each entry gets band::trsm_row's operations in its order.
+constexpr int kTrsmThreads = 128;
+__global__ void __launch_bounds__(kTrsmThreads) k_trsm(double *AB, int64_t ldab, int64_t kd, int64_t j0, int64_t jb,
+                                                       int64_t m2)
 {
+    __shared__ double L[32][33];
+    __shared__ double row[kTrsmThreads][33];
+    for (int q = threadIdx.x; q < 32 * 32; q += blockDim.x)
+    {
+        const int r = q / 32, c = q % 32;
+        L[r][c] = (r < jb && c <= r && r - c <= kd) ? band::at(AB, ldab, j0 + r, j0 + c) : 0.0;
+    }
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i = j0 + jb + t;
+    double *w = row[threadIdx.x];
     if (t < m2)
-        band::trsm_row(AB, ldab, kd, j0, jb, j0 + jb + t);
+        for (int jj = 0; jj < jb; ++jj)
+            w[jj] = (i - (j0 + jj) <= kd) ? band::at(AB, ldab, i, j0 + jj) : 0.0;
+    __syncthreads();
+    if (t >= m2)
+        return;
+    for (int jj = 0; jj < jb; ++jj)
+    {
+        const int64_t j = j0 + jj;
+        if (i - j > kd)
+            continue;
+        double v = w[jj];
+        for (int kk = 0; kk < jj; ++kk)
+            if (i - (j0 + kk) <= kd)
+                v = v - w[kk] * L[jj][kk];
+        v = v / L[jj][jj];
+        w[jj] = v;
+        band::at(AB, ldab, i, j) = v;
+    }
 }
 
 // threads along i (contiguous band columns), blocks along c
@@ -268,7 +342,7 @@ static cudaError_t factor(Problem &p)
     {
         const int64_t jb = std::min<int64_t>(kBandNB, ndof - j0);
         const int64_t m2 = band::below_end(ndof, kd, j0, jb) - (j0 + jb);
-        k_potrf<<<1, 1, 0, p.stream>>>(p.band_ab, ldab, kd, j0, jb, p.band_fail);
+        k_potrf<<<1, 32, 0, p.stream>>>(p.band_ab, ldab, kd, j0, jb, p.band_fail);
         p.ctr.kernel_launches++;
         if (m2 > 0)
         {
