@@ -246,7 +246,7 @@ struct FastArgs
 };
 
 template <int D>
-__global__ void __launch_bounds__(32 * kAsmWarps, 3) k_assemble_fast(FastArgs a)
+__global__ void __launch_bounds__(32 * kAsmWarps, D == 2 ? 4 : 3) k_assemble_fast(FastArgs a)
 {
     extern __shared__ __align__(16) unsigned char fsm[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
