@@ -868,6 +868,82 @@ __device__ __forceinline__ int sr_spmv_slice(int sl, const BInst &I, const float
     return i;
 }
 
+// The vector work of one row after its SpMV (acc = K v): the opening (INIT: r_0, w_0 = A r_0 and
+// the zeroed x, p, s_{-1}; gamma_0, delta_0) or iteration k of parity cur (s_k, p_k, x_{k+1},
+// r_{k+1}, w_{k+1}; gamma_{k+1}, delta_{k+1}), accumulated into lg, ld.
+template <int D, bool INIT>
+__device__ __forceinline__ void sr_row(const BInst &I, int i, const float *acc, int cur, bool fresh, float alpha,
+                                       float beta, uint64_t pl, double &lg, double &ld)
+{
+    if (i < 0)
+        return;
+    float *x = static_cast<float *>(I.x), *p = static_cast<float *>(I.pa);
+    float *r0 = static_cast<float *>(I.r), *r1 = static_cast<float *>(I.r1);
+    float *w0 = static_cast<float *>(I.q), *w1 = static_cast<float *>(I.w1);
+    float *s0b = static_cast<float *>(I.pb), *s1b = static_cast<float *>(I.s1);
+    // this iteration's buffers by parity: r_k, w_k in rc, wc; s_{k-1} in sp; s_k goes to sc,
+    // r_{k+1} to rn_, w_{k+1} to wn
+    float *rc = cur ? r1 : r0, *rn_ = cur ? r0 : r1, *wc = cur ? w1 : w0, *wn = cur ? w0 : w1;
+    float *sc = cur ? s1b : s0b, *sp = cur ? s0b : s1b;
+#pragma unroll
+    for (int c = 0; c < D; ++c)
+    {
+        const int64_t k = (int64_t)i * D + c;
+        if (INIT)
+        {
+            const float v = ld_keep((fresh ? static_cast<const float *>(I.b) : r0) + k, pl);
+            if (fresh)
+                st_keep(r0 + k, v, pl);
+            st_keep(w0 + k, acc[c], pl);
+            st_keep(x + k, 0.0f, pl);
+            st_keep(p + k, 0.0f, pl);
+            st_keep(s1b + k, 0.0f, pl);
+            lg += (double)v * (double)v;
+            ld += (double)acc[c] * (double)v;
+        }
+        else
+        {
+            const float sk = ld_keep(wc + k, pl) + beta * ld_keep(sp + k, pl);
+            const float rk = ld_keep(rc + k, pl);
+            const float pk = rk + beta * ld_keep(p + k, pl);
+            st_keep(x + k, ld_keep(x + k, pl) + alpha * pk, pl);
+            const float rn = rk - alpha * sk;
+            st_keep(sc + k, sk, pl);
+            st_keep(p + k, pk, pl);
+            st_keep(rn_ + k, rn, pl);
+            st_keep(wn + k, acc[c], pl);
+            lg += (double)rn * (double)rn;
+            ld += (double)acc[c] * (double)rn;
+        }
+    }
+}
+
+// the gathered sources of a phase: the opening reads b (fresh) or r_0; an iteration reads r_k,
+// w_k and s_{k-1}
+__device__ __forceinline__ void sr_sources(const BInst &I, bool init, int cur, bool fresh, const float **gr,
+                                           const float **gw, const float **gs)
+{
+    const float *r0 = static_cast<const float *>(I.r), *r1 = static_cast<const float *>(I.r1);
+    const float *w0 = static_cast<const float *>(I.q), *w1 = static_cast<const float *>(I.w1);
+    const float *s0b = static_cast<const float *>(I.pb), *s1b = static_cast<const float *>(I.s1);
+    *gr = init ? (fresh ? static_cast<const float *>(I.b) : r0) : (cur ? r1 : r0);
+    *gw = cur ? w1 : w0;
+    *gs = cur ? s0b : s1b;
+}
+
+// One slice of a piece by one warp (the flat work list of k_cg_batch_sr).
+template <int D, bool INIT, int UV>
+__device__ __forceinline__ void sr_slice(const BInst &I, int sl, int cur, bool fresh, float alpha, float beta,
+                                         uint64_t pf, uint64_t pl, double &lg, double &ld)
+{
+    constexpr int U = (D == 2) ? UV : 1;
+    const float *gr, *gw, *gs;
+    sr_sources(I, INIT, cur, fresh, &gr, &gw, &gs);
+    float acc[D];
+    const int i = sr_spmv_slice<D, U, INIT>(sl, I, gr, gw, gs, alpha, beta, acc, pf, pl, 0, 1);
+    sr_row<D, INIT>(I, i, acc, cur, fresh, alpha, beta, pl, lg, ld);
+}
+
 // One phase of a member's piece (slices [s0, s1)) in mode 0 (INIT false: iteration k of parity
 // cur) or mode 3/6 (INIT: w_0 = A r_0, the solve's opening; fresh: r_0 = b).  Whole block; with
 // fewer slices than warps several warps share a slice (column split through `red`).  Returns
@@ -878,53 +954,9 @@ __device__ __forceinline__ double sr_phase(const BInst &I, int s0, int s1, int c
 {
     constexpr int U = (D == 2) ? UV : 1;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    float *x = static_cast<float *>(I.x), *p = static_cast<float *>(I.pa);
-    float *r0 = static_cast<float *>(I.r), *r1 = static_cast<float *>(I.r1);
-    float *w0 = static_cast<float *>(I.q), *w1 = static_cast<float *>(I.w1);
-    float *s0b = static_cast<float *>(I.pb), *s1b = static_cast<float *>(I.s1);
-    // this iteration's buffers by parity: r_k, w_k in rc, wc; s_{k-1} in sp; writes s_k to sc,
-    // r_{k+1} to rn_, w_{k+1} to wn
-    float *rc = cur ? r1 : r0, *rn_ = cur ? r0 : r1, *wc = cur ? w1 : w0, *wn = cur ? w0 : w1;
-    float *sc = cur ? s1b : s0b, *sp = cur ? s0b : s1b;
-    // gathered sources: the opening reads b (fresh) or r_0; an iteration reads r_k, w_k, s_{k-1}
-    const float *gr = INIT ? (fresh ? static_cast<const float *>(I.b) : r0) : rc;
-    const float *gw = wc, *gs = sp;
+    const float *gr, *gw, *gs;
+    sr_sources(I, INIT, cur, fresh, &gr, &gw, &gs);
     double lg = 0, ld = 0;
-    auto epilogue = [&](int i, const float *acc) {
-        if (i < 0)
-            return;
-#pragma unroll
-        for (int c = 0; c < D; ++c)
-        {
-            const int64_t k = (int64_t)i * D + c;
-            if (INIT)
-            {
-                const float v = ld_keep(gr + k, pl);
-                if (fresh)
-                    st_keep(r0 + k, v, pl);
-                st_keep(w0 + k, acc[c], pl);
-                st_keep(x + k, 0.0f, pl);
-                st_keep(p + k, 0.0f, pl);
-                st_keep(s1b + k, 0.0f, pl);
-                lg += (double)v * (double)v;
-                ld += (double)acc[c] * (double)v;
-            }
-            else
-            {
-                const float sk = ld_keep(gw + k, pl) + beta * ld_keep(gs + k, pl);
-                const float rk = ld_keep(gr + k, pl);
-                const float pk = rk + beta * ld_keep(p + k, pl);
-                st_keep(x + k, ld_keep(x + k, pl) + alpha * pk, pl);
-                const float rn = rk - alpha * sk;
-                st_keep(sc + k, sk, pl);
-                st_keep(p + k, pk, pl);
-                st_keep(rn_ + k, rn, pl);
-                st_keep(wn + k, acc[c], pl);
-                lg += (double)rn * (double)rn;
-                ld += (double)acc[c] * (double)rn;
-            }
-        }
-    };
     const int ns = s1 - s0;
     if (ns > 0)
     {
@@ -934,7 +966,7 @@ __device__ __forceinline__ double sr_phase(const BInst &I, int s0, int s1, int c
             {
                 float acc[D];
                 const int i = sr_spmv_slice<D, U, INIT>(sl, I, gr, gw, gs, alpha, beta, acc, pf, pl, 0, 1);
-                epilogue(i, acc);
+                sr_row<D, INIT>(I, i, acc, cur, fresh, alpha, beta, pl, lg, ld);
             }
         }
         else
@@ -961,7 +993,7 @@ __device__ __forceinline__ double sr_phase(const BInst &I, int s0, int s1, int c
 #pragma unroll
                     for (int c = 0; c < D; ++c)
                         acc[c] += red[((warp + q) * D + c) * 32 + lane];
-                epilogue(i, acc);
+                sr_row<D, INIT>(I, i, acc, cur, fresh, alpha, beta, pl, lg, ld);
             }
             __syncthreads();
         }
@@ -1121,7 +1153,7 @@ __global__ void __launch_bounds__(kSrThreads<UV>, kCGMinBlocks) k_cg_batch_sr(BA
     BUnion<float> &Un = *reinterpret_cast<BUnion<float> *>(dsm + kBSharedBytes);
     __shared__ double sh[32];
     __shared__ int s_fail;
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31, nw = blockDim.x >> 5;
     if (t == 0)
     {
         s_fail = 0;
@@ -1152,6 +1184,15 @@ __global__ void __launch_bounds__(kSrThreads<UV>, kCGMinBlocks) k_cg_batch_sr(BA
     for (int64_t ph = 0; S.nact > 0; ++ph)
     {
         double *const P0 = a.part + (size_t)(2 * (ph & 1)) * kMaxVirt, *const P1 = P0 + kMaxVirt;
+        // slices of this block's pieces in a CG phase (opening or iteration)
+        int T = 0;
+        for (int k = 0; k < S.np; ++k)
+        {
+            const int md = S.mode[S.act[S.pr_lo + k]];
+            if (md == 0 || md == 3 || md == 6)
+                T += S.ps1[k] - S.ps0[k];
+        }
+        const bool flat = 2 * T > nw && S.np <= kMaxBatch / 2;
         for (int k = 0; k < S.np; ++k)
         {
             const int r = S.pr_lo + k, m = S.act[r], pidx = S.vs[r] + (int)blockIdx.x - S.fb[r];
@@ -1159,9 +1200,14 @@ __global__ void __launch_bounds__(kSrThreads<UV>, kCGMinBlocks) k_cg_batch_sr(BA
             const int md = S.mode[m];
             double g = 0, d = 0;
             if (md == 1)
+            {
                 refine_add<float>(I, S.ps0[k], S.ps1[k]);
-            else if (md == 2)
+                continue;
+            }
+            if (md == 2)
                 g = refine_residual<float>(I, S.ps0[k], S.ps1[k], pf, pl, &d);
+            else if (flat)
+                continue; // dealt below
             else
             {
                 const bool init = md != 0;
@@ -1176,6 +1222,67 @@ __global__ void __launch_bounds__(kSrThreads<UV>, kCGMinBlocks) k_cg_batch_sr(BA
             }
             block_partial_at(g, P0 + pidx, sh);
             block_partial_at(d, P1 + pidx, sh);
+        }
+        if (flat)
+        {
+            // one list of all those slices, dealt round-robin to the warps across the pieces; each
+            // warp leaves one (gamma, delta) pair per piece, summed per piece after one block sync
+            double *wg = Un.wpart, *wd = Un.wpart + (kMaxBatch / 2) * 32;
+            int off = 0;
+            for (int k = 0; k < S.np; ++k)
+            {
+                const int m = S.act[S.pr_lo + k];
+                const int md = S.mode[m];
+                if (md != 0 && md != 3 && md != 6)
+                    continue;
+                const BInst &I = a.inst[m];
+                const int nk = S.ps1[k] - S.ps0[k];
+                const int cur = (int)(S.cit[m] & 1);
+                const float al = (float)S.alpha[m], be = (float)S.beta[m];
+                double lg = 0, ld = 0;
+                for (int q = (warp - off % nw + nw) % nw; q < nk; q += nw)
+                {
+                    const int sl = S.ps0[k] + q;
+                    if (I.dim == 2)
+                    {
+                        if (md == 0)
+                            sr_slice<2, false, UV>(I, sl, cur, false, al, be, pf, pl, lg, ld);
+                        else
+                            sr_slice<2, true, UV>(I, sl, 0, md == 6, 0.0f, 0.0f, pf, pl, lg, ld);
+                    }
+                    else
+                    {
+                        if (md == 0)
+                            sr_slice<3, false, UV>(I, sl, cur, false, al, be, pf, pl, lg, ld);
+                        else
+                            sr_slice<3, true, UV>(I, sl, 0, md == 6, 0.0f, 0.0f, pf, pl, lg, ld);
+                    }
+                }
+                lg = wsum(lg);
+                ld = wsum(ld);
+                if (lane == 0)
+                {
+                    wg[k * 32 + warp] = lg;
+                    wd[k * 32 + warp] = ld;
+                }
+                off += nk;
+            }
+            __syncthreads();
+            for (int k = warp; k < S.np; k += nw)
+            {
+                const int r = S.pr_lo + k;
+                const int md = S.mode[S.act[r]];
+                if (md != 0 && md != 3 && md != 6)
+                    continue;
+                const double tg = wsum(lane < nw ? wg[k * 32 + lane] : 0.0);
+                const double td = wsum(lane < nw ? wd[k * 32 + lane] : 0.0);
+                if (lane == 0)
+                {
+                    const int pidx = S.vs[r] + (int)blockIdx.x - S.fb[r];
+                    P0[pidx] = tg;
+                    P1[pidx] = td;
+                }
+            }
         }
         if (!batch_barrier(a.ctl, epoch, &s_fail))
             return;
