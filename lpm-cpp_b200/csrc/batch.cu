@@ -1325,8 +1325,35 @@ struct BatchCtx
     int device = 0, num_sms = 0, grid = 0;
     int64_t slice = 512; // CG iterations per launch before unfinished solves pause
     size_t smem64 = 0, smem32 = 0; // dynamic shared memory of the two kernel variants
-    int sr = 1; // FP32 inner solves: 1, 2 the single-reduction kernel with 1 or 2 SpMV steps in flight;
-                // 0 the two-reduction kernel (LPMGPU_BATCH_SR)
+    int sr = 1; // FP32 inner solves: 1, 2 the single-reduction kernel with 1 or 2 SpMV steps in flight
+                // (768 or 512 threads a block); 0 the two-reduction kernel (LPMGPU_BATCH_SR fixes it)
+    // The batch's own tuner of that choice: unless LPMGPU_BATCH_SR is set, the first
+    // kTuneLaunches FP32 launches cycle through the three kernels, each launch scored by its
+    // matrix work (iterations x the members' matrix volume) per second of kernel time, and the
+    // best kernel serves every later launch.
+    static constexpr int kTuneLaunches = 9;
+    bool tuning = false;
+    int tune_n = 0, launched_sr = 1;
+    double tune_work[3] = {0, 0, 0}, tune_secs[3] = {0, 0, 0};
+    double last_ms = 0;
+
+    void tune_record(double work)
+    {
+        if (!tuning)
+            return;
+        tune_work[launched_sr] += work;
+        tune_secs[launched_sr] += last_ms * 1e-3;
+        if (++tune_n < kTuneLaunches)
+            return;
+        double best = -1;
+        for (int v = 0; v < 3; ++v)
+            if (tune_secs[v] > 0 && tune_work[v] / tune_secs[v] > best)
+            {
+                best = tune_work[v] / tune_secs[v];
+                sr = v;
+            }
+        tuning = false;
+    }
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_done = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
     std::vector<cudaEvent_t> ev_in; // one per item slot
@@ -1354,6 +1381,7 @@ struct BatchCtx
             sr = env ? std::atoi(env) : 1;
             if (sr < 0 || sr > 2)
                 sr = 1;
+            tuning = env == nullptr;
         }
         if ((e = cudaFuncSetAttribute(k_cg_batch_sr<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32)) !=
                 cudaSuccess ||
@@ -1530,9 +1558,12 @@ struct BatchCtx
         void *args[] = {&a};
         if ((e = cudaEventRecord(ev_t0, stream)) != cudaSuccess)
             return e;
-        e = (fp32 && sr == 1) ? cudaLaunchCooperativeKernel((const void *)k_cg_batch_sr<1>, dim3(grid),
+        static constexpr int kCand[3] = {1, 2, 0};
+        const int use = (fp32 && tuning) ? kCand[tune_n % 3] : sr;
+        launched_sr = use;
+        e = (fp32 && use == 1) ? cudaLaunchCooperativeKernel((const void *)k_cg_batch_sr<1>, dim3(grid),
                                                             dim3(kSrThreads<1>), args, smem32, stream)
-            : (fp32 && sr == 2) ? cudaLaunchCooperativeKernel((const void *)k_cg_batch_sr<2>, dim3(grid),
+            : (fp32 && use == 2) ? cudaLaunchCooperativeKernel((const void *)k_cg_batch_sr<2>, dim3(grid),
                                                               dim3(kSrThreads<2>), args, smem32, stream)
             : fp32 ? cudaLaunchCooperativeKernel((const void *)k_cg_batch<float, float>, dim3(grid), dim3(kBatchThreads<float>),
                                                args, smem32, stream)
@@ -1567,6 +1598,7 @@ struct BatchCtx
         float ms = 0;
         if (cudaEventElapsedTime(&ms, ev_t0, ev_t1) == cudaSuccess)
             kernel_seconds += ms * 1e-3;
+        last_ms = ms;
         timing_pending = false;
     }
 };
@@ -2049,6 +2081,14 @@ struct lpmgpu_batch
             return cuda_status(e, "batched CG");
         ctx.account();
         const bool timeout = ctx.h_ctl->fail != 0;
+        double work = 0;
+        for (size_t q = 0; q < ms.size(); ++q)
+        {
+            const int64_t before = ms[q]->ls_fresh ? 0 : ms[q]->ls_state.it_total;
+            work += (double)(ctx.h_st[q].it_total - before) * (double)ms[q]->cost;
+        }
+        if (fp32 && !timeout)
+            ctx.tune_record(work);
         for (size_t q = 0; q < ms.size(); ++q)
         {
             Member &m = *ms[q];
@@ -2526,6 +2566,8 @@ int32_t lpmgpu_batch_get_stats(const lpmgpu_batch *b, lpmgpu_batch_stats *st)
         return LPMGPU_ERR_INVALID_ARG;
     *st = b->stats;
     st->cg_kernel_seconds = b->kernel_seconds();
+    st->fp32_kernel = b->lanes.empty() ? -1 : b->lanes[0]->c32.sr;
+    st->fp32_tuning = (!b->lanes.empty() && b->lanes[0]->c32.tuning) ? 1 : 0;
     int64_t it = 0, di = 0;
     for (auto &up : b->members)
         if (up)

@@ -95,8 +95,16 @@ def test_batch_fp64_members_match_alone(lanes):
         g.close()
 
 
-@pytest.mark.parametrize("lanes", [1, 2])
-def test_batch_mixed_members_match_fp64_alone(lanes):
+@pytest.mark.parametrize("lanes,kernel", [(1, None), (2, None), (1, "0"), (1, "1"), (1, "2")])
+def test_batch_mixed_members_match_fp64_alone(lanes, kernel, monkeypatch):
+    """Mixed members (FP32 inner solves in FP64 refinement) against FP64 alone, with the batch's
+    own choice of the FP32 kernel (kernel None: its tuner tries the three over the first launches)
+    and with each kernel fixed: 0 the two-reduction CG, 1 and 2 the single-reduction CG with one or
+    two SpMV steps in flight."""
+    if kernel is not None:
+        monkeypatch.setenv("LPMGPU_BATCH_SR", kernel)
+    else:
+        monkeypatch.delenv("LPMGPU_BATCH_SR", raising=False)
     cases = _cases()[:3]
     refs = [_alone(c) for c in cases]
     batch = LPM.Batch()
@@ -110,6 +118,10 @@ def test_batch_mixed_members_match_fp64_alone(lanes):
     for c, g, mid, (ref_state, ref_steps) in zip(cases, gs, mids, refs):
         info = _check_member(c, batch, mid, g, ref_state, ref_steps, MIXED_TOL, compare_counts=False)
         assert info["total"]["refinements"] > 0
+    st = batch.stats()
+    assert st["fp32_kernel"] in (0, 1, 2)
+    if kernel is not None:
+        assert st["fp32_kernel"] == int(kernel) and st["fp32_tuning"] == 0
     batch.close()
     for g in gs:
         g.close()
