@@ -66,7 +66,7 @@ def args_():
     ap.add_argument("--autotune", action="store_true",
                     help="tune the CG grid of the headline problem after the first warm-up step (lpmgpu_autotune)")
     ap.add_argument("--tangent-steps", type=int, default=50, help="load steps of the FCC bar's 50-step path timed")
-    ap.add_argument("--serve-requests", type=int, default=24, help="requests in the serving-stream sample")
+    ap.add_argument("--serve-requests", type=int, default=20, help="requests in the serving-stream sample")
     ap.add_argument("--serve-max-particles", type=float, default=5e5,
                     help="upper end of the log-uniform particle count (the stream's range is 5e3-5e5)")
     return ap.parse_args()
@@ -851,6 +851,9 @@ def serving_leg(lpm, count, nmax, device, world, allreduce, lanes=0):
     import torch
     cfg = importlib.import_module("lpm-cpp_b200.configs")
     reqs = cfg.serving_requests(count=count, n_range=(5e3, nmax))
+    for _, c in reqs:
+        # the headline's Newton tolerance, so that mixed and FP64 results stay within 1e-6
+        c.tol_iter = NEWTON_TOL
     steps_of = lambda c: [c.load_step(s) for s in range(len(c.steps))]  # noqa: E731
 
     # plain FP64, one at a time
@@ -915,7 +918,7 @@ def serving_leg(lpm, count, nmax, device, world, allreduce, lanes=0):
              "dof_iter_per_s": dof_iters / span_plain}
     return {"workload": f"{len(reqs)} requests, Poisson arrivals 200/s (seed {reqs[0][1].meta['seed']}); hex-2D / "
                         f"SC-3D / BCC-3D, N log-uniform 5e3-{nmax:.0e} (the stream's range is 5e3-5e5), "
-                        f"E 50-250 GPa, nu 0.2-0.35, 5-50 steps to "
+                        f"E 50-250 GPa, nu 0.2-0.35, Newton tol {NEWTON_TOL}, 5-50 steps to "
                         f"0.1% strain, elastic or J2; {sum(c.n for _, c in reqs)} particles in total",
             "requests": len(reqs), "particles_range": [int(min(c.n for _, c in reqs)), int(max(c.n for _, c in reqs))],
             "plain_fp64_one_at_a_time": plain, "served_mixed": mixed, "served_fp64": fp64,

@@ -1327,33 +1327,39 @@ struct BatchCtx
     size_t smem64 = 0, smem32 = 0; // dynamic shared memory of the two kernel variants
     int sr = 1; // FP32 inner solves: 1, 2 the single-reduction kernel with 1 or 2 SpMV steps in flight
                 // (768 or 512 threads a block); 0 the two-reduction kernel (LPMGPU_BATCH_SR fixes it)
-    // The batch's own tuner of that choice: unless LPMGPU_BATCH_SR is set, the first
-    // kTuneLaunches FP32 launches cycle through the three kernels, each launch scored by its
-    // matrix work (iterations x the members' matrix volume) per second of kernel time, and the
-    // best kernel serves every later launch.
+    // The batch's own tuner of that choice, per launch size: a launch whose members' FP32 matrices
+    // total under kSmallVolume bytes is bound by the per-iteration floor (barriers and decision
+    // passes), a larger one by the matrix stream, and the best kernel differs between the two.
+    // Unless LPMGPU_BATCH_SR is set, the first kTuneLaunches FP32 launches of each size cycle
+    // through the three kernels, each launch scored by its matrix work (iterations x the members'
+    // matrix volume) per second of kernel time, and the best kernel serves every later launch of
+    // that size.
     static constexpr int kTuneLaunches = 9;
-    bool tuning = false;
-    int tune_n = 0, launched_sr = 1;
-    double tune_work[3] = {0, 0, 0}, tune_secs[3] = {0, 0, 0};
+    static constexpr double kSmallVolume = 64e6;
+    bool tuning[2] = {false, false};
+    int tune_n[2] = {0, 0}, pick[2] = {1, 1}, launched_sr = 1, launched_cls = 1;
+    double tune_work[2][3] = {{0, 0, 0}, {0, 0, 0}}, tune_secs[2][3] = {{0, 0, 0}, {0, 0, 0}};
     double last_ms = 0;
 
     void tune_record(double work)
     {
-        if (!tuning)
+        const int c = launched_cls;
+        if (!tuning[c])
             return;
-        tune_work[launched_sr] += work;
-        tune_secs[launched_sr] += last_ms * 1e-3;
-        if (++tune_n < kTuneLaunches)
+        tune_work[c][launched_sr] += work;
+        tune_secs[c][launched_sr] += last_ms * 1e-3;
+        if (++tune_n[c] < kTuneLaunches)
             return;
         double best = -1;
         for (int v = 0; v < 3; ++v)
-            if (tune_secs[v] > 0 && tune_work[v] / tune_secs[v] > best)
+            if (tune_secs[c][v] > 0 && tune_work[c][v] / tune_secs[c][v] > best)
             {
-                best = tune_work[v] / tune_secs[v];
-                sr = v;
+                best = tune_work[c][v] / tune_secs[c][v];
+                pick[c] = v;
             }
-        tuning = false;
+        tuning[c] = false;
     }
+
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_done = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
     std::vector<cudaEvent_t> ev_in; // one per item slot
@@ -1381,7 +1387,8 @@ struct BatchCtx
             sr = env ? std::atoi(env) : 1;
             if (sr < 0 || sr > 2)
                 sr = 1;
-            tuning = env == nullptr;
+            pick[0] = pick[1] = sr;
+            tuning[0] = tuning[1] = env == nullptr;
         }
         if ((e = cudaFuncSetAttribute(k_cg_batch_sr<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32)) !=
                 cudaSuccess ||
@@ -1559,8 +1566,13 @@ struct BatchCtx
         if ((e = cudaEventRecord(ev_t0, stream)) != cudaSuccess)
             return e;
         static constexpr int kCand[3] = {1, 2, 0};
-        const int use = (fp32 && tuning) ? kCand[tune_n % 3] : sr;
+        double volume = 0;
+        for (int m = 0; m < ni; ++m)
+            volume += 4.0 * (double)h_inst[m].cost;
+        const int cls = volume < kSmallVolume ? 0 : 1;
+        const int use = (fp32 && tuning[cls]) ? kCand[tune_n[cls] % 3] : pick[cls];
         launched_sr = use;
+        launched_cls = cls;
         e = (fp32 && use == 1) ? cudaLaunchCooperativeKernel((const void *)k_cg_batch_sr<1>, dim3(grid),
                                                             dim3(kSrThreads<1>), args, smem32, stream)
             : (fp32 && use == 2) ? cudaLaunchCooperativeKernel((const void *)k_cg_batch_sr<2>, dim3(grid),
@@ -2566,8 +2578,9 @@ int32_t lpmgpu_batch_get_stats(const lpmgpu_batch *b, lpmgpu_batch_stats *st)
         return LPMGPU_ERR_INVALID_ARG;
     *st = b->stats;
     st->cg_kernel_seconds = b->kernel_seconds();
-    st->fp32_kernel = b->lanes.empty() ? -1 : b->lanes[0]->c32.sr;
-    st->fp32_tuning = (!b->lanes.empty() && b->lanes[0]->c32.tuning) ? 1 : 0;
+    st->fp32_kernel = b->lanes.empty() ? -1 : b->lanes[0]->c32.pick[1];
+    st->fp32_kernel_small = b->lanes.empty() ? -1 : b->lanes[0]->c32.pick[0];
+    st->fp32_tuning = (!b->lanes.empty() && (b->lanes[0]->c32.tuning[0] || b->lanes[0]->c32.tuning[1])) ? 1 : 0;
     int64_t it = 0, di = 0;
     for (auto &up : b->members)
         if (up)

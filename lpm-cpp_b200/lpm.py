@@ -181,7 +181,7 @@ class BatchStats(C.Structure):
     _fields_ = [("rounds", C.c_int64), ("cg_launches", C.c_int64), ("members_done", C.c_int64),
                 ("members_failed", C.c_int64), ("cg_iters", C.c_int64), ("dof_iters", C.c_int64),
                 ("seconds", C.c_double), ("cg_kernel_seconds", C.c_double), ("fp32_kernel", C.c_int32),
-                ("fp32_tuning", C.c_int32)]
+                ("fp32_kernel_small", C.c_int32), ("fp32_tuning", C.c_int32), ("pad", C.c_int32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

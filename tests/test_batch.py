@@ -120,8 +120,9 @@ def test_batch_mixed_members_match_fp64_alone(lanes, kernel, monkeypatch):
         assert info["total"]["refinements"] > 0
     st = batch.stats()
     assert st["fp32_kernel"] in (0, 1, 2)
+    assert st["fp32_kernel_small"] in (0, 1, 2)
     if kernel is not None:
-        assert st["fp32_kernel"] == int(kernel) and st["fp32_tuning"] == 0
+        assert st["fp32_kernel"] == st["fp32_kernel_small"] == int(kernel) and st["fp32_tuning"] == 0
     batch.close()
     for g in gs:
         g.close()
