@@ -12,6 +12,7 @@
 //              and returns its memory to the budget.
 // Clients submit, poll, wait and fetch results from any thread.
 #include <algorithm>
+#include <cstdlib>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -73,6 +74,7 @@ struct Request
     int32_t nstatic = 0, cycle_len = 0, ncycles = 0;
     std::vector<double> dndt;
     int64_t est_bytes = 0, bytes = 0;
+    int64_t volume = 0; // bytes its CG streams per iteration (matrix values and block columns)
     lpmgpu_solver *h = nullptr;
     int32_t member = -1;
     lpmgpu_member_info info{};
@@ -139,6 +141,12 @@ struct lpmgpu_server
     int64_t rounds = 0, finished_epoch = 0;
     int64_t slice = -1; // requested CG slice, applied by the worker between rounds (-1: unchanged)
     int32_t lanes = 0;  // requested batch lanes, applied by the worker once no request runs (0: unchanged)
+    // Cap on the running requests' summed per-iteration matrix stream.  Past a few hundred MB the
+    // batched CG already streams at HBM speed; more members running at once only share that
+    // bandwidth, thrash L2 with their Krylov vectors and lengthen every round, so admitted
+    // requests beyond the cap wait (a request that alone exceeds it runs when nothing else does;
+    // smaller ones behind it may go first).  LPMGPU_SERVE_VOLUME_MB sets it.
+    int64_t volume_cap = int64_t(768) << 20, running_volume = 0;
     bool stop = false;
     int32_t worker_status = LPMGPU_OK;
     lpmgpu_batch *batch = nullptr;
@@ -196,6 +204,7 @@ struct lpmgpu_server
             }
             r->h = h;
             r->bytes = sz.device_bytes;
+            r->volume = sz.nnzb * ((int64_t)sz.dim * sz.dim * (r->desc.precision == LPMGPU_MIXED ? 4 : 8) + 4);
             used += r->bytes;
             peak = std::max(peak, used);
             // the description's host arrays were only needed by lpmgpu_create
@@ -227,6 +236,7 @@ struct lpmgpu_server
         std::lock_guard<std::mutex> lk(mu);
         used -= r->bytes;
         running--;
+        running_volume -= r->volume;
         r->t_done = Clock::now();
         if (r->info.state == 1)
         {
@@ -259,7 +269,26 @@ struct lpmgpu_server
                 cv_work.wait(lk, [&] { return stop || !ready.empty() || !live.empty(); });
                 if (stop)
                     break;
-                add.swap(ready);
+                // admitted requests join while the running stream volume has room (in admission
+                // order; a later, smaller one may pass a larger one that does not fit yet)
+                std::vector<Request *> wait;
+                int64_t vol = running_volume;
+                for (Request *r : ready)
+                {
+                    if (live.empty() && add.empty())
+                    {
+                        add.push_back(r);
+                        vol += r->volume;
+                    }
+                    else if (vol + r->volume <= volume_cap)
+                    {
+                        add.push_back(r);
+                        vol += r->volume;
+                    }
+                    else
+                        wait.push_back(r);
+                }
+                ready.swap(wait);
                 sl = slice;
                 slice = -1;
                 if (lanes > 0 && live.empty())
@@ -301,6 +330,7 @@ struct lpmgpu_server
                 r->state = 1;
                 r->t_start = Clock::now();
                 running++;
+                running_volume += r->volume;
                 live.push_back(r);
             }
             if (live.empty())
@@ -325,6 +355,7 @@ struct lpmgpu_server
                     std::lock_guard<std::mutex> lk(mu);
                     used -= r->bytes;
                     running--;
+                    running_volume -= r->volume;
                     r->state = 3;
                     r->status = s;
                     r->t_done = Clock::now();
@@ -381,6 +412,9 @@ int32_t lpmgpu_server_create(int32_t device, int64_t hbm_budget_bytes, lpmgpu_se
     auto *srv = new lpmgpu_server();
     srv->device = device;
     srv->budget = hbm_budget_bytes;
+    if (const char *env = std::getenv("LPMGPU_SERVE_VOLUME_MB"))
+        if (std::atoll(env) > 0)
+            srv->volume_cap = std::atoll(env) << 20;
     srv->batch = b;
     srv->t0 = Clock::now();
     srv->admit_thread = std::thread([srv] { srv->admission(); });
