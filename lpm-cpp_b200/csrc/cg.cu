@@ -29,7 +29,6 @@
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
-#include <mutex>
 #include <string>
 
 #include "cg_device.cuh"
@@ -834,24 +833,18 @@ __global__ void __launch_bounds__(kCGThreads, kCGMinBlocks)
     }
 }
 
-static std::mutex g_noalloc_mu;
-static double *g_noalloc_dev[64] = {nullptr};
-
-// Set-up, once per device, with that device current: the device address of the array.
+// The device address of the array in the current device's context, looked up on every call (the
+// lookup allocates nothing): a cached address would dangle after the host application resets the
+// device or re-creates its context, which reloads the module.
 static cudaError_t noalloc_scratch(int dev, double **out)
 {
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (dev < 0 || dev >= 64)
+    if (dev < 0)
         return cudaErrorInvalidDevice;
-    if (!g_noalloc_dev[dev])
-    {
-        double *ptr = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess)
-            return e;
-        g_noalloc_dev[dev] = ptr;
-    }
-    *out = g_noalloc_dev[dev];
+    double *ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess)
+        return e;
+    *out = ptr;
     return cudaSuccess;
 }
 
