@@ -1318,7 +1318,17 @@ struct BatchItem
     BState resume;
     bool refine;    // FP32 item: the FP64 refinement around it runs in the launch
     double stop64;  // its outer squared-norm target
+    int resume_kernel; // FP32 kernel (BatchCtx::launched_sr) that ran the paused solve's last launch
 };
+
+// The two FP32 kernel families keep different Krylov states (the single-reduction kernels, 1 and
+// 2, keep r, w, s by parity and the Chronopoulos-Gear alpha, beta; the two-reduction kernel, 0,
+// keeps p by parity and the textbook alpha, beta), so a paused inner solve resumes only in its own
+// family.
+inline int fp32_family(int kernel)
+{
+    return kernel == 0 ? 0 : 1;
+}
 
 struct BatchCtx
 {
@@ -1542,6 +1552,27 @@ struct BatchCtx
                 h_st[m].status &= ~int64_t(8);
             }
         }
+        static constexpr int kCand[3] = {1, 2, 0};
+        double volume = 0;
+        for (int m = 0; m < ni; ++m)
+            volume += 4.0 * (double)h_inst[m].cost;
+        const int cls = volume < kSmallVolume ? 0 : 1;
+        const int use = (fp32 && tuning[cls]) ? kCand[tune_n[cls] % 3] : pick[cls];
+        launched_sr = use;
+        launched_cls = cls;
+        if (fp32)
+            for (int m = 0; m < ni; ++m)
+            {
+                // a paused inner solve of the other kernel family ends here, as if it had met its
+                // stop: x64 += x32, the true residual, and a fresh inner solve in this kernel
+                BState &B = h_st[m];
+                if (items[m].fresh || !items[m].refine || B.mode != 0 ||
+                    fp32_family(items[m].resume_kernel) == fp32_family(use))
+                    continue;
+                B.last_inner = B.it > 0 ? B.it : 1;
+                B.refs += 1;
+                B.mode = 1;
+            }
         std::memset(h_ctl, 0, sizeof(BCtl));
         h_ctl->nact = ni;
         for (int m = 0; m < ni; ++m)
@@ -1565,14 +1596,6 @@ struct BatchCtx
         void *args[] = {&a};
         if ((e = cudaEventRecord(ev_t0, stream)) != cudaSuccess)
             return e;
-        static constexpr int kCand[3] = {1, 2, 0};
-        double volume = 0;
-        for (int m = 0; m < ni; ++m)
-            volume += 4.0 * (double)h_inst[m].cost;
-        const int cls = volume < kSmallVolume ? 0 : 1;
-        const int use = (fp32 && tuning[cls]) ? kCand[tune_n[cls] % 3] : pick[cls];
-        launched_sr = use;
-        launched_cls = cls;
         e = (fp32 && use == 1) ? cudaLaunchCooperativeKernel((const void *)k_cg_batch_sr<1>, dim3(grid),
                                                             dim3(kSrThreads<1>), args, smem32, stream)
             : (fp32 && use == 2) ? cudaLaunchCooperativeKernel((const void *)k_cg_batch_sr<2>, dim3(grid),
@@ -1682,6 +1705,7 @@ struct Member
     // the CG in progress (it may span several launches) and the mixed-precision refinement
     bool ls_fresh = true;
     BState ls_state{};
+    int ls_kernel = 1; // the FP32 kernel of the paused solve's last launch
     double ir_stop = 0, ir_rr = 0;
     // fatigue members (SolverFatigue, include/solver_fatigue.h): steps [0, nstatic) run as
     // solveProblemStatic's steps, the rest as cycle steps; cycle_end[s] = (closes a cycle, dN/dt)
@@ -2072,7 +2096,8 @@ struct lpmgpu_batch
                          fp32 ? 0.25 * m->ir_stop : -1.0,
                          p.desc.cg_maxit > 0 ? p.desc.cg_maxit : ndof,
                          m->ls_fresh,  m->ls_state,
-                         fp32,         m->ir_stop};
+                         fp32,         m->ir_stop,
+                         m->ls_kernel};
             items.push_back(it);
         }
         cudaError_t e = ctx.launch(items);
@@ -2113,6 +2138,7 @@ struct lpmgpu_batch
             m.dof_iters += done_now * (int64_t)p.n * p.dim;
             p.ctr.cg_iters += done_now;
             m.ls_state = S;
+            m.ls_kernel = ctx.launched_sr;
             if (timeout)
             {
                 set_last_error("a device-side barrier wait timed out in the batched CG kernel");
