@@ -394,6 +394,7 @@ typedef struct
     int32_t fp32_kernel_small;   /* the same for smaller launches */
     int32_t fp32_tuning;         /* 1 while the tuner is still trying the kernels */
     int32_t pad;
+    int64_t solo_solves;         /* linear solves of solo members (lpmgpu_batch_set_solo_bytes) */
 } lpmgpu_batch_stats;
 
 int32_t lpmgpu_batch_create(int32_t device, lpmgpu_batch **out);
@@ -433,6 +434,13 @@ int32_t lpmgpu_batch_set_slice(lpmgpu_batch *b, int64_t iterations);
  * the default is 1 (LPMGPU_BATCH_LANES in the environment sets a new batch's count).  No
  * counterpart in the reference. */
 int32_t lpmgpu_batch_set_lanes(lpmgpu_batch *b, int32_t lanes);
+/* Solo members: a member whose CG streams at least `bytes` of matrix per iteration (block values
+ * in its CG precision plus block columns) saturates HBM by itself, so batching it with others
+ * gains nothing; its linear solves run alone through the single-problem persistent CG (the path
+ * of lpmgpu_solve_linear), one at a time between the batched launches, and the rest of its load
+ * path stays in the batch's rounds.  Applies to members added afterwards; 0 = no solo members.
+ * Default 192 MB.  No counterpart in the reference. */
+int32_t lpmgpu_batch_set_solo_bytes(lpmgpu_batch *b, int64_t bytes);
 
 /* ---- Serving: LPM solves submitted while others run (continuous batching).  A request is a
  * problem description plus its load path (both copied at submit).  An admission thread builds a
@@ -475,6 +483,8 @@ int32_t lpmgpu_server_destroy(lpmgpu_server *s);
 int32_t lpmgpu_server_set_slice(lpmgpu_server *s, int64_t iterations);
 /* lpmgpu_batch_set_lanes for the server's batch, applied once no request is running */
 int32_t lpmgpu_server_set_lanes(lpmgpu_server *s, int32_t lanes);
+/* lpmgpu_batch_set_solo_bytes for the server's batch, for requests that join it afterwards */
+int32_t lpmgpu_server_set_solo_bytes(lpmgpu_server *s, int64_t bytes);
 int32_t lpmgpu_server_submit(lpmgpu_server *s, const lpmgpu_desc *d, const lpmgpu_load_step *steps, int32_t nsteps,
                              int64_t *request_id);
 /* A fatigue request: the problem and a SolverFatigue run as lpmgpu_batch_add_fatigue takes it

@@ -50,6 +50,7 @@ constexpr int kMaxStage = 1024 + kMaxBatch;          // virtual blocks a launch 
 constexpr int kMaxMembers = 4096;                    // running members of one batch (launched in groups
                                                      // of at most kMaxBatch)
 constexpr int kDefaultLanes = 1;                     // lanes of a new batch (LPMGPU_BATCH_LANES overrides)
+constexpr int64_t kDefaultSoloBytes = 192000000;      // per-iteration matrix stream of a solo member
 
 struct BInst
 {
@@ -1341,9 +1342,10 @@ struct BatchCtx
     // total under kSmallVolume bytes is bound by the per-iteration floor (barriers and decision
     // passes), a larger one by the matrix stream, and the best kernel differs between the two.
     // Unless LPMGPU_BATCH_SR is set, the first kTuneLaunches FP32 launches of each size cycle
-    // through the three kernels, each launch scored by its matrix work (iterations x the members'
-    // matrix volume) per second of kernel time, and the best kernel serves every later launch of
-    // that size.
+    // through the three kernels and the best kernel serves every later launch of that size.  A
+    // large launch is scored by its matrix work (iterations x the members' matrix volume) per
+    // second of kernel time; a small one, whose time is its iterations times the floor whatever the
+    // members' sizes, by the iterations of its longest solve per second.
     static constexpr int kTuneLaunches = 9;
     static constexpr double kSmallVolume = 64e6;
     bool tuning[2] = {false, false};
@@ -1351,11 +1353,13 @@ struct BatchCtx
     double tune_work[2][3] = {{0, 0, 0}, {0, 0, 0}}, tune_secs[2][3] = {{0, 0, 0}, {0, 0, 0}};
     double last_ms = 0;
 
-    void tune_record(double work)
+    void tune_record(double work, double phases)
     {
         const int c = launched_cls;
         if (!tuning[c])
             return;
+        if (c == 0)
+            work = phases;
         tune_work[c][launched_sr] += work;
         tune_secs[c][launched_sr] += last_ms * 1e-3;
         if (++tune_n[c] < kTuneLaunches)
@@ -1715,6 +1719,9 @@ struct Member
     // the lane that solves this member's linear systems, and the member's weight in its balance
     int lane = 0;
     int64_t cost = 0;
+    // solo: the member's linear solves run alone through the single-problem CG (solo_solves)
+    bool solo = false;
+    int64_t lane_cost() const { return solo ? 0 : cost; }
 };
 
 // A lane: a share of the SMs with its own batched CG launches (FP64 members, then the FP32 inner
@@ -1745,6 +1752,7 @@ struct lpmgpu_batch
 {
     int device = 0;
     int64_t slice = 512;
+    int64_t solo_bytes = kDefaultSoloBytes;
     std::vector<std::unique_ptr<Lane>> lanes;
     std::vector<std::unique_ptr<Member>> members; // index = member id; removed -> null
     lpmgpu_batch_stats stats{};
@@ -1805,7 +1813,7 @@ struct lpmgpu_batch
         m.pending = false;
         m.t_done = std::chrono::steady_clock::now();
         stats.members_failed++;
-        lanes[m.lane]->cost -= m.cost;
+        lanes[m.lane]->cost -= m.lane_cost();
         return LPMGPU_OK;
     }
 
@@ -1816,7 +1824,7 @@ struct lpmgpu_batch
         m.pending = false;
         m.t_done = std::chrono::steady_clock::now();
         stats.members_done++;
-        lanes[m.lane]->cost -= m.cost;
+        lanes[m.lane]->cost -= m.lane_cost();
     }
 
     double kernel_seconds() const
@@ -1987,9 +1995,9 @@ struct lpmgpu_batch
             if (e0 != cudaSuccess)
                 return fail_member(m, cuda_status(e0, "batch tangent assembly"));
         }
-        if (p.desc.precision != LPMGPU_MIXED)
+        if (p.desc.precision != LPMGPU_MIXED || m.solo)
         {
-            m.ph = Ph::NeedCG;
+            m.ph = Ph::NeedCG; // a solo member's solve sets up its own refinement
             return LPMGPU_OK;
         }
         m.ir_rr = p.scal_host->res_sq;
@@ -2119,13 +2127,15 @@ struct lpmgpu_batch
         ctx.account();
         const bool timeout = ctx.h_ctl->fail != 0;
         double work = 0;
+        int64_t phases = 0;
         for (size_t q = 0; q < ms.size(); ++q)
         {
             const int64_t before = ms[q]->ls_fresh ? 0 : ms[q]->ls_state.it_total;
             work += (double)(ctx.h_st[q].it_total - before) * (double)ms[q]->cost;
+            phases = std::max(phases, ctx.h_st[q].it_total - before);
         }
         if (fp32 && !timeout)
-            ctx.tune_record(work);
+            ctx.tune_record(work, (double)phases);
         for (size_t q = 0; q < ms.size(); ++q)
         {
             Member &m = *ms[q];
@@ -2164,6 +2174,58 @@ struct lpmgpu_batch
         return LPMGPU_OK;
     }
 
+    // The linear solves of the solo members waiting for one, each through the single-problem
+    // persistent CG (solve_linear: FP64, or FP32 inner solves in FP64 refinement, on the
+    // problem's own stream), one at a time with no batched launch in flight, so that every
+    // cooperative launch has the GPU to itself; then each one's Newton update is enqueued.
+    int32_t solo_solves(bool *ran)
+    {
+        *ran = false;
+        bool any = false;
+        for (auto &up : members)
+            if (up && up->solo && up->ph == Ph::NeedCG)
+                any = true;
+        if (!any)
+            return LPMGPU_OK;
+        for (auto &L : lanes)
+            if (L->inflight)
+            {
+                const int32_t r = complete_lane(*L);
+                if (r != LPMGPU_OK)
+                    return r;
+            }
+        for (auto &up : members)
+        {
+            if (!up || !up->solo || up->ph != Ph::NeedCG)
+                continue;
+            Member &m = *up;
+            Problem &p = P(m);
+            cudaSetDevice(p.device);
+            CGResult r;
+            const cudaError_t e = solve_linear(p, r);
+            *ran = true;
+            stats.solo_solves++;
+            if (e != cudaSuccess)
+            {
+                fail_member(m, cuda_status(e, "solo linear solve"));
+                continue;
+            }
+            if (r.timeout)
+            {
+                set_last_error("a device-side barrier wait timed out in the CG kernel");
+                fail_member(m, LPMGPU_ERR_TIMEOUT);
+                continue;
+            }
+            m.cur.cg_iters += r.iters;
+            m.cur.cg_maxit_hits += r.maxit_hits;
+            m.cur.refinements += r.refinements;
+            m.dof_iters += r.iters * (int64_t)p.n * p.dim;
+            round_max_it = std::max(round_max_it, r.iters);
+            finish_linear(m);
+        }
+        return LPMGPU_OK;
+    }
+
     // A lane's launches: the FP64 members waiting for a CG, then the FP32 inner solves of its
     // mixed members (at most kMaxBatch of each per launch; the rest wait for the next one).
     int32_t launch_lane(int l)
@@ -2172,7 +2234,7 @@ struct lpmgpu_batch
         L.g64.clear();
         L.g32.clear();
         for (auto &up : members)
-            if (up && up->lane == l && up->ph == Ph::NeedCG)
+            if (up && up->lane == l && up->ph == Ph::NeedCG && !up->solo)
             {
                 auto &g = P(*up).desc.precision == LPMGPU_MIXED ? L.g32 : L.g64;
                 if ((int)g.size() < kMaxBatch)
@@ -2260,6 +2322,13 @@ struct lpmgpu_batch
                     return r;
                 progressed = true;
             }
+        {
+            bool ran = false;
+            const int32_t r = solo_solves(&ran);
+            if (r != LPMGPU_OK)
+                return r;
+            progressed = progressed || ran;
+        }
         int launched = 0;
         for (int l = 0; l < (int)lanes.size(); ++l)
         {
@@ -2431,18 +2500,20 @@ static int32_t push_member(lpmgpu_batch *b, std::unique_ptr<Member> m, int32_t *
     // the lane with the least matrix volume among its running members
     const Problem &p = m->h->p;
     m->cost = p.nsb * (p.dim * p.dim + 1);
+    const int64_t stream_bytes = p.nsb * ((int64_t)p.dim * p.dim * (p.desc.precision == LPMGPU_MIXED ? 4 : 8) + 4);
+    m->solo = b->solo_bytes > 0 && stream_bytes >= b->solo_bytes;
     int best = 0;
     for (int l = 1; l < (int)b->lanes.size(); ++l)
         if (b->lanes[l]->cost < b->lanes[best]->cost)
             best = l;
     m->lane = best;
-    b->lanes[best]->cost += m->cost;
+    b->lanes[best]->cost += m->lane_cost();
     if (m->steps.empty())
     {
         m->ph = Ph::Done;
         m->t_done = m->t_add;
         b->stats.members_done++;
-        b->lanes[best]->cost -= m->cost;
+        b->lanes[best]->cost -= m->lane_cost();
     }
     b->members.push_back(std::move(m));
     if (member)
@@ -2595,6 +2666,14 @@ int32_t lpmgpu_batch_set_slice(lpmgpu_batch *b, int64_t iterations)
     b->slice = iterations;
     for (auto &L : b->lanes)
         L->c64.slice = L->c32.slice = iterations;
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_batch_set_solo_bytes(lpmgpu_batch *b, int64_t bytes)
+{
+    if (!b || bytes < 0)
+        return LPMGPU_ERR_INVALID_ARG;
+    b->solo_bytes = bytes;
     return LPMGPU_OK;
 }
 

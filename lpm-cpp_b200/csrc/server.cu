@@ -75,6 +75,7 @@ struct Request
     std::vector<double> dndt;
     int64_t est_bytes = 0, bytes = 0;
     int64_t volume = 0; // bytes its CG streams per iteration (matrix values and block columns)
+    int64_t counted = 0; // its share of the running volume (0 for a solo request)
     lpmgpu_solver *h = nullptr;
     int32_t member = -1;
     lpmgpu_member_info info{};
@@ -147,6 +148,13 @@ struct lpmgpu_server
     // requests beyond the cap wait (a request that alone exceeds it runs when nothing else does;
     // smaller ones behind it may go first).  LPMGPU_SERVE_VOLUME_MB sets it.
     int64_t volume_cap = int64_t(768) << 20, running_volume = 0;
+    // Solo requests (lpmgpu_batch_set_solo_bytes) solve alone between the batched launches, so
+    // they do not count against the cap.  solo_request: a new value for the worker to apply.
+    int64_t solo_bytes = 192000000, solo_request = -1;
+    int64_t counted_volume(const Request *r) const
+    {
+        return (solo_bytes > 0 && r->volume >= solo_bytes) ? 0 : r->volume;
+    }
     bool stop = false;
     int32_t worker_status = LPMGPU_OK;
     lpmgpu_batch *batch = nullptr;
@@ -236,7 +244,7 @@ struct lpmgpu_server
         std::lock_guard<std::mutex> lk(mu);
         used -= r->bytes;
         running--;
-        running_volume -= r->volume;
+        running_volume -= r->counted;
         r->t_done = Clock::now();
         if (r->info.state == 1)
         {
@@ -271,19 +279,21 @@ struct lpmgpu_server
                     break;
                 // admitted requests join while the running stream volume has room (in admission
                 // order; a later, smaller one may pass a larger one that does not fit yet)
+                if (solo_request >= 0)
+                {
+                    solo_bytes = solo_request;
+                    solo_request = -1;
+                    lpmgpu_batch_set_solo_bytes(batch, solo_bytes);
+                }
                 std::vector<Request *> wait;
                 int64_t vol = running_volume;
                 for (Request *r : ready)
                 {
-                    if (live.empty() && add.empty())
+                    const int64_t v = counted_volume(r);
+                    if ((live.empty() && add.empty()) || vol + v <= volume_cap)
                     {
                         add.push_back(r);
-                        vol += r->volume;
-                    }
-                    else if (vol + r->volume <= volume_cap)
-                    {
-                        add.push_back(r);
-                        vol += r->volume;
+                        vol += v;
                     }
                     else
                         wait.push_back(r);
@@ -330,7 +340,8 @@ struct lpmgpu_server
                 r->state = 1;
                 r->t_start = Clock::now();
                 running++;
-                running_volume += r->volume;
+                r->counted = counted_volume(r);
+                running_volume += r->counted;
                 live.push_back(r);
             }
             if (live.empty())
@@ -355,7 +366,7 @@ struct lpmgpu_server
                     std::lock_guard<std::mutex> lk(mu);
                     used -= r->bytes;
                     running--;
-                    running_volume -= r->volume;
+                    running_volume -= r->counted;
                     r->state = 3;
                     r->status = s;
                     r->t_done = Clock::now();
@@ -364,6 +375,8 @@ struct lpmgpu_server
                 }
                 live.clear();
                 lpmgpu_batch_create(device, &batch);
+                if (batch)
+                    lpmgpu_batch_set_solo_bytes(batch, solo_bytes);
                 cv_done.notify_all();
                 cv_admit.notify_all();
                 if (!batch)
@@ -460,6 +473,16 @@ int32_t lpmgpu_server_set_lanes(lpmgpu_server *s, int32_t lanes)
         return LPMGPU_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(s->mu);
     s->lanes = lanes; // applied by the worker once no request is running
+    s->cv_work.notify_all();
+    return LPMGPU_OK;
+}
+
+int32_t lpmgpu_server_set_solo_bytes(lpmgpu_server *s, int64_t bytes)
+{
+    if (!s || bytes < 0)
+        return LPMGPU_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->solo_request = bytes; // applied by the worker before its next admissions
     s->cv_work.notify_all();
     return LPMGPU_OK;
 }

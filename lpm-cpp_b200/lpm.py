@@ -181,7 +181,8 @@ class BatchStats(C.Structure):
     _fields_ = [("rounds", C.c_int64), ("cg_launches", C.c_int64), ("members_done", C.c_int64),
                 ("members_failed", C.c_int64), ("cg_iters", C.c_int64), ("dof_iters", C.c_int64),
                 ("seconds", C.c_double), ("cg_kernel_seconds", C.c_double), ("fp32_kernel", C.c_int32),
-                ("fp32_kernel_small", C.c_int32), ("fp32_tuning", C.c_int32), ("pad", C.c_int32)]
+                ("fp32_kernel_small", C.c_int32), ("fp32_tuning", C.c_int32), ("pad", C.c_int32),
+                ("solo_solves", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -205,8 +206,8 @@ EXPORTS = [
     "lpmgpu_batch_create", "lpmgpu_batch_destroy", "lpmgpu_batch_add", "lpmgpu_batch_add_fatigue",
     "lpmgpu_batch_round", "lpmgpu_batch_run",
     "lpmgpu_batch_member", "lpmgpu_batch_member_steps", "lpmgpu_batch_remove", "lpmgpu_batch_get_stats",
-    "lpmgpu_batch_set_slice", "lpmgpu_batch_set_lanes",
-    "lpmgpu_estimate_bytes", "lpmgpu_server_create", "lpmgpu_server_destroy", "lpmgpu_server_set_slice", "lpmgpu_server_set_lanes", "lpmgpu_server_submit",
+    "lpmgpu_batch_set_slice", "lpmgpu_batch_set_lanes", "lpmgpu_batch_set_solo_bytes",
+    "lpmgpu_estimate_bytes", "lpmgpu_server_create", "lpmgpu_server_destroy", "lpmgpu_server_set_slice", "lpmgpu_server_set_lanes", "lpmgpu_server_set_solo_bytes", "lpmgpu_server_submit",
     "lpmgpu_server_submit_fatigue",
     "lpmgpu_server_poll", "lpmgpu_server_wait", "lpmgpu_server_result", "lpmgpu_server_get_stats",
 ]
@@ -277,11 +278,13 @@ def lib():
         "lpmgpu_batch_get_stats": (C.c_int32, [vp, C.POINTER(BatchStats)]),
         "lpmgpu_batch_set_slice": (C.c_int32, [vp, C.c_int64]),
         "lpmgpu_batch_set_lanes": (C.c_int32, [vp, C.c_int32]),
+        "lpmgpu_batch_set_solo_bytes": (C.c_int32, [vp, C.c_int64]),
         "lpmgpu_estimate_bytes": (C.c_int32, [C.POINTER(Desc), lp]),
         "lpmgpu_server_create": (C.c_int32, [C.c_int32, C.c_int64, C.POINTER(vp)]),
         "lpmgpu_server_destroy": (C.c_int32, [vp]),
         "lpmgpu_server_set_slice": (C.c_int32, [vp, C.c_int64]),
         "lpmgpu_server_set_lanes": (C.c_int32, [vp, C.c_int32]),
+        "lpmgpu_server_set_solo_bytes": (C.c_int32, [vp, C.c_int64]),
         "lpmgpu_server_submit": (C.c_int32, [vp, C.POINTER(Desc), C.POINTER(CLoadStep), C.c_int32, lp]),
         "lpmgpu_server_submit_fatigue": (C.c_int32, [vp, C.POINTER(Desc), C.POINTER(CLoadStep), C.c_int32,
                                                      C.POINTER(CLoadStep), C.c_int32, C.c_int32, dp, lp]),
@@ -978,6 +981,12 @@ class Batch:
         (lpmgpu_batch_set_lanes); only while no member is running."""
         _check(lib().lpmgpu_batch_set_lanes(self._h, int(lanes)), "lpmgpu_batch_set_lanes")
 
+    def set_solo_bytes(self, nbytes: int):
+        """Members added afterwards whose CG streams at least `nbytes` of matrix per iteration
+        solve their linear systems alone through the single-problem CG, between the batched
+        launches (lpmgpu_batch_set_solo_bytes); 0 = none."""
+        _check(lib().lpmgpu_batch_set_solo_bytes(self._h, int(nbytes)), "lpmgpu_batch_set_solo_bytes")
+
     def round(self) -> int:
         running = C.c_int32(0)
         _check(lib().lpmgpu_batch_round(self._h, C.byref(running)), "lpmgpu_batch_round")
@@ -1047,6 +1056,10 @@ class Server:
     def set_lanes(self, lanes: int):
         """lpmgpu_server_set_lanes: the batch's lanes, applied once no request is running."""
         _check(lib().lpmgpu_server_set_lanes(self._h, int(lanes)), "lpmgpu_server_set_lanes")
+
+    def set_solo_bytes(self, nbytes: int):
+        """lpmgpu_server_set_solo_bytes: the batch's solo threshold for requests joining afterwards."""
+        _check(lib().lpmgpu_server_set_solo_bytes(self._h, int(nbytes)), "lpmgpu_server_set_solo_bytes")
 
     def submit(self, ass: Assembly, steps: Sequence[LoadStep], undamaged_pt_type=-1, max_iter=30, tol_iter=1e-5,
                precision: Precision = Precision.FP64, cg_rtol=1e-12, cg_atol=1e-12, cg_maxit=0,

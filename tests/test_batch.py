@@ -189,6 +189,34 @@ def test_batch_paused_solves_resume(precision, tol, monkeypatch):
 
 
 @pytest.mark.parametrize("precision,tol", [(0, FP64_TOL), (1, MIXED_TOL)])
+def test_batch_solo_members_match_alone(precision, tol):
+    """Solo members (lpmgpu_batch_set_solo_bytes: those whose CG streams at least that many bytes
+    per iteration) solve their linear systems alone through the single-problem CG between the
+    batched launches, while the other members share the launches.  Every member matches its twin
+    alone in the same precision; an FP64 solo member takes exactly the alone path's steps, so it
+    matches bit for bit."""
+    cases = _cases()
+    refs = [_alone(c, precision=precision) for c in cases]
+    batch = LPM.Batch()
+    gs, mids = [], []
+    for k, c in enumerate(cases):
+        batch.set_solo_bytes(1 if k % 2 == 0 else 0)  # members 0, 2, 4 solo
+        g = gpu_problem(c, precision=precision, **TIGHT)
+        gs.append(g)
+        mids.append(batch.add(g, [c.load_step(s) for s in range(len(c.steps))]))
+    batch.run()
+    for k, (c, g, mid, (ref_state, ref_steps)) in enumerate(zip(cases, gs, mids, refs)):
+        _check_member(c, batch, mid, g, ref_state, ref_steps, tol, compare_counts=(precision == 0))
+        if precision == 0 and k % 2 == 0:
+            assert np.array_equal(g.state()["xyz"], ref_state["xyz"]), c.name
+    st = batch.stats()
+    assert st["solo_solves"] > 0 and st["cg_launches"] > 0
+    batch.close()
+    for g in gs:
+        g.close()
+
+
+@pytest.mark.parametrize("precision,tol", [(0, FP64_TOL), (1, MIXED_TOL)])
 def test_batch_tangent_members_match_alone(precision, tol):
     """Tangent-mode members (K re-assembled before every Newton solve) in a batch give the
     results they give alone."""

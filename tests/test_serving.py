@@ -48,10 +48,15 @@ def _submit(srv, case, precision):
                       **TIGHT)
 
 
-def test_requests_submitted_while_others_run_match_alone():
+@pytest.mark.parametrize("solo", [False, True])
+def test_requests_submitted_while_others_run_match_alone(solo):
+    """solo: every request solves its linear systems alone through the single-problem CG between
+    the batched launches (lpmgpu_server_set_solo_bytes(1)), as the large requests of a stream do."""
     reqs = _requests()
     refs = [_alone(c) for c, _ in reqs]
     srv = LPM.Server()
+    if solo:
+        srv.set_solo_bytes(1)
     ids = [_submit(srv, c, p) for c, p in reqs[:3]]
     # the second wave arrives once the first is on the GPU
     t0 = time.time()
