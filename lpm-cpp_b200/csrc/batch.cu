@@ -2322,12 +2322,15 @@ struct lpmgpu_batch
                     return r;
                 progressed = true;
             }
+        double solo_ms = 0;
         {
+            const auto t_solo = std::chrono::steady_clock::now();
             bool ran = false;
             const int32_t r = solo_solves(&ran);
             if (r != LPMGPU_OK)
                 return r;
             progressed = progressed || ran;
+            solo_ms = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_solo).count() * 1e3;
         }
         int launched = 0;
         for (int l = 0; l < (int)lanes.size(); ++l)
@@ -2388,11 +2391,11 @@ struct lpmgpu_batch
                 infl += L->inflight ? 1 : 0;
             std::fprintf(stderr,
                          "lpmgpu batch round %lld: lanes in flight %d/%zu launches=%lld max_it=%lld kernel_ms=%.3f "
-                         "round_ms=%.3f phases(start,nf,n,cg,dmg,done,fail)=%d,%d,%d,%d,%d,%d,%d\n",
+                         "round_ms=%.3f solo_ms=%.3f phases(start,nf,n,cg,dmg,done,fail)=%d,%d,%d,%d,%d,%d,%d\n",
                          (long long)stats.rounds, infl, lanes.size(), (long long)(stats.cg_launches - l0),
                          (long long)round_max_it, (kernel_seconds() - k0) * 1e3,
                          std::chrono::duration<double>(std::chrono::steady_clock::now() - t_round).count() * 1e3,
-                         nph[0], nph[1], nph[2], nph[3], nph[4], nph[5], nph[6]);
+                         solo_ms, nph[0], nph[1], nph[2], nph[3], nph[4], nph[5], nph[6]);
         }
         return LPMGPU_OK;
     }
