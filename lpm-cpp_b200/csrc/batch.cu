@@ -38,6 +38,7 @@
 #include <string>
 #include <vector>
 
+#include "bulk_copy.cuh"
 #include "cg_device.cuh"
 
 namespace lpm
@@ -945,6 +946,288 @@ __device__ __forceinline__ void sr_slice(const BInst &I, int sl, int cur, bool f
     sr_row<D, INIT>(I, i, acc, cur, fresh, alpha, beta, pl, lg, ld);
 }
 
+// ---- the bulk-copy-fed SpMV of the single-reduction kernel (kernel 3)
+//
+// In a flat phase each warp walks its slices of a piece; the register-fed SpMV waits on the
+// matrix loads of every step (one DRAM latency per 2 x 2 step pair), which held the 64-plate
+// batch at about a quarter of HBM bandwidth.  Here the warp's lane 0 streams its slices' block
+// values and columns into two shared-memory chunk buffers with bulk asynchronous copies, two
+// chunks ahead, each completed on its own mbarrier; the lanes read values and columns from shared
+// memory and only the vector gathers (mostly L1/L2 hits) remain on the critical path.  A chunk is
+// kPipeSlots<D> block slots of one slice: D = 2: 8 x (4 values + 1 column) x 128 bytes; D = 3:
+// 4 x (9 + 1) x 128 bytes; both about 5 KB per buffer.  Per warp the region holds the two value
+// buffers, the two column buffers and the two mbarriers.
+template <int D>
+constexpr int kPipeSlots = D == 2 ? 8 : 4;
+// the FP64 true residual of a refinement streams K64: half the slots per chunk in the same bytes
+template <int D>
+constexpr int kPipeSlots64 = kPipeSlots<D> / 2;
+template <int D>
+constexpr int kPipeValBytes = kPipeSlots<D> * D * D * kSlice * 4; // one value buffer
+constexpr int kPipeBarOff = 10240;   // the two mbarriers, after the buffers of either dimension
+constexpr int kPipeWarpBytes = 10368; // per warp, a multiple of 128
+static_assert(2 * kPipeValBytes<2> + 2 * kPipeSlots<2> * kSlice * 4 == kPipeBarOff, "2D buffers");
+static_assert(2 * kPipeValBytes<3> + 2 * kPipeSlots<3> * kSlice * 4 == kPipeBarOff, "3D buffers");
+constexpr int kSrPipeThreads = 384;
+
+struct SrPipe
+{
+    unsigned char *base; // this warp's region
+    uint32_t n;          // chunks issued so far by this warp: chunk m uses buffer m & 1, phase m >> 1
+    bool ok;             // false after a wait ran out of time
+};
+
+template <typename V, int D>
+__device__ __forceinline__ V *pipe_vals(const SrPipe &P, uint32_t m)
+{
+    return reinterpret_cast<V *>(P.base + (m & 1) * kPipeValBytes<D>);
+}
+template <int D>
+__device__ __forceinline__ int *pipe_cols(const SrPipe &P, uint32_t m)
+{
+    return reinterpret_cast<int *>(P.base + 2 * kPipeValBytes<D>) + (m & 1) * kPipeSlots<D> * kSlice;
+}
+__device__ __forceinline__ uint64_t *pipe_bar(const SrPipe &P, uint32_t m)
+{
+    return reinterpret_cast<uint64_t *>(P.base + kPipeBarOff) + (m & 1);
+}
+
+// Waits for chunk m's copies (whole warp).  When the wait runs out of time: a bounded wait for the
+// warp's later copies still in flight, P.ok = false, and false.
+__device__ __forceinline__ bool pipe_wait(SrPipe &P, uint32_t m)
+{
+    const bool ok = mbar_wait_bounded(pipe_bar(P, m), (m >> 1) & 1, kBarrierTimeoutNs);
+    if (__all_sync(0xffffffffu, ok))
+        return true;
+    for (uint32_t q = m + 1; q < P.n; ++q)
+        mbar_wait_bounded(pipe_bar(P, q), (q >> 1) & 1, kBarrierTimeoutNs / 4);
+    P.ok = false;
+    return false;
+}
+
+// The issue cursor over a warp's chunks: slices s, s + step, ... < end, chunks of each slice.
+struct SrCursor
+{
+    int sl, step, end, c0, wd;
+    int64_t off;
+};
+
+__device__ __forceinline__ void cursor_load(const BInst &I, SrCursor &c)
+{
+    while (c.sl < c.end)
+    {
+        c.off = I.slice_off[c.sl];
+        c.wd = (int)(I.slice_off[c.sl + 1] - c.off);
+        if (c.wd > 0)
+            return;
+        c.sl += c.step;
+    }
+}
+
+// Issues the cursor's next chunk (lane 0), if any, and advances the cursor: C block slots of
+// values (V) from Kg and their columns.  Whole warp.
+template <typename V, int D, int C>
+__device__ __forceinline__ void pipe_issue_next(const BInst &I, const V *Kg, SrPipe &P, SrCursor &c, uint64_t pf)
+{
+    constexpr int E = D * D;
+    if (c.sl >= c.end)
+        return;
+    const int cn = min(C, c.wd - c.c0);
+    if ((threadIdx.x & 31) == 0)
+    {
+        // the lanes' reads of the buffer (ordered before this lane by the caller's __syncwarp)
+        // come before the copy's writes into it
+        fence_proxy_async_smem();
+        uint64_t *bar = pipe_bar(P, P.n);
+        const uint32_t vb = (uint32_t)(cn * E * kSlice * sizeof(V)), cb = (uint32_t)cn * kSlice * 4;
+        mbar_arrive_expect_tx(bar, vb + cb);
+        bulk_g2s(pipe_vals<V, D>(P, P.n), Kg + (c.off + c.c0) * E * kSlice, vb, bar, pf);
+        bulk_g2s(pipe_cols<D>(P, P.n), I.col_sell + (c.off + c.c0) * kSlice, cb, bar, pf);
+    }
+    P.n++;
+    c.c0 += C;
+    if (c.c0 >= c.wd)
+    {
+        c.c0 = 0;
+        c.sl += c.step;
+        cursor_load(I, c);
+    }
+}
+
+// A slice's offsets and the lane's row, loaded one slice ahead of its use: meta_begin issues the
+// offsets and the row id, meta_finish (after the current slice's chunks) the row's length.
+struct SliceMeta
+{
+    int64_t off;
+    int wd, i, myn;
+};
+
+__device__ __forceinline__ void meta_begin(const BInst &I, int sl, int end, SliceMeta &m)
+{
+    if (sl >= end)
+        return;
+    m.off = I.slice_off[sl];
+    m.wd = (int)(I.slice_off[sl + 1] - m.off);
+    const int pos = sl * kSlice + (threadIdx.x & 31);
+    m.i = pos < I.n ? I.perm[pos] : -1;
+}
+
+__device__ __forceinline__ void meta_finish(const BInst &I, SliceMeta &m)
+{
+    m.myn = m.i >= 0 ? (I.rowptr[m.i + 1] - I.rowptr[m.i]) : 0;
+}
+
+// The warp's slices s_first, s_first + s_step, ... < s_end of one piece in one phase (the work
+// of sr_slice for each), their block values and columns arriving by bulk copies.
+template <int D, bool INIT>
+__device__ void sr_slices_pipe(const BInst &I, int s_first, int s_step, int s_end, int cur, bool fresh, float alpha,
+                               float beta, uint64_t pf, uint64_t pl, double &lg, double &ld, SrPipe &P)
+{
+    constexpr int E = D * D, C = kPipeSlots<D>;
+    if (s_first >= s_end || !P.ok)
+        return;
+    const int lane = threadIdx.x & 31;
+    const float *gr, *gw, *gs;
+    sr_sources(I, INIT, cur, fresh, &gr, &gw, &gs);
+    SrCursor cur_i{s_first, s_step, s_end, 0, 0, 0};
+    cursor_load(I, cur_i);
+    uint32_t m = P.n; // next chunk to consume
+    const float *Kg = static_cast<const float *>(I.K);
+    pipe_issue_next<float, D, C>(I, Kg, P, cur_i, pf);
+    pipe_issue_next<float, D, C>(I, Kg, P, cur_i, pf);
+    SliceMeta cm{0, 0, -1, 0}, nm{0, 0, -1, 0};
+    meta_begin(I, s_first, s_end, cm);
+    meta_finish(I, cm);
+    for (int sl = s_first; sl < s_end; sl += s_step)
+    {
+        const int wd = cm.wd, i = cm.i, myn = cm.myn;
+        meta_begin(I, sl + s_step, s_end, nm);
+        float acc[D];
+#pragma unroll
+        for (int c = 0; c < D; ++c)
+            acc[c] = 0.0f;
+        for (int c0 = 0; c0 < wd; c0 += C)
+        {
+            const int cn = min(C, wd - c0);
+            if (!pipe_wait(P, m))
+                return;
+            const float *kv = pipe_vals<float, D>(P, m);
+            const int *cv = pipe_cols<D>(P, m);
+            float xv[C][D];
+#pragma unroll
+            for (int t = 0; t < C; ++t)
+                if (t < cn && c0 + t < myn)
+                {
+                    const int j = cv[t * kSlice + lane];
+#pragma unroll
+                    for (int c = 0; c < D; ++c)
+                    {
+                        const int64_t q = (int64_t)j * D + c;
+                        if (INIT)
+                            xv[t][c] = ld_keep(gr + q, pl);
+                        else
+                            xv[t][c] = ld_keep(gr + q, pl) - alpha * (ld_keep(gw + q, pl) + beta * ld_keep(gs + q, pl));
+                    }
+                }
+#pragma unroll
+            for (int t = 0; t < C; ++t)
+                if (t < cn && c0 + t < myn)
+#pragma unroll
+                    for (int rr = 0; rr < D; ++rr)
+#pragma unroll
+                        for (int c = 0; c < D; ++c)
+                            acc[rr] += kv[(t * E + rr * D + c) * kSlice + lane] * xv[t][c];
+            ++m;
+            __syncwarp();
+            // the buffer just read takes the chunk two ahead
+            pipe_issue_next<float, D, C>(I, Kg, P, cur_i, pf);
+        }
+        if (sl + s_step < s_end)
+            meta_finish(I, nm);
+        sr_row<D, INIT>(I, i, acc, cur, fresh, alpha, beta, pl, lg, ld);
+        cm = nm;
+    }
+}
+
+// The true residual of a refinement for the warp's slices s_first, s_first + s_step, ... < s_end
+// of one piece (the work of refine_residual for each row: r64 = res - K64 x64, then r32 =
+// (float) r64, x32 = 0, p = 0), the FP64 block values and columns arriving by bulk copies.  The
+// thread's shares of ||r64||^2 and ||(float) r64||^2 are added to v1, v2.
+template <int D>
+__device__ void res_slices_pipe(const BInst &I, int s_first, int s_step, int s_end, uint64_t pf, uint64_t pl, double &v1,
+                                double &v2, SrPipe &P)
+{
+    constexpr int E = D * D, C = kPipeSlots64<D>;
+    if (s_first >= s_end || !P.ok)
+        return;
+    const int lane = threadIdx.x & 31;
+    float *x32 = static_cast<float *>(I.x), *r32 = static_cast<float *>(I.r), *pa = static_cast<float *>(I.pa);
+    SrCursor cur_i{s_first, s_step, s_end, 0, 0, 0};
+    cursor_load(I, cur_i);
+    uint32_t m = P.n;
+    const double *Kg = I.K64;
+    pipe_issue_next<double, D, C>(I, Kg, P, cur_i, pf);
+    pipe_issue_next<double, D, C>(I, Kg, P, cur_i, pf);
+    SliceMeta cm{0, 0, -1, 0}, nm{0, 0, -1, 0};
+    meta_begin(I, s_first, s_end, cm);
+    meta_finish(I, cm);
+    for (int sl = s_first; sl < s_end; sl += s_step)
+    {
+        const int wd = cm.wd, i = cm.i, myn = cm.myn;
+        meta_begin(I, sl + s_step, s_end, nm);
+        double acc[D];
+#pragma unroll
+        for (int c = 0; c < D; ++c)
+            acc[c] = 0.0;
+        for (int c0 = 0; c0 < wd; c0 += C)
+        {
+            const int cn = min(C, wd - c0);
+            if (!pipe_wait(P, m))
+                return;
+            const double *kv = pipe_vals<double, D>(P, m);
+            const int *cv = pipe_cols<D>(P, m);
+            double xv[C][D];
+#pragma unroll
+            for (int t = 0; t < C; ++t)
+                if (t < cn && c0 + t < myn)
+                {
+                    const int j = cv[t * kSlice + lane];
+#pragma unroll
+                    for (int c = 0; c < D; ++c)
+                        xv[t][c] = ld_keep(I.x64 + (int64_t)j * D + c, pl);
+                }
+#pragma unroll
+            for (int t = 0; t < C; ++t)
+                if (t < cn && c0 + t < myn)
+#pragma unroll
+                    for (int rr = 0; rr < D; ++rr)
+#pragma unroll
+                        for (int c = 0; c < D; ++c)
+                            acc[rr] += kv[(t * E + rr * D + c) * kSlice + lane] * xv[t][c];
+            ++m;
+            __syncwarp();
+            pipe_issue_next<double, D, C>(I, Kg, P, cur_i, pf);
+        }
+        if (sl + s_step < s_end)
+            meta_finish(I, nm);
+        if (i >= 0)
+#pragma unroll
+            for (int c = 0; c < D; ++c)
+            {
+                const int64_t k = (int64_t)i * D + c;
+                const double v = I.res[k] - acc[c];
+                I.r64[k] = v;
+                v1 += v * v;
+                const float f = (float)v;
+                st_keep(r32 + k, f, pl);
+                st_keep(x32 + k, 0.0f, pl);
+                st_keep(pa + k, 0.0f, pl);
+                v2 += (double)f * (double)f;
+            }
+        cm = nm;
+    }
+}
+
 // One phase of a member's piece (slices [s0, s1)) in mode 0 (INIT false: iteration k of parity
 // cur) or mode 3/6 (INIT: w_0 = A r_0, the solve's opening; fresh: r_0 = b).  Whole block; with
 // fewer slices than warps several warps share a slice (column split through `red`).  Returns
@@ -1142,19 +1425,38 @@ __device__ void sr_reduce_decide(const BArgs &a, BShared &S, int64_t ph, double 
 }
 
 // UV: 2 x 2 FP32 steps in flight per warp in the 2D SpMV (1 or 2); 2 needs 128 registers, so its
-// blocks have 512 threads, against 768 at 80 registers for 1
+// blocks have 512 threads, against 768 at 80 registers for 1.  PIPE: the flat phases' SpMV is fed by
+// bulk copies (sr_slices_pipe; 384 threads at up to 168 registers, the 8-slot chunks' gathers in
+// flight without spills; each warp with its region after the shared state).
 template <int UV>
 constexpr int kSrThreads = UV == 2 ? 512 : 768;
+// Kernel 3 keeps only the first kPipeFlatPieces x 64 doubles of the union's per-(piece, warp)
+// partials (a flat phase needs np <= kPipeFlatPieces), so its union ends with the staged partials
+// and the warps' copy buffers follow.
+constexpr int kPipeFlatPieces = 16;
+constexpr size_t kPipeUnionBytes = sizeof(double) * 3 * kMaxStage;
+static_assert(kPipeUnionBytes >= sizeof(float) * 32 * 3 * 32 && kPipeUnionBytes >= sizeof(double) * kPipeFlatPieces * 64,
+              "the union's other members fit");
+constexpr size_t kSrPipeOffset = ((sizeof(BShared) + 15) / 16 * 16 + kPipeUnionBytes + 127) / 128 * 128;
+static_assert(kSrPipeOffset + (kSrPipeThreads / 32) * kPipeWarpBytes <= 232448, "shared memory of kernel 3");
 
-template <int UV>
-__global__ void __launch_bounds__(kSrThreads<UV>, kCGMinBlocks) k_cg_batch_sr(BArgs a)
+template <int UV, bool PIPE>
+__global__ void __launch_bounds__(PIPE ? kSrPipeThreads : kSrThreads<UV>, kCGMinBlocks) k_cg_batch_sr(BArgs a)
 {
-    extern __shared__ __align__(16) unsigned char dsm[];
+    extern __shared__ __align__(128) unsigned char dsm[];
     BShared &S = *reinterpret_cast<BShared *>(dsm);
     BUnion<float> &Un = *reinterpret_cast<BUnion<float> *>(dsm + kBSharedBytes);
     __shared__ double sh[32];
     __shared__ int s_fail;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31, nw = blockDim.x >> 5;
+    SrPipe pipe{dsm + kSrPipeOffset + (size_t)warp * kPipeWarpBytes, 0u, true};
+    if constexpr (PIPE)
+        if (lane == 0)
+        {
+            mbar_init(pipe_bar(pipe, 0), 1);
+            mbar_init(pipe_bar(pipe, 1), 1);
+            mbar_init_fence();
+        }
     if (t == 0)
     {
         s_fail = 0;
@@ -1185,15 +1487,15 @@ __global__ void __launch_bounds__(kSrThreads<UV>, kCGMinBlocks) k_cg_batch_sr(BA
     for (int64_t ph = 0; S.nact > 0; ++ph)
     {
         double *const P0 = a.part + (size_t)(2 * (ph & 1)) * kMaxVirt, *const P1 = P0 + kMaxVirt;
-        // slices of this block's pieces in a CG phase (opening or iteration)
+        // slices of this block's pieces in a CG phase (opening or iteration), and with PIPE in a
+        // refinement's true residual
+        auto listed = [](int md) { return md == 0 || md == 3 || md == 6 || (PIPE && md == 2); };
         int T = 0;
         for (int k = 0; k < S.np; ++k)
-        {
-            const int md = S.mode[S.act[S.pr_lo + k]];
-            if (md == 0 || md == 3 || md == 6)
+            if (listed(S.mode[S.act[S.pr_lo + k]]))
                 T += S.ps1[k] - S.ps0[k];
-        }
-        const bool flat = 2 * T > nw && S.np <= kMaxBatch / 2;
+        constexpr int kFlatPieces = PIPE ? kPipeFlatPieces : kMaxBatch / 2;
+        const bool flat = 2 * T > nw && S.np <= kFlatPieces;
         for (int k = 0; k < S.np; ++k)
         {
             const int r = S.pr_lo + k, m = S.act[r], pidx = S.vs[r] + (int)blockIdx.x - S.fb[r];
@@ -1205,10 +1507,10 @@ __global__ void __launch_bounds__(kSrThreads<UV>, kCGMinBlocks) k_cg_batch_sr(BA
                 refine_add<float>(I, S.ps0[k], S.ps1[k]);
                 continue;
             }
+            if (flat && listed(md))
+                continue; // dealt below
             if (md == 2)
                 g = refine_residual<float>(I, S.ps0[k], S.ps1[k], pf, pl, &d);
-            else if (flat)
-                continue; // dealt below
             else
             {
                 const bool init = md != 0;
@@ -1228,37 +1530,65 @@ __global__ void __launch_bounds__(kSrThreads<UV>, kCGMinBlocks) k_cg_batch_sr(BA
         {
             // one list of all those slices, dealt round-robin to the warps across the pieces; each
             // warp leaves one (gamma, delta) pair per piece, summed per piece after one block sync
-            double *wg = Un.wpart, *wd = Un.wpart + (kMaxBatch / 2) * 32;
+            double *wg = Un.wpart, *wd = Un.wpart + kFlatPieces * 32;
             int off = 0;
             for (int k = 0; k < S.np; ++k)
             {
                 const int m = S.act[S.pr_lo + k];
                 const int md = S.mode[m];
-                if (md != 0 && md != 3 && md != 6)
+                if (!listed(md))
                     continue;
                 const BInst &I = a.inst[m];
                 const int nk = S.ps1[k] - S.ps0[k];
                 const int cur = (int)(S.cit[m] & 1);
                 const float al = (float)S.alpha[m], be = (float)S.beta[m];
                 double lg = 0, ld = 0;
-                for (int q = (warp - off % nw + nw) % nw; q < nk; q += nw)
+                const int q0 = (warp - off % nw + nw) % nw;
+                if constexpr (PIPE)
                 {
-                    const int sl = S.ps0[k] + q;
-                    if (I.dim == 2)
+                    const int s_first = S.ps0[k] + q0, s_end = S.ps1[k];
+                    if (md == 2)
+                    {
+                        // lg, ld: the shares of ||r64||^2 and ||(float) r64||^2
+                        if (I.dim == 2)
+                            res_slices_pipe<2>(I, s_first, nw, s_end, pf, pl, lg, ld, pipe);
+                        else
+                            res_slices_pipe<3>(I, s_first, nw, s_end, pf, pl, lg, ld, pipe);
+                    }
+                    else if (I.dim == 2)
                     {
                         if (md == 0)
-                            sr_slice<2, false, UV>(I, sl, cur, false, al, be, pf, pl, lg, ld);
+                            sr_slices_pipe<2, false>(I, s_first, nw, s_end, cur, false, al, be, pf, pl, lg, ld, pipe);
                         else
-                            sr_slice<2, true, UV>(I, sl, 0, md == 6, 0.0f, 0.0f, pf, pl, lg, ld);
+                            sr_slices_pipe<2, true>(I, s_first, nw, s_end, 0, md == 6, 0.0f, 0.0f, pf, pl, lg, ld, pipe);
                     }
                     else
                     {
                         if (md == 0)
-                            sr_slice<3, false, UV>(I, sl, cur, false, al, be, pf, pl, lg, ld);
+                            sr_slices_pipe<3, false>(I, s_first, nw, s_end, cur, false, al, be, pf, pl, lg, ld, pipe);
                         else
-                            sr_slice<3, true, UV>(I, sl, 0, md == 6, 0.0f, 0.0f, pf, pl, lg, ld);
+                            sr_slices_pipe<3, true>(I, s_first, nw, s_end, 0, md == 6, 0.0f, 0.0f, pf, pl, lg, ld, pipe);
                     }
                 }
+                else
+                    for (int q = q0; q < nk; q += nw)
+                    {
+                        const int sl = S.ps0[k] + q;
+                        if (I.dim == 2)
+                        {
+                            if (md == 0)
+                                sr_slice<2, false, UV>(I, sl, cur, false, al, be, pf, pl, lg, ld);
+                            else
+                                sr_slice<2, true, UV>(I, sl, 0, md == 6, 0.0f, 0.0f, pf, pl, lg, ld);
+                        }
+                        else
+                        {
+                            if (md == 0)
+                                sr_slice<3, false, UV>(I, sl, cur, false, al, be, pf, pl, lg, ld);
+                            else
+                                sr_slice<3, true, UV>(I, sl, 0, md == 6, 0.0f, 0.0f, pf, pl, lg, ld);
+                        }
+                    }
                 lg = wsum(lg);
                 ld = wsum(ld);
                 if (lane == 0)
@@ -1272,8 +1602,7 @@ __global__ void __launch_bounds__(kSrThreads<UV>, kCGMinBlocks) k_cg_batch_sr(BA
             for (int k = warp; k < S.np; k += nw)
             {
                 const int r = S.pr_lo + k;
-                const int md = S.mode[S.act[r]];
-                if (md != 0 && md != 3 && md != 6)
+                if (!listed(S.mode[S.act[r]]))
                     continue;
                 const double tg = wsum(lane < nw ? wg[k * 32 + lane] : 0.0);
                 const double td = wsum(lane < nw ? wd[k * 32 + lane] : 0.0);
@@ -1284,6 +1613,12 @@ __global__ void __launch_bounds__(kSrThreads<UV>, kCGMinBlocks) k_cg_batch_sr(BA
                     P1[pidx] = td;
                 }
             }
+        }
+        if (PIPE && !pipe.ok && lane == 0)
+        {
+            // a chunk's copy did not complete in time: every block leaves at this barrier
+            atomicExch(&a.ctl->fail, 1);
+            s_fail = 1;
         }
         if (!batch_barrier(a.ctl, epoch, &s_fail))
             return;
@@ -1336,8 +1671,10 @@ struct BatchCtx
     int device = 0, num_sms = 0, grid = 0;
     int64_t slice = 512; // CG iterations per launch before unfinished solves pause
     size_t smem64 = 0, smem32 = 0; // dynamic shared memory of the two kernel variants
-    int sr = 1; // FP32 inner solves: 1, 2 the single-reduction kernel with 1 or 2 SpMV steps in flight
-                // (768 or 512 threads a block); 0 the two-reduction kernel (LPMGPU_BATCH_SR fixes it)
+    size_t smem_pipe = 0;          // and of the bulk-copy-fed single-reduction kernel
+    int sr = 3; // FP32 inner solves: 1, 2 the single-reduction kernel with 1 or 2 SpMV steps in flight
+                // (768 or 512 threads a block); 3 the same with its flat phases fed by bulk copies
+                // (384 threads); 0 the two-reduction kernel (LPMGPU_BATCH_SR fixes it)
     // The batch's own tuner of that choice, per launch size: a launch whose members' FP32 matrices
     // total under kSmallVolume bytes is bound by the per-iteration floor (barriers and decision
     // passes), a larger one by the matrix stream, and the best kernel differs between the two.
@@ -1346,11 +1683,12 @@ struct BatchCtx
     // large launch is scored by its matrix work (iterations x the members' matrix volume) per
     // second of kernel time; a small one, whose time is its iterations times the floor whatever the
     // members' sizes, by the iterations of its longest solve per second.
-    static constexpr int kTuneLaunches = 9;
+    static constexpr int kKernels = 4;
+    static constexpr int kTuneLaunches = 3 * kKernels;
     static constexpr double kSmallVolume = 64e6;
     bool tuning[2] = {false, false};
-    int tune_n[2] = {0, 0}, pick[2] = {1, 1}, launched_sr = 1, launched_cls = 1;
-    double tune_work[2][3] = {{0, 0, 0}, {0, 0, 0}}, tune_secs[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    int tune_n[2] = {0, 0}, pick[2] = {3, 3}, launched_sr = 3, launched_cls = 1;
+    double tune_work[2][kKernels] = {}, tune_secs[2][kKernels] = {};
     double last_ms = 0;
 
     void tune_record(double work, double phases)
@@ -1365,7 +1703,7 @@ struct BatchCtx
         if (++tune_n[c] < kTuneLaunches)
             return;
         double best = -1;
-        for (int v = 0; v < 3; ++v)
+        for (int v = 0; v < kKernels; ++v)
             if (tune_secs[c][v] > 0 && tune_work[c][v] / tune_secs[c][v] > best)
             {
                 best = tune_work[c][v] / tune_secs[c][v];
@@ -1396,18 +1734,21 @@ struct BatchCtx
             return e;
         smem64 = batch_smem_bytes<double>();
         smem32 = batch_smem_bytes<float>();
+        smem_pipe = kSrPipeOffset + (size_t)(kSrPipeThreads / 32) * kPipeWarpBytes;
         {
             const char *env = std::getenv("LPMGPU_BATCH_SR");
-            sr = env ? std::atoi(env) : 1;
-            if (sr < 0 || sr > 2)
-                sr = 1;
+            sr = env ? std::atoi(env) : 3;
+            if (sr < 0 || sr >= kKernels)
+                sr = 3;
             pick[0] = pick[1] = sr;
             tuning[0] = tuning[1] = env == nullptr;
         }
-        if ((e = cudaFuncSetAttribute(k_cg_batch_sr<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32)) !=
-                cudaSuccess ||
-            (e = cudaFuncSetAttribute(k_cg_batch_sr<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32)) !=
-                cudaSuccess)
+        if ((e = cudaFuncSetAttribute(k_cg_batch_sr<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem32)) != cudaSuccess ||
+            (e = cudaFuncSetAttribute(k_cg_batch_sr<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem32)) != cudaSuccess ||
+            (e = cudaFuncSetAttribute(k_cg_batch_sr<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem_pipe)) != cudaSuccess)
             return e;
         if ((e = cudaFuncSetAttribute(k_cg_batch<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem64)) != cudaSuccess ||
@@ -1421,13 +1762,15 @@ struct BatchCtx
         if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ32, k_cg_batch<float, float>, kBatchThreads<float>,
                                                                 smem32)) != cudaSuccess)
             return e;
-        int occsr1 = 0, occsr2 = 0;
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occsr1, k_cg_batch_sr<1>, kSrThreads<1>, smem32)) !=
-                cudaSuccess ||
-            (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occsr2, k_cg_batch_sr<2>, kSrThreads<2>, smem32)) !=
-                cudaSuccess)
+        int occsr1 = 0, occsr2 = 0, occsr3 = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occsr1, k_cg_batch_sr<1, false>, kSrThreads<1>,
+                                                                smem32)) != cudaSuccess ||
+            (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occsr2, k_cg_batch_sr<2, false>, kSrThreads<2>,
+                                                                smem32)) != cudaSuccess ||
+            (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occsr3, k_cg_batch_sr<1, true>, kSrPipeThreads,
+                                                                smem_pipe)) != cudaSuccess)
             return e;
-        occ32 = std::min({occ32, occsr1, occsr2});
+        occ32 = std::min({occ32, occsr1, occsr2, occsr3});
         grid = std::min(1024, num_sms * std::max(1, std::min({occ64, occ32, kCGMinBlocks})));
         if (grid_cap > 0)
             grid = std::max(1, std::min(grid, grid_cap));
@@ -1556,12 +1899,12 @@ struct BatchCtx
                 h_st[m].status &= ~int64_t(8);
             }
         }
-        static constexpr int kCand[3] = {1, 2, 0};
+        static constexpr int kCand[kKernels] = {3, 1, 2, 0};
         double volume = 0;
         for (int m = 0; m < ni; ++m)
             volume += 4.0 * (double)h_inst[m].cost;
         const int cls = volume < kSmallVolume ? 0 : 1;
-        const int use = (fp32 && tuning[cls]) ? kCand[tune_n[cls] % 3] : pick[cls];
+        const int use = (fp32 && tuning[cls]) ? kCand[tune_n[cls] % kKernels] : pick[cls];
         launched_sr = use;
         launched_cls = cls;
         if (fp32)
@@ -1600,9 +1943,11 @@ struct BatchCtx
         void *args[] = {&a};
         if ((e = cudaEventRecord(ev_t0, stream)) != cudaSuccess)
             return e;
-        e = (fp32 && use == 1) ? cudaLaunchCooperativeKernel((const void *)k_cg_batch_sr<1>, dim3(grid),
-                                                            dim3(kSrThreads<1>), args, smem32, stream)
-            : (fp32 && use == 2) ? cudaLaunchCooperativeKernel((const void *)k_cg_batch_sr<2>, dim3(grid),
+        e = (fp32 && use == 3) ? cudaLaunchCooperativeKernel((const void *)k_cg_batch_sr<1, true>, dim3(grid),
+                                                            dim3(kSrPipeThreads), args, smem_pipe, stream)
+            : (fp32 && use == 1) ? cudaLaunchCooperativeKernel((const void *)k_cg_batch_sr<1, false>, dim3(grid),
+                                                              dim3(kSrThreads<1>), args, smem32, stream)
+            : (fp32 && use == 2) ? cudaLaunchCooperativeKernel((const void *)k_cg_batch_sr<2, false>, dim3(grid),
                                                               dim3(kSrThreads<2>), args, smem32, stream)
             : fp32 ? cudaLaunchCooperativeKernel((const void *)k_cg_batch<float, float>, dim3(grid), dim3(kBatchThreads<float>),
                                                args, smem32, stream)
@@ -2503,8 +2848,7 @@ static int32_t push_member(lpmgpu_batch *b, std::unique_ptr<Member> m, int32_t *
     // the lane with the least matrix volume among its running members
     const Problem &p = m->h->p;
     m->cost = p.nsb * (p.dim * p.dim + 1);
-    const int64_t stream_bytes = p.nsb * ((int64_t)p.dim * p.dim * (p.desc.precision == LPMGPU_MIXED ? 4 : 8) + 4);
-    m->solo = b->solo_bytes > 0 && stream_bytes >= b->solo_bytes;
+    m->solo = b->solo_bytes > 0 && cg_stream_bytes(p) >= b->solo_bytes;
     int best = 0;
     for (int l = 1; l < (int)b->lanes.size(); ++l)
         if (b->lanes[l]->cost < b->lanes[best]->cost)

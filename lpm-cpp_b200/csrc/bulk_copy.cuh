@@ -1,0 +1,84 @@
+// Bulk asynchronous copies global -> shared memory (the TMA engine's untiled form,
+// cp.async.bulk) completed through shared-memory mbarriers, as hand-written PTX for sm_100a.
+//
+// Used by the batched CG's FP32 inner solves to stream a warp's stiffness slices into shared
+// memory two chunks ahead of the warp's SpMV, so the matrix stream no longer waits on each
+// step's loads.  Rules kept by every caller: source and destination 16-byte aligned, sizes a
+// multiple of 16 bytes, no cluster multicast, every wait bounded in time.
+#pragma once
+
+#include <cstdint>
+
+namespace lpm
+{
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// an mbarrier expecting `count` arrivals per phase
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// makes initialised mbarriers visible to the asynchronous proxy (the bulk copies)
+__device__ __forceinline__ void mbar_init_fence()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// orders this thread's earlier generic-proxy shared-memory accesses before later async-proxy ones
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// one arrival that also announces `bytes` of copies completing on this phase
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// `bytes` from global src to shared dst, counted on bar's current phase; L2 policy `pol`
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar, uint64_t pol)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, "
+                 "[%3], %4;" ::"r"(smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+// Waits for the phase of parity `parity` to complete, at most limit_ns; false when it did not.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, unsigned long long limit_ns)
+{
+    if (mbar_try_wait(bar, parity))
+        return true;
+    unsigned long long t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (;;)
+    {
+        if (mbar_try_wait(bar, parity))
+            return true;
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 > limit_ns)
+            return false;
+    }
+}
+
+} // namespace lpm

@@ -54,8 +54,9 @@ struct Scalars
 // partner id (assembly.h:218-229).
 //
 // The stiffness is full symmetric and stored sliced-ELL: particle rows are ordered by
-// descending connection count (perm: position -> id, stable, so equal counts keep id order),
-// grouped in slices of kSlice rows; slice s holds width(s) = its longest row's count of block
+// descending connection count (stable, so equal counts keep id order) and grouped in slices of
+// kSlice rows; in 2D the slices are then reordered whole so that each width is spread evenly
+// over the slice order (perm: position -> id).  Slice s holds width(s) = its longest row's count of block
 // columns starting at block slot slice_off[s].  Block slot b, entry e = r*d + c (row-major d x d)
 // of the row at lane l lives at K[(b*d*d + e)*kSlice + l]; its particle column at
 // col_sell[b*kSlice + l].  A row's k-th block is its k-th connection (ascending id).  A warp
@@ -242,6 +243,13 @@ cudaError_t dalloc(Problem &p, T **ptr, size_t count)
 }
 
 inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+// Bytes of matrix one CG iteration of the problem streams: its sliced-ELL block slots (nsb per
+// lane of a 32-row slice), each d*d values in the CG's precision (FP32 for mixed) and a column.
+inline int64_t cg_stream_bytes(const Problem &p)
+{
+    return p.nsb * kSlice * ((int64_t)p.dim * p.dim * (p.desc.precision == LPMGPU_MIXED ? 4 : 8) + 4);
+}
 
 } // namespace lpm
 

@@ -212,7 +212,7 @@ struct lpmgpu_server
             }
             r->h = h;
             r->bytes = sz.device_bytes;
-            r->volume = sz.nnzb * ((int64_t)sz.dim * sz.dim * (r->desc.precision == LPMGPU_MIXED ? 4 : 8) + 4);
+            r->volume = lpm::cg_stream_bytes(h->p);
             used += r->bytes;
             peak = std::max(peak, used);
             // the description's host arrays were only needed by lpmgpu_create
