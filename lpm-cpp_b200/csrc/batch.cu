@@ -1687,28 +1687,48 @@ struct BatchCtx
     static constexpr int kTuneLaunches = 3 * kKernels;
     static constexpr double kSmallVolume = 64e6;
     bool tuning[2] = {false, false};
-    int tune_n[2] = {0, 0}, pick[2] = {3, 3}, launched_sr = 3, launched_cls = 1;
-    double tune_work[2][kKernels] = {}, tune_secs[2][kKernels] = {};
+    static constexpr int kTunePerKernel = kTuneLaunches / kKernels;
+    static constexpr double kTuneMinPhases = 64; // shorter launches say little: not counted
+    int tune_n[2] = {0, 0}, tune_seen[2] = {0, 0}, pick[2] = {3, 3}, launched_sr = 3, launched_cls = 1;
+    double tune_score[2][kKernels][kTunePerKernel] = {};
     double last_ms = 0;
 
+    // Each counted launch scores its kernel (work per kernel second); a kernel's score is the
+    // median of its kTunePerKernel launches, robust to one launch that caught an unusual mix.
     void tune_record(double work, double phases)
     {
         const int c = launched_cls;
-        if (!tuning[c])
+        if (!tuning[c] || last_ms <= 0)
+            return;
+        // after three rounds' worth of launches the tuner stops with what it has
+        const bool late = ++tune_seen[c] >= 3 * kTuneLaunches;
+        if (phases < kTuneMinPhases && !late)
             return;
         if (c == 0)
             work = phases;
-        tune_work[c][launched_sr] += work;
-        tune_secs[c][launched_sr] += last_ms * 1e-3;
-        if (++tune_n[c] < kTuneLaunches)
+        const int v = launched_sr, slot = tune_n[c] / kKernels;
+        if (phases >= kTuneMinPhases && slot < kTunePerKernel)
+            tune_score[c][v][slot] = work / (last_ms * 1e-3);
+        if (++tune_n[c] < kTuneLaunches && !late)
             return;
         double best = -1;
-        for (int v = 0; v < kKernels; ++v)
-            if (tune_secs[c][v] > 0 && tune_work[c][v] / tune_secs[c][v] > best)
+        for (int k = 0; k < kKernels; ++k)
+        {
+            double sc[kTunePerKernel];
+            int m = 0;
+            for (int q = 0; q < kTunePerKernel; ++q)
+                if (tune_score[c][k][q] > 0)
+                    sc[m++] = tune_score[c][k][q];
+            if (m == 0)
+                continue;
+            std::sort(sc, sc + m);
+            const double med = sc[m / 2];
+            if (med > best)
             {
-                best = tune_work[c][v] / tune_secs[c][v];
-                pick[c] = v;
+                best = med;
+                pick[c] = k;
             }
+        }
         tuning[c] = false;
     }
 
