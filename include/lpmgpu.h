@@ -389,8 +389,9 @@ typedef struct
     double cg_kernel_seconds;    /* device time of the batched CG launches */
     int32_t fp32_kernel;         /* the mixed members' CG kernel for launches whose FP32 matrices
                                     total 64 MB or more: 1, 2 single reduction with 1 or 2 SpMV steps
-                                    in flight, 0 two reductions (the batch's tuner picks it over its
-                                    first launches unless LPMGPU_BATCH_SR fixes it) */
+                                    in flight, 3 single reduction with the matrix streamed into
+                                    shared memory by bulk copies, 0 two reductions (the batch's tuner
+                                    picks it over its first launches unless LPMGPU_BATCH_SR fixes it) */
     int32_t fp32_kernel_small;   /* the same for smaller launches */
     int32_t fp32_tuning;         /* 1 while the tuner is still trying the kernels */
     int32_t pad;
