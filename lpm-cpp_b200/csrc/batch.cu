@@ -1675,17 +1675,18 @@ struct BatchCtx
     int sr = 3; // FP32 inner solves: 1, 2 the single-reduction kernel with 1 or 2 SpMV steps in flight
                 // (768 or 512 threads a block); 3 the same with its flat phases fed by bulk copies
                 // (384 threads); 0 the two-reduction kernel (LPMGPU_BATCH_SR fixes it)
-    // The batch's own tuner of that choice, per launch size: a launch whose members' FP32 matrices
-    // total under kSmallVolume bytes is bound by the per-iteration floor (barriers and decision
-    // passes), a larger one by the matrix stream, and the best kernel differs between the two.
-    // Unless LPMGPU_BATCH_SR is set, the first kTuneLaunches FP32 launches of each size cycle
-    // through the three kernels and the best kernel serves every later launch of that size.  A
-    // large launch is scored by its matrix work (iterations x the members' matrix volume) per
-    // second of kernel time; a small one, whose time is its iterations times the floor whatever the
-    // members' sizes, by the iterations of its longest solve per second.
+    // The batch's own tuner of that choice, per launch size: a launch with fewer than kSmallSlices
+    // slices per block runs its phases on the column-split path and is bound by the per-iteration
+    // floor (barriers, decision passes, one slice's gather chain); a larger one runs the flat
+    // path and is bound by the matrix stream, and the best kernel differs between the two.  Unless
+    // LPMGPU_BATCH_SR is set, the first kTuneLaunches informative FP32 launches of each size cycle
+    // through the kernels and the best serves every later launch of that size.  A large launch is
+    // scored by its matrix work (iterations x the members' matrix volume) per second of kernel
+    // time; a small one, whose time is its iterations times the floor whatever the members' sizes,
+    // by the iterations of its longest solve per second.
     static constexpr int kKernels = 4;
     static constexpr int kTuneLaunches = 3 * kKernels;
-    static constexpr double kSmallVolume = 64e6;
+    static constexpr int kSmallSlices = 24;
     bool tuning[2] = {false, false};
     static constexpr int kTunePerKernel = kTuneLaunches / kKernels;
     static constexpr double kTuneMinPhases = 64; // shorter launches say little: not counted
@@ -1723,6 +1724,9 @@ struct BatchCtx
                 continue;
             std::sort(sc, sc + m);
             const double med = sc[m / 2];
+            if (std::getenv("LPMGPU_LOG"))
+                std::fprintf(stderr, "lpmgpu batch tuner: class %d kernel %d median score %.4g over %d launches\n", c, k,
+                             med, m);
             if (med > best)
             {
                 best = med;
@@ -1920,10 +1924,10 @@ struct BatchCtx
             }
         }
         static constexpr int kCand[kKernels] = {3, 1, 2, 0};
-        double volume = 0;
+        int64_t slices = 0;
         for (int m = 0; m < ni; ++m)
-            volume += 4.0 * (double)h_inst[m].cost;
-        const int cls = volume < kSmallVolume ? 0 : 1;
+            slices += h_inst[m].nslices;
+        const int cls = slices < (int64_t)kSmallSlices * grid ? 0 : 1;
         const int use = (fp32 && tuning[cls]) ? kCand[tune_n[cls] % kKernels] : pick[cls];
         launched_sr = use;
         launched_cls = cls;
