@@ -387,7 +387,7 @@ typedef struct
     int64_t cg_iters, dof_iters; /* over members still held by the batch */
     double seconds;              /* wall time inside lpmgpu_batch_run */
     double cg_kernel_seconds;    /* device time of the batched CG launches */
-    int32_t fp32_kernel;         /* the mixed members' CG kernel for launches with at least 24
+    int32_t fp32_kernel;         /* the mixed members' CG kernel for launches with at least 8
                                     slices of 32 rows per block: 1, 2 single reduction with 1 or 2 SpMV steps
                                     in flight, 3 single reduction with the matrix streamed into
                                     shared memory by bulk copies, 0 two reductions (the batch's tuner

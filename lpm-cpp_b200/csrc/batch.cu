@@ -1686,7 +1686,7 @@ struct BatchCtx
     // by the iterations of its longest solve per second.
     static constexpr int kKernels = 4;
     static constexpr int kTuneLaunches = 3 * kKernels;
-    static constexpr int kSmallSlices = 24;
+    static constexpr int kSmallSlices = 8;
     bool tuning[2] = {false, false};
     static constexpr int kTunePerKernel = kTuneLaunches / kKernels;
     static constexpr double kTuneMinPhases = 64; // shorter launches say little: not counted
