@@ -4,7 +4,7 @@
 // Used by the batched CG's FP32 inner solves to stream a warp's stiffness slices into shared
 // memory two chunks ahead of the warp's SpMV, so the matrix stream no longer waits on each
 // step's loads.  Rules kept by every caller: source and destination 16-byte aligned, sizes a
-// multiple of 16 bytes, no cluster multicast, every wait bounded in time.
+// multiple of 16 bytes, each copy into this CTA only, every wait bounded in time.
 #pragma once
 
 #include <cstdint>
