@@ -887,6 +887,27 @@ __device__ __forceinline__ void sr_row(const BInst &I, int i, const float *acc, 
     // r_{k+1} to rn_, w_{k+1} to wn
     float *rc = cur ? r1 : r0, *rn_ = cur ? r0 : r1, *wc = cur ? w1 : w0, *wn = cur ? w0 : w1;
     float *sc = cur ? s1b : s0b, *sp = cur ? s0b : s1b;
+    if constexpr (D == 2)
+        if (!INIT)
+        {
+            // the same arithmetic on both components, each vector moved 8 bytes at a time
+            const int64_t k = (int64_t)i * 2;
+            const float2 w2 = ld_keep2(wc + k, pl), s2 = ld_keep2(sp + k, pl), r2 = ld_keep2(rc + k, pl);
+            const float2 p2 = ld_keep2(p + k, pl), x2 = ld_keep2(x + k, pl);
+            const float2 sk = make_float2(w2.x + beta * s2.x, w2.y + beta * s2.y);
+            const float2 pk = make_float2(r2.x + beta * p2.x, r2.y + beta * p2.y);
+            st_keep2(x + k, make_float2(x2.x + alpha * pk.x, x2.y + alpha * pk.y), pl);
+            const float2 rn = make_float2(r2.x - alpha * sk.x, r2.y - alpha * sk.y);
+            st_keep2(sc + k, sk, pl);
+            st_keep2(p + k, pk, pl);
+            st_keep2(rn_ + k, rn, pl);
+            st_keep2(wn + k, make_float2(acc[0], acc[1]), pl);
+            lg += (double)rn.x * (double)rn.x;
+            ld += (double)acc[0] * (double)rn.x;
+            lg += (double)rn.y * (double)rn.y;
+            ld += (double)acc[1] * (double)rn.y;
+            return;
+        }
 #pragma unroll
     for (int c = 0; c < D; ++c)
     {
@@ -1119,15 +1140,34 @@ __device__ void sr_slices_pipe(const BInst &I, int s_first, int s_step, int s_en
                 if (t < cn && c0 + t < myn)
                 {
                     const int j = cv[t * kSlice + lane];
-#pragma unroll
-                    for (int c = 0; c < D; ++c)
+                    if constexpr (D == 2)
                     {
-                        const int64_t q = (int64_t)j * D + c;
+                        // a 2D particle's two components in one 8-byte load per vector
+                        const int64_t q = (int64_t)j * 2;
+                        const float2 rv = ld_keep2(gr + q, pl);
                         if (INIT)
-                            xv[t][c] = ld_keep(gr + q, pl);
+                        {
+                            xv[t][0] = rv.x;
+                            xv[t][1] = rv.y;
+                        }
                         else
-                            xv[t][c] = ld_keep(gr + q, pl) - alpha * (ld_keep(gw + q, pl) + beta * ld_keep(gs + q, pl));
+                        {
+                            const float2 wv = ld_keep2(gw + q, pl), sv = ld_keep2(gs + q, pl);
+                            xv[t][0] = rv.x - alpha * (wv.x + beta * sv.x);
+                            xv[t][1] = rv.y - alpha * (wv.y + beta * sv.y);
+                        }
                     }
+                    else
+#pragma unroll
+                        for (int c = 0; c < D; ++c)
+                        {
+                            const int64_t q = (int64_t)j * D + c;
+                            if (INIT)
+                                xv[t][c] = ld_keep(gr + q, pl);
+                            else
+                                xv[t][c] =
+                                    ld_keep(gr + q, pl) - alpha * (ld_keep(gw + q, pl) + beta * ld_keep(gs + q, pl));
+                        }
                 }
 #pragma unroll
             for (int t = 0; t < C; ++t)

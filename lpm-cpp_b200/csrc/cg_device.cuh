@@ -113,6 +113,17 @@ __device__ __forceinline__ float ld_keep(const float *a, uint64_t pol)
     asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol) : "memory");
     return v;
 }
+// two consecutive floats (8-byte aligned) in one load, as ld_keep
+__device__ __forceinline__ float2 ld_keep2(const float *a, uint64_t pol)
+{
+    float2 v;
+    asm volatile("ld.global.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(a), "l"(pol) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_keep2(float *a, float2 v, uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(a), "f"(v.x), "f"(v.y), "l"(pol) : "memory");
+}
 __device__ __forceinline__ void st_keep(double *a, double v, uint64_t pol)
 {
     asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol) : "memory");
