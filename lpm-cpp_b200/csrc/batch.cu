@@ -843,15 +843,32 @@ __device__ __forceinline__ int sr_spmv_slice(int sl, const BInst &I, const float
             const int kk = k + u * kstep;
             if (kk < myn)
             {
-#pragma unroll
-                for (int c = 0; c < D; ++c)
+                if constexpr (D == 2)
                 {
-                    const int64_t q = (int64_t)j[u] * D + c;
+                    const int64_t q = (int64_t)j[u] * 2;
+                    const float2 rv = ld_keep2(r + q, pl);
                     if (INIT)
-                        xv[u][c] = ld_keep(r + q, pl);
+                    {
+                        xv[u][0] = rv.x;
+                        xv[u][1] = rv.y;
+                    }
                     else
-                        xv[u][c] = ld_keep(r + q, pl) - alpha * (ld_keep(w + q, pl) + beta * ld_keep(sv + q, pl));
+                    {
+                        const float2 wv = ld_keep2(w + q, pl), s2 = ld_keep2(sv + q, pl);
+                        xv[u][0] = rv.x - alpha * (wv.x + beta * s2.x);
+                        xv[u][1] = rv.y - alpha * (wv.y + beta * s2.y);
+                    }
                 }
+                else
+#pragma unroll
+                    for (int c = 0; c < D; ++c)
+                    {
+                        const int64_t q = (int64_t)j[u] * D + c;
+                        if (INIT)
+                            xv[u][c] = ld_keep(r + q, pl);
+                        else
+                            xv[u][c] = ld_keep(r + q, pl) - alpha * (ld_keep(w + q, pl) + beta * ld_keep(sv + q, pl));
+                    }
                 const float *kb = kp + (int64_t)kk * E * kSlice;
 #pragma unroll
                 for (int e = 0; e < E; ++e)
