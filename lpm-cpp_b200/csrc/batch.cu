@@ -1249,9 +1249,16 @@ __device__ void res_slices_pipe(const BInst &I, int s_first, int s_step, int s_e
                 if (t < cn && c0 + t < myn)
                 {
                     const int j = cv[t * kSlice + lane];
+                    if constexpr (D == 2)
+                    {
+                        const double2 v = ld_keep2(I.x64 + (int64_t)j * 2, pl);
+                        xv[t][0] = v.x;
+                        xv[t][1] = v.y;
+                    }
+                    else
 #pragma unroll
-                    for (int c = 0; c < D; ++c)
-                        xv[t][c] = ld_keep(I.x64 + (int64_t)j * D + c, pl);
+                        for (int c = 0; c < D; ++c)
+                            xv[t][c] = ld_keep(I.x64 + (int64_t)j * D + c, pl);
                 }
 #pragma unroll
             for (int t = 0; t < C; ++t)

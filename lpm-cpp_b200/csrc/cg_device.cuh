@@ -113,6 +113,13 @@ __device__ __forceinline__ float ld_keep(const float *a, uint64_t pol)
     asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol) : "memory");
     return v;
 }
+// two consecutive doubles (16-byte aligned) in one load, as ld_keep
+__device__ __forceinline__ double2 ld_keep2(const double *a, uint64_t pol)
+{
+    double2 v;
+    asm volatile("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v.x), "=d"(v.y) : "l"(a), "l"(pol) : "memory");
+    return v;
+}
 // two consecutive floats (8-byte aligned) in one load, as ld_keep
 __device__ __forceinline__ float2 ld_keep2(const float *a, uint64_t pol)
 {
